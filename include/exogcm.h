@@ -1,0 +1,178 @@
+/*
+ * exogcm: a B200-native ExoPlaSim spectral-GCM timestep behind a C ABI.
+ *
+ * This header is the drop-in boundary for the engine interface of
+ * ryoung48/web-exoplasim (paths relative to src/model/climate/gcm/):
+ *   - GCM_RUNNER.start / GcmRunRequest / GcmRun (runner/index.ts:61-78,
+ *     runner/types.ts:47-74) drive an engine through configure, step, field
+ *     readback and checkpoint; a host (the TypeScript runner through N-API,
+ *     or any FFI) calls the functions below for those four operations.
+ *   - Every function returns 0 on success or a negative EXOGCM_E* code;
+ *     exogcm_last_error() gives the message (the reference's worker reports
+ *     failures as strings through `fail`, runner/webgpu/gcm.worker.ts:48-51).
+ *   - An engine is used from one host thread at a time. It owns one CUDA
+ *     stream and all device memory; buffers passed in are caller-owned.
+ *
+ * An engine holds `slots` planets of one resolution (truncation T, L levels)
+ * that step together in one batched launch sequence; slots are configured,
+ * stepped, read and released independently (continuous batching).
+ */
+#ifndef EXOGCM_H
+#define EXOGCM_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EXOGCM_OK 0
+#define EXOGCM_EINVAL (-1)     /* invalid argument */
+#define EXOGCM_ENOMEM (-2)     /* device or host allocation failed (admission) */
+#define EXOGCM_EUNSTABLE (-3)  /* a slot's state became non-finite */
+#define EXOGCM_ELAYOUT (-4)    /* checkpoint does not match this layout */
+#define EXOGCM_EDEVICE (-5)    /* CUDA error */
+#define EXOGCM_ESTATE (-6)     /* call not valid in the slot's state */
+
+typedef struct exogcm_engine exogcm_engine;
+
+/* A planet's configuration: the GcmConfig fields the reference turns into
+ * namelist edits (namelist/index.ts:40-182, types.ts:28-62), with the
+ * atmosphere already resolved to a pressure, gas constant and CO2. */
+typedef struct exogcm_planet {
+  int truncation;                /* 21, 42 or 63 */
+  int levels;                    /* 5 or 10 */
+  double radius_earth;           /* planet radius in Earth radii */
+  double gravity;                /* m/s^2 */
+  double flux;                   /* stellar flux, W/m^2 */
+  double eccentricity;
+  double obliquity_deg;
+  int fixed_orbit;               /* 1: orbit as given (NFIXORB = 1) */
+  int keplerian;                 /* NGENKEPLERIAN */
+  int synchronous;               /* tidally locked (NFIXED) */
+  double substellar_longitude_deg;
+  double ocean_depth_m;          /* slab ocean mixed-layer depth */
+  double year_days;
+  double rotation_period_days;
+  double timestep_minutes;
+  double pressure_bar;
+  double gas_constant;           /* J/(kg K) */
+  double co2_ppm;
+  int ozone;
+  int wet_soil;
+  int vegetation;                /* 0, 1 or 2 */
+  double initial_growth;
+  int glaciers;                  /* glacier model on */
+  double glacier_min_depth_m;
+  double glacier_initial_height_m;
+  int filter_gp;                 /* physics filter on grid-to-spectral sums */
+  int filter_sp;                 /* physics filter on spectral-to-grid sums */
+  int filter_kind;               /* NFILTER: 0 none, 1 Cesaro, 2 exp, 3 Landau-Hoskins, 4 */
+  double soil_depth_scale;
+  double star_temperature_k;     /* 0: no stellar-spectrum albedo split */
+} exogcm_planet;
+
+/* Boundary and initial fields on the Gaussian grid (NLAT x 2 NLAT points,
+ * north first), as the reference's .sra inputs (setup/surface/index.ts). */
+typedef struct exogcm_boundary {
+  const double* land_mask;   /* code 172, NHOR values; required */
+  const double* orography;   /* code 129 surface geopotential (m^2/s^2), NHOR; or NULL */
+  const double* sst;         /* code 169, 1 or 12 monthly fields; or NULL */
+  int sst_months;
+  const double* ice_cover;   /* code 210, 1 or 12 monthly fields; or NULL */
+  int ice_cover_months;
+  const double* t_init;      /* initial temperature (K) [levels][NHOR]; required */
+  const double* q_init;      /* initial specific humidity [levels][NHOR]; required */
+} exogcm_boundary;
+
+/* Message of the last failed call on this thread. */
+int exogcm_last_error(char* buffer, size_t size);
+
+/* Creates an engine of `slots` planet slots at T`truncation` L`levels` on
+ * the current CUDA device (STEPPER.context, stepper/index.ts:94-118).
+ * `mode` 0 plain FP32 transforms, 1 split-precision tensor-core transforms. */
+int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine** engine);
+void exogcm_destroy(exogcm_engine* engine);
+
+/* Set-up of one slot in FP64 on the host and upload of its tables and
+ * initial state (SETUP.state / SETUP.schedule, setup/index.ts:434-477;
+ * LAYOUT.write, layout/index.ts:66-71). The slot then runs the reference's
+ * start-up steps before its main loop. */
+int exogcm_configure(exogcm_engine* engine, int slot, const exogcm_planet* planet,
+                     const exogcm_boundary* boundary);
+
+/* Runs the FP64 set-up of exogcm_configure on the host only and returns one
+ * of its arrays, with no device involved (a dry run of configure). `name`
+ * is "state:<field>" (initial state, reference layout), "table:<name>"
+ * (per-planet constant table; bm1 holds the four timestep phases),
+ * "const:<NAME>" (one kernel constant), "shared:<q|fwd|inv|sines|weights>"
+ * (resolution tables; q* are the filtered Legendre tables) or
+ * "calendar:<step>" (that step's 16 host values: radiation_step[5],
+ * surface_step[7], carbon flag, next carbon counter from 0, start step,
+ * start-up steps). `*count` returns the array length; values may be NULL. */
+int exogcm_setup_preview(const exogcm_planet* planet, const exogcm_boundary* boundary, const char* name,
+                         double* values, size_t* count);
+
+/* Frees a slot for another planet (continuous batching). */
+int exogcm_release(exogcm_engine* engine, int slot);
+
+/* Runs `steps` model steps for every active slot (STEPPER.batch,
+ * stepper/index.ts:203-276): per-step CPU values computed on the host,
+ * uploaded once, then the whole batch as one CUDA graph. A slot whose step
+ * number is a multiple of `publish_every` packs its snapshot on that step.
+ * `steps` must not exceed `publish_every` so a slot publishes at most once. */
+int exogcm_step(exogcm_engine* engine, int steps, int publish_every);
+
+/* Snapshot of a slot published during the last exogcm_step (the 101/76
+ * fields of snapshot/index.ts, each NHOR values): returns the step it was
+ * taken at in *step, or -1 when the slot did not publish. `values` may be
+ * NULL to query only. */
+int exogcm_read_snapshot(exogcm_engine* engine, int slot, float* values, size_t count, long* step);
+
+/* Per-slot model step counter and start-up steps still to run. */
+int exogcm_slot_info(exogcm_engine* engine, int slot, long* step, int* startup_left, int* active);
+
+/* Field readback / write by the reference's state field names
+ * (LAYOUT.read / LAYOUT.write), one slot at a time, f32. */
+int exogcm_field_size(exogcm_engine* engine, const char* name, size_t* count);
+int exogcm_read_field(exogcm_engine* engine, int slot, const char* name, float* values, size_t count);
+int exogcm_write_field(exogcm_engine* engine, int slot, const char* name, const float* values, size_t count);
+
+/* Per-slot constant table readback (f32 as the kernels read it). */
+int exogcm_read_table(exogcm_engine* engine, int slot, const char* name, float* values, size_t count);
+
+/* Checkpoint of one slot in the reference's restart format
+ * (checkpoint/restart/index.ts:11-75: magic, JSON header with field names
+ * and counts, step and carbon counter, then every field's f32 values).
+ * Save returns a library-owned buffer released with exogcm_free. Load
+ * rejects a checkpoint whose field list does not match (EXOGCM_ELAYOUT). */
+int exogcm_checkpoint_save(exogcm_engine* engine, int slot, void** buffer, size_t* size);
+int exogcm_checkpoint_load(exogcm_engine* engine, int slot, const void* buffer, size_t size);
+void exogcm_free(void* buffer);
+
+/* Per-slot instability flags (1 = non-finite state seen since the last
+ * clear); the reference stops with "model became unstable at step N"
+ * (runner/webgpu/gcm.worker.ts:317-323). */
+int exogcm_unstable(exogcm_engine* engine, int* flags, int slots);
+
+/* Runs one named stage of the step for every active slot at its current
+ * step without advancing it: gridpointa, spectrala, physics_in, fixer,
+ * surface_flux, radiation, precipitation, surface, carbon, physics_out,
+ * spectrald, pack. For per-routine replay tests (the reference's
+ * scripts/exoplasim-webgpu/verify-dynamics.mjs). */
+int exogcm_run_stage(exogcm_engine* engine, const char* stage);
+
+/* Device time of the last exogcm_step in milliseconds (CUDA events). */
+int exogcm_last_step_ms(exogcm_engine* engine, float* ms);
+
+/* Raw device pointer of a field (slot-major layout [plane][slot][points])
+ * and the engine's CUDA stream, for in-process hosts that keep inputs
+ * resident. */
+int exogcm_device_field(exogcm_engine* engine, const char* name, void** pointer, size_t* floats);
+void* exogcm_stream(exogcm_engine* engine);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EXOGCM_H */

@@ -1,0 +1,274 @@
+"""exogcm: B200-native ExoPlaSim timestep behind the reference's engine interface.
+
+The product is the CUDA library libexogcm.so (csrc/, C ABI in include/exogcm.h).
+This package binds it with ctypes and mirrors the reference's host-side engine
+interface (src/model/climate/gcm/runner/{types,index}.ts): ``Engine`` is the
+configure/step/readback/checkpoint surface of one batch of planet slots, and
+``runner.GCM_RUNNER.start`` the GcmRun control handle on top of it.
+
+There is no CPU fallback: loading fails loudly when the library or a CUDA
+device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libexogcm.so")
+
+EXOGCM_OK = 0
+ERRORS = {-1: "invalid argument", -2: "out of memory", -3: "unstable", -4: "layout mismatch",
+          -5: "device error", -6: "invalid state"}
+
+
+class ExogcmError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+class Planet(ctypes.Structure):
+    """exogcm_planet (include/exogcm.h)."""
+    _fields_ = [
+        ("truncation", ctypes.c_int), ("levels", ctypes.c_int), ("radius_earth", ctypes.c_double),
+        ("gravity", ctypes.c_double), ("flux", ctypes.c_double), ("eccentricity", ctypes.c_double),
+        ("obliquity_deg", ctypes.c_double), ("fixed_orbit", ctypes.c_int), ("keplerian", ctypes.c_int),
+        ("synchronous", ctypes.c_int), ("substellar_longitude_deg", ctypes.c_double),
+        ("ocean_depth_m", ctypes.c_double), ("year_days", ctypes.c_double),
+        ("rotation_period_days", ctypes.c_double), ("timestep_minutes", ctypes.c_double),
+        ("pressure_bar", ctypes.c_double), ("gas_constant", ctypes.c_double), ("co2_ppm", ctypes.c_double),
+        ("ozone", ctypes.c_int), ("wet_soil", ctypes.c_int), ("vegetation", ctypes.c_int),
+        ("initial_growth", ctypes.c_double), ("glaciers", ctypes.c_int), ("glacier_min_depth_m", ctypes.c_double),
+        ("glacier_initial_height_m", ctypes.c_double), ("filter_gp", ctypes.c_int), ("filter_sp", ctypes.c_int),
+        ("filter_kind", ctypes.c_int), ("soil_depth_scale", ctypes.c_double),
+        ("star_temperature_k", ctypes.c_double),
+    ]
+
+
+_DP = ctypes.POINTER(ctypes.c_double)
+
+
+class Boundary(ctypes.Structure):
+    """exogcm_boundary (include/exogcm.h)."""
+    _fields_ = [("land_mask", _DP), ("orography", _DP), ("sst", _DP), ("sst_months", ctypes.c_int),
+                ("ice_cover", _DP), ("ice_cover_months", ctypes.c_int), ("t_init", _DP), ("q_init", _DP)]
+
+
+_lib = None
+
+# Every entry point include/exogcm.h declares: name -> (restype, argtypes).
+_VP = ctypes.c_void_p
+_FP = ctypes.POINTER(ctypes.c_float)
+SIGNATURES = {
+    "exogcm_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
+    "exogcm_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(_VP)]),
+    "exogcm_destroy": (None, [_VP]),
+    "exogcm_configure": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(Planet), ctypes.POINTER(Boundary)]),
+    "exogcm_setup_preview": (ctypes.c_int, [ctypes.POINTER(Planet), ctypes.POINTER(Boundary), ctypes.c_char_p,
+                                            _DP, ctypes.POINTER(ctypes.c_size_t)]),
+    "exogcm_release": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "exogcm_step": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
+    "exogcm_read_snapshot": (ctypes.c_int, [_VP, ctypes.c_int, _FP, ctypes.c_size_t,
+                                            ctypes.POINTER(ctypes.c_long)]),
+    "exogcm_slot_info": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_long),
+                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "exogcm_field_size": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.POINTER(ctypes.c_size_t)]),
+    "exogcm_read_field": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_char_p, _FP, ctypes.c_size_t]),
+    "exogcm_write_field": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_char_p, _FP, ctypes.c_size_t]),
+    "exogcm_read_table": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_char_p, _FP, ctypes.c_size_t]),
+    "exogcm_checkpoint_save": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(_VP),
+                                              ctypes.POINTER(ctypes.c_size_t)]),
+    "exogcm_checkpoint_load": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]),
+    "exogcm_free": (None, [_VP]),
+    "exogcm_unstable": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    "exogcm_run_stage": (ctypes.c_int, [_VP, ctypes.c_char_p]),
+    "exogcm_last_step_ms": (ctypes.c_int, [_VP, _FP]),
+    "exogcm_device_field": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.POINTER(_VP),
+                                           ctypes.POINTER(ctypes.c_size_t)]),
+    "exogcm_stream": (_VP, [_VP]),
+}
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libexogcm.so and binds every declared entry point. Raises when the
+    library is missing: there is no fallback implementation."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build it with web-exoplasim_b200/build.py")
+        lib = ctypes.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _check(code):
+    if code != EXOGCM_OK:
+        buf = ctypes.create_string_buffer(1024)
+        _lib.exogcm_last_error(buf, 1024)
+        raise ExogcmError(code, buf.value.decode())
+
+
+FILTER_KINDS = {"none": 0, "cesaro": 1, "exp": 2, "lh": 3}
+
+
+def planet_struct(config: dict) -> Planet:
+    """exogcm_planet from a GcmConfig-like dict (planets.BASE_CONFIG keys)."""
+    kind = 0
+    gp = sp = 0
+    for f in config.get("physicsFilter", ()):
+        if f == "gp":
+            gp = 1
+        elif f == "sp":
+            sp = 1
+        else:
+            kind = FILTER_KINDS[f]
+    return Planet(
+        truncation=int(config["truncation"]), levels=int(config["layers"]), radius_earth=config["radiusEarth"],
+        gravity=config["gravityMs2"], flux=config["fluxWm2"], eccentricity=config["eccentricity"],
+        obliquity_deg=config["obliquityDeg"], fixed_orbit=int(bool(config["fixedOrbit"])),
+        keplerian=int(bool(config["keplerian"])), synchronous=int(bool(config["synchronous"])),
+        substellar_longitude_deg=config["substellarLongitudeDeg"], ocean_depth_m=config["oceanDepthM"],
+        year_days=float(config["yearDays"]), rotation_period_days=float(config["rotationPeriodDays"]),
+        timestep_minutes=float(config["timestepMinutes"]), pressure_bar=float(config["pressureBar"]),
+        gas_constant=float(config["gasConstant"]), co2_ppm=float(config["co2Ppm"]),
+        ozone=int(bool(config["ozone"])), wet_soil=int(bool(config["wetSoil"])),
+        vegetation=int(config["vegetation"]), initial_growth=float(config["initialGrowth"]),
+        glaciers=int(bool(config["glaciersEnabled"])), glacier_min_depth_m=float(config["glaciersMinDepthM"]),
+        glacier_initial_height_m=float(config["glaciersInitialHeightM"]), filter_gp=gp, filter_sp=sp,
+        filter_kind=kind, soil_depth_scale=float(config["soilDepthScale"]),
+        star_temperature_k=float(config["starTemperatureK"]))
+
+
+def boundary_struct(planet, nhor: int, keep: dict) -> Boundary:
+    """exogcm_boundary for a planets.Planet; `keep` holds the arrays alive."""
+    def ptr(name, a):
+        if a is None:
+            return None
+        arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
+        keep[name] = arr
+        return arr.ctypes.data_as(_DP)
+    bd = planet.boundary
+    sst, ice = bd.get(169), bd.get(210)
+    return Boundary(land_mask=ptr("mask", bd[172]), orography=ptr("oro", bd.get(129)),
+                    sst=ptr("sst", sst), sst_months=0 if sst is None else int(np.size(sst) // nhor),
+                    ice_cover=ptr("ice", ice), ice_cover_months=0 if ice is None else int(np.size(ice) // nhor),
+                    t_init=ptr("t", planet.t_grid), q_init=ptr("q", planet.q_grid))
+
+
+def setup_preview(planet, name: str) -> np.ndarray:
+    """The FP64 set-up array `name` (see exogcm_setup_preview) for a planet,
+    computed on the host without a device."""
+    lib = load_library()
+    nhor = 2 * {21: 32, 42: 64, 63: 96}[planet.config["truncation"]] ** 2
+    keep = {}
+    p = planet_struct(planet.config)
+    b = boundary_struct(planet, nhor, keep)
+    n = ctypes.c_size_t(0)
+    _check(lib.exogcm_setup_preview(ctypes.byref(p), ctypes.byref(b), name.encode(), None, ctypes.byref(n)))
+    out = np.zeros(n.value)
+    _check(lib.exogcm_setup_preview(ctypes.byref(p), ctypes.byref(b), name.encode(), out.ctypes.data_as(_DP),
+                                    ctypes.byref(n)))
+    return out
+
+
+class Engine:
+    """One batch of `slots` planets at one resolution on the current device."""
+
+    def __init__(self, truncation: int, levels: int, slots: int = 1, mode: int = 0):
+        lib = load_library()
+        h = _VP()
+        _check(lib.exogcm_create(truncation, levels, slots, mode, ctypes.byref(h)))
+        self.h = h
+        self.truncation, self.levels, self.slots = truncation, levels, slots
+        self.nlat = {21: 32, 42: 64, 63: 96}[truncation]
+        self.nhor = 2 * self.nlat * self.nlat
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.exogcm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def configure(self, slot: int, planet) -> None:
+        """SETUP + LAYOUT.write for a planets.Planet."""
+        keep = {}
+        p = planet_struct(planet.config)
+        b = boundary_struct(planet, self.nhor, keep)
+        _check(_lib.exogcm_configure(self.h, slot, ctypes.byref(p), ctypes.byref(b)))
+
+    def release(self, slot: int) -> None:
+        _check(_lib.exogcm_release(self.h, slot))
+
+    def step(self, steps: int = 1, publish_every: int | None = None) -> None:
+        _check(_lib.exogcm_step(self.h, steps, publish_every or max(steps, 1 << 20)))
+
+    def run_stage(self, stage: str) -> None:
+        _check(_lib.exogcm_run_stage(self.h, stage.encode()))
+
+    def field_size(self, name: str) -> int:
+        n = ctypes.c_size_t()
+        _check(_lib.exogcm_field_size(self.h, name.encode(), ctypes.byref(n)))
+        return n.value
+
+    def read(self, slot: int, name: str) -> np.ndarray:
+        out = np.zeros(self.field_size(name), dtype=np.float32)
+        _check(_lib.exogcm_read_field(self.h, slot, name.encode(), out.ctypes.data_as(_FP), out.size))
+        return out
+
+    def write(self, slot: int, name: str, values) -> None:
+        arr = np.ascontiguousarray(np.asarray(values, dtype=np.float32).reshape(-1))
+        _check(_lib.exogcm_write_field(self.h, slot, name.encode(), arr.ctypes.data_as(_FP), arr.size))
+
+    def read_table(self, slot: int, name: str, count: int) -> np.ndarray:
+        out = np.zeros(count, dtype=np.float32)
+        _check(_lib.exogcm_read_table(self.h, slot, name.encode(), out.ctypes.data_as(_FP), count))
+        return out
+
+    def snapshot(self, slot: int):
+        """(step, values [fields][NHOR]) of the slot's snapshot published in
+        the last step() call, or (-1, None)."""
+        step = ctypes.c_long()
+        _check(_lib.exogcm_read_snapshot(self.h, slot, None, 0, ctypes.byref(step)))
+        if step.value < 0:
+            return -1, None
+        n = self.field_size("snapshot")
+        out = np.zeros(n, dtype=np.float32)
+        _check(_lib.exogcm_read_snapshot(self.h, slot, out.ctypes.data_as(_FP), n, ctypes.byref(step)))
+        return step.value, out.reshape(-1, self.nhor)
+
+    def slot_info(self, slot: int):
+        step, left, active = ctypes.c_long(), ctypes.c_int(), ctypes.c_int()
+        _check(_lib.exogcm_slot_info(self.h, slot, ctypes.byref(step), ctypes.byref(left), ctypes.byref(active)))
+        return dict(step=step.value, startup_left=left.value, active=bool(active.value))
+
+    def unstable(self) -> np.ndarray:
+        flags = (ctypes.c_int * self.slots)()
+        _check(_lib.exogcm_unstable(self.h, flags, self.slots))
+        return np.array(flags[:], dtype=bool)
+
+    def last_step_ms(self) -> float:
+        ms = ctypes.c_float()
+        _check(_lib.exogcm_last_step_ms(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def checkpoint_save(self, slot: int) -> bytes:
+        buf, size = _VP(), ctypes.c_size_t()
+        _check(_lib.exogcm_checkpoint_save(self.h, slot, ctypes.byref(buf), ctypes.byref(size)))
+        try:
+            return ctypes.string_at(buf, size.value)
+        finally:
+            _lib.exogcm_free(buf)
+
+    def checkpoint_load(self, slot: int, data: bytes) -> None:
+        _check(_lib.exogcm_checkpoint_load(self.h, slot, data, len(data)))

@@ -1,0 +1,52 @@
+"""Builds libexogcm.so (the CUDA engine and its C ABI) in-tree for sm_100a."""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libexogcm.so")
+SOURCES = ["engine.cu", "transforms.cu", "dynamics.cu", "physics.cu", "setup.cpp"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+         "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+
+
+def stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    built = os.path.getmtime(LIB)
+    for name in os.listdir(CSRC):
+        if os.path.getmtime(os.path.join(CSRC, name)) > built:
+            return True
+    header = os.path.join(HERE, "..", "include", "exogcm.h")
+    return os.path.getmtime(header) > built
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not stale():
+        return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objects = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, src + ".o")
+        cmd = [NVCC, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        if src.endswith(".cpp"):
+            cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-c",
+                   os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        objects.append(obj)
+    # cudart links statically (nvcc's default), so the library loads on a
+    # host without a CUDA runtime install and fails only at its first device call.
+    subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB, *objects],
+                   check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

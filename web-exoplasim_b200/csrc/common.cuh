@@ -1,0 +1,122 @@
+// Device-side data layout shared by every kernel of the batched GCM step.
+//
+// HBM layout. A batch holds S planet slots of one resolution (T, L). Every
+// state field is stored [plane][slot][plane floats], where a field's planes
+// are its levels (or climatology months, or table entries). So level l of
+// slot s of a grid field f is f[(l * S + s) * NHOR + h]: with the column
+// index c = s * NHOR + h the whole batch is one grid of S * NHOR columns and
+// the column kernels index it exactly as the reference indexes one planet
+// (state[field + l * NHOR + h], src/model/climate/gcm/kernel/index.ts). The
+// same holds for spectral fields (S * NRSP coefficients per level) and
+// Fourier fields (S * NLAT rows of NFC per level). Transforms see each field
+// as count * S contiguous planes.
+//
+// Per-planet values: PlanetConst (scalars) indexed by slot, and a block of
+// per-planet tables (PlaneTabs offsets) at tabs + slot * tab_stride.
+// Per-step values (the reference's CPU-written radiation_step, surface_step,
+// carbon_step, snapshot_step slots and the start-up phase) are StepParams,
+// indexed [step in batch][slot].
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include "fields.h"
+
+namespace exogcm {
+
+constexpr int MAXL = 16;   // largest level count a kernel's register arrays hold
+constexpr int NLSOIL = 5;  // landmod's soil layers
+constexpr int MONTHS = 14; // climatology months with December before and January after
+
+struct Dims {
+  int T, L, NLAT, NLON, NHOR, NTP1, NCSP, NRSP, NFC, NLEV, NLEM, NLEP, P;
+  int S;  // planet slots in the batch
+};
+
+inline Dims make_dims(int truncation, int levels, int slots) {
+  Dims d{};
+  d.T = truncation;
+  d.L = levels;
+  d.NLAT = truncation == 21 ? 32 : truncation == 42 ? 64 : truncation == 63 ? 96 : 0;
+  d.NLON = 2 * d.NLAT;
+  d.NHOR = d.NLAT * d.NLON;
+  d.NTP1 = truncation + 1;
+  d.NCSP = d.NTP1 * (d.NTP1 + 1) / 2;
+  d.NRSP = 2 * d.NCSP;
+  d.NFC = 2 * d.NTP1;
+  d.NLEV = levels;
+  d.NLEM = levels - 1;
+  d.NLEP = levels + 1;
+  d.P = 51 + 5 * levels;
+  d.S = slots;
+  return d;
+}
+
+struct PlanetConst {
+#define EXOGCM_DECLARE_CONST(n) float n;
+  EXOGCM_CONSTS(EXOGCM_DECLARE_CONST)
+#undef EXOGCM_DECLARE_CONST
+};
+
+// One step's host-computed values for one slot (stepper/index.ts:281-334)
+// and its timestep phase (setup/index.ts:44-49: halved per start-up step).
+struct StepParams {
+  float delt, delt2, deltsec, deltsec2;
+  float filter;   // leapfrog filter on (main loop)
+  float coupled;  // icestep coupled (main loop)
+  int phase;      // bm1 block: 0 main loop, k = start-up steps still to run
+  int active;     // slot holds a running planet
+  float rad[5];   // radiation_step
+  float surf[7];  // surface_step
+  float carbon;   // carbon_step
+  float snap[3];  // snapshot_step
+};
+
+struct FieldPtrs {
+#define EXOGCM_DECLARE_FIELD(name, shape, count) float* name;
+  EXOGCM_FIELDS(EXOGCM_DECLARE_FIELD)
+#undef EXOGCM_DECLARE_FIELD
+};
+
+struct TabOffsets {
+#define EXOGCM_DECLARE_TAB(name, count) int name;
+  EXOGCM_PTABLES(EXOGCM_DECLARE_TAB)
+#undef EXOGCM_DECLARE_TAB
+  int stride;
+};
+
+// Tables every slot of a batch shares (one resolution, one filter setting).
+struct SharedTabs {
+  const float* fwd;    // fourier_forward [NLON][NFC]
+  const float* inv;    // fourier_inverse [NFC][NLON]
+  const float* qi;     // legendre_q* [NLAT][NCSP], filtered
+  const float* qj;
+  const float* qc;
+  const float* qe;
+  const float* qm;
+  const float* qq;
+  const float* qu;
+  const float* qv;
+  const float* zgw;    // Gaussian weight per point [NHOR]
+  const float* rcsq;   // 1 / cos^2(latitude) per point [NHOR]
+  const float* sid;    // sin(latitude) [NLAT]
+  const float* cola;   // cos(latitude) [NLAT]
+  const float* nindex; // total wavenumber per real coefficient [NRSP]
+  const int* mode_m;   // zonal wavenumber m of mode w [NCSP]
+  const int* mode_n;   // total wavenumber n of mode w [NCSP]
+};
+
+// Everything a step kernel can reach.
+struct Model {
+  Dims d;
+  FieldPtrs f;
+  SharedTabs sh;
+  TabOffsets to;
+  const float* tabs;         // per-slot table blocks [S][to.stride]
+  const PlanetConst* pc;     // [S]
+  const StepParams* params;  // [S] for the step being run
+  double* sums;              // FP64 per-slot reductions scratch [S][4]
+  int* flags;                // per-slot status flags [S]
+};
+
+}  // namespace exogcm

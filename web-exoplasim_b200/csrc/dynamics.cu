@@ -1,0 +1,453 @@
+// Grid-point dynamics, semi-implicit spectral update, horizontal diffusion,
+// dissipative heating and the dimensional frame around the column physics,
+// for every slot of a batch in one launch each (FP32).
+//
+// Arithmetic follows src/model/climate/gcm/dynamics/wgsl/*.wgsl (ExoPlaSim
+// plasim.f90's gridpointa / spectrala / spectrald / gridpointd, in Fortran's
+// statement order), with the batch's [level][slot][point] layout: column
+// index c = slot * NHOR + h, spectral index c = slot * NRSP + s.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "launch.h"
+
+namespace exogcm {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+__device__ __forceinline__ const float* slot_tabs(const Model& m, int slot) {
+  return m.tabs + (size_t)slot * m.to.stride;
+}
+
+// gridpointa from gp = exp(gp) to the flux products (dynamics/wgsl/calcgp.wgsl).
+__global__ void __launch_bounds__(kBlock) k_calcgp(Model m) {
+  const Dims& d = m.d;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.S * d.NHOR) return;
+  const int slot = c / d.NHOR;
+  if (!m.params[slot].active) return;
+  const PlanetConst& K = m.pc[slot];
+  const float* tb = slot_tabs(m, slot);
+  const float* ds = tb + m.to.dsigma;
+  const float* t0T = tb + m.to.t0;
+  const float* sh = tb + m.to.sigmah;
+  const float* rd = tb + m.to.rdsig;
+  const float* t01 = tb + m.to.t01s2;
+  const float* tkpT = tb + m.to.tkp;
+  const float* C = tb + m.to.c;
+  const float* G = tb + m.to.g;
+  const int NL = d.NLEV;
+  const size_t SN = (size_t)d.S * d.NHOR;
+  const FieldPtrs& F = m.f;
+  const float rcsq = m.sh.rcsq[c % d.NHOR];
+  const float ps = expf(F.gp[c]);
+  F.gp[c] = ps;
+  const float gpm = F.gpmt[c], gpj = F.gpj[c];
+  float gu[MAXL], gv[MAXL], gt[MAXL], gd[MAXL], gz[MAXL], gq[MAXL], zvgpg[MAXL], ztv1[MAXL], ztv2[MAXL];
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    gu[l] = F.gu[at];
+    gv[l] = F.gv[at];
+    gt[l] = F.gt[at];
+    gd[l] = F.gd[at];
+    gz[l] = F.gz[at];
+    gq[l] = F.gq[at];
+    zvgpg[l] = rcsq * (gu[l] * gpm + gv[l] * gpj);
+    const float zq = fmaxf(gq[l] / ps, 0.f);
+    const float t0 = t0T[l];
+    const float tvirt = (gt[l] + t0) * (1.f + (1.f / K.RDBRV - 1.f) * zq);
+    ztv1[l] = tvirt - t0;
+    ztv2[l] = tvirt / (1.f + K.ADV * zq) - t0;
+  }
+  float zsdotp[MAXL];
+  float zsumd = ds[0] * gd[0];
+  float gvp = ds[0] * zvgpg[0];
+  zsdotp[0] = zsumd + gvp;
+  for (int l = 1; l < NL - 1; ++l) {
+    zsumd = zsumd + ds[l] * gd[l];
+    gvp = gvp + ds[l] * zvgpg[l];
+    zsdotp[l] = zsumd + gvp;
+  }
+  zsumd = zsumd + ds[NL - 1] * gd[NL - 1];
+  gvp = gvp + ds[NL - 1] * zvgpg[NL - 1];
+  float gtd[MAXL], gqm[MAXL], gud[MAXL], gvd[MAXL];
+  for (int l = 0; l < NL - 1; ++l) {
+    zsdotp[l] = sh[l] * (zsumd + gvp) - zsdotp[l];
+    gtd[l] = zsdotp[l] * (gt[l + 1] - gt[l]);
+    gqm[l] = zsdotp[l] * (gq[l + 1] + gq[l]);
+    gud[l] = zsdotp[l] * (gu[l + 1] - gu[l]);
+    gvd[l] = zsdotp[l] * (gv[l + 1] - gv[l]);
+  }
+  float gtn[MAXL], gqn[MAXL], guz[MAXL], gvz[MAXL], dw[MAXL];
+  zsumd = zvgpg[0] * ds[0];
+  const float rdsig0 = rd[0];
+  gtn[0] = gt[0] * gd[0] - K.AKAP * ztv2[0] * gd[0] - rdsig0 * (gtd[0] + t01[0] * (sh[0] * gvp - zsumd));
+  gqn[0] = -rdsig0 * gqm[0];
+  guz[0] = -gu[0] * gz[0] - gpj * ztv1[0] - rdsig0 * gvd[0];
+  gvz[0] = gv[0] * gz[0] - gpm * ztv1[0] - rdsig0 * gud[0];
+  dw[0] = gd[0] * ps * K.PSURF * K.WW;
+  for (int l = 1; l < NL; ++l) {
+    const int column = l * NL;
+    float ztpta = C[column] * zvgpg[0];
+    float ztptb = C[column] * (zvgpg[0] + gd[0]);
+    for (int j = 1; j <= l; ++j) {
+      ztpta = ztpta + C[column + j] * zvgpg[j];
+      ztptb = ztptb + C[column + j] * (zvgpg[j] + gd[j]);
+    }
+    const float rdsig = rd[l], t01s2 = t01[l], t01s2m = t01[l - 1], sigmah = sh[l], sigmahm = sh[l - 1];
+    const float tkp = tkpT[l];
+    if (l < NL - 1) {
+      zsumd = zsumd + zvgpg[l] * ds[l];
+      gtn[l] = gt[l] * gd[l] + K.AKAP * ztv2[l] * (zvgpg[l] - ztptb) + tkp * (zvgpg[l] - ztpta) -
+               rdsig * (gtd[l] + gtd[l - 1] + gvp * (t01s2 * sigmah + t01s2m * sigmahm) - zsumd * (t01s2m + t01s2) +
+                        zvgpg[l] * ds[l] * t01s2m);
+      gqn[l] = -rdsig * (gqm[l] - gqm[l - 1]);
+      guz[l] = -gu[l] * gz[l] - gpj * ztv1[l] - rdsig * (gvd[l] + gvd[l - 1]);
+      gvz[l] = gv[l] * gz[l] - gpm * ztv1[l] - rdsig * (gud[l] + gud[l - 1]);
+    } else {
+      gtn[l] = gt[l] * gd[l] + K.AKAP * ztv2[l] * (zvgpg[l] - ztptb) + tkp * (zvgpg[l] - ztpta) -
+               rdsig * (gtd[NL - 2] + t01s2m * (sigmahm * gvp - zsumd));
+      gqn[l] = rdsig * gqm[NL - 2];
+      guz[l] = -gu[l] * gz[l] - gpj * ztv1[l] - rdsig * gvd[NL - 2];
+      gvz[l] = gv[l] * gz[l] - gpm * ztv1[l] - rdsig * gud[NL - 2];
+    }
+    dw[l] = (zvgpg[l] - ztptb) * ps * K.PSURF * K.WW;
+  }
+  const float scale = sqrtf(rcsq);
+  for (int l = 0; l < NL; ++l) {
+    float gsum = 0.f;
+    for (int k = 0; k < NL; ++k) gsum = gsum + G[l * NL + k] * (ztv1[k] - gt[k]);
+    const float gphi = gsum * 2.f / rcsq;
+    const size_t at = l * SN + c;
+    F.gtn[at] = gtn[l];
+    F.gqn[at] = gqn[l];
+    F.guz[at] = guz[l];
+    F.gvz[at] = gvz[l];
+    F.dw[at] = dw[l];
+    F.gut[at] = gu[l] * gt[l];
+    F.gvt[at] = gv[l] * gt[l];
+    F.gke[at] = gu[l] * gu[l] + gv[l] * gv[l] + gphi;
+    F.guq[at] = gu[l] * gq[l];
+    F.gvq[at] = gv[l] * gq[l];
+    F.du0[at] = K.CV * gu[l] * scale;
+    F.dv0[at] = K.CV * gv[l] * scale;
+  }
+  F.gvpp[c] = gvp;
+  F.dp0[c] = K.PSURF * ps;
+}
+
+// spectrala for one real spectral coefficient (dynamics/wgsl/spectrala.wgsl):
+// the Hoskins-Simmons semi-implicit scheme with this slot's bm1 for its phase.
+__global__ void __launch_bounds__(kBlock) k_spectrala(Model m) {
+  const Dims& d = m.d;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.S * d.NRSP) return;
+  const int slot = c / d.NRSP, s = c % d.NRSP;
+  const StepParams& P = m.params[slot];
+  if (!P.active) return;
+  const PlanetConst& K = m.pc[slot];
+  const float* tb = slot_tabs(m, slot);
+  const float* G = tb + m.to.g;
+  const float* t0T = tb + m.to.t0;
+  const float* ds = tb + m.to.dsigma;
+  const float* tau = tb + m.to.tau;
+  const int NL = d.NLEV;
+  const float* bm1 = tb + m.to.bm1 + (size_t)P.phase * d.T * NL * NL;
+  const size_t SR = (size_t)d.S * d.NRSP;
+  const FieldPtrs& F = m.f;
+  const bool filter = P.filter != 0.f;
+  const float DELT = P.delt, DELT2 = P.delt2;
+  const float apm = F.spm[c];
+  float adm[MAXL], azm[MAXL], atm[MAXL], aqm[MAXL], adt[MAXL], stt[MAXL];
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SR + c;
+    adm[l] = F.sdm[at];
+    azm[l] = F.szm[at];
+    atm[l] = F.stm[at];
+    aqm[l] = F.sqm[at];
+    adt[l] = F.sdt[at];
+    stt[l] = F.stt[at];
+  }
+  float zgt[MAXL], zgm[MAXL];
+  for (int l = 0; l < NL; ++l) {
+    float gt = 0.f, gm = 0.f;
+    for (int k = 0; k < NL; ++k) {
+      gt = gt + G[l * NL + k] * stt[k];
+      gm = gm + G[l * NL + k] * atm[k];
+    }
+    zgt[l] = gt;
+    zgm[l] = gm;
+  }
+  float spt = F.spt[c];
+  const float spm = apm;
+  const float sop = tb[m.to.sop + s];
+  const int jn = (int)m.sh.nindex[s];
+  float sdt[MAXL];
+  for (int l = 0; l < NL; ++l) {
+    float zsum = 0.f;
+    if (jn > 0) {
+      const float zq = 1.f / (float)(jn * (jn + 1));
+      for (int l2 = 0; l2 < NL; ++l2) {
+        const float z0 = t0T[l2];
+        const float zt = zgt[l2] - z0 * spt;
+        const float zm = zgm[l2] + z0 * spm;
+        const float za = adt[l2] * zq + sop;
+        const float zb = adm[l2] * zq;
+        const float zz = zb + DELT * (zm + za + DELT * zt);
+        zsum = zsum + zz * bm1[((jn - 1) * NL + l) * NL + l2];
+      }
+    }
+    sdt[l] = s < 2 ? 0.f : zsum;
+  }
+  for (int l = 0; l < NL; ++l) spt = spt + ds[l] * sdt[l];
+  for (int l = 0; l < NL; ++l) {
+    float t = 0.f;
+    for (int k = 0; k < NL; ++k) t = t + tau[l * NL + k] * sdt[k];
+    stt[l] = stt[l] - t;
+  }
+  const float spp = F.spp[c];
+  if (filter) F.spm[c] = K.PNU21 * spp + K.PNU * apm;
+  const float sppNew = s < 2 ? 0.f : apm - DELT2 * spt;
+  F.spp[c] = sppNew;
+  F.sp[c] = sppNew;
+  F.spt[c] = spt;
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SR + c;
+    if (filter) {
+      F.sdm[at] = K.PNU21 * F.sdp[at] + K.PNU * adm[l];
+      F.szm[at] = K.PNU21 * F.szp[at] + K.PNU * azm[l];
+      F.stm[at] = K.PNU21 * F.stp[at] + K.PNU * atm[l];
+      F.sqm[at] = K.PNU21 * F.sqp[at] + K.PNU * aqm[l];
+    }
+    const float sdp = 2.f * sdt[l] - adm[l];
+    const float stp = DELT2 * stt[l] + atm[l];
+    const float szp = DELT2 * F.szt[at] + azm[l];
+    const float sqp = DELT2 * F.sqt[at] + aqm[l];
+    F.sdt[at] = sdt[l];
+    F.stt[at] = stt[l];
+    F.sdp[at] = sdp;
+    F.stp[at] = stp;
+    F.szp[at] = szp;
+    F.sqp[at] = sqp;
+    F.sd[at] = sdp;
+    F.st[at] = stp;
+    F.sz[at] = szp;
+    F.sq[at] = sqp;
+  }
+}
+
+// spectrald up to mkdheat (dynamics/wgsl/spectrald-diffusion.wgsl).
+__global__ void __launch_bounds__(kBlock) k_spectrald_diffusion(Model m) {
+  const Dims& d = m.d;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.S * d.NRSP) return;
+  const int slot = c / d.NRSP, s = c % d.NRSP;
+  const StepParams& P = m.params[slot];
+  if (!P.active) return;
+  const PlanetConst& K = m.pc[slot];
+  const float* tb = slot_tabs(m, slot);
+  const size_t SR = (size_t)d.S * d.NRSP;
+  const FieldPtrs& F = m.f;
+  const float D2 = P.delt2;
+  if (s < 2) F.spp[c] = 0.f;
+  for (int l = 0; l < d.NLEV; ++l) {
+    const size_t at = l * SR + c;
+    const float szp = F.szp[at] + D2 * F.szt[at];
+    const float stp = F.stp[at] + D2 * F.stt[at];
+    const float sdp = F.sdp[at] + D2 * F.sdt[at];
+    const float sqp = F.sqp[at] + D2 * F.sqt[at];
+    const float sakpp = tb[m.to.sakpp + l * d.NRSP + s];
+    const float damp = tb[m.to.damp + l], tdisst = tb[m.to.tdisst + l], tdissq = tb[m.to.tdissq + l];
+    const float tdissd = tb[m.to.tdissd + l], tdissz = tb[m.to.tdissz + l], tfrc = tb[m.to.tfrc + l];
+    const float srp = tb[m.to.srp + l * d.NRSP + s];
+    const float stt = ((-damp - tdisst * sakpp) * stp + damp * srp) / (1.f + D2 * (damp + tdisst * sakpp));
+    const float sqt = -tdissq * sakpp * sqp / (1.f + D2 * tdissq * sakpp);
+    const float zsdt1 = -tfrc * sdp / (1.f + D2 * tfrc);
+    const float zsdt2 = -tdissd * sakpp * sdp / (1.f + D2 * tdissd * sakpp);
+    float zszt1 = -tfrc * szp / (1.f + D2 * tfrc);
+    float zszt2 = -tdissz * sakpp * szp / (1.f + D2 * tdissz * sakpp);
+    float szt = zszt1 + zszt2;
+    if (s == 2) {
+      zszt1 = zszt1 + K.PLAVOR * tfrc / (1.f + D2 * tfrc);
+      zszt2 = zszt2 + K.PLAVOR * tdissz * sakpp / (1.f + D2 * tdissz * sakpp);
+      szt = szt + K.PLAVOR * (tfrc / (1.f + D2 * tfrc) + tdissz * sakpp / (1.f + D2 * tdissz * sakpp));
+    }
+    F.szp[at] = szp;
+    F.stp[at] = stp;
+    F.sdp[at] = sdp;
+    F.sqp[at] = sqp;
+    F.stt[at] = stt;
+    F.sqt[at] = sqt;
+    F.sdt[at] = zsdt1 + zsdt2;
+    F.szt[at] = szt;
+    F.zdsdp1[at] = zsdt1 * D2;
+    F.zdszp1[at] = zszt1 * D2;
+    F.zdsdp2[at] = zsdt2 * D2;
+    F.zdszp2[at] = zszt2 * D2;
+  }
+}
+
+// mkdheat's grid-point stages (dynamics/wgsl/mkdheat.wgsl).
+__global__ void __launch_bounds__(kBlock) k_mkdheat(Model m, int stage) {
+  const Dims& d = m.d;
+  const size_t SN = (size_t)d.S * d.NHOR;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.NLEV * SN) return;
+  const int l = (int)(i / SN);
+  const int c = (int)(i % SN);
+  const int slot = c / d.NHOR, h = c % d.NHOR;
+  const StepParams& P = m.params[slot];
+  if (!P.active) return;
+  const PlanetConst& K = m.pc[slot];
+  const float ds = m.tabs[(size_t)slot * m.to.stride + m.to.dsigma + l];
+  const FieldPtrs& F = m.f;
+  const float heat = 1.f + K.ADV * F.dq[i];
+  if (stage == 3) {
+    const float dp = F.dp[c];
+    const float dtdt = -F.zdekin[i] * 0.5f / K.ACPD / heat / dp * K.GA / ds;
+    F.zdtdt[i] = dtdt / K.CT / K.WW;
+    return;
+  }
+  const float scale = K.CV * sqrtf(m.sh.rcsq[h]);
+  const float u = F.zu[i] * scale, v = F.zv[i] * scale, du = F.zdu[i] * scale, dv = F.zdv[i] * scale;
+  const float change = du * (2.f * u + du) + dv * (2.f * v + dv);
+  if (stage == 1) {
+    const float dtdt = -change / P.deltsec2 * 0.5f / K.ACPD / heat;
+    F.zdtdt[i] = dtdt / K.CT / K.WW;
+  } else {
+    F.zdekin[i] = change / P.deltsec2 * F.dp[c] / K.GA * ds;
+  }
+}
+
+// mkdheat's zsdef(2:NESP,:) = 0 (dynamics/wgsl/mean-mode.wgsl).
+__global__ void k_mean_mode(float* t, size_t n, int nrsp) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (i % nrsp != 0) t[i] = 0.f;
+}
+
+// spectrald after mkdheat (dynamics/wgsl/spectrald-update.wgsl).
+__global__ void __launch_bounds__(kBlock) k_spectrald_update(Model m) {
+  const Dims& d = m.d;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.S * d.NRSP) return;
+  const int slot = c / d.NRSP;
+  const StepParams& P = m.params[slot];
+  if (!P.active) return;
+  const PlanetConst& K = m.pc[slot];
+  const size_t SR = (size_t)d.S * d.NRSP;
+  const FieldPtrs& F = m.f;
+  const bool filter = P.filter != 0.f;
+  const float D2 = P.delt2;
+  const float spp = F.spp[c];
+  if (filter) F.spm[c] = F.spm[c] + K.PNU * spp;
+  F.sp[c] = spp;
+  for (int l = 0; l < d.NLEV; ++l) {
+    const size_t at = l * SR + c;
+    const float stt = F.stt[at] + F.zstt1[at] + F.zstt2[at];
+    F.stt[at] = stt;
+    const float szp = F.szp[at] + D2 * F.szt[at];
+    const float stp = F.stp[at] + D2 * stt;
+    const float sdp = F.sdp[at] + D2 * F.sdt[at];
+    const float sqp = F.sqp[at] + D2 * F.sqt[at];
+    F.szp[at] = szp;
+    F.stp[at] = stp;
+    F.sdp[at] = sdp;
+    F.sqp[at] = sqp;
+    if (filter) {
+      F.szm[at] = F.szm[at] + K.PNU * szp;
+      F.stm[at] = F.stm[at] + K.PNU * stp;
+      F.sdm[at] = F.sdm[at] + K.PNU * sdp;
+      F.sqm[at] = F.sqm[at] + K.PNU * sqp;
+    }
+    F.sz[at] = szp;
+    F.st[at] = stp;
+    F.sd[at] = sdp;
+    F.sq[at] = sqp;
+  }
+}
+
+// gridpointd before the parameterizations (dynamics/wgsl/physics-in.wgsl).
+__global__ void __launch_bounds__(kBlock) k_physics_in(Model m) {
+  const Dims& d = m.d;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.S * d.NHOR) return;
+  const int slot = c / d.NHOR, h = c % d.NHOR;
+  if (!m.params[slot].active) return;
+  const PlanetConst& K = m.pc[slot];
+  const float* t0 = m.tabs + (size_t)slot * m.to.stride + m.to.t0;
+  const size_t SN = (size_t)d.S * d.NHOR;
+  const FieldPtrs& F = m.f;
+  const float dp = K.PSURF * expf(F.gp[c]);
+  F.dp[c] = dp;
+  const float scale = sqrtf(m.sh.rcsq[h]);
+  for (int l = 0; l < d.NLEP; ++l) {
+    const size_t at = l * SN + c;
+    F.dudt[at] = 0.f;
+    F.dvdt[at] = 0.f;
+    F.dtdt[at] = 0.f;
+    F.dqdt[at] = 0.f;
+    if (l < d.NLEV) {
+      F.gudt[at] = 0.f;
+      F.gvdt[at] = 0.f;
+      F.gtdt[at] = 0.f;
+      F.gqdt[at] = 0.f;
+      F.du[at] = K.CV * F.gu[at] * scale;
+      F.dv[at] = K.CV * F.gv[at] * scale;
+      F.dt[at] = K.CT * (F.gt[at] + t0[l]);
+      F.dq[at] = F.gq[at] * K.PSURF / dp;
+    }
+  }
+}
+
+// gridpointd after the parameterizations (dynamics/wgsl/physics-out.wgsl).
+__global__ void __launch_bounds__(kBlock) k_physics_out(Model m) {
+  const Dims& d = m.d;
+  const size_t SN = (size_t)d.S * d.NHOR;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.NLEV * SN) return;
+  const int c = (int)(i % SN);
+  const int slot = c / d.NHOR, h = c % d.NHOR;
+  if (!m.params[slot].active) return;
+  const PlanetConst& K = m.pc[slot];
+  const FieldPtrs& F = m.f;
+  const float scale = sqrtf(m.sh.rcsq[h]);
+  F.gudt[i] = F.dudt[i] / scale / K.CV / K.WW + F.gudt[i];
+  F.gvdt[i] = F.dvdt[i] / scale / K.CV / K.WW + F.gvdt[i];
+  F.gtdt[i] = F.dtdt[i] / K.CT / K.WW + F.gtdt[i];
+  F.gqdt[i] = F.dqdt[i] * F.dp[c] / K.WW / K.PSURF + F.gqdt[i];
+}
+
+inline unsigned blocks(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+}  // namespace
+
+void dyn_calcgp(const Model& m, cudaStream_t st) {
+  k_calcgp<<<blocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);
+}
+void dyn_spectrala(const Model& m, cudaStream_t st) {
+  k_spectrala<<<blocks((size_t)m.d.S * m.d.NRSP, kBlock), kBlock, 0, st>>>(m);
+}
+void dyn_spectrald_diffusion(const Model& m, cudaStream_t st) {
+  k_spectrald_diffusion<<<blocks((size_t)m.d.S * m.d.NRSP, kBlock), kBlock, 0, st>>>(m);
+}
+void dyn_mkdheat(const Model& m, int stage, cudaStream_t st) {
+  k_mkdheat<<<blocks((size_t)m.d.NLEV * m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m, stage);
+}
+void dyn_mean_mode(const Model& m, float* target, cudaStream_t st) {
+  const size_t n = (size_t)m.d.NLEV * m.d.S * m.d.NRSP;
+  k_mean_mode<<<blocks(n, 256), 256, 0, st>>>(target, n, m.d.NRSP);
+}
+void dyn_spectrald_update(const Model& m, cudaStream_t st) {
+  k_spectrald_update<<<blocks((size_t)m.d.S * m.d.NRSP, kBlock), kBlock, 0, st>>>(m);
+}
+void dyn_physics_in(const Model& m, cudaStream_t st) {
+  k_physics_in<<<blocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);
+}
+void dyn_physics_out(const Model& m, cudaStream_t st) {
+  k_physics_out<<<blocks((size_t)m.d.NLEV * m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);
+}
+
+}  // namespace exogcm

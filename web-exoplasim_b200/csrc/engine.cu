@@ -1,0 +1,897 @@
+// The batched GCM engine behind the C ABI of include/exogcm.h.
+//
+// Mirrors the reference's engine plumbing (src/model/climate/gcm/):
+//   configure  -> SETUP.state/schedule + STEPPER.context + LAYOUT.write
+//                 (setup/index.ts:434-477, stepper/index.ts:94-118)
+//   step       -> STEPPER.values + STEPPER.batch (stepper/index.ts:203-334):
+//                 the step's kernels in master's order
+//                 (stepper/index.ts:148-161, dynamics/index.ts:171-344)
+//   readback   -> LAYOUT.read (layout/index.ts:73-108)
+//   checkpoint -> RESTART.encode/decode (checkpoint/restart/index.ts:11-75)
+// for S planet slots at once. One device arena holds every field as
+// [plane][slot][points]; a batch of K steps is one CUDA graph whose step k
+// reads its per-slot host values at params + k * S.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/exogcm.h"
+#include "common.cuh"
+#include "launch.h"
+#include "setup.h"
+
+using namespace exogcm;
+
+namespace {
+
+thread_local std::string g_error;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Error(EXOGCM_EDEVICE, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+struct FieldInfo {
+  std::string name;
+  char shape;
+  int count;
+  size_t plane;   // floats per plane per slot
+  size_t offset;  // floats from the arena base
+};
+
+struct Slot {
+  bool active = false;
+  long step = 0;
+  int carbon_step = 0;
+  int startup_left = 0;
+  long published = -1;
+  double deltsec[4] = {0}, delt[4] = {0};
+  Calendar cal{};
+};
+
+constexpr int kMaxBatch = 64;
+
+}  // namespace
+
+struct exogcm_engine {
+  Dims d{};
+  int mode = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  std::vector<FieldInfo> fields;
+  std::map<std::string, size_t> field_index;
+  float* arena = nullptr;
+  size_t arena_floats = 0;
+  FieldPtrs fp{};
+  // shared tables
+  bool shared_ready = false;
+  int filter_kind = -1, filter_gp = -1, filter_sp = -1;
+  float* shared_buf = nullptr;
+  int* mode_buf = nullptr;
+  SharedTabs sh{};
+  // per-slot tables and constants
+  TabOffsets to{};
+  std::vector<std::pair<std::string, int>> tab_list;
+  float* tabs = nullptr;
+  PlanetConst* pc = nullptr;
+  StepParams* params = nullptr;   // device [kMaxBatch][S]
+  StepParams* hparams = nullptr;  // pinned host
+  double* sums = nullptr;
+  int* flags = nullptr;
+  std::vector<Slot> slots;
+  std::map<int, cudaGraphExec_t> graphs;
+
+  Model model(int k) const {
+    Model m{};
+    m.d = d;
+    m.f = fp;
+    m.sh = sh;
+    m.to = to;
+    m.tabs = tabs;
+    m.pc = pc;
+    m.params = params + (size_t)k * d.S;
+    m.sums = sums;
+    m.flags = flags;
+    return m;
+  }
+};
+
+namespace {
+
+size_t plane_floats(const Dims& d, char shape) {
+  switch (shape) {
+    case 'S': return d.NRSP;
+    case 'F': return (size_t)d.NLAT * d.NFC;
+    case 'G': return d.NHOR;
+    default: return 1;
+  }
+}
+
+void layout(exogcm_engine* e) {
+  const Dims& d = e->d;
+  const int L = d.L, H = d.L + 1, P = d.P;
+  (void)L;
+  (void)H;
+  (void)P;
+  size_t off = 0;
+#define EXOGCM_ADD_FIELD(name, shape, cnt)                                            \
+  {                                                                                   \
+    FieldInfo fi{#name, #shape[0], (int)(cnt), plane_floats(d, #shape[0]), off};      \
+    e->field_index[#name] = e->fields.size();                                         \
+    e->fields.push_back(fi);                                                          \
+    off += fi.plane * fi.count * d.S;                                                 \
+  }
+  {
+    const int L = d.L;
+    EXOGCM_FIELDS(EXOGCM_ADD_FIELD)
+  }
+#undef EXOGCM_ADD_FIELD
+  e->arena_floats = off;
+}
+
+void bind_fields(exogcm_engine* e) {
+#define EXOGCM_BIND(name, shape, count) e->fp.name = e->arena + e->fields[e->field_index[#name]].offset;
+  EXOGCM_FIELDS(EXOGCM_BIND)
+#undef EXOGCM_BIND
+}
+
+void table_layout(exogcm_engine* e) {
+  const int L = e->d.L, NTRU = e->d.T, NRSP = e->d.NRSP;
+  int off = 0;
+#define EXOGCM_TAB(name, count)                  \
+  e->to.name = off;                              \
+  e->tab_list.push_back({#name, (int)(count)});  \
+  off += (int)(count);
+  EXOGCM_PTABLES(EXOGCM_TAB)
+#undef EXOGCM_TAB
+  e->to.stride = (off + 31) / 32 * 32;
+}
+
+const FieldInfo& field(exogcm_engine* e, const char* name) {
+  auto it = e->field_index.find(name ? name : "");
+  if (it == e->field_index.end()) throw Error(EXOGCM_EINVAL, std::string("no state field ") + (name ? name : "(null)"));
+  return e->fields[it->second];
+}
+
+void check_slot(exogcm_engine* e, int slot) {
+  if (slot < 0 || slot >= e->d.S) throw Error(EXOGCM_EINVAL, "slot out of range");
+}
+
+// Copies between a host array [count][plane] and one slot's planes.
+void copy_field(exogcm_engine* e, const FieldInfo& fi, int slot, void* host, bool to_device) {
+  float* base = e->arena + fi.offset + (size_t)slot * fi.plane;
+  const size_t pitch = fi.plane * e->d.S * sizeof(float);
+  const size_t width = fi.plane * sizeof(float);
+  if (to_device)
+    check(cudaMemcpy2DAsync(base, pitch, host, width, width, fi.count, cudaMemcpyHostToDevice, e->stream),
+          "write field");
+  else
+    check(cudaMemcpy2DAsync(host, width, base, pitch, width, fi.count, cudaMemcpyDeviceToHost, e->stream),
+          "read field");
+  check(cudaStreamSynchronize(e->stream), "field copy");
+}
+
+void upload_shared(exogcm_engine* e, const SharedSetup& s) {
+  const Dims& d = e->d;
+  std::vector<float> buf;
+  auto put = [&](const Vec& v) {
+    size_t at = buf.size();
+    for (double x : v) buf.push_back((float)x);
+    while (buf.size() % 32) buf.push_back(0.f);
+    return at;
+  };
+  const size_t fwd = put(s.fwd), inv = put(s.inv);
+  size_t q[8];
+  const char* names[8] = {"qi", "qj", "qc", "qe", "qm", "qq", "qu", "qv"};
+  for (int i = 0; i < 8; ++i) q[i] = put(s.q.at(names[i]));
+  Vec zgw(d.NHOR), rcsq(d.NHOR), cola(d.NLAT), nindex(d.NRSP);
+  for (int h = 0; h < d.NHOR; ++h) {
+    const double sn = s.sines[h / d.NLON];
+    zgw[h] = s.weights[h / d.NLON];
+    rcsq[h] = 1 / (1 - sn * sn);
+  }
+  for (int l = 0; l < d.NLAT; ++l) cola[l] = std::sqrt(1 - s.sines[l] * s.sines[l]);
+  std::vector<int> mm(d.NCSP), nn(d.NCSP);
+  {
+    int w = 0, r = 0;
+    for (int m = 0; m <= d.T; ++m)
+      for (int n = m; n <= d.T; ++n) {
+        mm[w] = m;
+        nn[w] = n;
+        ++w;
+        nindex[r] = nindex[r + 1] = n;
+        r += 2;
+      }
+  }
+  const size_t izgw = put(zgw), ircsq = put(rcsq), isid = put(s.sines), icola = put(cola), inidx = put(nindex);
+  check(cudaMalloc(&e->shared_buf, buf.size() * sizeof(float)), "shared tables");
+  check(cudaMemcpy(e->shared_buf, buf.data(), buf.size() * sizeof(float), cudaMemcpyHostToDevice), "shared tables");
+  check(cudaMalloc(&e->mode_buf, 2 * d.NCSP * sizeof(int)), "mode tables");
+  check(cudaMemcpy(e->mode_buf, mm.data(), d.NCSP * sizeof(int), cudaMemcpyHostToDevice), "mode tables");
+  check(cudaMemcpy(e->mode_buf + d.NCSP, nn.data(), d.NCSP * sizeof(int), cudaMemcpyHostToDevice), "mode tables");
+  float* b = e->shared_buf;
+  e->sh.fwd = b + fwd;
+  e->sh.inv = b + inv;
+  e->sh.qi = b + q[0];
+  e->sh.qj = b + q[1];
+  e->sh.qc = b + q[2];
+  e->sh.qe = b + q[3];
+  e->sh.qm = b + q[4];
+  e->sh.qq = b + q[5];
+  e->sh.qu = b + q[6];
+  e->sh.qv = b + q[7];
+  e->sh.zgw = b + izgw;
+  e->sh.rcsq = b + ircsq;
+  e->sh.sid = b + isid;
+  e->sh.cola = b + icola;
+  e->sh.nindex = b + inidx;
+  e->sh.mode_m = e->mode_buf;
+  e->sh.mode_n = e->mode_buf + d.NCSP;
+  e->shared_ready = true;
+}
+
+// ---------------------------------------------------------------- the step
+void stage_gridpointa(const Model& m, cudaStream_t st) {
+  const Dims& d = m.d;
+  const FieldPtrs& F = m.f;
+  const int LP = d.L * d.S, SP = d.S;
+  tr_dv2uv(m, F.sd, F.sz, F.fgu, F.fgv, LP, 1.63299310207f, st);
+  tr_legendre_inverse(m, F.sd, F.fgd, LP, m.sh.qi, st);
+  tr_legendre_inverse(m, F.st, F.fgt, LP, m.sh.qi, st);
+  tr_legendre_inverse(m, F.sz, F.fgz, LP, m.sh.qi, st);
+  tr_legendre_inverse(m, F.sq, F.fgq, LP, m.sh.qi, st);
+  tr_legendre_inverse(m, F.sp, F.fgp, SP, m.sh.qi, st);
+  tr_legendre_inverse(m, F.sp, F.fgpj, SP, m.sh.qj, st);
+  tr_dlambda(m, F.fgp, F.fgpmt, SP, st);
+  tr_fourier_inverse(m, F.fgu, F.gu, LP, st);
+  tr_fourier_inverse(m, F.fgv, F.gv, LP, st);
+  tr_fourier_inverse(m, F.fgt, F.gt, LP, st);
+  tr_fourier_inverse(m, F.fgd, F.gd, LP, st);
+  tr_fourier_inverse(m, F.fgz, F.gz, LP, st);
+  tr_fourier_inverse(m, F.fgpj, F.gpj, SP, st);
+  tr_fourier_inverse(m, F.fgpmt, F.gpmt, SP, st);
+  tr_fourier_inverse(m, F.fgp, F.gp, SP, st);
+  tr_fourier_inverse(m, F.fgq, F.gq, LP, st);
+  dyn_calcgp(m, st);
+  tr_fourier_forward(m, F.gtn, F.fgtn, LP, st);
+  tr_fourier_forward(m, F.gqn, F.fgqn, LP, st);
+  tr_fourier_forward(m, F.gut, F.fgut, LP, st);
+  tr_fourier_forward(m, F.gvt, F.fgvt, LP, st);
+  tr_fourier_forward(m, F.guz, F.fguz, LP, st);
+  tr_fourier_forward(m, F.gvz, F.fgvz, LP, st);
+  tr_fourier_forward(m, F.gke, F.fgke, LP, st);
+  tr_fourier_forward(m, F.gvpp, F.fgvpp, SP, st);
+  tr_fourier_forward(m, F.guq, F.fguq, LP, st);
+  tr_fourier_forward(m, F.gvq, F.fgvq, LP, st);
+  tr_legendre_forward(m, F.fgvpp, F.spt, SP, m.sh.qc, st);
+  tr_uv2dv(m, F.fgvz, F.fguz, F.fgke, F.sdt, F.szt, LP, st);
+  tr_qtend(m, F.fgut, F.fgvt, F.fgtn, F.stt, LP, st);
+  tr_qtend(m, F.fguq, F.fgvq, F.fgqn, F.sqt, LP, st);
+}
+
+void stage_physics_in(const Model& m, cudaStream_t st) {
+  const Dims& d = m.d;
+  const FieldPtrs& F = m.f;
+  const int LP = d.L * d.S, SP = d.S;
+  tr_dv2uv(m, F.sd, F.sz, F.fgu, F.fgv, LP, 1.63299310207f, st);
+  tr_legendre_inverse(m, F.sq, F.fgq, LP, m.sh.qi, st);
+  tr_legendre_inverse(m, F.st, F.fgt, LP, m.sh.qi, st);
+  tr_legendre_inverse(m, F.sp, F.fgp, SP, m.sh.qi, st);
+  tr_fourier_inverse(m, F.fgu, F.gu, LP, st);
+  tr_fourier_inverse(m, F.fgv, F.gv, LP, st);
+  tr_fourier_inverse(m, F.fgt, F.gt, LP, st);
+  tr_fourier_inverse(m, F.fgp, F.gp, SP, st);
+  tr_fourier_inverse(m, F.fgq, F.gq, LP, st);
+  dyn_physics_in(m, st);
+}
+
+void stage_precipitation(const Model& m, cudaStream_t st) {
+  const int LP = m.d.L * m.d.S;
+  tr_legendre_inverse(m, m.f.sqt, m.f.fdqt, LP, m.sh.qi, st);
+  tr_fourier_inverse(m, m.f.fdqt, m.f.dqt, LP, st);
+  phy_precipitation_columns(m, st);
+}
+
+void stage_physics_out(const Model& m, cudaStream_t st) {
+  const int LP = m.d.L * m.d.S;
+  const FieldPtrs& F = m.f;
+  dyn_physics_out(m, st);
+  tr_fourier_forward(m, F.gtdt, F.fgtdt, LP, st);
+  tr_fourier_forward(m, F.gudt, F.fgudt, LP, st);
+  tr_fourier_forward(m, F.gvdt, F.fgvdt, LP, st);
+  tr_fourier_forward(m, F.gqdt, F.fgqdt, LP, st);
+  tr_legendre_forward(m, F.fgtdt, F.stt, LP, m.sh.qc, st);
+  tr_legendre_forward(m, F.fgqdt, F.sqt, LP, m.sh.qc, st);
+  tr_uv2dv(m, F.fgudt, F.fgvdt, nullptr, F.sdt, F.szt, LP, st);
+}
+
+void stage_spectrald(const Model& m, cudaStream_t st) {
+  const int LP = m.d.L * m.d.S;
+  const FieldPtrs& F = m.f;
+  const float plavor = 1.63299310207f;
+  dyn_spectrald_diffusion(m, st);
+  tr_dv2uv(m, F.sdp, F.szp, F.fzu, F.fzv, LP, plavor, st);
+  tr_fourier_inverse(m, F.fzu, F.zu, LP, st);
+  tr_fourier_inverse(m, F.fzv, F.zv, LP, st);
+  tr_dv2uv(m, F.zdsdp1, F.zdszp1, F.fzdu, F.fzdv, LP, 0.f, st);
+  tr_fourier_inverse(m, F.fzdu, F.zdu, LP, st);
+  tr_fourier_inverse(m, F.fzdv, F.zdv, LP, st);
+  dyn_mkdheat(m, 1, st);
+  tr_fourier_forward(m, F.zdtdt, F.fzdtdt, LP, st);
+  tr_legendre_forward(m, F.fzdtdt, F.zstt1, LP, m.sh.qc, st);
+  tr_dv2uv(m, F.zdsdp2, F.zdszp2, F.fzdu, F.fzdv, LP, 0.f, st);
+  tr_fourier_inverse(m, F.fzdu, F.zdu, LP, st);
+  tr_fourier_inverse(m, F.fzdv, F.zdv, LP, st);
+  dyn_mkdheat(m, 2, st);
+  tr_fourier_forward(m, F.zdekin, F.fzdekin, LP, st);
+  tr_legendre_forward(m, F.fzdekin, F.zsdef, LP, m.sh.qc, st);
+  dyn_mean_mode(m, F.zsdef, st);
+  tr_legendre_inverse(m, F.zsdef, F.fzdekin, LP, m.sh.qi, st);
+  tr_fourier_inverse(m, F.fzdekin, F.zdekin, LP, st);
+  dyn_mkdheat(m, 3, st);
+  tr_fourier_forward(m, F.zdtdt, F.fzdtdt, LP, st);
+  tr_legendre_forward(m, F.fzdtdt, F.zstt2, LP, m.sh.qc, st);
+  dyn_spectrald_update(m, st);
+}
+
+void run_stage(const Model& m, const std::string& s, cudaStream_t st) {
+  if (s == "gridpointa") stage_gridpointa(m, st);
+  else if (s == "spectrala") dyn_spectrala(m, st);
+  else if (s == "physics_in") stage_physics_in(m, st);
+  else if (s == "fixer") phy_fixer(m, st);
+  else if (s == "surface_flux") phy_surface_flux(m, st);
+  else if (s == "radiation") phy_radiation(m, st);
+  else if (s == "precipitation") stage_precipitation(m, st);
+  else if (s == "surface") phy_surface(m, st);
+  else if (s == "carbon") phy_carbon(m, st);
+  else if (s == "physics_out") stage_physics_out(m, st);
+  else if (s == "spectrald") stage_spectrald(m, st);
+  else if (s == "pack") phy_pack(m, st);
+  else throw Error(EXOGCM_EINVAL, "unknown stage " + s);
+}
+
+// master's step order (stepper/index.ts:148-161).
+void full_step(const Model& m, cudaStream_t st) {
+  stage_gridpointa(m, st);
+  dyn_spectrala(m, st);
+  stage_physics_in(m, st);
+  phy_fixer(m, st);
+  phy_surface_flux(m, st);
+  phy_radiation(m, st);
+  stage_precipitation(m, st);
+  phy_surface(m, st);
+  phy_carbon(m, st);
+  stage_physics_out(m, st);
+  stage_spectrald(m, st);
+  phy_pack(m, st);
+}
+
+// The host values of one slot's next step; advances the slot's counters when
+// `advance` (stepper/index.ts:281-334 with the start-up schedule of
+// runner/webgpu/gcm.worker.ts:137-153: start-up steps at the start step's
+// date with halved timesteps, no filter and no icestep).
+StepParams next_params(Slot& s, int publish_every, bool advance) {
+  StepParams p{};
+  if (!s.active) return p;
+  const int phase = s.startup_left;
+  p.phase = phase;
+  p.active = 1;
+  p.delt = (float)s.delt[phase];
+  p.delt2 = (float)(s.delt[phase] + s.delt[phase]);
+  p.deltsec = (float)s.deltsec[phase];
+  p.deltsec2 = (float)(s.deltsec[phase] + s.deltsec[phase]);
+  p.filter = phase == 0 ? 1.f : 0.f;
+  p.coupled = phase == 0 ? 1.f : 0.f;
+  const StepValues v = step_values(s.cal, s.step, s.carbon_step);
+  for (int i = 0; i < 5; ++i) p.rad[i] = (float)v.rad[i];
+  for (int i = 0; i < 7; ++i) p.surf[i] = (float)v.surf[i];
+  p.carbon = (float)v.carbon;
+  p.snap[0] = (float)s.step;
+  p.snap[1] = (float)s.cal.output_window_steps;
+  const bool publish = phase == 0 && publish_every > 0 && s.step % publish_every == 0;
+  p.snap[2] = publish ? 1.f : 0.f;
+  if (advance) {
+    s.carbon_step = v.next_carbon_step;
+    if (publish) s.published = s.step;
+    if (phase > 0)
+      s.startup_left--;
+    else
+      s.step++;
+  }
+  return p;
+}
+
+cudaGraphExec_t batch_graph(exogcm_engine* e, int K) {
+  auto it = e->graphs.find(K);
+  if (it != e->graphs.end()) return it->second;
+  cudaGraph_t graph;
+  check(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed), "capture");
+  for (int k = 0; k < K; ++k) full_step(e->model(k), e->stream);
+  check(cudaStreamEndCapture(e->stream, &graph), "capture end");
+  cudaGraphExec_t exec;
+  check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+  cudaGraphDestroy(graph);
+  e->graphs[K] = exec;
+  return exec;
+}
+
+void upload_slot_tables(exogcm_engine* e, int slot, const PlanetSetup& ps) {
+  std::vector<float> block(e->to.stride, 0.f);
+  int off = 0;
+  for (auto& t : e->tab_list) {
+    auto it = ps.tables.find(t.first);
+    if (it == ps.tables.end()) throw Error(EXOGCM_EINVAL, "set-up lacks table " + t.first);
+    const Vec& v = it->second;
+    for (int i = 0; i < t.second && i < (int)v.size(); ++i) block[off + i] = (float)v[i];
+    off += t.second;
+  }
+  check(cudaMemcpy(e->tabs + (size_t)slot * e->to.stride, block.data(), block.size() * sizeof(float),
+                   cudaMemcpyHostToDevice),
+        "slot tables");
+  PlanetConst pc{};
+#define EXOGCM_SET_CONST(n)                                                    \
+  {                                                                            \
+    auto c = ps.consts.find(#n);                                               \
+    if (c == ps.consts.end()) throw Error(EXOGCM_EINVAL, "set-up lacks " #n);  \
+    pc.n = (float)c->second;                                                   \
+  }
+  EXOGCM_CONSTS(EXOGCM_SET_CONST)
+#undef EXOGCM_SET_CONST
+  check(cudaMemcpy(e->pc + slot, &pc, sizeof(pc), cudaMemcpyHostToDevice), "slot constants");
+}
+
+void zero_slot(exogcm_engine* e, int slot) {
+  for (auto& fi : e->fields) {
+    float* base = e->arena + fi.offset + (size_t)slot * fi.plane;
+    check(cudaMemset2DAsync(base, fi.plane * e->d.S * sizeof(float), 0, fi.plane * sizeof(float), fi.count,
+                            e->stream),
+          "zero slot");
+  }
+}
+
+template <typename F>
+int guard(F&& f) {
+  try {
+    f();
+    return EXOGCM_OK;
+  } catch (const Error& err) {
+    g_error = err.what();
+    return err.code;
+  } catch (const std::invalid_argument& err) {
+    g_error = err.what();
+    return EXOGCM_EINVAL;
+  } catch (const std::bad_alloc&) {
+    g_error = "host allocation failed";
+    return EXOGCM_ENOMEM;
+  } catch (const std::exception& err) {
+    g_error = err.what();
+    return EXOGCM_EDEVICE;
+  }
+}
+
+// ---------------------------------------------------------------- checkpoint
+const char kMagic[] = "GCM-WEBGPU-STATE\n";
+
+std::string header_json(exogcm_engine* e, long step, int carbon_step) {
+  std::string s = "{\"fields\":[";
+  for (size_t i = 0; i < e->fields.size(); ++i) {
+    const FieldInfo& fi = e->fields[i];
+    if (i) s += ",";
+    s += "[\"" + fi.name + "\"," + std::to_string(fi.plane * fi.count) + "]";
+  }
+  s += "],\"step\":" + std::to_string(step) + ",\"carbonStep\":" + std::to_string(carbon_step) + "}";
+  return s;
+}
+
+long json_number(const std::string& s, const char* key) {
+  const std::string k = std::string("\"") + key + "\":";
+  const size_t at = s.find(k);
+  if (at == std::string::npos) throw Error(EXOGCM_ELAYOUT, std::string("checkpoint header lacks ") + key);
+  return std::stol(s.substr(at + k.size()));
+}
+
+}  // namespace
+
+// ================================================================= C ABI
+extern "C" {
+
+int exogcm_last_error(char* buffer, size_t size) {
+  if (!buffer || size == 0) return EXOGCM_EINVAL;
+  std::snprintf(buffer, size, "%s", g_error.c_str());
+  return EXOGCM_OK;
+}
+
+int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine** out) {
+  return guard([&] {
+    if (!out) throw Error(EXOGCM_EINVAL, "null engine pointer");
+    *out = nullptr;
+    if (truncation != 21 && truncation != 42 && truncation != 63)
+      throw Error(EXOGCM_EINVAL, "truncation must be 21, 42 or 63");
+    if (levels != 5 && levels != 10) throw Error(EXOGCM_EINVAL, "levels must be 5 or 10");
+    if (slots < 1 || slots > 4096) throw Error(EXOGCM_EINVAL, "slots must be 1..4096");
+    if (mode != 0) throw Error(EXOGCM_EINVAL, "mode must be 0 (plain FP32)");
+    auto e = std::make_unique<exogcm_engine>();
+    e->d = make_dims(truncation, levels, slots);
+    e->mode = mode;
+    check(cudaGetDevice(&e->device), "device");
+    layout(e.get());
+    table_layout(e.get());
+    if (cudaMalloc(&e->arena, e->arena_floats * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error(EXOGCM_ENOMEM, "device memory for the state arena (" +
+                                     std::to_string(e->arena_floats * 4 / (1 << 20)) + " MiB) not available");
+    }
+    check(cudaMemset(e->arena, 0, e->arena_floats * sizeof(float)), "arena clear");
+    bind_fields(e.get());
+    check(cudaMalloc(&e->tabs, (size_t)slots * e->to.stride * sizeof(float)), "slot tables");
+    check(cudaMemset(e->tabs, 0, (size_t)slots * e->to.stride * sizeof(float)), "slot tables");
+    check(cudaMalloc(&e->pc, slots * sizeof(PlanetConst)), "constants");
+    check(cudaMemset(e->pc, 0, slots * sizeof(PlanetConst)), "constants");
+    check(cudaMalloc(&e->params, (size_t)kMaxBatch * slots * sizeof(StepParams)), "params");
+    check(cudaMemset(e->params, 0, (size_t)kMaxBatch * slots * sizeof(StepParams)), "params");
+    check(cudaMallocHost(&e->hparams, (size_t)kMaxBatch * slots * sizeof(StepParams)), "pinned params");
+    check(cudaMalloc(&e->sums, (size_t)slots * 4 * sizeof(double)), "sums");
+    check(cudaMemset(e->sums, 0, (size_t)slots * 4 * sizeof(double)), "sums");
+    check(cudaMalloc(&e->flags, slots * sizeof(int)), "flags");
+    check(cudaMemset(e->flags, 0, slots * sizeof(int)), "flags");
+    check(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "stream");
+    check(cudaEventCreate(&e->ev0), "event");
+    check(cudaEventCreate(&e->ev1), "event");
+    tr_init();
+    e->slots.resize(slots);
+    *out = e.release();
+  });
+}
+
+void exogcm_destroy(exogcm_engine* e) {
+  if (!e) return;
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  for (auto& g : e->graphs) cudaGraphExecDestroy(g.second);
+  cudaFree(e->arena);
+  cudaFree(e->shared_buf);
+  cudaFree(e->mode_buf);
+  cudaFree(e->tabs);
+  cudaFree(e->pc);
+  cudaFree(e->params);
+  cudaFreeHost(e->hparams);
+  cudaFree(e->sums);
+  cudaFree(e->flags);
+  if (e->ev0) cudaEventDestroy(e->ev0);
+  if (e->ev1) cudaEventDestroy(e->ev1);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+int exogcm_configure(exogcm_engine* e, int slot, const exogcm_planet* planet, const exogcm_boundary* boundary) {
+  return guard([&] {
+    if (!e || !planet || !boundary) throw Error(EXOGCM_EINVAL, "null argument");
+    check_slot(e, slot);
+    if (planet->truncation != e->d.T || planet->levels != e->d.L)
+      throw Error(EXOGCM_EINVAL, "planet resolution differs from the engine's");
+    if (!e->shared_ready) {
+      SharedSetup sh = build_shared(e->d.T, planet->filter_kind, planet->filter_gp, planet->filter_sp);
+      upload_shared(e, sh);
+      e->filter_kind = planet->filter_kind;
+      e->filter_gp = planet->filter_gp;
+      e->filter_sp = planet->filter_sp;
+    } else if (planet->filter_kind != e->filter_kind || planet->filter_gp != e->filter_gp ||
+               planet->filter_sp != e->filter_sp) {
+      throw Error(EXOGCM_EINVAL, "planets of one engine share the physics filter setting");
+    }
+    SharedSetup sh = build_shared(e->d.T, e->filter_kind, e->filter_gp, e->filter_sp);
+    PlanetSetup ps = build_planet(*planet, *boundary, sh);
+    zero_slot(e, slot);
+    for (auto& kv : ps.state) {
+      const FieldInfo& fi = field(e, kv.first.c_str());
+      const size_t n = fi.plane * fi.count;
+      if (kv.second.size() != n) throw Error(EXOGCM_EINVAL, "set-up field " + kv.first + " has the wrong size");
+      std::vector<float> f(kv.second.begin(), kv.second.end());
+      copy_field(e, fi, slot, f.data(), true);
+    }
+    upload_slot_tables(e, slot, ps);
+    int zero = 0;
+    check(cudaMemcpy(e->flags + slot, &zero, sizeof(int), cudaMemcpyHostToDevice), "flags");
+    Slot& s = e->slots[slot];
+    s = Slot{};
+    s.active = true;
+    s.step = ps.start_step;
+    s.carbon_step = 0;
+    s.startup_left = ps.nkits;
+    for (int k = 0; k < 4; ++k) {
+      s.deltsec[k] = ps.deltsec[k];
+      s.delt[k] = ps.delt[k];
+    }
+    s.cal = ps.cal;
+    check(cudaStreamSynchronize(e->stream), "configure");
+  });
+}
+
+int exogcm_setup_preview(const exogcm_planet* planet, const exogcm_boundary* boundary, const char* name,
+                         double* values, size_t* count) {
+  return guard([&] {
+    if (!planet || !boundary || !name || !count) throw Error(EXOGCM_EINVAL, "null argument");
+    const SharedSetup sh = build_shared(planet->truncation, planet->filter_kind, planet->filter_gp, planet->filter_sp);
+    const PlanetSetup ps = build_planet(*planet, *boundary, sh);
+    const std::string n(name);
+    const size_t colon = n.find(':');
+    if (colon == std::string::npos) throw Error(EXOGCM_EINVAL, "name needs a kind: prefix");
+    const std::string kind = n.substr(0, colon), key = n.substr(colon + 1);
+    Vec out;
+    if (kind == "state") {
+      auto it = ps.state.find(key);
+      if (it == ps.state.end()) throw Error(EXOGCM_EINVAL, "no initial field " + key);
+      out = it->second;
+    } else if (kind == "table") {
+      auto it = ps.tables.find(key);
+      if (it == ps.tables.end()) throw Error(EXOGCM_EINVAL, "no table " + key);
+      out = it->second;
+    } else if (kind == "const") {
+      auto it = ps.consts.find(key);
+      if (it == ps.consts.end()) throw Error(EXOGCM_EINVAL, "no constant " + key);
+      out = {it->second};
+    } else if (kind == "shared") {
+      if (key == "fwd") out = sh.fwd;
+      else if (key == "inv") out = sh.inv;
+      else if (key == "sines") out = sh.sines;
+      else if (key == "weights") out = sh.weights;
+      else {
+        auto it = sh.q.find(key);
+        if (it == sh.q.end()) throw Error(EXOGCM_EINVAL, "no shared table " + key);
+        out = it->second;
+      }
+    } else if (kind == "calendar") {
+      const long step = std::stol(key);
+      const StepValues v = step_values(ps.cal, step, 0);
+      out.assign(v.rad, v.rad + 5);
+      out.insert(out.end(), v.surf, v.surf + 7);
+      out.push_back(v.carbon);
+      out.push_back(v.next_carbon_step);
+      out.push_back((double)ps.start_step);
+      out.push_back(ps.nkits);
+    } else {
+      throw Error(EXOGCM_EINVAL, "unknown kind " + kind);
+    }
+    if (values) {
+      if (*count < out.size()) throw Error(EXOGCM_EINVAL, "buffer too small");
+      std::copy(out.begin(), out.end(), values);
+    }
+    *count = out.size();
+  });
+}
+
+int exogcm_release(exogcm_engine* e, int slot) {
+  return guard([&] {
+    if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    check_slot(e, slot);
+    e->slots[slot].active = false;
+    e->slots[slot].published = -1;
+  });
+}
+
+int exogcm_step(exogcm_engine* e, int steps, int publish_every) {
+  return guard([&] {
+    if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    if (steps < 1 || steps > kMaxBatch) throw Error(EXOGCM_EINVAL, "steps must be 1..64");
+    if (publish_every < 1 || steps > publish_every)
+      throw Error(EXOGCM_EINVAL, "publish_every must be >= steps so each slot publishes at most once");
+    if (!e->shared_ready) throw Error(EXOGCM_ESTATE, "no slot configured");
+    const int S = e->d.S;
+    for (int s = 0; s < S; ++s) e->slots[s].published = -1;
+    for (int k = 0; k < steps; ++k)
+      for (int s = 0; s < S; ++s) e->hparams[(size_t)k * S + s] = next_params(e->slots[s], publish_every, true);
+    check(cudaMemcpyAsync(e->params, e->hparams, (size_t)steps * S * sizeof(StepParams), cudaMemcpyHostToDevice,
+                          e->stream),
+          "params upload");
+    cudaGraphExec_t g = batch_graph(e, steps);
+    check(cudaEventRecord(e->ev0, e->stream), "event");
+    check(cudaGraphLaunch(g, e->stream), "graph launch");
+    check(cudaEventRecord(e->ev1, e->stream), "event");
+    phy_finite_check(e->model(steps - 1), e->stream);
+    check(cudaStreamSynchronize(e->stream), "step");
+    check(cudaEventElapsedTime(&e->last_ms, e->ev0, e->ev1), "event time");
+  });
+}
+
+int exogcm_read_snapshot(exogcm_engine* e, int slot, float* values, size_t count, long* step) {
+  return guard([&] {
+    if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    check_slot(e, slot);
+    const long pub = e->slots[slot].published;
+    if (step) *step = pub;
+    if (!values || pub < 0) return;
+    const FieldInfo& fi = field(e, "snapshot");
+    if (count != fi.plane * fi.count) throw Error(EXOGCM_EINVAL, "snapshot buffer size mismatch");
+    copy_field(e, fi, slot, values, false);
+  });
+}
+
+int exogcm_slot_info(exogcm_engine* e, int slot, long* step, int* startup_left, int* active) {
+  return guard([&] {
+    if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    check_slot(e, slot);
+    if (step) *step = e->slots[slot].step;
+    if (startup_left) *startup_left = e->slots[slot].startup_left;
+    if (active) *active = e->slots[slot].active ? 1 : 0;
+  });
+}
+
+int exogcm_field_size(exogcm_engine* e, const char* name, size_t* count) {
+  return guard([&] {
+    if (!e || !count) throw Error(EXOGCM_EINVAL, "null argument");
+    const FieldInfo& fi = field(e, name);
+    *count = fi.plane * fi.count;
+  });
+}
+
+int exogcm_read_field(exogcm_engine* e, int slot, const char* name, float* values, size_t count) {
+  return guard([&] {
+    if (!e || !values) throw Error(EXOGCM_EINVAL, "null argument");
+    check_slot(e, slot);
+    const FieldInfo& fi = field(e, name);
+    if (count != fi.plane * fi.count) throw Error(EXOGCM_EINVAL, std::string(name) + ": wrong value count");
+    copy_field(e, fi, slot, values, false);
+  });
+}
+
+int exogcm_write_field(exogcm_engine* e, int slot, const char* name, const float* values, size_t count) {
+  return guard([&] {
+    if (!e || !values) throw Error(EXOGCM_EINVAL, "null argument");
+    check_slot(e, slot);
+    const FieldInfo& fi = field(e, name);
+    if (count != fi.plane * fi.count) throw Error(EXOGCM_EINVAL, std::string(name) + ": wrong value count");
+    copy_field(e, fi, slot, const_cast<float*>(values), true);
+  });
+}
+
+int exogcm_read_table(exogcm_engine* e, int slot, const char* name, float* values, size_t count) {
+  return guard([&] {
+    if (!e || !values || !name) throw Error(EXOGCM_EINVAL, "null argument");
+    check_slot(e, slot);
+    int off = 0;
+    for (auto& t : e->tab_list) {
+      if (t.first == name) {
+        if ((int)count != t.second) throw Error(EXOGCM_EINVAL, "table size mismatch");
+        check(cudaMemcpy(values, e->tabs + (size_t)slot * e->to.stride + off, count * sizeof(float),
+                         cudaMemcpyDeviceToHost),
+              "read table");
+        return;
+      }
+      off += t.second;
+    }
+    throw Error(EXOGCM_EINVAL, std::string("no table ") + name);
+  });
+}
+
+int exogcm_checkpoint_save(exogcm_engine* e, int slot, void** buffer, size_t* size) {
+  return guard([&] {
+    if (!e || !buffer || !size) throw Error(EXOGCM_EINVAL, "null argument");
+    check_slot(e, slot);
+    const Slot& s = e->slots[slot];
+    if (!s.active) throw Error(EXOGCM_ESTATE, "slot is not running");
+    if (s.startup_left > 0) throw Error(EXOGCM_ESTATE, "slot is still in its start-up steps");
+    const std::string json = header_json(e, s.step, s.carbon_step);
+    const size_t mlen = sizeof(kMagic) - 1;
+    const size_t start = (mlen + 4 + json.size() + 3) / 4 * 4;
+    size_t floats = 0;
+    for (auto& fi : e->fields) floats += fi.plane * fi.count;
+    const size_t total = start + floats * 4;
+    unsigned char* out = static_cast<unsigned char*>(std::calloc(total, 1));
+    if (!out) throw Error(EXOGCM_ENOMEM, "checkpoint buffer");
+    std::memcpy(out, kMagic, mlen);
+    const uint32_t len = (uint32_t)json.size();
+    std::memcpy(out + mlen, &len, 4);  // little-endian hosts
+    std::memcpy(out + mlen + 4, json.data(), json.size());
+    float* data = reinterpret_cast<float*>(out + start);
+    try {
+      for (auto& fi : e->fields) {
+        copy_field(e, fi, slot, data, false);
+        data += fi.plane * fi.count;
+      }
+    } catch (...) {
+      std::free(out);
+      throw;
+    }
+    *buffer = out;
+    *size = total;
+  });
+}
+
+int exogcm_checkpoint_load(exogcm_engine* e, int slot, const void* buffer, size_t size) {
+  return guard([&] {
+    if (!e || !buffer) throw Error(EXOGCM_EINVAL, "null argument");
+    check_slot(e, slot);
+    Slot& s = e->slots[slot];
+    if (!s.active) throw Error(EXOGCM_ESTATE, "configure the slot before loading a checkpoint");
+    const unsigned char* in = static_cast<const unsigned char*>(buffer);
+    const size_t mlen = sizeof(kMagic) - 1;
+    if (size < mlen + 4 || std::memcmp(in, kMagic, mlen) != 0)
+      throw Error(EXOGCM_ELAYOUT, "This checkpoint was not saved by the WebGPU model");
+    uint32_t len;
+    std::memcpy(&len, in + mlen, 4);
+    if (mlen + 4 + (size_t)len > size) throw Error(EXOGCM_ELAYOUT, "truncated checkpoint header");
+    const std::string json(reinterpret_cast<const char*>(in + mlen + 4), len);
+    const std::string expected = header_json(e, 0, 0);
+    const size_t cut = expected.find("],\"step\"");
+    if (json.compare(0, cut, expected, 0, cut) != 0)
+      throw Error(EXOGCM_ELAYOUT, "This checkpoint's model state does not match this version of the model");
+    const long step = json_number(json, "step");
+    const long carbon = json_number(json, "carbonStep");
+    const size_t start = (mlen + 4 + len + 3) / 4 * 4;
+    size_t floats = 0;
+    for (auto& fi : e->fields) floats += fi.plane * fi.count;
+    if (start + floats * 4 != size) throw Error(EXOGCM_ELAYOUT, "checkpoint data size does not match its header");
+    std::vector<float> buf;
+    const unsigned char* data = in + start;
+    for (auto& fi : e->fields) {
+      const size_t n = fi.plane * fi.count;
+      buf.resize(n);
+      std::memcpy(buf.data(), data, n * 4);
+      copy_field(e, fi, slot, buf.data(), true);
+      data += n * 4;
+    }
+    s.step = step;
+    s.carbon_step = (int)carbon;
+    s.startup_left = 0;
+    s.published = -1;
+  });
+}
+
+void exogcm_free(void* buffer) { std::free(buffer); }
+
+int exogcm_unstable(exogcm_engine* e, int* flags, int n) {
+  return guard([&] {
+    if (!e || !flags || n != e->d.S) throw Error(EXOGCM_EINVAL, "flags must hold one int per slot");
+    check(cudaMemcpy(flags, e->flags, n * sizeof(int), cudaMemcpyDeviceToHost), "flags");
+  });
+}
+
+int exogcm_run_stage(exogcm_engine* e, const char* stage) {
+  return guard([&] {
+    if (!e || !stage) throw Error(EXOGCM_EINVAL, "null argument");
+    if (!e->shared_ready) throw Error(EXOGCM_ESTATE, "no slot configured");
+    const int S = e->d.S;
+    for (int s = 0; s < S; ++s) {
+      Slot copy = e->slots[s];
+      e->hparams[s] = next_params(copy, 1 << 30, false);
+    }
+    check(cudaMemcpyAsync(e->params, e->hparams, S * sizeof(StepParams), cudaMemcpyHostToDevice, e->stream),
+          "params");
+    run_stage(e->model(0), stage, e->stream);
+    check(cudaGetLastError(), "stage launch");
+    check(cudaStreamSynchronize(e->stream), "stage");
+  });
+}
+
+int exogcm_last_step_ms(exogcm_engine* e, float* ms) {
+  return guard([&] {
+    if (!e || !ms) throw Error(EXOGCM_EINVAL, "null argument");
+    *ms = e->last_ms;
+  });
+}
+
+int exogcm_device_field(exogcm_engine* e, const char* name, void** pointer, size_t* floats) {
+  return guard([&] {
+    if (!e || !pointer) throw Error(EXOGCM_EINVAL, "null argument");
+    const FieldInfo& fi = field(e, name);
+    *pointer = e->arena + fi.offset;
+    if (floats) *floats = fi.plane * fi.count * e->d.S;
+  });
+}
+
+void* exogcm_stream(exogcm_engine* e) { return e ? (void*)e->stream : nullptr; }
+
+}  // extern "C"

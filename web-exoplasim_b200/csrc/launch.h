@@ -1,0 +1,43 @@
+// Host-side launchers of the step's kernels (one call each, all slots).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace exogcm {
+
+// transforms.cu
+void tr_init();
+void tr_fourier_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st);
+void tr_fourier_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st);
+void tr_dlambda(const Model& m, const float* a, float* b, int planes, cudaStream_t st);
+void tr_legendre_inverse(const Model& m, const float* s, float* f, int planes, const float* q, cudaStream_t st);
+void tr_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V, int planes, float plavor,
+              cudaStream_t st);
+void tr_legendre_forward(const Model& m, const float* f, float* s, int planes, const float* q, cudaStream_t st);
+void tr_uv2dv(const Model& m, const float* u, const float* v, const float* ke, float* D, float* Z, int planes,
+              cudaStream_t st);
+void tr_qtend(const Model& m, const float* u, const float* v, const float* src, float* out, int planes,
+              cudaStream_t st);
+
+// dynamics.cu
+void dyn_calcgp(const Model& m, cudaStream_t st);
+void dyn_spectrala(const Model& m, cudaStream_t st);
+void dyn_spectrald_diffusion(const Model& m, cudaStream_t st);
+void dyn_mkdheat(const Model& m, int stage, cudaStream_t st);
+void dyn_mean_mode(const Model& m, float* target, cudaStream_t st);
+void dyn_spectrald_update(const Model& m, cudaStream_t st);
+void dyn_physics_in(const Model& m, cudaStream_t st);
+void dyn_physics_out(const Model& m, cudaStream_t st);
+
+// physics.cu
+void phy_fixer(const Model& m, cudaStream_t st);
+void phy_surface_flux(const Model& m, cudaStream_t st);
+void phy_radiation(const Model& m, cudaStream_t st);
+void phy_precipitation_columns(const Model& m, cudaStream_t st);
+void phy_surface(const Model& m, cudaStream_t st);
+void phy_carbon(const Model& m, cudaStream_t st);
+void phy_pack(const Model& m, cudaStream_t st);
+void phy_finite_check(const Model& m, cudaStream_t st);
+
+}  // namespace exogcm

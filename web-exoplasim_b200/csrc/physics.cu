@@ -1,0 +1,2013 @@
+// Column physics of the GCM step for every slot of a batch (FP32), plus the
+// per-planet reductions and the snapshot pack.
+//
+// Arithmetic follows src/model/climate/gcm/physics/*/wgsl/*.wgsl and
+// snapshot/wgsl/pack.wgsl (ExoPlaSim's miscmod fixer, fluxmod, radmod,
+// rainmod, landmod, vegmod, glaciermod, icemod, oceanmod, seamod,
+// carbonmod). One thread owns one column c = slot * NHOR + h of the batch and
+// keeps its levels in registers (kernels are instantiated per level count).
+// The reference's per-planet global sums (fixer, getiflx) and the mkdca pass
+// limit run as one block per slot with a fixed summation order, in FP64.
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "common.cuh"
+#include "launch.h"
+
+namespace exogcm {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+#define COLUMN_PROLOGUE                                              \
+  const Dims& d = m.d;                                               \
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;               \
+  if (c >= d.S * d.NHOR) return;                                     \
+  const int slot = c / d.NHOR;                                       \
+  const int h = c % d.NHOR;                                          \
+  const StepParams& P = m.params[slot];                              \
+  if (!P.active) return;                                             \
+  const PlanetConst& K = m.pc[slot];                                 \
+  const float* tb = m.tabs + (size_t)slot * m.to.stride;             \
+  const size_t SN = (size_t)d.S * d.NHOR;                            \
+  const FieldPtrs& F = m.f;                                          \
+  (void)h; (void)K; (void)tb; (void)SN; (void)F; (void)P;
+
+__device__ __forceinline__ float sat_capped(const PlanetConst& K, float t, float p) {
+  return fminf(K.RDBRV * K.RA1 * expf(K.RA2 * (t - K.TMELT) / (t - K.RA4)) / p, K.RDBRV);
+}
+__device__ __forceinline__ float sat_divided(const PlanetConst& K, float t, float p) {
+  const float q = sat_capped(K, t, p);
+  return q / (1.f - K.MOIST * q);
+}
+// x^y for x >= 0 with 0^y = 0, as Fortran's powf gives (precise.wgsl's
+// precise_pow semantics with CUDA's own powf).
+__device__ __forceinline__ float fpow(float x, float y) { return x == 0.f ? 0.f : powf(x, y); }
+// x^n by binary exponentiation, as libgcc's __powisf2 computes x**n.
+__device__ __forceinline__ float powi(float x, int n) {
+  float base = x;
+  unsigned mm = (unsigned)abs(n);
+  float result = (mm & 1u) ? x : 1.f;
+  mm >>= 1;
+  while (mm) {
+    base = base * base;
+    if (mm & 1u) result = result * base;
+    mm >>= 1;
+  }
+  return n < 0 ? 1.f / result : result;
+}
+
+// ---------------------------------------------------------------- fixer
+// physics/fixer/wgsl/column.wgsl: fix0d per column.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_fixer_column(Model m) {
+  COLUMN_PROLOGUE
+  const float* ds = tb + m.to.dsigma;
+  float negative = 0.f, positive = 0.f;
+  for (int l = 0; l < NL; ++l) {
+    const float dq = F.dq[l * SN + c];
+    const float q = dq * ds[l];
+    if (dq < 0.f) negative = negative + q;
+    if (dq > 0.f) positive = positive + q;
+  }
+  const float zgw = m.sh.zgw[h];
+  float zneg = -negative * F.dp[c] * zgw;
+  float zpos = positive * F.dp[c] * zgw;
+  float factor = 1.f;
+  const bool fixed = zneg > 0.f && zpos >= zneg;
+  if (fixed) {
+    factor = (zpos - zneg) / zpos;
+    zneg = 0.f;
+    zpos = zpos * factor;
+  }
+  for (int l = 0; l < NL; ++l) {
+    const float q = F.dq[l * SN + c];
+    F.fixq[l * SN + c] = fixed ? fmaxf(q * factor, 0.f) : q;
+  }
+  F.fixneg[c] = zneg;
+  F.fixpos[c] = zpos;
+}
+
+// physics/fixer/wgsl/row.wgsl: fix1d per latitude row, summed in longitude order.
+template <int NL>
+__global__ void k_fixer_row(Model m) {
+  const Dims& d = m.d;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= d.S * d.NLAT) return;
+  const int slot = r / d.NLAT;
+  if (!m.params[slot].active) return;
+  const size_t SN = (size_t)d.S * d.NHOR;
+  const FieldPtrs& F = m.f;
+  const int first = r * d.NLON;  // slot * NHOR + lat * NLON
+  float zneg = 0.f;
+  for (int j = 0; j < d.NLON; ++j) zneg = zneg + F.fixneg[first + j];
+  if (zneg <= 0.f) return;
+  float zpos = 0.f;
+  for (int j = 0; j < d.NLON; ++j) zpos = zpos + F.fixpos[first + j];
+  if (zpos < zneg) return;
+  const float factor = (zpos - zneg) / zpos;
+  for (int j = 0; j < d.NLON; ++j) {
+    for (int l = 0; l < NL; ++l) {
+      float& q = F.fixq[l * SN + first + j];
+      q = fmaxf(q * factor, 0.f);
+    }
+    F.fixneg[first + j] = 0.f;
+    F.fixpos[first + j] = F.fixpos[first + j] * factor;
+  }
+}
+
+// Per-slot global sums of two grid fields in FP64 with a fixed order (the
+// reference's reduction/wgsl/sum.wgsl, kept in double as the build asks of
+// global budget reductions). Writes the sums as floats to target[0|1 * S + slot]
+// and as doubles to sums[slot * 4 + which * 2 + 0|1].
+constexpr int kSumThreads = 256;
+__global__ void __launch_bounds__(kSumThreads) k_slot_sums(Model m, const float* a, const float* b, float* target,
+                                                           int which) {
+  const Dims& d = m.d;
+  const int slot = blockIdx.x;
+  if (!m.params[slot].active) return;
+  if (which == 1 && m.params[slot].coupled == 0.f) return;  // getiflx runs with icestep only
+  __shared__ double sa[kSumThreads], sb[kSumThreads];
+  double x = 0.0, y = 0.0;
+  const size_t base = (size_t)slot * d.NHOR;
+  for (int h = threadIdx.x; h < d.NHOR; h += kSumThreads) {
+    x += (double)a[base + h];
+    y += (double)b[base + h];
+  }
+  sa[threadIdx.x] = x;
+  sb[threadIdx.x] = y;
+  __syncthreads();
+  for (int stride = kSumThreads / 2; stride > 0; stride /= 2) {
+    if (threadIdx.x < stride) {
+      sa[threadIdx.x] += sa[threadIdx.x + stride];
+      sb[threadIdx.x] += sb[threadIdx.x + stride];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    target[slot] = (float)sa[0];
+    target[d.S + slot] = (float)sb[0];
+    m.sums[slot * 4 + which * 2] = sa[0];
+    m.sums[slot * 4 + which * 2 + 1] = sb[0];
+  }
+}
+
+// physics/fixer/wgsl/apply.wgsl: the global step, gqdt and the new dq.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_fixer_apply(Model m) {
+  COLUMN_PROLOGUE
+  const double zzneg = m.sums[slot * 4], zzpos = m.sums[slot * 4 + 1];
+  const float scale = zzneg > 0.0 ? (float)((zzpos - zzneg) / zzpos) : 1.f;
+  const float dp = F.dp[c];
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    float q = F.fixq[at];
+    if (zzneg > 0.0) q = fmaxf(q * scale, 0.f);
+    F.gqdt[at] = F.gqdt[at] + dp * (q - F.dq[at]) / P.delt2 / K.PSURF;
+    F.dq[at] = q;
+  }
+}
+
+// ---------------------------------------------------------------- surface flux
+// physics/surface-flux/wgsl/surflx.wgsl: transfer coefficients, implicit
+// stress, sensible heat and evaporation.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_surflx(Model m) {
+  COLUMN_PROLOGUE
+  const int low = NL - 1;
+  const size_t lo = low * SN + c, sf = NL * SN + c;
+  const float u = F.du[lo], v = F.dv[lo], t = F.dt[lo], q = F.dq[lo], ts = F.dt[sf], qs = F.dq[sf];
+  const float dp = F.dp[c], dls = F.dls[c];
+  const float dsigma = tb[m.to.dsigma + low];
+  const float zfac = tb[m.to.flux_sigfac], zlnsig = tb[m.to.flux_lnsig];
+  const float moisture = 1.f / K.RDBRV - 1.f;
+  const float VK = 0.4f;
+  const float D2 = P.deltsec2;
+  float dtsa = t * zfac * (1.f + moisture * q);
+  const float zabsu2 = fmaxf(K.ZUMIN, u * u + v * v);
+  const float znl = -K.GASCON * 0.5f * (t + dtsa) * zlnsig / K.GA;
+  const float zbz0 = znl / F.dz0[c];
+  const float zri = K.GA * znl / (zabsu2 * dtsa) * (dtsa - ts * (1.f + moisture * qs));
+  const float zkblnz = VK / logf(zbz0 + 1.f);
+  const float zkblnz2 = zkblnz * zkblnz;
+  float zrifm, zrifh;
+  if (zri <= 0.f) {
+    const float zdenom = 1.f + 3.f * K.VDIFF_C * K.VDIFF_B * sqrtf(-1.f * zri * (zbz0 + 1.f)) * zkblnz2;
+    zrifm = 1.f - 2.f * K.VDIFF_B * zri / zdenom;
+    if (dls < 1.f) {
+      const float zdth = -(dtsa - ts * (1.f + moisture * qs));
+      zrifh = powf(1.f + powf(0.0016f * powf(zdth, 1.f / 3.f) / sqrtf(zabsu2) / zkblnz2, 1.25f), 0.8f);
+    } else {
+      zrifh = 1.f - 3.f * K.VDIFF_B * zri / zdenom;
+    }
+  } else {
+    const float zdenom = sqrtf(1.f + K.VDIFF_D * zri);
+    zrifh = 1.f / (1.f + 3.f * K.VDIFF_B * zri * zdenom);
+    zrifm = 1.f / (1.f + 2.f * K.VDIFF_B * zri / zdenom);
+  }
+  const float ztrans = sqrtf(zabsu2) * zkblnz2;
+  const float transh = ztrans * zrifh, transm = ztrans * zrifm;
+  F.dtransh[c] = transh;
+  F.dtransm[c] = transm;
+  const float zkonst1 = K.GA * D2 / (K.GASCON * dsigma);
+  const float zkonst2 = dsigma / D2 / K.GA;
+  const float zkdiffm = zkonst1 * transm / ts;
+  const float zun = u / (1.f + zkdiffm), zvn = v / (1.f + zkdiffm);
+  F.dudt[lo] = F.dudt[lo] + (zun - u) / D2;
+  F.dvdt[lo] = F.dvdt[lo] + (zvn - v) / D2;
+  float dtdt = F.dtdt[lo];
+  if (K.NDHEAT != 0.f) dtdt = dtdt + -(zun * zun - u * u + zvn * zvn - v * v) / D2 * 0.5f / K.ACPD / (1.f + K.ADV * q);
+  const float taux = dp * zkonst2 * zkdiffm * zun, tauy = dp * zkonst2 * zkdiffm * zvn;
+  F.dtaux[c] = taux;
+  F.dtauy[c] = tauy;
+  const float ustar = sqrtf(sqrtf(taux * taux + tauy * tauy) * K.GASCON * ts / dp);
+  F.dust3[c] = ustar * ustar * ustar;
+  const float zkdiffh = zkonst1 * transh / ts;
+  const float ztn = (t + zkdiffh * ts) / (1.f + zkdiffh * zfac);
+  dtdt = dtdt + (ztn - t) / D2;
+  F.dtdt[lo] = dtdt;
+  const float moist = fmaxf(1.f, 1.f + K.ADV * q);
+  F.dshfl[c] = zkonst2 * zkdiffh * dp * K.ACPD * moist * (ztn * zfac - ts);
+  F.dshdt[c] = -1.f * zkonst2 * zkdiffh * dp * K.ACPD * moist;
+  dtsa = ztn * zfac;
+  F.dtsa[c] = dtsa;
+  const float zkdiffq = F.drhs[c] * zkonst1 * transh / ts;
+  float zqn = fmaxf(q, (q + zkdiffq * qs) / (1.f + zkdiffq));
+  if (dls > 0.f) zqn = fminf(zqn, F.dwatc[c] / P.deltsec * 1000.f / dp / zkonst2 + q);
+  F.dqdt[lo] = F.dqdt[lo] + (zqn - q) / D2;
+  const float devap = -dp * zkonst2 / 1000.f * (zqn - q);
+  F.devap[c] = devap;
+  const float latent = (ts > K.TMELT || dls < 0.5f) ? K.ALV : K.ALS;
+  const float dlhfl = devap * latent * 1000.f;
+  F.dlhfl[c] = dlhfl;
+  const float curvature = (ts - K.RA4) * (ts - K.RA4);
+  const float dlhdt = -1.f * latent * zkdiffq * zkonst2 * dp * K.RA2 * (K.TMELT - K.RA4) * qs / curvature;
+  F.dlhdt[c] = dlhfl == 0.f ? 0.f : dlhdt;
+}
+
+// physics/diffusion/wgsl/implicit.wgsl: ECHAM tridiagonal eliminations.
+template <int NL>
+__device__ __forceinline__ void diffuse(const float* ds, float* x, const float* k) {
+  float ebs[NL];
+  const float ds0 = ds[0];
+  ebs[0] = k[0] / (ds0 + k[0]);
+  x[0] = ds0 * x[0] / (ds0 + k[0]);
+#pragma unroll
+  for (int l = 1; l < NL - 1; ++l) {
+    const float den = ds[l] + k[l] + k[l - 1] * (1.f - ebs[l - 1]);
+    ebs[l] = k[l] / den;
+    x[l] = (x[l] * ds[l] + k[l - 1] * x[l - 1]) / den;
+  }
+  const float dsn = ds[NL - 1];
+  x[NL - 1] = (x[NL - 1] * dsn + k[NL - 2] * x[NL - 2]) / (dsn + k[NL - 2] * (1.f - ebs[NL - 2]));
+#pragma unroll
+  for (int l = NL - 2; l >= 0; --l) x[l] = x[l] + ebs[l] * x[l + 1];
+}
+
+template <int NL>
+__device__ __forceinline__ void diffuse_potential(const float* ds, float* x, const float* k, const float* skap) {
+  float ebs[NL];
+  const float ds0 = ds[0];
+  ebs[0] = k[0] / (ds0 + k[0] / skap[0]);
+  x[0] = ds0 * x[0] / (ds0 + k[0] / skap[0]);
+#pragma unroll
+  for (int l = 1; l < NL - 1; ++l) {
+    const float den = ds[l] + (k[l] + k[l - 1] * (1.f - ebs[l - 1] / skap[l - 1])) / skap[l];
+    ebs[l] = k[l] / den;
+    x[l] = (x[l] * ds[l] + k[l - 1] / skap[l - 1] * x[l - 1]) / den;
+  }
+  const int last = NL - 1;
+  const float dsn = ds[last];
+  x[last] = (x[last] * dsn + k[NL - 2] * x[NL - 2] / skap[NL - 2]) /
+            (dsn + k[NL - 2] / skap[last] * (1.f - ebs[NL - 2] / skap[NL - 2]));
+#pragma unroll
+  for (int l = NL - 2; l >= 0; --l) x[l] = x[l] + ebs[l] * x[l + 1] / skap[l + 1];
+}
+
+// physics/surface-flux/wgsl/vdiff.wgsl: Richardson-number vertical diffusion.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_vdiff(Model m) {
+  COLUMN_PROLOGUE
+  const float* ds = tb + m.to.dsigma;
+  const float* sh = tb + m.to.sigmah;
+  const float D2 = P.deltsec2;
+  float zt[NL], zq[NL], zu[NL], zv[NL], zabsu[NL], zskap[NL], zskaph[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    zt[l] = F.dt[at] + F.dtdt[at] * D2;
+    zq[l] = F.dq[at] + F.dqdt[at] * D2;
+    zu[l] = F.du[at] + F.dudt[at] * D2;
+    zv[l] = F.dv[at] + F.dvdt[at] * D2;
+    zabsu[l] = sqrtf(zu[l] * zu[l] + zv[l] * zv[l]);
+    zskap[l] = tb[m.to.vdiff_skap + l];
+    zskaph[l] = tb[m.to.vdiff_skaph + l];
+  }
+  const float zkonst1 = K.GA * D2 / K.GASCON;
+  const float zkonst2 = zkonst1 * K.GA / K.GASCON;
+  const float zkonst3 = zkonst2 * K.GA / K.GASCON;
+  const float moisture = 1.f / K.RDBRV - 1.f;
+  float kh[NL], km[NL];
+  kh[NL - 1] = 0.f;
+  km[NL - 1] = 0.f;
+#pragma unroll
+  for (int l = 0; l < NL - 1; ++l) {
+    const int lp = l + 1;
+    const float sigmah = sh[l], dsigma = ds[l], dsigmap = ds[lp];
+    const float zmixh2 = tb[m.to.vdiff_mixh2 + l], zmixm2 = tb[m.to.vdiff_mixm2 + l];
+    const float zrdsig = tb[m.to.vdiff_rdsig + l];
+    const float zfac = zkonst3 * tb[m.to.vdiff_sigmah3 + l];
+    const float zzkfac = tb[m.to.vdiff_kfac + l];
+    const float zrthl = (dsigmap + dsigma) / (zt[l] * dsigmap + zt[lp] * dsigma);
+    const float zdvds = fmaxf(K.ZUMIN, fabsf(zabsu[l] - zabsu[lp])) * zrdsig;
+    const float zdthds =
+        (zt[l] * (1.f + moisture * zq[l]) / zskap[l] - zt[lp] * (1.f + moisture * zq[lp]) / zskap[lp]) * zrdsig;
+    const float zri = zskaph[l] * K.GASCON * zdthds / (sigmah * zdvds * zdvds);
+    float zrifh, zrifm;
+    if (zri <= 0.f) {
+      const float dh = 1.f + 3.f * K.VDIFF_C * K.VDIFF_B * sqrtf(-1.f * zri) * zzkfac * zmixh2;
+      const float dm = 1.f + 3.f * K.VDIFF_C * K.VDIFF_B * sqrtf(-1.f * zri) * zzkfac * zmixm2;
+      zrifh = 1.f - 3.f * K.VDIFF_B * zri / dh;
+      zrifm = 1.f - 2.f * K.VDIFF_B * zri / dm;
+    } else {
+      const float zdenom = sqrtf(1.f + K.VDIFF_D * zri);
+      zrifh = 1.f / (1.f + 3.f * K.VDIFF_B * zri * zdenom);
+      zrifm = 1.f / (1.f + 2.f * K.VDIFF_B * zri / zdenom);
+    }
+    kh[l] = zfac * zmixh2 * zrifh * zdvds * zrthl * zrthl * zrthl;
+    km[l] = zfac * zmixm2 * zrifm * zdvds * zrthl * zrthl * zrthl;
+  }
+  float zun[NL], zvn[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    zun[l] = zu[l];
+    zvn[l] = zv[l];
+  }
+  diffuse<NL>(ds, zun, km);
+  diffuse<NL>(ds, zvn, km);
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    F.dudt[at] = F.dudt[at] + (zun[l] - zu[l]) / D2;
+    F.dvdt[at] = F.dvdt[at] + (zvn[l] - zv[l]) / D2;
+  }
+  if (K.NDHEAT != 0.f) {
+    float zke[NL], zken[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) zke[l] = zken[l] = 0.5f * zabsu[l] * zabsu[l];
+    diffuse<NL>(ds, zken, km);
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+      const size_t at = l * SN + c;
+      const float zdtdt = -((zun[l] * zun[l] - zu[l] * zu[l] + zvn[l] * zvn[l] - zv[l] * zv[l]) / D2 -
+                            (zken[l] - zke[l]) / D2) * 0.5f / K.ACPD / (1.f + K.ADV * F.dq[at]);
+      F.dtdt[at] = F.dtdt[at] + zdtdt;
+    }
+  }
+  float zqn[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) zqn[l] = zq[l];
+  diffuse<NL>(ds, zqn, kh);
+#pragma unroll
+  for (int l = 0; l < NL; ++l) F.dqdt[l * SN + c] = F.dqdt[l * SN + c] + (zqn[l] - zq[l]) / D2;
+#pragma unroll
+  for (int l = 0; l < NL - 1; ++l) kh[l] = kh[l] * zskaph[l];
+  float ztn[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) ztn[l] = zt[l];
+  diffuse_potential<NL>(ds, ztn, kh, zskap);
+#pragma unroll
+  for (int l = 0; l < NL; ++l) F.dtdt[l * SN + c] = F.dtdt[l * SN + c] + (ztn[l] - zt[l]) / D2;
+}
+
+// ---------------------------------------------------------------- radiation
+constexpr float kPI = 3.14159265359f;
+constexpr float kTWOPI = kPI + kPI;
+
+// solang (physics/radiation/wgsl/solang.wgsl) and mko3 (mko3.wgsl) for one column.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_solang_mko3(Model m) {
+  COLUMN_PROLOGUE
+  const int lat = h / d.NLON, lon = h % d.NLON;
+  float hangle = P.rad[2] + (float)lon * K.ZRLON - kPI;
+  if (hangle < -kPI) hangle = hangle + kTWOPI;
+  if (hangle > kPI) hangle = hangle - kTWOPI;
+  if (K.NFIXED == 1.f) hangle = hangle + kPI;
+  const float muz = P.rad[0] * m.sh.sid[lat] + m.sh.cola[lat] * P.rad[1] * cosf(hangle);
+  F.gmu0[c] = muz > K.ZDAWN ? muz : 0.f;
+  if (K.OZONE == 0.f) return;
+  const float ZFO3 = 100.f / 2.14f;
+  const float sid = m.sh.sid[lat];
+  const float za = K.A0O3 + K.A1O3 * fabsf(sid) + K.ACO3 * sid * P.rad[4];
+  const float dp = F.dp[c];
+  const float* ds = tb + m.to.dsigma;
+  const float* lnsig = tb + m.to.rad_lnsig;
+  float o3t = za, zh = 0.f;
+  for (int l = NL - 1; l >= 1; --l) {
+    zh = zh - F.dt[l * SN + c] * K.GASCON / K.GA * lnsig[l];
+    const float o3 = -(za + za * K.ZCONST) / (1.f + expf((zh - K.BO3) / K.CO3)) + o3t;
+    F.dqo3[l * SN + c] = o3 * K.GA / (ZFO3 * ds[l] * dp);
+    o3t = o3t - o3;
+  }
+  F.dqo3[c] = o3t * K.GA / (ZFO3 * ds[0] * dp);
+}
+
+__device__ __forceinline__ float ozone_absorption(float o3, float zsolar1) {
+  return (0.02118f * o3 / (1.f + 0.042f * o3 + 0.000323f * (o3 * o3)) + 1.082f * o3 / fpow(1.f + 138.6f * o3, 0.805f) +
+          0.0658f * o3 / (1.f + (103.6f * o3) * (103.6f * o3) * (103.6f * o3))) /
+         zsolar1;
+}
+__device__ __forceinline__ float vapour_absorption(float wv, float zsolar2) {
+  return 2.9f * wv / (fpow(1.f + 141.5f * wv, 0.635f) + 5.925f * wv) / zsolar2;
+}
+
+// swr (physics/radiation/wgsl/swr.wgsl): two-band shortwave by the adding method.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_swr(Model m) {
+  COLUMN_PROLOGUE
+  const int NP = NL + 1;
+  const float ZERO = 1.0e-6f, ZBETTA = 1.66f, ZMBAR = 1.9f, ZFO3 = 100.f / 2.14f, ZMU00 = 0.5f,
+              INV_LN10 = 0.43429448190325176f;
+  const float* ds = tb + m.to.dsigma;
+  const float* sg = tb + m.to.sigma;
+  const float mu0 = F.gmu0[c];
+  const float gdist2 = P.rad[3];
+  const float ftop1 = K.ZSOLAR1 * K.GSOL0 * gdist2 * mu0;
+  const float ftop2 = K.ZSOLAR2 * K.GSOL0 * gdist2 * mu0;
+  if (!(ftop1 + ftop2 > ZERO)) {
+    for (int l = 0; l < NP; ++l) {
+      F.dfu[l * SN + c] = 0.f;
+      F.dfd[l * SN + c] = 0.f;
+      F.dswfl[l * SN + c] = 0.f;
+    }
+    return;
+  }
+  const float dp = F.dp[c];
+  float cc_[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) cc_[l] = F.dcc[l * SN + c];
+  float rcl1[NL], rcl1s[NL], rcl2[NL], rcl2s[NL], tcl2[NL], tcl2s[NL];
+  float cs = 1.f;
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const float cc = cc_[l];
+    rcl1[l] = rcl1s[l] = rcl2[l] = rcl2s[l] = 0.f;
+    tcl2[l] = tcl2s[l] = 1.f;
+    if (cc > 0.f) {
+      const float lwp = fminf(1000.f, 1000.f * F.dql[l * SN + c] * dp / K.GA * ds[l]);
+      const float tau = 2.f * fpow(logf(lwp + 1.5f) * INV_LN10, 3.9f);
+      const float zlog = logf(1000.f / tau);
+      float b2 = K.ZB4 / logf(3.f + 0.1f * tau);
+      float om0 = fminf(0.9999f, 1.f - K.ZB5 * zlog);
+      float un = 1.f - om0;
+      float uz = un + 2.f * b2 * om0;
+      float u = sqrtf(uz / un);
+      float ex = expf(fminf(25.f, tau * sqrtf(uz * un) / ZMU00));
+      float r = (u + 1.f) * (u + 1.f) * ex - (u - 1.f) * (u - 1.f) / ex;
+      rcl1s[l] = 1.f - 1.f / (1.f + K.ZB3 * tau);
+      tcl2s[l] = 4.f * u / r;
+      rcl2s[l] = (u * u - 1.f) / r * (ex - 1.f / ex);
+      const float b1 = K.TSWR1 * sqrtf(mu0);
+      b2 = K.TSWR2 * sqrtf(mu0) / logf(3.f + 0.1f * tau);
+      om0 = fminf(0.9999f, 1.f - K.TSWR3 * mu0 * mu0 * zlog);
+      un = 1.f - om0;
+      uz = un + 2.f * b2 * om0;
+      u = sqrtf(uz / un);
+      ex = expf(fminf(25.f, tau * sqrtf(uz * un) / mu0));
+      r = (u + 1.f) * (u + 1.f) * ex - (u - 1.f) * (u - 1.f) / ex;
+      const float direct1 = 1.f - 1.f / (1.f + b1 * tau / mu0);
+      const float directT = 4.f * u / r;
+      const float direct2 = (u * u - 1.f) / r * (ex - 1.f / ex);
+      rcl1[l] = cs * direct1 + (1.f - cs) * rcl1s[l];
+      tcl2[l] = cs * directT + (1.f - cs) * tcl2s[l];
+      rcl2[l] = cs * direct2 + (1.f - cs) * rcl2s[l];
+    }
+    cs = cs * (1.f - cc);
+  }
+  const float zm = 35.f / sqrtf(1.f + 1224.f * mu0 * mu0);
+  float o3l[NL], xo3l[NL], wvl[NL], ywvl[NL];
+  float o3t = 0.f, xo3t = 0.f, wvt = 0.f, ywvt = 0.f;
+  cs = 1.f;
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const float dsigma = ds[l];
+    const float o3 = ZFO3 * dsigma * dp * F.dqo3[l * SN + c] / K.GA;
+    o3t = o3t + o3;
+    xo3t = cs * (xo3t + zm * o3) + (1.f - cs) * (xo3t + ZMBAR * o3);
+    o3l[l] = o3t;
+    xo3l[l] = xo3t;
+    const float wv = 0.1f * dsigma * F.dq[l * SN + c] * dp / K.GA * sqrtf(273.f / F.dt[l * SN + c]) * sg[l] * dp / 100000.f;
+    wvt = wvt + wv;
+    ywvt = cs * (ywvt + zm * wv) + (1.f - cs) * (ywvt + ZBETTA * wv);
+    wvl[l] = wvt;
+    ywvl[l] = ywvt;
+    cs = cs * (1.f - cc_[l]);
+  }
+  float ta1 = 1.f, ta1s = 1.f, ra1 = 0.f, ra1s = 0.f, ta2 = 1.f, ta2s = 1.f, ra2 = 0.f, ra2s = 0.f;
+  float to3t = 1.f, to3tu = 1.f - ozone_absorption(xo3t + ZMBAR * o3t, K.ZSOLAR1);
+  float twvt = 1.f, twvtu = 1.f - vapour_absorption(ywvt + ZBETTA * wvt, K.ZSOLAR2);
+  const float ccn = cc_[NL - 1];
+  const float scf = K.RCOEFF * dp / 101100.f * 9.80665f / K.GA;
+  const float diffuseRayleigh = 1.f - expf(scf * K.LN_DIFFUSE_RAYLEIGH);
+  const float rcsuSurface = diffuseRayleigh * (1.f - ccn);
+  const float rcsSurface =
+      (1.f - expf(scf * logf(1.f - 0.219f / (1.f + 0.816f * mu0)))) * cs + diffuseRayleigh * (1.f - cs - ccn);
+  float t1[NL + 1], t2[NL + 1], r1s[NL + 1], r2s[NL + 1];
+  float tb1[NL], tb1u[NL], rb1[NL], rb1s[NL], tb2[NL], tb2u[NL], rb2[NL], rb2s[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const float cc = cc_[l];
+    t1[l] = ta1;
+    t2[l] = ta2;
+    r1s[l] = ra1s;
+    r2s[l] = ra2s;
+    const bool surface = l == NL - 1;
+    rb1[l] = (surface ? rcsSurface : 0.f) + rcl1[l] * cc;
+    rb1s[l] = (surface ? rcsuSurface : 0.f) + rcl1s[l] * cc;
+    float o3 = xo3l[l];
+    const float to3 = (1.f - ozone_absorption(o3, K.ZSOLAR1)) / to3t;
+    to3t = to3t * to3;
+    o3 = xo3t + ZMBAR * (o3t - o3l[l]);
+    const float to3u = to3tu / (1.f - ozone_absorption(o3, K.ZSOLAR1));
+    to3tu = to3tu / to3u;
+    tb1[l] = 1.f - (1.f - to3) * (1.f - cc) - rb1[l];
+    tb1u[l] = 1.f - (1.f - to3u) * (1.f - cc) - rb1s[l];
+    const float m1 = 1.f / (1.f - ra1s * rb1s[l]);
+    ra1 = ra1 + ta1 * rb1[l] * ta1s * m1;
+    ta1 = ta1 * tb1[l] * m1;
+    ra1s = rb1s[l] + tb1u[l] * ra1s * tb1[l] * m1;
+    ta1s = tb1u[l] * ta1s * m1;
+    rb2[l] = rcl2[l] * cc;
+    rb2s[l] = rcl2s[l] * cc;
+    float wv = ywvl[l];
+    const float twv = (1.f - vapour_absorption(wv, K.ZSOLAR2)) / twvt;
+    twvt = twvt * twv;
+    wv = ywvt + ZBETTA * (wvt - wvl[l]);
+    const float twvu = twvtu / (1.f - vapour_absorption(wv, K.ZSOLAR2));
+    twvtu = twvtu / twvu;
+    tb2[l] = 1.f - (1.f - twv) * (1.f - cc) - (1.f - tcl2[l]) * cc;
+    tb2u[l] = 1.f - (1.f - twvu) * (1.f - cc) - (1.f - tcl2s[l]) * cc;
+    const float m2 = 1.f / (1.f - ra2s * rb2s[l]);
+    ra2 = ra2 + ta2 * rb2[l] * ta2s * m2;
+    ta2 = ta2 * tb2[l] * m2;
+    ra2s = rb2s[l] + tb2u[l] * ra2s * tb2[l] * m2;
+    ta2s = tb2u[l] * ta2s * m2;
+  }
+  t1[NL] = ta1;
+  t2[NL] = ta2;
+  r1s[NL] = ra1s;
+  r2s[NL] = ra2s;
+  const bool star = K.NSTARTEMP != 0.f;
+  const float dalb = F.dalb[c], salb1 = F.dsalb[c], salb2 = F.dsalb[SN + c];
+  ra1s = star ? salb1 : dalb;
+  ra2s = star ? salb2 : dalb;
+  const float dls = F.dls[c], dicec = F.dicec[c];
+  const float water = (1.f - dls) * (1.f - dicec) * fminf(0.05f / (mu0 + 0.15f), 0.15f);
+  const float nalb1 = dls * salb1 + (1.f - dls) * dicec * salb1 + water;
+  const float nalb2 = dls * salb2 + (1.f - dls) * dicec * salb2 + water;
+  F.dsalb[c] = nalb1;
+  F.dsalb[SN + c] = nalb2;
+  const float albedo = star ? K.ZSOLARS1 * nalb1 + K.ZSOLARS2 * nalb2 : dls * dalb + (1.f - dls) * dicec * dalb + water;
+  F.dalb[c] = albedo;
+  ra1 = star ? nalb1 : albedo;
+  ra2 = star ? nalb2 : albedo;
+  float rl1[NL + 1], rl2[NL + 1], rl1s[NL + 1], rl2s[NL + 1];
+#pragma unroll
+  for (int l = NL - 1; l >= 0; --l) {
+    rl1[l + 1] = ra1;
+    rl2[l + 1] = ra2;
+    rl1s[l + 1] = ra1s;
+    rl2s[l + 1] = ra2s;
+    const float d1 = 1.f - ra1s * rb1s[l];
+    ra1 = rb1[l] + tb1[l] * ra1 * tb1u[l] / d1;
+    ra1s = rb1s[l] + tb1u[l] * ra1s * tb1u[l] / d1;
+    const float d2 = 1.f - ra2s * rb2s[l];
+    ra2 = rb2[l] + tb2[l] * ra2 * tb2u[l] / d2;
+    ra2s = rb2s[l] + tb2u[l] * ra2s * tb2u[l] / d2;
+  }
+  rl1[0] = ra1;
+  rl2[0] = ra2;
+  rl1s[0] = ra1s;
+  rl2s[0] = ra2s;
+#pragma unroll
+  for (int l = 0; l < NP; ++l) {
+    const float m1 = 1.f / (1.f - r1s[l] * rl1s[l]);
+    const float m2 = 1.f / (1.f - r2s[l] * rl2s[l]);
+    const float fu = -t1[l] * rl1[l] * m1 * ftop1 + -t2[l] * rl2[l] * m2 * ftop2;
+    const float fd = t1[l] * m1 * ftop1 + t2[l] * m2 * ftop2;
+    F.dfu[l * SN + c] = fu;
+    F.dfd[l * SN + c] = fd;
+    F.dswfl[l * SN + c] = fu + fd;
+  }
+}
+
+// lwr (physics/radiation/wgsl/lwr.wgsl) then radstep (radstep.wgsl).
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_lwr_radstep(Model m) {
+  COLUMN_PROLOGUE
+  const int NP = NL + 1;
+  const float ZERO = 1.0e-6f, ZFH2O = 0.1f, ZFO3 = 100.f / 2.14f, INV_LN10 = 0.43429448190325176f;
+  const float* sg = tb + m.to.sigma;
+  const float* sh = tb + m.to.sigmah;
+  const float dp = F.dp[c];
+  const float ps2 = dp * dp;
+  float st4[NL + 1], st4h[NL + 1];
+#pragma unroll
+  for (int l = 0; l < NP; ++l) {
+    const float t = F.dt[l * SN + c];
+    const float t2 = t * t;
+    st4[l] = K.SBK * (t2 * t2);
+  }
+  st4h[0] = st4[0] - (st4[0] - st4[1]) * sg[0] / (sg[0] - sg[1]);
+#pragma unroll
+  for (int l = 1; l < NL; ++l) {
+    const float above = sg[l - 1], half = sh[l - 1], level = sg[l];
+    st4h[l] = (st4[l] * (above - half) + st4[l - 1] * (half - level)) / (above - level);
+  }
+  const int n = NL - 1;
+  if ((st4[n] - st4h[n]) * (st4[n] - st4[NL]) > 0.f) {
+    st4h[NL] = st4[NL];
+  } else {
+    const float sn = sg[n], sm = sg[n - 1];
+    st4h[NL] = st4[n] + (st4[n] - st4[n - 1]) * (1.f - sn) / (sn - sm);
+  }
+  float bu[NL + 2], bd[NL + 2];
+  bd[0] = 0.f;
+  const float dls = F.dls[c];
+  const float eps = dls + 0.98f * (1.f - dls);
+  bu[NP] = eps * st4[NL];
+  float q[NL], qo3[NL], qco2[NL], taucc0[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const float sfac = tb[m.to.lwr_zzf1 + l] * ps2;
+    q[l] = ZFH2O * sfac * F.dq[l * SN + c];
+    qo3[l] = ZFO3 * sfac * F.dqo3[l * SN + c];
+    qco2[l] = K.ZFCO2_ZZF2 * sfac * F.dqco2[l * SN + c];
+    taucc0[l] = 1.f - F.dcc[l * SN + c] * (1.f - expf(tb[m.to.lwr_zzf3 + l] * F.dql[l * SN + c] * dp));
+  }
+  float dftu[NL + 1], dftd[NL + 1];
+#pragma unroll
+  for (int l = 0; l < NP; ++l) dftu[l] = dftd[l] = 0.f;
+  float taucs[NL], tau[NL], tausf[NL];
+  for (int j = 0; j < NL; ++j) {
+    float taucc = 1.f, sumwv = 0.f, sumo3 = 0.f, sumco2 = 0.f;
+    for (int k = j; k < NL; ++k) {
+      sumwv = sumwv + q[k];
+      sumo3 = sumo3 + qo3[k];
+      sumco2 = sumco2 + qco2[k];
+      float ah2o = sumwv <= 0.01f ? 0.846f * fpow(sumwv + 3.59e-5f, 0.243f) - K.ZH2O0A
+                                  : 0.24f * (logf(sumwv + 0.01f) * INV_LN10) + K.ZAH2OC;
+      if (K.TH2OC > 0.f) ah2o = fminf(ah2o + (1.f - expf(-K.TH2OC * sumwv)), 1.f);
+      const float aco2 = sumco2 <= 1.f ? 0.0676f * fpow(sumco2 + 0.01022f, 0.421f) - K.ZCO20
+                                       : 0.0546f * (logf(sumco2) * INV_LN10) + K.ZACO2C;
+      const float th2o = sumwv <= 2.f ? 1.f - (0.832f * fpow(sumwv + 0.0286f, 0.26f) - K.ZH2O0)
+                                      : fmaxf(0.f, K.ZTH2OC - 0.1196f * logf(sumwv - 0.6931f));
+      const float ao3 = sumo3 <= 0.01f ? 0.209f * fpow(sumo3 + 7.0e-5f, 0.436f) - K.ZAO30
+                                       : 0.0212f * (logf(sumo3) * INV_LN10) + K.ZAO3C;
+      const float cs = fminf(1.f - ZERO, fmaxf(ZERO, 1.f - ah2o - ao3 - aco2 * th2o));
+      taucs[k] = cs;
+      taucc = taucc * taucc0[k];
+      tau[k] = cs * taucc;
+    }
+    if (j == 0) {
+      float tau0 = 1.f - ZERO;
+      for (int k = 0; k < NL; ++k) {
+        tau0 = taucs[k] / tau0 * taucc0[k] * K.TPOFMT;
+        tau0 = fminf(1.f - ZERO, fmaxf(ZERO, tau0));
+        if ((st4[k] - st4h[k]) * (st4[k] - st4h[k + 1]) > 0.f) {
+          bd[k + 1] = 0.5f * st4[k] + 0.25f * (st4h[k] + st4h[k + 1]);
+          bu[k + 1] = bd[k + 1];
+        } else {
+          bd[k + 1] = (st4h[k + 1] - tau0 * st4h[k]) / (1.f - tau0) - (st4h[k] - st4h[k + 1]) / logf(tau0);
+          bu[k + 1] = st4h[k] + st4h[k + 1] - bd[k + 1];
+        }
+        tau0 = taucs[k];
+      }
+    }
+    dftu[j] = dftu[j] - bu[j + 1];
+    dftd[j] = dftd[j] + bd[j];
+    const float bdl = bd[j] - bd[j + 1];
+    for (int k = j; k < NL; ++k) {
+      dftu[j] = dftu[j] - (bu[k + 2] - bu[k + 1]) * tau[k];
+      dftd[k + 1] = dftd[k + 1] + bdl * tau[k];
+    }
+    tausf[j] = tau[NL - 1];
+  }
+  dftu[NL] = dftu[NL] - bu[NP];
+  dftd[NL] = dftd[NL] + bd[NL];
+  const float reflected = (1.f - eps) * dftd[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) dftu[l] = dftu[l] - tausf[l] * reflected;
+  float lw[NL + 1], flux[NL + 1];
+#pragma unroll
+  for (int l = 0; l < NP; ++l) {
+    F.dftu[l * SN + c] = dftu[l];
+    F.dftd[l * SN + c] = dftd[l];
+    lw[l] = dftu[l] + dftd[l];
+    F.dlwfl[l * SN + c] = lw[l];
+  }
+  // radstep
+  float sw[NL + 1];
+#pragma unroll
+  for (int l = 0; l < NP; ++l) {
+    sw[l] = F.dswfl[l * SN + c];
+    flux[l] = lw[l] + sw[l];
+    F.dflux[l * SN + c] = flux[l];
+  }
+  const float* ds = tb + m.to.dsigma;
+  const float* lnsig = tb + m.to.rad_lnsig;
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    const float zdh = -F.dt[at] * K.GASCON / K.GA * lnsig[l];
+    const float den = ds[l] * dp * K.ACPD * (1.f + K.ADV * F.dq[at]);
+    F.dtdt[at] = F.dtdt[at] - K.GA * (flux[l + 1] - flux[l]) / den;
+    F.dtdtswr[at] = -K.GA * (sw[l + 1] - sw[l]) / den;
+    F.dtdtlwr[at] = -K.GA * (lw[l + 1] - lw[l]) / den;
+    F.dconv[at] = (flux[l] - flux[l + 1]) / (zdh + 1.0e-9f);
+  }
+}
+
+// ---------------------------------------------------------------- precipitation
+struct Parcel {
+  float t, q, cor;
+  bool saturated;
+};
+
+// kuo.wgsl's condense: a lifted parcel's two Newton condensation steps.
+__device__ __forceinline__ Parcel condense(const PlanetConst& K, float t0, float q0, float p) {
+  float s = sat_capped(K, t0, p);
+  float cor = 1.f / (1.f - K.MOIST * s);
+  s = s * cor;
+  if (!(s < q0)) return {t0, q0, cor, false};
+  float t = t0, q = q0;
+  const float lcp = (t0 < K.TMELT ? K.ALS : K.ALV) / (K.ACPD * (1.f + K.ADV * q0));
+  for (int i = 0; i < 2; ++i) {
+    if (i == 1) {
+      s = sat_capped(K, t, p);
+      cor = 1.f / (1.f - K.MOIST * s);
+      s = s * cor;
+    }
+    const float dqsdt = K.RA2 * (K.TMELT - K.RA4) * s * cor / ((t - K.RA4) * (t - K.RA4));
+    const float rain = (q - s) / (1.f + lcp * dqsdt);
+    t = t + lcp * rain;
+    q = q - rain;
+  }
+  return {t, q, cor, true};
+}
+
+// mkdqtgp scaling, kuo and mkshallow (physics/precipitation/wgsl/kuo.wgsl).
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_kuo(Model m) {
+  COLUMN_PROLOGUE
+  const int NM = NL - 1;
+  const float* ds = tb + m.to.dsigma;
+  const float* sg = tb + m.to.sigma;
+  const float D2 = P.deltsec2;
+  const float dp = F.dp[c];
+  float zdqt[NL], zqe[NL], zte[NL], zdqtot[NL], zalcpe[NL], zacpe[NL], zdqdt[NL], zdtdt[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    zdqt[l] = F.dqt[at] * K.PSURF * K.WW / dp;
+    F.dqt[at] = zdqt[l];
+    const float dq = F.dq[at], dqdt = F.dqdt[at];
+    zdqtot[l] = (zdqt[l] + dqdt) * D2;
+    zqe[l] = dq + dqdt * D2;
+    zte[l] = F.dt[at] + F.dtdt[at] * D2;
+    zacpe[l] = K.ACPD * (1.f + K.ADV * dq);
+    zalcpe[l] = K.ALV / zacpe[l];
+    zdqdt[l] = 0.f;
+    zdtdt[l] = 0.f;
+  }
+  int ilift = -1, itop = -1;
+  float zi = 0.f, zpt = 0.f, zpq = 0.f, zbeta = 0.f, zpbeta = 0.f, ztp = 0.f, zqp = 0.f;
+  {
+    const int n = NL - 1;
+    const float dsn = ds[n];
+    const float ztsurf = F.dt[NL * SN + c] * tb[m.to.vdiff_skap + n];
+    if (zdqtot[n] > 0.f && ztsurf > zte[n]) {
+      const float p = dp * sg[n];
+      const float zqsnl = sat_divided(K, zte[n], p);
+      const float zqnew = F.dq[NL * SN + c] * fminf(1.f, zqe[n] / zqsnl);
+      const Parcel parcel = condense(K, ztsurf, zqnew, p);
+      if (parcel.saturated) {
+        ilift = NL + 1;
+        itop = NL;
+        ztp = parcel.t;
+        zqp = parcel.q;
+        const float zqsa = sat_divided(K, zte[n], p);
+        zdqdt[n] = fmaxf(zqsa - zqe[n], 0.f);
+        zdtdt[n] = ztp - zte[n];
+        zpt = zdtdt[n] * dsn * zacpe[n];
+        zpq = zdqdt[n] * dsn * K.ALV;
+        zbeta = fminf(1.f, zqe[n] / zqsa) * dsn;
+        zpbeta = dsn;
+        zi = zdqtot[n] * dsn * K.ALV;
+      }
+    }
+  }
+  for (int l = NM - 1; l >= 0; --l) {
+    const int lp = l + 1;
+    if (ilift == -1 && zdqtot[lp] > 0.f) {
+      const float p = dp * sg[l];
+      const Parcel parcel = condense(K, zte[lp] * tb[m.to.kuo_zfac + l], zqe[lp], p);
+      if (parcel.saturated && parcel.t > zte[l]) {
+        const float dsl = ds[l], dsp = ds[lp];
+        ilift = l + 2;
+        itop = l + 1;
+        ztp = parcel.t;
+        zqp = parcel.q;
+        const float zqsa = sat_divided(K, zte[l], p);
+        zdqdt[l] = fmaxf(zqsa - zqe[l], 0.f);
+        zdtdt[l] = ztp - zte[l];
+        zpt = zdtdt[l] * dsl * zacpe[l];
+        zpq = zdqdt[l] * dsl * K.ALV;
+        zbeta = fminf(1.f, zqe[l] / zqsa) * dsl;
+        zpbeta = dsl;
+        const float pp = dp * sg[lp];
+        float zqsnl = sat_divided(K, zte[lp], pp);
+        if (zqe[lp] > zqsnl) {
+          float t = zte[lp], q = zqe[lp];
+          const float lcp = (t < K.TMELT ? K.ALS : K.ALV) / (K.ACPD * (1.f + K.ADV * q));
+          float cor = parcel.cor;
+          for (int i = 0; i < 2; ++i) {
+            if (i == 1) {
+              zqsnl = sat_capped(K, t, pp);
+              cor = 1.f / (1.f - K.MOIST * zqsnl);
+              zqsnl = zqsnl * cor;
+            }
+            const float dqsdt = K.RA2 * (K.TMELT - K.RA4) * zqsnl * cor / ((t - K.RA4) * (t - K.RA4));
+            const float rain = (q - zqsnl) / (1.f + lcp * dqsdt);
+            t = t + lcp * rain;
+            q = q - rain;
+          }
+          zdqdt[lp] = fmaxf(q - zqe[lp], 0.f);
+          zdtdt[lp] = t - zte[lp];
+          zpt = zdtdt[lp] * dsp * zacpe[lp] + zpt;
+          zpq = zdqdt[lp] * dsp * K.ALV + zpq;
+          zbeta = fminf(1.f, zqe[lp] / zqsnl) * dsp + zbeta;
+          zpbeta = dsp + zpbeta;
+        }
+        zi = zdqtot[l] * dsl * K.ALV + zdqtot[lp] * dsp * K.ALV;
+      }
+    }
+  }
+  for (int l = NM - 1; l >= 0; --l) {
+    if (itop == l + 2) {
+      const float p = dp * sg[l];
+      const Parcel parcel = condense(K, ztp * tb[m.to.kuo_zfac + l], zqp, p);
+      if (parcel.saturated && parcel.t > zte[l]) {
+        const float dsl = ds[l];
+        itop = l + 1;
+        ztp = parcel.t;
+        zqp = parcel.q;
+        const float zqsa = sat_divided(K, zte[l], p);
+        zdqdt[l] = fmaxf(zqsa - zqe[l], 0.f);
+        zdtdt[l] = ztp - zte[l];
+        zpt = zdtdt[l] * dsl * zacpe[l] + zpt;
+        zpq = zdqdt[l] * dsl * K.ALV + zpq;
+        zbeta = fminf(1.f, zqe[l] / zqsa) * dsl + zbeta;
+        zpbeta = zpbeta + dsl;
+        zi = zdqtot[l] * dsl * K.ALV + zi;
+      }
+    }
+  }
+  zi = fmaxf(0.f, zi);
+  const float zrhm = zpbeta > 0.f ? zbeta / zpbeta : 0.f;
+  float beta = 1.f;
+  if (zrhm >= K.RHBETA) beta = powi((1.f - zrhm) / (1.f - K.RHBETA), (int)K.NBETA);
+  const float zat = zpt > 0.f ? zi * (1.f - beta) / zpt : 0.f;
+  const float zaq = zpq > 0.f ? zi * beta / zpq : 0.f;
+  const bool shallow = itop > 0 && (dp * sg[itop - 1] > K.PDEEP || zi <= 0.f);
+  float icctot = 0.f;
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const int level = l + 1;
+    const size_t at = l * SN + c;
+    float dprcl = 0.f, icclev = 0.f;
+    if (ilift >= level && itop <= level && zi > 0.f && !shallow) {
+      F.dqdt[at] = zaq * zdqdt[l] / D2 - zdqt[l];
+      F.dtdt[at] = zat * zdtdt[l] / D2 + F.dtdt[at];
+      dprcl = zat * zdtdt[l] * ds[l] / zalcpe[l] / D2;
+    }
+    if (dprcl > 0.f) {
+      icclev = 1.f;
+      icctot = icctot + 1.f;
+    }
+    if (sg[l] < 0.4f && icclev == 1.f && itop == level) icclev = 2.f;
+    F.dprcl[at] = dprcl;
+    F.dprscl[at] = 0.f;
+    F.icclev[at] = icclev;
+  }
+  F.icctot[c] = icctot;
+  if (!shallow) return;
+  const float zkonst1 = K.GA * D2 / K.GASCON;
+  const float zkonst2 = K.RKSHALLOW * zkonst1 * K.GA / K.GASCON;
+  int kktop = 1;
+  for (int level = 2; level <= NM; ++level)
+    if (dp * sg[level - 1] < K.PDEEPTH) kktop = level;
+  const int ktop = max(itop, kktop);
+  float zkdiff[NL], skap[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    zkdiff[l] = 0.f;
+    skap[l] = tb[m.to.vdiff_skap + l];
+  }
+#pragma unroll
+  for (int l = 0; l < NM; ++l) {
+    const int lp = l + 1, level = l + 1;
+    const float sigmah = tb[m.to.sigmah + l];
+    const float zfac = zkonst2 * sigmah * sigmah * tb[m.to.vdiff_rdsig + l];
+    const float dsl = ds[l], dsp = ds[lp];
+    const float zrthl = (dsp + dsl) / (zte[l] * dsp + zte[lp] * dsl);
+    if (level >= ktop && level < ilift) zkdiff[l] = zfac * zrthl * zrthl;
+    if (level + 1 == ktop) {
+      float zzqs = sat_capped(K, zte[l], dp * sg[l]);
+      zzqs = zzqs * (1.f / (1.f - K.MOIST * zzqs));
+      float zzqsp = sat_capped(K, zte[lp], dp * sg[lp]);
+      zzqsp = zzqsp * (1.f / (1.f - K.MOIST * zzqsp));
+      const float zrh = zqe[l] / zzqs, zrhp = zqe[lp] / zzqsp;
+      const float zzf = fabsf((zrh - 0.8f) / 0.2f * (zrhp - zrh));
+      zkdiff[l] = zfac * zrthl * zrthl * zzf;
+    }
+  }
+  float zqn[NL], ztn[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    zqn[l] = zqe[l];
+    ztn[l] = zte[l];
+  }
+  diffuse<NL>(ds, zqn, zkdiff);
+#pragma unroll
+  for (int l = 0; l < NM; ++l) zkdiff[l] = zkdiff[l] * tb[m.to.vdiff_skaph + l];
+  diffuse_potential<NL>(ds, ztn, zkdiff, skap);
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    F.dtdt[at] = F.dtdt[at] + (ztn[l] - zte[l]) / D2;
+    F.dqdt[at] = F.dqdt[at] + (zqn[l] - zqe[l]) / D2;
+  }
+}
+
+// mkdca (physics/precipitation/wgsl/mkdca.wgsl): dry convective adjustment.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_mkdca(Model m) {
+  COLUMN_PROLOGUE
+  const int NM = NL - 1;
+  const float D2 = P.deltsec2;
+  float zt[NL], zth[NL], zq[NL], zqn[NL], skap[NL], ds[NL];
+  bool mixed[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    skap[l] = tb[m.to.vdiff_skap + l];
+    ds[l] = tb[m.to.dsigma + l];
+    zt[l] = F.dt[at] + F.dtdt[at] * D2;
+    zth[l] = zt[l] / skap[l];
+    zq[l] = F.dq[at] + F.dqdt[at] * D2;
+    zqn[l] = zq[l];
+    mixed[l] = false;
+  }
+  float limited = 0.f;
+  int passes = 0;
+  for (;;) {
+    bool unstable = false;
+    int ibase = 0, itop = NL;
+    float ztht = 0.f, zqt = 0.f, zsum1 = 0.f, zsum2 = 0.f, zsumq1 = 0.f, zsumq2 = 0.f;
+    for (int l = 0; l < NM; ++l) {
+      const int lp = l + 1;
+      if (zth[l] < zth[lp]) {
+        ibase = l + 2;
+        itop = l;
+        zsum1 = skap[lp] * ds[lp] + skap[l] * ds[l];
+        zsum2 = skap[lp] * ds[lp] * zth[lp] + skap[l] * ds[l] * zth[l];
+        zsumq1 = ds[lp] + ds[l];
+        zsumq2 = ds[lp] * zqn[lp] + ds[l] * zqn[l];
+        ztht = zsum2 / zsum1;
+        zqt = zsumq2 / zsumq1;
+        unstable = true;
+      }
+    }
+    if (!unstable) break;
+    for (int level = NM - 1; level >= 1; --level) {
+      const int l = level - 1;
+      if (itop == level && zth[l] < ztht) {
+        itop = level - 1;
+        zsum1 = zsum1 + skap[l] * ds[l];
+        zsum2 = zsum2 + skap[l] * ds[l] * zth[l];
+        zsumq1 = zsumq1 + ds[l];
+        zsumq2 = zsumq2 + ds[l] * zqn[l];
+        ztht = zsum2 / zsum1;
+        zqt = zsumq2 / zsumq1;
+      }
+    }
+    for (int l = 0; l < NL; ++l) {
+      const int level = l + 1;
+      if (level > itop && level <= ibase) {
+        zth[l] = ztht;
+        zqn[l] = zqt;
+        mixed[l] = true;
+      }
+    }
+    passes = passes + 1;
+    if (passes > 2 * NL) {  // the reference's pass limit bounds this loop
+      limited = 1.f;
+      break;
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    F.dca_dtdt[at] = mixed[l] ? (zth[l] * skap[l] - zt[l]) / D2 : 0.f;
+    F.dca_dqdt[at] = (zqn[l] - zq[l]) / D2;
+  }
+  F.dca_limited[c] = limited;
+}
+
+// mkdca-limit (physics/precipitation/wgsl/mkdca-limit.wgsl): per slot, skip
+// every adjustment when any column needed more than 2 NL passes.
+__global__ void __launch_bounds__(kSumThreads) k_mkdca_limit(Model m) {
+  const Dims& d = m.d;
+  const int slot = blockIdx.x;
+  if (!m.params[slot].active) return;
+  __shared__ float part[kSumThreads];
+  float flag = 0.f;
+  for (int h = threadIdx.x; h < d.NHOR; h += kSumThreads) flag = fmaxf(flag, m.f.dca_limited[slot * d.NHOR + h]);
+  part[threadIdx.x] = flag;
+  __syncthreads();
+  for (int stride = kSumThreads / 2; stride > 0; stride /= 2) {
+    if (threadIdx.x < stride) part[threadIdx.x] = fmaxf(part[threadIdx.x], part[threadIdx.x + stride]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) m.f.dca_skip[slot] = part[0];
+}
+
+// column.wgsl: mkdca's adjustment (unless skipped), mklsp, mkrain, mkclouds.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_rain_column(Model m) {
+  COLUMN_PROLOGUE
+  const float* ds = tb + m.to.dsigma;
+  const float* sg = tb + m.to.sigma;
+  const float D2 = P.deltsec2;
+  const bool skip = F.dca_skip[slot] != 0.f;
+  const float dp = F.dp[c];
+  float dq_[NL], dt_[NL], dtdt_[NL], dqdt_[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    dq_[l] = F.dq[at];
+    dt_[l] = F.dt[at];
+    dtdt_[l] = F.dtdt[at];
+    dqdt_[l] = F.dqdt[at];
+    if (!skip) {
+      dtdt_[l] = dtdt_[l] + F.dca_dtdt[at];
+      dqdt_[l] = dqdt_[l] + F.dca_dqdt[at];
+    }
+  }
+  // mklsp
+  float dprll[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    dprll[l] = 0.f;
+    const float dq = dq_[l];
+    const float zq = dq + dqdt_[l] * D2;
+    const float zt = dt_[l] + dtdt_[l] * D2;
+    const float zlcpe = K.ALV / (K.ACPD * (1.f + K.ADV * dq));
+    const float p = dp * sg[l];
+    float zqsat = sat_capped(K, zt, p);
+    float zcor = 1.f / (1.f - K.MOIST * zqsat);
+    zqsat = zqsat * zcor;
+    if (zqsat < 0.f) zqsat = 0.f;
+    if (zq > zqsat) {
+      float zdqdt = (zqsat - zq) / (1.f + zlcpe * K.RA2 * (K.TMELT - K.RA4) * zqsat * zcor / ((zt - K.RA4) * (zt - K.RA4)));
+      float ztn = zt - zdqdt * zlcpe;
+      float zqn = zq + zdqdt;
+      zqsat = sat_capped(K, ztn, p);
+      zcor = 1.f / (1.f - K.MOIST * zqsat);
+      zqsat = zqsat * zcor;
+      zdqdt = (zqsat - zqn) / (1.f + zlcpe * K.RA2 * (K.TMELT - K.RA4) * zqsat * zcor / ((ztn - K.RA4) * (ztn - K.RA4)));
+      ztn = ztn - zdqdt * zlcpe;
+      zqn = zqn + zdqdt;
+      const float dqdt = (zqn - zq) / D2, dtdt = (ztn - zt) / D2;
+      dqdt_[l] = dqdt_[l] + dqdt;
+      dtdt_[l] = dtdt_[l] + dtdt;
+      dprll[l] = -fminf(dqdt, 0.f) * ds[l];
+    }
+    F.dprsll[l * SN + c] = 0.f;
+    F.dprll[l * SN + c] = dprll[l];
+  }
+  // mkrain
+  float zprc = 0.f, zprl = 0.f, zprsc = 0.f, zprsl = 0.f;
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    const float dsl = ds[l], dq = dq_[l];
+    float zdtdt = 0.f, zdqdtl = 0.f, zdqdts = 0.f;
+    const float dprscl = F.dprscl[at];
+    zprc = zprc + F.dprcl[at] - dprscl;
+    zprl = zprl + dprll[l] - 0.f;
+    zprsc = zprsc + dprscl;
+    zprsl = zprsl + 0.f;
+    const int surface = l == NL - 1 ? 2 : 1;
+    for (int below = 0; below < surface; ++below) {
+      const float temperature = F.dt[(l + below) * SN + c];
+      const float zlcp = (K.ALS - K.ALV) / (K.ACPD * (1.f + K.ADV * dq));
+      if (zprsc + zprsl > 0.f && temperature > K.TMELT) {
+        zdtdt = -(zprsc + zprsl) / dsl * zlcp + zdtdt;
+        zprc = zprsc + zprc;
+        zprl = zprsl + zprl;
+        zprsc = 0.f;
+        zprsl = 0.f;
+      } else if (zprc + zprl > 0.f && temperature <= K.TMELT) {
+        zdtdt = (zprc + zprl) / dsl * zlcp + zdtdt;
+        zprsc = zprc + zprsc;
+        zprsl = zprl + zprsl;
+        zprc = 0.f;
+        zprl = 0.f;
+      }
+    }
+    const float zq = dq + dqdt_[l] * D2;
+    const float zt = dt_[l] + dtdt_[l] * D2;
+    float zqsat = sat_capped(K, zt, dp * sg[l]);
+    const float zcor = 1.f / (1.f - K.MOIST * zqsat);
+    zqsat = zqsat * zcor;
+    if (zqsat < 0.f) zqsat = 0.f;
+    if (zq < zqsat) {
+      const float deficit = zqsat - zq;
+      const float water = K.ALV / (K.ACPD * (1.f + K.ADV * dq));
+      const float ice = K.ALS / (K.ACPD * (1.f + K.ADV * dq));
+      const float curve = K.RA2 * (K.TMELT - K.RA4) * zqsat * zcor / ((zt - K.RA4) * (zt - K.RA4));
+      auto evap = [&](float& flux, float zlcpe) {
+        const float zd = fminf(K.GAMMA * deficit * dsl / D2 / (1.f + zlcpe * curve), flux);
+        flux = flux - zd;
+        return zd / dsl;
+      };
+      if (zprl > 0.f) {
+        const float e = evap(zprl, water);
+        zdtdt = zdtdt - e * water;
+        zdqdtl = zdqdtl + e;
+      }
+      if (zprc > 0.f) {
+        const float e = evap(zprc, water);
+        zdtdt = zdtdt - e * water;
+        zdqdtl = zdqdtl + e;
+      }
+      if (zprsl > 0.f) {
+        const float e = evap(zprsl, ice);
+        zdtdt = zdtdt - e * ice;
+        zdqdts = zdqdts + e;
+      }
+      if (zprsc > 0.f) {
+        const float e = evap(zprsc, ice);
+        zdtdt = zdtdt - e * ice;
+        zdqdts = zdqdts + e;
+      }
+    }
+    dqdt_[l] = dqdt_[l] + zdqdtl + zdqdts;
+    dtdt_[l] = dtdt_[l] + zdtdt;
+  }
+  const float dprc = (zprc + zprsc) * dp / K.GA / 1000.f;
+  F.dprc[c] = dprc;
+  F.dprl[c] = (zprl + zprsl) * dp / K.GA / 1000.f;
+  F.dprs[c] = (zprsc + zprsl) * dp / K.GA / 1000.f;
+  // mkclouds
+  const float ZCLMAX = 1.f, ZCCA = 0.245f, ZCCB = 0.125f, ZCCMAX = 0.8f, ZCCMIN = 0.05f;
+  float zcctot = ZCCMIN, zccconv = ZCCMIN;
+  if (dprc > 0.f) {
+    zcctot = ZCCA + ZCCB * logf(dprc * K.ZRFAC);
+    zcctot = fminf(ZCCMAX, fmaxf(ZCCMIN, zcctot));
+    const float levels = F.icctot[c];
+    zccconv = levels == 0.f ? 1.f : 1.f - fpow(1.f - zcctot, 1.f / levels);
+  }
+  float cover[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    const float zt = dt_[l] + dtdt_[l] * D2;
+    const float zq = dq_[l] + dqdt_[l] * D2;
+    const float zqsat = sat_divided(K, zt, dp * sg[l]);
+    float zrh = zq / zqsat;
+    const float icclev = F.icclev[at];
+    float dcc = icclev > 0.f ? zccconv : 0.f;
+    if (icclev == 2.f && zcctot >= 0.3f) dcc = fminf(dcc + 2.f * (zcctot - 0.3f), ZCLMAX);
+    zrh = zrh * (1.f - dcc);
+    const float zrcrit = tb[m.to.rcrit + l];
+    float zwfac = 1.f;
+    if (sg[l] > 0.8f && K.CLWFAC > 0.f) {
+      const float dw = F.dw[at];
+      zwfac = K.CLWFAC * fmaxf(0.f, K.CLWCRIT1 - dw);
+      if (K.CLWCRIT2 > dw) zwfac = 1.f;
+    }
+    const float excess = fmaxf(0.f, (zrh - zrcrit) / (1.f - zrcrit));
+    cover[l] = fminf(dcc + zwfac * (excess * excess), ZCLMAX);
+  }
+  const float* lnsig = tb + m.to.rad_lnsig;
+  float zzf[NL];
+  float dqvi = 0.f, zzh = 0.f;
+#pragma unroll
+  for (int l = NL - 1; l >= 1; --l) {
+    dqvi = dq_[l] * ds[l] + dqvi;
+    const float zdh = -dt_[l] * K.GASCON / K.GA * lnsig[l];
+    zzf[l] = zzh + zdh * 0.5f;
+    zzh = zzh + zdh;
+  }
+  dqvi = dq_[0] * ds[0] + dqvi;
+  zzf[0] = zzh - dt_[0] * K.GASCON / K.GA * lnsig[0];
+  dqvi = dqvi * dp / K.GA;
+  F.dqvi[c] = dqvi;
+  zzh = 700.f * logf(1.f + dqvi);
+  float clear = 1.f;
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    float dql = 0.f;
+    if (zzh > 0.f && cover[l] > 0.f) {
+      dql = 0.00021f * expf(-zzf[l] / zzh) * K.GASCON * dt_[l] / (sg[l] * dp);
+      dql = fmaxf(dql, 1.0e-9f);
+    }
+    F.dql[at] = dql;
+    F.dcc[at] = cover[l];
+    F.dtdt[at] = dtdt_[l];
+    F.dqdt[at] = dqdt_[l];
+    clear = clear * (1.f - cover[l]);
+  }
+  F.dql[NL * SN + c] = 0.f;
+  F.dcc[NL * SN + c] = 1.f - clear;
+}
+
+// ---------------------------------------------------------------- surface
+struct SnowLayer {
+  float ctop, soilz1, diff1, cap1;
+};
+
+__device__ __forceinline__ SnowLayer snow_layer(const PlanetConst& K, float snowz, float cap0, float diff0,
+                                                float soilz0) {
+  const float zsntop = fminf(snowz * 1000.f / K.RHOSNOW, K.DZTOP);
+  const float ctop = cap0 * K.SNOWCAP * K.DZTOP / (cap0 * zsntop + K.SNOWCAP * (K.DZTOP - zsntop));
+  const float zsnowz = fminf(snowz * 1000.f / K.RHOSNOW, 1.f) - zsntop;
+  const float soilz1 = soilz0 + zsnowz;
+  const float diff1 = diff0 * K.SNOWDIFF * soilz1 / (K.SNOWDIFF * soilz0 + diff0 * zsnowz);
+  const float cap1 = cap0 * K.SNOWCAP * soilz1 / (cap0 * zsnowz + K.SNOWCAP * soilz0);
+  return {ctop, soilz1, diff1, cap1};
+}
+
+__device__ __forceinline__ float surface_temperature(const PlanetConst& K, float deltsec, const SnowLayer& ly,
+                                                     float dtsm, float flux, float soil1) {
+  const float conduction = 2.f * ly.diff1;
+  return (ly.ctop * K.DZTOP * dtsm / deltsec + flux + conduction * soil1 / ly.soilz1) /
+         (ly.ctop * K.DZTOP / deltsec + conduction / ly.soilz1);
+}
+
+// landmod's soilstep (physics/land/wgsl/soil.wgsl): tands, mktsoil, wandr.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_soil(Model m) {
+  COLUMN_PROLOGUE
+  const float DS = P.deltsec;
+  const float dls = F.dls[c];
+  const bool land = dls > 0.f;
+  const float snowStart = F.dsnowz[c];
+  float dwater = 0.f, dsmelt = 0.f;
+  if (snowStart == 0.f) F.dsnowt[c] = K.TMELT;
+  if (land) {
+    const float glac = F.dglac[c];
+    float soilz[NLSOIL], cap[NLSOIL], diff[NLSOIL];
+#pragma unroll
+    for (int l = 0; l < NLSOIL; ++l) {
+      cap[l] = K.SICECAP * glac + K.SOILCAP * (1.f - glac);
+      diff[l] = K.SICEDIFF * glac + K.SOILDIFF * (1.f - glac);
+      soilz[l] = tb[m.to.dsoilz + l];
+    }
+    const float zhfla = F.dshfl[c] + F.dlhfl[c] + F.dflux[NL * SN + c];
+    const float devap = F.devap[c];
+    float zdsnowz = 0.f;
+    if (F.dprs[c] > 0.f) zdsnowz = F.dprs[c];
+    if (snowStart > 0.f) zdsnowz = zdsnowz + devap;
+    float zsnowz = fmaxf(0.f, snowStart + zdsnowz * DS);
+    zdsnowz = (zsnowz - snowStart) / DS;
+    dwater = devap + F.dprl[c] + F.dprc[c] - zdsnowz;
+    float dsnowz = zsnowz;
+    const float dtsm = F.land_dtsm[c];
+    const float soil1 = F.dsoilt[c];
+    SnowLayer layer = snow_layer(K, dsnowz, cap[0], diff[0], soilz[0]);
+    float dts = surface_temperature(K, DS, layer, dtsm, zhfla, soil1);
+    float zhfls = 2.f * layer.diff1 / layer.soilz1 * (dts - soil1);
+    float zhflm = 0.f;
+    if (dsnowz > 0.f && dts > K.TMELT) {
+      dts = K.TMELT;
+      zhflm = fmaxf(0.f, zhfla - layer.ctop * K.DZTOP * (dts - dtsm) / DS + 2.f * layer.diff1 * (soil1 - dts) / layer.soilz1);
+      zsnowz = fmaxf(0.f, dsnowz - zhflm * DS / ((K.ALS - K.ALV) * 1000.f));
+      zdsnowz = (zsnowz - dsnowz) / DS;
+      zhflm = -zdsnowz * 1000.f * (K.ALS - K.ALV);
+      dsnowz = zsnowz;
+      dsmelt = -zdsnowz;
+      zhfls = 2.f * layer.diff1 / layer.soilz1 * (dts - soil1);
+      dwater = dwater - zdsnowz;
+      layer = snow_layer(K, dsnowz, cap[0], diff[0], soilz[0]);
+    }
+    if (dsnowz == 0.f && zhflm > 0.f) {
+      dts = surface_temperature(K, DS, layer, dtsm, zhfla - zhflm, soil1);
+      zhfls = 2.f * layer.diff1 / layer.soilz1 * (dts - soil1);
+    }
+    soilz[0] = layer.soilz1;
+    cap[0] = layer.cap1;
+    diff[0] = layer.diff1;
+    // mktsoil
+    float zdiff[NLSOIL], zcap[NLSOIL], zebs[NLSOIL], ztn[NLSOIL];
+    const int n = NLSOIL - 1;
+    zdiff[n - 1] = 2.f * diff[n] * diff[n - 1] / (diff[n] * soilz[n - 1] + diff[n - 1] * soilz[n]);
+    zcap[n] = cap[n] * soilz[n] / DS;
+    zebs[n] = 1.f / (zcap[n] + zdiff[n - 1]);
+    ztn[n] = zcap[n] * F.dsoilt[n * SN + c] * zebs[n];
+#pragma unroll
+    for (int l = n - 1; l >= 1; --l) {
+      zdiff[l - 1] = 2.f * diff[l] * diff[l - 1] / (diff[l] * soilz[l - 1] + diff[l - 1] * soilz[l]);
+      zcap[l] = cap[l] * soilz[l] / DS;
+      zebs[l] = 1.f / (zcap[l] + zdiff[l - 1] + zdiff[l] * (1.f - zdiff[l] * zebs[l + 1]));
+      ztn[l] = zebs[l] * (zcap[l] * F.dsoilt[l * SN + c] + zdiff[l] * ztn[l + 1]);
+    }
+    zcap[0] = cap[0] * soilz[0] / DS;
+    zebs[0] = 1.f / (zcap[0] + zdiff[0] * (1.f - zdiff[0] * zebs[1]));
+    ztn[0] = zebs[0] * (zcap[0] * F.dsoilt[c] + zdiff[0] * ztn[1] + zhfls);
+#pragma unroll
+    for (int l = 1; l < NLSOIL; ++l) ztn[l] = ztn[l] + zebs[l] * zdiff[l - 1] * ztn[l - 1];
+    const bool glacier = F.dglac[c] > 0.5f;
+#pragma unroll
+    for (int l = 0; l < NLSOIL; ++l) F.dsoilt[l * SN + c] = glacier ? fminf(ztn[l], K.TMELT) : ztn[l];
+    if (dsnowz > 0.f) F.dsnowt[c] = dts;
+    if (K.DSMAX > 0.f && dsnowz > K.DSMAX) {
+      zdsnowz = (K.DSMAX - dsnowz) / DS;
+      dsnowz = K.DSMAX;
+      dwater = dwater - zdsnowz;
+      dts = dts + zdsnowz * 1000.f * (K.ALS - K.ALV) * DS / layer.ctop / K.DZTOP;
+      dsmelt = dsmelt - zdsnowz;
+    }
+    F.dsnowz[c] = dsnowz;
+    F.land_dts[c] = dts;
+    F.dsndch[c] = dsnowz - snowStart;
+  } else {
+    F.dsndch[c] = snowStart;
+  }
+  F.dwater[c] = dwater;
+  F.dsmelt[c] = dsmelt;
+  float drunoff = 0.f;
+  if (land) {
+    const float dwatc = F.dwatc[c] + DS * dwater;
+    const float dwmax = F.dwmax[c];
+    drunoff = fmaxf(0.f, dwatc - dwmax) / DS;
+    F.dwatc[c] = fmaxf(fminf(dwmax, dwatc), 0.f);
+  }
+  F.drunoff[c] = drunoff;
+}
+
+// mkradv (physics/land/wgsl/mkradv.wgsl): river routing stencil within one
+// slot. Each thread reads only its own drunoff and its neighbours' driver,
+// which nothing here writes, so the update is in place.
+__device__ __forceinline__ float river(const FieldPtrs& F, int c) { return F.driver[c] * F.darea[c] * F.dls[c]; }
+
+__global__ void __launch_bounds__(kBlock) k_mkradv(Model m) {
+  const Dims& d = m.d;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.S * d.NHOR) return;
+  const int slot = c / d.NHOR, h = c % d.NHOR;
+  if (!m.params[slot].active) return;
+  const FieldPtrs& F = m.f;
+  const int base = slot * d.NHOR;
+  const int lat = h / d.NLON, lon = h % d.NLON;
+  const int row = base + lat * d.NLON;
+  auto eastward = [&](int lo, float& out, float& into) {
+    const int at = row + lo, nx = row + (lo + 1) % d.NLON;
+    const float u = F.duroff[at];
+    const float water = u > 0.f ? river(F, at) : river(F, nx);
+    out = u * water / F.darea[at];
+    into = u * water / F.darea[nx];
+  };
+  float runoff = F.drunoff[c], o, in;
+  if (lon == 0) {
+    eastward(0, o, in);
+    runoff = runoff - o;
+    eastward(d.NLON - 1, o, in);
+    runoff = runoff + in;
+  } else {
+    eastward(lon - 1, o, in);
+    runoff = runoff + in;
+    eastward(lon, o, in);
+    runoff = runoff - o;
+  }
+  const float area = F.darea[c], v = F.dvroff[c];
+  const float below = lat + 1 < d.NLAT ? river(F, c + d.NLON) : 0.f;
+  if (v < 0.f)
+    runoff = runoff + v * river(F, c) / area;
+  else
+    runoff = runoff + v * below / area;
+  float fromAbove = 0.f;
+  if (lat > 0) {
+    const int above = c - d.NLON;
+    const float va = F.dvroff[above];
+    fromAbove = va < 0.f ? -va * river(F, above) : -va * river(F, c);
+  }
+  F.drunoff[c] = runoff + fromAbove / area;
+}
+
+__device__ __forceinline__ float clim14(const float* f, const float* w3, int c, size_t SN) {
+  const float w = w3[2];
+  return (1.f - w) * f[(size_t)w3[0] * SN + c] + w * f[(size_t)w3[1] * SN + c];
+}
+
+// Land surface after mkradv (physics/land/wgsl/surface.wgsl) with vegstep
+// (vegetation/wgsl/vegstep.wgsl) and glacierstep (glacier/wgsl/glacierstep.wgsl).
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_land_surface(Model m) {
+  COLUMN_PROLOGUE
+  const float DS = P.deltsec;
+  const float dls = F.dls[c];
+  if (dls > 0.f) F.driver[c] = F.driver[c] + F.drunoff[c] * DS;
+  const float dts = F.land_dts[c];
+  float albclim = clim14(F.dalbcl, P.surf + 3, c, SN);
+  float albclim1 = clim14(F.dalbcl1, P.surf + 3, c, SN);
+  float albclim2 = clim14(F.dalbcl2, P.surf + 3, c, SN);
+  if (K.NWETSOIL != 0.f && dls > 0.5f) {
+    if (dts > 273.15f) {
+      const float bf = F.dwater[c] / K.WSMAX;
+      const float al = 1.f / 5.2f * fpow(fpow(fmaxf(bf, 1.0e-3f), (1.f - 4.f) / 4.f) - 1.f, 1.f / 4.f);
+      const float dry = expf(-powi(bf * 25.f, 6));
+      const float wet = expf(-powi((1.f - bf) * 30.f, 9));
+      albclim = K.ALBLANDMAX * dry + al * (1.f - dry - wet) + K.DOCEANALB1 * wet;
+      albclim1 = albclim;
+      albclim2 = K.ALBLANDMAX * dry + al * (1.f - dry - wet) + K.DOCEANALB2 * wet;
+    } else {
+      albclim = K.ALBLAND;
+      albclim1 = K.DGROUNDALB1;
+      albclim2 = K.DGROUNDALB2;
+    }
+  }
+  F.dalbclim[c] = albclim;
+  F.dalbclim1[c] = albclim1;
+  F.dalbclim2[c] = albclim2;
+  if (dls > 0.f) {
+    F.land_dtsm[c] = dts;
+    float dqs = K.RDBRV * K.RA1 * expf(K.RA2 * (dts - K.TMELT) / (dts - K.RA4)) / F.dp[c];
+    dqs = dqs / (1.f - (1.f / K.RDBRV - 1.f) * dqs);
+    F.land_dqs[c] = dqs;
+    const float dsnow = F.dsnowz[c];
+    F.dsnow[c] = dsnow;
+    if (dsnow > 0.f) {
+      const float forest = F.dforest[c];
+      auto snow_albedo = [&](float mxf, float mxb, float mnf, float mnb) {
+        const float zmax = forest * mxf + (1.f - forest) * mxb;
+        const float zmin = forest * mnf + (1.f - forest) * mnb;
+        const float zd = (zmax - zmin) * (dts - 263.16f) / (K.TMELT - 263.16f);
+        return fmaxf(zmin, fminf(zmax, zmax - zd));
+      };
+      const float s0 = snow_albedo(K.ALBSMAXF, K.ALBSMAX, K.ALBSMINF, K.ALBSMIN);
+      const float s1 = snow_albedo(K.ALBSMAXF1, K.ALBSMAX1, K.ALBSMINF1, K.ALBSMIN1);
+      const float s2 = snow_albedo(K.ALBSMAXF2, K.ALBSMAX2, K.ALBSMINF2, K.ALBSMIN2);
+      F.dalb[c] = albclim + (s0 - albclim) * dsnow / (dsnow + 0.01f);
+      F.dsalb[c] = albclim1 + (s1 - albclim1) * dsnow / (dsnow + 0.01f);
+      F.dsalb[SN + c] = albclim2 + (s2 - albclim2) * dsnow / (dsnow + 0.01f);
+      F.drhs[c] = 1.f;
+    } else {
+      F.dalb[c] = albclim;
+      F.dsalb[c] = albclim1;
+      F.dsalb[SN + c] = albclim2;
+      const float dwmax = F.dwmax[c];
+      if (dwmax > 0.f) F.drhs[c] = fminf(1.f, F.dwatc[c] / (K.DRHSFULL * dwmax));
+    }
+    F.dtsoil[c] = F.dsoilt[c];
+    F.dtd2[c] = F.dsoilt[SN + c];
+    F.dtd3[c] = F.dsoilt[2 * SN + c];
+    F.dtd4[c] = F.dsoilt[3 * SN + c];
+    F.dtd5[c] = F.dsoilt[4 * SN + c];
+    F.dt[NL * SN + c] = dts;
+    F.dq[NL * SN + c] = dqs;
+  }
+  if (K.NVEG > 0.f && F.dls[c] > 0.f && F.dglac[c] < 0.90f) {
+    const float co2 = F.co2[slot];
+    float zbeta = 0.f;
+    if (!(co2 < 1.0e-8f)) zbeta = fmaxf(0.f, 1.f + K.CO2_SENS * logf((co2 - K.CO2_COMP) / (K.CO2_REF - K.CO2_COMP)));
+    const float ts = F.dt[NL * SN + c], dp = F.dp[c], dwatc = F.dwatc[c], dsnow = F.dsnow[c];
+    float zwmax = F.dwmax[c];
+    const float zglacfree = 1.f - F.dglac[c];
+    const float zsvp = K.RA1 * expf(K.RA2 * (ts - K.TMELT) / (ts - K.RA4));
+    const float zvpd = fmaxf(0.01f, zsvp - dp * F.dq[(NL - 1) * SN + c] / 0.622f);
+    float dcveg = F.dcveg[c], dcsoil = F.dcsoil[c];
+    const float zlaim = K.ZLAIMIN + 0.63661977236758f * K.ZLAIMAX * atanf(K.CVEG_L * 2.f * F.dagg[c] * dcveg);
+    const float zvegm = 1.f - expf(-K.CVEG_K * zlaim);
+    float zveg = 0.f;
+    if (zwmax > 0.f) zveg = fminf(fminf(1.f, zvegm), fmaxf(0.f, dwatc / (zwmax * K.VWS_CRIT)));
+    const float zft = fminf(1.f, fmaxf(0.f, (ts - K.TMELT) / K.CT_CRIT));
+    const float zgppl = K.RLUE * zbeta * zft * zveg * F.dfd[NL * SN + c];
+    float zgppw = 0.f;
+    if (!(co2 < 1.0e-8f)) zgppw = K.CO2CONV * dp * zveg * (-F.devap[c]) / zvpd * (0.3f * co2);
+    zgppw = fminf(1.f, fmaxf(0.f, zgppw));
+    const float zgpp = fminf(zgppl, zgppw);
+    const float znpp = F.dgrow[c] * 0.5f * zgpp * zglacfree;
+    F.dnpp[c] = znpp;
+    const float zlitter = dcveg / K.TAU_VEG;
+    const float zres = fpow(K.Q10, (ts - K.TMELT - 10.f) / 10.f) * dcsoil / K.TAU_SOIL;
+    dcveg = dcveg + (znpp - zlitter) * DS * K.NCVEG;
+    dcsoil = dcsoil + (zlitter - zres) * DS * K.NCVEG;
+    const float zforest = fminf(1.f, fmaxf(0.f, (atanf(dcveg - K.CVEG_A) - K.CVEG_E) / (K.CVEG_C - K.CVEG_E)));
+    const float dvsoil = fminf(1.f, fmaxf(0.f, (atanf(dcveg - K.CVEG_F) - K.CVEG_G) / (K.CVEG_C - K.CVEG_G)));
+    F.dcveg[c] = dcveg;
+    F.dcsoil[c] = dcsoil;
+    F.dvsoil[c] = dvsoil;
+    F.dlai[c] = -logf(1.f - zveg) / K.CVEG_K;
+    const float zvz0 = F.dmr[c] * zforest + K.VZ0_MIN * (1.f - zforest);
+    float zvalb = K.VALB_MIN * zveg + K.VALB_MAX * (1.f - zveg);
+    zwmax = K.VWMAX_MAX * dvsoil + K.VWMAX_MIN * (1.f - dvsoil);
+    float zvrhs = F.dsc[c] * fminf(1.f, fmaxf(0.f, dwatc / (zwmax * K.VWS_CRIT)));
+    if (dsnow > 0.f) {
+      float zalbsn = (K.ALBSMAX - K.ALBSMIN) * (ts - 263.16f) / (K.TMELT - 263.16f);
+      zalbsn = fmaxf(K.ALBSMIN, fminf(K.ALBSMAX, K.ALBSMAX - zalbsn));
+      zvalb = zvalb + (zalbsn - zvalb) * dsnow / (dsnow + 0.01f);
+      zvalb = K.VSALB_MIN * zforest + zvalb * (1.f - zforest);
+      zvrhs = 1.f;
+    }
+    if (K.NVEG == 2.f) {
+      const float z0c = F.dz0climo[c];
+      F.dz0[c] = sqrtf(zvz0 * zvz0 + z0c * z0c);
+      F.dwmax[c] = zwmax;
+      F.drhs[c] = zvrhs;
+      F.dalb[c] = zvalb;
+      F.dforest[c] = zforest;
+    }
+  }
+  if (F.dglac[c] > 0.5f && dls > 0.f) {
+    auto glacier_albedo = [&](float mx, float mn) {
+      return fmaxf(mn, fminf(mx, mx - (mx - mn) * (dts - 263.16f) / (K.TMELT - 263.16f)));
+    };
+    F.dalb[c] = glacier_albedo(K.ALBGMAX, K.ALBGMIN);
+    F.dsalb[c] = glacier_albedo(K.ALBGMAX1, K.ALBGMIN1);
+    F.dsalb[SN + c] = glacier_albedo(K.ALBGMAX2, K.ALBGMIN2);
+    F.drhs[c] = 1.f;
+  }
+  if (K.NGLACIER != 0.f) {
+    const bool lnd = F.dls[c] > 0.5f;
+    if (lnd && F.dsnowz[c] < K.GLACELIM) F.dpersist[c] = 0.f;
+    if (lnd && F.dsnowz[c] < 0.1f) F.dglac[c] = 0.f;
+    if (P.surf[6] > 0.5f) {
+      if (F.dpersist[c] > 0.5f) F.dglac[c] = 1.f;
+      F.dpersist[c] = F.dls[c] >= 0.5f ? 1.f : 0.f;
+    }
+  }
+}
+
+// seastep coupling and icestep up to getiflx (physics/sea-ice/wgsl/ice.wgsl).
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_sea_ice(Model m) {
+  COLUMN_PROLOGUE
+  if (P.coupled == 0.f) return;
+  const bool sea = F.dls[c] < 0.5f;
+  float xheat = 0.f, xprs = 0.f;
+  if (sea) {
+    const float naccua = F.sea_naccua[c] + 1.f;
+    xheat = (F.dshfl[c] + F.dswfl[NL * SN + c] + F.dlwfl[NL * SN + c] + F.dlhfl[c] + F.sea_cheata[c]) / naccua;
+    xprs = (F.dprs[c] + F.sea_cprsa[c]) / naccua;
+  }
+  F.sea_cheata[c] = 0.f;
+  F.sea_cprsa[c] = 0.f;
+  F.sea_naccua[c] = 0.f;
+  const float zrhoilfdt = K.CRHOI * K.CLFI / K.XDT;
+  F.xclssto[c] = clim14(F.xclsst, P.surf, c, SN);
+  F.xclsst2[c] = clim14(F.xclsst, P.surf + 3, c, SN);
+  const float cliced = fmaxf(clim14(F.xcliced, P.surf + 3, c, SN), 0.f);
+  float clicec = fmaxf(clim14(F.xclicec, P.surf + 3, c, SN), 0.f);
+  if (cliced <= 0.f) clicec = 0.f;
+  F.xcliced2[c] = cliced;
+  F.xclicec2[c] = clicec;
+  const float xls = F.xls[c], xsst = F.xsst[c];
+  float xiced = F.xiced[c], xsnow = F.xsnow[c], xicecc = F.xicecc[c], xcflux = F.xcflux[c], xcfluxf = F.xcfluxf[c];
+  F.ice_snowold[c] = xsnow;
+  const float zicedold = xls < 0.5f ? xiced : 0.f;
+  float ximelt = 0.f, xsmelt = 0.f, xsmflx = 0.f, xscflx = 0.f, xsndch = 0.f, xcfluxr = 0.f;
+  if (F.xicec[c] >= K.CICEMIN) {
+    xsnow = xsnow + xprs * K.XDT;
+    xprs = 0.f;
+  }
+  float xts = F.xts[c], xqmelt = 0.f;
+  const float ztso = fminf(K.TMELT, xts);
+  const float zhsnow = 1.0e3f / K.CRHOSN * xsnow;
+  if (xiced >= K.XMIND) {
+    const float zcpdt = K.XMIND * K.CRHOI * K.CPI / K.XDT;
+    const float zckap = (K.CKAPSN * zhsnow + K.CKAPI * xiced) / (zhsnow + xiced);
+    float zkapz = zckap / (xiced + zhsnow);
+    if (xiced >= K.XMAXD && K.XMAXD >= 0.f) zkapz = 0.f;
+    const float zflx = xheat + zkapz * xsst;
+    xts = (zcpdt * ztso + zflx) / (zcpdt + zkapz);
+    if (xts > K.TMELT) {
+      xqmelt = xheat + zkapz * (xsst - K.TMELT) - zcpdt * (K.TMELT - ztso);
+      xts = K.TMELT;
+    }
+  } else {
+    xts = xsst;
+    if (xiced > 0.f) xqmelt = xheat;
+  }
+  F.xts[c] = xts;
+  F.xqmelt[c] = xqmelt;
+  if (xiced < K.XMIND) {
+    xcflux = xheat;
+    xcfluxf = 0.f;
+  } else {
+    const float zhsnowc = 1.0e3f / K.CRHOSN * xsnow;
+    float zckap = (K.CKAPSN * zhsnowc + K.CKAPI * xiced) / (zhsnowc + xiced);
+    if (K.XMAXD >= 0.f && xiced >= K.XMAXD) zckap = 0.f;
+    xcflux = zckap * (xts - xsst) / (zhsnowc + xiced);
+    xcfluxf = zckap * (K.TFREEZE - xsst) / (zhsnowc + xiced);
+  }
+  if (F.xicec[c] < K.CICEMIN && xprs > 0.f) {
+    xcflux = xcflux - xprs * 1000.f * K.CLFSN;
+    xsmelt = xprs + xsmelt;
+    xsmflx = xsmflx + xprs * 1000.f * K.CLFSN;
+    xprs = 0.f;
+  }
+  float zqmelt = xqmelt;
+  if (xiced > 0.f) {
+    if (xqmelt > xsnow * 1000.f * K.CLFSN / K.XDT) {
+      xsmelt = xsmelt + xsnow / K.XDT;
+      xsmflx = xsmflx + xsnow * 1000.f * K.CLFSN / K.XDT;
+      zqmelt = xqmelt - xsnow * 1000.f * K.CLFSN / K.XDT;
+      xsnow = 0.f;
+    } else if (xqmelt > 0.f && xsnow > 0.f) {
+      xsmelt = xsmelt + xqmelt / K.CLFSN / 1000.f;
+      xsnow = xsnow - xqmelt * K.XDT / K.CLFSN / 1000.f;
+      xsmflx = xsmflx + xqmelt;
+      zqmelt = 0.f;
+    }
+    xcflux = xcflux + zqmelt;
+  } else {
+    xsmelt = xsmelt + xsnow / K.XDT;
+    xcflux = xcflux - xsnow * 1000.f * K.CLFSN / K.XDT;
+    xsmflx = xsmflx + xsnow * 1000.f * K.CLFSN / K.XDT;
+    xsnow = 0.f;
+  }
+  if (xls < 0.5f && 1.0e3f * xsnow > (K.CRHOS - K.CRHOI) * xiced) {
+    const float zhice = (1.0e3f * xsnow + K.CRHOI * xiced) / K.CRHOS;
+    const float zdice = zhice - xiced;
+    const float zdsnow = -zdice * K.CRHOI / 1.0e3f;
+    xsnow = xsnow + zdsnow;
+    xscflx = zdsnow * 1.0e3f * K.CLFSN / K.XDT;
+    xsmelt = xsmelt - zdsnow / K.XDT;
+    xsmflx = xsmflx - zdsnow * 1.0e3f * K.CLFSN / K.XDT;
+  }
+  if (xls < 0.5f) xcflux = xcflux + F.xoflux[c];
+  if (xsst <= K.TFREEZE || xiced > 0.f) {
+    ximelt = xcflux + xscflx - xcfluxf;
+    xiced = xiced - ximelt / zrhoilfdt;
+    xcflux = xcfluxf;
+  }
+  if (xiced <= 0.f) {
+    xcflux = xcflux - xiced * zrhoilfdt;
+    ximelt = ximelt + xiced * zrhoilfdt;
+    xiced = 0.f;
+  }
+  if (fabsf(xiced) < 1.0e-9f) xiced = 0.f;
+  if (xiced > zicedold) xicecc = fminf(xicecc + (1.f - xicecc) * (xiced - zicedold) / 0.5f, 1.f);
+  if (xiced < zicedold) xicecc = fmaxf(xicecc + xicecc * (xiced - zicedold) / (2.f * zicedold), 0.f);
+  if (xiced <= 0.f) xicecc = 0.f;
+  if (K.XMAXD >= 0.f && xiced > K.XMAXD) {
+    const float zcflux = (xiced - K.XMAXD) * zrhoilfdt;
+    xiced = K.XMAXD;
+    xcfluxr = xcfluxr + zcflux;
+    ximelt = ximelt + zcflux;
+    xsndch = xsndch + zcflux * 1000.f / K.CRHOI / zrhoilfdt;
+  }
+  float zflx = F.ice_zflx[c];
+  if (xls < 1.f) zflx = fmaxf(0.f, K.XMAXD - xiced) * zrhoilfdt;
+  F.ice_zflx[c] = zflx;
+  const float xgw = F.xgw[c];
+  F.ice_part1[c] = xls < 1.f ? xcfluxr * xgw : 0.f;
+  F.ice_part2[c] = xls < 1.f ? zflx * xgw : 0.f;
+  F.xiced[c] = xiced;
+  F.xsnow[c] = xsnow;
+  F.xicecc[c] = xicecc;
+  F.xicec[c] = xicecc;
+  F.xcflux[c] = xcflux;
+  F.xcfluxf[c] = xcfluxf;
+  F.xcfluxr[c] = xcfluxr;
+  F.ximelt[c] = ximelt;
+  F.xsmelt[c] = xsmelt;
+  F.xsmflx[c] = xsmflx;
+  F.xsndch[c] = xsndch;
+}
+
+// seastep (physics/sea/wgsl/seastep.wgsl) with ice_finish (sea-ice/wgsl/finish.wgsl)
+// and oceanstep (ocean/wgsl/oceanstep.wgsl).
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_sea(Model m) {
+  COLUMN_PROLOGUE
+  const bool coupled = P.coupled != 0.f;
+  if (coupled) {
+    const float xls = F.xls[c];
+    float xcflux = F.xcflux[c], xcfluxr = F.xcfluxr[c];
+    const double s1 = m.sums[slot * 4 + 2], s2 = m.sums[slot * 4 + 3];
+    if (s1 > 0.0 && s2 > 0.0 && xls < 1.f) {
+      float zflx = F.ice_zflx[c];
+      const float zfac = (float)(s1 / s2);
+      if (zfac <= 1.f) zflx = zflx * zfac;
+      xcfluxr = xcfluxr - zflx;
+      xcflux = xcflux - zflx;
+    }
+    F.xcfluxr[c] = xcfluxr;
+    const float xiced = F.xiced[c];
+    const float xicec = F.xicec[c] >= K.THICEC ? 1.f : 0.f;
+    float xsnow = F.xsnow[c], xsmelt = F.xsmelt[c];
+    if (xiced <= 0.f && xsnow > 0.f) {
+      const float zcflux = xsnow * 1000.f * K.CLFSN / K.XDT;
+      xsmelt = xsmelt + xsnow / K.XDT;
+      F.xsmflx[c] = F.xsmflx[c] + zcflux;
+      xcflux = xcflux - zcflux;
+      xsnow = 0.f;
+    }
+    F.xicec[c] = xicec;
+    F.xsnow[c] = xsnow;
+    F.xsmelt[c] = xsmelt;
+    F.xcflux[c] = xcflux;
+    const bool sea = xls < 0.5f;
+    const float heat = sea ? xcflux : 0.f;
+    F.yclsst2[c] = clim14(F.yclsst, P.surf + 3, c, SN);
+    const float yls = F.yls[c], yiced = F.xiced[c], ymld = F.ymld[c], yfldo = F.yfldo[c];
+    const float zcpsdt = K.DTMIX / (K.CRHOS * K.CPS);
+    const float ysst = F.ysst[c];
+    float zsst = ysst, yiflux = 0.f;
+    if (yls < 1.f && yiced <= 0.f) zsst = zsst + (heat + yfldo) * zcpsdt / ymld;
+    if (yls < 1.f && yiced > 0.f) yiflux = yiflux - yfldo - heat;
+    if (ysst < K.TFREEZE && yls < 1.f) {
+      yiflux = yiflux + (K.TFREEZE - zsst) * ymld / zcpsdt;
+      zsst = K.TFREEZE;
+    }
+    if (yiced > 0.f && yls < 1.f) {
+      const float zf = (K.TFREEZE - zsst) * ymld / zcpsdt;
+      zsst = zsst + zf * zcpsdt / ymld;
+      yiflux = yiflux + zf;
+    }
+    F.ysst[c] = zsst;
+    F.xsst[c] = zsst;
+    F.xmld[c] = ymld;
+    F.xoheat[c] = -yiflux;
+    F.xoflux[c] = -yiflux;
+    if (sea) F.xsndch[c] = F.xsndch[c] + (xsnow - F.ice_snowold[c]);
+  } else {
+    F.sea_naccua[c] = F.sea_naccua[c] + 1.f;
+  }
+  if (!(F.dls[c] < 0.5f)) return;
+  const float dts = F.xts[c], dicec = F.xicec[c];
+  if (coupled) {
+    F.sea_dsst[c] = F.xsst[c];
+    F.sea_dts[c] = dts;
+    F.dmld[c] = F.xmld[c];
+    F.dicec[c] = dicec;
+    F.diced[c] = F.xiced[c];
+    F.dsnow[c] = F.xsnow[c];
+    F.dsmelt[c] = F.xsmelt[c];
+    F.dsndch[c] = F.xsndch[c];
+  } else {
+    F.sea_cheata[c] = F.dshfl[c] + F.dswfl[NL * SN + c] + F.dlwfl[NL * SN + c] + F.dlhfl[c] + F.sea_cheata[c];
+    F.sea_cprsa[c] = F.dprs[c] + F.sea_cprsa[c];
+  }
+  const float dp = F.dp[c];
+  F.dt[NL * SN + c] = dts;
+  float dqs = K.RDBRV * K.RA1 * expf(K.RA2 * (dts - K.TMELT) / (dts - K.RA4)) / dp;
+  dqs = dqs / (1.f - (1.f / K.RDBRV - 1.f) * dqs);
+  F.sea_dqs[c] = dqs;
+  F.dq[NL * SN + c] = dqs;
+  const float taux = F.dtaux[c], tauy = F.dtauy[c];
+  const float zz0 = fmaxf(K.CHARNOCK * sqrtf(taux * taux + tauy * tauy) * K.GASCON * dts / (K.GA * dp), K.DZ0SEA);
+  F.drhs[c] = K.DRHSSEA * (1.f - dicec) + K.DRHSICE * dicec;
+  F.dalb[c] = K.ALBSEA * (1.f - dicec) + dicec * fminf(K.ALBICE, 0.5f + 0.025f * (273.f - dts));
+  F.dsalb[c] = K.DOCEANALB1 * (1.f - dicec) + dicec * fminf(K.DICEALBMX1, K.DICEALBMN1 + 0.025f * (273.f - dts));
+  F.dsalb[SN + c] = K.DOCEANALB2 * (1.f - dicec) + dicec * fminf(K.DICEALBMX2, K.DICEALBMN2 + 0.025f * (273.f - dts));
+  F.dz0[c] = zz0 * (1.f - dicec) + K.DZ0ICE * dicec;
+}
+
+// carbonstep (physics/carbon/wgsl/carbonstep.wgsl).
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_carbon(Model m) {
+  COLUMN_PROLOGUE
+  const float precip = (F.dprc[c] + F.dprl[c]) * 3.154e9f;
+  F.localprecip[c] = precip;
+  F.localavgprecip[c] = F.localavgprecip[c] + precip * K.TIMEWEIGHT;
+  if (P.carbon == 0.f) return;
+  const float tsurf = F.dt[NL * SN + c];
+  if (K.NCARBON != 0.f) {
+    float weathering = 0.f;
+    if (F.dls[c] > 0.5f && tsurf >= 273.15f) {
+      const float pco2 = F.co2[slot] * F.dp[c] * 1.0e-5f;
+      weathering = fpow(pco2 / K.CO2EARTH, K.BETA) * expf(K.KACT * (tsurf - 288.f)) * fpow(precip / K.PEARTH, 0.65f);
+      if (K.NSUPPLY != 0.f) {
+        const float wmaxp = fmaxf(K.WMAX / K.VEARTH, 2.0e-15f);
+        weathering = wmaxp * (1.f - expf(-weathering / wmaxp));
+      }
+    }
+    F.localweathering[c] = weathering * (K.PLARAD * K.PLARAD) / (K.RAD_EARTHSQ * 0.29f);
+  }
+  F.localavgtemps[c] = F.localavgtemps[c] + tsurf * K.TIMEWEIGHT;
+  F.localavgweather[c] = F.localavgweather[c] + F.localweathering[c] * K.TIMEWEIGHT;
+}
+
+// snapshot/wgsl/pack.wgsl: the published fields, window extrema, RH.
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_pack(Model m) {
+  COLUMN_PROLOGUE
+  const int step = (int)P.snap[0], window = (int)P.snap[1];
+  const float t = F.dt[NL * SN + c];
+  float* tr = F.snapshot_tracking + c;
+  if (tr[7 * SN] == 0.f) {
+    tr[0] = t;
+    tr[SN] = t;
+    tr[7 * SN] = 1.f;
+  }
+  tr[0] = fminf(tr[0], t);
+  tr[SN] = fmaxf(tr[SN], t);
+  if (step > 0 && window > 0 && step % window == 0) {
+    const float range = tr[SN] - tr[0];
+    tr[2 * SN] = tr[0];
+    tr[3 * SN] = tr[SN];
+    tr[4 * SN] = range;
+    tr[5 * SN] += range;
+    tr[6 * SN] += 1.f;
+    tr[7 * SN] = 0.f;
+    tr[8 * SN] = 1.f;
+  }
+  // The pack itself writes the publishing step's snapshot (snap[2] = 1).
+  // F.dca_skip and the scratch slots are not published.
+  float* S = F.snapshot + c;
+  auto put = [&](int index, float v) { S[(size_t)index * SN] = v; };
+  const float snapflag = P.snap[2];
+  if (h == 0) {
+    // The step's CPU values, kept in their state slots for checkpoints.
+    for (int i = 0; i < 3; ++i) F.snapshot_step[i * d.S + slot] = P.snap[i];
+    for (int i = 0; i < 5; ++i) F.radiation_step[i * d.S + slot] = P.rad[i];
+    for (int i = 0; i < 7; ++i) F.surface_step[i * d.S + slot] = P.surf[i];
+    F.carbon_step[slot] = P.carbon;
+  }
+  if (snapflag == 0.f) return;
+  const int jet = (int)K.JET;
+  put(0, F.dt[NL * SN + c]);
+  put(1, F.dtsa[c]);
+  put(2, F.du[(NL - 1) * SN + c]);
+  put(3, F.dv[(NL - 1) * SN + c]);
+  put(4, F.dcc[NL * SN + c]);
+  put(5, F.dprc[c] + F.dprl[c]);
+  put(6, F.dp[c]);
+  put(7, F.dqvi[c]);
+  put(8, F.dicec[c]);
+  put(9, F.dsnow[c]);
+  put(10, F.dwatc[c]);
+  put(11, F.dalb[c]);
+  put(12, F.du[jet * SN + c]);
+  put(13, F.dv[jet * SN + c]);
+  put(14, -F.dlwfl[c]);
+  put(15, F.dls[c]);
+  put(16, F.dswfl[c] + F.dlwfl[c]);
+  put(17, F.dsmelt[c] * -333700000.f + F.dswfl[NL * SN + c] + F.dlwfl[NL * SN + c] + F.dshfl[c] + F.dlhfl[c]);
+  put(18, -F.devap[c]);
+  put(19, F.drunoff[c]);
+  put(20, F.dforest[c]);
+  put(21, F.dlai[c]);
+  put(22, F.dprs[c]);
+  put(23, F.dsmelt[c]);
+  put(24, F.diced[c]);
+  put(25, F.dglac[c]);
+  put(27, F.dswfl[NL * SN + c]);
+  put(28, F.dlwfl[NL * SN + c]);
+  put(29, F.dshfl[c]);
+  put(30, F.dlhfl[c]);
+  put(31, F.dprc[c]);
+  put(32, F.dprl[c]);
+  put(33, F.dswfl[c]);
+  put(34, F.dlwfl[c]);
+  const bool windowed = tr[8 * SN] != 0.f;
+  put(35, windowed ? tr[2 * SN] : tr[0]);
+  put(36, windowed ? tr[3 * SN] : tr[SN]);
+  put(37, windowed ? tr[4 * SN] : tr[SN] - tr[0]);
+  put(38, tr[5 * SN]);
+  put(39, tr[6 * SN]);
+  put(40, F.dnpp[c]);
+  put(41, F.gmu0[c]);
+  tr[5 * SN] = 0.f;
+  tr[6 * SN] = 0.f;
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const int f = 51 + 5 * l;
+    put(f, F.dt[l * SN + c]);
+    put(f + 1, F.du[l * SN + c]);
+    put(f + 2, F.dv[l * SN + c]);
+    put(f + 4, F.dcc[l * SN + c]);
+  }
+  put(42, F.capen[c]);
+  put(43, F.lnb[c]);
+  put(44, F.mpoti[c]);
+  put(45, F.chim[c]);
+  put(46, F.laav[c]);
+  put(47, F.venti[c]);
+  put(48, F.vrmpi[c]);
+  put(49, F.gpi[c]);
+  put(50, F.shear[c]);
+  const int lowest = NL - 1;
+  const float qsat = sat_divided(K, F.dt[lowest * SN + c], F.dp[c] * K.SIGMA_LOW);
+  put(51 + 5 * lowest + 3, fmaxf(0.f, F.dq[lowest * SN + c]) / fmaxf(1.17549435e-38f, qsat));
+}
+
+// Non-finite check per slot over the prognostic spectral state: sets
+// flags[slot] = 1 when any coefficient of sp, st, sz, sd or sq is NaN or Inf.
+__global__ void k_finite(Model m) {
+  const Dims& d = m.d;
+  const size_t SR = (size_t)d.S * d.NRSP;
+  const size_t n = (size_t)d.NLEV * SR;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % SR);
+    const int slot = c / d.NRSP;
+    if (!m.params[slot].active) continue;
+    const float v = m.f.st[i] + m.f.sz[i] + m.f.sd[i] + m.f.sq[i] + (i < SR ? m.f.sp[i] : 0.f);
+    if (!isfinite(v)) m.flags[slot] = 1;
+  }
+}
+
+inline unsigned nblocks(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+template <template <int> class Launch, typename... A>
+void by_levels(int L, A&&... a) {
+  if (L == 10)
+    Launch<10>::run(a...);
+  else if (L == 5)
+    Launch<5>::run(a...);
+}
+
+#define COLUMN_LAUNCHER(name, kernel)                                                      \
+  template <int NL>                                                                        \
+  struct name {                                                                            \
+    static void run(const Model& m, cudaStream_t st) {                                     \
+      kernel<NL><<<nblocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);         \
+    }                                                                                      \
+  };
+
+COLUMN_LAUNCHER(FixerColumn, k_fixer_column)
+COLUMN_LAUNCHER(FixerApply, k_fixer_apply)
+COLUMN_LAUNCHER(Surflx, k_surflx)
+COLUMN_LAUNCHER(Vdiff, k_vdiff)
+COLUMN_LAUNCHER(SolangMko3, k_solang_mko3)
+COLUMN_LAUNCHER(Swr, k_swr)
+COLUMN_LAUNCHER(LwrRadstep, k_lwr_radstep)
+COLUMN_LAUNCHER(Kuo, k_kuo)
+COLUMN_LAUNCHER(Mkdca, k_mkdca)
+COLUMN_LAUNCHER(RainColumn, k_rain_column)
+COLUMN_LAUNCHER(Soil, k_soil)
+COLUMN_LAUNCHER(LandSurface, k_land_surface)
+COLUMN_LAUNCHER(SeaIce, k_sea_ice)
+COLUMN_LAUNCHER(Sea, k_sea)
+COLUMN_LAUNCHER(Carbon, k_carbon)
+COLUMN_LAUNCHER(Pack, k_pack)
+
+template <int NL>
+struct FixerRow {
+  static void run(const Model& m, cudaStream_t st) {
+    k_fixer_row<NL><<<nblocks((size_t)m.d.S * m.d.NLAT, 64), 64, 0, st>>>(m);
+  }
+};
+
+}  // namespace
+
+void phy_fixer(const Model& m, cudaStream_t st) {
+  by_levels<FixerColumn>(m.d.L, m, st);
+  by_levels<FixerRow>(m.d.L, m, st);
+  k_slot_sums<<<m.d.S, kSumThreads, 0, st>>>(m, m.f.fixneg, m.f.fixpos, m.f.fixsum, 0);
+  by_levels<FixerApply>(m.d.L, m, st);
+}
+
+void phy_surface_flux(const Model& m, cudaStream_t st) {
+  by_levels<Surflx>(m.d.L, m, st);
+  by_levels<Vdiff>(m.d.L, m, st);
+}
+
+void phy_radiation(const Model& m, cudaStream_t st) {
+  by_levels<SolangMko3>(m.d.L, m, st);
+  by_levels<Swr>(m.d.L, m, st);
+  by_levels<LwrRadstep>(m.d.L, m, st);
+}
+
+void phy_precipitation_columns(const Model& m, cudaStream_t st) {
+  by_levels<Kuo>(m.d.L, m, st);
+  by_levels<Mkdca>(m.d.L, m, st);
+  k_mkdca_limit<<<m.d.S, kSumThreads, 0, st>>>(m);
+  by_levels<RainColumn>(m.d.L, m, st);
+}
+
+void phy_surface(const Model& m, cudaStream_t st) {
+  by_levels<Soil>(m.d.L, m, st);
+  k_mkradv<<<nblocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);
+  by_levels<LandSurface>(m.d.L, m, st);
+  by_levels<SeaIce>(m.d.L, m, st);
+  k_slot_sums<<<m.d.S, kSumThreads, 0, st>>>(m, m.f.ice_part1, m.f.ice_part2, m.f.ice_sums, 1);
+  by_levels<Sea>(m.d.L, m, st);
+}
+
+void phy_carbon(const Model& m, cudaStream_t st) { by_levels<Carbon>(m.d.L, m, st); }
+
+void phy_pack(const Model& m, cudaStream_t st) { by_levels<Pack>(m.d.L, m, st); }
+
+void phy_finite_check(const Model& m, cudaStream_t st) { k_finite<<<592, 256, 0, st>>>(m); }
+
+}  // namespace exogcm
