@@ -129,6 +129,11 @@ int exogcm_step(exogcm_engine* engine, int steps, int publish_every);
  * NULL to query only. */
 int exogcm_read_snapshot(exogcm_engine* engine, int slot, float* values, size_t count, long* step);
 
+/* Stops a slot at model step `step`: later steps of a batch leave the slot
+ * untouched (its kernels skip it), so a run ends exactly on its last step
+ * whatever the batch length. A negative step removes the limit. */
+int exogcm_set_stop(exogcm_engine* engine, int slot, long step);
+
 /* Per-slot model step counter and start-up steps still to run. */
 int exogcm_slot_info(exogcm_engine* engine, int slot, long* step, int* startup_left, int* active);
 
@@ -164,6 +169,18 @@ int exogcm_run_stage(exogcm_engine* engine, const char* stage);
 
 /* Device time of the last exogcm_step in milliseconds (CUDA events). */
 int exogcm_last_step_ms(exogcm_engine* engine, float* ms);
+
+/* Launches one of the step's kernels `reps` times on the current state of
+ * every slot and returns its mean device time per launch in *ms (CUDA events
+ * on the engine's stream), with the algorithmic bytes one launch moves in
+ * *bytes. Kernels: "dft_forward", "dft_inverse", "legendre_forward",
+ * "legendre_inverse", "dv2uv", "uv2dv", "qtend", "calcgp", "spectrala",
+ * "vdiff", "swr", "lwr_radstep", "kuo", "rain_column". The launches change
+ * the state; use it for measurement only. */
+int exogcm_time_kernel(exogcm_engine* engine, const char* kernel, int reps, float* ms, double* bytes);
+
+/* Kernel launches in the CUDA graph of a `steps`-step batch. */
+int exogcm_graph_launches(exogcm_engine* engine, int steps, size_t* launches);
 
 /* Raw device pointer of a field (slot-major layout [plane][slot][points])
  * and the engine's CUDA stream, for in-process hosts that keep inputs

@@ -15,6 +15,7 @@ golden dumps are not in the checkout.
 """
 from __future__ import annotations
 
+import functools
 import math
 
 import numpy as np
@@ -69,6 +70,7 @@ def _ql(k: int, p: float) -> float:
     return norm * s
 
 
+@functools.lru_cache(maxsize=None)
 def gaussian_latitudes(count: int):
     """grid/index.ts:32-63 (inigau): sines, weights and degrees, north first."""
     inigau_pi = 3.14159265358979
@@ -134,6 +136,16 @@ def fourier_analyse(values, longitudes, truncation):
 # ---------------------------------------------------------------- legendre
 def legendre_tables(sines, weights, truncation):
     """legendre/index.ts:29-108 (legini): qi qj qc qe qm qq qu qv [lat][mode]."""
+    key = (truncation, tuple(np.asarray(sines).tolist()), tuple(np.asarray(weights).tolist()))
+    if key not in _LEGINI:
+        _LEGINI[key] = _legendre_tables(sines, weights, truncation)
+    return {k: v.copy() for k, v in _LEGINI[key].items()}
+
+
+_LEGINI: dict = {}
+
+
+def _legendre_tables(sines, weights, truncation):
     nlat = len(sines)
     modes = (truncation + 1) * (truncation + 2) // 2
     out = {k: np.zeros((nlat, modes)) for k in ("qi", "qj", "qc", "qe", "qm", "qq", "qu", "qv")}

@@ -74,6 +74,7 @@ SIGNATURES = {
     "exogcm_step": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
     "exogcm_read_snapshot": (ctypes.c_int, [_VP, ctypes.c_int, _FP, ctypes.c_size_t,
                                             ctypes.POINTER(ctypes.c_long)]),
+    "exogcm_set_stop": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_long]),
     "exogcm_slot_info": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_long),
                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "exogcm_field_size": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.POINTER(ctypes.c_size_t)]),
@@ -90,6 +91,8 @@ SIGNATURES = {
     "exogcm_device_field": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.POINTER(_VP),
                                            ctypes.POINTER(ctypes.c_size_t)]),
     "exogcm_stream": (_VP, [_VP]),
+    "exogcm_time_kernel": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.c_int, _FP, _DP]),
+    "exogcm_graph_launches": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
 }
 
 
@@ -247,6 +250,17 @@ class Engine:
         _check(_lib.exogcm_read_snapshot(self.h, slot, out.ctypes.data_as(_FP), n, ctypes.byref(step)))
         return step.value, out.reshape(-1, self.nhor)
 
+    def set_stop(self, slot: int, step: int) -> None:
+        """The slot stops advancing at model step `step` (-1: no limit)."""
+        _check(_lib.exogcm_set_stop(self.h, slot, step))
+
+    def read_snapshot_into(self, slot: int, out: np.ndarray) -> int:
+        """Copies the slot's last published snapshot into a float32 host
+        array; returns its step, or -1 (and leaves `out`) if none."""
+        step = ctypes.c_long()
+        _check(_lib.exogcm_read_snapshot(self.h, slot, out.ctypes.data_as(_FP), out.size, ctypes.byref(step)))
+        return step.value
+
     def slot_info(self, slot: int):
         step, left, active = ctypes.c_long(), ctypes.c_int(), ctypes.c_int()
         _check(_lib.exogcm_slot_info(self.h, slot, ctypes.byref(step), ctypes.byref(left), ctypes.byref(active)))
@@ -261,6 +275,17 @@ class Engine:
         ms = ctypes.c_float()
         _check(_lib.exogcm_last_step_ms(self.h, ctypes.byref(ms)))
         return ms.value
+
+    def time_kernel(self, kernel: str, reps: int = 10):
+        """(ms per launch, algorithmic bytes per launch) of one step kernel."""
+        ms, nbytes = ctypes.c_float(), ctypes.c_double()
+        _check(_lib.exogcm_time_kernel(self.h, kernel.encode(), reps, ctypes.byref(ms), ctypes.byref(nbytes)))
+        return ms.value, nbytes.value
+
+    def graph_launches(self, steps: int) -> int:
+        n = ctypes.c_size_t()
+        _check(_lib.exogcm_graph_launches(self.h, steps, ctypes.byref(n)))
+        return n.value
 
     def checkpoint_save(self, slot: int) -> bytes:
         buf, size = _VP(), ctypes.c_size_t()

@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -57,6 +58,7 @@ struct Slot {
   int carbon_step = 0;
   int startup_left = 0;
   long published = -1;
+  long stop = -1;  // model step at which the slot stops (-1: never)
   double deltsec[4] = {0}, delt[4] = {0};
   Calendar cal{};
 };
@@ -387,6 +389,7 @@ void full_step(const Model& m, cudaStream_t st) {
 StepParams next_params(Slot& s, int publish_every, bool advance) {
   StepParams p{};
   if (!s.active) return p;
+  if (s.stop >= 0 && s.startup_left == 0 && s.step >= s.stop) return p;  // finished: kernels skip the slot
   const int phase = s.startup_left;
   p.phase = phase;
   p.active = 1;
@@ -719,6 +722,14 @@ int exogcm_read_snapshot(exogcm_engine* e, int slot, float* values, size_t count
   });
 }
 
+int exogcm_set_stop(exogcm_engine* e, int slot, long step) {
+  return guard([&] {
+    if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    check_slot(e, slot);
+    e->slots[slot].stop = step;
+  });
+}
+
 int exogcm_slot_info(exogcm_engine* e, int slot, long* step, int* startup_left, int* active) {
   return guard([&] {
     if (!e) throw Error(EXOGCM_EINVAL, "null engine");
@@ -880,6 +891,91 @@ int exogcm_last_step_ms(exogcm_engine* e, float* ms) {
   return guard([&] {
     if (!e || !ms) throw Error(EXOGCM_EINVAL, "null argument");
     *ms = e->last_ms;
+  });
+}
+
+int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms, double* bytes) {
+  return guard([&] {
+    if (!e || !kernel || !ms || reps < 1) throw Error(EXOGCM_EINVAL, "bad argument");
+    if (!e->shared_ready) throw Error(EXOGCM_ESTATE, "no slot configured");
+    const Dims& d = e->d;
+    const int S = d.S;
+    for (int s = 0; s < S; ++s) {
+      Slot copy = e->slots[s];
+      e->hparams[s] = next_params(copy, 1 << 30, false);
+    }
+    check(cudaMemcpyAsync(e->params, e->hparams, S * sizeof(StepParams), cudaMemcpyHostToDevice, e->stream),
+          "params");
+    const Model m = e->model(0);
+    const FieldPtrs& F = m.f;
+    const int LP = d.L * S;
+    const double grid = (double)d.NHOR * 4, four = (double)d.NLAT * d.NFC * 4, spec = (double)d.NRSP * 4;
+    const double cols = (double)S * d.NHOR;
+    const std::string k(kernel);
+    std::function<void()> launch;
+    double b = 0;
+    if (k == "dft_forward") {
+      launch = [&] { tr_fourier_forward(m, F.gtn, F.fgtn, LP, e->stream); };
+      b = LP * (grid + four);
+    } else if (k == "dft_inverse") {
+      launch = [&] { tr_fourier_inverse(m, F.fgu, F.gu, LP, e->stream); };
+      b = LP * (four + grid);
+    } else if (k == "legendre_forward") {
+      launch = [&] { tr_legendre_forward(m, F.fgtdt, F.zstt1, LP, m.sh.qc, e->stream); };
+      b = LP * (four + spec);
+    } else if (k == "legendre_inverse") {
+      launch = [&] { tr_legendre_inverse(m, F.st, F.fgt, LP, m.sh.qi, e->stream); };
+      b = LP * (spec + four);
+    } else if (k == "dv2uv") {
+      launch = [&] { tr_dv2uv(m, F.sd, F.sz, F.fgu, F.fgv, LP, 1.63299310207f, e->stream); };
+      b = LP * 2 * (spec + four);
+    } else if (k == "uv2dv") {
+      launch = [&] { tr_uv2dv(m, F.fgvz, F.fguz, F.fgke, F.zdsdp1, F.zdszp1, LP, e->stream); };
+      b = LP * (3 * four + 2 * spec);
+    } else if (k == "qtend") {
+      launch = [&] { tr_qtend(m, F.fgut, F.fgvt, F.fgtn, F.zstt2, LP, e->stream); };
+      b = LP * (3 * four + spec);
+    } else if (k == "calcgp") {
+      launch = [&] { dyn_calcgp(m, e->stream); };
+      b = cols * 4 * (6.0 * d.L + 3 + 12.0 * d.L + 2);
+    } else if (k == "spectrala") {
+      launch = [&] { dyn_spectrala(m, e->stream); };
+      b = (double)S * d.NRSP * 4 * (6.0 * d.L + 3 + 14.0 * d.L + 3);
+    } else if (k == "vdiff") {
+      launch = [&] { phy_surface_flux(m, e->stream); };
+      b = cols * 4 * (8.0 * d.L + 4 * d.L);
+    } else if (k == "swr" || k == "lwr_radstep") {
+      launch = [&] { phy_radiation(m, e->stream); };
+      b = cols * 4 * (10.0 * d.L + 9.0 * (d.L + 1));
+    } else if (k == "kuo" || k == "rain_column") {
+      launch = [&] { phy_precipitation_columns(m, e->stream); };
+      b = cols * 4 * (12.0 * d.L + 10.0 * d.L);
+    } else {
+      throw Error(EXOGCM_EINVAL, "unknown kernel " + k);
+    }
+    launch();  // warm
+    check(cudaEventRecord(e->ev0, e->stream), "event");
+    for (int r = 0; r < reps; ++r) launch();
+    check(cudaEventRecord(e->ev1, e->stream), "event");
+    check(cudaStreamSynchronize(e->stream), "time kernel");
+    float total = 0;
+    check(cudaEventElapsedTime(&total, e->ev0, e->ev1), "event time");
+    *ms = total / reps;
+    if (bytes) *bytes = b;
+  });
+}
+
+int exogcm_graph_launches(exogcm_engine* e, int steps, size_t* launches) {
+  return guard([&] {
+    if (!e || !launches || steps < 1 || steps > kMaxBatch) throw Error(EXOGCM_EINVAL, "bad argument");
+    cudaGraph_t graph;
+    check(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed), "capture");
+    for (int k = 0; k < steps; ++k) full_step(e->model(k), e->stream);
+    check(cudaStreamEndCapture(e->stream, &graph), "capture end");
+    size_t n = 0;
+    check(cudaGraphGetNodes(graph, nullptr, &n), "graph nodes");
+    cudaGraphDestroy(graph);
+    *launches = n;
   });
 }
 
