@@ -18,9 +18,9 @@ TRANSFORM_TOL = 1e-5
 PHYSICS_TOL = 2e-3
 
 
-def build(truncation, levels, seed=11, slots=1, **kw):
+def build(truncation, levels, seed=11, slots=1, mode=0, **kw):
     p = planets.make_planet(seed, truncation=truncation, levels=levels, **kw)
-    e = pkg.Engine(truncation, levels, slots)
+    e = pkg.Engine(truncation, levels, slots, mode=mode)
     for s in range(slots):
         e.configure(s, p)
     return p, e
@@ -38,8 +38,8 @@ def test_initial_state_matches_oracle(truncation, levels):
         assert np.array_equal(got, ref32) or rel_rms(got, ref) < 1e-6, name
 
 
-def _stage_errors(truncation, levels, warm_steps, seed=11):
-    p, e = build(truncation, levels, seed=seed)
+def _stage_errors(truncation, levels, warm_steps, seed=11, mode=0):
+    p, e = build(truncation, levels, seed=seed, mode=mode)
     m = oracle.model_for(p)
     o = oracle.Oracle(m)
     e.step(warm_steps)
@@ -80,9 +80,10 @@ PHYSICS_FIELDS = {
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("truncation,levels,warm", [(21, 10, 6), (21, 5, 6), (42, 10, 4)])
-def test_stage_replay_matches_oracle(truncation, levels, warm):
-    worst = _stage_errors(truncation, levels, warm)
+@pytest.mark.parametrize("truncation,levels,warm,mode", [(21, 10, 6, 0), (21, 5, 6, 0), (42, 10, 4, 0),
+                                                         (21, 10, 6, 1), (42, 10, 4, 1), (63, 10, 4, 1)])
+def test_stage_replay_matches_oracle(truncation, levels, warm, mode):
+    worst = _stage_errors(truncation, levels, warm, mode=mode)
     report = sorted(((v[0], k, v[1]) for k, v in worst.items()), reverse=True)[:12]
     print("worst relative RMS per field:", [(f"{a:.2e}", b, c) for a, b, c in report])
     for name, (err, stage) in worst.items():
@@ -91,13 +92,14 @@ def test_stage_replay_matches_oracle(truncation, levels, warm):
 
 
 @pytest.mark.gpu
-def test_one_day_trajectory_t21_l10():
+@pytest.mark.parametrize("mode", [0, 1])
+def test_one_day_trajectory_t21_l10(mode):
     """1 day (3 start-up + 32 steps) from the same initial state: per-field
     relative RMS of the prognostic state against FP64."""
-    p, e = build(21, 10, seed=21)
+    p, e = build(21, 10, seed=21, mode=mode)
     m = oracle.model_for(p)
     o = oracle.Oracle(m)
-    e.step(35 if False else 3)  # start-up steps
+    e.step(3)  # start-up steps
     o.startup()
     for _ in range(4):
         e.step(8)
@@ -107,6 +109,26 @@ def test_one_day_trajectory_t21_l10():
     print("1-day relative RMS vs FP64:", errs, "dt", dt)
     assert errs["st"] < 5e-3 and errs["sz"] < 1e-3 and errs["sq"] < 5e-2 and errs["sp"] < 5e-2
     assert dt < 1e-3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("truncation", [21, 42, 63])
+def test_fft_matches_dense_dft(truncation):
+    """The optimized path's FFTs give the plain path's truncated DFT: one
+    gridpointa from the same state in both modes."""
+    p = planets.make_planet(71, truncation=truncation, levels=10)
+    plain = pkg.Engine(truncation, 10, 1, mode=0)
+    fast = pkg.Engine(truncation, 10, 1, mode=1)
+    plain.configure(0, p)
+    fast.configure(0, p)
+    plain.step(4)
+    for name in field_names(oracle.Oracle(oracle.model_for(p))):
+        fast.write(0, name, plain.read(0, name))
+    plain.run_stage("gridpointa")
+    fast.run_stage("gridpointa")
+    for name in ("gu", "gv", "gt", "gd", "gz", "gq", "gp", "gpj", "gpmt", "fgtn", "fgke", "fgvz", "sdt", "stt", "sqt"):
+        err = rel_rms(fast.read(0, name), plain.read(0, name))
+        assert err < 2e-6, f"{name}: {err:.2e}"
 
 
 @pytest.mark.gpu

@@ -104,6 +104,7 @@ struct SharedTabs {
   const float* nindex; // total wavenumber per real coefficient [NRSP]
   const int* mode_m;   // zonal wavenumber m of mode w [NCSP]
   const int* mode_n;   // total wavenumber n of mode w [NCSP]
+  const float* tw;     // e^{2 pi i j / NLON} as (cos, sin) pairs [NLON][2], for the FFTs
 };
 
 // Everything a step kernel can reach.
@@ -117,6 +118,7 @@ struct Model {
   const StepParams* params;  // [S] for the step being run
   double* sums;              // FP64 per-slot reductions scratch [S][4]
   int* flags;                // per-slot status flags [S]
+  int mode;                  // 0 plain FP32 path, 1 optimized path (FFTs, fused and tensor-core kernels)
 };
 
 }  // namespace exogcm

@@ -108,6 +108,7 @@ struct exogcm_engine {
     m.params = params + (size_t)k * d.S;
     m.sums = sums;
     m.flags = flags;
+    m.mode = mode;
     return m;
   }
 };
@@ -219,7 +220,13 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
         r += 2;
       }
   }
+  Vec tw(2 * (size_t)d.NLON);
+  for (int j = 0; j < d.NLON; ++j) {
+    tw[2 * j] = std::cos(2 * M_PI * j / d.NLON);
+    tw[2 * j + 1] = std::sin(2 * M_PI * j / d.NLON);
+  }
   const size_t izgw = put(zgw), ircsq = put(rcsq), isid = put(s.sines), icola = put(cola), inidx = put(nindex);
+  const size_t itw = put(tw);
   check(cudaMalloc(&e->shared_buf, buf.size() * sizeof(float)), "shared tables");
   check(cudaMemcpy(e->shared_buf, buf.data(), buf.size() * sizeof(float), cudaMemcpyHostToDevice), "shared tables");
   check(cudaMalloc(&e->mode_buf, 2 * d.NCSP * sizeof(int)), "mode tables");
@@ -241,6 +248,7 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
   e->sh.sid = b + isid;
   e->sh.cola = b + icola;
   e->sh.nindex = b + inidx;
+  e->sh.tw = b + itw;
   e->sh.mode_m = e->mode_buf;
   e->sh.mode_n = e->mode_buf + d.NCSP;
   e->shared_ready = true;
@@ -526,7 +534,7 @@ int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine
       throw Error(EXOGCM_EINVAL, "truncation must be 21, 42 or 63");
     if (levels != 5 && levels != 10) throw Error(EXOGCM_EINVAL, "levels must be 5 or 10");
     if (slots < 1 || slots > 4096) throw Error(EXOGCM_EINVAL, "slots must be 1..4096");
-    if (mode != 0) throw Error(EXOGCM_EINVAL, "mode must be 0 (plain FP32)");
+    if (mode != 0 && mode != 1) throw Error(EXOGCM_EINVAL, "mode must be 0 (plain FP32) or 1 (optimized)");
     auto e = std::make_unique<exogcm_engine>();
     e->d = make_dims(truncation, levels, slots);
     e->mode = mode;

@@ -20,6 +20,10 @@ void tr_uv2dv(const Model& m, const float* u, const float* v, const float* ke, f
 void tr_qtend(const Model& m, const float* u, const float* v, const float* src, float* out, int planes,
               cudaStream_t st);
 
+// fft.cu
+void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st);
+void fft_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st);
+
 // dynamics.cu
 void dyn_calcgp(const Model& m, cudaStream_t st);
 void dyn_spectrala(const Model& m, cudaStream_t st);

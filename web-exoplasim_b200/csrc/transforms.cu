@@ -290,6 +290,7 @@ void tr_init() {
 }
 
 void tr_fourier_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st) {
+  if (m.mode == 1) return fft_forward(m, g, c, planes, st);
   const int rows = planes * m.d.NLAT;
   const int rpb = dft_rows_per_block(m.d);
   const size_t smem = ((size_t)m.d.NLON * m.d.NFC + (size_t)rpb * m.d.NLON) * sizeof(float);
@@ -297,6 +298,7 @@ void tr_fourier_forward(const Model& m, const float* g, float* c, int planes, cu
 }
 
 void tr_fourier_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st) {
+  if (m.mode == 1) return fft_inverse(m, c, g, planes, st);
   const int rows = planes * m.d.NLAT;
   const int rpb = dft_rows_per_block(m.d);
   const size_t smem = ((size_t)m.d.NLON * m.d.NFC + (size_t)rpb * m.d.NFC) * sizeof(float);
