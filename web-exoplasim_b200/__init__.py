@@ -282,6 +282,12 @@ class Engine:
         _check(_lib.exogcm_time_kernel(self.h, kernel.encode(), reps, ctypes.byref(ms), ctypes.byref(nbytes)))
         return ms.value, nbytes.value
 
+    def device_field(self, name: str):
+        """(device pointer, floats across all slots) of a state field."""
+        ptr, n = _VP(), ctypes.c_size_t()
+        _check(_lib.exogcm_device_field(self.h, name.encode(), ctypes.byref(ptr), ctypes.byref(n)))
+        return ptr.value, n.value
+
     def graph_launches(self, steps: int) -> int:
         n = ctypes.c_size_t()
         _check(_lib.exogcm_graph_launches(self.h, steps, ctypes.byref(n)))

@@ -131,8 +131,11 @@ void layout(exogcm_engine* e) {
   (void)H;
   (void)P;
   size_t off = 0;
+  // Every field starts on a 256-byte boundary (vector loads in the FFTs need
+  // at least 8-byte aligned rows whatever the slot count).
 #define EXOGCM_ADD_FIELD(name, shape, cnt)                                            \
   {                                                                                   \
+    off = (off + 63) / 64 * 64;                                                       \
     FieldInfo fi{#name, #shape[0], (int)(cnt), plane_floats(d, #shape[0]), off};      \
     e->field_index[#name] = e->fields.size();                                         \
     e->fields.push_back(fi);                                                          \

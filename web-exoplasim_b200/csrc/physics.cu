@@ -423,10 +423,25 @@ __device__ __forceinline__ float vapour_absorption(float wv, float zsolar2) {
   return 2.9f * wv / (fpow(1.f + 141.5f * wv, 0.635f) + 5.925f * wv) / zsolar2;
 }
 
-// swr (physics/radiation/wgsl/swr.wgsl): two-band shortwave by the adding method.
+// swr (physics/radiation/wgsl/swr.wgsl): two-band shortwave by the adding
+// method. The bands (ozone below 0.75 um, water vapour above) are
+// independent until the fluxes are summed, so two neighbouring threads share
+// a column, one per band, and add their fluxes with a pair shuffle.
 template <int NL>
 __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
-  COLUMN_PROLOGUE
+  const Dims& d = m.d;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = t >> 1;
+  const int band = t & 1;
+  if (c >= d.S * d.NHOR) return;  // both threads of a pair leave together
+  const int slot = c / d.NHOR;
+  const StepParams& P = m.params[slot];
+  if (!P.active) return;
+  const PlanetConst& K = m.pc[slot];
+  const float* tb = m.tabs + (size_t)slot * m.to.stride;
+  const size_t SN = (size_t)d.S * d.NHOR;
+  const FieldPtrs& F = m.f;
+  const unsigned pair = 3u << ((threadIdx.x & 31) & ~1);
   const int NP = NL + 1;
   const float ZERO = 1.0e-6f, ZBETTA = 1.66f, ZMBAR = 1.9f, ZFO3 = 100.f / 2.14f, ZMU00 = 0.5f,
               INV_LN10 = 0.43429448190325176f;
@@ -437,169 +452,167 @@ __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
   const float ftop1 = K.ZSOLAR1 * K.GSOL0 * gdist2 * mu0;
   const float ftop2 = K.ZSOLAR2 * K.GSOL0 * gdist2 * mu0;
   if (!(ftop1 + ftop2 > ZERO)) {
-    for (int l = 0; l < NP; ++l) {
+    for (int l = band; l < NP; l += 2) {
       F.dfu[l * SN + c] = 0.f;
       F.dfd[l * SN + c] = 0.f;
       F.dswfl[l * SN + c] = 0.f;
     }
     return;
   }
+  const float ftop = band == 0 ? ftop1 : ftop2;
   const float dp = F.dp[c];
   float cc_[NL];
 #pragma unroll
   for (int l = 0; l < NL; ++l) cc_[l] = F.dcc[l * SN + c];
-  float rcl1[NL], rcl1s[NL], rcl2[NL], rcl2s[NL], tcl2[NL], tcl2s[NL];
+  // Cloud optics: band 0 keeps (rcl1, rcl1s), band 1 (rcl2, rcl2s, tcl2, tcl2s).
+  float rcl[NL], rcls[NL], tcl[NL], tcls[NL];
   float cs = 1.f;
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
     const float cc = cc_[l];
-    rcl1[l] = rcl1s[l] = rcl2[l] = rcl2s[l] = 0.f;
-    tcl2[l] = tcl2s[l] = 1.f;
+    rcl[l] = rcls[l] = 0.f;
+    tcl[l] = tcls[l] = 1.f;
     if (cc > 0.f) {
       const float lwp = fminf(1000.f, 1000.f * F.dql[l * SN + c] * dp / K.GA * ds[l]);
       const float tau = 2.f * fpow(logf(lwp + 1.5f) * INV_LN10, 3.9f);
-      const float zlog = logf(1000.f / tau);
-      float b2 = K.ZB4 / logf(3.f + 0.1f * tau);
-      float om0 = fminf(0.9999f, 1.f - K.ZB5 * zlog);
-      float un = 1.f - om0;
-      float uz = un + 2.f * b2 * om0;
-      float u = sqrtf(uz / un);
-      float ex = expf(fminf(25.f, tau * sqrtf(uz * un) / ZMU00));
-      float r = (u + 1.f) * (u + 1.f) * ex - (u - 1.f) * (u - 1.f) / ex;
-      rcl1s[l] = 1.f - 1.f / (1.f + K.ZB3 * tau);
-      tcl2s[l] = 4.f * u / r;
-      rcl2s[l] = (u * u - 1.f) / r * (ex - 1.f / ex);
-      const float b1 = K.TSWR1 * sqrtf(mu0);
-      b2 = K.TSWR2 * sqrtf(mu0) / logf(3.f + 0.1f * tau);
-      om0 = fminf(0.9999f, 1.f - K.TSWR3 * mu0 * mu0 * zlog);
-      un = 1.f - om0;
-      uz = un + 2.f * b2 * om0;
-      u = sqrtf(uz / un);
-      ex = expf(fminf(25.f, tau * sqrtf(uz * un) / mu0));
-      r = (u + 1.f) * (u + 1.f) * ex - (u - 1.f) * (u - 1.f) / ex;
-      const float direct1 = 1.f - 1.f / (1.f + b1 * tau / mu0);
-      const float directT = 4.f * u / r;
-      const float direct2 = (u * u - 1.f) / r * (ex - 1.f / ex);
-      rcl1[l] = cs * direct1 + (1.f - cs) * rcl1s[l];
-      tcl2[l] = cs * directT + (1.f - cs) * tcl2s[l];
-      rcl2[l] = cs * direct2 + (1.f - cs) * rcl2s[l];
+      if (band == 0) {
+        rcls[l] = 1.f - 1.f / (1.f + K.ZB3 * tau);
+        const float b1 = K.TSWR1 * sqrtf(mu0);
+        const float direct1 = 1.f - 1.f / (1.f + b1 * tau / mu0);
+        rcl[l] = cs * direct1 + (1.f - cs) * rcls[l];
+      } else {
+        const float zlog = logf(1000.f / tau);
+        float b2 = K.ZB4 / logf(3.f + 0.1f * tau);
+        float om0 = fminf(0.9999f, 1.f - K.ZB5 * zlog);
+        float un = 1.f - om0;
+        float uz = un + 2.f * b2 * om0;
+        float u = sqrtf(uz / un);
+        float ex = expf(fminf(25.f, tau * sqrtf(uz * un) / ZMU00));
+        float r = (u + 1.f) * (u + 1.f) * ex - (u - 1.f) * (u - 1.f) / ex;
+        tcls[l] = 4.f * u / r;
+        rcls[l] = (u * u - 1.f) / r * (ex - 1.f / ex);
+        b2 = K.TSWR2 * sqrtf(mu0) / logf(3.f + 0.1f * tau);
+        om0 = fminf(0.9999f, 1.f - K.TSWR3 * mu0 * mu0 * zlog);
+        un = 1.f - om0;
+        uz = un + 2.f * b2 * om0;
+        u = sqrtf(uz / un);
+        ex = expf(fminf(25.f, tau * sqrtf(uz * un) / mu0));
+        r = (u + 1.f) * (u + 1.f) * ex - (u - 1.f) * (u - 1.f) / ex;
+        const float directT = 4.f * u / r;
+        const float direct2 = (u * u - 1.f) / r * (ex - 1.f / ex);
+        tcl[l] = cs * directT + (1.f - cs) * tcls[l];
+        rcl[l] = cs * direct2 + (1.f - cs) * rcls[l];
+      }
     }
     cs = cs * (1.f - cc);
   }
+  // Absorber paths: ozone (band 0) or water vapour (band 1), slant above the
+  // first cloud and diffuse below.
   const float zm = 35.f / sqrtf(1.f + 1224.f * mu0 * mu0);
-  float o3l[NL], xo3l[NL], wvl[NL], ywvl[NL];
-  float o3t = 0.f, xo3t = 0.f, wvt = 0.f, ywvt = 0.f;
+  const float diffusivity = band == 0 ? ZMBAR : ZBETTA;
+  float pl[NL], xpl[NL];
+  float pt = 0.f, xpt = 0.f;
   cs = 1.f;
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
     const float dsigma = ds[l];
-    const float o3 = ZFO3 * dsigma * dp * F.dqo3[l * SN + c] / K.GA;
-    o3t = o3t + o3;
-    xo3t = cs * (xo3t + zm * o3) + (1.f - cs) * (xo3t + ZMBAR * o3);
-    o3l[l] = o3t;
-    xo3l[l] = xo3t;
-    const float wv = 0.1f * dsigma * F.dq[l * SN + c] * dp / K.GA * sqrtf(273.f / F.dt[l * SN + c]) * sg[l] * dp / 100000.f;
-    wvt = wvt + wv;
-    ywvt = cs * (ywvt + zm * wv) + (1.f - cs) * (ywvt + ZBETTA * wv);
-    wvl[l] = wvt;
-    ywvl[l] = ywvt;
+    const float amount = band == 0 ? ZFO3 * dsigma * dp * F.dqo3[l * SN + c] / K.GA
+                                   : 0.1f * dsigma * F.dq[l * SN + c] * dp / K.GA * sqrtf(273.f / F.dt[l * SN + c]) *
+                                         sg[l] * dp / 100000.f;
+    pt = pt + amount;
+    xpt = cs * (xpt + zm * amount) + (1.f - cs) * (xpt + diffusivity * amount);
+    pl[l] = pt;
+    xpl[l] = xpt;
     cs = cs * (1.f - cc_[l]);
   }
-  float ta1 = 1.f, ta1s = 1.f, ra1 = 0.f, ra1s = 0.f, ta2 = 1.f, ta2s = 1.f, ra2 = 0.f, ra2s = 0.f;
-  float to3t = 1.f, to3tu = 1.f - ozone_absorption(xo3t + ZMBAR * o3t, K.ZSOLAR1);
-  float twvt = 1.f, twvtu = 1.f - vapour_absorption(ywvt + ZBETTA * wvt, K.ZSOLAR2);
+  auto absorption = [&](float x) {
+    return band == 0 ? ozone_absorption(x, K.ZSOLAR1) : vapour_absorption(x, K.ZSOLAR2);
+  };
+  float ta = 1.f, tas = 1.f, ra = 0.f, ras = 0.f;
+  float tt = 1.f, ttu = 1.f - absorption(xpt + diffusivity * pt);
   const float ccn = cc_[NL - 1];
   const float scf = K.RCOEFF * dp / 101100.f * 9.80665f / K.GA;
   const float diffuseRayleigh = 1.f - expf(scf * K.LN_DIFFUSE_RAYLEIGH);
   const float rcsuSurface = diffuseRayleigh * (1.f - ccn);
   const float rcsSurface =
       (1.f - expf(scf * logf(1.f - 0.219f / (1.f + 0.816f * mu0)))) * cs + diffuseRayleigh * (1.f - cs - ccn);
-  float t1[NL + 1], t2[NL + 1], r1s[NL + 1], r2s[NL + 1];
-  float tb1[NL], tb1u[NL], rb1[NL], rb1s[NL], tb2[NL], tb2u[NL], rb2[NL], rb2s[NL];
+  float tl[NL + 1], rls[NL + 1];
+  float tbd[NL], tbu[NL], rb[NL], rbs[NL];
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
     const float cc = cc_[l];
-    t1[l] = ta1;
-    t2[l] = ta2;
-    r1s[l] = ra1s;
-    r2s[l] = ra2s;
+    tl[l] = ta;
+    rls[l] = ras;
     const bool surface = l == NL - 1;
-    rb1[l] = (surface ? rcsSurface : 0.f) + rcl1[l] * cc;
-    rb1s[l] = (surface ? rcsuSurface : 0.f) + rcl1s[l] * cc;
-    float o3 = xo3l[l];
-    const float to3 = (1.f - ozone_absorption(o3, K.ZSOLAR1)) / to3t;
-    to3t = to3t * to3;
-    o3 = xo3t + ZMBAR * (o3t - o3l[l]);
-    const float to3u = to3tu / (1.f - ozone_absorption(o3, K.ZSOLAR1));
-    to3tu = to3tu / to3u;
-    tb1[l] = 1.f - (1.f - to3) * (1.f - cc) - rb1[l];
-    tb1u[l] = 1.f - (1.f - to3u) * (1.f - cc) - rb1s[l];
-    const float m1 = 1.f / (1.f - ra1s * rb1s[l]);
-    ra1 = ra1 + ta1 * rb1[l] * ta1s * m1;
-    ta1 = ta1 * tb1[l] * m1;
-    ra1s = rb1s[l] + tb1u[l] * ra1s * tb1[l] * m1;
-    ta1s = tb1u[l] * ta1s * m1;
-    rb2[l] = rcl2[l] * cc;
-    rb2s[l] = rcl2s[l] * cc;
-    float wv = ywvl[l];
-    const float twv = (1.f - vapour_absorption(wv, K.ZSOLAR2)) / twvt;
-    twvt = twvt * twv;
-    wv = ywvt + ZBETTA * (wvt - wvl[l]);
-    const float twvu = twvtu / (1.f - vapour_absorption(wv, K.ZSOLAR2));
-    twvtu = twvtu / twvu;
-    tb2[l] = 1.f - (1.f - twv) * (1.f - cc) - (1.f - tcl2[l]) * cc;
-    tb2u[l] = 1.f - (1.f - twvu) * (1.f - cc) - (1.f - tcl2s[l]) * cc;
-    const float m2 = 1.f / (1.f - ra2s * rb2s[l]);
-    ra2 = ra2 + ta2 * rb2[l] * ta2s * m2;
-    ta2 = ta2 * tb2[l] * m2;
-    ra2s = rb2s[l] + tb2u[l] * ra2s * tb2[l] * m2;
-    ta2s = tb2u[l] * ta2s * m2;
+    float x = xpl[l];
+    const float tr = (1.f - absorption(x)) / tt;
+    tt = tt * tr;
+    x = xpt + diffusivity * (pt - pl[l]);
+    const float tru = ttu / (1.f - absorption(x));
+    ttu = ttu / tru;
+    if (band == 0) {
+      rb[l] = (surface ? rcsSurface : 0.f) + rcl[l] * cc;
+      rbs[l] = (surface ? rcsuSurface : 0.f) + rcls[l] * cc;
+      tbd[l] = 1.f - (1.f - tr) * (1.f - cc) - rb[l];
+      tbu[l] = 1.f - (1.f - tru) * (1.f - cc) - rbs[l];
+    } else {
+      rb[l] = rcl[l] * cc;
+      rbs[l] = rcls[l] * cc;
+      tbd[l] = 1.f - (1.f - tr) * (1.f - cc) - (1.f - tcl[l]) * cc;
+      tbu[l] = 1.f - (1.f - tru) * (1.f - cc) - (1.f - tcls[l]) * cc;
+    }
+    const float mm = 1.f / (1.f - ras * rbs[l]);
+    ra = ra + ta * rb[l] * tas * mm;
+    ta = ta * tbd[l] * mm;
+    ras = rbs[l] + tbu[l] * ras * tbd[l] * mm;
+    tas = tbu[l] * tas * mm;
   }
-  t1[NL] = ta1;
-  t2[NL] = ta2;
-  r1s[NL] = ra1s;
-  r2s[NL] = ra2s;
+  tl[NL] = ta;
+  rls[NL] = ras;
+  // Surface albedo: land and sea ice keep theirs, open water gets a
+  // zenith-angle dependent one (band 0 writes the updated fields).
   const bool star = K.NSTARTEMP != 0.f;
   const float dalb = F.dalb[c], salb1 = F.dsalb[c], salb2 = F.dsalb[SN + c];
-  ra1s = star ? salb1 : dalb;
-  ra2s = star ? salb2 : dalb;
+  const float salb = band == 0 ? salb1 : salb2;
+  ras = star ? salb : dalb;
   const float dls = F.dls[c], dicec = F.dicec[c];
   const float water = (1.f - dls) * (1.f - dicec) * fminf(0.05f / (mu0 + 0.15f), 0.15f);
   const float nalb1 = dls * salb1 + (1.f - dls) * dicec * salb1 + water;
   const float nalb2 = dls * salb2 + (1.f - dls) * dicec * salb2 + water;
-  F.dsalb[c] = nalb1;
-  F.dsalb[SN + c] = nalb2;
   const float albedo = star ? K.ZSOLARS1 * nalb1 + K.ZSOLARS2 * nalb2 : dls * dalb + (1.f - dls) * dicec * dalb + water;
-  F.dalb[c] = albedo;
-  ra1 = star ? nalb1 : albedo;
-  ra2 = star ? nalb2 : albedo;
-  float rl1[NL + 1], rl2[NL + 1], rl1s[NL + 1], rl2s[NL + 1];
+  __syncwarp(pair);  // both bands have read dalb and dsalb
+  if (band == 0) {
+    F.dsalb[c] = nalb1;
+    F.dsalb[SN + c] = nalb2;
+    F.dalb[c] = albedo;
+  }
+  ra = star ? (band == 0 ? nalb1 : nalb2) : albedo;
+  float rl[NL + 1], rlsu[NL + 1];
 #pragma unroll
   for (int l = NL - 1; l >= 0; --l) {
-    rl1[l + 1] = ra1;
-    rl2[l + 1] = ra2;
-    rl1s[l + 1] = ra1s;
-    rl2s[l + 1] = ra2s;
-    const float d1 = 1.f - ra1s * rb1s[l];
-    ra1 = rb1[l] + tb1[l] * ra1 * tb1u[l] / d1;
-    ra1s = rb1s[l] + tb1u[l] * ra1s * tb1u[l] / d1;
-    const float d2 = 1.f - ra2s * rb2s[l];
-    ra2 = rb2[l] + tb2[l] * ra2 * tb2u[l] / d2;
-    ra2s = rb2s[l] + tb2u[l] * ra2s * tb2u[l] / d2;
+    rl[l + 1] = ra;
+    rlsu[l + 1] = ras;
+    const float dd = 1.f - ras * rbs[l];
+    ra = rb[l] + tbd[l] * ra * tbu[l] / dd;
+    ras = rbs[l] + tbu[l] * ras * tbu[l] / dd;
   }
-  rl1[0] = ra1;
-  rl2[0] = ra2;
-  rl1s[0] = ra1s;
-  rl2s[0] = ra2s;
+  rl[0] = ra;
+  rlsu[0] = ras;
 #pragma unroll
   for (int l = 0; l < NP; ++l) {
-    const float m1 = 1.f / (1.f - r1s[l] * rl1s[l]);
-    const float m2 = 1.f / (1.f - r2s[l] * rl2s[l]);
-    const float fu = -t1[l] * rl1[l] * m1 * ftop1 + -t2[l] * rl2[l] * m2 * ftop2;
-    const float fd = t1[l] * m1 * ftop1 + t2[l] * m2 * ftop2;
-    F.dfu[l * SN + c] = fu;
-    F.dfd[l * SN + c] = fd;
-    F.dswfl[l * SN + c] = fu + fd;
+    const float mm = 1.f / (1.f - rls[l] * rlsu[l]);
+    const float fu = -tl[l] * rl[l] * mm * ftop;
+    const float fd = tl[l] * mm * ftop;
+    const float fu2 = __shfl_xor_sync(pair, fu, 1);
+    const float fd2 = __shfl_xor_sync(pair, fd, 1);
+    // band 1 + band 2, in the reference's order
+    const float fut = band == 0 ? fu + fu2 : fu2 + fu;
+    const float fdt = band == 0 ? fd + fd2 : fd2 + fd;
+    if ((l & 1) == band) {
+      F.dfu[l * SN + c] = fut;
+      F.dfd[l * SN + c] = fdt;
+      F.dswfl[l * SN + c] = fut + fdt;
+    }
   }
 }
 
@@ -1949,7 +1962,12 @@ COLUMN_LAUNCHER(FixerApply, k_fixer_apply)
 COLUMN_LAUNCHER(Surflx, k_surflx)
 COLUMN_LAUNCHER(Vdiff, k_vdiff)
 COLUMN_LAUNCHER(SolangMko3, k_solang_mko3)
-COLUMN_LAUNCHER(Swr, k_swr)
+template <int NL>
+struct Swr {
+  static void run(const Model& m, cudaStream_t st) {
+    k_swr<NL><<<nblocks(2 * (size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);
+  }
+};
 COLUMN_LAUNCHER(LwrRadstep, k_lwr_radstep)
 COLUMN_LAUNCHER(Kuo, k_kuo)
 COLUMN_LAUNCHER(Mkdca, k_mkdca)

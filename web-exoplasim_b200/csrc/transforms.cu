@@ -78,53 +78,79 @@ __global__ void k_dlambda(const float* __restrict__ a, float* __restrict__ b, in
 }
 
 // ---------------------------------------------------------------- Legendre
-// Inverse transforms (sp2fc, sp2fcdmu, dv2uv): each output (plane, lat, m)
-// sums modes n = m..NTRU of its plane; a block stages kPlanes spectral
-// planes and serves kLats latitudes.
+// Inverse transforms (sp2fc, sp2fcdmu, dv2uv): output (plane, lat, m) sums
+// modes n = m..NTRU of its plane. A block stages a tile of spectral planes
+// and the table rows of a tile of latitudes in shared memory (coalesced
+// loads, reused by every plane), and each thread computes wavenumbers j and
+// NTRU - j together so every thread sums NTRU + 2 terms.
 constexpr int kInvPlanes = 4;
-constexpr int kInvLats = 8;
 
-__global__ void __launch_bounds__(kThreads) k_leg_inverse(const float* __restrict__ s,
-                                                          float* __restrict__ f, int planes,
-                                                          const float* __restrict__ q, Dims d) {
-  extern __shared__ float sp[];  // [kInvPlanes][NRSP]
+struct InvTile {
+  int lats;    // latitudes per block
+  size_t smem; // bytes
+};
+
+InvTile inverse_tile(const Dims& d, int tables, int inputs) {
+  const size_t budget = 160 * 1024;
+  for (int lats = 16; lats >= 2; lats /= 2) {
+    const size_t smem = (size_t)inputs * kInvPlanes * d.NRSP * 4 + (size_t)tables * lats * d.NCSP * 4;
+    if (smem <= budget && d.NLAT % lats == 0) return {lats, smem};
+  }
+  return {1, (size_t)inputs * kInvPlanes * d.NRSP * 4 + (size_t)tables * d.NCSP * 4};
+}
+
+__device__ __forceinline__ int mode_first(int m, int ntp1) { return m * (2 * ntp1 - m + 1) / 2; }
+
+__global__ void __launch_bounds__(kThreads) k_leg_inverse(const float* __restrict__ s, float* __restrict__ f,
+                                                          int planes, const float* __restrict__ q, Dims d,
+                                                          int lats) {
+  extern __shared__ float smem[];
+  float* sp = smem;                        // [kInvPlanes][NRSP]
+  float* qs = smem + kInvPlanes * d.NRSP;  // [lats][NCSP]
   const int p0 = blockIdx.x * kInvPlanes;
   const int np = min(kInvPlanes, planes - p0);
-  const int lat0 = blockIdx.y * kInvLats;
+  const int lat0 = blockIdx.y * lats;
   for (int i = threadIdx.x; i < np * d.NRSP; i += blockDim.x) sp[i] = s[(size_t)p0 * d.NRSP + i];
+  for (int i = threadIdx.x; i < lats * d.NCSP; i += blockDim.x) qs[i] = q[(size_t)lat0 * d.NCSP + i];
   __syncthreads();
-  const int outputs = np * kInvLats * d.NTP1;
-  for (int o = threadIdx.x; o < outputs; o += blockDim.x) {
-    const int m = o % d.NTP1;
-    const int lat = lat0 + (o / d.NTP1) % kInvLats;
-    const int p = o / (d.NTP1 * kInvLats);
-    const int first = m * (2 * d.NTP1 - m + 1) / 2;
+  const int pairs = (d.NTP1 + 1) / 2;
+  for (int o = threadIdx.x; o < np * lats * pairs; o += blockDim.x) {
+    const int j = o % pairs;
+    const int lat = (o / pairs) % lats;
+    const int p = o / (pairs * lats);
     const float* spp = sp + p * d.NRSP;
-    const float* qr = q + (size_t)lat * d.NCSP;
-    float re = 0.f, im = 0.f;
-    for (int w = first; w < first + d.NTP1 - m; ++w) {
-      const float qq = qr[w];
-      re = fmaf(qq, spp[2 * w], re);
-      im = fmaf(qq, spp[2 * w + 1], im);
+    const float* qr = qs + lat * d.NCSP;
+    float* out = f + ((size_t)(p0 + p) * d.NLAT + lat0 + lat) * d.NFC;
+#pragma unroll 1
+    for (int half = 0; half < 2; ++half) {
+      const int m = half == 0 ? j : d.T - j;
+      if (half == 1 && m == j) break;
+      const int first = mode_first(m, d.NTP1);
+      float re = 0.f, im = 0.f;
+      for (int w = first; w < first + d.NTP1 - m; ++w) {
+        const float qq = qr[w];
+        re = fmaf(qq, spp[2 * w], re);
+        im = fmaf(qq, spp[2 * w + 1], im);
+      }
+      out[2 * m] = re;
+      out[2 * m + 1] = im;
     }
-    const size_t at = ((size_t)(p0 + p) * d.NLAT + lat) * d.NFC + 2 * m;
-    f[at] = re;
-    f[at + 1] = im;
   }
 }
 
 // dv2uv: winds at every latitude from spectral divergence and vorticity,
 // with plavor removed from vorticity mode w = 1 (legendre/wgsl/dv2uv.wgsl).
-__global__ void __launch_bounds__(kThreads) k_dv2uv(const float* __restrict__ D,
-                                                    const float* __restrict__ Z,
-                                                    float* __restrict__ U, float* __restrict__ V,
-                                                    int planes, const float* __restrict__ qu,
-                                                    const float* __restrict__ qv, float plavor,
-                                                    Dims d) {
-  extern __shared__ float sp[];  // [kInvPlanes][2][NRSP]
+__global__ void __launch_bounds__(kThreads) k_dv2uv(const float* __restrict__ D, const float* __restrict__ Z,
+                                                    float* __restrict__ U, float* __restrict__ V, int planes,
+                                                    const float* __restrict__ qu, const float* __restrict__ qv,
+                                                    float plavor, Dims d, int lats) {
+  extern __shared__ float smem[];
+  float* sp = smem;                                 // [kInvPlanes][2][NRSP]
+  float* qus = smem + 2 * kInvPlanes * d.NRSP;      // [lats][NCSP]
+  float* qvs = qus + (size_t)lats * d.NCSP;         // [lats][NCSP]
   const int p0 = blockIdx.x * kInvPlanes;
   const int np = min(kInvPlanes, planes - p0);
-  const int lat0 = blockIdx.y * kInvLats;
+  const int lat0 = blockIdx.y * lats;
   for (int i = threadIdx.x; i < np * d.NRSP; i += blockDim.x) {
     const int p = i / d.NRSP, k = i % d.NRSP;
     sp[(2 * p) * d.NRSP + k] = D[(size_t)p0 * d.NRSP + i];
@@ -132,31 +158,40 @@ __global__ void __launch_bounds__(kThreads) k_dv2uv(const float* __restrict__ D,
     if (k == 2) z -= plavor;  // w == 1, real part
     sp[(2 * p + 1) * d.NRSP + k] = z;
   }
+  for (int i = threadIdx.x; i < lats * d.NCSP; i += blockDim.x) {
+    qus[i] = qu[(size_t)lat0 * d.NCSP + i];
+    qvs[i] = qv[(size_t)lat0 * d.NCSP + i];
+  }
   __syncthreads();
-  const int outputs = np * kInvLats * d.NTP1;
-  for (int o = threadIdx.x; o < outputs; o += blockDim.x) {
-    const int m = o % d.NTP1;
-    const int lat = lat0 + (o / d.NTP1) % kInvLats;
-    const int p = o / (d.NTP1 * kInvLats);
-    const int first = m * (2 * d.NTP1 - m + 1) / 2;
+  const int pairs = (d.NTP1 + 1) / 2;
+  for (int o = threadIdx.x; o < np * lats * pairs; o += blockDim.x) {
+    const int j = o % pairs;
+    const int lat = (o / pairs) % lats;
+    const int p = o / (pairs * lats);
     const float* dd = sp + (2 * p) * d.NRSP;
     const float* zz = sp + (2 * p + 1) * d.NRSP;
-    const float* qur = qu + (size_t)lat * d.NCSP;
-    const float* qvr = qv + (size_t)lat * d.NCSP;
-    float ure = 0.f, uim = 0.f, vre = 0.f, vim = 0.f;
-    for (int w = first; w < first + d.NTP1 - m; ++w) {
-      const float a = qur[w], b = qvr[w];
-      const float zre = zz[2 * w], zim = zz[2 * w + 1], dre = dd[2 * w], dim = dd[2 * w + 1];
-      ure = ure + b * zre + a * dim;
-      uim = uim + b * zim - a * dre;
-      vre = vre + a * zim - b * dre;
-      vim = vim - a * zre - b * dim;
+    const float* qur = qus + lat * d.NCSP;
+    const float* qvr = qvs + lat * d.NCSP;
+    const size_t row = ((size_t)(p0 + p) * d.NLAT + lat0 + lat) * d.NFC;
+#pragma unroll 1
+    for (int half = 0; half < 2; ++half) {
+      const int m = half == 0 ? j : d.T - j;
+      if (half == 1 && m == j) break;
+      const int first = mode_first(m, d.NTP1);
+      float ure = 0.f, uim = 0.f, vre = 0.f, vim = 0.f;
+      for (int w = first; w < first + d.NTP1 - m; ++w) {
+        const float a = qur[w], b = qvr[w];
+        const float zre = zz[2 * w], zim = zz[2 * w + 1], dre = dd[2 * w], dim = dd[2 * w + 1];
+        ure = ure + b * zre + a * dim;
+        uim = uim + b * zim - a * dre;
+        vre = vre + a * zim - b * dre;
+        vim = vim - a * zre - b * dim;
+      }
+      U[row + 2 * m] = ure;
+      U[row + 2 * m + 1] = uim;
+      V[row + 2 * m] = vre;
+      V[row + 2 * m + 1] = vim;
     }
-    const size_t at = ((size_t)(p0 + p) * d.NLAT + lat) * d.NFC + 2 * m;
-    U[at] = ure;
-    U[at + 1] = uim;
-    V[at] = vre;
-    V[at + 1] = vim;
   }
 }
 
@@ -312,16 +347,16 @@ void tr_dlambda(const Model& m, const float* a, float* b, int planes, cudaStream
 
 void tr_legendre_inverse(const Model& m, const float* s, float* f, int planes, const float* q,
                          cudaStream_t st) {
-  dim3 grid((planes + kInvPlanes - 1) / kInvPlanes, m.d.NLAT / kInvLats);
-  const size_t smem = (size_t)kInvPlanes * m.d.NRSP * sizeof(float);
-  k_leg_inverse<<<grid, kThreads, smem, st>>>(s, f, planes, q, m.d);
+  const InvTile t = inverse_tile(m.d, 1, 1);
+  dim3 grid((planes + kInvPlanes - 1) / kInvPlanes, m.d.NLAT / t.lats);
+  k_leg_inverse<<<grid, kThreads, t.smem, st>>>(s, f, planes, q, m.d, t.lats);
 }
 
 void tr_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V, int planes, float plavor,
               cudaStream_t st) {
-  dim3 grid((planes + kInvPlanes - 1) / kInvPlanes, m.d.NLAT / kInvLats);
-  const size_t smem = (size_t)2 * kInvPlanes * m.d.NRSP * sizeof(float);
-  k_dv2uv<<<grid, kThreads, smem, st>>>(D, Z, U, V, planes, m.sh.qu, m.sh.qv, plavor, m.d);
+  const InvTile t = inverse_tile(m.d, 2, 2);
+  dim3 grid((planes + kInvPlanes - 1) / kInvPlanes, m.d.NLAT / t.lats);
+  k_dv2uv<<<grid, kThreads, t.smem, st>>>(D, Z, U, V, planes, m.sh.qu, m.sh.qv, plavor, m.d, t.lats);
 }
 
 void tr_legendre_forward(const Model& m, const float* f, float* s, int planes, const float* q,
