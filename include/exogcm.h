@@ -182,6 +182,27 @@ int exogcm_time_kernel(exogcm_engine* engine, const char* kernel, int reps, floa
 /* Kernel launches in the CUDA graph of a `steps`-step batch. */
 int exogcm_graph_launches(exogcm_engine* engine, int steps, size_t* launches);
 
+/* Allocation-free per-slot FP64 sums (no counterpart in the reference).
+ *
+ * For callers that cannot allocate device memory: a host embedded in another
+ * framework's memory pool where cudaMalloc is not allowed, a runtime whose
+ * device footprint is fixed after start-up, or code that must not trigger
+ * the device synchronization cudaMalloc/cudaFree can cause. It computes what
+ * the step's fixer and getiflx reductions compute: for each of `slots`
+ * planets, the sums of `points` values of `first` and of `second`
+ * (device arrays [slots][points], the layout exogcm_device_field gives for a
+ * one-level grid field), in double precision with a fixed order, written as
+ * floats to the device array `sums` [2][slots] (first sums, then second).
+ * It calls no allocator: its scratch is a static device array sized for at
+ * most 256 slots (1 MiB, held on every GPU that loads the library until the
+ * process exits); larger `slots` are rejected with EXOGCM_EINVAL. The first
+ * call on a device looks up that array's device address, so make the first
+ * call before any stream capture. Every call shares the scratch and keeps
+ * the last call's contents; calls that overlap on the GPU race. `stream` is
+ * a cudaStream_t (NULL: the legacy default stream). */
+int exogcm_slot_sums_noalloc(const float* first, const float* second, int slots, int points, float* sums,
+                             void* stream);
+
 /* Raw device pointer of a field (slot-major layout [plane][slot][points])
  * and the engine's CUDA stream, for in-process hosts that keep inputs
  * resident. */

@@ -92,6 +92,7 @@ SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_size_t)]),
     "exogcm_stream": (_VP, [_VP]),
     "exogcm_time_kernel": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.c_int, _FP, _DP]),
+    "exogcm_slot_sums_noalloc": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_int, _VP, _VP]),
     "exogcm_graph_launches": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
 }
 

@@ -35,6 +35,14 @@ namespace {
 
 thread_local std::string g_error;
 
+}  // namespace
+
+namespace exogcm {
+void set_error(const std::string& message) { g_error = message; }
+}  // namespace exogcm
+
+namespace {
+
 struct Error : std::runtime_error {
   int code;
   Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
