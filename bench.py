@@ -14,6 +14,7 @@ Reference arm: python bench.py --impl reference ...
 from __future__ import annotations
 
 import argparse
+import datetime
 import importlib
 import json
 import os
@@ -50,47 +51,81 @@ def dist_env():
 
 
 class Clocks:
-    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    """nvidia-smi samples of SM clock and throttle reasons during a region.
+
+    The sampler starts before the region and is waited for until its first
+    row is written; rows are kept by their timestamps, those inside the
+    region (or, for a region shorter than the 50 ms interval, the rows just
+    before and after it)."""
+
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.path = os.path.join("/tmp", f"exogcm_clocks_{os.getpid()}.csv")
+        self.t0 = self.t1 = None
+
+    def _rows(self):
+        try:
+            text = open(self.path).read()
+        except OSError:
+            return []
+        out = []
+        for line in text.strip().splitlines():
+            r = [x.strip() for x in line.split(",")]
+            if len(r) < 7:
+                continue
+            try:
+                stamp = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                out.append((stamp, float(r[1]), float(r[2]), r[3:7]))
+            except ValueError:
+                continue
+        return out
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}",
-                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
-                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                ["nvidia-smi", f"--id={self.index}", "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            deadline = time.time() + 5.0
+            while not self._rows() and time.time() < deadline:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
+        self.t0 = time.time()
         return self
 
     def __exit__(self, *exc):
+        self.t1 = time.time()
         if self.proc:
+            deadline = time.time() + 1.0
+            while time.time() < deadline and not any(r[0] > self.t1 for r in self._rows()):
+                time.sleep(0.02)
             self.proc.terminate()
             self.proc.wait()
 
     def summary(self):
-        try:
-            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
-        except Exception:
-            return None
+        rows = self._rows()
         if not rows:
             return None
-        sm = sorted(float(r[0]) for r in rows)
+        inside = [r for r in rows if self.t0 <= r[0] <= self.t1]
+        if not inside:
+            before = [r for r in rows if r[0] < self.t0][-1:]
+            after = [r for r in rows if r[0] > self.t1][:1]
+            inside = before + after or rows[-1:]
+        sm = sorted(r[1] for r in inside)
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            for name, v in zip(names, r[2:]):
-                if v.strip() == "Active":
+        for r in inside:
+            for name, v in zip(names, r[3]):
+                if v == "Active":
                     reasons.add(name)
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][1]), "reasons": sorted(reasons),
-                "samples": len(rows)}
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": inside[0][2], "reasons": sorted(reasons),
+                "samples": len(inside), "region_s": round(self.t1 - self.t0, 3)}
 
 
 def make_planets(count, seed0=1000):

@@ -38,3 +38,14 @@ def oracle_at_phase(o, phase, step):
     """Sets the oracle's constants and host values to one step of a slot."""
     o.set_phase(phase)
     o.write_step_values(step, publish=False)
+
+
+def rel_rms_without_worst_columns(got, ref, nhor, drop):
+    """Relative RMS of a grid field after removing its `drop` columns with
+    the largest squared error (summed over the field's planes)."""
+    got = np.asarray(got, dtype=np.float64).reshape(-1, nhor)
+    ref = np.asarray(ref, dtype=np.float64).reshape(-1, nhor)
+    col = ((got - ref) ** 2).sum(axis=0)
+    keep = np.ones(nhor, dtype=bool)
+    keep[np.argsort(col)[::-1][:drop]] = False
+    return rel_rms(got[:, keep], ref[:, keep])

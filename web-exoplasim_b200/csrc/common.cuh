@@ -105,6 +105,12 @@ struct SharedTabs {
   const int* mode_m;   // zonal wavenumber m of mode w [NCSP]
   const int* mode_n;   // total wavenumber n of mode w [NCSP]
   const float* tw;     // e^{2 pi i j / NLON} as (cos, sin) pairs [NLON][2], for the FFTs
+  // Northern halves of the inverse tables, transposed to [NCSP][NLAT / 2]
+  // for the optimized path's latitude-pair transforms.
+  const float* qiT;
+  const float* qjT;
+  const float* quT;
+  const float* qvT;
 };
 
 // Everything a step kernel can reach.

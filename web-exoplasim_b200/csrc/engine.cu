@@ -238,6 +238,17 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
   }
   const size_t izgw = put(zgw), ircsq = put(rcsq), isid = put(s.sines), icola = put(cola), inidx = put(nindex);
   const size_t itw = put(tw);
+  // Transposed northern halves of qi, qj, qu, qv ([mode][pair]).
+  size_t qt[4];
+  const char* tnames[4] = {"qi", "qj", "qu", "qv"};
+  for (int i = 0; i < 4; ++i) {
+    const Vec& q = s.q.at(tnames[i]);
+    const int JH = d.NLAT / 2;
+    Vec t((size_t)d.NCSP * JH);
+    for (int j = 0; j < JH; ++j)
+      for (int w = 0; w < d.NCSP; ++w) t[(size_t)w * JH + j] = q[(size_t)j * d.NCSP + w];
+    qt[i] = put(t);
+  }
   check(cudaMalloc(&e->shared_buf, buf.size() * sizeof(float)), "shared tables");
   check(cudaMemcpy(e->shared_buf, buf.data(), buf.size() * sizeof(float), cudaMemcpyHostToDevice), "shared tables");
   check(cudaMalloc(&e->mode_buf, 2 * d.NCSP * sizeof(int)), "mode tables");
@@ -260,6 +271,10 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
   e->sh.cola = b + icola;
   e->sh.nindex = b + inidx;
   e->sh.tw = b + itw;
+  e->sh.qiT = b + qt[0];
+  e->sh.qjT = b + qt[1];
+  e->sh.quT = b + qt[2];
+  e->sh.qvT = b + qt[3];
   e->sh.mode_m = e->mode_buf;
   e->sh.mode_n = e->mode_buf + d.NCSP;
   e->shared_ready = true;

@@ -20,6 +20,17 @@ void tr_uv2dv(const Model& m, const float* u, const float* v, const float* ke, f
 void tr_qtend(const Model& m, const float* u, const float* v, const float* src, float* out, int planes,
               cudaStream_t st);
 
+// legendre.cu (optimized path)
+void leg_init();
+void leg_inverse(const Model& m, const float* s, float* f, int planes, bool derivative, cudaStream_t st);
+void leg_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V, int planes, float plavor,
+               cudaStream_t st);
+void leg_forward(const Model& m, const float* f, float* s, int planes, const float* q, cudaStream_t st);
+void leg_uv2dv(const Model& m, const float* u, const float* v, const float* ke, float* D, float* Z, int planes,
+               cudaStream_t st);
+void leg_qtend(const Model& m, const float* u, const float* v, const float* src, float* out, int planes,
+               cudaStream_t st);
+
 // fft.cu
 void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st);
 void fft_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st);

@@ -42,9 +42,10 @@ __device__ __forceinline__ float sat_divided(const PlanetConst& K, float t, floa
   const float q = sat_capped(K, t, p);
   return q / (1.f - K.MOIST * q);
 }
-// x^y for x >= 0 with 0^y = 0, as Fortran's powf gives (precise.wgsl's
-// precise_pow semantics with CUDA's own powf).
-__device__ __forceinline__ float fpow(float x, float y) { return x == 0.f ? 0.f : powf(x, y); }
+// x^y for x >= 0 with 0^y = 0: precise_pow (src/model/shared/gpu/math/wgsl/
+// precise.wgsl:100-103) is exp(y * log(x)); here exp2(y * log2(x)) with
+// CUDA's own exp2f and log2f.
+__device__ __forceinline__ float fpow(float x, float y) { return x == 0.f ? 0.f : exp2f(y * log2f(x)); }
 // x^n by binary exponentiation, as libgcc's __powisf2 computes x**n.
 __device__ __forceinline__ float powi(float x, int n) {
   float base = x;
@@ -423,63 +424,68 @@ __device__ __forceinline__ float vapour_absorption(float wv, float zsolar2) {
   return 2.9f * wv / (fpow(1.f + 141.5f * wv, 0.635f) + 5.925f * wv) / zsolar2;
 }
 
-// swr (physics/radiation/wgsl/swr.wgsl): two-band shortwave by the adding
-// method. The bands (ozone below 0.75 um, water vapour above) are
-// independent until the fluxes are summed, so two neighbouring threads share
-// a column, one per band, and add their fluxes with a pair shuffle.
-template <int NL>
-__global__ void __launch_bounds__(kBlock) k_swr(Model m) {
-  const Dims& d = m.d;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int c = t >> 1;
-  const int band = t & 1;
-  if (c >= d.S * d.NHOR) return;  // both threads of a pair leave together
-  const int slot = c / d.NHOR;
-  const StepParams& P = m.params[slot];
-  if (!P.active) return;
-  const PlanetConst& K = m.pc[slot];
-  const float* tb = m.tabs + (size_t)slot * m.to.stride;
-  const size_t SN = (size_t)d.S * d.NHOR;
+// One band of swr (physics/radiation/wgsl/swr.wgsl) for one column: ozone
+// absorption below 0.75 um (BAND 0) or water vapour above (BAND 1), by the
+// adding method. The band's cloud optics, layer reflectances and
+// transmissivities follow the shader's expressions in its order; the flux
+// of each level goes to fu/fd as soon as the upward pass reaches it.
+// Returns the new surface albedos (nalb1, nalb2, albedo) the column writes.
+template <int NL, int BAND>
+__device__ __forceinline__ void swr_band(const Model& m, const PlanetConst& K, const float* tb, size_t SN, int c,
+                                         float mu0, float ftop, float* fu, float* fd, float* alb) {
   const FieldPtrs& F = m.f;
-  const unsigned pair = 3u << ((threadIdx.x & 31) & ~1);
-  const int NP = NL + 1;
-  const float ZERO = 1.0e-6f, ZBETTA = 1.66f, ZMBAR = 1.9f, ZFO3 = 100.f / 2.14f, ZMU00 = 0.5f,
-              INV_LN10 = 0.43429448190325176f;
+  const float ZBETTA = 1.66f, ZMBAR = 1.9f, ZFO3 = 100.f / 2.14f, ZMU00 = 0.5f, INV_LN10 = 0.43429448190325176f;
+  const float diffusivity = BAND == 0 ? ZMBAR : ZBETTA;
   const float* ds = tb + m.to.dsigma;
   const float* sg = tb + m.to.sigma;
-  const float mu0 = F.gmu0[c];
-  const float gdist2 = P.rad[3];
-  const float ftop1 = K.ZSOLAR1 * K.GSOL0 * gdist2 * mu0;
-  const float ftop2 = K.ZSOLAR2 * K.GSOL0 * gdist2 * mu0;
-  if (!(ftop1 + ftop2 > ZERO)) {
-    for (int l = band; l < NP; l += 2) {
-      F.dfu[l * SN + c] = 0.f;
-      F.dfd[l * SN + c] = 0.f;
-      F.dswfl[l * SN + c] = 0.f;
-    }
-    return;
-  }
-  const float ftop = band == 0 ? ftop1 : ftop2;
   const float dp = F.dp[c];
-  float cc_[NL];
-#pragma unroll
-  for (int l = 0; l < NL; ++l) cc_[l] = F.dcc[l * SN + c];
-  // Cloud optics: band 0 keeps (rcl1, rcl1s), band 1 (rcl2, rcl2s, tcl2, tcl2s).
-  float rcl[NL], rcls[NL], tcl[NL], tcls[NL];
-  float cs = 1.f;
+  const float zm = 35.f / sqrtf(1.f + 1224.f * mu0 * mu0);
+  auto amount_at = [&](int l) {
+    const float dsigma = ds[l];
+    return BAND == 0 ? ZFO3 * dsigma * dp * F.dqo3[l * SN + c] / K.GA
+                     : 0.1f * dsigma * F.dq[l * SN + c] * dp / K.GA * sqrtf(273.f / F.dt[l * SN + c]) * sg[l] * dp /
+                           100000.f;
+  };
+  auto absorption = [&](float x) {
+    return BAND == 0 ? ozone_absorption(x, K.ZSOLAR1) : vapour_absorption(x, K.ZSOLAR2);
+  };
+  // Column totals of the absorber path (slant above the first cloud,
+  // diffuse below).
+  float pt = 0.f, xpt = 0.f, cs = 1.f;
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
-    const float cc = cc_[l];
-    rcl[l] = rcls[l] = 0.f;
-    tcl[l] = tcls[l] = 1.f;
+    const float amount = amount_at(l);
+    pt = pt + amount;
+    xpt = cs * (xpt + zm * amount) + (1.f - cs) * (xpt + diffusivity * amount);
+    cs = cs * (1.f - F.dcc[l * SN + c]);
+  }
+  const float ccn = F.dcc[(NL - 1) * SN + c];
+  float rcsSurface = 0.f, rcsuSurface = 0.f;
+  if (BAND == 0) {
+    const float scf = K.RCOEFF * dp / 101100.f * 9.80665f / K.GA;
+    const float diffuseRayleigh = 1.f - expf(scf * K.LN_DIFFUSE_RAYLEIGH);
+    rcsuSurface = diffuseRayleigh * (1.f - ccn);
+    rcsSurface =
+        (1.f - expf(scf * logf(1.f - 0.219f / (1.f + 0.816f * mu0)))) * cs + diffuseRayleigh * (1.f - cs - ccn);
+  }
+  // Downward pass: layer properties and the adding recursion from the top.
+  float tl[NL + 1], rls[NL + 1], tbd[NL], tbu[NL], rb[NL], rbs[NL];
+  float ta = 1.f, tas = 1.f, ra = 0.f, ras = 0.f;
+  float tt = 1.f, ttu = 1.f - absorption(xpt + diffusivity * pt);
+  float pl = 0.f, xpl = 0.f;
+  cs = 1.f;
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const float cc = F.dcc[l * SN + c];
+    float rcl = 0.f, rcls = 0.f, tcl = 1.f, tcls = 1.f;
     if (cc > 0.f) {
       const float lwp = fminf(1000.f, 1000.f * F.dql[l * SN + c] * dp / K.GA * ds[l]);
       const float tau = 2.f * fpow(logf(lwp + 1.5f) * INV_LN10, 3.9f);
-      if (band == 0) {
-        rcls[l] = 1.f - 1.f / (1.f + K.ZB3 * tau);
+      if (BAND == 0) {
+        rcls = 1.f - 1.f / (1.f + K.ZB3 * tau);
         const float b1 = K.TSWR1 * sqrtf(mu0);
         const float direct1 = 1.f - 1.f / (1.f + b1 * tau / mu0);
-        rcl[l] = cs * direct1 + (1.f - cs) * rcls[l];
+        rcl = cs * direct1 + (1.f - cs) * rcls;
       } else {
         const float zlog = logf(1000.f / tau);
         float b2 = K.ZB4 / logf(3.f + 0.1f * tau);
@@ -489,8 +495,8 @@ __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
         float u = sqrtf(uz / un);
         float ex = expf(fminf(25.f, tau * sqrtf(uz * un) / ZMU00));
         float r = (u + 1.f) * (u + 1.f) * ex - (u - 1.f) * (u - 1.f) / ex;
-        tcls[l] = 4.f * u / r;
-        rcls[l] = (u * u - 1.f) / r * (ex - 1.f / ex);
+        tcls = 4.f * u / r;
+        rcls = (u * u - 1.f) / r * (ex - 1.f / ex);
         b2 = K.TSWR2 * sqrtf(mu0) / logf(3.f + 0.1f * tau);
         om0 = fminf(0.9999f, 1.f - K.TSWR3 * mu0 * mu0 * zlog);
         un = 1.f - om0;
@@ -500,66 +506,31 @@ __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
         r = (u + 1.f) * (u + 1.f) * ex - (u - 1.f) * (u - 1.f) / ex;
         const float directT = 4.f * u / r;
         const float direct2 = (u * u - 1.f) / r * (ex - 1.f / ex);
-        tcl[l] = cs * directT + (1.f - cs) * tcls[l];
-        rcl[l] = cs * direct2 + (1.f - cs) * rcls[l];
+        tcl = cs * directT + (1.f - cs) * tcls;
+        rcl = cs * direct2 + (1.f - cs) * rcls;
       }
     }
+    const float amount = amount_at(l);
+    pl = pl + amount;
+    xpl = cs * (xpl + zm * amount) + (1.f - cs) * (xpl + diffusivity * amount);
     cs = cs * (1.f - cc);
-  }
-  // Absorber paths: ozone (band 0) or water vapour (band 1), slant above the
-  // first cloud and diffuse below.
-  const float zm = 35.f / sqrtf(1.f + 1224.f * mu0 * mu0);
-  const float diffusivity = band == 0 ? ZMBAR : ZBETTA;
-  float pl[NL], xpl[NL];
-  float pt = 0.f, xpt = 0.f;
-  cs = 1.f;
-#pragma unroll
-  for (int l = 0; l < NL; ++l) {
-    const float dsigma = ds[l];
-    const float amount = band == 0 ? ZFO3 * dsigma * dp * F.dqo3[l * SN + c] / K.GA
-                                   : 0.1f * dsigma * F.dq[l * SN + c] * dp / K.GA * sqrtf(273.f / F.dt[l * SN + c]) *
-                                         sg[l] * dp / 100000.f;
-    pt = pt + amount;
-    xpt = cs * (xpt + zm * amount) + (1.f - cs) * (xpt + diffusivity * amount);
-    pl[l] = pt;
-    xpl[l] = xpt;
-    cs = cs * (1.f - cc_[l]);
-  }
-  auto absorption = [&](float x) {
-    return band == 0 ? ozone_absorption(x, K.ZSOLAR1) : vapour_absorption(x, K.ZSOLAR2);
-  };
-  float ta = 1.f, tas = 1.f, ra = 0.f, ras = 0.f;
-  float tt = 1.f, ttu = 1.f - absorption(xpt + diffusivity * pt);
-  const float ccn = cc_[NL - 1];
-  const float scf = K.RCOEFF * dp / 101100.f * 9.80665f / K.GA;
-  const float diffuseRayleigh = 1.f - expf(scf * K.LN_DIFFUSE_RAYLEIGH);
-  const float rcsuSurface = diffuseRayleigh * (1.f - ccn);
-  const float rcsSurface =
-      (1.f - expf(scf * logf(1.f - 0.219f / (1.f + 0.816f * mu0)))) * cs + diffuseRayleigh * (1.f - cs - ccn);
-  float tl[NL + 1], rls[NL + 1];
-  float tbd[NL], tbu[NL], rb[NL], rbs[NL];
-#pragma unroll
-  for (int l = 0; l < NL; ++l) {
-    const float cc = cc_[l];
     tl[l] = ta;
     rls[l] = ras;
     const bool surface = l == NL - 1;
-    float x = xpl[l];
-    const float tr = (1.f - absorption(x)) / tt;
+    const float tr = (1.f - absorption(xpl)) / tt;
     tt = tt * tr;
-    x = xpt + diffusivity * (pt - pl[l]);
-    const float tru = ttu / (1.f - absorption(x));
+    const float tru = ttu / (1.f - absorption(xpt + diffusivity * (pt - pl)));
     ttu = ttu / tru;
-    if (band == 0) {
-      rb[l] = (surface ? rcsSurface : 0.f) + rcl[l] * cc;
-      rbs[l] = (surface ? rcsuSurface : 0.f) + rcls[l] * cc;
+    if (BAND == 0) {
+      rb[l] = (surface ? rcsSurface : 0.f) + rcl * cc;
+      rbs[l] = (surface ? rcsuSurface : 0.f) + rcls * cc;
       tbd[l] = 1.f - (1.f - tr) * (1.f - cc) - rb[l];
       tbu[l] = 1.f - (1.f - tru) * (1.f - cc) - rbs[l];
     } else {
-      rb[l] = rcl[l] * cc;
-      rbs[l] = rcls[l] * cc;
-      tbd[l] = 1.f - (1.f - tr) * (1.f - cc) - (1.f - tcl[l]) * cc;
-      tbu[l] = 1.f - (1.f - tru) * (1.f - cc) - (1.f - tcls[l]) * cc;
+      rb[l] = rcl * cc;
+      rbs[l] = rcls * cc;
+      tbd[l] = 1.f - (1.f - tr) * (1.f - cc) - (1.f - tcl) * cc;
+      tbu[l] = 1.f - (1.f - tru) * (1.f - cc) - (1.f - tcls) * cc;
     }
     const float mm = 1.f / (1.f - ras * rbs[l]);
     ra = ra + ta * rb[l] * tas * mm;
@@ -570,49 +541,92 @@ __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
   tl[NL] = ta;
   rls[NL] = ras;
   // Surface albedo: land and sea ice keep theirs, open water gets a
-  // zenith-angle dependent one (band 0 writes the updated fields).
+  // zenith-angle dependent one.
   const bool star = K.NSTARTEMP != 0.f;
   const float dalb = F.dalb[c], salb1 = F.dsalb[c], salb2 = F.dsalb[SN + c];
-  const float salb = band == 0 ? salb1 : salb2;
-  ras = star ? salb : dalb;
   const float dls = F.dls[c], dicec = F.dicec[c];
   const float water = (1.f - dls) * (1.f - dicec) * fminf(0.05f / (mu0 + 0.15f), 0.15f);
   const float nalb1 = dls * salb1 + (1.f - dls) * dicec * salb1 + water;
   const float nalb2 = dls * salb2 + (1.f - dls) * dicec * salb2 + water;
   const float albedo = star ? K.ZSOLARS1 * nalb1 + K.ZSOLARS2 * nalb2 : dls * dalb + (1.f - dls) * dicec * dalb + water;
-  __syncwarp(pair);  // both bands have read dalb and dsalb
-  if (band == 0) {
-    F.dsalb[c] = nalb1;
-    F.dsalb[SN + c] = nalb2;
-    F.dalb[c] = albedo;
-  }
-  ra = star ? (band == 0 ? nalb1 : nalb2) : albedo;
-  float rl[NL + 1], rlsu[NL + 1];
+  alb[0] = nalb1;
+  alb[1] = nalb2;
+  alb[2] = albedo;
+  ras = star ? (BAND == 0 ? salb1 : salb2) : dalb;
+  ra = star ? (BAND == 0 ? nalb1 : nalb2) : albedo;
+  // Upward pass from the surface; level l + 1's flux is complete once its
+  // reflectances (ra, ras) are.
 #pragma unroll
-  for (int l = NL - 1; l >= 0; --l) {
-    rl[l + 1] = ra;
-    rlsu[l + 1] = ras;
+  for (int l = NL - 1; l >= -1; --l) {
+    const int k = l + 1;
+    const float mm = 1.f / (1.f - rls[k] * ras);
+    fu[k] = -tl[k] * ra * mm * ftop;
+    fd[k] = tl[k] * mm * ftop;
+    if (l < 0) break;
     const float dd = 1.f - ras * rbs[l];
     ra = rb[l] + tbd[l] * ra * tbu[l] / dd;
     ras = rbs[l] + tbu[l] * ras * tbu[l] / dd;
   }
-  rl[0] = ra;
-  rlsu[0] = ras;
+}
+
+// swr: the two bands are independent until their fluxes are summed, so the
+// block's warps pair up on the same 32 columns, one band each (no branch
+// diverges inside a warp), and add their fluxes through shared memory in the
+// shader's order (band 1 + band 2).
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_swr(Model m) {
+  constexpr int NP = NL + 1;
+  constexpr int kCols = kBlock / 2;
+  __shared__ float sfu[2][NP][kCols], sfd[2][NP][kCols];
+  const Dims& d = m.d;
+  const int warp = threadIdx.x >> 5;
+  const int band = warp & 1;
+  const int lc = (warp >> 1) * 32 + (threadIdx.x & 31);
+  const int c = blockIdx.x * kCols + lc;
+  const bool inside = c < d.S * d.NHOR;
+  const int slot = inside ? c / d.NHOR : 0;
+  const bool run = inside && m.params[slot].active;
+  const PlanetConst& K = m.pc[slot];
+  const float* tb = m.tabs + (size_t)slot * m.to.stride;
+  const size_t SN = (size_t)d.S * d.NHOR;
+  const FieldPtrs& F = m.f;
+  bool lit = false;
+  float alb[3];
+  if (run) {
+    const float mu0 = F.gmu0[c];
+    const float gdist2 = m.params[slot].rad[3];
+    const float ftop1 = K.ZSOLAR1 * K.GSOL0 * gdist2 * mu0;
+    const float ftop2 = K.ZSOLAR2 * K.GSOL0 * gdist2 * mu0;
+    lit = ftop1 + ftop2 > 1.0e-6f;
+    if (lit) {
+      float fu[NP], fd[NP];
+      if (band == 0)
+        swr_band<NL, 0>(m, K, tb, SN, c, mu0, ftop1, fu, fd, alb);
+      else
+        swr_band<NL, 1>(m, K, tb, SN, c, mu0, ftop2, fu, fd, alb);
 #pragma unroll
-  for (int l = 0; l < NP; ++l) {
-    const float mm = 1.f / (1.f - rls[l] * rlsu[l]);
-    const float fu = -tl[l] * rl[l] * mm * ftop;
-    const float fd = tl[l] * mm * ftop;
-    const float fu2 = __shfl_xor_sync(pair, fu, 1);
-    const float fd2 = __shfl_xor_sync(pair, fd, 1);
-    // band 1 + band 2, in the reference's order
-    const float fut = band == 0 ? fu + fu2 : fu2 + fu;
-    const float fdt = band == 0 ? fd + fd2 : fd2 + fd;
-    if ((l & 1) == band) {
-      F.dfu[l * SN + c] = fut;
-      F.dfd[l * SN + c] = fdt;
-      F.dswfl[l * SN + c] = fut + fdt;
+      for (int l = 0; l < NP; ++l) {
+        sfu[band][l][lc] = fu[l];
+        sfd[band][l][lc] = fd[l];
+      }
     }
+  }
+  __syncthreads();  // both bands' fluxes are in, and both have read dalb, dsalb
+  if (!run) return;
+  if (lit && band == 0) {
+    F.dsalb[c] = alb[0];
+    F.dsalb[SN + c] = alb[1];
+    F.dalb[c] = alb[2];
+  }
+  for (int l = band; l < NP; l += 2) {
+    float fut = 0.f, fdt = 0.f;
+    if (lit) {
+      fut = sfu[0][l][lc] + sfu[1][l][lc];
+      fdt = sfd[0][l][lc] + sfd[1][l][lc];
+    }
+    F.dfu[l * SN + c] = fut;
+    F.dfd[l * SN + c] = fdt;
+    F.dswfl[l * SN + c] = fut + fdt;
   }
 }
 
@@ -664,8 +678,10 @@ __global__ void __launch_bounds__(kBlock) k_lwr_radstep(Model m) {
 #pragma unroll
   for (int l = 0; l < NP; ++l) dftu[l] = dftd[l] = 0.f;
   float taucs[NL], tau[NL], tausf[NL];
+#pragma unroll
   for (int j = 0; j < NL; ++j) {
     float taucc = 1.f, sumwv = 0.f, sumo3 = 0.f, sumco2 = 0.f;
+#pragma unroll
     for (int k = j; k < NL; ++k) {
       sumwv = sumwv + q[k];
       sumo3 = sumo3 + qo3[k];
@@ -686,6 +702,7 @@ __global__ void __launch_bounds__(kBlock) k_lwr_radstep(Model m) {
     }
     if (j == 0) {
       float tau0 = 1.f - ZERO;
+#pragma unroll
       for (int k = 0; k < NL; ++k) {
         tau0 = taucs[k] / tau0 * taucc0[k] * K.TPOFMT;
         tau0 = fminf(1.f - ZERO, fmaxf(ZERO, tau0));
@@ -702,6 +719,7 @@ __global__ void __launch_bounds__(kBlock) k_lwr_radstep(Model m) {
     dftu[j] = dftu[j] - bu[j + 1];
     dftd[j] = dftd[j] + bd[j];
     const float bdl = bd[j] - bd[j + 1];
+#pragma unroll
     for (int k = j; k < NL; ++k) {
       dftu[j] = dftu[j] - (bu[k + 2] - bu[k + 1]) * tau[k];
       dftd[k + 1] = dftd[k + 1] + bdl * tau[k];
@@ -822,6 +840,7 @@ __global__ void __launch_bounds__(kBlock) k_kuo(Model m) {
       }
     }
   }
+#pragma unroll
   for (int l = NM - 1; l >= 0; --l) {
     const int lp = l + 1;
     if (ilift == -1 && zdqtot[lp] > 0.f) {
@@ -868,6 +887,7 @@ __global__ void __launch_bounds__(kBlock) k_kuo(Model m) {
       }
     }
   }
+#pragma unroll
   for (int l = NM - 1; l >= 0; --l) {
     if (itop == l + 2) {
       const float p = dp * sg[l];
@@ -1965,7 +1985,7 @@ COLUMN_LAUNCHER(SolangMko3, k_solang_mko3)
 template <int NL>
 struct Swr {
   static void run(const Model& m, cudaStream_t st) {
-    k_swr<NL><<<nblocks(2 * (size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);
+    k_swr<NL><<<nblocks((size_t)m.d.S * m.d.NHOR, kBlock / 2), kBlock, 0, st>>>(m);
   }
 };
 COLUMN_LAUNCHER(LwrRadstep, k_lwr_radstep)
