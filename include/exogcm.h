@@ -173,10 +173,12 @@ int exogcm_last_step_ms(exogcm_engine* engine, float* ms);
 /* Launches one of the step's kernels `reps` times on the current state of
  * every slot and returns its mean device time per launch in *ms (CUDA events
  * on the engine's stream), with the algorithmic bytes one launch moves in
- * *bytes. Kernels: "dft_forward", "dft_inverse", "legendre_forward",
- * "legendre_inverse", "dv2uv", "uv2dv", "qtend", "calcgp", "spectrala",
- * "vdiff", "swr", "lwr_radstep", "kuo", "rain_column". The launches change
- * the state; use it for measurement only. */
+ * *bytes. Kernels: "fourier_forward", "fourier_inverse" (FFTs on the
+ * optimized path, DFTs on the plain one), "legendre_forward",
+ * "legendre_inverse", "dv2uv", "uv2dv", "qtend", "calcgp", "spectrala", and
+ * the single column kernels "vdiff", "swr", "lwr_radstep", "kuo",
+ * "rain_column". The launches change the state; use it for measurement
+ * only. */
 int exogcm_time_kernel(exogcm_engine* engine, const char* kernel, int reps, float* ms, double* bytes);
 
 /* Kernel launches in the CUDA graph of a `steps`-step batch. */

@@ -24,7 +24,6 @@
 
 namespace exogcm {
 
-constexpr int MAXL = 16;   // largest level count a kernel's register arrays hold
 constexpr int NLSOIL = 5;  // landmod's soil layers
 constexpr int MONTHS = 14; // climatology months with December before and January after
 

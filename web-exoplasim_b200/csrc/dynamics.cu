@@ -22,6 +22,7 @@ __device__ __forceinline__ const float* slot_tabs(const Model& m, int slot) {
 }
 
 // gridpointa from gp = exp(gp) to the flux products (dynamics/wgsl/calcgp.wgsl).
+template <int NL>
 __global__ void __launch_bounds__(kBlock) k_calcgp(Model m) {
   const Dims& d = m.d;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -38,14 +39,14 @@ __global__ void __launch_bounds__(kBlock) k_calcgp(Model m) {
   const float* tkpT = tb + m.to.tkp;
   const float* C = tb + m.to.c;
   const float* G = tb + m.to.g;
-  const int NL = d.NLEV;
   const size_t SN = (size_t)d.S * d.NHOR;
   const FieldPtrs& F = m.f;
   const float rcsq = m.sh.rcsq[c % d.NHOR];
   const float ps = expf(F.gp[c]);
   F.gp[c] = ps;
   const float gpm = F.gpmt[c], gpj = F.gpj[c];
-  float gu[MAXL], gv[MAXL], gt[MAXL], gd[MAXL], gz[MAXL], gq[MAXL], zvgpg[MAXL], ztv1[MAXL], ztv2[MAXL];
+  float gu[NL], gv[NL], gt[NL], gd[NL], gz[NL], gq[NL], zvgpg[NL], ztv1[NL], ztv2[NL];
+#pragma unroll
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SN + c;
     gu[l] = F.gu[at];
@@ -61,10 +62,11 @@ __global__ void __launch_bounds__(kBlock) k_calcgp(Model m) {
     ztv1[l] = tvirt - t0;
     ztv2[l] = tvirt / (1.f + K.ADV * zq) - t0;
   }
-  float zsdotp[MAXL];
+  float zsdotp[NL];
   float zsumd = ds[0] * gd[0];
   float gvp = ds[0] * zvgpg[0];
   zsdotp[0] = zsumd + gvp;
+#pragma unroll
   for (int l = 1; l < NL - 1; ++l) {
     zsumd = zsumd + ds[l] * gd[l];
     gvp = gvp + ds[l] * zvgpg[l];
@@ -72,7 +74,8 @@ __global__ void __launch_bounds__(kBlock) k_calcgp(Model m) {
   }
   zsumd = zsumd + ds[NL - 1] * gd[NL - 1];
   gvp = gvp + ds[NL - 1] * zvgpg[NL - 1];
-  float gtd[MAXL], gqm[MAXL], gud[MAXL], gvd[MAXL];
+  float gtd[NL], gqm[NL], gud[NL], gvd[NL];
+#pragma unroll
   for (int l = 0; l < NL - 1; ++l) {
     zsdotp[l] = sh[l] * (zsumd + gvp) - zsdotp[l];
     gtd[l] = zsdotp[l] * (gt[l + 1] - gt[l]);
@@ -80,52 +83,52 @@ __global__ void __launch_bounds__(kBlock) k_calcgp(Model m) {
     gud[l] = zsdotp[l] * (gu[l + 1] - gu[l]);
     gvd[l] = zsdotp[l] * (gv[l + 1] - gv[l]);
   }
-  float gtn[MAXL], gqn[MAXL], guz[MAXL], gvz[MAXL], dw[MAXL];
+  // Level tendencies go out as soon as they are formed (fewer live arrays).
   zsumd = zvgpg[0] * ds[0];
   const float rdsig0 = rd[0];
-  gtn[0] = gt[0] * gd[0] - K.AKAP * ztv2[0] * gd[0] - rdsig0 * (gtd[0] + t01[0] * (sh[0] * gvp - zsumd));
-  gqn[0] = -rdsig0 * gqm[0];
-  guz[0] = -gu[0] * gz[0] - gpj * ztv1[0] - rdsig0 * gvd[0];
-  gvz[0] = gv[0] * gz[0] - gpm * ztv1[0] - rdsig0 * gud[0];
-  dw[0] = gd[0] * ps * K.PSURF * K.WW;
+  F.gtn[c] = gt[0] * gd[0] - K.AKAP * ztv2[0] * gd[0] - rdsig0 * (gtd[0] + t01[0] * (sh[0] * gvp - zsumd));
+  F.gqn[c] = -rdsig0 * gqm[0];
+  F.guz[c] = -gu[0] * gz[0] - gpj * ztv1[0] - rdsig0 * gvd[0];
+  F.gvz[c] = gv[0] * gz[0] - gpm * ztv1[0] - rdsig0 * gud[0];
+  F.dw[c] = gd[0] * ps * K.PSURF * K.WW;
+#pragma unroll
   for (int l = 1; l < NL; ++l) {
     const int column = l * NL;
     float ztpta = C[column] * zvgpg[0];
     float ztptb = C[column] * (zvgpg[0] + gd[0]);
+#pragma unroll
     for (int j = 1; j <= l; ++j) {
       ztpta = ztpta + C[column + j] * zvgpg[j];
       ztptb = ztptb + C[column + j] * (zvgpg[j] + gd[j]);
     }
     const float rdsig = rd[l], t01s2 = t01[l], t01s2m = t01[l - 1], sigmah = sh[l], sigmahm = sh[l - 1];
     const float tkp = tkpT[l];
+    const size_t at = l * SN + c;
     if (l < NL - 1) {
       zsumd = zsumd + zvgpg[l] * ds[l];
-      gtn[l] = gt[l] * gd[l] + K.AKAP * ztv2[l] * (zvgpg[l] - ztptb) + tkp * (zvgpg[l] - ztpta) -
+      F.gtn[at] = gt[l] * gd[l] + K.AKAP * ztv2[l] * (zvgpg[l] - ztptb) + tkp * (zvgpg[l] - ztpta) -
                rdsig * (gtd[l] + gtd[l - 1] + gvp * (t01s2 * sigmah + t01s2m * sigmahm) - zsumd * (t01s2m + t01s2) +
                         zvgpg[l] * ds[l] * t01s2m);
-      gqn[l] = -rdsig * (gqm[l] - gqm[l - 1]);
-      guz[l] = -gu[l] * gz[l] - gpj * ztv1[l] - rdsig * (gvd[l] + gvd[l - 1]);
-      gvz[l] = gv[l] * gz[l] - gpm * ztv1[l] - rdsig * (gud[l] + gud[l - 1]);
+      F.gqn[at] = -rdsig * (gqm[l] - gqm[l - 1]);
+      F.guz[at] = -gu[l] * gz[l] - gpj * ztv1[l] - rdsig * (gvd[l] + gvd[l - 1]);
+      F.gvz[at] = gv[l] * gz[l] - gpm * ztv1[l] - rdsig * (gud[l] + gud[l - 1]);
     } else {
-      gtn[l] = gt[l] * gd[l] + K.AKAP * ztv2[l] * (zvgpg[l] - ztptb) + tkp * (zvgpg[l] - ztpta) -
+      F.gtn[at] = gt[l] * gd[l] + K.AKAP * ztv2[l] * (zvgpg[l] - ztptb) + tkp * (zvgpg[l] - ztpta) -
                rdsig * (gtd[NL - 2] + t01s2m * (sigmahm * gvp - zsumd));
-      gqn[l] = rdsig * gqm[NL - 2];
-      guz[l] = -gu[l] * gz[l] - gpj * ztv1[l] - rdsig * gvd[NL - 2];
-      gvz[l] = gv[l] * gz[l] - gpm * ztv1[l] - rdsig * gud[NL - 2];
+      F.gqn[at] = rdsig * gqm[NL - 2];
+      F.guz[at] = -gu[l] * gz[l] - gpj * ztv1[l] - rdsig * gvd[NL - 2];
+      F.gvz[at] = gv[l] * gz[l] - gpm * ztv1[l] - rdsig * gud[NL - 2];
     }
-    dw[l] = (zvgpg[l] - ztptb) * ps * K.PSURF * K.WW;
+    F.dw[at] = (zvgpg[l] - ztptb) * ps * K.PSURF * K.WW;
   }
   const float scale = sqrtf(rcsq);
+#pragma unroll
   for (int l = 0; l < NL; ++l) {
     float gsum = 0.f;
+#pragma unroll
     for (int k = 0; k < NL; ++k) gsum = gsum + G[l * NL + k] * (ztv1[k] - gt[k]);
     const float gphi = gsum * 2.f / rcsq;
     const size_t at = l * SN + c;
-    F.gtn[at] = gtn[l];
-    F.gqn[at] = gqn[l];
-    F.guz[at] = guz[l];
-    F.gvz[at] = gvz[l];
-    F.dw[at] = dw[l];
     F.gut[at] = gu[l] * gt[l];
     F.gvt[at] = gv[l] * gt[l];
     F.gke[at] = gu[l] * gu[l] + gv[l] * gv[l] + gphi;
@@ -140,6 +143,7 @@ __global__ void __launch_bounds__(kBlock) k_calcgp(Model m) {
 
 // spectrala for one real spectral coefficient (dynamics/wgsl/spectrala.wgsl):
 // the Hoskins-Simmons semi-implicit scheme with this slot's bm1 for its phase.
+template <int NL>
 __global__ void __launch_bounds__(kBlock) k_spectrala(Model m) {
   const Dims& d = m.d;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -153,14 +157,14 @@ __global__ void __launch_bounds__(kBlock) k_spectrala(Model m) {
   const float* t0T = tb + m.to.t0;
   const float* ds = tb + m.to.dsigma;
   const float* tau = tb + m.to.tau;
-  const int NL = d.NLEV;
   const float* bm1 = tb + m.to.bm1 + (size_t)P.phase * d.T * NL * NL;
   const size_t SR = (size_t)d.S * d.NRSP;
   const FieldPtrs& F = m.f;
   const bool filter = P.filter != 0.f;
   const float DELT = P.delt, DELT2 = P.delt2;
   const float apm = F.spm[c];
-  float adm[MAXL], azm[MAXL], atm[MAXL], aqm[MAXL], adt[MAXL], stt[MAXL];
+  float adm[NL], azm[NL], atm[NL], aqm[NL], adt[NL], stt[NL];
+#pragma unroll
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SR + c;
     adm[l] = F.sdm[at];
@@ -170,9 +174,11 @@ __global__ void __launch_bounds__(kBlock) k_spectrala(Model m) {
     adt[l] = F.sdt[at];
     stt[l] = F.stt[at];
   }
-  float zgt[MAXL], zgm[MAXL];
+  float zgt[NL], zgm[NL];
+#pragma unroll
   for (int l = 0; l < NL; ++l) {
     float gt = 0.f, gm = 0.f;
+#pragma unroll
     for (int k = 0; k < NL; ++k) {
       gt = gt + G[l * NL + k] * stt[k];
       gm = gm + G[l * NL + k] * atm[k];
@@ -184,11 +190,13 @@ __global__ void __launch_bounds__(kBlock) k_spectrala(Model m) {
   const float spm = apm;
   const float sop = tb[m.to.sop + s];
   const int jn = (int)m.sh.nindex[s];
-  float sdt[MAXL];
+  float sdt[NL];
+#pragma unroll
   for (int l = 0; l < NL; ++l) {
     float zsum = 0.f;
     if (jn > 0) {
       const float zq = 1.f / (float)(jn * (jn + 1));
+#pragma unroll
       for (int l2 = 0; l2 < NL; ++l2) {
         const float z0 = t0T[l2];
         const float zt = zgt[l2] - z0 * spt;
@@ -201,9 +209,12 @@ __global__ void __launch_bounds__(kBlock) k_spectrala(Model m) {
     }
     sdt[l] = s < 2 ? 0.f : zsum;
   }
+#pragma unroll
   for (int l = 0; l < NL; ++l) spt = spt + ds[l] * sdt[l];
+#pragma unroll
   for (int l = 0; l < NL; ++l) {
     float t = 0.f;
+#pragma unroll
     for (int k = 0; k < NL; ++k) t = t + tau[l * NL + k] * sdt[k];
     stt[l] = stt[l] - t;
   }
@@ -213,6 +224,7 @@ __global__ void __launch_bounds__(kBlock) k_spectrala(Model m) {
   F.spp[c] = sppNew;
   F.sp[c] = sppNew;
   F.spt[c] = spt;
+#pragma unroll
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SR + c;
     if (filter) {
@@ -425,10 +437,18 @@ inline unsigned blocks(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
 }  // namespace
 
 void dyn_calcgp(const Model& m, cudaStream_t st) {
-  k_calcgp<<<blocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);
+  const unsigned n = blocks((size_t)m.d.S * m.d.NHOR, kBlock);
+  if (m.d.L == 10)
+    k_calcgp<10><<<n, kBlock, 0, st>>>(m);
+  else
+    k_calcgp<5><<<n, kBlock, 0, st>>>(m);
 }
 void dyn_spectrala(const Model& m, cudaStream_t st) {
-  k_spectrala<<<blocks((size_t)m.d.S * m.d.NRSP, kBlock), kBlock, 0, st>>>(m);
+  const unsigned n = blocks((size_t)m.d.S * m.d.NRSP, kBlock);
+  if (m.d.L == 10)
+    k_spectrala<10><<<n, kBlock, 0, st>>>(m);
+  else
+    k_spectrala<5><<<n, kBlock, 0, st>>>(m);
 }
 void dyn_spectrald_diffusion(const Model& m, cudaStream_t st) {
   k_spectrald_diffusion<<<blocks((size_t)m.d.S * m.d.NRSP, kBlock), kBlock, 0, st>>>(m);

@@ -186,17 +186,53 @@ void check_slot(exogcm_engine* e, int slot) {
 }
 
 // Copies between a host array [count][plane] and one slot's planes.
+// The optimized path keeps Fourier planes m-major, [m][lat] (re, im) pairs,
+// where the reference (and the plain path) keeps them [lat][m]. Host copies
+// always see the reference's layout.
+void fourier_to_m_major(const Dims& d, const float* src, float* dst, int planes) {
+  for (int p = 0; p < planes; ++p) {
+    const float* a = src + (size_t)p * d.NLAT * d.NFC;
+    float* b = dst + (size_t)p * d.NLAT * d.NFC;
+    for (int lat = 0; lat < d.NLAT; ++lat)
+      for (int m = 0; m < d.NTP1; ++m) {
+        b[2 * ((size_t)m * d.NLAT + lat)] = a[(size_t)lat * d.NFC + 2 * m];
+        b[2 * ((size_t)m * d.NLAT + lat) + 1] = a[(size_t)lat * d.NFC + 2 * m + 1];
+      }
+  }
+}
+
+void fourier_from_m_major(const Dims& d, const float* src, float* dst, int planes) {
+  for (int p = 0; p < planes; ++p) {
+    const float* b = src + (size_t)p * d.NLAT * d.NFC;
+    float* a = dst + (size_t)p * d.NLAT * d.NFC;
+    for (int lat = 0; lat < d.NLAT; ++lat)
+      for (int m = 0; m < d.NTP1; ++m) {
+        a[(size_t)lat * d.NFC + 2 * m] = b[2 * ((size_t)m * d.NLAT + lat)];
+        a[(size_t)lat * d.NFC + 2 * m + 1] = b[2 * ((size_t)m * d.NLAT + lat) + 1];
+      }
+  }
+}
+
 void copy_field(exogcm_engine* e, const FieldInfo& fi, int slot, void* host, bool to_device) {
   float* base = e->arena + fi.offset + (size_t)slot * fi.plane;
   const size_t pitch = fi.plane * e->d.S * sizeof(float);
   const size_t width = fi.plane * sizeof(float);
+  const bool m_major = e->mode == 1 && fi.shape == 'F';
+  std::vector<float> staged;
+  void* h = host;
+  if (m_major) {
+    staged.resize(fi.plane * fi.count);
+    if (to_device) fourier_to_m_major(e->d, static_cast<const float*>(host), staged.data(), fi.count);
+    h = staged.data();
+  }
   if (to_device)
-    check(cudaMemcpy2DAsync(base, pitch, host, width, width, fi.count, cudaMemcpyHostToDevice, e->stream),
+    check(cudaMemcpy2DAsync(base, pitch, h, width, width, fi.count, cudaMemcpyHostToDevice, e->stream),
           "write field");
   else
-    check(cudaMemcpy2DAsync(host, width, base, pitch, width, fi.count, cudaMemcpyDeviceToHost, e->stream),
+    check(cudaMemcpy2DAsync(h, width, base, pitch, width, fi.count, cudaMemcpyDeviceToHost, e->stream),
           "read field");
   check(cudaStreamSynchronize(e->stream), "field copy");
+  if (m_major && !to_device) fourier_from_m_major(e->d, staged.data(), static_cast<float*>(host), fi.count);
 }
 
 void upload_shared(exogcm_engine* e, const SharedSetup& s) {
@@ -948,10 +984,11 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
     const std::string k(kernel);
     std::function<void()> launch;
     double b = 0;
-    if (k == "dft_forward") {
+    const double L = d.L;
+    if (k == "fourier_forward") {
       launch = [&] { tr_fourier_forward(m, F.gtn, F.fgtn, LP, e->stream); };
       b = LP * (grid + four);
-    } else if (k == "dft_inverse") {
+    } else if (k == "fourier_inverse") {
       launch = [&] { tr_fourier_inverse(m, F.fgu, F.gu, LP, e->stream); };
       b = LP * (four + grid);
     } else if (k == "legendre_forward") {
@@ -975,17 +1012,21 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
     } else if (k == "spectrala") {
       launch = [&] { dyn_spectrala(m, e->stream); };
       b = (double)S * d.NRSP * 4 * (6.0 * d.L + 3 + 14.0 * d.L + 3);
-    } else if (k == "vdiff") {
-      launch = [&] { phy_surface_flux(m, e->stream); };
-      b = cols * 4 * (8.0 * d.L + 4 * d.L);
-    } else if (k == "swr" || k == "lwr_radstep") {
-      launch = [&] { phy_radiation(m, e->stream); };
-      b = cols * 4 * (10.0 * d.L + 9.0 * (d.L + 1));
-    } else if (k == "kuo" || k == "rain_column") {
-      launch = [&] { phy_precipitation_columns(m, e->stream); };
-      b = cols * 4 * (12.0 * d.L + 10.0 * d.L);
     } else {
-      throw Error(EXOGCM_EINVAL, "unknown kernel " + k);
+      // Column kernels: compulsory reads + writes per column, in floats.
+      const std::map<std::string, double> per_column = {
+          {"vdiff", 12 * L},                                 // t, q, u, v and tendencies in; 4 tendencies out
+          {"swr", 5 * L + 7 + 3 * (L + 1) + 3},              // dcc, dql, dq, dt, dqo3 + surface in; 3 fluxes + albedos out
+          {"lwr_radstep", 7 * L + 4 + 4 * (L + 1) + 4 * L},  // t, q, o3, co2, clouds, sw flux, dtdt in; 4 fluxes + 4 rates out
+          {"kuo", 5 * L + 3 + 6 * L + 1},                    // dqt, q, t and tendencies in; tendencies, rain, cloud levels out
+          {"rain_column", 12 * L + 4 + 6 * L + 8},
+      };
+      auto it = per_column.find(k);
+      if (it == per_column.end()) throw Error(EXOGCM_EINVAL, "unknown kernel " + k);
+      launch = [&] {
+        if (!phy_launch_one(m, k, e->stream)) throw Error(EXOGCM_EINVAL, "unknown kernel " + k);
+      };
+      b = cols * 4 * it->second;
     }
     launch();  // warm
     check(cudaEventRecord(e->ev0, e->stream), "event");

@@ -10,7 +10,13 @@
 // a 32-point decimation-in-frequency FFT across the lanes (five xor-shuffle
 // butterfly stages). Twiddles come from a table of e^{2 pi i j / N} built in
 // FP64 on the host and rounded once. Shared memory reorders the bit-reversed
-// FFT output and stages each warp's spectrum.
+// FFT output.
+//
+// The optimized path stores Fourier planes m-major (coefficient (m, lat) at
+// 2 * (m * NLAT + lat)), so that the Legendre transforms on either side
+// stream whole runs of latitudes. One block transforms one plane: the
+// plane's coefficients pass through shared memory ([m][lat], padded) between
+// that layout and the warps' rows, and both global sides stay contiguous.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -39,140 +45,202 @@ __device__ __forceinline__ float2 twiddle(const float2* tw, int t, int N) {
 
 __device__ __forceinline__ int bitrev5(int x) { return __brev(x) >> 27; }
 
-// In-register M-point FFT of the R values x[r] = z[lane + 32 r]; on return
-// x[k2] holds Z[R * bitrev5(lane) + k2].
-template <int R, int SIGN>
-__device__ __forceinline__ void warp_fft(float2 (&x)[R], const float2* tw, int N, int lane) {
-  const int M = 32 * R;
+// In-register M-point FFTs of B rows at once (independent instruction
+// streams for the shuffle chains): x[b][r] = z_b[lane + 32 r]; on return
+// x[b][k2] holds Z_b[R * bitrev5(lane) + k2].
+template <int B, int R, int SIGN>
+__device__ __forceinline__ void warp_fft(float2 (&x)[B][R], const float2* tw, int N, int lane) {
   // radix-R step per lane, then the twiddle w_M^{n1 k2}
   if (R == 2) {
-    const float2 a = x[0], b = x[1];
-    x[0] = cadd(a, b);
-    x[1] = cmul(csub(a, b), twiddle<SIGN>(tw, 2 * lane, N));
+    const float2 w = twiddle<SIGN>(tw, 2 * lane, N);
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      const float2 p = x[b][0], q = x[b][1];
+      x[b][0] = cadd(p, q);
+      x[b][1] = cmul(csub(p, q), w);
+    }
   } else if (R == 3) {
-    const float2 a = x[0], b = x[1], c = x[2];
     const float2 w3 = twiddle<SIGN>(tw, N / 3, N);      // e^{sign 2 pi i / 3}
     const float2 w32 = twiddle<SIGN>(tw, 2 * N / 3, N); // e^{sign 4 pi i / 3}
-    x[0] = cadd(cadd(a, b), c);
-    x[1] = cmul(cadd(cadd(a, cmul(b, w3)), cmul(c, w32)), twiddle<SIGN>(tw, 2 * lane, N));
-    x[2] = cmul(cadd(cadd(a, cmul(b, w32)), cmul(c, w3)), twiddle<SIGN>(tw, 4 * lane, N));
+    const float2 t1 = twiddle<SIGN>(tw, 2 * lane, N), t2 = twiddle<SIGN>(tw, 4 * lane, N);
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      const float2 p = x[b][0], q = x[b][1], u = x[b][2];
+      x[b][0] = cadd(cadd(p, q), u);
+      x[b][1] = cmul(cadd(cadd(p, cmul(q, w3)), cmul(u, w32)), t1);
+      x[b][2] = cmul(cadd(cadd(p, cmul(q, w32)), cmul(u, w3)), t2);
+    }
   }
-  (void)M;
   // 32-point DIF across lanes for each of the R sub-sequences
 #pragma unroll
   for (int half = 16; half >= 1; half >>= 1) {
     const bool upper = (lane & half) != 0;
     const float2 w = twiddle<SIGN>(tw, (lane & (half - 1)) * (N / (2 * half)), N);
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      float2 y;
-      y.x = __shfl_xor_sync(0xffffffffu, x[r].x, half);
-      y.y = __shfl_xor_sync(0xffffffffu, x[r].y, half);
-      x[r] = upper ? cmul(csub(y, x[r]), w) : cadd(x[r], y);
-    }
+    for (int b = 0; b < B; ++b)
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        float2 y;
+        y.x = __shfl_xor_sync(0xffffffffu, x[b][r].x, half);
+        y.y = __shfl_xor_sync(0xffffffffu, x[b][r].y, half);
+        x[b][r] = upper ? cmul(csub(y, x[b][r]), w) : cadd(x[b][r], y);
+      }
   }
 }
 
-// gp2fc: rows of N grid values -> rows of NTP1 (re, im) coefficients.
+constexpr int kRowsPerWarp = 2;
+
+// Shared memory of a plane block: twiddles, the plane's coefficients
+// [ntp1][nlat + 1] and per-warp row buffers [kWarps][kRowsPerWarp][M + 1].
+inline size_t plane_smem(int nlon, int nlat, int ntp1) {
+  const int M = nlon / 2;
+  return ((size_t)nlon + (size_t)ntp1 * (nlat + 1) + (size_t)kWarps * kRowsPerWarp * (M + 1)) * sizeof(float2);
+}
+
+// gp2fc for one plane per block: rows of N grid values -> m-major
+// coefficients. A warp transforms kRowsPerWarp rows together.
 template <int R>
 __global__ void __launch_bounds__(kWarps * 32) k_fft_forward(const float* __restrict__ g, float* __restrict__ c,
-                                                             int rows, const float2* __restrict__ twg, int ntp1) {
-  constexpr int M = 32 * R, N = 2 * M;
-  __shared__ float2 tw[N];
-  __shared__ float2 zs[kWarps][M];
+                                                             const float2* __restrict__ twg, int nlat, int ntp1) {
+  constexpr int M = 32 * R, N = 2 * M, B = kRowsPerWarp;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* fc = tw + N;                        // [ntp1][nlat + 1]
+  float2* zs = fc + (size_t)ntp1 * (nlat + 1);  // [kWarps][B][M + 1]
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const float inv_n = 1.f / (float)N;
-  for (int row = blockIdx.x * kWarps + warp; row < rows; row += gridDim.x * kWarps) {
-    const float2* in = reinterpret_cast<const float2*>(g + (size_t)row * N);
-    float2 x[R];
+  const size_t plane = blockIdx.x;
+  float2* zw = zs + (size_t)warp * B * (M + 1);
+  for (int row0 = warp * B; row0 < nlat; row0 += kWarps * B) {
+    float2 x[B][R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) x[r] = in[lane + 32 * r];
-    warp_fft<R, -1>(x, tw, N, lane);
+    for (int b = 0; b < B; ++b) {
+      const float2* in = reinterpret_cast<const float2*>(g + (plane * nlat + row0 + b) * N);
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[b][r] = in[lane + 32 * r];
+    }
+    warp_fft<B, R, -1>(x, tw, N, lane);
     const int k1 = bitrev5(lane);
 #pragma unroll
-    for (int r = 0; r < R; ++r) zs[warp][R * k1 + r] = x[r];
+    for (int b = 0; b < B; ++b)
+#pragma unroll
+      for (int r = 0; r < R; ++r) zw[b * (M + 1) + R * k1 + r] = x[b][r];
     __syncwarp();
-    float2* out = reinterpret_cast<float2*>(c + (size_t)row * 2 * ntp1);
-    for (int m = lane; m < ntp1; m += 32) {
-      const float2 zm = zs[warp][m];
-      const float2 zc = conj2(zs[warp][(M - m) % M]);
-      const float2 even = make_float2(0.5f * (zm.x + zc.x), 0.5f * (zm.y + zc.y));
-      // (zm - zc) / 2i = ((zm - zc).y, -(zm - zc).x) / 2
-      const float2 odd = make_float2(0.5f * (zm.y - zc.y), -0.5f * (zm.x - zc.x));
-      const float2 gm = cadd(even, cmul(twiddle<-1>(tw, m, N), odd));
-      out[m] = make_float2(gm.x * inv_n, m == 0 ? 0.f : gm.y * inv_n);
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      const float2* z = zw + b * (M + 1);
+      for (int m = lane; m < ntp1; m += 32) {
+        const float2 zm = z[m];
+        const float2 zc = conj2(z[(M - m) % M]);
+        const float2 even = make_float2(0.5f * (zm.x + zc.x), 0.5f * (zm.y + zc.y));
+        // (zm - zc) / 2i = ((zm - zc).y, -(zm - zc).x) / 2
+        const float2 odd = make_float2(0.5f * (zm.y - zc.y), -0.5f * (zm.x - zc.x));
+        const float2 gm = cadd(even, cmul(twiddle<-1>(tw, m, N), odd));
+        fc[m * (nlat + 1) + row0 + b] = make_float2(gm.x * inv_n, m == 0 ? 0.f : gm.y * inv_n);
+      }
     }
     __syncwarp();
   }
+  __syncthreads();
+  float2* out = reinterpret_cast<float2*>(c) + plane * nlat * ntp1;
+  for (int i = threadIdx.x; i < ntp1 * nlat; i += blockDim.x) {
+    const int m = i / nlat, lat = i - m * nlat;
+    out[i] = fc[m * (nlat + 1) + lat];
+  }
 }
 
-// fc2gp: rows of NTP1 coefficients -> rows of N grid values.
+// fc2gp for one plane per block: m-major coefficients -> rows of N grid
+// values, kRowsPerWarp rows per warp at once.
 template <int R>
 __global__ void __launch_bounds__(kWarps * 32) k_fft_inverse(const float* __restrict__ c, float* __restrict__ g,
-                                                             int rows, const float2* __restrict__ twg, int ntp1) {
-  constexpr int M = 32 * R, N = 2 * M;
-  __shared__ float2 tw[N];
-  __shared__ float2 gs[kWarps][M + 1];
+                                                             const float2* __restrict__ twg, int nlat, int ntp1) {
+  constexpr int M = 32 * R, N = 2 * M, B = kRowsPerWarp;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* fc = tw + N;                          // [ntp1][nlat + 1]
+  float2* gs = fc + (size_t)ntp1 * (nlat + 1);  // [kWarps][B][M + 1]
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
+  const size_t plane = blockIdx.x;
+  const float2* in = reinterpret_cast<const float2*>(c) + plane * nlat * ntp1;
+  for (int i = threadIdx.x; i < ntp1 * nlat; i += blockDim.x) {
+    const int m = i / nlat, lat = i - m * nlat;
+    float2 v = in[i];
+    if (m == 0) v.y = 0.f;  // Im c_0 is ignored
+    fc[m * (nlat + 1) + lat] = v;
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int row = blockIdx.x * kWarps + warp; row < rows; row += gridDim.x * kWarps) {
-    const float2* in = reinterpret_cast<const float2*>(c + (size_t)row * 2 * ntp1);
-    for (int m = lane; m <= M; m += 32) {
-      float2 v = m < ntp1 ? in[m] : make_float2(0.f, 0.f);
-      if (m == 0) v.y = 0.f;  // Im c_0 is ignored
-      gs[warp][m] = v;
-    }
-    __syncwarp();
-    float2 x[R];
+  float2* gw = gs + (size_t)warp * B * (M + 1);
+  for (int row0 = warp * B; row0 < nlat; row0 += kWarps * B) {
+    float2 x[B][R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int k = lane + 32 * r;
-      const float2 gk = gs[warp][k];
-      const float2 gmk = conj2(gs[warp][M - k]);
-      const float2 e = cadd(gk, gmk);
-      const float2 o = cmul(csub(gk, gmk), twiddle<1>(tw, k, N));
-      x[r] = make_float2(e.x - o.y, e.y + o.x);  // e + i o
+    for (int b = 0; b < B; ++b) {
+      const int row = row0 + b;
+      auto coef = [&](int k) { return k < ntp1 ? fc[k * (nlat + 1) + row] : make_float2(0.f, 0.f); };
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int k = lane + 32 * r;
+        const float2 gk = coef(k);
+        const float2 gmk = conj2(coef(M - k));
+        const float2 e = cadd(gk, gmk);
+        const float2 o = cmul(csub(gk, gmk), twiddle<1>(tw, k, N));
+        x[b][r] = make_float2(e.x - o.y, e.y + o.x);  // e + i o
+      }
     }
-    warp_fft<R, 1>(x, tw, N, lane);
-    __syncwarp();
+    warp_fft<B, R, 1>(x, tw, N, lane);
     const int k1 = bitrev5(lane);
 #pragma unroll
-    for (int r = 0; r < R; ++r) gs[warp][R * k1 + r] = x[r];
-    __syncwarp();
-    float2* out = reinterpret_cast<float2*>(g + (size_t)row * N);
+    for (int b = 0; b < B; ++b)
 #pragma unroll
-    for (int r = 0; r < R; ++r) out[lane + 32 * r] = gs[warp][lane + 32 * r];
+      for (int r = 0; r < R; ++r) gw[b * (M + 1) + R * k1 + r] = x[b][r];
+    __syncwarp();
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      float2* out = reinterpret_cast<float2*>(g + (plane * nlat + row0 + b) * N);
+#pragma unroll
+      for (int r = 0; r < R; ++r) out[lane + 32 * r] = gw[b * (M + 1) + lane + 32 * r];
+    }
     __syncwarp();
   }
 }
 
-inline unsigned fft_blocks(int rows) {
-  const int want = (rows + kWarps - 1) / kWarps;
-  return (unsigned)(want < 148 * 16 ? want : 148 * 16);
+template <typename K>
+void allow_plane_smem(K kernel) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
 }
 
 }  // namespace
 
+void fft_init() {
+  allow_plane_smem(k_fft_forward<1>);
+  allow_plane_smem(k_fft_forward<2>);
+  allow_plane_smem(k_fft_forward<3>);
+  allow_plane_smem(k_fft_inverse<1>);
+  allow_plane_smem(k_fft_inverse<2>);
+  allow_plane_smem(k_fft_inverse<3>);
+}
+
+// The plane blocks need NLAT to be a multiple of kWarps * kRowsPerWarp (16):
+// NLAT is 32, 64 or 96.
 void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st) {
-  const int rows = planes * m.d.NLAT;
   const float2* tw = reinterpret_cast<const float2*>(m.sh.tw);
+  const size_t smem = plane_smem(m.d.NLON, m.d.NLAT, m.d.NTP1);
   switch (m.d.NLON) {
-    case 64: k_fft_forward<1><<<fft_blocks(rows), kWarps * 32, 0, st>>>(g, c, rows, tw, m.d.NTP1); break;
-    case 128: k_fft_forward<2><<<fft_blocks(rows), kWarps * 32, 0, st>>>(g, c, rows, tw, m.d.NTP1); break;
-    default: k_fft_forward<3><<<fft_blocks(rows), kWarps * 32, 0, st>>>(g, c, rows, tw, m.d.NTP1); break;
+    case 64: k_fft_forward<1><<<planes, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1); break;
+    case 128: k_fft_forward<2><<<planes, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1); break;
+    default: k_fft_forward<3><<<planes, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1); break;
   }
 }
 
 void fft_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st) {
-  const int rows = planes * m.d.NLAT;
   const float2* tw = reinterpret_cast<const float2*>(m.sh.tw);
+  const size_t smem = plane_smem(m.d.NLON, m.d.NLAT, m.d.NTP1);
   switch (m.d.NLON) {
-    case 64: k_fft_inverse<1><<<fft_blocks(rows), kWarps * 32, 0, st>>>(c, g, rows, tw, m.d.NTP1); break;
-    case 128: k_fft_inverse<2><<<fft_blocks(rows), kWarps * 32, 0, st>>>(c, g, rows, tw, m.d.NTP1); break;
-    default: k_fft_inverse<3><<<fft_blocks(rows), kWarps * 32, 0, st>>>(c, g, rows, tw, m.d.NTP1); break;
+    case 64: k_fft_inverse<1><<<planes, kWarps * 32, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1); break;
+    case 128: k_fft_inverse<2><<<planes, kWarps * 32, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1); break;
+    default: k_fft_inverse<3><<<planes, kWarps * 32, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1); break;
   }
 }
 

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "common.cuh"
 
 namespace exogcm {
@@ -31,7 +33,8 @@ void leg_uv2dv(const Model& m, const float* u, const float* v, const float* ke, 
 void leg_qtend(const Model& m, const float* u, const float* v, const float* src, float* out, int planes,
                cudaStream_t st);
 
-// fft.cu
+// fft.cu (optimized path; Fourier planes m-major)
+void fft_init();
 void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st);
 void fft_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st);
 
@@ -54,5 +57,7 @@ void phy_surface(const Model& m, cudaStream_t st);
 void phy_carbon(const Model& m, cudaStream_t st);
 void phy_pack(const Model& m, cudaStream_t st);
 void phy_finite_check(const Model& m, cudaStream_t st);
+// One named column kernel of the physics (for timing); false if unknown.
+bool phy_launch_one(const Model& m, const std::string& kernel, cudaStream_t st);
 
 }  // namespace exogcm

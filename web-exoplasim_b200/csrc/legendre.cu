@@ -18,12 +18,15 @@
 //    shared memory instead of once per mode, with the shaders' arithmetic
 //    in their order, so the results equal the plain path's bit for bit.
 //
-// Work is tiled as one block per (group of kGroup consecutive wavenumbers,
-// tile of planes). The coefficients of a group are contiguous in a spectral
-// plane (modes are m-major), and its Fourier outputs are a contiguous chunk
-// of every row, so both directions read and write whole sectors. The
-// transposed northern tables of the inverse ([mode][pair]) make the table
-// reads coalesce across the threads of a warp, which own consecutive pairs.
+// Fourier planes are m-major on this path (coefficient (m, lat) at
+// 2 * (m * NLAT + lat)), so an output wavenumber of the inverse is one
+// contiguous run of latitudes, written by the threads that own consecutive
+// latitude pairs (north run ascending, south run descending), and the
+// forward transform reads such runs. Work is tiled as one block per (group
+// of consecutive wavenumbers, tile of planes): a group's coefficients are
+// contiguous in a spectral plane (modes are m-major) and a group's table
+// slice is contiguous in the transposed northern tables ([mode][pair]), so
+// both are staged in shared memory by contiguous loads.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -33,17 +36,17 @@ namespace exogcm {
 
 namespace {
 
-constexpr int kGroup = 4;         // zonal wavenumbers per block
-constexpr int kRow = 2 * kGroup + 1;  // staged output row: 2 floats per m, padded to an odd stride
 constexpr int kForwardThreads = 256;
+constexpr int kForwardGroup = 4;  // wavenumbers per forward block
+constexpr size_t kInverseBudget = 48 * 1024;
 constexpr size_t kSmemBudget = 100 * 1024;
 
 __device__ __forceinline__ int first_mode(int m, int ntp1) { return m * (2 * ntp1 - m + 1) / 2; }
 inline int first_mode_host(int m, int ntp1) { return m * (2 * ntp1 - m + 1) / 2; }
 
-// Largest number of terms (modes) of one group: the first.
-inline int group_terms(const Dims& d) {
-  const int m1 = kGroup < d.NTP1 ? kGroup : d.NTP1;
+// Terms (modes) of the first, largest group of `group` wavenumbers.
+inline int group_terms(const Dims& d, int group) {
+  const int m1 = group < d.NTP1 ? group : d.NTP1;
   return first_mode_host(m1, d.NTP1);
 }
 
@@ -54,124 +57,127 @@ inline int group_terms(const Dims& d) {
 // Each thread owns latitude pair j and two planes of the tile.
 template <int KIND>
 __global__ void k_sym_inverse(const float* __restrict__ s0, const float* __restrict__ s1, float* __restrict__ f0,
-                              float* __restrict__ f1, int planes, int tile, const float* __restrict__ qa,
+                              float* __restrict__ f1, int planes, int tile, int group, const float* __restrict__ qa,
                               const float* __restrict__ qb, int odd, float plavor, Dims d) {
   constexpr int NIN = KIND == 0 ? 1 : 2;
   extern __shared__ float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
   const int JH = d.NLAT / 2;
-  const int m0 = blockIdx.x * kGroup;
-  const int m1 = min(m0 + kGroup, d.NTP1);
+  const int m0 = blockIdx.x * group;
+  const int m1 = min(m0 + group, d.NTP1);
   const int w0 = first_mode(m0, d.NTP1);
   const int nt = first_mode(m1, d.NTP1) - w0;
   const int p0 = blockIdx.y * tile;
   const int np = min(tile, planes - p0);
-  float2* ss = reinterpret_cast<float2*>(smem);  // [NIN][tile][nt] (re, im)
-  float* so = smem + 2 * NIN * tile * nt;        // [NIN][tile][NLAT][kRow]
+  const size_t plane_floats = (size_t)d.NLAT * d.NFC;
+  // [NIN][nt][tile] (re, im): term-major, so two planes are one float4.
+  float2* ss = reinterpret_cast<float2*>(smem);
+  float* qs = smem + 2 * (size_t)NIN * nt * tile;  // [NIN tables][nt][JH]
+  for (int i = threadIdx.x; i < nt * JH; i += blockDim.x) {
+    qs[i] = __ldg(qa + (size_t)w0 * JH + i);
+    if (KIND == 1) qs[nt * JH + i] = __ldg(qb + (size_t)w0 * JH + i);
+  }
   for (int k = 0; k < NIN; ++k) {
     const float* src = k == 0 ? s0 : s1;
-    for (int i = threadIdx.x; i < np * nt; i += blockDim.x) {
+    for (int i = threadIdx.x; i < tile * nt; i += blockDim.x) {
       const int p = i / nt, t = i - p * nt;
-      float2 v = *reinterpret_cast<const float2*>(src + (size_t)(p0 + p) * d.NRSP + 2 * (w0 + t));
-      if (KIND == 1 && k == 1 && w0 + t == 1) v.x -= plavor;
-      ss[(k * tile + p) * nt + t] = v;
+      float2 v = make_float2(0.f, 0.f);
+      if (p < np) {
+        v = *reinterpret_cast<const float2*>(src + (size_t)(p0 + p) * d.NRSP + 2 * (w0 + t));
+        if (KIND == 1 && k == 1 && w0 + t == 1) v.x -= plavor;
+      }
+      ss[((size_t)k * nt + t) * tile + p] = v;
     }
   }
   __syncthreads();
   const int j = threadIdx.x % JH;
   const int pa = 2 * (threadIdx.x / JH);  // planes pa, pa + 1 of the tile
   const int south = d.NLAT - 1 - j;
+  const bool has_a = pa < np, has_b = pa + 1 < np;
+  float2* outa0 = reinterpret_cast<float2*>(f0 + (size_t)(p0 + pa) * plane_floats);
+  float2* outb0 = outa0 + plane_floats / 2;
   for (int m = m0; m < m1; ++m) {
-    const int mi = m - m0;
     const int toff = first_mode(m, d.NTP1) - w0;
     const int K = d.NTP1 - m;
-    const float* ta = qa + (size_t)(w0 + toff) * JH + j;
+    const float* qc = qs + toff * JH + j;
+    const float4* sc = reinterpret_cast<const float4*>(ss + (size_t)toff * tile + pa);
+    const int step4 = tile / 2;  // float4 stride between terms
+    const size_t rn = (size_t)m * d.NLAT + j, rs = (size_t)m * d.NLAT + south;
     if (KIND == 0) {
-      const float2* sa = ss + pa * nt + toff;
-      const float2* sb = sa + nt;
-      float e0r = 0.f, e0i = 0.f, o0r = 0.f, o0i = 0.f, e1r = 0.f, e1i = 0.f, o1r = 0.f, o1i = 0.f;
+      float4 e = make_float4(0.f, 0.f, 0.f, 0.f), o = e;  // (re a, im a, re b, im b)
       int t = 0;
       for (; t + 1 < K; t += 2) {
-        const float qe = __ldg(ta + t * JH), qo = __ldg(ta + (t + 1) * JH);
-        const float2 a0 = sa[t], a1 = sa[t + 1], b0 = sb[t], b1 = sb[t + 1];
-        e0r = fmaf(qe, a0.x, e0r);
-        e0i = fmaf(qe, a0.y, e0i);
-        e1r = fmaf(qe, b0.x, e1r);
-        e1i = fmaf(qe, b0.y, e1i);
-        o0r = fmaf(qo, a1.x, o0r);
-        o0i = fmaf(qo, a1.y, o0i);
-        o1r = fmaf(qo, b1.x, o1r);
-        o1i = fmaf(qo, b1.y, o1i);
+        const float qe = qc[t * JH], qo = qc[(t + 1) * JH];
+        const float4 ve = sc[t * step4], vo = sc[(t + 1) * step4];
+        e.x = fmaf(qe, ve.x, e.x);
+        e.y = fmaf(qe, ve.y, e.y);
+        e.z = fmaf(qe, ve.z, e.z);
+        e.w = fmaf(qe, ve.w, e.w);
+        o.x = fmaf(qo, vo.x, o.x);
+        o.y = fmaf(qo, vo.y, o.y);
+        o.z = fmaf(qo, vo.z, o.z);
+        o.w = fmaf(qo, vo.w, o.w);
       }
       if (t < K) {
-        const float qe = __ldg(ta + t * JH);
-        const float2 a0 = sa[t], b0 = sb[t];
-        e0r = fmaf(qe, a0.x, e0r);
-        e0i = fmaf(qe, a0.y, e0i);
-        e1r = fmaf(qe, b0.x, e1r);
-        e1i = fmaf(qe, b0.y, e1i);
+        const float qe = qc[t * JH];
+        const float4 ve = sc[t * step4];
+        e.x = fmaf(qe, ve.x, e.x);
+        e.y = fmaf(qe, ve.y, e.y);
+        e.z = fmaf(qe, ve.z, e.z);
+        e.w = fmaf(qe, ve.w, e.w);
       }
       const float sg = odd ? -1.f : 1.f;
-      float* r0 = so + (size_t)pa * d.NLAT * kRow + 2 * mi;
-      float* r1 = r0 + (size_t)d.NLAT * kRow;
-      r0[j * kRow] = e0r + o0r;
-      r0[j * kRow + 1] = e0i + o0i;
-      r0[south * kRow] = sg * (e0r - o0r);
-      r0[south * kRow + 1] = sg * (e0i - o0i);
-      r1[j * kRow] = e1r + o1r;
-      r1[j * kRow + 1] = e1i + o1i;
-      r1[south * kRow] = sg * (e1r - o1r);
-      r1[south * kRow + 1] = sg * (e1i - o1i);
+      if (has_a) {
+        outa0[rn] = make_float2(e.x + o.x, e.y + o.y);
+        outa0[rs] = make_float2(sg * (e.x - o.x), sg * (e.y - o.y));
+      }
+      if (has_b) {
+        outb0[rn] = make_float2(e.z + o.z, e.w + o.w);
+        outb0[rs] = make_float2(sg * (e.z - o.z), sg * (e.w - o.w));
+      }
     } else {
-      const float* tb = qb + (size_t)(w0 + toff) * JH + j;
-      // X collects the terms whose table is even at this t (a at even t,
-      // b at odd t), Y the others: north = X + Y, south = X - Y.
+      const float* qd = qc + nt * JH;
+      const float4* zc = sc + (size_t)nt * step4;
+      // Term t's contribution to u and v: a(t) * (dim, -dre, zim, -zre)
+      // + b(t) * (zre, zim, -dre, -dim); the even-t a part and odd-t b part
+      // go to X, the rest to Y: north = X + Y, south = X - Y.
       float X[2][4] = {}, Y[2][4] = {};
-      for (int t = 0; t < K; ++t) {
-        const float a = __ldg(ta + t * JH), b = __ldg(tb + t * JH);
+      auto add = [&](float (*acc_a)[4], float (*acc_b)[4], float a, float b, int t) {
+        const float4 D = sc[t * step4], Z = zc[t * step4];
+        const float2 Dp[2] = {make_float2(D.x, D.y), make_float2(D.z, D.w)};
+        const float2 Zp[2] = {make_float2(Z.x, Z.y), make_float2(Z.z, Z.w)};
 #pragma unroll
         for (int pp = 0; pp < 2; ++pp) {
-          const float2 D = ss[(pa + pp) * nt + toff + t];
-          const float2 Z = ss[(tile + pa + pp) * nt + toff + t];
-          const float au[4] = {a * D.y, -a * D.x, a * Z.y, -a * Z.x};
-          const float bu[4] = {b * Z.x, b * Z.y, -b * D.x, -b * D.y};
-#pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            if ((t & 1) == 0) {
-              X[pp][c] += au[c];
-              Y[pp][c] += bu[c];
-            } else {
-              X[pp][c] += bu[c];
-              Y[pp][c] += au[c];
-            }
-          }
+          acc_a[pp][0] = fmaf(a, Dp[pp].y, acc_a[pp][0]);
+          acc_a[pp][1] = fmaf(-a, Dp[pp].x, acc_a[pp][1]);
+          acc_a[pp][2] = fmaf(a, Zp[pp].y, acc_a[pp][2]);
+          acc_a[pp][3] = fmaf(-a, Zp[pp].x, acc_a[pp][3]);
+          acc_b[pp][0] = fmaf(b, Zp[pp].x, acc_b[pp][0]);
+          acc_b[pp][1] = fmaf(b, Zp[pp].y, acc_b[pp][1]);
+          acc_b[pp][2] = fmaf(-b, Dp[pp].x, acc_b[pp][2]);
+          acc_b[pp][3] = fmaf(-b, Dp[pp].y, acc_b[pp][3]);
         }
+      };
+      int t = 0;
+      for (; t + 1 < K; t += 2) {
+        add(X, Y, qc[t * JH], qd[t * JH], t);
+        add(Y, X, qc[(t + 1) * JH], qd[(t + 1) * JH], t + 1);
       }
-#pragma unroll
-      for (int pp = 0; pp < 2; ++pp) {
-        float* ru = so + (size_t)(pa + pp) * d.NLAT * kRow + 2 * mi;
-        float* rv = ru + (size_t)tile * d.NLAT * kRow;
-        ru[j * kRow] = X[pp][0] + Y[pp][0];
-        ru[j * kRow + 1] = X[pp][1] + Y[pp][1];
-        rv[j * kRow] = X[pp][2] + Y[pp][2];
-        rv[j * kRow + 1] = X[pp][3] + Y[pp][3];
-        ru[south * kRow] = X[pp][0] - Y[pp][0];
-        ru[south * kRow + 1] = X[pp][1] - Y[pp][1];
-        rv[south * kRow] = X[pp][2] - Y[pp][2];
-        rv[south * kRow + 1] = X[pp][3] - Y[pp][3];
+      if (t < K) add(X, Y, qc[t * JH], qd[t * JH], t);
+      float2* outa1 = reinterpret_cast<float2*>(f1 + (size_t)(p0 + pa) * plane_floats);
+      float2* outb1 = outa1 + plane_floats / 2;
+      if (has_a) {
+        outa0[rn] = make_float2(X[0][0] + Y[0][0], X[0][1] + Y[0][1]);
+        outa0[rs] = make_float2(X[0][0] - Y[0][0], X[0][1] - Y[0][1]);
+        outa1[rn] = make_float2(X[0][2] + Y[0][2], X[0][3] + Y[0][3]);
+        outa1[rs] = make_float2(X[0][2] - Y[0][2], X[0][3] - Y[0][3]);
       }
-    }
-  }
-  __syncthreads();
-  // Flush: each row gets its group's 2 * (m1 - m0) consecutive floats.
-  const int width = 2 * (m1 - m0);
-  const int rows = np * d.NLAT;
-  for (int k = 0; k < NIN; ++k) {
-    float* dst = k == 0 ? f0 : f1;
-    const float* src = so + (size_t)k * tile * d.NLAT * kRow;
-    for (int i = threadIdx.x; i < rows * width; i += blockDim.x) {
-      const int row = i / width, c = i - row * width;
-      dst[((size_t)p0 * d.NLAT + row) * d.NFC + 2 * m0 + c] = src[row * kRow + c];
+      if (has_b) {
+        outb0[rn] = make_float2(X[1][0] + Y[1][0], X[1][1] + Y[1][1]);
+        outb0[rs] = make_float2(X[1][0] - Y[1][0], X[1][1] - Y[1][1]);
+        outb1[rn] = make_float2(X[1][2] + Y[1][2], X[1][3] + Y[1][3]);
+        outb1[rs] = make_float2(X[1][2] - Y[1][2], X[1][3] - Y[1][3]);
+      }
     }
   }
 }
@@ -186,33 +192,33 @@ struct SymIn {
 // KIND 1: uv2dv, in = {u, v}, outputs D, Z (uv2dv.wgsl without the KE term).
 // KIND 2: mktend's uv2dv, in = {u, v, ke} (uv2dv.wgsl with HAS_KINETIC).
 // KIND 3: qtend, in = {u, v, source} (qtend.wgsl).
-// Staged per (input, plane, pair, m): (north + south, north - south) of the
-// real and imaginary parts. For mode (m, n) the shader's north + s * south
-// with s = (-1)^(m+n) is the sum for even n - m and the difference for odd.
+// Staged per (input, plane, m, pair): (north + south, north - south) of the
+// real and imaginary parts, read from the m-major planes as contiguous runs
+// of latitudes. For mode (m, n) the shader's north + s * south with
+// s = (-1)^(m+n) is the sum for even n - m and the difference for odd.
 template <int KIND, int NIN>
 __global__ void __launch_bounds__(kForwardThreads) k_sym_forward(SymIn<NIN> in, float* __restrict__ out0,
                                                                  float* __restrict__ out1, int planes, int tile,
                                                                  SharedTabs sh, const float* __restrict__ q, Dims d) {
-  extern __shared__ float4 pm[];  // [NIN][tile][JH][kGroup]: (sum re, sum im, difference re, difference im)
+  extern __shared__ float4 pm[];  // [NIN][tile][kForwardGroup][JH]
   const int JH = d.NLAT / 2;
-  const int m0 = blockIdx.x * kGroup;
-  const int m1 = min(m0 + kGroup, d.NTP1);
+  const int m0 = blockIdx.x * kForwardGroup;
+  const int m1 = min(m0 + kForwardGroup, d.NTP1);
   const int gm = m1 - m0;
   const int w0 = first_mode(m0, d.NTP1);
   const int nt = first_mode(m1, d.NTP1) - w0;
   const int p0 = blockIdx.y * tile;
   const int np = min(tile, planes - p0);
-  const int plane_floats = d.NLAT * d.NFC;
+  const size_t plane_floats = (size_t)d.NLAT * d.NFC;
   for (int k = 0; k < NIN; ++k) {
-    const float* src = in.p[k] + (size_t)p0 * plane_floats + 2 * m0;
-    for (int i = threadIdx.x; i < np * JH * gm; i += blockDim.x) {
-      const int mi = i % gm;
-      const int j = (i / gm) % JH;
-      const int p = i / (gm * JH);
-      const float2 n = *reinterpret_cast<const float2*>(src + (size_t)p * plane_floats + j * d.NFC + 2 * mi);
-      const float2 s =
-          *reinterpret_cast<const float2*>(src + (size_t)p * plane_floats + (d.NLAT - 1 - j) * d.NFC + 2 * mi);
-      pm[((k * tile + p) * JH + j) * kGroup + mi] = make_float4(n.x + s.x, n.y + s.y, n.x - s.x, n.y - s.y);
+    for (int i = threadIdx.x; i < np * gm * JH; i += blockDim.x) {
+      const int j = i % JH;
+      const int mi = (i / JH) % gm;
+      const int p = i / (JH * gm);
+      const float2* row =
+          reinterpret_cast<const float2*>(in.p[k] + (size_t)(p0 + p) * plane_floats) + (size_t)(m0 + mi) * d.NLAT;
+      const float2 n = row[j], s = row[d.NLAT - 1 - j];
+      pm[((k * tile + p) * kForwardGroup + mi) * JH + j] = make_float4(n.x + s.x, n.y + s.y, n.x - s.x, n.y - s.y);
     }
   }
   __syncthreads();
@@ -224,14 +230,14 @@ __global__ void __launch_bounds__(kForwardThreads) k_sym_forward(SymIn<NIN> in, 
     const int mi = m - m0;
     const bool even = ((m + n) & 1) == 0;
     const size_t at = (size_t)(p0 + p) * d.NRSP + 2 * w;
-    const float4* A = pm + ((size_t)(0 * tile + p) * JH) * kGroup + mi;
-    const float4* B = pm + ((size_t)((NIN > 1 ? 1 : 0) * tile + p) * JH) * kGroup + mi;
-    const float4* C = pm + ((size_t)((NIN > 2 ? 2 : 0) * tile + p) * JH) * kGroup + mi;
+    const float4* A = pm + ((size_t)(0 * tile + p) * kForwardGroup + mi) * JH;
+    const float4* B = pm + ((size_t)((NIN > 1 ? 1 : 0) * tile + p) * kForwardGroup + mi) * JH;
+    const float4* C = pm + ((size_t)((NIN > 2 ? 2 : 0) * tile + p) * kForwardGroup + mi) * JH;
     if (KIND == 0) {
       float re = 0.f, im = 0.f;
       for (int l = 0; l < JH; ++l) {
         const float qq = __ldg(q + l * d.NCSP + w);
-        const float4 f = A[l * kGroup];
+        const float4 f = A[l];
         re = fmaf(qq, even ? f.x : f.z, re);
         im = fmaf(qq, even ? f.y : f.w, im);
       }
@@ -241,7 +247,7 @@ __global__ void __launch_bounds__(kForwardThreads) k_sym_forward(SymIn<NIN> in, 
       float dre = 0.f, dim = 0.f, zre = 0.f, zim = 0.f;
       for (int l = 0; l < JH; ++l) {
         const float e = __ldg(sh.qe + l * d.NCSP + w), mq = __ldg(sh.qm + l * d.NCSP + w);
-        const float4 U = A[l * kGroup], V = B[l * kGroup];
+        const float4 U = A[l], V = B[l];
         // north - s * south and north + s * south of u and v
         const float dure = even ? U.z : U.x, duim = even ? U.w : U.y;
         const float dvre = even ? V.z : V.x, dvim = even ? V.w : V.y;
@@ -249,7 +255,7 @@ __global__ void __launch_bounds__(kForwardThreads) k_sym_forward(SymIn<NIN> in, 
         const float svre = even ? V.x : V.z, svim = even ? V.y : V.w;
         if (KIND == 2) {
           const float q2 = __ldg(sh.qq + l * d.NCSP + w);
-          const float4 Kf = C[l * kGroup];
+          const float4 Kf = C[l];
           dre = dre + q2 * (even ? Kf.x : Kf.z);
           dim = dim + q2 * (even ? Kf.y : Kf.w);
         }
@@ -267,7 +273,7 @@ __global__ void __launch_bounds__(kForwardThreads) k_sym_forward(SymIn<NIN> in, 
       for (int l = 0; l < JH; ++l) {
         const float e = __ldg(sh.qe + l * d.NCSP + w), c = __ldg(sh.qc + l * d.NCSP + w),
                     mq = __ldg(sh.qm + l * d.NCSP + w);
-        const float4 U = A[l * kGroup], V = B[l * kGroup], X = C[l * kGroup];
+        const float4 U = A[l], V = B[l], X = C[l];
         re = re + e * (even ? V.z : V.x) + c * (even ? X.x : X.z) + mq * (even ? U.y : U.w);
         im = im + e * (even ? V.w : V.y) + c * (even ? X.y : X.w) - mq * (even ? U.x : U.z);
       }
@@ -277,30 +283,35 @@ __global__ void __launch_bounds__(kForwardThreads) k_sym_forward(SymIn<NIN> in, 
   }
 }
 
-// Planes per block: the largest of 32, 16, 8, 4, 2 whose shared memory fits
-// the budget (two blocks per SM at most of it).
-template <typename F>
-int pick_tile(F bytes_for) {
-  for (int tile = 32; tile > 2; tile /= 2)
-    if (bytes_for(tile) <= kSmemBudget) return tile;
-  return 2;
+// Inverse tiling: 16 planes per block (32 at T21, 8 threads per latitude
+// pair either way) and the largest group of 4, 2 or 1 wavenumbers whose
+// staged coefficients and table slices fit the budget (several blocks per
+// SM).
+struct InverseTiling {
+  int tile, group;
+  size_t smem;
+};
+
+InverseTiling inverse_tiling(const Dims& d, int nin) {
+  const int tile = d.NLAT == 32 ? 32 : 16;
+  const int JH = d.NLAT / 2;
+  for (int group = 4;; group /= 2) {
+    const size_t nt = group_terms(d, group);
+    const size_t smem = (size_t)nin * nt * tile * 8 + (size_t)nin * nt * JH * 4;
+    if (smem <= kInverseBudget || group == 1) return {tile, group, smem};
+  }
 }
 
-size_t inverse_smem(const Dims& d, int nin, int tile) {
-  return (size_t)nin * tile * group_terms(d) * 8 + (size_t)nin * tile * d.NLAT * kRow * 4;
-}
-
-size_t forward_smem(const Dims& d, int nin, int tile) { return (size_t)nin * tile * (d.NLAT / 2) * kGroup * 16; }
-
-int inverse_tile_for(const Dims& d, int nin) {
-  // Threads = pairs * tile / 2; keep blocks at or under 512 threads.
-  int tile = pick_tile([&](int t) { return inverse_smem(d, nin, t); });
-  while (tile > 2 && (d.NLAT / 2) * tile / 2 > 512) tile /= 2;
-  return tile;
+// Forward planes per block: the largest of 32, 16, 8, 4, 2 whose staged
+// sums and differences fit the budget.
+size_t forward_smem(const Dims& d, int nin, int tile) {
+  return (size_t)nin * tile * kForwardGroup * (d.NLAT / 2) * 16;
 }
 
 int forward_tile_for(const Dims& d, int nin) {
-  return pick_tile([&](int t) { return forward_smem(d, nin, t); });
+  for (int tile = 32; tile > 2; tile /= 2)
+    if (forward_smem(d, nin, tile) <= kSmemBudget) return tile;
+  return 2;
 }
 
 template <typename K>
@@ -312,7 +323,7 @@ template <int KIND, int NIN>
 void launch_sym_forward(const Model& m, SymIn<NIN> in, float* out0, float* out1, int planes, const float* q,
                         cudaStream_t st) {
   const int tile = forward_tile_for(m.d, NIN);
-  dim3 grid((m.d.NTP1 + kGroup - 1) / kGroup, (planes + tile - 1) / tile);
+  dim3 grid((m.d.NTP1 + kForwardGroup - 1) / kForwardGroup, (planes + tile - 1) / tile);
   k_sym_forward<KIND, NIN><<<grid, kForwardThreads, forward_smem(m.d, NIN, tile), st>>>(in, out0, out1, planes, tile,
                                                                                       m.sh, q, m.d);
 }
@@ -329,20 +340,21 @@ void leg_init() {
 }
 
 void leg_inverse(const Model& m, const float* s, float* f, int planes, bool derivative, cudaStream_t st) {
-  const int tile = inverse_tile_for(m.d, 1);
-  dim3 grid((m.d.NTP1 + kGroup - 1) / kGroup, (planes + tile - 1) / tile);
-  const int threads = (m.d.NLAT / 2) * tile / 2;
-  k_sym_inverse<0><<<grid, threads, inverse_smem(m.d, 1, tile), st>>>(
-      s, nullptr, f, nullptr, planes, tile, derivative ? m.sh.qjT : m.sh.qiT, nullptr, derivative ? 1 : 0, 0.f, m.d);
+  const InverseTiling t = inverse_tiling(m.d, 1);
+  dim3 grid((m.d.NTP1 + t.group - 1) / t.group, (planes + t.tile - 1) / t.tile);
+  const int threads = (m.d.NLAT / 2) * t.tile / 2;
+  k_sym_inverse<0><<<grid, threads, t.smem, st>>>(s, nullptr, f, nullptr, planes, t.tile, t.group,
+                                                  derivative ? m.sh.qjT : m.sh.qiT, nullptr, derivative ? 1 : 0, 0.f,
+                                                  m.d);
 }
 
 void leg_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V, int planes, float plavor,
                cudaStream_t st) {
-  const int tile = inverse_tile_for(m.d, 2);
-  dim3 grid((m.d.NTP1 + kGroup - 1) / kGroup, (planes + tile - 1) / tile);
-  const int threads = (m.d.NLAT / 2) * tile / 2;
-  k_sym_inverse<1><<<grid, threads, inverse_smem(m.d, 2, tile), st>>>(D, Z, U, V, planes, tile, m.sh.quT, m.sh.qvT,
-                                                                      0, plavor, m.d);
+  const InverseTiling t = inverse_tiling(m.d, 2);
+  dim3 grid((m.d.NTP1 + t.group - 1) / t.group, (planes + t.tile - 1) / t.tile);
+  const int threads = (m.d.NLAT / 2) * t.tile / 2;
+  k_sym_inverse<1><<<grid, threads, t.smem, st>>>(D, Z, U, V, planes, t.tile, t.group, m.sh.quT, m.sh.qvT, 0, plavor,
+                                                  m.d);
 }
 
 void leg_forward(const Model& m, const float* f, float* s, int planes, const float* q, cudaStream_t st) {

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <string>
 
 #include "common.cuh"
 #include "launch.h"
@@ -424,15 +425,28 @@ __device__ __forceinline__ float vapour_absorption(float wv, float zsolar2) {
   return 2.9f * wv / (fpow(1.f + 141.5f * wv, 0.635f) + 5.925f * wv) / zsolar2;
 }
 
+// Per-level state of one swr band for the block's threads, [level][thread]
+// in shared memory: the level loops stay rolled, so both bands' code fits
+// the instruction cache, and the accesses are conflict-free.
+struct SwrLevels {
+  float* p;
+  __device__ float& at(int array, int level) const { return p[(array * (MAXLEV + 1) + level) * kBlock + threadIdx.x]; }
+  static constexpr int MAXLEV = 10;
+  static constexpr int kArrays = 6;  // tl, rls (NL + 1 levels), tbd, tbu, rb, rbs
+};
+
 // One band of swr (physics/radiation/wgsl/swr.wgsl) for one column: ozone
 // absorption below 0.75 um (BAND 0) or water vapour above (BAND 1), by the
 // adding method. The band's cloud optics, layer reflectances and
 // transmissivities follow the shader's expressions in its order; the flux
-// of each level goes to fu/fd as soon as the upward pass reaches it.
-// Returns the new surface albedos (nalb1, nalb2, albedo) the column writes.
+// of each level goes to fu/fd (shared memory, [level][column]) as soon as
+// the upward pass reaches it. Returns the new surface albedos (nalb1,
+// nalb2, albedo) the column writes.
 template <int NL, int BAND>
 __device__ __forceinline__ void swr_band(const Model& m, const PlanetConst& K, const float* tb, size_t SN, int c,
-                                         float mu0, float ftop, float* fu, float* fd, float* alb) {
+                                         float mu0, float ftop, SwrLevels lv, float* fu, float* fd, int stride,
+                                         float* alb) {
+  enum { TL = 0, RLS = 1, TBD = 2, TBU = 3, RB = 4, RBS = 5 };
   const FieldPtrs& F = m.f;
   const float ZBETTA = 1.66f, ZMBAR = 1.9f, ZFO3 = 100.f / 2.14f, ZMU00 = 0.5f, INV_LN10 = 0.43429448190325176f;
   const float diffusivity = BAND == 0 ? ZMBAR : ZBETTA;
@@ -452,7 +466,7 @@ __device__ __forceinline__ void swr_band(const Model& m, const PlanetConst& K, c
   // Column totals of the absorber path (slant above the first cloud,
   // diffuse below).
   float pt = 0.f, xpt = 0.f, cs = 1.f;
-#pragma unroll
+#pragma unroll 1
   for (int l = 0; l < NL; ++l) {
     const float amount = amount_at(l);
     pt = pt + amount;
@@ -469,12 +483,11 @@ __device__ __forceinline__ void swr_band(const Model& m, const PlanetConst& K, c
         (1.f - expf(scf * logf(1.f - 0.219f / (1.f + 0.816f * mu0)))) * cs + diffuseRayleigh * (1.f - cs - ccn);
   }
   // Downward pass: layer properties and the adding recursion from the top.
-  float tl[NL + 1], rls[NL + 1], tbd[NL], tbu[NL], rb[NL], rbs[NL];
   float ta = 1.f, tas = 1.f, ra = 0.f, ras = 0.f;
   float tt = 1.f, ttu = 1.f - absorption(xpt + diffusivity * pt);
   float pl = 0.f, xpl = 0.f;
   cs = 1.f;
-#pragma unroll
+#pragma unroll 1
   for (int l = 0; l < NL; ++l) {
     const float cc = F.dcc[l * SN + c];
     float rcl = 0.f, rcls = 0.f, tcl = 1.f, tcls = 1.f;
@@ -514,32 +527,37 @@ __device__ __forceinline__ void swr_band(const Model& m, const PlanetConst& K, c
     pl = pl + amount;
     xpl = cs * (xpl + zm * amount) + (1.f - cs) * (xpl + diffusivity * amount);
     cs = cs * (1.f - cc);
-    tl[l] = ta;
-    rls[l] = ras;
+    lv.at(TL, l) = ta;
+    lv.at(RLS, l) = ras;
     const bool surface = l == NL - 1;
     const float tr = (1.f - absorption(xpl)) / tt;
     tt = tt * tr;
     const float tru = ttu / (1.f - absorption(xpt + diffusivity * (pt - pl)));
     ttu = ttu / tru;
+    float rb, rbs, tbd, tbu;
     if (BAND == 0) {
-      rb[l] = (surface ? rcsSurface : 0.f) + rcl * cc;
-      rbs[l] = (surface ? rcsuSurface : 0.f) + rcls * cc;
-      tbd[l] = 1.f - (1.f - tr) * (1.f - cc) - rb[l];
-      tbu[l] = 1.f - (1.f - tru) * (1.f - cc) - rbs[l];
+      rb = (surface ? rcsSurface : 0.f) + rcl * cc;
+      rbs = (surface ? rcsuSurface : 0.f) + rcls * cc;
+      tbd = 1.f - (1.f - tr) * (1.f - cc) - rb;
+      tbu = 1.f - (1.f - tru) * (1.f - cc) - rbs;
     } else {
-      rb[l] = rcl * cc;
-      rbs[l] = rcls * cc;
-      tbd[l] = 1.f - (1.f - tr) * (1.f - cc) - (1.f - tcl) * cc;
-      tbu[l] = 1.f - (1.f - tru) * (1.f - cc) - (1.f - tcls) * cc;
+      rb = rcl * cc;
+      rbs = rcls * cc;
+      tbd = 1.f - (1.f - tr) * (1.f - cc) - (1.f - tcl) * cc;
+      tbu = 1.f - (1.f - tru) * (1.f - cc) - (1.f - tcls) * cc;
     }
-    const float mm = 1.f / (1.f - ras * rbs[l]);
-    ra = ra + ta * rb[l] * tas * mm;
-    ta = ta * tbd[l] * mm;
-    ras = rbs[l] + tbu[l] * ras * tbd[l] * mm;
-    tas = tbu[l] * tas * mm;
+    lv.at(RB, l) = rb;
+    lv.at(RBS, l) = rbs;
+    lv.at(TBD, l) = tbd;
+    lv.at(TBU, l) = tbu;
+    const float mm = 1.f / (1.f - ras * rbs);
+    ra = ra + ta * rb * tas * mm;
+    ta = ta * tbd * mm;
+    ras = rbs + tbu * ras * tbd * mm;
+    tas = tbu * tas * mm;
   }
-  tl[NL] = ta;
-  rls[NL] = ras;
+  lv.at(TL, NL) = ta;
+  lv.at(RLS, NL) = ras;
   // Surface albedo: land and sea ice keep theirs, open water gets a
   // zenith-angle dependent one.
   const bool star = K.NSTARTEMP != 0.f;
@@ -556,16 +574,18 @@ __device__ __forceinline__ void swr_band(const Model& m, const PlanetConst& K, c
   ra = star ? (BAND == 0 ? nalb1 : nalb2) : albedo;
   // Upward pass from the surface; level l + 1's flux is complete once its
   // reflectances (ra, ras) are.
-#pragma unroll
+#pragma unroll 1
   for (int l = NL - 1; l >= -1; --l) {
     const int k = l + 1;
-    const float mm = 1.f / (1.f - rls[k] * ras);
-    fu[k] = -tl[k] * ra * mm * ftop;
-    fd[k] = tl[k] * mm * ftop;
+    const float tl = lv.at(TL, k);
+    const float mm = 1.f / (1.f - lv.at(RLS, k) * ras);
+    fu[k * stride] = -tl * ra * mm * ftop;
+    fd[k * stride] = tl * mm * ftop;
     if (l < 0) break;
-    const float dd = 1.f - ras * rbs[l];
-    ra = rb[l] + tbd[l] * ra * tbu[l] / dd;
-    ras = rbs[l] + tbu[l] * ras * tbu[l] / dd;
+    const float rbs = lv.at(RBS, l), tbu = lv.at(TBU, l);
+    const float dd = 1.f - ras * rbs;
+    ra = lv.at(RB, l) + lv.at(TBD, l) * ra * tbu / dd;
+    ras = rbs + tbu * ras * tbu / dd;
   }
 }
 
@@ -575,9 +595,11 @@ __device__ __forceinline__ void swr_band(const Model& m, const PlanetConst& K, c
 // shader's order (band 1 + band 2).
 template <int NL>
 __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
+  static_assert(NL <= SwrLevels::MAXLEV, "swr level state holds at most MAXLEV levels");
   constexpr int NP = NL + 1;
   constexpr int kCols = kBlock / 2;
   __shared__ float sfu[2][NP][kCols], sfd[2][NP][kCols];
+  __shared__ float levels[SwrLevels::kArrays * (SwrLevels::MAXLEV + 1) * kBlock];
   const Dims& d = m.d;
   const int warp = threadIdx.x >> 5;
   const int band = warp & 1;
@@ -599,16 +621,11 @@ __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
     const float ftop2 = K.ZSOLAR2 * K.GSOL0 * gdist2 * mu0;
     lit = ftop1 + ftop2 > 1.0e-6f;
     if (lit) {
-      float fu[NP], fd[NP];
+      const SwrLevels lv{levels};
       if (band == 0)
-        swr_band<NL, 0>(m, K, tb, SN, c, mu0, ftop1, fu, fd, alb);
+        swr_band<NL, 0>(m, K, tb, SN, c, mu0, ftop1, lv, &sfu[0][0][lc], &sfd[0][0][lc], kCols, alb);
       else
-        swr_band<NL, 1>(m, K, tb, SN, c, mu0, ftop2, fu, fd, alb);
-#pragma unroll
-      for (int l = 0; l < NP; ++l) {
-        sfu[band][l][lc] = fu[l];
-        sfd[band][l][lc] = fd[l];
-      }
+        swr_band<NL, 1>(m, K, tb, SN, c, mu0, ftop2, lv, &sfu[1][0][lc], &sfd[1][0][lc], kCols, alb);
     }
   }
   __syncthreads();  // both bands' fluxes are in, and both have read dalb, dsalb
@@ -678,10 +695,8 @@ __global__ void __launch_bounds__(kBlock) k_lwr_radstep(Model m) {
 #pragma unroll
   for (int l = 0; l < NP; ++l) dftu[l] = dftd[l] = 0.f;
   float taucs[NL], tau[NL], tausf[NL];
-#pragma unroll
   for (int j = 0; j < NL; ++j) {
     float taucc = 1.f, sumwv = 0.f, sumo3 = 0.f, sumco2 = 0.f;
-#pragma unroll
     for (int k = j; k < NL; ++k) {
       sumwv = sumwv + q[k];
       sumo3 = sumo3 + qo3[k];
@@ -702,7 +717,6 @@ __global__ void __launch_bounds__(kBlock) k_lwr_radstep(Model m) {
     }
     if (j == 0) {
       float tau0 = 1.f - ZERO;
-#pragma unroll
       for (int k = 0; k < NL; ++k) {
         tau0 = taucs[k] / tau0 * taucc0[k] * K.TPOFMT;
         tau0 = fminf(1.f - ZERO, fmaxf(ZERO, tau0));
@@ -719,7 +733,6 @@ __global__ void __launch_bounds__(kBlock) k_lwr_radstep(Model m) {
     dftu[j] = dftu[j] - bu[j + 1];
     dftd[j] = dftd[j] + bd[j];
     const float bdl = bd[j] - bd[j + 1];
-#pragma unroll
     for (int k = j; k < NL; ++k) {
       dftu[j] = dftu[j] - (bu[k + 2] - bu[k + 1]) * tau[k];
       dftd[k + 1] = dftd[k + 1] + bdl * tau[k];
@@ -840,7 +853,6 @@ __global__ void __launch_bounds__(kBlock) k_kuo(Model m) {
       }
     }
   }
-#pragma unroll
   for (int l = NM - 1; l >= 0; --l) {
     const int lp = l + 1;
     if (ilift == -1 && zdqtot[lp] > 0.f) {
@@ -887,7 +899,6 @@ __global__ void __launch_bounds__(kBlock) k_kuo(Model m) {
       }
     }
   }
-#pragma unroll
   for (int l = NM - 1; l >= 0; --l) {
     if (itop == l + 2) {
       const float p = dp * sg[l];
@@ -2047,5 +2058,28 @@ void phy_carbon(const Model& m, cudaStream_t st) { by_levels<Carbon>(m.d.L, m, s
 void phy_pack(const Model& m, cudaStream_t st) { by_levels<Pack>(m.d.L, m, st); }
 
 void phy_finite_check(const Model& m, cudaStream_t st) { k_finite<<<592, 256, 0, st>>>(m); }
+
+bool phy_launch_one(const Model& m, const std::string& kernel, cudaStream_t st) {
+  const int L = m.d.L;
+  if (kernel == "surflx")
+    by_levels<Surflx>(L, m, st);
+  else if (kernel == "vdiff")
+    by_levels<Vdiff>(L, m, st);
+  else if (kernel == "solang_mko3")
+    by_levels<SolangMko3>(L, m, st);
+  else if (kernel == "swr")
+    by_levels<Swr>(L, m, st);
+  else if (kernel == "lwr_radstep")
+    by_levels<LwrRadstep>(L, m, st);
+  else if (kernel == "kuo")
+    by_levels<Kuo>(L, m, st);
+  else if (kernel == "mkdca")
+    by_levels<Mkdca>(L, m, st);
+  else if (kernel == "rain_column")
+    by_levels<RainColumn>(L, m, st);
+  else
+    return false;
+  return true;
+}
 
 }  // namespace exogcm

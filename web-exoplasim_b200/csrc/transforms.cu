@@ -77,6 +77,18 @@ __global__ void k_dlambda(const float* __restrict__ a, float* __restrict__ b, in
   b[at + 1] = re * (float)m;
 }
 
+// The same on the optimized path's m-major Fourier planes (coefficient
+// (m, lat) at 2 * (m * NLAT + lat)).
+__global__ void k_dlambda_m_major(const float* __restrict__ a, float* __restrict__ b, int n, int nlat, int ntp1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int m = (i / nlat) % ntp1;
+  const size_t at = 2 * (size_t)i;
+  const float re = a[at], im = a[at + 1];
+  b[at] = -im * (float)m;
+  b[at + 1] = re * (float)m;
+}
+
 // ---------------------------------------------------------------- Legendre
 // Inverse transforms (sp2fc, sp2fcdmu, dv2uv): output (plane, lat, m) sums
 // modes n = m..NTRU of its plane. A block stages a tile of spectral planes
@@ -315,6 +327,7 @@ int dft_rows_per_block(const Dims& d) { return d.NLAT == 96 ? 24 : 32; }
 
 void tr_init() {
   leg_init();
+  fft_init();
   allow_smem(k_dft_forward);
   allow_smem(k_dft_inverse);
   allow_smem(k_leg_inverse);
@@ -343,6 +356,10 @@ void tr_fourier_inverse(const Model& m, const float* c, float* g, int planes, cu
 
 void tr_dlambda(const Model& m, const float* a, float* b, int planes, cudaStream_t st) {
   const int n = planes * m.d.NLAT * m.d.NTP1;
+  if (m.mode == 1) {
+    k_dlambda_m_major<<<(n + 255) / 256, 256, 0, st>>>(a, b, n, m.d.NLAT, m.d.NTP1);
+    return;
+  }
   k_dlambda<<<(n + 255) / 256, 256, 0, st>>>(a, b, n, m.d.NTP1, m.d.NFC);
 }
 
