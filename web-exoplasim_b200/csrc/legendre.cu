@@ -37,7 +37,6 @@ namespace exogcm {
 namespace {
 
 constexpr int kForwardThreads = 256;
-constexpr int kForwardGroup = 4;  // wavenumbers per forward block
 constexpr size_t kInverseBudget = 48 * 1024;
 constexpr size_t kSmemBudget = 100 * 1024;
 
@@ -194,91 +193,117 @@ struct SymIn {
 // KIND 3: qtend, in = {u, v, source} (qtend.wgsl).
 // Staged per (input, plane, m, pair): (north + south, north - south) of the
 // real and imaginary parts, read from the m-major planes as contiguous runs
-// of latitudes. For mode (m, n) the shader's north + s * south with
-// s = (-1)^(m+n) is the sum for even n - m and the difference for odd.
+// of latitudes, and the group's table slices ([table][pair][term]). For mode
+// (m, n) the shader's north + s * south with s = (-1)^(m+n) is the sum for
+// even n - m and the difference for odd. A thread owns one term (mode) for
+// kFwdPlanes planes, so every table value it loads serves all of them.
+constexpr int kFwdTile = 8;    // planes per block
+constexpr int kFwdPlanes = 4;  // planes per thread
+
+template <int KIND>
+struct FwdTables {
+  static constexpr int N = KIND == 0 ? 1 : KIND == 3 ? 3 : KIND == 2 ? 3 : 2;
+};
+
 template <int KIND, int NIN>
 __global__ void __launch_bounds__(kForwardThreads) k_sym_forward(SymIn<NIN> in, float* __restrict__ out0,
-                                                                 float* __restrict__ out1, int planes, int tile,
+                                                                 float* __restrict__ out1, int planes, int group,
                                                                  SharedTabs sh, const float* __restrict__ q, Dims d) {
-  extern __shared__ float4 pm[];  // [NIN][tile][kForwardGroup][JH]
+  constexpr int NTAB = FwdTables<KIND>::N;
+  extern __shared__ float4 pm[];  // [NIN][kFwdTile][group][JH], then the tables
   const int JH = d.NLAT / 2;
-  const int m0 = blockIdx.x * kForwardGroup;
-  const int m1 = min(m0 + kForwardGroup, d.NTP1);
+  const int m0 = blockIdx.x * group;
+  const int m1 = min(m0 + group, d.NTP1);
   const int gm = m1 - m0;
   const int w0 = first_mode(m0, d.NTP1);
   const int nt = first_mode(m1, d.NTP1) - w0;
-  const int p0 = blockIdx.y * tile;
-  const int np = min(tile, planes - p0);
+  const int p0 = blockIdx.y * kFwdTile;
+  const int np = min(kFwdTile, planes - p0);
   const size_t plane_floats = (size_t)d.NLAT * d.NFC;
+  float* tab = reinterpret_cast<float*>(pm + (size_t)NIN * kFwdTile * group * JH);  // [NTAB][JH][nt]
+  // Tables in KIND order: 0: q; 1: qe, qm; 2: qe, qm, qq; 3: qe, qc, qm.
+  const float* tsrc[3] = {KIND == 0 ? q : sh.qe, KIND == 3 ? sh.qc : sh.qm, KIND == 2 ? sh.qq : sh.qm};
+#pragma unroll
+  for (int k = 0; k < NTAB; ++k)
+    for (int i = threadIdx.x; i < JH * nt; i += blockDim.x) {
+      const int l = i / nt, t = i - l * nt;
+      tab[(k * JH + l) * nt + t] = __ldg(tsrc[k] + (size_t)l * d.NCSP + w0 + t);
+    }
   for (int k = 0; k < NIN; ++k) {
-    for (int i = threadIdx.x; i < np * gm * JH; i += blockDim.x) {
+    for (int i = threadIdx.x; i < kFwdTile * gm * JH; i += blockDim.x) {
       const int j = i % JH;
       const int mi = (i / JH) % gm;
       const int p = i / (JH * gm);
-      const float2* row =
-          reinterpret_cast<const float2*>(in.p[k] + (size_t)(p0 + p) * plane_floats) + (size_t)(m0 + mi) * d.NLAT;
-      const float2 n = row[j], s = row[d.NLAT - 1 - j];
-      pm[((k * tile + p) * kForwardGroup + mi) * JH + j] = make_float4(n.x + s.x, n.y + s.y, n.x - s.x, n.y - s.y);
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (p < np) {
+        const float2* row = reinterpret_cast<const float2*>(in.p[k] + (size_t)(p0 + p) * plane_floats) +
+                            (size_t)(m0 + mi) * d.NLAT;
+        const float2 n = row[j], s = row[d.NLAT - 1 - j];
+        v = make_float4(n.x + s.x, n.y + s.y, n.x - s.x, n.y - s.y);
+      }
+      pm[((k * kFwdTile + p) * group + mi) * JH + j] = v;
     }
   }
   __syncthreads();
-  for (int o = threadIdx.x; o < np * nt; o += blockDim.x) {
+  constexpr int NPG = kFwdTile / kFwdPlanes;
+  for (int o = threadIdx.x; o < nt * NPG; o += blockDim.x) {
     const int t = o % nt;
-    const int p = o / nt;
+    const int pg = o / nt;
     const int w = w0 + t;
     const int m = sh.mode_m[w], n = sh.mode_n[w];
     const int mi = m - m0;
     const bool even = ((m + n) & 1) == 0;
-    const size_t at = (size_t)(p0 + p) * d.NRSP + 2 * w;
-    const float4* A = pm + ((size_t)(0 * tile + p) * kForwardGroup + mi) * JH;
-    const float4* B = pm + ((size_t)((NIN > 1 ? 1 : 0) * tile + p) * kForwardGroup + mi) * JH;
-    const float4* C = pm + ((size_t)((NIN > 2 ? 2 : 0) * tile + p) * kForwardGroup + mi) * JH;
-    if (KIND == 0) {
-      float re = 0.f, im = 0.f;
-      for (int l = 0; l < JH; ++l) {
-        const float qq = __ldg(q + l * d.NCSP + w);
-        const float4 f = A[l];
-        re = fmaf(qq, even ? f.x : f.z, re);
-        im = fmaf(qq, even ? f.y : f.w, im);
-      }
-      out0[at] = re;
-      out0[at + 1] = im;
-    } else if (KIND == 1 || KIND == 2) {
-      float dre = 0.f, dim = 0.f, zre = 0.f, zim = 0.f;
-      for (int l = 0; l < JH; ++l) {
-        const float e = __ldg(sh.qe + l * d.NCSP + w), mq = __ldg(sh.qm + l * d.NCSP + w);
-        const float4 U = A[l], V = B[l];
-        // north - s * south and north + s * south of u and v
-        const float dure = even ? U.z : U.x, duim = even ? U.w : U.y;
-        const float dvre = even ? V.z : V.x, dvim = even ? V.w : V.y;
-        const float sure = even ? U.x : U.z, suim = even ? U.y : U.w;
-        const float svre = even ? V.x : V.z, svim = even ? V.y : V.w;
-        if (KIND == 2) {
-          const float q2 = __ldg(sh.qq + l * d.NCSP + w);
-          const float4 Kf = C[l];
-          dre = dre + q2 * (even ? Kf.x : Kf.z);
-          dim = dim + q2 * (even ? Kf.y : Kf.w);
+    const float* tq = tab + t;
+    // pm row of input k, plane p of this thread's group, at pair l: pin(k, pp)[l]
+    auto pin = [&](int k, int pp) { return pm + ((size_t)(k * kFwdTile + pg * kFwdPlanes + pp) * group + mi) * JH; };
+    float r0[kFwdPlanes] = {}, r1[kFwdPlanes] = {}, r2[kFwdPlanes] = {}, r3[kFwdPlanes] = {};
+    for (int l = 0; l < JH; ++l) {
+      const float qa = tq[l * nt];
+      const float qb = NTAB > 1 ? tq[(JH + l) * nt] : 0.f;
+      const float qc = NTAB > 2 ? tq[(2 * JH + l) * nt] : 0.f;
+#pragma unroll
+      for (int pp = 0; pp < kFwdPlanes; ++pp) {
+        if (KIND == 0) {
+          const float4 f = pin(0, pp)[l];
+          r0[pp] = fmaf(qa, even ? f.x : f.z, r0[pp]);
+          r1[pp] = fmaf(qa, even ? f.y : f.w, r1[pp]);
+        } else if (KIND == 1 || KIND == 2) {
+          const float e = qa, mq = qb;
+          const float4 U = pin(0, pp)[l], V = pin(NIN > 1 ? 1 : 0, pp)[l];
+          // north - s * south and north + s * south of u and v
+          const float dure = even ? U.z : U.x, duim = even ? U.w : U.y;
+          const float dvre = even ? V.z : V.x, dvim = even ? V.w : V.y;
+          const float sure = even ? U.x : U.z, suim = even ? U.y : U.w;
+          const float svre = even ? V.x : V.z, svim = even ? V.y : V.w;
+          if (KIND == 2) {
+            const float q2 = qc;
+            const float4 Kf = pin(NIN > 2 ? 2 : 0, pp)[l];
+            r0[pp] = r0[pp] + q2 * (even ? Kf.x : Kf.z);
+            r1[pp] = r1[pp] + q2 * (even ? Kf.y : Kf.w);
+          }
+          r0[pp] = r0[pp] - e * dvre - mq * suim;
+          r1[pp] = r1[pp] - e * dvim + mq * sure;
+          r2[pp] = r2[pp] + e * dure - mq * svim;
+          r3[pp] = r3[pp] + e * duim + mq * svre;
+        } else {
+          const float e = qa, c = qb, mq = qc;
+          const float4 U = pin(0, pp)[l], V = pin(NIN > 1 ? 1 : 0, pp)[l], X = pin(NIN > 2 ? 2 : 0, pp)[l];
+          r0[pp] = r0[pp] + e * (even ? V.z : V.x) + c * (even ? X.x : X.z) + mq * (even ? U.y : U.w);
+          r1[pp] = r1[pp] + e * (even ? V.w : V.y) + c * (even ? X.y : X.w) - mq * (even ? U.x : U.z);
         }
-        dre = dre - e * dvre - mq * suim;
-        dim = dim - e * dvim + mq * sure;
-        zre = zre + e * dure - mq * svim;
-        zim = zim + e * duim + mq * svre;
       }
-      out0[at] = dre;
-      out0[at + 1] = dim;
-      out1[at] = zre;
-      out1[at + 1] = zim;
-    } else {
-      float re = 0.f, im = 0.f;
-      for (int l = 0; l < JH; ++l) {
-        const float e = __ldg(sh.qe + l * d.NCSP + w), c = __ldg(sh.qc + l * d.NCSP + w),
-                    mq = __ldg(sh.qm + l * d.NCSP + w);
-        const float4 U = A[l], V = B[l], X = C[l];
-        re = re + e * (even ? V.z : V.x) + c * (even ? X.x : X.z) + mq * (even ? U.y : U.w);
-        im = im + e * (even ? V.w : V.y) + c * (even ? X.y : X.w) - mq * (even ? U.x : U.z);
+    }
+#pragma unroll
+    for (int pp = 0; pp < kFwdPlanes; ++pp) {
+      const int p = pg * kFwdPlanes + pp;
+      if (p >= np) break;
+      const size_t at = (size_t)(p0 + p) * d.NRSP + 2 * w;
+      out0[at] = r0[pp];
+      out0[at + 1] = r1[pp];
+      if (KIND == 1 || KIND == 2) {
+        out1[at] = r2[pp];
+        out1[at + 1] = r3[pp];
       }
-      out0[at] = re;
-      out0[at + 1] = im;
     }
   }
 }
@@ -302,16 +327,17 @@ InverseTiling inverse_tiling(const Dims& d, int nin) {
   }
 }
 
-// Forward planes per block: the largest of 32, 16, 8, 4, 2 whose staged
-// sums and differences fit the budget.
-size_t forward_smem(const Dims& d, int nin, int tile) {
-  return (size_t)nin * tile * kForwardGroup * (d.NLAT / 2) * 16;
+// Forward: kFwdTile planes per block and the largest group of 4, 2 or 1
+// wavenumbers whose staged sums, differences and table slices fit about
+// 60 KB (three blocks per SM).
+size_t forward_smem(const Dims& d, int nin, int ntab, int group) {
+  return (size_t)nin * kFwdTile * group * (d.NLAT / 2) * 16 + (size_t)ntab * (d.NLAT / 2) * group_terms(d, group) * 4;
 }
 
-int forward_tile_for(const Dims& d, int nin) {
-  for (int tile = 32; tile > 2; tile /= 2)
-    if (forward_smem(d, nin, tile) <= kSmemBudget) return tile;
-  return 2;
+int forward_group_for(const Dims& d, int nin, int ntab) {
+  for (int group = 4; group > 1; group /= 2)
+    if (forward_smem(d, nin, ntab, group) <= 60 * 1024) return group;
+  return 1;
 }
 
 template <typename K>
@@ -322,10 +348,11 @@ void allow_smem(K kernel) {
 template <int KIND, int NIN>
 void launch_sym_forward(const Model& m, SymIn<NIN> in, float* out0, float* out1, int planes, const float* q,
                         cudaStream_t st) {
-  const int tile = forward_tile_for(m.d, NIN);
-  dim3 grid((m.d.NTP1 + kForwardGroup - 1) / kForwardGroup, (planes + tile - 1) / tile);
-  k_sym_forward<KIND, NIN><<<grid, kForwardThreads, forward_smem(m.d, NIN, tile), st>>>(in, out0, out1, planes, tile,
-                                                                                      m.sh, q, m.d);
+  constexpr int NTAB = FwdTables<KIND>::N;
+  const int group = forward_group_for(m.d, NIN, NTAB);
+  dim3 grid((m.d.NTP1 + group - 1) / group, (planes + kFwdTile - 1) / kFwdTile);
+  k_sym_forward<KIND, NIN><<<grid, kForwardThreads, forward_smem(m.d, NIN, NTAB, group), st>>>(
+      in, out0, out1, planes, group, m.sh, q, m.d);
 }
 
 }  // namespace
