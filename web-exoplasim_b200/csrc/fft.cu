@@ -9,8 +9,8 @@
 // elements n1 + 32 n2 of its row; a radix-R step in registers is followed by
 // a 32-point decimation-in-frequency FFT across the lanes (five xor-shuffle
 // butterfly stages). Twiddles come from a table of e^{2 pi i j / N} built in
-// FP64 on the host and rounded once. Shared memory reorders the bit-reversed
-// FFT output.
+// FP64 on the host and rounded once. Warp shuffles put the bit-reversed FFT
+// output back in natural order.
 //
 // The optimized path stores Fourier planes m-major (coefficient (m, lat) at
 // 2 * (m * NLAT + lat)), so that the Legendre transforms on either side
@@ -26,7 +26,7 @@ namespace exogcm {
 
 namespace {
 
-constexpr int kWarps = 8;
+constexpr int kWarps = 4;
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -90,11 +90,29 @@ __device__ __forceinline__ void warp_fft(float2 (&x)[B][R], const float2* tw, in
 
 constexpr int kRowsPerWarp = 2;
 
-// Shared memory of a plane block: twiddles, the plane's coefficients
-// [ntp1][nlat + 1] and per-warp row buffers [kWarps][kRowsPerWarp][M + 1].
+// After warp_fft lane l holds Z[R * bitrev5(l) + r] in x[r]; this returns
+// y[r'] = Z[lane + 32 r'] for the calling lane. Element k sits in lane
+// bitrev5(k / R), register k % R: R shuffles of every register, one kept.
+template <int R>
+__device__ __forceinline__ void natural_order(const float2 (&x)[R], float2 (&y)[R], int lane) {
+#pragma unroll
+  for (int rp = 0; rp < R; ++rp) {
+    const int k = lane + 32 * rp;
+    const int src = bitrev5(k / R), reg = k % R;
+    float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const float a = __shfl_sync(0xffffffffu, x[r].x, src), b = __shfl_sync(0xffffffffu, x[r].y, src);
+      if (reg == r) v = make_float2(a, b);
+    }
+    y[rp] = v;
+  }
+}
+
+// Shared memory of a plane block: twiddles and the plane's coefficients
+// [ntp1][nlat + 1] (the odd row pitch keeps column reads conflict-free).
 inline size_t plane_smem(int nlon, int nlat, int ntp1) {
-  const int M = nlon / 2;
-  return ((size_t)nlon + (size_t)ntp1 * (nlat + 1) + (size_t)kWarps * kRowsPerWarp * (M + 1)) * sizeof(float2);
+  return ((size_t)nlon + (size_t)ntp1 * (nlat + 1)) * sizeof(float2);
 }
 
 // gp2fc for one plane per block: rows of N grid values -> m-major
@@ -105,14 +123,12 @@ __global__ void __launch_bounds__(kWarps * 32) k_fft_forward(const float* __rest
   constexpr int M = 32 * R, N = 2 * M, B = kRowsPerWarp;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* fc = tw + N;                        // [ntp1][nlat + 1]
-  float2* zs = fc + (size_t)ntp1 * (nlat + 1);  // [kWarps][B][M + 1]
+  float2* fc = tw + N;  // [ntp1][nlat + 1]
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const float inv_n = 1.f / (float)N;
   const size_t plane = blockIdx.x;
-  float2* zw = zs + (size_t)warp * B * (M + 1);
   for (int row0 = warp * B; row0 < nlat; row0 += kWarps * B) {
     float2 x[B][R];
 #pragma unroll
@@ -122,26 +138,31 @@ __global__ void __launch_bounds__(kWarps * 32) k_fft_forward(const float* __rest
       for (int r = 0; r < R; ++r) x[b][r] = in[lane + 32 * r];
     }
     warp_fft<B, R, -1>(x, tw, N, lane);
-    const int k1 = bitrev5(lane);
-#pragma unroll
-    for (int b = 0; b < B; ++b)
-#pragma unroll
-      for (int r = 0; r < R; ++r) zw[b * (M + 1) + R * k1 + r] = x[b][r];
-    __syncwarp();
 #pragma unroll
     for (int b = 0; b < B; ++b) {
-      const float2* z = zw + b * (M + 1);
-      for (int m = lane; m < ntp1; m += 32) {
-        const float2 zm = z[m];
-        const float2 zc = conj2(z[(M - m) % M]);
-        const float2 even = make_float2(0.5f * (zm.x + zc.x), 0.5f * (zm.y + zc.y));
-        // (zm - zc) / 2i = ((zm - zc).y, -(zm - zc).x) / 2
-        const float2 odd = make_float2(0.5f * (zm.y - zc.y), -0.5f * (zm.x - zc.x));
-        const float2 gm = cadd(even, cmul(twiddle<-1>(tw, m, N), odd));
-        fc[m * (nlat + 1) + row0 + b] = make_float2(gm.x * inv_n, m == 0 ? 0.f : gm.y * inv_n);
+      float2 y[R];
+      natural_order<R>(x[b], y, lane);
+#pragma unroll
+      for (int rp = 0; rp < R; ++rp) {
+        // Z[m] and Z[(M - m) % M] for m = lane + 32 rp: the second sits in
+        // lane 32 - lane, register R - 1 - rp (lane 0: lane 0, register
+        // (R - rp) % R).
+        const float2 zm = y[rp];
+        const float ax = __shfl_sync(0xffffffffu, y[R - 1 - rp].x, (32 - lane) & 31);
+        const float ay = __shfl_sync(0xffffffffu, y[R - 1 - rp].y, (32 - lane) & 31);
+        const float bx = __shfl_sync(0xffffffffu, y[(R - rp) % R].x, 0);
+        const float by = __shfl_sync(0xffffffffu, y[(R - rp) % R].y, 0);
+        const float2 zc = lane == 0 ? make_float2(bx, -by) : make_float2(ax, -ay);
+        const int m = lane + 32 * rp;
+        if (m < ntp1) {
+          const float2 even = make_float2(0.5f * (zm.x + zc.x), 0.5f * (zm.y + zc.y));
+          // (zm - zc) / 2i = ((zm - zc).y, -(zm - zc).x) / 2
+          const float2 odd = make_float2(0.5f * (zm.y - zc.y), -0.5f * (zm.x - zc.x));
+          const float2 gm = cadd(even, cmul(twiddle<-1>(tw, m, N), odd));
+          fc[m * (nlat + 1) + row0 + b] = make_float2(gm.x * inv_n, m == 0 ? 0.f : gm.y * inv_n);
+        }
       }
     }
-    __syncwarp();
   }
   __syncthreads();
   float2* out = reinterpret_cast<float2*>(c) + plane * nlat * ntp1;
@@ -159,8 +180,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_fft_inverse(const float* __rest
   constexpr int M = 32 * R, N = 2 * M, B = kRowsPerWarp;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* fc = tw + N;                          // [ntp1][nlat + 1]
-  float2* gs = fc + (size_t)ntp1 * (nlat + 1);  // [kWarps][B][M + 1]
+  float2* fc = tw + N;  // [ntp1][nlat + 1]
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
   const size_t plane = blockIdx.x;
   const float2* in = reinterpret_cast<const float2*>(c) + plane * nlat * ntp1;
@@ -172,7 +192,6 @@ __global__ void __launch_bounds__(kWarps * 32) k_fft_inverse(const float* __rest
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float2* gw = gs + (size_t)warp * B * (M + 1);
   for (int row0 = warp * B; row0 < nlat; row0 += kWarps * B) {
     float2 x[B][R];
 #pragma unroll
@@ -190,19 +209,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_fft_inverse(const float* __rest
       }
     }
     warp_fft<B, R, 1>(x, tw, N, lane);
-    const int k1 = bitrev5(lane);
-#pragma unroll
-    for (int b = 0; b < B; ++b)
-#pragma unroll
-      for (int r = 0; r < R; ++r) gw[b * (M + 1) + R * k1 + r] = x[b][r];
-    __syncwarp();
 #pragma unroll
     for (int b = 0; b < B; ++b) {
+      float2 y[R];
+      natural_order<R>(x[b], y, lane);
       float2* out = reinterpret_cast<float2*>(g + (plane * nlat + row0 + b) * N);
 #pragma unroll
-      for (int r = 0; r < R; ++r) out[lane + 32 * r] = gw[b * (M + 1) + lane + 32 * r];
+      for (int r = 0; r < R; ++r) out[lane + 32 * r] = y[r];
     }
-    __syncwarp();
   }
 }
 
@@ -222,7 +236,7 @@ void fft_init() {
   allow_plane_smem(k_fft_inverse<3>);
 }
 
-// The plane blocks need NLAT to be a multiple of kWarps * kRowsPerWarp (16):
+// The plane blocks need NLAT to be a multiple of kWarps * kRowsPerWarp (8):
 // NLAT is 32, 64 or 96.
 void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st) {
   const float2* tw = reinterpret_cast<const float2*>(m.sh.tw);

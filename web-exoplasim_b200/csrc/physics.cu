@@ -691,55 +691,105 @@ __global__ void __launch_bounds__(kBlock) k_lwr_radstep(Model m) {
     qco2[l] = K.ZFCO2_ZZF2 * sfac * F.dqco2[l * SN + c];
     taucc0[l] = 1.f - F.dcc[l * SN + c] * (1.f - expf(tb[m.to.lwr_zzf3 + l] * F.dql[l * SN + c] * dp));
   }
-  float dftu[NL + 1], dftd[NL + 1];
+  // The transmissivity between levels j and k (k >= j) depends on the
+  // absorber sums from j down to k. Row j = 0 also sets the layer Planck
+  // terms bu, bd; every row j adds its fluxes. The outer loop over j is
+  // unrolled (j-indexed values in registers); the inner loop over k stays
+  // rolled, reading the absorber amounts, bu and dftd from this thread's
+  // column of shared memory ([level][thread], conflict-free, private to the
+  // thread), so the code stays small and nothing spills.
+  __shared__ float s_q[NL][kBlock], s_o3[NL][kBlock], s_co2[NL][kBlock], s_tc[NL][kBlock];
+  __shared__ float s_bu[NL + 2][kBlock], s_dftd[NL + 1][kBlock];
+  const int tx = threadIdx.x;
 #pragma unroll
-  for (int l = 0; l < NP; ++l) dftu[l] = dftd[l] = 0.f;
-  float taucs[NL], tau[NL], tausf[NL];
-  for (int j = 0; j < NL; ++j) {
+  for (int l = 0; l < NL; ++l) {
+    s_q[l][tx] = q[l];
+    s_o3[l][tx] = qo3[l];
+    s_co2[l][tx] = qco2[l];
+    s_tc[l][tx] = taucc0[l];
+  }
+#pragma unroll
+  for (int l = 0; l < NP; ++l) s_dftd[l][tx] = 0.f;
+  // Clear-sky transmissivity for absorber sums (lwr.wgsl's band fits).
+  auto clear_sky = [&](float sumwv, float sumo3, float sumco2) {
+    float ah2o = sumwv <= 0.01f ? 0.846f * fpow(sumwv + 3.59e-5f, 0.243f) - K.ZH2O0A
+                                : 0.24f * (logf(sumwv + 0.01f) * INV_LN10) + K.ZAH2OC;
+    if (K.TH2OC > 0.f) ah2o = fminf(ah2o + (1.f - expf(-K.TH2OC * sumwv)), 1.f);
+    const float aco2 = sumco2 <= 1.f ? 0.0676f * fpow(sumco2 + 0.01022f, 0.421f) - K.ZCO20
+                                     : 0.0546f * (logf(sumco2) * INV_LN10) + K.ZACO2C;
+    const float th2o = sumwv <= 2.f ? 1.f - (0.832f * fpow(sumwv + 0.0286f, 0.26f) - K.ZH2O0)
+                                    : fmaxf(0.f, K.ZTH2OC - 0.1196f * logf(sumwv - 0.6931f));
+    const float ao3 = sumo3 <= 0.01f ? 0.209f * fpow(sumo3 + 7.0e-5f, 0.436f) - K.ZAO30
+                                     : 0.0212f * (logf(sumo3) * INV_LN10) + K.ZAO3C;
+    return fminf(1.f - ZERO, fmaxf(ZERO, 1.f - ah2o - ao3 - aco2 * th2o));
+  };
+  float dftu[NL + 1], tausf[NL];
+  // Row j = 0 (unrolled): transmissivities from the top, then bu, bd.
+  {
+    float taucs[NL], tau[NL];
     float taucc = 1.f, sumwv = 0.f, sumo3 = 0.f, sumco2 = 0.f;
-    for (int k = j; k < NL; ++k) {
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
       sumwv = sumwv + q[k];
       sumo3 = sumo3 + qo3[k];
       sumco2 = sumco2 + qco2[k];
-      float ah2o = sumwv <= 0.01f ? 0.846f * fpow(sumwv + 3.59e-5f, 0.243f) - K.ZH2O0A
-                                  : 0.24f * (logf(sumwv + 0.01f) * INV_LN10) + K.ZAH2OC;
-      if (K.TH2OC > 0.f) ah2o = fminf(ah2o + (1.f - expf(-K.TH2OC * sumwv)), 1.f);
-      const float aco2 = sumco2 <= 1.f ? 0.0676f * fpow(sumco2 + 0.01022f, 0.421f) - K.ZCO20
-                                       : 0.0546f * (logf(sumco2) * INV_LN10) + K.ZACO2C;
-      const float th2o = sumwv <= 2.f ? 1.f - (0.832f * fpow(sumwv + 0.0286f, 0.26f) - K.ZH2O0)
-                                      : fmaxf(0.f, K.ZTH2OC - 0.1196f * logf(sumwv - 0.6931f));
-      const float ao3 = sumo3 <= 0.01f ? 0.209f * fpow(sumo3 + 7.0e-5f, 0.436f) - K.ZAO30
-                                       : 0.0212f * (logf(sumo3) * INV_LN10) + K.ZAO3C;
-      const float cs = fminf(1.f - ZERO, fmaxf(ZERO, 1.f - ah2o - ao3 - aco2 * th2o));
+      const float cs = clear_sky(sumwv, sumo3, sumco2);
       taucs[k] = cs;
       taucc = taucc * taucc0[k];
       tau[k] = cs * taucc;
     }
-    if (j == 0) {
-      float tau0 = 1.f - ZERO;
-      for (int k = 0; k < NL; ++k) {
-        tau0 = taucs[k] / tau0 * taucc0[k] * K.TPOFMT;
-        tau0 = fminf(1.f - ZERO, fmaxf(ZERO, tau0));
-        if ((st4[k] - st4h[k]) * (st4[k] - st4h[k + 1]) > 0.f) {
-          bd[k + 1] = 0.5f * st4[k] + 0.25f * (st4h[k] + st4h[k + 1]);
-          bu[k + 1] = bd[k + 1];
-        } else {
-          bd[k + 1] = (st4h[k + 1] - tau0 * st4h[k]) / (1.f - tau0) - (st4h[k] - st4h[k + 1]) / logf(tau0);
-          bu[k + 1] = st4h[k] + st4h[k + 1] - bd[k + 1];
-        }
-        tau0 = taucs[k];
+    float tau0 = 1.f - ZERO;
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+      tau0 = taucs[k] / tau0 * taucc0[k] * K.TPOFMT;
+      tau0 = fminf(1.f - ZERO, fmaxf(ZERO, tau0));
+      if ((st4[k] - st4h[k]) * (st4[k] - st4h[k + 1]) > 0.f) {
+        bd[k + 1] = 0.5f * st4[k] + 0.25f * (st4h[k] + st4h[k + 1]);
+        bu[k + 1] = bd[k + 1];
+      } else {
+        bd[k + 1] = (st4h[k + 1] - tau0 * st4h[k]) / (1.f - tau0) - (st4h[k] - st4h[k + 1]) / logf(tau0);
+        bu[k + 1] = st4h[k] + st4h[k + 1] - bd[k + 1];
       }
+      tau0 = taucs[k];
     }
-    dftu[j] = dftu[j] - bu[j + 1];
-    dftd[j] = dftd[j] + bd[j];
-    const float bdl = bd[j] - bd[j + 1];
-    for (int k = j; k < NL; ++k) {
-      dftu[j] = dftu[j] - (bu[k + 2] - bu[k + 1]) * tau[k];
-      dftd[k + 1] = dftd[k + 1] + bdl * tau[k];
+#pragma unroll
+    for (int l = 1; l < NL + 2; ++l) s_bu[l][tx] = bu[l];
+    float u = 0.f - bu[1];
+    s_dftd[0][tx] = 0.f + bd[0];
+    const float bdl = bd[0] - bd[1];
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+      u = u - (bu[k + 2] - bu[k + 1]) * tau[k];
+      s_dftd[k + 1][tx] = s_dftd[k + 1][tx] + bdl * tau[k];
     }
-    tausf[j] = tau[NL - 1];
+    dftu[0] = u;
+    tausf[0] = tau[NL - 1];
   }
-  dftu[NL] = dftu[NL] - bu[NP];
+  // Rows j >= 1: one rolled pass over k per row.
+#pragma unroll
+  for (int j = 1; j < NL; ++j) {
+    float taucc = 1.f, sumwv = 0.f, sumo3 = 0.f, sumco2 = 0.f, tau = 0.f;
+    float u = 0.f - bu[j + 1];
+    s_dftd[j][tx] = s_dftd[j][tx] + bd[j];
+    const float bdl = bd[j] - bd[j + 1];
+#pragma unroll 1
+    for (int k = j; k < NL; ++k) {
+      sumwv = sumwv + s_q[k][tx];
+      sumo3 = sumo3 + s_o3[k][tx];
+      sumco2 = sumco2 + s_co2[k][tx];
+      const float cs = clear_sky(sumwv, sumo3, sumco2);
+      taucc = taucc * s_tc[k][tx];
+      tau = cs * taucc;
+      u = u - (s_bu[k + 2][tx] - s_bu[k + 1][tx]) * tau;
+      s_dftd[k + 1][tx] = s_dftd[k + 1][tx] + bdl * tau;
+    }
+    dftu[j] = u;
+    tausf[j] = tau;
+  }
+  float dftd[NL + 1];
+#pragma unroll
+  for (int l = 0; l < NP; ++l) dftd[l] = s_dftd[l][tx];
+  dftu[NL] = 0.f - bu[NP];
   dftd[NL] = dftd[NL] + bd[NL];
   const float reflected = (1.f - eps) * dftd[NL];
 #pragma unroll
