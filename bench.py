@@ -40,6 +40,7 @@ def parse():
     ap.add_argument("--slots", type=int, default=128)
     ap.add_argument("--chunk", type=int, default=32, help="model steps per engine call (one CUDA graph)")
     ap.add_argument("--no-baseline", action="store_true", help="skip the timed CPU baseline sample")
+    ap.add_argument("--no-served", action="store_true", help="skip the continuous-batching latency sample")
     return ap.parse_args()
 
 
@@ -181,6 +182,25 @@ def cpu_baseline_sample(planet_list, threads, steps):
     return threads * steps * DAYS_PER_STEP / dt, dt
 
 
+def served_sample(seconds, slots, rate, seed=7):
+    """Continuous batching of T42 L10 runs of 0.5-2 simulated days arriving
+    as a Poisson stream: time from arrival to result (p50, p99) and the
+    simulated days served per second. Planets are built before the window
+    (they are the clients' input); admission, set-up and stepping are in
+    it."""
+    serving = importlib.import_module("web-exoplasim_b200.serving")
+    planets = importlib.import_module("web-exoplasim_b200.planets")
+    reqs = serving.poisson_requests(rate, seconds, seed=seed, max_days=2.0, min_days=0.5, resolutions=((42, 10),))
+    for r in reqs:
+        r.planet = planets.make_planet(r.seed, truncation=42, levels=10)
+    server = serving.Server({(42, 10): slots}, chunk=16, keep_results=False)
+    rep = server.run(reqs, window=seconds * 10, drain=True)
+    return {"p50_s": round(rep["p50_s"], 3), "p99_s": round(rep["p99_s"], 3), "completed": rep["completed"],
+            "failed": rep["failed"], "sim_days_per_s": round(rep["sim_days_per_s"], 2),
+            "requests": len(reqs), "arrival_rate_per_s": rate, "run_days": "0.5-2 (uniform)", "slots": slots,
+            "window_s": round(rep["window_s"], 2)}
+
+
 def reference_arm(args, rank):
     if rank != 0:
         return
@@ -298,6 +318,12 @@ def main():
 
     launches = engine.graph_launches(1) * args.steps
     roof = roofline(engine, peaks) if rank == 0 else None
+    tuning = engine.tuning()
+    served = None
+    if rank == 0 and world == 1 and not args.no_served:
+        engine.close()
+        engine = None
+        served = served_sample(seconds=4.0, slots=64, rate=16.0)
     cpu = None
     if rank == 0 and world == 1 and not args.no_baseline:
         v, dt = cpu_baseline_sample(plist, 1, 4)
@@ -320,12 +346,14 @@ def main():
                     "d2h_bytes_per_step": int(d2h_per_step)},
             "gpu_launches": launches,
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks.summary(),
+            "served": served, "tuning": tuning,
         }
         print(json.dumps(line), flush=True)
-    unstable = engine.unstable()
-    if unstable.any() and rank == 0:
-        print(json.dumps({"warning": f"{int(unstable.sum())} planets became unstable"}), file=sys.stderr)
-    engine.close()
+    if engine is not None:
+        unstable = engine.unstable()
+        if unstable.any() and rank == 0:
+            print(json.dumps({"warning": f"{int(unstable.sum())} planets became unstable"}), file=sys.stderr)
+        engine.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()

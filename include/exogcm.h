@@ -90,7 +90,10 @@ int exogcm_last_error(char* buffer, size_t size);
 
 /* Creates an engine of `slots` planet slots at T`truncation` L`levels` on
  * the current CUDA device (STEPPER.context, stepper/index.ts:94-118).
- * `mode` 0 plain FP32 transforms, 1 split-precision tensor-core transforms. */
+ * `mode` 0: the plain path (truncated-DFT longitude transforms and one thread
+ * per Legendre output, as the reference's shaders); 1: the optimized path
+ * (warp-shuffle FFTs, latitude-pair Legendre transforms on m-major Fourier
+ * planes). Both compute in FP32 and share the physics. */
 int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine** engine);
 void exogcm_destroy(exogcm_engine* engine);
 
@@ -180,6 +183,14 @@ int exogcm_last_step_ms(exogcm_engine* engine, float* ms);
  * "rain_column". The launches change the state; use it for measurement
  * only. */
 int exogcm_time_kernel(exogcm_engine* engine, const char* kernel, int reps, float* ms, double* bytes);
+
+/* Launch shapes the autotuner chose for the optimized path's transforms at
+ * the engine's first configure (plain path: the defaults): values[0] FFT
+ * latitudes per block; [1], [2] sp2fc wavenumbers and planes per block;
+ * [3], [4] the same for dv2uv; [5..8] forward Legendre wavenumbers per block
+ * for fc2sp, uv2dv, mktend's uv2dv and qtend. `count` must be at least 9.
+ * The shapes split work differently but leave every result unchanged. */
+int exogcm_tuning(exogcm_engine* engine, int* values, int count);
 
 /* Kernel launches in the CUDA graph of a `steps`-step batch. */
 int exogcm_graph_launches(exogcm_engine* engine, int steps, size_t* launches);

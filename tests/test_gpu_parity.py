@@ -44,7 +44,16 @@ def test_initial_state_matches_oracle(truncation, levels):
 
 
 def _stage_errors(truncation, levels, warm_steps, seed=11, mode=0):
-    p, e = build(truncation, levels, seed=seed, mode=mode)
+    return _replay_errors(planets.make_planet(seed, truncation=truncation, levels=levels), truncation, levels,
+                          warm_steps, mode)
+
+
+def _replay_errors(p, truncation, levels, warm_steps, mode=0):
+    """Per-stage replay (the reference's verify-dynamics.mjs): the engine's
+    state is copied into the oracle before each stage, both run the stage,
+    and every field's relative RMS against FP64 is kept at its worst."""
+    e = pkg.Engine(truncation, levels, 1, mode=mode)
+    e.configure(0, p)
     m = oracle.model_for(p)
     o = oracle.Oracle(m)
     e.step(warm_steps)
@@ -85,6 +94,8 @@ PHYSICS_FIELDS = {
     "zdekin", "zstt1", "zstt2", "zsdef", "fzdtdt", "fzdekin", "zdu", "zdv", "fzdu", "fzdv", "zdsdp1", "zdszp1",
     "zdsdp2", "zdszp2", "localweathering", "localavgweather", "dflux", "dswfl", "dlwfl", "dfu", "dfd", "dftu",
     "dftd", "dqo3", "gmu0", "dalb", "dsalb",
+    # sea ice and slab ocean (freezing and melting thresholds)
+    "xts", "xsst", "xiced", "xicec", "xsnow", "xicecc", "xclsst2", "xclicec2", "xcliced2", "xclssto",
 }
 
 
@@ -227,3 +238,29 @@ def test_snapshot_publishes_on_schedule():
     dt = e.read(0, "dt").reshape(11, -1)
     # field 0 is the surface temperature at the publishing step; the state has moved 3 steps on
     assert np.all(np.abs(snap[0] - dt[10]) < 30)
+
+
+@pytest.mark.gpu
+def test_autotuned_shapes_leave_results_unchanged():
+    """Each engine times its own transform shapes at its first configure;
+    engines of 1 and 3 slots may pick different ones, and the shared planet
+    must still step identically."""
+    p = planets.make_planet(81, truncation=21, levels=10)
+    one = pkg.Engine(21, 10, 1, mode=1)
+    three = pkg.Engine(21, 10, 3, mode=1)
+    one.configure(0, p)
+    for s in range(3):
+        three.configure(s, p)
+    for e in (one, three):
+        t = e.tuning()
+        assert t["fft_rows"] in (8, 16, 32)
+        for group, tile in (t["sp2fc"], t["dv2uv"]):
+            assert group in (1, 2, 4) and tile in (8, 16, 32)
+        assert set(t["forward_groups"].values()) <= {1, 2, 4}
+    print("tunings:", one.tuning(), three.tuning())
+    one.step(3)
+    three.step(3)
+    one.step(8)
+    three.step(8)
+    for name in ("st", "sz", "sd", "sq", "sp", "fgt", "gu"):
+        assert np.array_equal(one.read(0, name), three.read(2, name)), name

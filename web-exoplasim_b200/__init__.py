@@ -92,6 +92,7 @@ SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_size_t)]),
     "exogcm_stream": (_VP, [_VP]),
     "exogcm_time_kernel": (ctypes.c_int, [_VP, ctypes.c_char_p, ctypes.c_int, _FP, _DP]),
+    "exogcm_tuning": (ctypes.c_int, [_VP, _VP, ctypes.c_int]),
     "exogcm_slot_sums_noalloc": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_int, _VP, _VP]),
     "exogcm_graph_launches": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
 }
@@ -288,6 +289,13 @@ class Engine:
         ptr, n = _VP(), ctypes.c_size_t()
         _check(_lib.exogcm_device_field(self.h, name.encode(), ctypes.byref(ptr), ctypes.byref(n)))
         return ptr.value, n.value
+
+    def tuning(self) -> dict:
+        """The transform launch shapes chosen at the first configure."""
+        v = (ctypes.c_int * 9)()
+        _check(_lib.exogcm_tuning(self.h, v, 9))
+        return {"fft_rows": v[0], "sp2fc": (v[1], v[2]), "dv2uv": (v[3], v[4]),
+                "forward_groups": {"fc2sp": v[5], "uv2dv": v[6], "mktend": v[7], "qtend": v[8]}}
 
     def graph_launches(self, steps: int) -> int:
         n = ctypes.c_size_t()

@@ -112,6 +112,17 @@ struct SharedTabs {
   const float* qvT;
 };
 
+// Launch shapes of the optimized path's transforms, measured per engine by
+// the autotuner among the shapes each kernel supports. They change how work
+// is split over blocks, never the order of any sum, so results do not
+// depend on them.
+struct Tuning {
+  int fft_rows;      // latitudes per FFT block (a multiple of 8 dividing NLAT)
+  int inv_group[2];  // wavenumbers per inverse Legendre block: [0] sp2fc, [1] dv2uv
+  int inv_tile[2];   // planes per inverse Legendre block (even)
+  int fwd_group[4];  // wavenumbers per forward Legendre block, by kind
+};
+
 // Everything a step kernel can reach.
 struct Model {
   Dims d;
@@ -123,7 +134,8 @@ struct Model {
   const StepParams* params;  // [S] for the step being run
   double* sums;              // FP64 per-slot reductions scratch [S][4]
   int* flags;                // per-slot status flags [S]
-  int mode;                  // 0 plain FP32 path, 1 optimized path (FFTs, fused and tensor-core kernels)
+  int mode;                  // 0 plain path, 1 optimized path (FFTs, latitude-pair Legendre, m-major Fourier)
+  Tuning tune;               // optimized path launch shapes
 };
 
 }  // namespace exogcm

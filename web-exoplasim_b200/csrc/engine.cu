@@ -104,6 +104,8 @@ struct exogcm_engine {
   int* flags = nullptr;
   std::vector<Slot> slots;
   std::map<int, cudaGraphExec_t> graphs;
+  Tuning tune{};
+  SharedSetup shared_setup;  // host copy of the shared tables (set-up of later planets)
 
   Model model(int k) const {
     Model m{};
@@ -117,6 +119,7 @@ struct exogcm_engine {
     m.sums = sums;
     m.flags = flags;
     m.mode = mode;
+    m.tune = tune;
     return m;
   }
 };
@@ -580,6 +583,86 @@ long json_number(const std::string& s, const char* key) {
 }  // namespace
 
 // ================================================================= C ABI
+namespace {
+
+// Times each transform kernel of the optimized path over the launch shapes
+// it supports and keeps the fastest: full-level launches over every slot,
+// two warm-up and five timed launches per shape (CUDA events on the
+// engine's stream). Runs once, at the first configure, before any slot holds
+// state; the shapes change how work is split, not any result.
+void autotune(exogcm_engine* e) {
+  const Dims& d = e->d;
+  const int LP = d.L * d.S, JH = d.NLAT / 2;
+  const FieldPtrs& F = e->fp;
+  Tuning& t = e->tune;
+  auto time = [&](const std::function<void(const Model&)>& launch) {
+    const Model m = e->model(0);
+    for (int r = 0; r < 2; ++r) launch(m);
+    check(cudaEventRecord(e->ev0, e->stream), "event");
+    for (int r = 0; r < 5; ++r) launch(m);
+    check(cudaEventRecord(e->ev1, e->stream), "event");
+    check(cudaStreamSynchronize(e->stream), "autotune");
+    float ms = 0.f;
+    check(cudaEventElapsedTime(&ms, e->ev0, e->ev1), "event time");
+    return ms;
+  };
+  {
+    float best = 1e30f;
+    int pick = t.fft_rows;
+    for (int rows : {8, 16, 32, 48, 64, 96}) {
+      if (rows > d.NLAT || d.NLAT % rows || fft_chunk_smem(d, rows) > kLegSmemLimit) continue;
+      t.fft_rows = rows;
+      const float ms = time([&](const Model& m) {
+        tr_fourier_inverse(m, F.fgu, F.gu, LP, e->stream);
+        tr_fourier_forward(m, F.gtn, F.fgtn, LP, e->stream);
+      });
+      if (ms < best) best = ms, pick = rows;
+    }
+    t.fft_rows = pick;
+  }
+  for (int k = 0; k < 2; ++k) {
+    float best = 1e30f;
+    int pg = t.inv_group[k], pt = t.inv_tile[k];
+    for (int group : {1, 2, 4})
+      for (int tile : {8, 16, 32}) {
+        if (JH * tile / 2 > 1024 || leg_inverse_smem(d, k, group, tile) > kLegSmemLimit) continue;
+        t.inv_group[k] = group;
+        t.inv_tile[k] = tile;
+        const float ms = time([&](const Model& m) {
+          if (k == 0)
+            tr_legendre_inverse(m, F.st, F.fgt, LP, m.sh.qi, e->stream);
+          else
+            tr_dv2uv(m, F.sd, F.sz, F.fgu, F.fgv, LP, 0.f, e->stream);
+        });
+        if (ms < best) best = ms, pg = group, pt = tile;
+      }
+    t.inv_group[k] = pg;
+    t.inv_tile[k] = pt;
+  }
+  for (int k = 0; k < 4; ++k) {
+    float best = 1e30f;
+    int pick = t.fwd_group[k];
+    for (int group : {1, 2, 4}) {
+      if (leg_forward_smem(d, k, group) > kLegSmemLimit) continue;
+      t.fwd_group[k] = group;
+      const float ms = time([&](const Model& m) {
+        if (k == 0)
+          tr_legendre_forward(m, F.fgtdt, F.zstt1, LP, m.sh.qc, e->stream);
+        else if (k == 1)
+          tr_uv2dv(m, F.fgudt, F.fgvdt, nullptr, F.sdt, F.szt, LP, e->stream);
+        else if (k == 2)
+          tr_uv2dv(m, F.fgvz, F.fguz, F.fgke, F.zdsdp1, F.zdszp1, LP, e->stream);
+        else
+          tr_qtend(m, F.fgut, F.fgvt, F.fgtn, F.zstt2, LP, e->stream);
+      });
+      if (ms < best) best = ms, pick = group;
+    }
+    t.fwd_group[k] = pick;
+  }
+}
+
+}  // namespace
+
 extern "C" {
 
 int exogcm_last_error(char* buffer, size_t size) {
@@ -600,6 +683,7 @@ int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine
     auto e = std::make_unique<exogcm_engine>();
     e->d = make_dims(truncation, levels, slots);
     e->mode = mode;
+    e->tune = default_tuning(e->d);
     check(cudaGetDevice(&e->device), "device");
     layout(e.get());
     table_layout(e.get());
@@ -656,8 +740,9 @@ int exogcm_configure(exogcm_engine* e, int slot, const exogcm_planet* planet, co
     if (planet->truncation != e->d.T || planet->levels != e->d.L)
       throw Error(EXOGCM_EINVAL, "planet resolution differs from the engine's");
     if (!e->shared_ready) {
-      SharedSetup sh = build_shared(e->d.T, planet->filter_kind, planet->filter_gp, planet->filter_sp);
-      upload_shared(e, sh);
+      e->shared_setup = build_shared(e->d.T, planet->filter_kind, planet->filter_gp, planet->filter_sp);
+      upload_shared(e, e->shared_setup);
+      if (e->mode == 1) autotune(e);
       e->filter_kind = planet->filter_kind;
       e->filter_gp = planet->filter_gp;
       e->filter_sp = planet->filter_sp;
@@ -665,8 +750,7 @@ int exogcm_configure(exogcm_engine* e, int slot, const exogcm_planet* planet, co
                planet->filter_sp != e->filter_sp) {
       throw Error(EXOGCM_EINVAL, "planets of one engine share the physics filter setting");
     }
-    SharedSetup sh = build_shared(e->d.T, e->filter_kind, e->filter_gp, e->filter_sp);
-    PlanetSetup ps = build_planet(*planet, *boundary, sh);
+    PlanetSetup ps = build_planet(*planet, *boundary, e->shared_setup);
     zero_slot(e, slot);
     for (auto& kv : ps.state) {
       const FieldInfo& fi = field(e, kv.first.c_str());
@@ -1037,6 +1121,16 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
     check(cudaEventElapsedTime(&total, e->ev0, e->ev1), "event time");
     *ms = total / reps;
     if (bytes) *bytes = b;
+  });
+}
+
+int exogcm_tuning(exogcm_engine* e, int* values, int count) {
+  return guard([&] {
+    if (!e || !values || count < 9) throw Error(EXOGCM_EINVAL, "need room for 9 values");
+    const Tuning& t = e->tune;
+    const int v[9] = {t.fft_rows,     t.inv_group[0], t.inv_tile[0], t.inv_group[1], t.inv_tile[1],
+                      t.fwd_group[0], t.fwd_group[1], t.fwd_group[2], t.fwd_group[3]};
+    std::copy(v, v + 9, values);
   });
 }
 

@@ -14,9 +14,12 @@
 //
 // The optimized path stores Fourier planes m-major (coefficient (m, lat) at
 // 2 * (m * NLAT + lat)), so that the Legendre transforms on either side
-// stream whole runs of latitudes. One block transforms one plane: the
-// plane's coefficients pass through shared memory ([m][lat], padded) between
-// that layout and the warps' rows, and both global sides stay contiguous.
+// stream whole runs of latitudes. One block transforms a chunk of `rows`
+// consecutive latitudes of one plane: the chunk's coefficients pass through
+// shared memory ([m][rows + 1]) between that layout (runs of `rows`
+// latitudes per m) and the warps' rows, so both global sides stay
+// contiguous. Small chunks give many blocks per SM at different phases, so
+// one block's loads overlap another's arithmetic.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -109,31 +112,34 @@ __device__ __forceinline__ void natural_order(const float2 (&x)[R], float2 (&y)[
   }
 }
 
-// Shared memory of a plane block: twiddles and the plane's coefficients
-// [ntp1][nlat + 1] (the odd row pitch keeps column reads conflict-free).
-inline size_t plane_smem(int nlon, int nlat, int ntp1) {
-  return ((size_t)nlon + (size_t)ntp1 * (nlat + 1)) * sizeof(float2);
+// Shared memory of a chunk block: twiddles and the chunk's coefficients
+// [ntp1][rows + 1] (the odd row pitch keeps column reads conflict-free).
+inline size_t chunk_smem(int nlon, int rows, int ntp1) {
+  return ((size_t)nlon + (size_t)ntp1 * (rows + 1)) * sizeof(float2);
 }
 
 // gp2fc for one plane per block: rows of N grid values -> m-major
 // coefficients. A warp transforms kRowsPerWarp rows together.
 template <int R>
 __global__ void __launch_bounds__(kWarps * 32) k_fft_forward(const float* __restrict__ g, float* __restrict__ c,
-                                                             const float2* __restrict__ twg, int nlat, int ntp1) {
+                                                             const float2* __restrict__ twg, int nlat, int ntp1,
+                                                             int rows) {
   constexpr int M = 32 * R, N = 2 * M, B = kRowsPerWarp;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* fc = tw + N;  // [ntp1][nlat + 1]
+  float2* fc = tw + N;  // [ntp1][rows + 1]
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const float inv_n = 1.f / (float)N;
-  const size_t plane = blockIdx.x;
-  for (int row0 = warp * B; row0 < nlat; row0 += kWarps * B) {
+  const int chunks = nlat / rows;
+  const size_t plane = blockIdx.x / chunks;
+  const int lat0 = (blockIdx.x % chunks) * rows;
+  for (int row0 = warp * B; row0 < rows; row0 += kWarps * B) {
     float2 x[B][R];
 #pragma unroll
     for (int b = 0; b < B; ++b) {
-      const float2* in = reinterpret_cast<const float2*>(g + (plane * nlat + row0 + b) * N);
+      const float2* in = reinterpret_cast<const float2*>(g + (plane * nlat + lat0 + row0 + b) * N);
 #pragma unroll
       for (int r = 0; r < R; ++r) x[b][r] = in[lane + 32 * r];
     }
@@ -159,16 +165,16 @@ __global__ void __launch_bounds__(kWarps * 32) k_fft_forward(const float* __rest
           // (zm - zc) / 2i = ((zm - zc).y, -(zm - zc).x) / 2
           const float2 odd = make_float2(0.5f * (zm.y - zc.y), -0.5f * (zm.x - zc.x));
           const float2 gm = cadd(even, cmul(twiddle<-1>(tw, m, N), odd));
-          fc[m * (nlat + 1) + row0 + b] = make_float2(gm.x * inv_n, m == 0 ? 0.f : gm.y * inv_n);
+          fc[m * (rows + 1) + row0 + b] = make_float2(gm.x * inv_n, m == 0 ? 0.f : gm.y * inv_n);
         }
       }
     }
   }
   __syncthreads();
-  float2* out = reinterpret_cast<float2*>(c) + plane * nlat * ntp1;
-  for (int i = threadIdx.x; i < ntp1 * nlat; i += blockDim.x) {
-    const int m = i / nlat, lat = i - m * nlat;
-    out[i] = fc[m * (nlat + 1) + lat];
+  float2* out = reinterpret_cast<float2*>(c) + plane * nlat * ntp1 + lat0;
+  for (int i = threadIdx.x; i < ntp1 * rows; i += blockDim.x) {
+    const int m = i / rows, lat = i - m * rows;
+    out[(size_t)m * nlat + lat] = fc[m * (rows + 1) + lat];
   }
 }
 
@@ -176,28 +182,31 @@ __global__ void __launch_bounds__(kWarps * 32) k_fft_forward(const float* __rest
 // values, kRowsPerWarp rows per warp at once.
 template <int R>
 __global__ void __launch_bounds__(kWarps * 32) k_fft_inverse(const float* __restrict__ c, float* __restrict__ g,
-                                                             const float2* __restrict__ twg, int nlat, int ntp1) {
+                                                             const float2* __restrict__ twg, int nlat, int ntp1,
+                                                             int rows) {
   constexpr int M = 32 * R, N = 2 * M, B = kRowsPerWarp;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* fc = tw + N;  // [ntp1][nlat + 1]
+  float2* fc = tw + N;  // [ntp1][rows + 1]
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
-  const size_t plane = blockIdx.x;
-  const float2* in = reinterpret_cast<const float2*>(c) + plane * nlat * ntp1;
-  for (int i = threadIdx.x; i < ntp1 * nlat; i += blockDim.x) {
-    const int m = i / nlat, lat = i - m * nlat;
-    float2 v = in[i];
+  const int chunks = nlat / rows;
+  const size_t plane = blockIdx.x / chunks;
+  const int lat0 = (blockIdx.x % chunks) * rows;
+  const float2* in = reinterpret_cast<const float2*>(c) + plane * nlat * ntp1 + lat0;
+  for (int i = threadIdx.x; i < ntp1 * rows; i += blockDim.x) {
+    const int m = i / rows, lat = i - m * rows;
+    float2 v = in[(size_t)m * nlat + lat];
     if (m == 0) v.y = 0.f;  // Im c_0 is ignored
-    fc[m * (nlat + 1) + lat] = v;
+    fc[m * (rows + 1) + lat] = v;
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int row0 = warp * B; row0 < nlat; row0 += kWarps * B) {
+  for (int row0 = warp * B; row0 < rows; row0 += kWarps * B) {
     float2 x[B][R];
 #pragma unroll
     for (int b = 0; b < B; ++b) {
       const int row = row0 + b;
-      auto coef = [&](int k) { return k < ntp1 ? fc[k * (nlat + 1) + row] : make_float2(0.f, 0.f); };
+      auto coef = [&](int k) { return k < ntp1 ? fc[k * (rows + 1) + row] : make_float2(0.f, 0.f); };
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const int k = lane + 32 * r;
@@ -213,7 +222,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_fft_inverse(const float* __rest
     for (int b = 0; b < B; ++b) {
       float2 y[R];
       natural_order<R>(x[b], y, lane);
-      float2* out = reinterpret_cast<float2*>(g + (plane * nlat + row0 + b) * N);
+      float2* out = reinterpret_cast<float2*>(g + (plane * nlat + lat0 + row0 + b) * N);
 #pragma unroll
       for (int r = 0; r < R; ++r) out[lane + 32 * r] = y[r];
     }
@@ -236,25 +245,31 @@ void fft_init() {
   allow_plane_smem(k_fft_inverse<3>);
 }
 
-// The plane blocks need NLAT to be a multiple of kWarps * kRowsPerWarp (8):
-// NLAT is 32, 64 or 96.
+size_t fft_chunk_smem(const Dims& d, int rows) { return chunk_smem(d.NLON, rows, d.NTP1); }
+
+// A chunk is `rows` latitudes (m.tune.fft_rows, a multiple of
+// kWarps * kRowsPerWarp = 8 that divides NLAT = 32, 64 or 96).
 void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st) {
   const float2* tw = reinterpret_cast<const float2*>(m.sh.tw);
-  const size_t smem = plane_smem(m.d.NLON, m.d.NLAT, m.d.NTP1);
+  const int rows = m.tune.fft_rows;
+  const size_t smem = chunk_smem(m.d.NLON, rows, m.d.NTP1);
+  const unsigned blocks = planes * (m.d.NLAT / rows);
   switch (m.d.NLON) {
-    case 64: k_fft_forward<1><<<planes, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1); break;
-    case 128: k_fft_forward<2><<<planes, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1); break;
-    default: k_fft_forward<3><<<planes, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1); break;
+    case 64: k_fft_forward<1><<<blocks, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
+    case 128: k_fft_forward<2><<<blocks, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
+    default: k_fft_forward<3><<<blocks, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
   }
 }
 
 void fft_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st) {
   const float2* tw = reinterpret_cast<const float2*>(m.sh.tw);
-  const size_t smem = plane_smem(m.d.NLON, m.d.NLAT, m.d.NTP1);
+  const int rows = m.tune.fft_rows;
+  const size_t smem = chunk_smem(m.d.NLON, rows, m.d.NTP1);
+  const unsigned blocks = planes * (m.d.NLAT / rows);
   switch (m.d.NLON) {
-    case 64: k_fft_inverse<1><<<planes, kWarps * 32, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1); break;
-    case 128: k_fft_inverse<2><<<planes, kWarps * 32, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1); break;
-    default: k_fft_inverse<3><<<planes, kWarps * 32, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1); break;
+    case 64: k_fft_inverse<1><<<blocks, kWarps * 32, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1, rows); break;
+    case 128: k_fft_inverse<2><<<blocks, kWarps * 32, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1, rows); break;
+    default: k_fft_inverse<3><<<blocks, kWarps * 32, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1, rows); break;
   }
 }
 

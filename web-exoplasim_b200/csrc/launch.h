@@ -23,7 +23,11 @@ void tr_qtend(const Model& m, const float* u, const float* v, const float* src, 
               cudaStream_t st);
 
 // legendre.cu (optimized path)
+constexpr size_t kLegSmemLimit = 100 * 1024;  // dynamic shared memory the transform kernels may ask
 void leg_init();
+size_t leg_inverse_smem(const Dims& d, int kind, int group, int tile);
+size_t leg_forward_smem(const Dims& d, int kind, int group);
+Tuning default_tuning(const Dims& d);
 void leg_inverse(const Model& m, const float* s, float* f, int planes, bool derivative, cudaStream_t st);
 void leg_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V, int planes, float plavor,
                cudaStream_t st);
@@ -35,6 +39,7 @@ void leg_qtend(const Model& m, const float* u, const float* v, const float* src,
 
 // fft.cu (optimized path; Fourier planes m-major)
 void fft_init();
+size_t fft_chunk_smem(const Dims& d, int rows);
 void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st);
 void fft_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st);
 

@@ -37,8 +37,7 @@ namespace exogcm {
 namespace {
 
 constexpr int kForwardThreads = 256;
-constexpr size_t kInverseBudget = 48 * 1024;
-constexpr size_t kSmemBudget = 100 * 1024;
+constexpr size_t kSmemBudget = kLegSmemLimit;
 
 __device__ __forceinline__ int first_mode(int m, int ntp1) { return m * (2 * ntp1 - m + 1) / 2; }
 inline int first_mode_host(int m, int ntp1) { return m * (2 * ntp1 - m + 1) / 2; }
@@ -308,36 +307,14 @@ __global__ void __launch_bounds__(kForwardThreads) k_sym_forward(SymIn<NIN> in, 
   }
 }
 
-// Inverse tiling: 16 planes per block (32 at T21, 8 threads per latitude
-// pair either way) and the largest group of 4, 2 or 1 wavenumbers whose
-// staged coefficients and table slices fit the budget (several blocks per
-// SM).
-struct InverseTiling {
-  int tile, group;
-  size_t smem;
-};
-
-InverseTiling inverse_tiling(const Dims& d, int nin) {
-  const int tile = d.NLAT == 32 ? 32 : 16;
-  const int JH = d.NLAT / 2;
-  for (int group = 4;; group /= 2) {
-    const size_t nt = group_terms(d, group);
-    const size_t smem = (size_t)nin * nt * tile * 8 + (size_t)nin * nt * JH * 4;
-    if (smem <= kInverseBudget || group == 1) return {tile, group, smem};
-  }
+size_t inverse_smem(const Dims& d, int nin, int group, int tile) {
+  const size_t nt = group_terms(d, group);
+  return (size_t)nin * nt * tile * 8 + (size_t)nin * nt * (d.NLAT / 2) * 4;
 }
 
-// Forward: kFwdTile planes per block and the largest group of 4, 2 or 1
-// wavenumbers whose staged sums, differences and table slices fit about
-// 60 KB (three blocks per SM).
+// Forward: kFwdTile planes per block; the group of wavenumbers is tuned.
 size_t forward_smem(const Dims& d, int nin, int ntab, int group) {
   return (size_t)nin * kFwdTile * group * (d.NLAT / 2) * 16 + (size_t)ntab * (d.NLAT / 2) * group_terms(d, group) * 4;
-}
-
-int forward_group_for(const Dims& d, int nin, int ntab) {
-  for (int group = 4; group > 1; group /= 2)
-    if (forward_smem(d, nin, ntab, group) <= 60 * 1024) return group;
-  return 1;
 }
 
 template <typename K>
@@ -349,7 +326,7 @@ template <int KIND, int NIN>
 void launch_sym_forward(const Model& m, SymIn<NIN> in, float* out0, float* out1, int planes, const float* q,
                         cudaStream_t st) {
   constexpr int NTAB = FwdTables<KIND>::N;
-  const int group = forward_group_for(m.d, NIN, NTAB);
+  const int group = m.tune.fwd_group[KIND];
   dim3 grid((m.d.NTP1 + group - 1) / group, (planes + kFwdTile - 1) / kFwdTile);
   k_sym_forward<KIND, NIN><<<grid, kForwardThreads, forward_smem(m.d, NIN, NTAB, group), st>>>(
       in, out0, out1, planes, group, m.sh, q, m.d);
@@ -367,21 +344,58 @@ void leg_init() {
 }
 
 void leg_inverse(const Model& m, const float* s, float* f, int planes, bool derivative, cudaStream_t st) {
-  const InverseTiling t = inverse_tiling(m.d, 1);
-  dim3 grid((m.d.NTP1 + t.group - 1) / t.group, (planes + t.tile - 1) / t.tile);
-  const int threads = (m.d.NLAT / 2) * t.tile / 2;
-  k_sym_inverse<0><<<grid, threads, t.smem, st>>>(s, nullptr, f, nullptr, planes, t.tile, t.group,
-                                                  derivative ? m.sh.qjT : m.sh.qiT, nullptr, derivative ? 1 : 0, 0.f,
-                                                  m.d);
+  const int group = m.tune.inv_group[0], tile = m.tune.inv_tile[0];
+  dim3 grid((m.d.NTP1 + group - 1) / group, (planes + tile - 1) / tile);
+  const int threads = (m.d.NLAT / 2) * tile / 2;
+  k_sym_inverse<0><<<grid, threads, inverse_smem(m.d, 1, group, tile), st>>>(
+      s, nullptr, f, nullptr, planes, tile, group, derivative ? m.sh.qjT : m.sh.qiT, nullptr, derivative ? 1 : 0, 0.f,
+      m.d);
 }
 
 void leg_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V, int planes, float plavor,
                cudaStream_t st) {
-  const InverseTiling t = inverse_tiling(m.d, 2);
-  dim3 grid((m.d.NTP1 + t.group - 1) / t.group, (planes + t.tile - 1) / t.tile);
-  const int threads = (m.d.NLAT / 2) * t.tile / 2;
-  k_sym_inverse<1><<<grid, threads, t.smem, st>>>(D, Z, U, V, planes, t.tile, t.group, m.sh.quT, m.sh.qvT, 0, plavor,
-                                                  m.d);
+  const int group = m.tune.inv_group[1], tile = m.tune.inv_tile[1];
+  dim3 grid((m.d.NTP1 + group - 1) / group, (planes + tile - 1) / tile);
+  const int threads = (m.d.NLAT / 2) * tile / 2;
+  k_sym_inverse<1><<<grid, threads, inverse_smem(m.d, 2, group, tile), st>>>(D, Z, U, V, planes, tile, group,
+                                                                             m.sh.quT, m.sh.qvT, 0, plavor, m.d);
+}
+
+// Shared memory a tuning asks of each transform kernel, and the default
+// tuning: the largest wavenumber groups that fit about 48 KB (inverse) and
+// 60 KB (forward), 16-plane inverse tiles (32 at T21) and 16-latitude FFT
+// chunks. The autotuner times the shapes that fit kLegSmemLimit.
+size_t leg_inverse_smem(const Dims& d, int kind, int group, int tile) {
+  return inverse_smem(d, kind == 0 ? 1 : 2, group, tile);
+}
+
+size_t leg_forward_smem(const Dims& d, int kind, int group) {
+  const int nin = kind == 0 ? 1 : kind == 1 ? 2 : 3;
+  const int ntab = kind == 0 ? 1 : kind == 1 ? 2 : 3;
+  return forward_smem(d, nin, ntab, group);
+}
+
+Tuning default_tuning(const Dims& d) {
+  Tuning t{};
+  t.fft_rows = 16;
+  for (int k = 0; k < 2; ++k) {
+    t.inv_tile[k] = d.NLAT == 32 ? 32 : 16;
+    t.inv_group[k] = 1;
+    for (int g = 4; g > 1; g /= 2)
+      if (leg_inverse_smem(d, k, g, t.inv_tile[k]) <= 48 * 1024) {
+        t.inv_group[k] = g;
+        break;
+      }
+  }
+  for (int k = 0; k < 4; ++k) {
+    t.fwd_group[k] = 1;
+    for (int g = 4; g > 1; g /= 2)
+      if (leg_forward_smem(d, k, g) <= 60 * 1024) {
+        t.fwd_group[k] = g;
+        break;
+      }
+  }
+  return t;
 }
 
 void leg_forward(const Model& m, const float* f, float* s, int planes, const float* q, cudaStream_t st) {

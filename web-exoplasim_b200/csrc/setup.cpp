@@ -167,12 +167,16 @@ Vec analyse(const SharedSetup& sh, const double* grid) {
   const int T = sh.truncation, nlat = sh.nlat, nlon = sh.nlon, nfc = 2 * (T + 1);
   const int modes = (T + 1) * (T + 2) / 2;
   Vec four((size_t)nlat * nfc, 0);
-  for (int row = 0; row < nlat; ++row)
-    for (int c = 0; c < nfc; ++c) {
-      double s = 0;
-      for (int j = 0; j < nlon; ++j) s += grid[(size_t)row * nlon + j] * sh.fwd[(size_t)j * nfc + c];
-      four[(size_t)row * nfc + c] = s;
+  // Each coefficient sums the longitudes in order j = 0, 1, ...; the loop
+  // over coefficients is innermost so the table rows are read contiguously.
+  for (int row = 0; row < nlat; ++row) {
+    double* out = &four[(size_t)row * nfc];
+    for (int j = 0; j < nlon; ++j) {
+      const double g = grid[(size_t)row * nlon + j];
+      const double* f = &sh.fwd[(size_t)j * nfc];
+      for (int c = 0; c < nfc; ++c) out[c] += g * f[c];
     }
+  }
   Vec sp(2 * modes, 0);
   for (int l = 0; l < nlat / 2; ++l) {
     const double* north = &four[(size_t)l * nfc];

@@ -41,6 +41,7 @@ class Request:
     seed: int
     arrival: float = 0.0
     overrides: dict = field(default_factory=dict)
+    planet: object = None  # a prebuilt planets.Planet (the client's input); else made from the seed
     # filled in by the server
     admitted: float | None = None
     finished: float | None = None
@@ -82,8 +83,10 @@ class Group:
 
     def admit(self, req: Request, now: float):
         slot = self.free.popleft()
-        planet = planets_mod.make_planet(req.seed, truncation=req.truncation, levels=req.levels,
-                                         timestepMinutes=STEP_MINUTES[req.truncation], **req.overrides)
+        planet = req.planet
+        if planet is None:
+            planet = planets_mod.make_planet(req.seed, truncation=req.truncation, levels=req.levels,
+                                             timestepMinutes=STEP_MINUTES[req.truncation], **req.overrides)
         self.engine.configure(slot, planet)
         steps_per_day = 1440.0 / STEP_MINUTES[req.truncation]
         req.steps = max(1, int(round(req.days * steps_per_day)))
