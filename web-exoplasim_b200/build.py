@@ -12,10 +12,14 @@ SOURCES = ["engine.cu", "transforms.cu", "legendre.cu", "fft.cu", "dynamics.cu",
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
-# Column physics divides and takes square roots at full range to 2 ulp (the
-# error WGSL allows its division, 2.5 ulp) instead of IEEE rounding, whose
-# slow-path calls cost the per-column kernels registers and issue slots.
-FILE_FLAGS = {"physics.cu": ["-prec-div=false", "-prec-sqrt=false"]}
+# Column physics uses the GPU's fast arithmetic: division and square root to
+# 2 ulp (WGSL allows its division 2.5 ulp), exp/log/pow from the
+# special-function unit (relative error about 1e-6), denormals flushed to
+# zero. These fits (absorptivities, saturation, cloud optics) carry
+# empirical coefficients of 3-4 digits, and the per-column kernels are
+# bound by their instruction count, so the accurate library routines would
+# cost speed and add nothing the FP64 comparison can see.
+FILE_FLAGS = {"physics.cu": ["-use_fast_math"]}
 
 
 def stale() -> bool:

@@ -22,6 +22,9 @@
 // one block's loads overlap another's arithmetic.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
+#include "async_copy.cuh"
 #include "common.cuh"
 #include "launch.h"
 
@@ -112,9 +115,22 @@ __device__ __forceinline__ void natural_order(const float2 (&x)[R], float2 (&y)[
   }
 }
 
-// Shared memory of a chunk block: twiddles and the chunk's coefficients
-// [ntp1][rows + 1] (the odd row pitch keeps column reads conflict-free).
-inline size_t chunk_smem(int nlon, int rows, int ntp1) {
+// Work items are (plane, chunk of `rows` latitudes) pairs, walked by
+// persistent blocks: while a block transforms one item, cp.async brings the
+// next item's input into the other half of its staging memory.
+//
+// Inverse staging: the chunk's coefficients [ntp1][rows + 2] (a pitch that
+// keeps every 16-byte copy aligned). Forward staging: the chunk's grid rows
+// [rows][N] (one contiguous run of the plane), plus one output buffer
+// [ntp1][rows + 1] for the m-major write.
+
+__host__ __device__ inline int coef_pitch(int rows) { return rows + 2; }
+
+inline size_t inverse_chunk_smem(int nlon, int rows, int ntp1) {
+  return ((size_t)nlon + 2 * (size_t)ntp1 * coef_pitch(rows)) * sizeof(float2);
+}
+
+inline size_t forward_chunk_smem(int nlon, int rows, int ntp1) {
   return ((size_t)nlon + (size_t)ntp1 * (rows + 1)) * sizeof(float2);
 }
 
@@ -178,60 +194,80 @@ __global__ void __launch_bounds__(kWarps * 32) k_fft_forward(const float* __rest
   }
 }
 
-// fc2gp for one plane per block: m-major coefficients -> rows of N grid
-// values, kRowsPerWarp rows per warp at once.
+// fc2gp: m-major coefficients -> rows of N grid values, kRowsPerWarp rows
+// per warp at once.
 template <int R>
 __global__ void __launch_bounds__(kWarps * 32) k_fft_inverse(const float* __restrict__ c, float* __restrict__ g,
                                                              const float2* __restrict__ twg, int nlat, int ntp1,
-                                                             int rows) {
+                                                             int rows, int items) {
   constexpr int M = 32 * R, N = 2 * M, B = kRowsPerWarp;
-  extern __shared__ float2 sm[];
-  float2* tw = sm;
-  float2* fc = tw + N;  // [ntp1][rows + 1]
+  extern __shared__ float4 sm4[];
+  float2* tw = reinterpret_cast<float2*>(sm4);
+  float2* fcb = tw + N;  // [2][ntp1][pitch]
+  const int pitch = coef_pitch(rows);
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
   const int chunks = nlat / rows;
-  const size_t plane = blockIdx.x / chunks;
-  const int lat0 = (blockIdx.x % chunks) * rows;
-  const float2* in = reinterpret_cast<const float2*>(c) + plane * nlat * ntp1 + lat0;
-  for (int i = threadIdx.x; i < ntp1 * rows; i += blockDim.x) {
-    const int m = i / rows, lat = i - m * rows;
-    float2 v = in[(size_t)m * nlat + lat];
-    if (m == 0) v.y = 0.f;  // Im c_0 is ignored
-    fc[m * (rows + 1) + lat] = v;
-  }
-  __syncthreads();
+  auto stage = [&](int item, float2* buf) {
+    const float2* src =
+        reinterpret_cast<const float2*>(c) + (size_t)(item / chunks) * nlat * ntp1 + (item % chunks) * rows;
+    const int pieces = rows / 2;
+    for (int i = threadIdx.x; i < ntp1 * pieces; i += blockDim.x) {
+      const int m = i / pieces, q = i - m * pieces;
+      cp_async16(buf + m * pitch + 2 * q, src + (size_t)m * nlat + 2 * q);
+    }
+  };
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int row0 = warp * B; row0 < rows; row0 += kWarps * B) {
-    float2 x[B][R];
+  int item = blockIdx.x;
+  if (item < items) stage(item, fcb);
+  cp_async_commit();
+  for (int it = 0; item < items; ++it) {
+    const float2* fc = fcb + (size_t)(it & 1) * ntp1 * pitch;
+    const int next = item + gridDim.x;
+    if (next < items) stage(next, fcb + (size_t)((it + 1) & 1) * ntp1 * pitch);
+    cp_async_commit();
+    cp_async_wait_one();
+    __syncthreads();
+    const size_t plane = item / chunks;
+    const int lat0 = (item % chunks) * rows;
+    for (int row0 = warp * B; row0 < rows; row0 += kWarps * B) {
+      float2 x[B][R];
 #pragma unroll
-    for (int b = 0; b < B; ++b) {
-      const int row = row0 + b;
-      auto coef = [&](int k) { return k < ntp1 ? fc[k * (rows + 1) + row] : make_float2(0.f, 0.f); };
+      for (int b = 0; b < B; ++b) {
+        const int row = row0 + b;
+        auto coef = [&](int k) {
+          float2 v = k < ntp1 ? fc[k * pitch + row] : make_float2(0.f, 0.f);
+          if (k == 0) v.y = 0.f;  // Im c_0 is ignored
+          return v;
+        };
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int k = lane + 32 * r;
-        const float2 gk = coef(k);
-        const float2 gmk = conj2(coef(M - k));
-        const float2 e = cadd(gk, gmk);
-        const float2 o = cmul(csub(gk, gmk), twiddle<1>(tw, k, N));
-        x[b][r] = make_float2(e.x - o.y, e.y + o.x);  // e + i o
+        for (int r = 0; r < R; ++r) {
+          const int k = lane + 32 * r;
+          const float2 gk = coef(k);
+          const float2 gmk = conj2(coef(M - k));
+          const float2 e = cadd(gk, gmk);
+          const float2 o = cmul(csub(gk, gmk), twiddle<1>(tw, k, N));
+          x[b][r] = make_float2(e.x - o.y, e.y + o.x);  // e + i o
+        }
+      }
+      warp_fft<B, R, 1>(x, tw, N, lane);
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        float2 y[R];
+        natural_order<R>(x[b], y, lane);
+        float2* out = reinterpret_cast<float2*>(g + (plane * nlat + lat0 + row0 + b) * N);
+#pragma unroll
+        for (int r = 0; r < R; ++r) out[lane + 32 * r] = y[r];
       }
     }
-    warp_fft<B, R, 1>(x, tw, N, lane);
-#pragma unroll
-    for (int b = 0; b < B; ++b) {
-      float2 y[R];
-      natural_order<R>(x[b], y, lane);
-      float2* out = reinterpret_cast<float2*>(g + (plane * nlat + lat0 + row0 + b) * N);
-#pragma unroll
-      for (int r = 0; r < R; ++r) out[lane + 32 * r] = y[r];
-    }
+    __syncthreads();  // this staging buffer is reused two items on
+    item = next;
   }
+  cp_async_wait_all();
 }
 
 template <typename K>
 void allow_plane_smem(K kernel) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLegSmemLimit);
 }
 
 }  // namespace
@@ -245,14 +281,24 @@ void fft_init() {
   allow_plane_smem(k_fft_inverse<3>);
 }
 
-size_t fft_chunk_smem(const Dims& d, int rows) { return chunk_smem(d.NLON, rows, d.NTP1); }
+size_t fft_chunk_smem(const Dims& d, int rows) {
+  return std::max(inverse_chunk_smem(d.NLON, rows, d.NTP1), forward_chunk_smem(d.NLON, rows, d.NTP1));
+}
 
 // A chunk is `rows` latitudes (m.tune.fft_rows, a multiple of
 // kWarps * kRowsPerWarp = 8 that divides NLAT = 32, 64 or 96).
+template <typename K>
+void launch_chunks(K kernel, const void* entry, size_t smem, int items, const float* a, float* b, const Model& m,
+                   cudaStream_t st) {
+  const int grid = std::min(items, persistent_grid(entry, kWarps * 32, smem));
+  kernel<<<grid, kWarps * 32, smem, st>>>(a, b, reinterpret_cast<const float2*>(m.sh.tw), m.d.NLAT, m.d.NTP1,
+                                          m.tune.fft_rows, items);
+}
+
 void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st) {
   const float2* tw = reinterpret_cast<const float2*>(m.sh.tw);
   const int rows = m.tune.fft_rows;
-  const size_t smem = chunk_smem(m.d.NLON, rows, m.d.NTP1);
+  const size_t smem = forward_chunk_smem(m.d.NLON, rows, m.d.NTP1);
   const unsigned blocks = planes * (m.d.NLAT / rows);
   switch (m.d.NLON) {
     case 64: k_fft_forward<1><<<blocks, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
@@ -262,14 +308,13 @@ void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStrea
 }
 
 void fft_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st) {
-  const float2* tw = reinterpret_cast<const float2*>(m.sh.tw);
   const int rows = m.tune.fft_rows;
-  const size_t smem = chunk_smem(m.d.NLON, rows, m.d.NTP1);
-  const unsigned blocks = planes * (m.d.NLAT / rows);
+  const size_t smem = inverse_chunk_smem(m.d.NLON, rows, m.d.NTP1);
+  const int items = planes * (m.d.NLAT / rows);
   switch (m.d.NLON) {
-    case 64: k_fft_inverse<1><<<blocks, kWarps * 32, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1, rows); break;
-    case 128: k_fft_inverse<2><<<blocks, kWarps * 32, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1, rows); break;
-    default: k_fft_inverse<3><<<blocks, kWarps * 32, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1, rows); break;
+    case 64: launch_chunks(k_fft_inverse<1>, (const void*)k_fft_inverse<1>, smem, items, c, g, m, st); break;
+    case 128: launch_chunks(k_fft_inverse<2>, (const void*)k_fft_inverse<2>, smem, items, c, g, m, st); break;
+    default: launch_chunks(k_fft_inverse<3>, (const void*)k_fft_inverse<3>, smem, items, c, g, m, st); break;
   }
 }
 

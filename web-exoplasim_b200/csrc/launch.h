@@ -23,8 +23,10 @@ void tr_qtend(const Model& m, const float* u, const float* v, const float* src, 
               cudaStream_t st);
 
 // legendre.cu (optimized path)
-constexpr size_t kLegSmemLimit = 100 * 1024;  // dynamic shared memory the transform kernels may ask
+constexpr size_t kLegSmemLimit = 200 * 1024;  // dynamic shared memory the transform kernels may ask
 void leg_init();
+// Resident blocks of `kernel` per SM for a launch shape, times the SM count.
+int persistent_grid(const void* kernel, int threads, size_t smem);
 size_t leg_inverse_smem(const Dims& d, int kind, int group, int tile);
 size_t leg_forward_smem(const Dims& d, int kind, int group);
 Tuning default_tuning(const Dims& d);

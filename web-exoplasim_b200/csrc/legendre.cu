@@ -29,6 +29,9 @@
 // both are staged in shared memory by contiguous loads.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
+#include "async_copy.cuh"
 #include "common.cuh"
 #include "launch.h"
 
@@ -52,132 +55,160 @@ inline int group_terms(const Dims& d, int group) {
 // KIND 0: f0 = sum over modes of table * s0 (one table, parity `odd`).
 // KIND 1: dv2uv: (f0, f1) = (U, V) from (s0, s1) = (D, Z), tables qa = qu
 // (even) and qb = qv (odd), plavor taken from vorticity mode w = 1.
-// Each thread owns latitude pair j and two planes of the tile.
+// Persistent blocks walk the (wavenumber group, plane tile) items; while a
+// block computes one item, cp.async brings the next item's coefficients
+// and table slice into the other half of its shared memory, so staging
+// latency overlaps arithmetic. Each thread owns latitude pair j and two
+// planes of the tile.
 template <int KIND>
 __global__ void k_sym_inverse(const float* __restrict__ s0, const float* __restrict__ s1, float* __restrict__ f0,
-                              float* __restrict__ f1, int planes, int tile, int group, const float* __restrict__ qa,
-                              const float* __restrict__ qb, int odd, float plavor, Dims d) {
+                              float* __restrict__ f1, int planes, int tile, int group, int ntmax, int buf_floats,
+                              const float* __restrict__ qa, const float* __restrict__ qb, int odd, float plavor,
+                              Dims d) {
   constexpr int NIN = KIND == 0 ? 1 : 2;
   extern __shared__ float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
   const int JH = d.NLAT / 2;
-  const int m0 = blockIdx.x * group;
-  const int m1 = min(m0 + group, d.NTP1);
-  const int w0 = first_mode(m0, d.NTP1);
-  const int nt = first_mode(m1, d.NTP1) - w0;
-  const int p0 = blockIdx.y * tile;
-  const int np = min(tile, planes - p0);
+  const int ngroups = (d.NTP1 + group - 1) / group;
+  const int items = ngroups * ((planes + tile - 1) / tile);
   const size_t plane_floats = (size_t)d.NLAT * d.NFC;
-  // [NIN][nt][tile] (re, im): term-major, so two planes are one float4.
-  float2* ss = reinterpret_cast<float2*>(smem);
-  float* qs = smem + 2 * (size_t)NIN * nt * tile;  // [NIN tables][nt][JH]
-  for (int i = threadIdx.x; i < nt * JH; i += blockDim.x) {
-    qs[i] = __ldg(qa + (size_t)w0 * JH + i);
-    if (KIND == 1) qs[nt * JH + i] = __ldg(qb + (size_t)w0 * JH + i);
-  }
-  for (int k = 0; k < NIN; ++k) {
-    const float* src = k == 0 ? s0 : s1;
-    for (int i = threadIdx.x; i < tile * nt; i += blockDim.x) {
-      const int p = i / nt, t = i - p * nt;
-      float2 v = make_float2(0.f, 0.f);
-      if (p < np) {
-        v = *reinterpret_cast<const float2*>(src + (size_t)(p0 + p) * d.NRSP + 2 * (w0 + t));
-        if (KIND == 1 && k == 1 && w0 + t == 1) v.x -= plavor;
-      }
-      ss[((size_t)k * nt + t) * tile + p] = v;
+  // One buffer: [NIN][nt][tile] (re, im) term-major coefficients, then the
+  // [NIN tables][nt][JH] table slice at a fixed 16-byte aligned offset.
+  const int qs_at = 2 * NIN * ntmax * tile;
+  auto stage = [&](int item, float* buf) {
+    const int m0 = (item % ngroups) * group, p0 = (item / ngroups) * tile;
+    const int m1 = min(m0 + group, d.NTP1);
+    const int w0 = first_mode(m0, d.NTP1), nt = first_mode(m1, d.NTP1) - w0;
+    const int np = min(tile, planes - p0);
+    float* qs = buf + qs_at;
+    for (int i = threadIdx.x; i < nt * JH / 4; i += blockDim.x) {
+      cp_async16(qs + 4 * i, qa + (size_t)w0 * JH + 4 * i);
+      if (KIND == 1) cp_async16(qs + nt * JH + 4 * i, qb + (size_t)w0 * JH + 4 * i);
     }
-  }
-  __syncthreads();
-  const int j = threadIdx.x % JH;
-  const int pa = 2 * (threadIdx.x / JH);  // planes pa, pa + 1 of the tile
-  const int south = d.NLAT - 1 - j;
-  const bool has_a = pa < np, has_b = pa + 1 < np;
-  float2* outa0 = reinterpret_cast<float2*>(f0 + (size_t)(p0 + pa) * plane_floats);
-  float2* outb0 = outa0 + plane_floats / 2;
-  for (int m = m0; m < m1; ++m) {
-    const int toff = first_mode(m, d.NTP1) - w0;
-    const int K = d.NTP1 - m;
-    const float* qc = qs + toff * JH + j;
-    const float4* sc = reinterpret_cast<const float4*>(ss + (size_t)toff * tile + pa);
-    const int step4 = tile / 2;  // float4 stride between terms
-    const size_t rn = (size_t)m * d.NLAT + j, rs = (size_t)m * d.NLAT + south;
-    if (KIND == 0) {
-      float4 e = make_float4(0.f, 0.f, 0.f, 0.f), o = e;  // (re a, im a, re b, im b)
-      int t = 0;
-      for (; t + 1 < K; t += 2) {
-        const float qe = qc[t * JH], qo = qc[(t + 1) * JH];
-        const float4 ve = sc[t * step4], vo = sc[(t + 1) * step4];
-        e.x = fmaf(qe, ve.x, e.x);
-        e.y = fmaf(qe, ve.y, e.y);
-        e.z = fmaf(qe, ve.z, e.z);
-        e.w = fmaf(qe, ve.w, e.w);
-        o.x = fmaf(qo, vo.x, o.x);
-        o.y = fmaf(qo, vo.y, o.y);
-        o.z = fmaf(qo, vo.z, o.z);
-        o.w = fmaf(qo, vo.w, o.w);
+    float2* ss = reinterpret_cast<float2*>(buf);
+    for (int k = 0; k < NIN; ++k) {
+      const float* src = k == 0 ? s0 : s1;
+      for (int i = threadIdx.x; i < np * nt; i += blockDim.x) {
+        const int p = i / nt, t = i - p * nt;
+        cp_async8(ss + ((size_t)k * nt + t) * tile + p, src + (size_t)(p0 + p) * d.NRSP + 2 * (w0 + t));
       }
-      if (t < K) {
-        const float qe = qc[t * JH];
-        const float4 ve = sc[t * step4];
-        e.x = fmaf(qe, ve.x, e.x);
-        e.y = fmaf(qe, ve.y, e.y);
-        e.z = fmaf(qe, ve.z, e.z);
-        e.w = fmaf(qe, ve.w, e.w);
-      }
-      const float sg = odd ? -1.f : 1.f;
-      if (has_a) {
-        outa0[rn] = make_float2(e.x + o.x, e.y + o.y);
-        outa0[rs] = make_float2(sg * (e.x - o.x), sg * (e.y - o.y));
-      }
-      if (has_b) {
-        outb0[rn] = make_float2(e.z + o.z, e.w + o.w);
-        outb0[rs] = make_float2(sg * (e.z - o.z), sg * (e.w - o.w));
-      }
-    } else {
-      const float* qd = qc + nt * JH;
-      const float4* zc = sc + (size_t)nt * step4;
-      // Term t's contribution to u and v: a(t) * (dim, -dre, zim, -zre)
-      // + b(t) * (zre, zim, -dre, -dim); the even-t a part and odd-t b part
-      // go to X, the rest to Y: north = X + Y, south = X - Y.
-      float X[2][4] = {}, Y[2][4] = {};
-      auto add = [&](float (*acc_a)[4], float (*acc_b)[4], float a, float b, int t) {
-        const float4 D = sc[t * step4], Z = zc[t * step4];
-        const float2 Dp[2] = {make_float2(D.x, D.y), make_float2(D.z, D.w)};
-        const float2 Zp[2] = {make_float2(Z.x, Z.y), make_float2(Z.z, Z.w)};
-#pragma unroll
-        for (int pp = 0; pp < 2; ++pp) {
-          acc_a[pp][0] = fmaf(a, Dp[pp].y, acc_a[pp][0]);
-          acc_a[pp][1] = fmaf(-a, Dp[pp].x, acc_a[pp][1]);
-          acc_a[pp][2] = fmaf(a, Zp[pp].y, acc_a[pp][2]);
-          acc_a[pp][3] = fmaf(-a, Zp[pp].x, acc_a[pp][3]);
-          acc_b[pp][0] = fmaf(b, Zp[pp].x, acc_b[pp][0]);
-          acc_b[pp][1] = fmaf(b, Zp[pp].y, acc_b[pp][1]);
-          acc_b[pp][2] = fmaf(-b, Dp[pp].x, acc_b[pp][2]);
-          acc_b[pp][3] = fmaf(-b, Dp[pp].y, acc_b[pp][3]);
+    }
+  };
+  int item = blockIdx.x;
+  if (item < items) stage(item, smem);
+  cp_async_commit();
+  for (int it = 0; item < items; ++it) {
+    float* buf = smem + (size_t)(it & 1) * buf_floats;
+    const int next = item + gridDim.x;
+    if (next < items) stage(next, smem + (size_t)((it + 1) & 1) * buf_floats);
+    cp_async_commit();
+    cp_async_wait_one();  // this item's copies have landed (the next item's may be in flight)
+    __syncthreads();
+    const int m0 = (item % ngroups) * group, p0 = (item / ngroups) * tile;
+    const int m1 = min(m0 + group, d.NTP1);
+    const int w0 = first_mode(m0, d.NTP1), nt = first_mode(m1, d.NTP1) - w0;
+    const int np = min(tile, planes - p0);
+    float2* ss = reinterpret_cast<float2*>(buf);
+    const float* qs = buf + qs_at;
+    if (KIND == 1 && w0 <= 1 && 1 < w0 + nt) {
+      // vorticity mode w = 1 (real part) without plavor
+      for (int p = threadIdx.x; p < np; p += blockDim.x) ss[((size_t)nt + (1 - w0)) * tile + p].x -= plavor;
+      __syncthreads();
+    }
+    const int j = threadIdx.x % JH;
+    const int pa = 2 * (threadIdx.x / JH);  // planes pa, pa + 1 of the tile
+    const int south = d.NLAT - 1 - j;
+    const bool has_a = pa < np, has_b = pa + 1 < np;
+    float2* outa0 = reinterpret_cast<float2*>(f0 + (size_t)(p0 + pa) * plane_floats);
+    float2* outb0 = outa0 + plane_floats / 2;
+    for (int m = m0; m < m1; ++m) {
+      const int toff = first_mode(m, d.NTP1) - w0;
+      const int K = d.NTP1 - m;
+      const float* qc = qs + toff * JH + j;
+      const float4* sc = reinterpret_cast<const float4*>(ss + (size_t)toff * tile + pa);
+      const int step4 = tile / 2;  // float4 stride between terms
+      const size_t rn = (size_t)m * d.NLAT + j, rs = (size_t)m * d.NLAT + south;
+      if (KIND == 0) {
+        float4 e = make_float4(0.f, 0.f, 0.f, 0.f), o = e;  // (re a, im a, re b, im b)
+        int t = 0;
+        for (; t + 1 < K; t += 2) {
+          const float qe = qc[t * JH], qo = qc[(t + 1) * JH];
+          const float4 ve = sc[t * step4], vo = sc[(t + 1) * step4];
+          e.x = fmaf(qe, ve.x, e.x);
+          e.y = fmaf(qe, ve.y, e.y);
+          e.z = fmaf(qe, ve.z, e.z);
+          e.w = fmaf(qe, ve.w, e.w);
+          o.x = fmaf(qo, vo.x, o.x);
+          o.y = fmaf(qo, vo.y, o.y);
+          o.z = fmaf(qo, vo.z, o.z);
+          o.w = fmaf(qo, vo.w, o.w);
         }
-      };
-      int t = 0;
-      for (; t + 1 < K; t += 2) {
-        add(X, Y, qc[t * JH], qd[t * JH], t);
-        add(Y, X, qc[(t + 1) * JH], qd[(t + 1) * JH], t + 1);
-      }
-      if (t < K) add(X, Y, qc[t * JH], qd[t * JH], t);
-      float2* outa1 = reinterpret_cast<float2*>(f1 + (size_t)(p0 + pa) * plane_floats);
-      float2* outb1 = outa1 + plane_floats / 2;
-      if (has_a) {
-        outa0[rn] = make_float2(X[0][0] + Y[0][0], X[0][1] + Y[0][1]);
-        outa0[rs] = make_float2(X[0][0] - Y[0][0], X[0][1] - Y[0][1]);
-        outa1[rn] = make_float2(X[0][2] + Y[0][2], X[0][3] + Y[0][3]);
-        outa1[rs] = make_float2(X[0][2] - Y[0][2], X[0][3] - Y[0][3]);
-      }
-      if (has_b) {
-        outb0[rn] = make_float2(X[1][0] + Y[1][0], X[1][1] + Y[1][1]);
-        outb0[rs] = make_float2(X[1][0] - Y[1][0], X[1][1] - Y[1][1]);
-        outb1[rn] = make_float2(X[1][2] + Y[1][2], X[1][3] + Y[1][3]);
-        outb1[rs] = make_float2(X[1][2] - Y[1][2], X[1][3] - Y[1][3]);
+        if (t < K) {
+          const float qe = qc[t * JH];
+          const float4 ve = sc[t * step4];
+          e.x = fmaf(qe, ve.x, e.x);
+          e.y = fmaf(qe, ve.y, e.y);
+          e.z = fmaf(qe, ve.z, e.z);
+          e.w = fmaf(qe, ve.w, e.w);
+        }
+        const float sg = odd ? -1.f : 1.f;
+        if (has_a) {
+          outa0[rn] = make_float2(e.x + o.x, e.y + o.y);
+          outa0[rs] = make_float2(sg * (e.x - o.x), sg * (e.y - o.y));
+        }
+        if (has_b) {
+          outb0[rn] = make_float2(e.z + o.z, e.w + o.w);
+          outb0[rs] = make_float2(sg * (e.z - o.z), sg * (e.w - o.w));
+        }
+      } else {
+        const float* qd = qc + nt * JH;
+        const float4* zc = sc + (size_t)nt * step4;
+        // Term t's contribution to u and v: a(t) * (dim, -dre, zim, -zre)
+        // + b(t) * (zre, zim, -dre, -dim); the even-t a part and odd-t b
+        // part go to X, the rest to Y: north = X + Y, south = X - Y.
+        float X[2][4] = {}, Y[2][4] = {};
+        auto add = [&](float (*acc_a)[4], float (*acc_b)[4], float a, float b, int t) {
+          const float4 D = sc[t * step4], Z = zc[t * step4];
+          const float2 Dp[2] = {make_float2(D.x, D.y), make_float2(D.z, D.w)};
+          const float2 Zp[2] = {make_float2(Z.x, Z.y), make_float2(Z.z, Z.w)};
+#pragma unroll
+          for (int pp = 0; pp < 2; ++pp) {
+            acc_a[pp][0] = fmaf(a, Dp[pp].y, acc_a[pp][0]);
+            acc_a[pp][1] = fmaf(-a, Dp[pp].x, acc_a[pp][1]);
+            acc_a[pp][2] = fmaf(a, Zp[pp].y, acc_a[pp][2]);
+            acc_a[pp][3] = fmaf(-a, Zp[pp].x, acc_a[pp][3]);
+            acc_b[pp][0] = fmaf(b, Zp[pp].x, acc_b[pp][0]);
+            acc_b[pp][1] = fmaf(b, Zp[pp].y, acc_b[pp][1]);
+            acc_b[pp][2] = fmaf(-b, Dp[pp].x, acc_b[pp][2]);
+            acc_b[pp][3] = fmaf(-b, Dp[pp].y, acc_b[pp][3]);
+          }
+        };
+        int t = 0;
+        for (; t + 1 < K; t += 2) {
+          add(X, Y, qc[t * JH], qd[t * JH], t);
+          add(Y, X, qc[(t + 1) * JH], qd[(t + 1) * JH], t + 1);
+        }
+        if (t < K) add(X, Y, qc[t * JH], qd[t * JH], t);
+        float2* outa1 = reinterpret_cast<float2*>(f1 + (size_t)(p0 + pa) * plane_floats);
+        float2* outb1 = outa1 + plane_floats / 2;
+        if (has_a) {
+          outa0[rn] = make_float2(X[0][0] + Y[0][0], X[0][1] + Y[0][1]);
+          outa0[rs] = make_float2(X[0][0] - Y[0][0], X[0][1] - Y[0][1]);
+          outa1[rn] = make_float2(X[0][2] + Y[0][2], X[0][3] + Y[0][3]);
+          outa1[rs] = make_float2(X[0][2] - Y[0][2], X[0][3] - Y[0][3]);
+        }
+        if (has_b) {
+          outb0[rn] = make_float2(X[1][0] + Y[1][0], X[1][1] + Y[1][1]);
+          outb0[rs] = make_float2(X[1][0] - Y[1][0], X[1][1] - Y[1][1]);
+          outb1[rn] = make_float2(X[1][2] + Y[1][2], X[1][3] + Y[1][3]);
+          outb1[rs] = make_float2(X[1][2] - Y[1][2], X[1][3] - Y[1][3]);
+        }
       }
     }
+    __syncthreads();  // this buffer is restaged two items on
+    item = next;
   }
+  cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------- forward
@@ -307,9 +338,16 @@ __global__ void __launch_bounds__(kForwardThreads) k_sym_forward(SymIn<NIN> in, 
   }
 }
 
-size_t inverse_smem(const Dims& d, int nin, int group, int tile) {
+// Floats of one staging buffer of the inverse (a 16-byte multiple); a
+// block holds two.
+size_t inverse_buffer_floats(const Dims& d, int nin, int group, int tile) {
   const size_t nt = group_terms(d, group);
-  return (size_t)nin * nt * tile * 8 + (size_t)nin * nt * (d.NLAT / 2) * 4;
+  const size_t f = (size_t)2 * nin * nt * tile + (size_t)nin * nt * (d.NLAT / 2);
+  return (f + 3) / 4 * 4;
+}
+
+size_t inverse_smem(const Dims& d, int nin, int group, int tile) {
+  return 2 * inverse_buffer_floats(d, nin, group, tile) * sizeof(float);
 }
 
 // Forward: kFwdTile planes per block; the group of wavenumbers is tuned.
@@ -334,6 +372,20 @@ void launch_sym_forward(const Model& m, SymIn<NIN> in, float* out0, float* out1,
 
 }  // namespace
 
+// The persistent grid: resident blocks per SM for a launch shape, times
+// the SM count.
+int persistent_grid(const void* kernel, int threads, size_t smem) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  return sms * (per_sm > 0 ? per_sm : 1);
+}
+
 void leg_init() {
   allow_smem(k_sym_inverse<0>);
   allow_smem(k_sym_inverse<1>);
@@ -343,22 +395,28 @@ void leg_init() {
   allow_smem(k_sym_forward<3, 3>);
 }
 
-void leg_inverse(const Model& m, const float* s, float* f, int planes, bool derivative, cudaStream_t st) {
-  const int group = m.tune.inv_group[0], tile = m.tune.inv_tile[0];
-  dim3 grid((m.d.NTP1 + group - 1) / group, (planes + tile - 1) / tile);
+template <int KIND>
+void launch_inverse(const Model& m, const float* s0, const float* s1, float* f0, float* f1, int planes,
+                    const float* qa, const float* qb, int odd, float plavor, cudaStream_t st) {
+  const int nin = KIND == 0 ? 1 : 2;
+  const int group = m.tune.inv_group[KIND], tile = m.tune.inv_tile[KIND];
   const int threads = (m.d.NLAT / 2) * tile / 2;
-  k_sym_inverse<0><<<grid, threads, inverse_smem(m.d, 1, group, tile), st>>>(
-      s, nullptr, f, nullptr, planes, tile, group, derivative ? m.sh.qjT : m.sh.qiT, nullptr, derivative ? 1 : 0, 0.f,
-      m.d);
+  const size_t smem = inverse_smem(m.d, nin, group, tile);
+  const int items = ((m.d.NTP1 + group - 1) / group) * ((planes + tile - 1) / tile);
+  const int grid = std::min(items, persistent_grid((const void*)k_sym_inverse<KIND>, threads, smem));
+  k_sym_inverse<KIND><<<grid, threads, smem, st>>>(s0, s1, f0, f1, planes, tile, group, group_terms(m.d, group),
+                                                   (int)inverse_buffer_floats(m.d, nin, group, tile), qa, qb, odd,
+                                                   plavor, m.d);
+}
+
+void leg_inverse(const Model& m, const float* s, float* f, int planes, bool derivative, cudaStream_t st) {
+  launch_inverse<0>(m, s, nullptr, f, nullptr, planes, derivative ? m.sh.qjT : m.sh.qiT, nullptr,
+                    derivative ? 1 : 0, 0.f, st);
 }
 
 void leg_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V, int planes, float plavor,
                cudaStream_t st) {
-  const int group = m.tune.inv_group[1], tile = m.tune.inv_tile[1];
-  dim3 grid((m.d.NTP1 + group - 1) / group, (planes + tile - 1) / tile);
-  const int threads = (m.d.NLAT / 2) * tile / 2;
-  k_sym_inverse<1><<<grid, threads, inverse_smem(m.d, 2, group, tile), st>>>(D, Z, U, V, planes, tile, group,
-                                                                             m.sh.quT, m.sh.qvT, 0, plavor, m.d);
+  launch_inverse<1>(m, D, Z, U, V, planes, m.sh.quT, m.sh.qvT, 0, plavor, st);
 }
 
 // Shared memory a tuning asks of each transform kernel, and the default
