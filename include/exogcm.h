@@ -93,7 +93,9 @@ int exogcm_last_error(char* buffer, size_t size);
  * `mode` 0: the plain path (truncated-DFT longitude transforms and one thread
  * per Legendre output, as the reference's shaders); 1: the optimized path
  * (warp-shuffle FFTs, latitude-pair Legendre transforms on m-major Fourier
- * planes). Both compute in FP32 and share the physics. */
+ * planes); 2: the optimized path with sp2fc and sp2fcdmu as tcgen05 tensor-
+ * core contractions in 3xTF32 (FP32-equivalent to about 2^-21). All compute
+ * in FP32 and share the physics. */
 int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine** engine);
 void exogcm_destroy(exogcm_engine* engine);
 

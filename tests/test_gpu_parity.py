@@ -101,7 +101,8 @@ PHYSICS_FIELDS = {
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("truncation,levels,warm,mode", [(21, 10, 6, 0), (21, 5, 6, 0), (42, 10, 4, 0),
-                                                         (21, 10, 6, 1), (42, 10, 4, 1), (63, 10, 4, 1)])
+                                                         (21, 10, 6, 1), (42, 10, 4, 1), (63, 10, 4, 1),
+                                                         (42, 10, 4, 2)])
 def test_stage_replay_matches_oracle(truncation, levels, warm, mode):
     worst = _stage_errors(truncation, levels, warm, mode=mode)
     report = sorted(((v[0], k, v[1]) for k, v in worst.items()), reverse=True)[:12]
@@ -132,13 +133,14 @@ def test_one_day_trajectory_t21_l10(mode):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("truncation", [21, 42, 63])
-def test_fft_matches_dense_dft(truncation):
-    """The optimized path's FFTs give the plain path's truncated DFT: one
+@pytest.mark.parametrize("truncation,mode", [(21, 1), (42, 1), (63, 1), (21, 2), (42, 2), (63, 2)])
+def test_fft_matches_dense_dft(truncation, mode):
+    """The optimized paths' transforms (FFTs, latitude-pair Legendre; mode 2
+    with sp2fc and sp2fcdmu on the tensor cores) give the plain path's: one
     gridpointa from the same state in both modes."""
     p = planets.make_planet(71, truncation=truncation, levels=10)
     plain = pkg.Engine(truncation, 10, 1, mode=0)
-    fast = pkg.Engine(truncation, 10, 1, mode=1)
+    fast = pkg.Engine(truncation, 10, 1, mode=mode)
     plain.configure(0, p)
     fast.configure(0, p)
     plain.step(4)

@@ -110,6 +110,11 @@ struct SharedTabs {
   const float* qjT;
   const float* quT;
   const float* qvT;
+  // Tensor-core inverse operands: per m, the hi and lo images of the full
+  // qi / qj tables in the MMA's shared-memory layout, at float offset tc_at[m].
+  const float* tc_qi;
+  const float* tc_qj;
+  const int* tc_at;
 };
 
 // Launch shapes of the optimized path's transforms, measured per engine by
@@ -134,7 +139,9 @@ struct Model {
   const StepParams* params;  // [S] for the step being run
   double* sums;              // FP64 per-slot reductions scratch [S][4]
   int* flags;                // per-slot status flags [S]
-  int mode;                  // 0 plain path, 1 optimized path (FFTs, latitude-pair Legendre, m-major Fourier)
+  int* fault;                // nonzero after a kernel gave up a bounded wait
+  int mode;                  // 0 plain path, 1 optimized path (FFTs, latitude-pair Legendre, m-major Fourier),
+                             // 2 optimized path with sp2fc / sp2fcdmu on the tensor cores
   Tuning tune;               // optimized path launch shapes
 };
 

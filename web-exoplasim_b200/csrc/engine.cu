@@ -102,6 +102,7 @@ struct exogcm_engine {
   StepParams* hparams = nullptr;  // pinned host
   double* sums = nullptr;
   int* flags = nullptr;
+  int* fault = nullptr;  // device word: a kernel gave up a bounded wait
   std::vector<Slot> slots;
   std::map<int, cudaGraphExec_t> graphs;
   Tuning tune{};
@@ -118,6 +119,7 @@ struct exogcm_engine {
     m.params = params + (size_t)k * d.S;
     m.sums = sums;
     m.flags = flags;
+    m.fault = fault;
     m.mode = mode;
     m.tune = tune;
     return m;
@@ -220,7 +222,7 @@ void copy_field(exogcm_engine* e, const FieldInfo& fi, int slot, void* host, boo
   float* base = e->arena + fi.offset + (size_t)slot * fi.plane;
   const size_t pitch = fi.plane * e->d.S * sizeof(float);
   const size_t width = fi.plane * sizeof(float);
-  const bool m_major = e->mode == 1 && fi.shape == 'F';
+  const bool m_major = e->mode >= 1 && fi.shape == 'F';
   std::vector<float> staged;
   void* h = host;
   if (m_major) {
@@ -288,11 +290,24 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
       for (int w = 0; w < d.NCSP; ++w) t[(size_t)w * JH + j] = q[(size_t)j * d.NCSP + w];
     qt[i] = put(t);
   }
+  // Tensor-core inverse: hi/lo images of the full qi and qj tables per m.
+  std::vector<int> tc_at;
+  const std::vector<float> img_qi = tc_table_images(d, s.q.at("qi"), tc_at);
+  const std::vector<float> img_qj = tc_table_images(d, s.q.at("qj"), tc_at);
+  auto put_floats = [&](const std::vector<float>& v) {
+    while (buf.size() % 32) buf.push_back(0.f);
+    const size_t at = buf.size();
+    buf.insert(buf.end(), v.begin(), v.end());
+    return at;
+  };
+  const size_t itc_qi = put_floats(img_qi), itc_qj = put_floats(img_qj);
   check(cudaMalloc(&e->shared_buf, buf.size() * sizeof(float)), "shared tables");
   check(cudaMemcpy(e->shared_buf, buf.data(), buf.size() * sizeof(float), cudaMemcpyHostToDevice), "shared tables");
-  check(cudaMalloc(&e->mode_buf, 2 * d.NCSP * sizeof(int)), "mode tables");
+  check(cudaMalloc(&e->mode_buf, (2 * d.NCSP + tc_at.size()) * sizeof(int)), "mode tables");
   check(cudaMemcpy(e->mode_buf, mm.data(), d.NCSP * sizeof(int), cudaMemcpyHostToDevice), "mode tables");
   check(cudaMemcpy(e->mode_buf + d.NCSP, nn.data(), d.NCSP * sizeof(int), cudaMemcpyHostToDevice), "mode tables");
+  check(cudaMemcpy(e->mode_buf + 2 * d.NCSP, tc_at.data(), tc_at.size() * sizeof(int), cudaMemcpyHostToDevice),
+        "mode tables");
   float* b = e->shared_buf;
   e->sh.fwd = b + fwd;
   e->sh.inv = b + inv;
@@ -314,6 +329,9 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
   e->sh.qjT = b + qt[1];
   e->sh.quT = b + qt[2];
   e->sh.qvT = b + qt[3];
+  e->sh.tc_qi = b + itc_qi;
+  e->sh.tc_qj = b + itc_qj;
+  e->sh.tc_at = e->mode_buf + 2 * d.NCSP;
   e->sh.mode_m = e->mode_buf;
   e->sh.mode_n = e->mode_buf + d.NCSP;
   e->shared_ready = true;
@@ -679,7 +697,8 @@ int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine
       throw Error(EXOGCM_EINVAL, "truncation must be 21, 42 or 63");
     if (levels != 5 && levels != 10) throw Error(EXOGCM_EINVAL, "levels must be 5 or 10");
     if (slots < 1 || slots > 4096) throw Error(EXOGCM_EINVAL, "slots must be 1..4096");
-    if (mode != 0 && mode != 1) throw Error(EXOGCM_EINVAL, "mode must be 0 (plain FP32) or 1 (optimized)");
+    if (mode < 0 || mode > 2)
+      throw Error(EXOGCM_EINVAL, "mode must be 0 (plain FP32), 1 (optimized) or 2 (optimized, tensor-core sp2fc)");
     auto e = std::make_unique<exogcm_engine>();
     e->d = make_dims(truncation, levels, slots);
     e->mode = mode;
@@ -705,6 +724,8 @@ int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine
     check(cudaMemset(e->sums, 0, (size_t)slots * 4 * sizeof(double)), "sums");
     check(cudaMalloc(&e->flags, slots * sizeof(int)), "flags");
     check(cudaMemset(e->flags, 0, slots * sizeof(int)), "flags");
+    check(cudaMalloc(&e->fault, sizeof(int)), "fault word");
+    check(cudaMemset(e->fault, 0, sizeof(int)), "fault word");
     check(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "stream");
     check(cudaEventCreate(&e->ev0), "event");
     check(cudaEventCreate(&e->ev1), "event");
@@ -727,6 +748,7 @@ void exogcm_destroy(exogcm_engine* e) {
   cudaFreeHost(e->hparams);
   cudaFree(e->sums);
   cudaFree(e->flags);
+  cudaFree(e->fault);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -742,7 +764,7 @@ int exogcm_configure(exogcm_engine* e, int slot, const exogcm_planet* planet, co
     if (!e->shared_ready) {
       e->shared_setup = build_shared(e->d.T, planet->filter_kind, planet->filter_gp, planet->filter_sp);
       upload_shared(e, e->shared_setup);
-      if (e->mode == 1) autotune(e);
+      if (e->mode >= 1) autotune(e);
       e->filter_kind = planet->filter_kind;
       e->filter_gp = planet->filter_gp;
       e->filter_sp = planet->filter_sp;
@@ -859,6 +881,12 @@ int exogcm_step(exogcm_engine* e, int steps, int publish_every) {
     check(cudaEventRecord(e->ev1, e->stream), "event");
     phy_finite_check(e->model(steps - 1), e->stream);
     check(cudaStreamSynchronize(e->stream), "step");
+    int fault = 0;
+    check(cudaMemcpy(&fault, e->fault, sizeof(int), cudaMemcpyDeviceToHost), "fault word");
+    if (fault) {
+      check(cudaMemset(e->fault, 0, sizeof(int)), "fault word");
+      throw Error(EXOGCM_EDEVICE, "a tensor-core transform gave up waiting for its MMAs; this step's results are invalid");
+    }
     check(cudaEventElapsedTime(&e->last_ms, e->ev0, e->ev1), "event time");
   });
 }

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 
@@ -38,6 +39,11 @@ void leg_uv2dv(const Model& m, const float* u, const float* v, const float* ke, 
                cudaStream_t st);
 void leg_qtend(const Model& m, const float* u, const float* v, const float* src, float* out, int planes,
                cudaStream_t st);
+
+// legendre_tc.cu (optimized path, tensor cores)
+void tc_init();
+std::vector<float> tc_table_images(const Dims& d, const std::vector<double>& q, std::vector<int>& at);
+void tc_inverse(const Model& m, const float* s, float* f, int planes, bool derivative, cudaStream_t st);
 
 // fft.cu (optimized path; Fourier planes m-major)
 void fft_init();

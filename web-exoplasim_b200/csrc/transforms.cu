@@ -327,6 +327,7 @@ int dft_rows_per_block(const Dims& d) { return d.NLAT == 96 ? 24 : 32; }
 
 void tr_init() {
   leg_init();
+  tc_init();
   fft_init();
   allow_smem(k_dft_forward);
   allow_smem(k_dft_inverse);
@@ -339,7 +340,7 @@ void tr_init() {
 }
 
 void tr_fourier_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st) {
-  if (m.mode == 1) return fft_forward(m, g, c, planes, st);
+  if (m.mode >= 1) return fft_forward(m, g, c, planes, st);
   const int rows = planes * m.d.NLAT;
   const int rpb = dft_rows_per_block(m.d);
   const size_t smem = ((size_t)m.d.NLON * m.d.NFC + (size_t)rpb * m.d.NLON) * sizeof(float);
@@ -347,7 +348,7 @@ void tr_fourier_forward(const Model& m, const float* g, float* c, int planes, cu
 }
 
 void tr_fourier_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st) {
-  if (m.mode == 1) return fft_inverse(m, c, g, planes, st);
+  if (m.mode >= 1) return fft_inverse(m, c, g, planes, st);
   const int rows = planes * m.d.NLAT;
   const int rpb = dft_rows_per_block(m.d);
   const size_t smem = ((size_t)m.d.NLON * m.d.NFC + (size_t)rpb * m.d.NFC) * sizeof(float);
@@ -356,7 +357,7 @@ void tr_fourier_inverse(const Model& m, const float* c, float* g, int planes, cu
 
 void tr_dlambda(const Model& m, const float* a, float* b, int planes, cudaStream_t st) {
   const int n = planes * m.d.NLAT * m.d.NTP1;
-  if (m.mode == 1) {
+  if (m.mode >= 1) {
     k_dlambda_m_major<<<(n + 255) / 256, 256, 0, st>>>(a, b, n, m.d.NLAT, m.d.NTP1);
     return;
   }
@@ -365,7 +366,10 @@ void tr_dlambda(const Model& m, const float* a, float* b, int planes, cudaStream
 
 void tr_legendre_inverse(const Model& m, const float* s, float* f, int planes, const float* q,
                          cudaStream_t st) {
-  if (m.mode == 1 && (q == m.sh.qi || q == m.sh.qj)) return leg_inverse(m, s, f, planes, q == m.sh.qj, st);
+  if (m.mode >= 1 && (q == m.sh.qi || q == m.sh.qj)) {
+    if (m.mode == 2) return tc_inverse(m, s, f, planes, q == m.sh.qj, st);
+    return leg_inverse(m, s, f, planes, q == m.sh.qj, st);
+  }
   const InvTile t = inverse_tile(m.d, 1, 1);
   dim3 grid((planes + kInvPlanes - 1) / kInvPlanes, m.d.NLAT / t.lats);
   k_leg_inverse<<<grid, kThreads, t.smem, st>>>(s, f, planes, q, m.d, t.lats);
@@ -373,7 +377,7 @@ void tr_legendre_inverse(const Model& m, const float* s, float* f, int planes, c
 
 void tr_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V, int planes, float plavor,
               cudaStream_t st) {
-  if (m.mode == 1) return leg_dv2uv(m, D, Z, U, V, planes, plavor, st);
+  if (m.mode >= 1) return leg_dv2uv(m, D, Z, U, V, planes, plavor, st);
   const InvTile t = inverse_tile(m.d, 2, 2);
   dim3 grid((planes + kInvPlanes - 1) / kInvPlanes, m.d.NLAT / t.lats);
   k_dv2uv<<<grid, kThreads, t.smem, st>>>(D, Z, U, V, planes, m.sh.qu, m.sh.qv, plavor, m.d, t.lats);
@@ -381,14 +385,14 @@ void tr_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V
 
 void tr_legendre_forward(const Model& m, const float* f, float* s, int planes, const float* q,
                          cudaStream_t st) {
-  if (m.mode == 1) return leg_forward(m, f, s, planes, q, st);
+  if (m.mode >= 1) return leg_forward(m, f, s, planes, q, st);
   FwdIn<1> in{{f}};
   launch_forward<0, 1>(m, in, s, nullptr, planes, q, st);
 }
 
 void tr_uv2dv(const Model& m, const float* u, const float* v, const float* ke, float* D, float* Z, int planes,
               cudaStream_t st) {
-  if (m.mode == 1) return leg_uv2dv(m, u, v, ke, D, Z, planes, st);
+  if (m.mode >= 1) return leg_uv2dv(m, u, v, ke, D, Z, planes, st);
   if (ke) {
     FwdIn<3> in{{u, v, ke}};
     launch_forward<2, 3>(m, in, D, Z, planes, nullptr, st);
@@ -400,7 +404,7 @@ void tr_uv2dv(const Model& m, const float* u, const float* v, const float* ke, f
 
 void tr_qtend(const Model& m, const float* u, const float* v, const float* src, float* out, int planes,
               cudaStream_t st) {
-  if (m.mode == 1) return leg_qtend(m, u, v, src, out, planes, st);
+  if (m.mode >= 1) return leg_qtend(m, u, v, src, out, planes, st);
   FwdIn<3> in{{u, v, src}};
   launch_forward<3, 3>(m, in, out, nullptr, planes, nullptr, st);
 }
