@@ -285,13 +285,14 @@ def main():
     e2e_calls = max(1, args.steps // publish)
     snap_floats = engine.field_size("snapshot")
     import numpy as np
-    host = np.zeros(snap_floats, dtype=np.float32)
+    # every slot's published snapshot lands in its own row of pinned host memory
+    host = torch.empty((slots, snap_floats), dtype=torch.float32, pin_memory=True).numpy()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_calls):
         engine.step(publish, publish_every=publish)
         for s in range(slots):
-            engine.read_snapshot_into(s, host)
+            engine.read_snapshot_into(s, host[s])
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_steps = e2e_calls * publish
