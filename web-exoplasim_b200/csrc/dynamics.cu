@@ -25,20 +25,37 @@ __device__ __forceinline__ const float* slot_tabs(const Model& m, int slot) {
 template <int NL>
 __global__ void __launch_bounds__(kBlock) k_calcgp(Model m) {
   const Dims& d = m.d;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.S * d.NHOR) return;
-  const int slot = c / d.NHOR;
+  // NHOR is a multiple of kBlock at every truncation, so a block lies in one
+  // slot and that slot's vertical tables are staged in shared memory once.
+  const int slot = blockIdx.x * kBlock / d.NHOR;
   if (!m.params[slot].active) return;
+  __shared__ float stage[6 * NL + 2 * NL * NL];
+  float* ds = stage;
+  float* t0T = ds + NL;
+  float* sh = t0T + NL;
+  float* rd = sh + NL;
+  float* t01 = rd + NL;
+  float* tkpT = t01 + NL;
+  float* C = tkpT + NL;
+  float* G = C + NL * NL;
+  {
+    const float* tb = slot_tabs(m, slot);
+    for (int i = threadIdx.x; i < NL * NL; i += kBlock) {
+      C[i] = tb[m.to.c + i];
+      G[i] = tb[m.to.g + i];
+    }
+    for (int i = threadIdx.x; i < NL; i += kBlock) {
+      ds[i] = tb[m.to.dsigma + i];
+      t0T[i] = tb[m.to.t0 + i];
+      sh[i] = tb[m.to.sigmah + i];
+      rd[i] = tb[m.to.rdsig + i];
+      t01[i] = tb[m.to.t01s2 + i];
+      tkpT[i] = tb[m.to.tkp + i];
+    }
+  }
+  __syncthreads();
+  const int c = blockIdx.x * kBlock + threadIdx.x;
   const PlanetConst& K = m.pc[slot];
-  const float* tb = slot_tabs(m, slot);
-  const float* ds = tb + m.to.dsigma;
-  const float* t0T = tb + m.to.t0;
-  const float* sh = tb + m.to.sigmah;
-  const float* rd = tb + m.to.rdsig;
-  const float* t01 = tb + m.to.t01s2;
-  const float* tkpT = tb + m.to.tkp;
-  const float* C = tb + m.to.c;
-  const float* G = tb + m.to.g;
   const size_t SN = (size_t)d.S * d.NHOR;
   const FieldPtrs& F = m.f;
   const float rcsq = m.sh.rcsq[c % d.NHOR];
@@ -304,12 +321,11 @@ __global__ void __launch_bounds__(kBlock) k_spectrald_diffusion(Model m) {
 // mkdheat's grid-point stages (dynamics/wgsl/mkdheat.wgsl).
 __global__ void __launch_bounds__(kBlock) k_mkdheat(Model m, int stage) {
   const Dims& d = m.d;
-  const size_t SN = (size_t)d.S * d.NHOR;
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.NLEV * SN) return;
-  const int l = (int)(i / SN);
-  const int c = (int)(i % SN);
-  const int slot = c / d.NHOR, h = c % d.NHOR;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.S * d.NHOR) return;
+  const int l = blockIdx.y;
+  const size_t i = (size_t)l * d.S * d.NHOR + c;
+  const int slot = c / d.NHOR, h = c - slot * d.NHOR;
   const StepParams& P = m.params[slot];
   if (!P.active) return;
   const PlanetConst& K = m.pc[slot];
@@ -334,10 +350,11 @@ __global__ void __launch_bounds__(kBlock) k_mkdheat(Model m, int stage) {
 }
 
 // mkdheat's zsdef(2:NESP,:) = 0 (dynamics/wgsl/mean-mode.wgsl).
-__global__ void k_mean_mode(float* t, size_t n, int nrsp) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (i % nrsp != 0) t[i] = 0.f;
+// One block row per plane: blockIdx.y = slot, blockIdx.z = level.
+__global__ void k_mean_mode(float* t, int nrsp) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrsp || r == 0) return;
+  t[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * nrsp + r] = 0.f;
 }
 
 // spectrald after mkdheat (dynamics/wgsl/spectrald-update.wgsl).
@@ -417,11 +434,10 @@ __global__ void __launch_bounds__(kBlock) k_physics_in(Model m) {
 // gridpointd after the parameterizations (dynamics/wgsl/physics-out.wgsl).
 __global__ void __launch_bounds__(kBlock) k_physics_out(Model m) {
   const Dims& d = m.d;
-  const size_t SN = (size_t)d.S * d.NHOR;
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.NLEV * SN) return;
-  const int c = (int)(i % SN);
-  const int slot = c / d.NHOR, h = c % d.NHOR;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.S * d.NHOR) return;
+  const size_t i = (size_t)blockIdx.y * d.S * d.NHOR + c;
+  const int slot = c / d.NHOR, h = c - slot * d.NHOR;
   if (!m.params[slot].active) return;
   const PlanetConst& K = m.pc[slot];
   const FieldPtrs& F = m.f;
@@ -437,7 +453,8 @@ inline unsigned blocks(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
 }  // namespace
 
 void dyn_calcgp(const Model& m, cudaStream_t st) {
-  const unsigned n = blocks((size_t)m.d.S * m.d.NHOR, kBlock);
+  static_assert(2048 % kBlock == 0, "k_calcgp assumes a block lies in one slot");
+  const unsigned n = (unsigned)((size_t)m.d.S * m.d.NHOR / kBlock);
   if (m.d.L == 10)
     k_calcgp<10><<<n, kBlock, 0, st>>>(m);
   else
@@ -454,11 +471,12 @@ void dyn_spectrald_diffusion(const Model& m, cudaStream_t st) {
   k_spectrald_diffusion<<<blocks((size_t)m.d.S * m.d.NRSP, kBlock), kBlock, 0, st>>>(m);
 }
 void dyn_mkdheat(const Model& m, int stage, cudaStream_t st) {
-  k_mkdheat<<<blocks((size_t)m.d.NLEV * m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m, stage);
+  const dim3 grid(blocks((size_t)m.d.S * m.d.NHOR, kBlock), m.d.NLEV);
+  k_mkdheat<<<grid, kBlock, 0, st>>>(m, stage);
 }
 void dyn_mean_mode(const Model& m, float* target, cudaStream_t st) {
-  const size_t n = (size_t)m.d.NLEV * m.d.S * m.d.NRSP;
-  k_mean_mode<<<blocks(n, 256), 256, 0, st>>>(target, n, m.d.NRSP);
+  const dim3 grid(blocks((size_t)m.d.NRSP, 256), m.d.S, m.d.NLEV);
+  k_mean_mode<<<grid, 256, 0, st>>>(target, m.d.NRSP);
 }
 void dyn_spectrald_update(const Model& m, cudaStream_t st) {
   k_spectrald_update<<<blocks((size_t)m.d.S * m.d.NRSP, kBlock), kBlock, 0, st>>>(m);
@@ -467,7 +485,8 @@ void dyn_physics_in(const Model& m, cudaStream_t st) {
   k_physics_in<<<blocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);
 }
 void dyn_physics_out(const Model& m, cudaStream_t st) {
-  k_physics_out<<<blocks((size_t)m.d.NLEV * m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);
+  const dim3 grid(blocks((size_t)m.d.S * m.d.NHOR, kBlock), m.d.NLEV);
+  k_physics_out<<<grid, kBlock, 0, st>>>(m);
 }
 
 }  // namespace exogcm

@@ -2009,15 +2009,15 @@ __global__ void __launch_bounds__(kBlock) k_pack(Model m) {
 // flags[slot] = 1 when any coefficient of sp, st, sz, sd or sq is NaN or Inf.
 __global__ void k_finite(Model m) {
   const Dims& d = m.d;
-  const size_t SR = (size_t)d.S * d.NRSP;
-  const size_t n = (size_t)d.NLEV * SR;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int c = (int)(i % SR);
-    const int slot = c / d.NRSP;
-    if (!m.params[slot].active) continue;
-    const float v = m.f.st[i] + m.f.sz[i] + m.f.sd[i] + m.f.sq[i] + (i < SR ? m.f.sp[i] : 0.f);
-    if (!isfinite(v)) m.flags[slot] = 1;
-  }
+  const int SR = d.S * d.NRSP;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= SR) return;
+  const int slot = c / d.NRSP;
+  if (!m.params[slot].active) return;
+  const int l = blockIdx.y;
+  const size_t i = (size_t)l * SR + c;
+  const float v = m.f.st[i] + m.f.sz[i] + m.f.sd[i] + m.f.sq[i] + (l == 0 ? m.f.sp[c] : 0.f);
+  if (!isfinite(v)) m.flags[slot] = 1;
 }
 
 inline unsigned nblocks(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -2107,7 +2107,10 @@ void phy_carbon(const Model& m, cudaStream_t st) { by_levels<Carbon>(m.d.L, m, s
 
 void phy_pack(const Model& m, cudaStream_t st) { by_levels<Pack>(m.d.L, m, st); }
 
-void phy_finite_check(const Model& m, cudaStream_t st) { k_finite<<<592, 256, 0, st>>>(m); }
+void phy_finite_check(const Model& m, cudaStream_t st) {
+  const dim3 grid(nblocks((size_t)m.d.S * m.d.NRSP, 256), m.d.NLEV);
+  k_finite<<<grid, 256, 0, st>>>(m);
+}
 
 bool phy_launch_one(const Model& m, const std::string& kernel, cudaStream_t st) {
   const int L = m.d.L;
