@@ -628,7 +628,7 @@ void autotune(exogcm_engine* e) {
     float best = 1e30f;
     int pick = t.fft_rows;
     for (int rows : {8, 16, 32, 48, 64, 96}) {
-      if (rows > d.NLAT || d.NLAT % rows || fft_chunk_smem(d, rows) > kLegSmemLimit) continue;
+      if (!fft_rows_supported(d, rows)) continue;
       t.fft_rows = rows;
       const float ms = time([&](const Model& m) {
         tr_fourier_inverse(m, F.fgu, F.gu, LP, e->stream);

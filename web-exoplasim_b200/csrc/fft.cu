@@ -1,30 +1,32 @@
-// Longitude transforms as warp-per-row real FFTs (the optimized path).
+// Longitude transforms as register FFTs, T threads per latitude row (the
+// optimized path).
 //
 // Same results as the truncated DFT of fourier/index.ts:19-36 (gp2fc keeps
 // c_m = (1/N) sum_j g_j e^{-i m lambda_j} for m <= NTRU; fc2gp sums
 // Re c_0 + 2 Re sum_{m>=1} c_m e^{i m lambda_j}, ignoring Im c_0), computed in
 // O(N log N): a real row of N = 2M points is packed as z_n = g_2n + i g_2n+1,
 // transformed by an M-point complex FFT, and split into the even/odd halves.
-// M = 32 R with R = 1, 2, 3 (T21, T42, T63): each lane of a warp holds the R
-// elements n1 + 32 n2 of its row; a radix-R step in registers is followed by
-// a 32-point decimation-in-frequency FFT across the lanes (five xor-shuffle
-// butterfly stages). Twiddles come from a table of e^{2 pi i j / N} built in
-// FP64 on the host and rounded once. Warp shuffles put the bit-reversed FFT
-// output back in natural order.
 //
-// The optimized path stores Fourier planes m-major (coefficient (m, lat) at
-// 2 * (m * NLAT + lat)), so that the Legendre transforms on either side
-// stream whole runs of latitudes. One block transforms a chunk of `rows`
-// consecutive latitudes of one plane: the chunk's coefficients pass through
-// shared memory ([m][rows + 1]) between that layout (runs of `rows`
-// latitudes per m) and the warps' rows, so both global sides stay
-// contiguous. Small chunks give many blocks per SM at different phases, so
-// one block's loads overlap another's arithmetic.
+// The M-point FFT is the four-step factorisation M = 8 Q (Q = 4, 8, 12 for
+// T21, T42, T63): with n = Q p + q and k = k1 + 8 k2,
+//   A[q][k1] = sum_p z[Q p + q] w_8^{p k1}          (Q DFT-8s)
+//   B[q][k1] = A[q][k1] w_M^{q k1}                  (twiddle)
+//   Z[k1 + 8 k2] = sum_q B[q][k1] w_Q^{q k2}        (8 DFT-Qs)
+// A row's T threads (consecutive lanes of one warp) each run Q/T DFT-8s and
+// 8/T DFT-Qs in registers; B passes between them through shared memory at
+// position 9 q + k1, a pitch that keeps every 64-bit access of a half-warp on
+// distinct banks. Twiddles come from a table of e^{2 pi i j / N} built in FP64
+// on the host and rounded once.
+//
+// Fourier planes are m-major on this path (coefficient (m, lat) at
+// 2 * (m * NLAT + lat)). A block transforms `rows` consecutive latitudes of
+// one plane; the chunk's coefficients pass through shared memory
+// ([m][pitch]) so that the m-major side is read and written in runs of
+// `rows` latitudes.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 
-#include "async_copy.cuh"
 #include "common.cuh"
 #include "launch.h"
 
@@ -32,237 +34,282 @@ namespace exogcm {
 
 namespace {
 
-constexpr int kWarps = 4;
+constexpr int kMaxThreads = 512;
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float2 conj2(float2 a) { return make_float2(a.x, -a.y); }
 
-// e^{sign 2 pi i t / N} from the table tw[t] = (cos, sin)(2 pi t / N).
-template <int SIGN>
-__device__ __forceinline__ float2 twiddle(const float2* tw, int t, int N) {
-  float2 w = tw[t % N];
-  if (SIGN < 0) w.y = -w.y;
-  return w;
+// a * (S i)
+template <int S>
+__device__ __forceinline__ float2 mul_i(float2 a) {
+  return S > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
 
-__device__ __forceinline__ int bitrev5(int x) { return __brev(x) >> 27; }
-
-// In-register M-point FFTs of B rows at once (independent instruction
-// streams for the shuffle chains): x[b][r] = z_b[lane + 32 r]; on return
-// x[b][k2] holds Z_b[R * bitrev5(lane) + k2].
-template <int B, int R, int SIGN>
-__device__ __forceinline__ void warp_fft(float2 (&x)[B][R], const float2* tw, int N, int lane) {
-  // radix-R step per lane, then the twiddle w_M^{n1 k2}
-  if (R == 2) {
-    const float2 w = twiddle<SIGN>(tw, 2 * lane, N);
-#pragma unroll
-    for (int b = 0; b < B; ++b) {
-      const float2 p = x[b][0], q = x[b][1];
-      x[b][0] = cadd(p, q);
-      x[b][1] = cmul(csub(p, q), w);
-    }
-  } else if (R == 3) {
-    const float2 w3 = twiddle<SIGN>(tw, N / 3, N);      // e^{sign 2 pi i / 3}
-    const float2 w32 = twiddle<SIGN>(tw, 2 * N / 3, N); // e^{sign 4 pi i / 3}
-    const float2 t1 = twiddle<SIGN>(tw, 2 * lane, N), t2 = twiddle<SIGN>(tw, 4 * lane, N);
-#pragma unroll
-    for (int b = 0; b < B; ++b) {
-      const float2 p = x[b][0], q = x[b][1], u = x[b][2];
-      x[b][0] = cadd(cadd(p, q), u);
-      x[b][1] = cmul(cadd(cadd(p, cmul(q, w3)), cmul(u, w32)), t1);
-      x[b][2] = cmul(cadd(cadd(p, cmul(q, w32)), cmul(u, w3)), t2);
-    }
-  }
-  // 32-point DIF across lanes for each of the R sub-sequences
-#pragma unroll
-  for (int half = 16; half >= 1; half >>= 1) {
-    const bool upper = (lane & half) != 0;
-    const float2 w = twiddle<SIGN>(tw, (lane & (half - 1)) * (N / (2 * half)), N);
-#pragma unroll
-    for (int b = 0; b < B; ++b)
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        float2 y;
-        y.x = __shfl_xor_sync(0xffffffffu, x[b][r].x, half);
-        y.y = __shfl_xor_sync(0xffffffffu, x[b][r].y, half);
-        x[b][r] = upper ? cmul(csub(y, x[b][r]), w) : cadd(x[b][r], y);
-      }
-  }
+// a * e^{S 2 pi i j / 12} for a compile-time j in 0..6 (cos and sin of
+// multiples of 30 degrees).
+template <int S, int J>
+__device__ __forceinline__ float2 rot12(float2 a) {
+  constexpr float c30 = 0.866025403784438647f;
+  constexpr float cs[7] = {1.f, c30, 0.5f, 0.f, -0.5f, -c30, -1.f};
+  constexpr float sn[7] = {0.f, 0.5f, c30, 1.f, c30, 0.5f, 0.f};
+  if (J == 0) return a;
+  if (J == 3) return mul_i<S>(a);
+  if (J == 6) return make_float2(-a.x, -a.y);
+  const float c = cs[J], s = S * sn[J];
+  return make_float2(a.x * c - a.y * s, a.x * s + a.y * c);
 }
 
-constexpr int kRowsPerWarp = 2;
+// y_k = sum_p x_p e^{S 2 pi i p k / 4}, in place.
+template <int S>
+__device__ __forceinline__ void dft4(float2& x0, float2& x1, float2& x2, float2& x3) {
+  const float2 c0 = cadd(x0, x2), c1 = csub(x0, x2), d0 = cadd(x1, x3), d1 = mul_i<S>(csub(x1, x3));
+  x0 = cadd(c0, d0);
+  x2 = csub(c0, d0);
+  x1 = cadd(c1, d1);
+  x3 = csub(c1, d1);
+}
 
-// After warp_fft lane l holds Z[R * bitrev5(l) + r] in x[r]; this returns
-// y[r'] = Z[lane + 32 r'] for the calling lane. Element k sits in lane
-// bitrev5(k / R), register k % R: R shuffles of every register, one kept.
-template <int R>
-__device__ __forceinline__ void natural_order(const float2 (&x)[R], float2 (&y)[R], int lane) {
+// y_k = sum_p x_p e^{S 2 pi i p k / 3}, in place.
+template <int S>
+__device__ __forceinline__ void dft3(float2& x0, float2& x1, float2& x2) {
+  constexpr float h3 = 0.866025403784438647f;  // sin(60 degrees)
+  const float2 s = cadd(x1, x2), d = csub(x1, x2);
+  const float2 t = make_float2(x0.x - 0.5f * s.x, x0.y - 0.5f * s.y);
+  const float2 r = mul_i<S>(make_float2(h3 * d.x, h3 * d.y));
+  x0 = cadd(x0, s);
+  x1 = cadd(t, r);
+  x2 = csub(t, r);
+}
+
+// Radix-2 decimation in frequency onto two DFT-4s; natural-order output.
+template <int S>
+__device__ __forceinline__ void dft8(float2 (&x)[8]) {
+  constexpr float h = 0.707106781186547524f;  // cos(45 degrees)
+  float2 a[4], b[4];
 #pragma unroll
-  for (int rp = 0; rp < R; ++rp) {
-    const int k = lane + 32 * rp;
-    const int src = bitrev5(k / R), reg = k % R;
-    float2 v = make_float2(0.f, 0.f);
+  for (int p = 0; p < 4; ++p) {
+    a[p] = cadd(x[p], x[p + 4]);
+    b[p] = csub(x[p], x[p + 4]);
+  }
+  b[1] = make_float2(h * (b[1].x - S * b[1].y), h * (b[1].y + S * b[1].x));   // * e^{S i pi/4}
+  b[2] = mul_i<S>(b[2]);                                                       // * e^{S i pi/2}
+  b[3] = make_float2(h * (-b[3].x - S * b[3].y), h * (-b[3].y + S * b[3].x));  // * e^{S 3i pi/4}
+  dft4<S>(a[0], a[1], a[2], a[3]);
+  dft4<S>(b[0], b[1], b[2], b[3]);
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const float a = __shfl_sync(0xffffffffu, x[r].x, src), b = __shfl_sync(0xffffffffu, x[r].y, src);
-      if (reg == r) v = make_float2(a, b);
-    }
-    y[rp] = v;
+  for (int k = 0; k < 4; ++k) {
+    x[2 * k] = a[k];
+    x[2 * k + 1] = b[k];
   }
 }
 
-// Work items are (plane, chunk of `rows` latitudes) pairs, walked by
-// persistent blocks: while a block transforms one item, cp.async brings the
-// next item's input into the other half of its staging memory.
-//
-// Inverse staging: the chunk's coefficients [ntp1][rows + 2] (a pitch that
-// keeps every 16-byte copy aligned). Forward staging: the chunk's grid rows
-// [rows][N] (one contiguous run of the plane), plus one output buffer
-// [ntp1][rows + 1] for the m-major write.
-
-__host__ __device__ inline int coef_pitch(int rows) { return rows + 2; }
-
-inline size_t inverse_chunk_smem(int nlon, int rows, int ntp1) {
-  return ((size_t)nlon + 2 * (size_t)ntp1 * coef_pitch(rows)) * sizeof(float2);
+// 12 = 3 x 4 by the same four-step factorisation (n = 4 p + q, k = k1 + 3 k2).
+template <int S>
+__device__ __forceinline__ void dft12(float2 (&x)[12]) {
+  float2 a[4][3];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    a[q][0] = x[q];
+    a[q][1] = x[4 + q];
+    a[q][2] = x[8 + q];
+    dft3<S>(a[q][0], a[q][1], a[q][2]);
+  }
+  a[1][1] = rot12<S, 1>(a[1][1]);
+  a[1][2] = rot12<S, 2>(a[1][2]);
+  a[2][1] = rot12<S, 2>(a[2][1]);
+  a[2][2] = rot12<S, 4>(a[2][2]);
+  a[3][1] = rot12<S, 3>(a[3][1]);
+  a[3][2] = rot12<S, 6>(a[3][2]);
+#pragma unroll
+  for (int k1 = 0; k1 < 3; ++k1) {
+    dft4<S>(a[0][k1], a[1][k1], a[2][k1], a[3][k1]);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) x[k1 + 3 * k2] = a[k2][k1];
+  }
 }
 
-inline size_t forward_chunk_smem(int nlon, int rows, int ntp1) {
-  return ((size_t)nlon + (size_t)ntp1 * (rows + 1)) * sizeof(float2);
+template <int Q, int S>
+__device__ __forceinline__ void dft_q(float2 (&x)[Q]) {
+  if constexpr (Q == 4)
+    dft4<S>(x[0], x[1], x[2], x[3]);
+  else if constexpr (Q == 8)
+    dft8<S>(x);
+  else
+    dft12<S>(x);
 }
 
-// gp2fc for one plane per block: rows of N grid values -> m-major
-// coefficients. A warp transforms kRowsPerWarp rows together.
-template <int R>
-__global__ void __launch_bounds__(kWarps * 32) k_fft_forward(const float* __restrict__ g, float* __restrict__ c,
+// Shared-memory position of Z[k] (k = k1 + 8 k2) and of B[q][k1]: 9 per 8.
+__device__ __forceinline__ int zpos(int k) { return k + (k >> 3); }
+
+// Pitch of the [m][pitch] coefficient stage: pitch = 16 / T (mod 16), so
+// that a half-warp's 64-bit accesses fc[(t + T i) * pitch + r] fall on
+// distinct banks.
+__host__ __device__ inline int fc_pitch(int rows, int T) {
+  return rows + (((16 / T - rows) % 16) + 16) % 16;
+}
+
+template <int Q>
+struct Shape {
+  static constexpr int M = 8 * Q, N = 2 * M;
+  static constexpr int T = Q == 8 ? 8 : 4;  // threads per row
+  static constexpr int QT = Q / T, KT = 8 / T;
+  static constexpr int XP = 9 * Q;  // exchange floats2 per row
+};
+
+inline size_t chunk_smem(int Q, int T, int rows, int ntp1) {
+  return ((size_t)2 * 8 * Q + 9 * Q + (size_t)rows * 9 * Q + (size_t)ntp1 * fc_pitch(rows, T)) * sizeof(float2);
+}
+
+// Twiddle tables into shared memory: tw[j] = e^{2 pi i j / N};
+// twq[9 q + k1] = w_M^{q k1}.
+template <int Q>
+__device__ __forceinline__ void load_twiddles(const float2* __restrict__ twg, float2* tw, float2* twq) {
+  using Sh = Shape<Q>;
+  for (int i = threadIdx.x; i < Sh::N; i += blockDim.x) tw[i] = twg[i];
+  for (int i = threadIdx.x; i < 9 * Q; i += blockDim.x) {
+    const int q = i / 9, k1 = i - 9 * q;
+    twq[i] = k1 < 8 ? twg[(2 * q * k1) % Sh::N] : make_float2(0.f, 0.f);
+  }
+}
+
+// Steps two and three of the four-step FFT for one row: a[i] holds the
+// DFT-8 input of q = t + T i; on return b[j][k2] = Z[t + T j + 8 k2].
+template <int Q, int S>
+__device__ __forceinline__ void four_step(float2 (&a)[Shape<Q>::QT][8], float2 (&b)[Shape<Q>::KT][Q],
+                                          const float2* twq, float2* xr, int t) {
+  using Sh = Shape<Q>;
+#pragma unroll
+  for (int i = 0; i < Sh::QT; ++i) {
+    const int q = t + Sh::T * i;
+    dft8<S>(a[i]);
+#pragma unroll
+    for (int k1 = 1; k1 < 8; ++k1) {
+      const float2 w = twq[9 * q + k1];
+      a[i][k1] = S > 0 ? cmul(a[i][k1], w) : cmulc(a[i][k1], w);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 8; ++k1) xr[9 * q + k1] = a[i][k1];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < Sh::KT; ++j) {
+    const int k1 = t + Sh::T * j;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) b[j][q] = xr[9 * q + k1];
+    dft_q<Q, S>(b[j]);
+  }
+}
+
+// gp2fc: rows of N grid values -> m-major coefficients.
+template <int Q>
+__global__ void __launch_bounds__(kMaxThreads) k_fft_forward(const float* __restrict__ g, float* __restrict__ c,
                                                              const float2* __restrict__ twg, int nlat, int ntp1,
                                                              int rows) {
-  constexpr int M = 32 * R, N = 2 * M, B = kRowsPerWarp;
+  using Sh = Shape<Q>;
+  constexpr int T = Sh::T, M = Sh::M, N = Sh::N;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* fc = tw + N;  // [ntp1][rows + 1]
-  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const float inv_n = 1.f / (float)N;
+  float2* twq = tw + N;
+  float2* xb = twq + 9 * Q;
+  float2* fc = xb + rows * Sh::XP;
+  const int pitch = fc_pitch(rows, T);
   const int chunks = nlat / rows;
   const size_t plane = blockIdx.x / chunks;
   const int lat0 = (blockIdx.x % chunks) * rows;
-  for (int row0 = warp * B; row0 < rows; row0 += kWarps * B) {
-    float2 x[B][R];
+  const int r = threadIdx.x / T, t = threadIdx.x % T;
+  // z_n = g_2n + i g_2n+1 for n = Q p + q
+  const float2* in = reinterpret_cast<const float2*>(g + (plane * nlat + lat0 + r) * N);
+  float2 a[Sh::QT][8];
 #pragma unroll
-    for (int b = 0; b < B; ++b) {
-      const float2* in = reinterpret_cast<const float2*>(g + (plane * nlat + lat0 + row0 + b) * N);
+  for (int i = 0; i < Sh::QT; ++i)
 #pragma unroll
-      for (int r = 0; r < R; ++r) x[b][r] = in[lane + 32 * r];
-    }
-    warp_fft<B, R, -1>(x, tw, N, lane);
+    for (int p = 0; p < 8; ++p) a[i][p] = in[Q * p + t + T * i];
+  load_twiddles<Q>(twg, tw, twq);
+  __syncthreads();
+  float2* xr = xb + r * Sh::XP;
+  float2 b[Sh::KT][Q];
+  four_step<Q, -1>(a, b, twq, xr, t);
+  __syncwarp();
 #pragma unroll
-    for (int b = 0; b < B; ++b) {
-      float2 y[R];
-      natural_order<R>(x[b], y, lane);
+  for (int j = 0; j < Sh::KT; ++j)
 #pragma unroll
-      for (int rp = 0; rp < R; ++rp) {
-        // Z[m] and Z[(M - m) % M] for m = lane + 32 rp: the second sits in
-        // lane 32 - lane, register R - 1 - rp (lane 0: lane 0, register
-        // (R - rp) % R).
-        const float2 zm = y[rp];
-        const float ax = __shfl_sync(0xffffffffu, y[R - 1 - rp].x, (32 - lane) & 31);
-        const float ay = __shfl_sync(0xffffffffu, y[R - 1 - rp].y, (32 - lane) & 31);
-        const float bx = __shfl_sync(0xffffffffu, y[(R - rp) % R].x, 0);
-        const float by = __shfl_sync(0xffffffffu, y[(R - rp) % R].y, 0);
-        const float2 zc = lane == 0 ? make_float2(bx, -by) : make_float2(ax, -ay);
-        const int m = lane + 32 * rp;
-        if (m < ntp1) {
-          const float2 even = make_float2(0.5f * (zm.x + zc.x), 0.5f * (zm.y + zc.y));
-          // (zm - zc) / 2i = ((zm - zc).y, -(zm - zc).x) / 2
-          const float2 odd = make_float2(0.5f * (zm.y - zc.y), -0.5f * (zm.x - zc.x));
-          const float2 gm = cadd(even, cmul(twiddle<-1>(tw, m, N), odd));
-          fc[m * (rows + 1) + row0 + b] = make_float2(gm.x * inv_n, m == 0 ? 0.f : gm.y * inv_n);
-        }
-      }
-    }
+    for (int k2 = 0; k2 < Q; ++k2) xr[zpos(t + T * j + 8 * k2)] = b[j][k2];
+  __syncwarp();
+  const float inv_n = 1.f / (float)N;
+  for (int m = t; m < ntp1; m += T) {
+    const float2 zm = xr[zpos(m)];
+    const float2 zc = conj2(xr[zpos((M - m) % M)]);
+    const float2 even = make_float2(0.5f * (zm.x + zc.x), 0.5f * (zm.y + zc.y));
+    // (zm - zc) / 2i = ((zm - zc).y, -(zm - zc).x) / 2
+    const float2 odd = make_float2(0.5f * (zm.y - zc.y), -0.5f * (zm.x - zc.x));
+    const float2 gm = cadd(even, cmulc(odd, tw[m]));
+    fc[m * pitch + r] = make_float2(gm.x * inv_n, m == 0 ? 0.f : gm.y * inv_n);
   }
   __syncthreads();
   float2* out = reinterpret_cast<float2*>(c) + plane * nlat * ntp1 + lat0;
   for (int i = threadIdx.x; i < ntp1 * rows; i += blockDim.x) {
     const int m = i / rows, lat = i - m * rows;
-    out[(size_t)m * nlat + lat] = fc[m * (rows + 1) + lat];
+    out[(size_t)m * nlat + lat] = fc[m * pitch + lat];
   }
 }
 
-// fc2gp: m-major coefficients -> rows of N grid values, kRowsPerWarp rows
-// per warp at once.
-template <int R>
-__global__ void __launch_bounds__(kWarps * 32) k_fft_inverse(const float* __restrict__ c, float* __restrict__ g,
+// fc2gp: m-major coefficients -> rows of N grid values.
+template <int Q>
+__global__ void __launch_bounds__(kMaxThreads) k_fft_inverse(const float* __restrict__ c, float* __restrict__ g,
                                                              const float2* __restrict__ twg, int nlat, int ntp1,
-                                                             int rows, int items) {
-  constexpr int M = 32 * R, N = 2 * M, B = kRowsPerWarp;
-  extern __shared__ float4 sm4[];
-  float2* tw = reinterpret_cast<float2*>(sm4);
-  float2* fcb = tw + N;  // [2][ntp1][pitch]
-  const int pitch = coef_pitch(rows);
-  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
+                                                             int rows) {
+  using Sh = Shape<Q>;
+  constexpr int T = Sh::T, M = Sh::M, N = Sh::N;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* twq = tw + N;
+  float2* xb = twq + 9 * Q;
+  float2* fc = xb + rows * Sh::XP;
+  const int pitch = fc_pitch(rows, T);
   const int chunks = nlat / rows;
-  auto stage = [&](int item, float2* buf) {
-    const float2* src =
-        reinterpret_cast<const float2*>(c) + (size_t)(item / chunks) * nlat * ntp1 + (item % chunks) * rows;
-    const int pieces = rows / 2;
-    for (int i = threadIdx.x; i < ntp1 * pieces; i += blockDim.x) {
-      const int m = i / pieces, q = i - m * pieces;
-      cp_async16(buf + m * pitch + 2 * q, src + (size_t)m * nlat + 2 * q);
-    }
-  };
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int item = blockIdx.x;
-  if (item < items) stage(item, fcb);
-  cp_async_commit();
-  for (int it = 0; item < items; ++it) {
-    const float2* fc = fcb + (size_t)(it & 1) * ntp1 * pitch;
-    const int next = item + gridDim.x;
-    if (next < items) stage(next, fcb + (size_t)((it + 1) & 1) * ntp1 * pitch);
-    cp_async_commit();
-    cp_async_wait_one();
-    __syncthreads();
-    const size_t plane = item / chunks;
-    const int lat0 = (item % chunks) * rows;
-    for (int row0 = warp * B; row0 < rows; row0 += kWarps * B) {
-      float2 x[B][R];
-#pragma unroll
-      for (int b = 0; b < B; ++b) {
-        const int row = row0 + b;
-        auto coef = [&](int k) {
-          float2 v = k < ntp1 ? fc[k * pitch + row] : make_float2(0.f, 0.f);
-          if (k == 0) v.y = 0.f;  // Im c_0 is ignored
-          return v;
-        };
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int k = lane + 32 * r;
-          const float2 gk = coef(k);
-          const float2 gmk = conj2(coef(M - k));
-          const float2 e = cadd(gk, gmk);
-          const float2 o = cmul(csub(gk, gmk), twiddle<1>(tw, k, N));
-          x[b][r] = make_float2(e.x - o.y, e.y + o.x);  // e + i o
-        }
-      }
-      warp_fft<B, R, 1>(x, tw, N, lane);
-#pragma unroll
-      for (int b = 0; b < B; ++b) {
-        float2 y[R];
-        natural_order<R>(x[b], y, lane);
-        float2* out = reinterpret_cast<float2*>(g + (plane * nlat + lat0 + row0 + b) * N);
-#pragma unroll
-        for (int r = 0; r < R; ++r) out[lane + 32 * r] = y[r];
-      }
-    }
-    __syncthreads();  // this staging buffer is reused two items on
-    item = next;
+  const size_t plane = blockIdx.x / chunks;
+  const int lat0 = (blockIdx.x % chunks) * rows;
+  const float2* src = reinterpret_cast<const float2*>(c) + plane * nlat * ntp1 + lat0;
+  for (int i = threadIdx.x; i < ntp1 * rows; i += blockDim.x) {
+    const int m = i / rows, lat = i - m * rows;
+    fc[m * pitch + lat] = src[(size_t)m * nlat + lat];
   }
-  cp_async_wait_all();
+  load_twiddles<Q>(twg, tw, twq);
+  __syncthreads();
+  const int r = threadIdx.x / T, t = threadIdx.x % T;
+  auto coef = [&](int k) {
+    float2 v = k < ntp1 ? fc[k * pitch + r] : make_float2(0.f, 0.f);
+    if (k == 0) v.y = 0.f;  // Im c_0 is ignored
+    return v;
+  };
+  float2 a[Sh::QT][8];
+#pragma unroll
+  for (int i = 0; i < Sh::QT; ++i)
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+      const int k = Q * p + t + T * i;
+      const float2 gk = coef(k);
+      const float2 gmk = conj2(coef(M - k));
+      const float2 e = cadd(gk, gmk);
+      const float2 o = cmul(csub(gk, gmk), tw[k]);
+      a[i][p] = make_float2(e.x - o.y, e.y + o.x);  // e + i o
+    }
+  float2* xr = xb + r * Sh::XP;
+  float2 b[Sh::KT][Q];
+  four_step<Q, 1>(a, b, twq, xr, t);
+  float2* out = reinterpret_cast<float2*>(g + (plane * nlat + lat0 + r) * N);
+#pragma unroll
+  for (int j = 0; j < Sh::KT; ++j)
+#pragma unroll
+    for (int k2 = 0; k2 < Q; ++k2) out[t + T * j + 8 * k2] = b[j][k2];
 }
 
 template <typename K>
@@ -270,51 +317,52 @@ void allow_plane_smem(K kernel) {
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLegSmemLimit);
 }
 
+int q_of(const Dims& d) { return d.NLON / 16; }
+int t_of(const Dims& d) { return q_of(d) == 8 ? 8 : 4; }
+
 }  // namespace
 
 void fft_init() {
-  allow_plane_smem(k_fft_forward<1>);
-  allow_plane_smem(k_fft_forward<2>);
-  allow_plane_smem(k_fft_forward<3>);
-  allow_plane_smem(k_fft_inverse<1>);
-  allow_plane_smem(k_fft_inverse<2>);
-  allow_plane_smem(k_fft_inverse<3>);
+  allow_plane_smem(k_fft_forward<4>);
+  allow_plane_smem(k_fft_forward<8>);
+  allow_plane_smem(k_fft_forward<12>);
+  allow_plane_smem(k_fft_inverse<4>);
+  allow_plane_smem(k_fft_inverse<8>);
+  allow_plane_smem(k_fft_inverse<12>);
 }
 
-size_t fft_chunk_smem(const Dims& d, int rows) {
-  return std::max(inverse_chunk_smem(d.NLON, rows, d.NTP1), forward_chunk_smem(d.NLON, rows, d.NTP1));
-}
+size_t fft_chunk_smem(const Dims& d, int rows) { return chunk_smem(q_of(d), t_of(d), rows, d.NTP1); }
 
-// A chunk is `rows` latitudes (m.tune.fft_rows, a multiple of
-// kWarps * kRowsPerWarp = 8 that divides NLAT = 32, 64 or 96).
-template <typename K>
-void launch_chunks(K kernel, const void* entry, size_t smem, int items, const float* a, float* b, const Model& m,
-                   cudaStream_t st) {
-  const int grid = std::min(items, persistent_grid(entry, kWarps * 32, smem));
-  kernel<<<grid, kWarps * 32, smem, st>>>(a, b, reinterpret_cast<const float2*>(m.sh.tw), m.d.NLAT, m.d.NTP1,
-                                          m.tune.fft_rows, items);
+// A chunk is `rows` latitudes (m.tune.fft_rows, a multiple of 8 dividing
+// NLAT = 32, 64 or 96), one block of rows * T threads.
+bool fft_rows_supported(const Dims& d, int rows) {
+  return rows % 8 == 0 && rows <= d.NLAT && d.NLAT % rows == 0 && rows * t_of(d) <= kMaxThreads &&
+         fft_chunk_smem(d, rows) <= kLegSmemLimit;
 }
 
 void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st) {
   const float2* tw = reinterpret_cast<const float2*>(m.sh.tw);
   const int rows = m.tune.fft_rows;
-  const size_t smem = forward_chunk_smem(m.d.NLON, rows, m.d.NTP1);
+  const size_t smem = fft_chunk_smem(m.d, rows);
   const unsigned blocks = planes * (m.d.NLAT / rows);
-  switch (m.d.NLON) {
-    case 64: k_fft_forward<1><<<blocks, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
-    case 128: k_fft_forward<2><<<blocks, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
-    default: k_fft_forward<3><<<blocks, kWarps * 32, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
+  const int threads = rows * t_of(m.d);
+  switch (q_of(m.d)) {
+    case 4: k_fft_forward<4><<<blocks, threads, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
+    case 8: k_fft_forward<8><<<blocks, threads, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
+    default: k_fft_forward<12><<<blocks, threads, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
   }
 }
 
 void fft_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st) {
+  const float2* tw = reinterpret_cast<const float2*>(m.sh.tw);
   const int rows = m.tune.fft_rows;
-  const size_t smem = inverse_chunk_smem(m.d.NLON, rows, m.d.NTP1);
-  const int items = planes * (m.d.NLAT / rows);
-  switch (m.d.NLON) {
-    case 64: launch_chunks(k_fft_inverse<1>, (const void*)k_fft_inverse<1>, smem, items, c, g, m, st); break;
-    case 128: launch_chunks(k_fft_inverse<2>, (const void*)k_fft_inverse<2>, smem, items, c, g, m, st); break;
-    default: launch_chunks(k_fft_inverse<3>, (const void*)k_fft_inverse<3>, smem, items, c, g, m, st); break;
+  const size_t smem = fft_chunk_smem(m.d, rows);
+  const unsigned blocks = planes * (m.d.NLAT / rows);
+  const int threads = rows * t_of(m.d);
+  switch (q_of(m.d)) {
+    case 4: k_fft_inverse<4><<<blocks, threads, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1, rows); break;
+    case 8: k_fft_inverse<8><<<blocks, threads, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1, rows); break;
+    default: k_fft_inverse<12><<<blocks, threads, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1, rows); break;
   }
 }
 

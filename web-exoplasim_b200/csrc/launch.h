@@ -48,6 +48,7 @@ void tc_inverse(const Model& m, const float* s, float* f, int planes, bool deriv
 // fft.cu (optimized path; Fourier planes m-major)
 void fft_init();
 size_t fft_chunk_smem(const Dims& d, int rows);
+bool fft_rows_supported(const Dims& d, int rows);
 void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st);
 void fft_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st);
 
