@@ -159,13 +159,17 @@ __host__ __device__ inline int fc_pitch(int rows, int T) {
 template <int Q>
 struct Shape {
   static constexpr int M = 8 * Q, N = 2 * M;
-  static constexpr int T = Q == 8 ? 8 : 4;  // threads per row
+  static constexpr int NTP1 = Q == 4 ? 22 : Q == 8 ? 43 : 64;  // T21, T42, T63
+  static constexpr int T = Q == 8 ? 8 : 4;                      // threads per row
   static constexpr int QT = Q / T, KT = 8 / T;
-  static constexpr int XP = 9 * Q;  // exchange floats2 per row
+  static constexpr int XP = 9 * Q;  // exchange float2s per row
 };
 
-inline size_t chunk_smem(int Q, int T, int rows, int ntp1) {
-  return ((size_t)2 * 8 * Q + 9 * Q + (size_t)rows * 9 * Q + (size_t)ntp1 * fc_pitch(rows, T)) * sizeof(float2);
+// Twiddles, the exchange rows and the coefficient stage, whose M + 1 rows
+// hold zeros from NTP1 on (the inverse reads c_k and c_{M-k} for every k).
+inline size_t chunk_smem(int Q, int T, int rows) {
+  return ((size_t)2 * 8 * Q + 9 * Q + (size_t)rows * 9 * Q + (size_t)(8 * Q + 1) * fc_pitch(rows, T)) *
+         sizeof(float2);
 }
 
 // Twiddle tables into shared memory: tw[j] = e^{2 pi i j / N};
@@ -211,10 +215,9 @@ __device__ __forceinline__ void four_step(float2 (&a)[Shape<Q>::QT][8], float2 (
 // gp2fc: rows of N grid values -> m-major coefficients.
 template <int Q>
 __global__ void __launch_bounds__(kMaxThreads) k_fft_forward(const float* __restrict__ g, float* __restrict__ c,
-                                                             const float2* __restrict__ twg, int nlat, int ntp1,
-                                                             int rows) {
+                                                             const float2* __restrict__ twg, int nlat, int rows) {
   using Sh = Shape<Q>;
-  constexpr int T = Sh::T, M = Sh::M, N = Sh::N;
+  constexpr int T = Sh::T, M = Sh::M, N = Sh::N, NTP1 = Sh::NTP1;
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* twq = tw + N;
@@ -244,30 +247,33 @@ __global__ void __launch_bounds__(kMaxThreads) k_fft_forward(const float* __rest
     for (int k2 = 0; k2 < Q; ++k2) xr[zpos(t + T * j + 8 * k2)] = b[j][k2];
   __syncwarp();
   const float inv_n = 1.f / (float)N;
-  for (int m = t; m < ntp1; m += T) {
-    const float2 zm = xr[zpos(m)];
-    const float2 zc = conj2(xr[zpos((M - m) % M)]);
-    const float2 even = make_float2(0.5f * (zm.x + zc.x), 0.5f * (zm.y + zc.y));
-    // (zm - zc) / 2i = ((zm - zc).y, -(zm - zc).x) / 2
-    const float2 odd = make_float2(0.5f * (zm.y - zc.y), -0.5f * (zm.x - zc.x));
-    const float2 gm = cadd(even, cmulc(odd, tw[m]));
-    fc[m * pitch + r] = make_float2(gm.x * inv_n, m == 0 ? 0.f : gm.y * inv_n);
+#pragma unroll
+  for (int i = 0; i < (NTP1 + T - 1) / T; ++i) {
+    const int m = t + T * i;
+    if (m < NTP1) {
+      const float2 zm = xr[zpos(m)];
+      const float2 zc = conj2(xr[zpos(m == 0 ? 0 : M - m)]);
+      const float2 even = make_float2(0.5f * (zm.x + zc.x), 0.5f * (zm.y + zc.y));
+      // (zm - zc) / 2i = ((zm - zc).y, -(zm - zc).x) / 2
+      const float2 odd = make_float2(0.5f * (zm.y - zc.y), -0.5f * (zm.x - zc.x));
+      const float2 gm = cadd(even, cmulc(odd, tw[m]));
+      fc[m * pitch + r] = make_float2(gm.x * inv_n, m == 0 ? 0.f : gm.y * inv_n);
+    }
   }
   __syncthreads();
-  float2* out = reinterpret_cast<float2*>(c) + plane * nlat * ntp1 + lat0;
-  for (int i = threadIdx.x; i < ntp1 * rows; i += blockDim.x) {
-    const int m = i / rows, lat = i - m * rows;
-    out[(size_t)m * nlat + lat] = fc[m * pitch + lat];
-  }
+  // rows * T threads: thread (m0, lat) writes m = m0, m0 + T, ...
+  const int lat = threadIdx.x % rows, m0 = threadIdx.x / rows;
+  float2* out = reinterpret_cast<float2*>(c) + plane * nlat * NTP1 + lat0 + lat;
+#pragma unroll 4
+  for (int m = m0; m < NTP1; m += T) out[(size_t)m * nlat] = fc[m * pitch + lat];
 }
 
 // fc2gp: m-major coefficients -> rows of N grid values.
 template <int Q>
 __global__ void __launch_bounds__(kMaxThreads) k_fft_inverse(const float* __restrict__ c, float* __restrict__ g,
-                                                             const float2* __restrict__ twg, int nlat, int ntp1,
-                                                             int rows) {
+                                                             const float2* __restrict__ twg, int nlat, int rows) {
   using Sh = Shape<Q>;
-  constexpr int T = Sh::T, M = Sh::M, N = Sh::N;
+  constexpr int T = Sh::T, M = Sh::M, N = Sh::N, NTP1 = Sh::NTP1;
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* twq = tw + N;
@@ -277,27 +283,29 @@ __global__ void __launch_bounds__(kMaxThreads) k_fft_inverse(const float* __rest
   const int chunks = nlat / rows;
   const size_t plane = blockIdx.x / chunks;
   const int lat0 = (blockIdx.x % chunks) * rows;
-  const float2* src = reinterpret_cast<const float2*>(c) + plane * nlat * ntp1 + lat0;
-  for (int i = threadIdx.x; i < ntp1 * rows; i += blockDim.x) {
-    const int m = i / rows, lat = i - m * rows;
-    fc[m * pitch + lat] = src[(size_t)m * nlat + lat];
+  {
+    // rows * T threads: thread (m0, lat) stages m = m0, m0 + T, ... <= M,
+    // zeros from NTP1 on; Im c_0 is ignored.
+    const int lat = threadIdx.x % rows, m0 = threadIdx.x / rows;
+    const float2* src = reinterpret_cast<const float2*>(c) + plane * nlat * NTP1 + lat0 + lat;
+#pragma unroll 4
+    for (int m = m0; m <= M; m += T) {
+      float2 v = m < NTP1 ? src[(size_t)m * nlat] : make_float2(0.f, 0.f);
+      if (m == 0) v.y = 0.f;
+      fc[m * pitch + lat] = v;
+    }
   }
   load_twiddles<Q>(twg, tw, twq);
   __syncthreads();
   const int r = threadIdx.x / T, t = threadIdx.x % T;
-  auto coef = [&](int k) {
-    float2 v = k < ntp1 ? fc[k * pitch + r] : make_float2(0.f, 0.f);
-    if (k == 0) v.y = 0.f;  // Im c_0 is ignored
-    return v;
-  };
   float2 a[Sh::QT][8];
 #pragma unroll
   for (int i = 0; i < Sh::QT; ++i)
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
       const int k = Q * p + t + T * i;
-      const float2 gk = coef(k);
-      const float2 gmk = conj2(coef(M - k));
+      const float2 gk = fc[k * pitch + r];
+      const float2 gmk = conj2(fc[(M - k) * pitch + r]);
       const float2 e = cadd(gk, gmk);
       const float2 o = cmul(csub(gk, gmk), tw[k]);
       a[i][p] = make_float2(e.x - o.y, e.y + o.x);  // e + i o
@@ -331,7 +339,7 @@ void fft_init() {
   allow_plane_smem(k_fft_inverse<12>);
 }
 
-size_t fft_chunk_smem(const Dims& d, int rows) { return chunk_smem(q_of(d), t_of(d), rows, d.NTP1); }
+size_t fft_chunk_smem(const Dims& d, int rows) { return chunk_smem(q_of(d), t_of(d), rows); }
 
 // A chunk is `rows` latitudes (m.tune.fft_rows, a multiple of 8 dividing
 // NLAT = 32, 64 or 96), one block of rows * T threads.
@@ -347,9 +355,9 @@ void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStrea
   const unsigned blocks = planes * (m.d.NLAT / rows);
   const int threads = rows * t_of(m.d);
   switch (q_of(m.d)) {
-    case 4: k_fft_forward<4><<<blocks, threads, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
-    case 8: k_fft_forward<8><<<blocks, threads, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
-    default: k_fft_forward<12><<<blocks, threads, smem, st>>>(g, c, tw, m.d.NLAT, m.d.NTP1, rows); break;
+    case 4: k_fft_forward<4><<<blocks, threads, smem, st>>>(g, c, tw, m.d.NLAT, rows); break;
+    case 8: k_fft_forward<8><<<blocks, threads, smem, st>>>(g, c, tw, m.d.NLAT, rows); break;
+    default: k_fft_forward<12><<<blocks, threads, smem, st>>>(g, c, tw, m.d.NLAT, rows); break;
   }
 }
 
@@ -360,9 +368,9 @@ void fft_inverse(const Model& m, const float* c, float* g, int planes, cudaStrea
   const unsigned blocks = planes * (m.d.NLAT / rows);
   const int threads = rows * t_of(m.d);
   switch (q_of(m.d)) {
-    case 4: k_fft_inverse<4><<<blocks, threads, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1, rows); break;
-    case 8: k_fft_inverse<8><<<blocks, threads, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1, rows); break;
-    default: k_fft_inverse<12><<<blocks, threads, smem, st>>>(c, g, tw, m.d.NLAT, m.d.NTP1, rows); break;
+    case 4: k_fft_inverse<4><<<blocks, threads, smem, st>>>(c, g, tw, m.d.NLAT, rows); break;
+    case 8: k_fft_inverse<8><<<blocks, threads, smem, st>>>(c, g, tw, m.d.NLAT, rows); break;
+    default: k_fft_inverse<12><<<blocks, threads, smem, st>>>(c, g, tw, m.d.NLAT, rows); break;
   }
 }
 
