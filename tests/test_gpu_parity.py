@@ -258,7 +258,7 @@ def test_autotuned_shapes_leave_results_unchanged():
         assert t["fft_rows"] in (8, 16, 32)
         for group, tile in (t["sp2fc"], t["dv2uv"]):
             assert group in (1, 2, 4) and tile in (8, 16, 32)
-        assert set(t["forward_groups"].values()) <= {1, 2, 4}
+        assert set(t["forward_tiles"].values()) <= {8, 16}
     print("tunings:", one.tuning(), three.tuning())
     one.step(3)
     three.step(3)

@@ -295,7 +295,7 @@ class Engine:
         v = (ctypes.c_int * 9)()
         _check(_lib.exogcm_tuning(self.h, v, 9))
         return {"fft_rows": v[0], "sp2fc": (v[1], v[2]), "dv2uv": (v[3], v[4]),
-                "forward_groups": {"fc2sp": v[5], "uv2dv": v[6], "mktend": v[7], "qtend": v[8]}}
+                "forward_tiles": {"fc2sp": v[5], "uv2dv": v[6], "mktend": v[7], "qtend": v[8]}}
 
     def graph_launches(self, steps: int) -> int:
         n = ctypes.c_size_t()

@@ -125,7 +125,7 @@ struct Tuning {
   int fft_rows;      // latitudes per FFT block (a multiple of 8 dividing NLAT)
   int inv_group[2];  // wavenumbers per inverse Legendre block: [0] sp2fc, [1] dv2uv
   int inv_tile[2];   // planes per inverse Legendre block (even)
-  int fwd_group[4];  // wavenumbers per forward Legendre block, by kind
+  int fwd_tile[4];   // planes per forward Legendre tile (8 or 16), by kind
 };
 
 // Everything a step kernel can reach.

@@ -705,10 +705,10 @@ void autotune(exogcm_engine* e) {
   }
   for (int k = 0; k < 4; ++k) {
     float best = 1e30f;
-    int pick = t.fwd_group[k];
-    for (int group : {1, 2, 4}) {
-      if (leg_forward_smem(d, k, group) > kLegSmemLimit) continue;
-      t.fwd_group[k] = group;
+    int pick = t.fwd_tile[k];
+    for (int tile : {8, 16}) {
+      if (leg_forward_smem(d, k, tile) > kLegSmemLimit) continue;
+      t.fwd_tile[k] = tile;
       const float ms = time([&](const Model& m) {
         if (k == 0)
           tr_legendre_forward(m, F.fgtdt, F.zstt1, LP, m.sh.qc, e->stream);
@@ -719,9 +719,9 @@ void autotune(exogcm_engine* e) {
         else
           tr_qtend(m, F.fgut, F.fgvt, F.fgtn, F.zstt2, LP, e->stream);
       });
-      if (ms < best) best = ms, pick = group;
+      if (ms < best) best = ms, pick = tile;
     }
-    t.fwd_group[k] = pick;
+    t.fwd_tile[k] = pick;
   }
 }
 
@@ -1203,7 +1203,7 @@ int exogcm_tuning(exogcm_engine* e, int* values, int count) {
     if (!e || !values || count < 9) throw Error(EXOGCM_EINVAL, "need room for 9 values");
     const Tuning& t = e->tune;
     const int v[9] = {t.fft_rows,     t.inv_group[0], t.inv_tile[0], t.inv_group[1], t.inv_tile[1],
-                      t.fwd_group[0], t.fwd_group[1], t.fwd_group[2], t.fwd_group[3]};
+                      t.fwd_tile[0], t.fwd_tile[1], t.fwd_tile[2], t.fwd_tile[3]};
     std::copy(v, v + 9, values);
   });
 }

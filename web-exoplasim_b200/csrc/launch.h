@@ -29,7 +29,7 @@ void leg_init();
 // Resident blocks of `kernel` per SM for a launch shape, times the SM count.
 int persistent_grid(const void* kernel, int threads, size_t smem);
 size_t leg_inverse_smem(const Dims& d, int kind, int group, int tile);
-size_t leg_forward_smem(const Dims& d, int kind, int group);
+size_t leg_forward_smem(const Dims& d, int kind, int tile);
 Tuning default_tuning(const Dims& d);
 void leg_inverse(const Model& m, const float* s, float* f, int planes, bool derivative, cudaStream_t st);
 void leg_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V, int planes, float plavor,

@@ -22,11 +22,12 @@
 // 2 * (m * NLAT + lat)), so an output wavenumber of the inverse is one
 // contiguous run of latitudes, written by the threads that own consecutive
 // latitude pairs (north run ascending, south run descending), and the
-// forward transform reads such runs. Work is tiled as one block per (group
+// forward transform reads such runs. The inverse's work items are (group
 // of consecutive wavenumbers, tile of planes): a group's coefficients are
 // contiguous in a spectral plane (modes are m-major) and a group's table
 // slice is contiguous in the transposed northern tables ([mode][pair]), so
-// both are staged in shared memory by contiguous loads.
+// both are staged in shared memory by contiguous loads. The forward's
+// blocks own wavenumber pairs (see k_sym_forward).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,7 +40,6 @@ namespace exogcm {
 
 namespace {
 
-constexpr int kForwardThreads = 256;
 constexpr size_t kSmemBudget = kLegSmemLimit;
 
 __device__ __forceinline__ int first_mode(int m, int ntp1) { return m * (2 * ntp1 - m + 1) / 2; }
@@ -221,120 +221,172 @@ struct SymIn {
 // KIND 1: uv2dv, in = {u, v}, outputs D, Z (uv2dv.wgsl without the KE term).
 // KIND 2: mktend's uv2dv, in = {u, v, ke} (uv2dv.wgsl with HAS_KINETIC).
 // KIND 3: qtend, in = {u, v, source} (qtend.wgsl).
-// Staged per (input, plane, m, pair): (north + south, north - south) of the
-// real and imaginary parts, read from the m-major planes as contiguous runs
-// of latitudes, and the group's table slices ([table][pair][term]). For mode
-// (m, n) the shader's north + s * south with s = (-1)^(m+n) is the sum for
-// even n - m and the difference for odd. A thread owns one term (mode) for
-// kFwdPlanes planes, so every table value it loads serves all of them.
-constexpr int kFwdTile = 8;    // planes per block
-constexpr int kFwdPlanes = 4;  // planes per thread
-
+//
+// A block owns the wavenumber pair (g, NTP1 - 1 - g), or the middle
+// wavenumber alone: NTP1 + 1 modes for every pair, so blocks carry equal
+// work. Its table slices ([table][pair][mode]) are staged once, and it then
+// walks a range of planes in tiles of TP. While one tile is computed, the
+// next tile's inputs are fetched into registers; they are stored as
+// (north + south, north - south) of the real and imaginary parts per
+// (input, plane, wavenumber, pair). For mode (m, n) the shaders'
+// north + s * south with s = (-1)^(m+n) is the sum for even n - m and the
+// difference for odd. A thread owns one mode for TP / 4 planes, so each
+// table value it loads serves all of them. Every mode's sum runs over the
+// pairs in the shaders' order and expression, so the results equal the
+// plain path's bit for bit, whatever the tiling.
 template <int KIND>
 struct FwdTables {
   static constexpr int N = KIND == 0 ? 1 : KIND == 3 ? 3 : KIND == 2 ? 3 : 2;
 };
 
-template <int KIND, int NIN>
-__global__ void __launch_bounds__(kForwardThreads) k_sym_forward(SymIn<NIN> in, float* __restrict__ out0,
-                                                                 float* __restrict__ out1, int planes, int group,
-                                                                 SharedTabs sh, const float* __restrict__ q, Dims d) {
+template <int JH, int TP>
+struct FwdShape {
+  static constexpr int NLAT = 2 * JH;
+  static constexpr int NTP1 = JH == 16 ? 22 : JH == 32 ? 43 : 64;  // T21, T42, T63
+  static constexpr int NT = NTP1 + 1;                               // modes of a wavenumber pair
+  static constexpr int GROUPS = (NTP1 + 1) / 2;
+  static constexpr int PP = TP / 4;                                 // planes per thread
+  static constexpr int THREADS = (4 * NT + 31) / 32 * 32;           // (mode, plane quarter) tasks
+  static constexpr int ROW = JH + 1;                                // float4s per staged row, padded
+};
+
+template <int KIND, int NIN, int JH, int TP>
+__global__ void __launch_bounds__(FwdShape<JH, TP>::THREADS)
+    k_sym_forward(SymIn<NIN> in, float* __restrict__ out0, float* __restrict__ out1, int planes, int per_block,
+                  SharedTabs sh, const float* __restrict__ q, int ncsp) {
+  using S = FwdShape<JH, TP>;
   constexpr int NTAB = FwdTables<KIND>::N;
-  extern __shared__ float4 pm[];  // [NIN][kFwdTile][group][JH], then the tables
-  const int JH = d.NLAT / 2;
-  const int m0 = blockIdx.x * group;
-  const int m1 = min(m0 + group, d.NTP1);
-  const int gm = m1 - m0;
-  const int w0 = first_mode(m0, d.NTP1);
-  const int nt = first_mode(m1, d.NTP1) - w0;
-  const int p0 = blockIdx.y * kFwdTile;
-  const int np = min(kFwdTile, planes - p0);
-  const size_t plane_floats = (size_t)d.NLAT * d.NFC;
-  float* tab = reinterpret_cast<float*>(pm + (size_t)NIN * kFwdTile * group * JH);  // [NTAB][JH][nt]
-  // Tables in KIND order: 0: q; 1: qe, qm; 2: qe, qm, qq; 3: qe, qc, qm.
-  const float* tsrc[3] = {KIND == 0 ? q : sh.qe, KIND == 3 ? sh.qc : sh.qm, KIND == 2 ? sh.qq : sh.qm};
+  constexpr int NLAT = S::NLAT, NTP1 = S::NTP1, NT = S::NT, PP = S::PP, ROW = S::ROW;
+  constexpr size_t PLANE = (size_t)NLAT * 2 * NTP1;  // floats of a Fourier plane
+  constexpr int CONV = NIN * TP * 2 * ROW;            // float4s of one staged tile
+  extern __shared__ float4 fsm[];
+  float* tab = reinterpret_cast<float*>(fsm);           // [NTAB][JH][NT]
+  float4* conv = fsm + (NTAB * JH * NT + 3) / 4;        // [2][NIN][TP][2][ROW]
+  const int g = blockIdx.x % S::GROUPS;
+  const int pbeg = (blockIdx.x / S::GROUPS) * per_block;
+  const int pend = min(planes, pbeg + per_block);
+  const int ma = g, mb = NTP1 - 1 - g;
+  const bool pair = mb != ma;
+  const int Ka = NTP1 - ma;
+  const int nt = pair ? NT : Ka;
+  const int wa = first_mode(ma, NTP1), wb = first_mode(mb, NTP1);
+
+  // Fetch: element e = ((k * TP + p) * 2 + mi) * JH + l of a tile, the
+  // north and south values of pair l.
+  constexpr int E = NIN * TP * 2 * JH;
+  constexpr int R = (E + S::THREADS - 1) / S::THREADS;
+  float2 rn[R], rs[R];
+  auto fetch = [&](int tile) {
 #pragma unroll
-  for (int k = 0; k < NTAB; ++k)
-    for (int i = threadIdx.x; i < JH * nt; i += blockDim.x) {
-      const int l = i / nt, t = i - l * nt;
-      tab[(k * JH + l) * nt + t] = __ldg(tsrc[k] + (size_t)l * d.NCSP + w0 + t);
-    }
-  for (int k = 0; k < NIN; ++k) {
-    for (int i = threadIdx.x; i < kFwdTile * gm * JH; i += blockDim.x) {
-      const int j = i % JH;
-      const int mi = (i / JH) % gm;
-      const int p = i / (JH * gm);
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (p < np) {
-        const float2* row = reinterpret_cast<const float2*>(in.p[k] + (size_t)(p0 + p) * plane_floats) +
-                            (size_t)(m0 + mi) * d.NLAT;
-        const float2 n = row[j], s = row[d.NLAT - 1 - j];
-        v = make_float4(n.x + s.x, n.y + s.y, n.x - s.x, n.y - s.y);
+    for (int i = 0; i < R; ++i) {
+      const int e = threadIdx.x + i * S::THREADS;
+      const int l = e % JH, mi = (e / JH) % 2, p = (e / (2 * JH)) % TP, k = e / (2 * JH * TP);
+      const int plane = tile + p;
+      float2 a = make_float2(0.f, 0.f), b = a;
+      if (e < E && plane < pend && (mi == 0 || pair)) {
+        const float* base = k == 0 ? in.p[0] : k == 1 ? in.p[NIN > 1 ? 1 : 0] : in.p[NIN > 2 ? 2 : 0];
+        const float2* row =
+            reinterpret_cast<const float2*>(base + (size_t)plane * PLANE) + (size_t)(mi ? mb : ma) * NLAT;
+        a = row[l];
+        b = row[NLAT - 1 - l];
       }
-      pm[((k * kFwdTile + p) * group + mi) * JH + j] = v;
+      rn[i] = a;
+      rs[i] = b;
+    }
+  };
+  auto store = [&](float4* buf) {
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int e = threadIdx.x + i * S::THREADS;
+      if (e < E) {
+        const int l = e % JH, row = e / JH;
+        const float2 n = rn[i], so = rs[i];
+        buf[row * ROW + l] = make_float4(n.x + so.x, n.y + so.y, n.x - so.x, n.y - so.y);
+      }
+    }
+  };
+
+  fetch(pbeg);
+  // Tables in KIND order: 0: q; 1: qe, qm; 2: qe, qm, qq; 3: qe, qc, qm.
+#pragma unroll
+  for (int k = 0; k < NTAB; ++k) {
+    const float* src = k == 0 ? (KIND == 0 ? q : sh.qe) : k == 1 ? (KIND == 3 ? sh.qc : sh.qm)
+                                                                 : (KIND == 2 ? sh.qq : sh.qm);
+    for (int i = threadIdx.x; i < JH * NT; i += S::THREADS) {
+      const int t = i % NT, l = i / NT;
+      const int w = t < Ka ? wa + t : wb + (t - Ka);
+      tab[k * JH * NT + i] = t < nt ? __ldg(src + (size_t)l * ncsp + w) : 0.f;
     }
   }
+  store(conv);
   __syncthreads();
-  constexpr int NPG = kFwdTile / kFwdPlanes;
-  for (int o = threadIdx.x; o < nt * NPG; o += blockDim.x) {
-    const int t = o % nt;
-    const int pg = o / nt;
-    const int w = w0 + t;
-    const int m = sh.mode_m[w], n = sh.mode_n[w];
-    const int mi = m - m0;
-    const bool even = ((m + n) & 1) == 0;
-    const float* tq = tab + t;
-    // pm row of input k, plane p of this thread's group, at pair l: pin(k, pp)[l]
-    auto pin = [&](int k, int pp) { return pm + ((size_t)(k * kFwdTile + pg * kFwdPlanes + pp) * group + mi) * JH; };
-    float r0[kFwdPlanes] = {}, r1[kFwdPlanes] = {}, r2[kFwdPlanes] = {}, r3[kFwdPlanes] = {};
-    for (int l = 0; l < JH; ++l) {
-      const float qa = tq[l * nt];
-      const float qb = NTAB > 1 ? tq[(JH + l) * nt] : 0.f;
-      const float qc = NTAB > 2 ? tq[(2 * JH + l) * nt] : 0.f;
+
+  // This thread's task: mode t of the block, planes pq * PP .. of each tile.
+  const int t = threadIdx.x % nt, pq = threadIdx.x / nt;
+  const bool active = pq < 4;
+  const int mi = t < Ka ? 0 : 1;
+  const int toff = mi ? t - Ka : t;  // n - m
+  const int w = (mi ? wb : wa) + toff;
+  const bool even = (toff & 1) == 0;
+  const float* tq = tab + t;
+  int it = 0;
+  for (int tile = pbeg; tile < pend; tile += TP, ++it) {
+    const float4* cur = conv + (it & 1) * CONV;
+    const int next = tile + TP;
+    if (next < pend) fetch(next);
+    if (active) {
+      // staged row of input k, plane pp of this thread's planes, at pair l: pin(k, pp)[l]
+      auto pin = [&](int k, int pp) { return cur + ((k * TP + pq * PP + pp) * 2 + mi) * ROW; };
+      float r0[PP] = {}, r1[PP] = {}, r2[PP] = {}, r3[PP] = {};
+#pragma unroll 4
+      for (int l = 0; l < JH; ++l) {
+        const float qa = tq[l * NT];
+        const float qb = NTAB > 1 ? tq[(JH + l) * NT] : 0.f;
+        const float qc = NTAB > 2 ? tq[(2 * JH + l) * NT] : 0.f;
 #pragma unroll
-      for (int pp = 0; pp < kFwdPlanes; ++pp) {
-        if (KIND == 0) {
-          const float4 f = pin(0, pp)[l];
-          r0[pp] = fmaf(qa, even ? f.x : f.z, r0[pp]);
-          r1[pp] = fmaf(qa, even ? f.y : f.w, r1[pp]);
-        } else if (KIND == 1 || KIND == 2) {
-          const float e = qa, mq = qb;
-          const float4 U = pin(0, pp)[l], V = pin(NIN > 1 ? 1 : 0, pp)[l];
-          // north - s * south and north + s * south of u and v
-          const float dure = even ? U.z : U.x, duim = even ? U.w : U.y;
-          const float dvre = even ? V.z : V.x, dvim = even ? V.w : V.y;
-          const float sure = even ? U.x : U.z, suim = even ? U.y : U.w;
-          const float svre = even ? V.x : V.z, svim = even ? V.y : V.w;
-          if (KIND == 2) {
-            const float q2 = qc;
-            const float4 Kf = pin(NIN > 2 ? 2 : 0, pp)[l];
-            r0[pp] = r0[pp] + q2 * (even ? Kf.x : Kf.z);
-            r1[pp] = r1[pp] + q2 * (even ? Kf.y : Kf.w);
+        for (int pp = 0; pp < PP; ++pp) {
+          if (KIND == 0) {
+            const float4 f = pin(0, pp)[l];
+            r0[pp] = fmaf(qa, even ? f.x : f.z, r0[pp]);
+            r1[pp] = fmaf(qa, even ? f.y : f.w, r1[pp]);
+          } else if (KIND == 1 || KIND == 2) {
+            const float e = qa, mq = qb;
+            const float4 U = pin(0, pp)[l], V = pin(NIN > 1 ? 1 : 0, pp)[l];
+            // north - s * south and north + s * south of u and v
+            const float dure = even ? U.z : U.x, duim = even ? U.w : U.y;
+            const float dvre = even ? V.z : V.x, dvim = even ? V.w : V.y;
+            const float sure = even ? U.x : U.z, suim = even ? U.y : U.w;
+            const float svre = even ? V.x : V.z, svim = even ? V.y : V.w;
+            if (KIND == 2) {
+              const float q2 = qc;
+              const float4 Kf = pin(NIN > 2 ? 2 : 0, pp)[l];
+              r0[pp] = r0[pp] + q2 * (even ? Kf.x : Kf.z);
+              r1[pp] = r1[pp] + q2 * (even ? Kf.y : Kf.w);
+            }
+            r0[pp] = r0[pp] - e * dvre - mq * suim;
+            r1[pp] = r1[pp] - e * dvim + mq * sure;
+            r2[pp] = r2[pp] + e * dure - mq * svim;
+            r3[pp] = r3[pp] + e * duim + mq * svre;
+          } else {
+            const float e = qa, c = qb, mq = qc;
+            const float4 U = pin(0, pp)[l], V = pin(NIN > 1 ? 1 : 0, pp)[l], X = pin(NIN > 2 ? 2 : 0, pp)[l];
+            r0[pp] = r0[pp] + e * (even ? V.z : V.x) + c * (even ? X.x : X.z) + mq * (even ? U.y : U.w);
+            r1[pp] = r1[pp] + e * (even ? V.w : V.y) + c * (even ? X.y : X.w) - mq * (even ? U.x : U.z);
           }
-          r0[pp] = r0[pp] - e * dvre - mq * suim;
-          r1[pp] = r1[pp] - e * dvim + mq * sure;
-          r2[pp] = r2[pp] + e * dure - mq * svim;
-          r3[pp] = r3[pp] + e * duim + mq * svre;
-        } else {
-          const float e = qa, c = qb, mq = qc;
-          const float4 U = pin(0, pp)[l], V = pin(NIN > 1 ? 1 : 0, pp)[l], X = pin(NIN > 2 ? 2 : 0, pp)[l];
-          r0[pp] = r0[pp] + e * (even ? V.z : V.x) + c * (even ? X.x : X.z) + mq * (even ? U.y : U.w);
-          r1[pp] = r1[pp] + e * (even ? V.w : V.y) + c * (even ? X.y : X.w) - mq * (even ? U.x : U.z);
+        }
+      }
+#pragma unroll
+      for (int pp = 0; pp < PP; ++pp) {
+        const int plane = tile + pq * PP + pp;
+        if (plane < pend) {
+          const size_t at = (size_t)plane * (2 * ncsp) + 2 * w;
+          *reinterpret_cast<float2*>(out0 + at) = make_float2(r0[pp], r1[pp]);
+          if (KIND == 1 || KIND == 2) *reinterpret_cast<float2*>(out1 + at) = make_float2(r2[pp], r3[pp]);
         }
       }
     }
-#pragma unroll
-    for (int pp = 0; pp < kFwdPlanes; ++pp) {
-      const int p = pg * kFwdPlanes + pp;
-      if (p >= np) break;
-      const size_t at = (size_t)(p0 + p) * d.NRSP + 2 * w;
-      out0[at] = r0[pp];
-      out0[at + 1] = r1[pp];
-      if (KIND == 1 || KIND == 2) {
-        out1[at] = r2[pp];
-        out1[at + 1] = r3[pp];
-      }
-    }
+    if (next < pend) store(conv + ((it + 1) & 1) * CONV);
+    __syncthreads();
   }
 }
 
@@ -350,9 +402,11 @@ size_t inverse_smem(const Dims& d, int nin, int group, int tile) {
   return 2 * inverse_buffer_floats(d, nin, group, tile) * sizeof(float);
 }
 
-// Forward: kFwdTile planes per block; the group of wavenumbers is tuned.
-size_t forward_smem(const Dims& d, int nin, int ntab, int group) {
-  return (size_t)nin * kFwdTile * group * (d.NLAT / 2) * 16 + (size_t)ntab * (d.NLAT / 2) * group_terms(d, group) * 4;
+// Forward: the table slices of a wavenumber pair and two staged tiles.
+template <int KIND, int NIN, int JH, int TP>
+size_t forward_smem() {
+  using S = FwdShape<JH, TP>;
+  return ((size_t)(FwdTables<KIND>::N * JH * S::NT + 3) / 4 + 2 * (size_t)NIN * TP * 2 * S::ROW) * sizeof(float4);
 }
 
 template <typename K>
@@ -360,14 +414,50 @@ void allow_smem(K kernel) {
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget);
 }
 
+template <int KIND, int NIN, int JH, int TP>
+void launch_forward_shape(const Model& m, SymIn<NIN> in, float* out0, float* out1, int planes, const float* q,
+                          cudaStream_t st) {
+  using S = FwdShape<JH, TP>;
+  const auto kernel = k_sym_forward<KIND, NIN, JH, TP>;
+  const size_t smem = forward_smem<KIND, NIN, JH, TP>();
+  // Blocks per wavenumber pair: enough for every SM's resident blocks, in
+  // whole tiles of planes.
+  const int tiles = (planes + TP - 1) / TP;
+  const int target = persistent_grid((const void*)kernel, S::THREADS, smem);
+  const int splits = std::max(1, std::min(tiles, (target + S::GROUPS - 1) / S::GROUPS));
+  const int per_tiles = (tiles + splits - 1) / splits;
+  const int blocks = S::GROUPS * ((tiles + per_tiles - 1) / per_tiles);
+  kernel<<<blocks, S::THREADS, smem, st>>>(in, out0, out1, planes, per_tiles * TP, m.sh, q, m.d.NCSP);
+}
+
 template <int KIND, int NIN>
 void launch_sym_forward(const Model& m, SymIn<NIN> in, float* out0, float* out1, int planes, const float* q,
                         cudaStream_t st) {
-  constexpr int NTAB = FwdTables<KIND>::N;
-  const int group = m.tune.fwd_group[KIND];
-  dim3 grid((m.d.NTP1 + group - 1) / group, (planes + kFwdTile - 1) / kFwdTile);
-  k_sym_forward<KIND, NIN><<<grid, kForwardThreads, forward_smem(m.d, NIN, NTAB, group), st>>>(
-      in, out0, out1, planes, group, m.sh, q, m.d);
+  const bool big = m.tune.fwd_tile[KIND] == 16;
+  switch (m.d.NLAT) {
+    case 32:
+      big ? launch_forward_shape<KIND, NIN, 16, 16>(m, in, out0, out1, planes, q, st)
+          : launch_forward_shape<KIND, NIN, 16, 8>(m, in, out0, out1, planes, q, st);
+      break;
+    case 64:
+      big ? launch_forward_shape<KIND, NIN, 32, 16>(m, in, out0, out1, planes, q, st)
+          : launch_forward_shape<KIND, NIN, 32, 8>(m, in, out0, out1, planes, q, st);
+      break;
+    default:
+      big ? launch_forward_shape<KIND, NIN, 48, 16>(m, in, out0, out1, planes, q, st)
+          : launch_forward_shape<KIND, NIN, 48, 8>(m, in, out0, out1, planes, q, st);
+      break;
+  }
+}
+
+template <int KIND, int NIN>
+size_t forward_smem_for(const Dims& d, int tile) {
+  const bool big = tile == 16;
+  switch (d.NLAT) {
+    case 32: return big ? forward_smem<KIND, NIN, 16, 16>() : forward_smem<KIND, NIN, 16, 8>();
+    case 64: return big ? forward_smem<KIND, NIN, 32, 16>() : forward_smem<KIND, NIN, 32, 8>();
+    default: return big ? forward_smem<KIND, NIN, 48, 16>() : forward_smem<KIND, NIN, 48, 8>();
+  }
 }
 
 }  // namespace
@@ -386,13 +476,23 @@ int persistent_grid(const void* kernel, int threads, size_t smem) {
   return sms * (per_sm > 0 ? per_sm : 1);
 }
 
+template <int KIND, int NIN>
+void allow_forward_smem() {
+  allow_smem(k_sym_forward<KIND, NIN, 16, 8>);
+  allow_smem(k_sym_forward<KIND, NIN, 16, 16>);
+  allow_smem(k_sym_forward<KIND, NIN, 32, 8>);
+  allow_smem(k_sym_forward<KIND, NIN, 32, 16>);
+  allow_smem(k_sym_forward<KIND, NIN, 48, 8>);
+  allow_smem(k_sym_forward<KIND, NIN, 48, 16>);
+}
+
 void leg_init() {
   allow_smem(k_sym_inverse<0>);
   allow_smem(k_sym_inverse<1>);
-  allow_smem(k_sym_forward<0, 1>);
-  allow_smem(k_sym_forward<1, 2>);
-  allow_smem(k_sym_forward<2, 3>);
-  allow_smem(k_sym_forward<3, 3>);
+  allow_forward_smem<0, 1>();
+  allow_forward_smem<1, 2>();
+  allow_forward_smem<2, 3>();
+  allow_forward_smem<3, 3>();
 }
 
 template <int KIND>
@@ -420,17 +520,20 @@ void leg_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* 
 }
 
 // Shared memory a tuning asks of each transform kernel, and the default
-// tuning: the largest wavenumber groups that fit about 48 KB (inverse) and
-// 60 KB (forward), 16-plane inverse tiles (32 at T21) and 16-latitude FFT
-// chunks. The autotuner times the shapes that fit kLegSmemLimit.
+// tuning: the largest inverse wavenumber groups that fit about 48 KB,
+// 16-plane inverse tiles (32 at T21), 8-plane forward tiles and 16-latitude
+// FFT chunks. The autotuner times the shapes that fit kLegSmemLimit.
 size_t leg_inverse_smem(const Dims& d, int kind, int group, int tile) {
   return inverse_smem(d, kind == 0 ? 1 : 2, group, tile);
 }
 
-size_t leg_forward_smem(const Dims& d, int kind, int group) {
-  const int nin = kind == 0 ? 1 : kind == 1 ? 2 : 3;
-  const int ntab = kind == 0 ? 1 : kind == 1 ? 2 : 3;
-  return forward_smem(d, nin, ntab, group);
+size_t leg_forward_smem(const Dims& d, int kind, int tile) {
+  switch (kind) {
+    case 0: return forward_smem_for<0, 1>(d, tile);
+    case 1: return forward_smem_for<1, 2>(d, tile);
+    case 2: return forward_smem_for<2, 3>(d, tile);
+    default: return forward_smem_for<3, 3>(d, tile);
+  }
 }
 
 Tuning default_tuning(const Dims& d) {
@@ -445,14 +548,7 @@ Tuning default_tuning(const Dims& d) {
         break;
       }
   }
-  for (int k = 0; k < 4; ++k) {
-    t.fwd_group[k] = 1;
-    for (int g = 4; g > 1; g /= 2)
-      if (leg_forward_smem(d, k, g) <= 60 * 1024) {
-        t.fwd_group[k] = g;
-        break;
-      }
-  }
+  for (int k = 0; k < 4; ++k) t.fwd_tile[k] = 8;
   return t;
 }
 
