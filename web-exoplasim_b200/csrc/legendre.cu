@@ -337,6 +337,10 @@ __global__ void __launch_bounds__(FwdShape<JH, TP>::THREADS)
     if (active) {
       // staged row of input k, plane pp of this thread's planes, at pair l: pin(k, pp)[l]
       auto pin = [&](int k, int pp) { return cur + ((k * TP + pq * PP + pp) * 2 + mi) * ROW; };
+      // the (sum) or (difference) half of a staged float4 as one float2:
+      // half(k, pp, 0)[2 l] is (re, im) of north + south, half(k, pp, 1)[2 l] of north - south
+      auto half = [&](int k, int pp, int h) { return reinterpret_cast<const float2*>(pin(k, pp)) + h; };
+      const int hs = even ? 0 : 1;  // the half the shaders' north + s * south selects
       float r0[PP] = {}, r1[PP] = {}, r2[PP] = {}, r3[PP] = {};
 #pragma unroll 4
       for (int l = 0; l < JH; ++l) {
@@ -346,32 +350,31 @@ __global__ void __launch_bounds__(FwdShape<JH, TP>::THREADS)
 #pragma unroll
         for (int pp = 0; pp < PP; ++pp) {
           if (KIND == 0) {
-            const float4 f = pin(0, pp)[l];
-            r0[pp] = fmaf(qa, even ? f.x : f.z, r0[pp]);
-            r1[pp] = fmaf(qa, even ? f.y : f.w, r1[pp]);
+            const float2 f = half(0, pp, hs)[2 * l];
+            r0[pp] = fmaf(qa, f.x, r0[pp]);
+            r1[pp] = fmaf(qa, f.y, r1[pp]);
           } else if (KIND == 1 || KIND == 2) {
             const float e = qa, mq = qb;
-            const float4 U = pin(0, pp)[l], V = pin(NIN > 1 ? 1 : 0, pp)[l];
-            // north - s * south and north + s * south of u and v
-            const float dure = even ? U.z : U.x, duim = even ? U.w : U.y;
-            const float dvre = even ? V.z : V.x, dvim = even ? V.w : V.y;
-            const float sure = even ? U.x : U.z, suim = even ? U.y : U.w;
-            const float svre = even ? V.x : V.z, svim = even ? V.y : V.w;
+            // north + s * south (Us, Vs) and north - s * south (Ud, Vd) of u and v
+            const float2 Us = half(0, pp, hs)[2 * l], Ud = half(0, pp, 1 - hs)[2 * l];
+            const float2 Vs = half(NIN > 1 ? 1 : 0, pp, hs)[2 * l], Vd = half(NIN > 1 ? 1 : 0, pp, 1 - hs)[2 * l];
             if (KIND == 2) {
               const float q2 = qc;
-              const float4 Kf = pin(NIN > 2 ? 2 : 0, pp)[l];
-              r0[pp] = r0[pp] + q2 * (even ? Kf.x : Kf.z);
-              r1[pp] = r1[pp] + q2 * (even ? Kf.y : Kf.w);
+              const float2 Ks = half(NIN > 2 ? 2 : 0, pp, hs)[2 * l];
+              r0[pp] = r0[pp] + q2 * Ks.x;
+              r1[pp] = r1[pp] + q2 * Ks.y;
             }
-            r0[pp] = r0[pp] - e * dvre - mq * suim;
-            r1[pp] = r1[pp] - e * dvim + mq * sure;
-            r2[pp] = r2[pp] + e * dure - mq * svim;
-            r3[pp] = r3[pp] + e * duim + mq * svre;
+            r0[pp] = r0[pp] - e * Vd.x - mq * Us.y;
+            r1[pp] = r1[pp] - e * Vd.y + mq * Us.x;
+            r2[pp] = r2[pp] + e * Ud.x - mq * Vs.y;
+            r3[pp] = r3[pp] + e * Ud.y + mq * Vs.x;
           } else {
             const float e = qa, c = qb, mq = qc;
-            const float4 U = pin(0, pp)[l], V = pin(NIN > 1 ? 1 : 0, pp)[l], X = pin(NIN > 2 ? 2 : 0, pp)[l];
-            r0[pp] = r0[pp] + e * (even ? V.z : V.x) + c * (even ? X.x : X.z) + mq * (even ? U.y : U.w);
-            r1[pp] = r1[pp] + e * (even ? V.w : V.y) + c * (even ? X.y : X.w) - mq * (even ? U.x : U.z);
+            // V's difference and X's and U's sums for even n - m, the other halves for odd
+            const float2 U = half(0, pp, hs)[2 * l], V = half(NIN > 1 ? 1 : 0, pp, 1 - hs)[2 * l],
+                         X = half(NIN > 2 ? 2 : 0, pp, hs)[2 * l];
+            r0[pp] = r0[pp] + e * V.x + c * X.x + mq * U.y;
+            r1[pp] = r1[pp] + e * V.y + c * X.y - mq * U.x;
           }
         }
       }
