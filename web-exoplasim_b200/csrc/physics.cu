@@ -652,7 +652,7 @@ template <int NL>
 __global__ void __launch_bounds__(kBlock) k_lwr_radstep(Model m) {
   COLUMN_PROLOGUE
   const int NP = NL + 1;
-  const float ZERO = 1.0e-6f, ZFH2O = 0.1f, ZFO3 = 100.f / 2.14f, INV_LN10 = 0.43429448190325176f;
+  const float ZERO = 1.0e-6f, ZFH2O = 0.1f, ZFO3 = 100.f / 2.14f;
   const float* sg = tb + m.to.sigma;
   const float* sh = tb + m.to.sigmah;
   const float dp = F.dp[c];
@@ -710,17 +710,26 @@ __global__ void __launch_bounds__(kBlock) k_lwr_radstep(Model m) {
   }
 #pragma unroll
   for (int l = 0; l < NP; ++l) s_dftd[l][tx] = 0.f;
-  // Clear-sky transmissivity for absorber sums (lwr.wgsl's band fits).
+  // Clear-sky transmissivity for absorber sums (lwr.wgsl's band fits). Each
+  // fit is a power law below its threshold and a logarithm above; both
+  // sides are written through one base-2 logarithm of the side's argument,
+  // x^y = 2^(y log2 x) and log10 x = log10(2) log2 x, so that the columns of
+  // a warp, whichever side they take, share one instruction stream (no
+  // divergent branches) and two special-function operations per fit. All
+  // power-law arguments are positive.
   auto clear_sky = [&](float sumwv, float sumo3, float sumco2) {
-    float ah2o = sumwv <= 0.01f ? 0.846f * fpow(sumwv + 3.59e-5f, 0.243f) - K.ZH2O0A
-                                : 0.24f * (logf(sumwv + 0.01f) * INV_LN10) + K.ZAH2OC;
+    const float LOG10_2 = 0.30102999566398120f, LN_2 = 0.69314718055994531f;
+    const bool wv1 = sumwv <= 0.01f, wv2 = sumwv <= 2.f, co2 = sumco2 <= 1.f, o3 = sumo3 <= 0.01f;
+    const float lah = log2f(sumwv + (wv1 ? 3.59e-5f : 0.01f));
+    const float lth = log2f(wv2 ? sumwv + 0.0286f : sumwv - 0.6931f);
+    const float lco = log2f(co2 ? sumco2 + 0.01022f : sumco2);
+    const float lo3 = log2f(o3 ? sumo3 + 7.0e-5f : sumo3);
+    float ah2o = wv1 ? 0.846f * exp2f(0.243f * lah) - K.ZH2O0A : 0.24f * (LOG10_2 * lah) + K.ZAH2OC;
     if (K.TH2OC > 0.f) ah2o = fminf(ah2o + (1.f - expf(-K.TH2OC * sumwv)), 1.f);
-    const float aco2 = sumco2 <= 1.f ? 0.0676f * fpow(sumco2 + 0.01022f, 0.421f) - K.ZCO20
-                                     : 0.0546f * (logf(sumco2) * INV_LN10) + K.ZACO2C;
-    const float th2o = sumwv <= 2.f ? 1.f - (0.832f * fpow(sumwv + 0.0286f, 0.26f) - K.ZH2O0)
-                                    : fmaxf(0.f, K.ZTH2OC - 0.1196f * logf(sumwv - 0.6931f));
-    const float ao3 = sumo3 <= 0.01f ? 0.209f * fpow(sumo3 + 7.0e-5f, 0.436f) - K.ZAO30
-                                     : 0.0212f * (logf(sumo3) * INV_LN10) + K.ZAO3C;
+    const float aco2 = co2 ? 0.0676f * exp2f(0.421f * lco) - K.ZCO20 : 0.0546f * (LOG10_2 * lco) + K.ZACO2C;
+    const float th2o = wv2 ? 1.f - (0.832f * exp2f(0.26f * lth) - K.ZH2O0)
+                           : fmaxf(0.f, K.ZTH2OC - 0.1196f * (LN_2 * lth));
+    const float ao3 = o3 ? 0.209f * exp2f(0.436f * lo3) - K.ZAO30 : 0.0212f * (LOG10_2 * lo3) + K.ZAO3C;
     return fminf(1.f - ZERO, fmaxf(ZERO, 1.f - ah2o - ao3 - aco2 * th2o));
   };
   float dftu[NL + 1], tausf[NL];
