@@ -36,6 +36,36 @@ constexpr int kBlock = 128;
   const FieldPtrs& F = m.f;                                          \
   (void)h; (void)K; (void)tb; (void)SN; (void)F; (void)P;
 
+// The same for a kernel that reads its planet's constants inside long
+// loops: column kernels run kBlock threads per block over S * NHOR columns,
+// and kBlock divides NHOR (2048, 8192 or 18432), so a block's columns
+// belong to one slot, whose constants are staged once in shared memory.
+#define COLUMN_PROLOGUE_STAGED                                       \
+  const Dims& d = m.d;                                               \
+  const int slot = blockIdx.x * kBlock / d.NHOR;                     \
+  const StepParams& P = m.params[slot];                              \
+  if (!P.active) return;                                             \
+  __shared__ PlanetConst s_planet;                                   \
+  stage_planet(m.pc + slot, &s_planet);                              \
+  const PlanetConst& K = s_planet;                                   \
+  const int c = blockIdx.x * kBlock + threadIdx.x;                   \
+  if (c >= d.S * d.NHOR) return;                                     \
+  const int h = c - slot * d.NHOR;                                   \
+  const float* tb = m.tabs + (size_t)slot * m.to.stride;             \
+  const size_t SN = (size_t)d.S * d.NHOR;                            \
+  const FieldPtrs& F = m.f;                                          \
+  (void)h; (void)K; (void)tb; (void)SN; (void)F; (void)P;
+
+// Copies one slot's constants into shared memory (all threads of the block
+// take part and meet at the barrier).
+__device__ __forceinline__ void stage_planet(const PlanetConst* src, PlanetConst* dst) {
+  constexpr int n = sizeof(PlanetConst) / sizeof(float);
+  const float* a = reinterpret_cast<const float*>(src);
+  float* b = reinterpret_cast<float*>(dst);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = a[i];
+  __syncthreads();
+}
+
 __device__ __forceinline__ float sat_capped(const PlanetConst& K, float t, float p) {
   return fminf(K.RDBRV * K.RA1 * expf(K.RA2 * (t - K.TMELT) / (t - K.RA4)) / p, K.RDBRV);
 }
@@ -649,8 +679,10 @@ __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
 
 // lwr (physics/radiation/wgsl/lwr.wgsl) then radstep (radstep.wgsl).
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_lwr_radstep(Model m) {
-  COLUMN_PROLOGUE
+// Six blocks per SM (85 registers, no spills): the kernel is latency-bound,
+// and residency hides the field loads at either end of the O(L^2) rows.
+__global__ void __launch_bounds__(kBlock, 6) k_lwr_radstep(Model m) {
+  COLUMN_PROLOGUE_STAGED
   const int NP = NL + 1;
   const float ZERO = 1.0e-6f, ZFH2O = 0.1f, ZFO3 = 100.f / 2.14f;
   const float* sg = tb + m.to.sigma;
