@@ -22,8 +22,10 @@ __device__ __forceinline__ const float* slot_tabs(const Model& m, int slot) {
 }
 
 // gridpointa from gp = exp(gp) to the flux products (dynamics/wgsl/calcgp.wgsl).
+// Four resident blocks per SM: a few spilled registers cost less than the
+// latency the fourth block hides.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_calcgp(Model m) {
+__global__ void __launch_bounds__(kBlock, 4) k_calcgp(Model m) {
   const Dims& d = m.d;
   // NHOR is a multiple of kBlock at every truncation, so a block lies in one
   // slot and that slot's vertical tables are staged in shared memory once.
@@ -160,8 +162,9 @@ __global__ void __launch_bounds__(kBlock) k_calcgp(Model m) {
 
 // spectrala for one real spectral coefficient (dynamics/wgsl/spectrala.wgsl):
 // the Hoskins-Simmons semi-implicit scheme with this slot's bm1 for its phase.
+// Five resident blocks per SM (latency-bound; measured faster than four).
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_spectrala(Model m) {
+__global__ void __launch_bounds__(kBlock, 5) k_spectrala(Model m) {
   const Dims& d = m.d;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.S * d.NRSP) return;

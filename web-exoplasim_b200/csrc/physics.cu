@@ -679,7 +679,7 @@ __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
 
 // lwr (physics/radiation/wgsl/lwr.wgsl) then radstep (radstep.wgsl).
 template <int NL>
-// Six blocks per SM (85 registers, no spills): the kernel is latency-bound,
+// Six blocks per SM (at most 85 registers, no spills): the kernel is latency-bound,
 // and residency hides the field loads at either end of the O(L^2) rows.
 __global__ void __launch_bounds__(kBlock, 6) k_lwr_radstep(Model m) {
   COLUMN_PROLOGUE_STAGED
@@ -894,8 +894,9 @@ __device__ __forceinline__ Parcel condense(const PlanetConst& K, float t0, float
 }
 
 // mkdqtgp scaling, kuo and mkshallow (physics/precipitation/wgsl/kuo.wgsl).
+// Six resident blocks per SM (latency-bound; measured faster than four).
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_kuo(Model m) {
+__global__ void __launch_bounds__(kBlock, 6) k_kuo(Model m) {
   COLUMN_PROLOGUE
   const int NM = NL - 1;
   const float* ds = tb + m.to.dsigma;
