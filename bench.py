@@ -139,7 +139,7 @@ def make_planets(count, seed0=1000):
 # full-level launch; the timed launches are all full-level.
 PER_STEP = {"fourier_inverse": 18.4, "fourier_forward": 16.1, "legendre_inverse": 8.3, "dv2uv": 5,
             "legendre_forward": 5.1, "uv2dv": 2, "qtend": 2, "swr": 1, "lwr_radstep": 1, "vdiff": 1, "kuo": 1,
-            "rain_column": 1, "calcgp": 1, "spectrala": 1}
+            "rain_column": 1, "calcgp": 1, "spectrala": 1, "mkdheat": 3, "physics_in": 1, "physics_out": 1}
 
 
 def roofline(engine, peaks):

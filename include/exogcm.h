@@ -180,10 +180,10 @@ int exogcm_last_step_ms(exogcm_engine* engine, float* ms);
  * on the engine's stream), with the algorithmic bytes one launch moves in
  * *bytes. Kernels: "fourier_forward", "fourier_inverse" (FFTs on the
  * optimized path, DFTs on the plain one), "legendre_forward",
- * "legendre_inverse", "dv2uv", "uv2dv", "qtend", "calcgp", "spectrala", and
- * the single column kernels "vdiff", "swr", "lwr_radstep", "kuo",
- * "rain_column". The launches change the state; use it for measurement
- * only. */
+ * "legendre_inverse", "dv2uv", "uv2dv", "qtend", "calcgp", "spectrala",
+ * "mkdheat" (its first stage), "physics_in", "physics_out", and the single
+ * column kernels "vdiff", "swr", "lwr_radstep", "kuo", "rain_column". The
+ * launches change the state; use it for measurement only. */
 int exogcm_time_kernel(exogcm_engine* engine, const char* kernel, int reps, float* ms, double* bytes);
 
 /* Launch shapes the autotuner chose for the optimized path's transforms at

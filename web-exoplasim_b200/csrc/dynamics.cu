@@ -270,65 +270,68 @@ __global__ void __launch_bounds__(kBlock, 5) k_spectrala(Model m) {
   }
 }
 
-// spectrald up to mkdheat (dynamics/wgsl/spectrald-diffusion.wgsl).
+// spectrald up to mkdheat (dynamics/wgsl/spectrald-diffusion.wgsl), one
+// thread per (level, spectral coefficient). A thread reads all its inputs
+// before its first store: the fields are distinct arrays, but the compiler
+// cannot prove it, and would otherwise order each load after the stores
+// before it.
 __global__ void __launch_bounds__(kBlock) k_spectrald_diffusion(Model m) {
   const Dims& d = m.d;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.S * d.NRSP) return;
-  const int slot = c / d.NRSP, s = c % d.NRSP;
+  const int l = blockIdx.y;
+  const int slot = c / d.NRSP, s = c - slot * d.NRSP;
   const StepParams& P = m.params[slot];
   if (!P.active) return;
-  const PlanetConst& K = m.pc[slot];
   const float* tb = slot_tabs(m, slot);
-  const size_t SR = (size_t)d.S * d.NRSP;
+  const size_t at = (size_t)l * d.S * d.NRSP + c;
   const FieldPtrs& F = m.f;
-  const float D2 = P.delt2;
-  if (s < 2) F.spp[c] = 0.f;
-  for (int l = 0; l < d.NLEV; ++l) {
-    const size_t at = l * SR + c;
-    const float szp = F.szp[at] + D2 * F.szt[at];
-    const float stp = F.stp[at] + D2 * F.stt[at];
-    const float sdp = F.sdp[at] + D2 * F.sdt[at];
-    const float sqp = F.sqp[at] + D2 * F.sqt[at];
-    const float sakpp = tb[m.to.sakpp + l * d.NRSP + s];
-    const float damp = tb[m.to.damp + l], tdisst = tb[m.to.tdisst + l], tdissq = tb[m.to.tdissq + l];
-    const float tdissd = tb[m.to.tdissd + l], tdissz = tb[m.to.tdissz + l], tfrc = tb[m.to.tfrc + l];
-    const float srp = tb[m.to.srp + l * d.NRSP + s];
-    const float stt = ((-damp - tdisst * sakpp) * stp + damp * srp) / (1.f + D2 * (damp + tdisst * sakpp));
-    const float sqt = -tdissq * sakpp * sqp / (1.f + D2 * tdissq * sakpp);
-    const float zsdt1 = -tfrc * sdp / (1.f + D2 * tfrc);
-    const float zsdt2 = -tdissd * sakpp * sdp / (1.f + D2 * tdissd * sakpp);
-    float zszt1 = -tfrc * szp / (1.f + D2 * tfrc);
-    float zszt2 = -tdissz * sakpp * szp / (1.f + D2 * tdissz * sakpp);
-    float szt = zszt1 + zszt2;
-    if (s == 2) {
-      zszt1 = zszt1 + K.PLAVOR * tfrc / (1.f + D2 * tfrc);
-      zszt2 = zszt2 + K.PLAVOR * tdissz * sakpp / (1.f + D2 * tdissz * sakpp);
-      szt = szt + K.PLAVOR * (tfrc / (1.f + D2 * tfrc) + tdissz * sakpp / (1.f + D2 * tdissz * sakpp));
-    }
-    F.szp[at] = szp;
-    F.stp[at] = stp;
-    F.sdp[at] = sdp;
-    F.sqp[at] = sqp;
-    F.stt[at] = stt;
-    F.sqt[at] = sqt;
-    F.sdt[at] = zsdt1 + zsdt2;
-    F.szt[at] = szt;
-    F.zdsdp1[at] = zsdt1 * D2;
-    F.zdszp1[at] = zszt1 * D2;
-    F.zdsdp2[at] = zsdt2 * D2;
-    F.zdszp2[at] = zszt2 * D2;
+  const float D2 = P.delt2, PLAVOR = m.pc[slot].PLAVOR;
+  const float szp0 = F.szp[at], szt0 = F.szt[at], stp0 = F.stp[at], stt0 = F.stt[at];
+  const float sdp0 = F.sdp[at], sdt0 = F.sdt[at], sqp0 = F.sqp[at], sqt0 = F.sqt[at];
+  const float sakpp = tb[m.to.sakpp + l * d.NRSP + s];
+  const float damp = tb[m.to.damp + l], tdisst = tb[m.to.tdisst + l], tdissq = tb[m.to.tdissq + l];
+  const float tdissd = tb[m.to.tdissd + l], tdissz = tb[m.to.tdissz + l], tfrc = tb[m.to.tfrc + l];
+  const float srp = tb[m.to.srp + l * d.NRSP + s];
+  const float szp = szp0 + D2 * szt0;
+  const float stp = stp0 + D2 * stt0;
+  const float sdp = sdp0 + D2 * sdt0;
+  const float sqp = sqp0 + D2 * sqt0;
+  const float stt = ((-damp - tdisst * sakpp) * stp + damp * srp) / (1.f + D2 * (damp + tdisst * sakpp));
+  const float sqt = -tdissq * sakpp * sqp / (1.f + D2 * tdissq * sakpp);
+  const float zsdt1 = -tfrc * sdp / (1.f + D2 * tfrc);
+  const float zsdt2 = -tdissd * sakpp * sdp / (1.f + D2 * tdissd * sakpp);
+  float zszt1 = -tfrc * szp / (1.f + D2 * tfrc);
+  float zszt2 = -tdissz * sakpp * szp / (1.f + D2 * tdissz * sakpp);
+  float szt = zszt1 + zszt2;
+  if (s == 2) {
+    zszt1 = zszt1 + PLAVOR * tfrc / (1.f + D2 * tfrc);
+    zszt2 = zszt2 + PLAVOR * tdissz * sakpp / (1.f + D2 * tdissz * sakpp);
+    szt = szt + PLAVOR * (tfrc / (1.f + D2 * tfrc) + tdissz * sakpp / (1.f + D2 * tdissz * sakpp));
   }
+  if (l == 0 && s < 2) F.spp[c] = 0.f;
+  F.szp[at] = szp;
+  F.stp[at] = stp;
+  F.sdp[at] = sdp;
+  F.sqp[at] = sqp;
+  F.stt[at] = stt;
+  F.sqt[at] = sqt;
+  F.sdt[at] = zsdt1 + zsdt2;
+  F.szt[at] = szt;
+  F.zdsdp1[at] = zsdt1 * D2;
+  F.zdszp1[at] = zszt1 * D2;
+  F.zdsdp2[at] = zsdt2 * D2;
+  F.zdszp2[at] = zszt2 * D2;
 }
 
 // mkdheat's grid-point stages (dynamics/wgsl/mkdheat.wgsl).
 __global__ void __launch_bounds__(kBlock) k_mkdheat(Model m, int stage) {
   const Dims& d = m.d;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.S * d.NHOR) return;
+  const int slot = blockIdx.x * kBlock / d.NHOR;  // kBlock divides NHOR
+  const int c = blockIdx.x * kBlock + threadIdx.x;
   const int l = blockIdx.y;
   const size_t i = (size_t)l * d.S * d.NHOR + c;
-  const int slot = c / d.NHOR, h = c - slot * d.NHOR;
+  const int h = c - slot * d.NHOR;
   const StepParams& P = m.params[slot];
   if (!P.active) return;
   const PlanetConst& K = m.pc[slot];
@@ -360,95 +363,129 @@ __global__ void k_mean_mode(float* t, int nrsp) {
   t[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * nrsp + r] = 0.f;
 }
 
-// spectrald after mkdheat (dynamics/wgsl/spectrald-update.wgsl).
+// spectrald after mkdheat (dynamics/wgsl/spectrald-update.wgsl), one thread
+// per (level, spectral coefficient), all inputs read before the first store.
 __global__ void __launch_bounds__(kBlock) k_spectrald_update(Model m) {
   const Dims& d = m.d;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.S * d.NRSP) return;
+  const int l = blockIdx.y;
   const int slot = c / d.NRSP;
   const StepParams& P = m.params[slot];
   if (!P.active) return;
-  const PlanetConst& K = m.pc[slot];
-  const size_t SR = (size_t)d.S * d.NRSP;
+  const float PNU = m.pc[slot].PNU;
+  const size_t at = (size_t)l * d.S * d.NRSP + c;
   const FieldPtrs& F = m.f;
   const bool filter = P.filter != 0.f;
   const float D2 = P.delt2;
-  const float spp = F.spp[c];
-  if (filter) F.spm[c] = F.spm[c] + K.PNU * spp;
-  F.sp[c] = spp;
-  for (int l = 0; l < d.NLEV; ++l) {
-    const size_t at = l * SR + c;
-    const float stt = F.stt[at] + F.zstt1[at] + F.zstt2[at];
-    F.stt[at] = stt;
-    const float szp = F.szp[at] + D2 * F.szt[at];
-    const float stp = F.stp[at] + D2 * stt;
-    const float sdp = F.sdp[at] + D2 * F.sdt[at];
-    const float sqp = F.sqp[at] + D2 * F.sqt[at];
-    F.szp[at] = szp;
-    F.stp[at] = stp;
-    F.sdp[at] = sdp;
-    F.sqp[at] = sqp;
-    if (filter) {
-      F.szm[at] = F.szm[at] + K.PNU * szp;
-      F.stm[at] = F.stm[at] + K.PNU * stp;
-      F.sdm[at] = F.sdm[at] + K.PNU * sdp;
-      F.sqm[at] = F.sqm[at] + K.PNU * sqp;
-    }
-    F.sz[at] = szp;
-    F.st[at] = stp;
-    F.sd[at] = sdp;
-    F.sq[at] = sqp;
+  const float stt0 = F.stt[at], zstt1 = F.zstt1[at], zstt2 = F.zstt2[at];
+  const float szp0 = F.szp[at], szt = F.szt[at], stp0 = F.stp[at], sdp0 = F.sdp[at], sdt = F.sdt[at];
+  const float sqp0 = F.sqp[at], sqt = F.sqt[at];
+  float szm = 0.f, stm = 0.f, sdm = 0.f, sqm = 0.f;
+  if (filter) {
+    szm = F.szm[at];
+    stm = F.stm[at];
+    sdm = F.sdm[at];
+    sqm = F.sqm[at];
   }
+  const bool surface = l == 0;  // the level-0 thread also updates sp
+  const float spp = surface ? F.spp[c] : 0.f;
+  const float spm = surface && filter ? F.spm[c] : 0.f;
+  const float stt = stt0 + zstt1 + zstt2;
+  const float szp = szp0 + D2 * szt;
+  const float stp = stp0 + D2 * stt;
+  const float sdp = sdp0 + D2 * sdt;
+  const float sqp = sqp0 + D2 * sqt;
+  if (surface) {
+    if (filter) F.spm[c] = spm + PNU * spp;
+    F.sp[c] = spp;
+  }
+  F.stt[at] = stt;
+  F.szp[at] = szp;
+  F.stp[at] = stp;
+  F.sdp[at] = sdp;
+  F.sqp[at] = sqp;
+  if (filter) {
+    F.szm[at] = szm + PNU * szp;
+    F.stm[at] = stm + PNU * stp;
+    F.sdm[at] = sdm + PNU * sdp;
+    F.sqm[at] = sqm + PNU * sqp;
+  }
+  F.sz[at] = szp;
+  F.st[at] = stp;
+  F.sd[at] = sdp;
+  F.sq[at] = sqp;
 }
 
-// gridpointd before the parameterizations (dynamics/wgsl/physics-in.wgsl).
+// gridpointd before the parameterizations (dynamics/wgsl/physics-in.wgsl),
+// one thread per column, every input read before the first store. A block's
+// columns share one slot: kBlock divides NHOR.
+template <int NL>
 __global__ void __launch_bounds__(kBlock) k_physics_in(Model m) {
   const Dims& d = m.d;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.S * d.NHOR) return;
-  const int slot = c / d.NHOR, h = c % d.NHOR;
+  const int slot = blockIdx.x * kBlock / d.NHOR;
   if (!m.params[slot].active) return;
+  const int c = blockIdx.x * kBlock + threadIdx.x;
+  const int h = c - slot * d.NHOR;
   const PlanetConst& K = m.pc[slot];
+  const float PSURF = K.PSURF, CV = K.CV, CT = K.CT;
   const float* t0 = m.tabs + (size_t)slot * m.to.stride + m.to.t0;
   const size_t SN = (size_t)d.S * d.NHOR;
   const FieldPtrs& F = m.f;
-  const float dp = K.PSURF * expf(F.gp[c]);
+  const float gp = F.gp[c], rcsq = m.sh.rcsq[h];
+  float gu[NL], gv[NL], gt[NL], gq[NL], t0l[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    gu[l] = F.gu[at];
+    gv[l] = F.gv[at];
+    gt[l] = F.gt[at];
+    gq[l] = F.gq[at];
+    t0l[l] = t0[l];
+  }
+  const float dp = PSURF * expf(gp);
   F.dp[c] = dp;
-  const float scale = sqrtf(m.sh.rcsq[h]);
-  for (int l = 0; l < d.NLEP; ++l) {
+  const float scale = sqrtf(rcsq);
+#pragma unroll
+  for (int l = 0; l < NL + 1; ++l) {
     const size_t at = l * SN + c;
     F.dudt[at] = 0.f;
     F.dvdt[at] = 0.f;
     F.dtdt[at] = 0.f;
     F.dqdt[at] = 0.f;
-    if (l < d.NLEV) {
+    if (l < NL) {
       F.gudt[at] = 0.f;
       F.gvdt[at] = 0.f;
       F.gtdt[at] = 0.f;
       F.gqdt[at] = 0.f;
-      F.du[at] = K.CV * F.gu[at] * scale;
-      F.dv[at] = K.CV * F.gv[at] * scale;
-      F.dt[at] = K.CT * (F.gt[at] + t0[l]);
-      F.dq[at] = F.gq[at] * K.PSURF / dp;
+      F.du[at] = CV * gu[l] * scale;
+      F.dv[at] = CV * gv[l] * scale;
+      F.dt[at] = CT * (gt[l] + t0l[l]);
+      F.dq[at] = gq[l] * PSURF / dp;
     }
   }
 }
 
-// gridpointd after the parameterizations (dynamics/wgsl/physics-out.wgsl).
+// gridpointd after the parameterizations (dynamics/wgsl/physics-out.wgsl),
+// one thread per (level, column), inputs read before the stores.
 __global__ void __launch_bounds__(kBlock) k_physics_out(Model m) {
   const Dims& d = m.d;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.S * d.NHOR) return;
-  const size_t i = (size_t)blockIdx.y * d.S * d.NHOR + c;
-  const int slot = c / d.NHOR, h = c - slot * d.NHOR;
+  const int slot = blockIdx.x * kBlock / d.NHOR;
   if (!m.params[slot].active) return;
+  const int c = blockIdx.x * kBlock + threadIdx.x;
+  const int h = c - slot * d.NHOR;
+  const size_t i = (size_t)blockIdx.y * d.S * d.NHOR + c;
   const PlanetConst& K = m.pc[slot];
+  const float CV = K.CV, WW = K.WW, CT = K.CT, PSURF = K.PSURF;
   const FieldPtrs& F = m.f;
+  const float dudt = F.dudt[i], dvdt = F.dvdt[i], dtdt = F.dtdt[i], dqdt = F.dqdt[i];
+  const float gudt = F.gudt[i], gvdt = F.gvdt[i], gtdt = F.gtdt[i], gqdt = F.gqdt[i];
+  const float dp = F.dp[c];
   const float scale = sqrtf(m.sh.rcsq[h]);
-  F.gudt[i] = F.dudt[i] / scale / K.CV / K.WW + F.gudt[i];
-  F.gvdt[i] = F.dvdt[i] / scale / K.CV / K.WW + F.gvdt[i];
-  F.gtdt[i] = F.dtdt[i] / K.CT / K.WW + F.gtdt[i];
-  F.gqdt[i] = F.dqdt[i] * F.dp[c] / K.WW / K.PSURF + F.gqdt[i];
+  F.gudt[i] = dudt / scale / CV / WW + gudt;
+  F.gvdt[i] = dvdt / scale / CV / WW + gvdt;
+  F.gtdt[i] = dtdt / CT / WW + gtdt;
+  F.gqdt[i] = dqdt * dp / WW / PSURF + gqdt;
 }
 
 inline unsigned blocks(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -471,7 +508,8 @@ void dyn_spectrala(const Model& m, cudaStream_t st) {
     k_spectrala<5><<<n, kBlock, 0, st>>>(m);
 }
 void dyn_spectrald_diffusion(const Model& m, cudaStream_t st) {
-  k_spectrald_diffusion<<<blocks((size_t)m.d.S * m.d.NRSP, kBlock), kBlock, 0, st>>>(m);
+  const dim3 grid(blocks((size_t)m.d.S * m.d.NRSP, kBlock), m.d.NLEV);
+  k_spectrald_diffusion<<<grid, kBlock, 0, st>>>(m);
 }
 void dyn_mkdheat(const Model& m, int stage, cudaStream_t st) {
   const dim3 grid(blocks((size_t)m.d.S * m.d.NHOR, kBlock), m.d.NLEV);
@@ -482,10 +520,15 @@ void dyn_mean_mode(const Model& m, float* target, cudaStream_t st) {
   k_mean_mode<<<grid, 256, 0, st>>>(target, m.d.NRSP);
 }
 void dyn_spectrald_update(const Model& m, cudaStream_t st) {
-  k_spectrald_update<<<blocks((size_t)m.d.S * m.d.NRSP, kBlock), kBlock, 0, st>>>(m);
+  const dim3 grid(blocks((size_t)m.d.S * m.d.NRSP, kBlock), m.d.NLEV);
+  k_spectrald_update<<<grid, kBlock, 0, st>>>(m);
 }
 void dyn_physics_in(const Model& m, cudaStream_t st) {
-  k_physics_in<<<blocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);
+  const unsigned n = (unsigned)((size_t)m.d.S * m.d.NHOR / kBlock);
+  if (m.d.L == 10)
+    k_physics_in<10><<<n, kBlock, 0, st>>>(m);
+  else
+    k_physics_in<5><<<n, kBlock, 0, st>>>(m);
 }
 void dyn_physics_out(const Model& m, cudaStream_t st) {
   const dim3 grid(blocks((size_t)m.d.S * m.d.NHOR, kBlock), m.d.NLEV);

@@ -1170,6 +1170,18 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
     } else if (k == "spectrala") {
       launch = [&] { dyn_spectrala(m, e->stream); };
       b = (double)S * d.NRSP * 4 * (6.0 * d.L + 3 + 14.0 * d.L + 3);
+    } else if (k == "mkdheat") {
+      // stage 1: dq, u, v, du, dv per level and dp in; dtdt out
+      launch = [&] { dyn_mkdheat(m, 1, e->stream); };
+      b = cols * 4 * (6.0 * d.L + 1);
+    } else if (k == "physics_in") {
+      // gp, u, v, t, q in; dp, the dimensional u, v, t, q and the zeroed tendencies out
+      launch = [&] { dyn_physics_in(m, e->stream); };
+      b = cols * 4 * (4.0 * d.L + 1 + 1 + 4.0 * d.L + 4.0 * (d.L + 1) + 4.0 * d.L);
+    } else if (k == "physics_out") {
+      // four physics tendencies, four dynamics tendencies and dp in; four tendencies out
+      launch = [&] { dyn_physics_out(m, e->stream); };
+      b = cols * 4 * (8.0 * d.L + 1 + 4.0 * d.L);
     } else {
       // Column kernels: compulsory reads + writes per column, in floats.
       const std::map<std::string, double> per_column = {
