@@ -324,11 +324,21 @@ __global__ void __launch_bounds__(kBlock) k_spectrald_diffusion(Model m) {
   F.zdszp2[at] = zszt2 * D2;
 }
 
+// Elementwise grid-point kernels give each thread four adjacent columns of
+// one level (16-byte loads and stores): a block covers kCols4 = 512
+// columns, and 512 divides NHOR (2048, 8192, 18432), so a block's columns
+// share one slot. Four columns per thread keep four times the bytes in
+// flight for the same number of resident warps.
+constexpr int kCols4 = 4 * kBlock;
+
+__device__ __forceinline__ float4 ld4(const float* p, size_t i) { return *reinterpret_cast<const float4*>(p + i); }
+__device__ __forceinline__ void st4(float* p, size_t i, float4 v) { *reinterpret_cast<float4*>(p + i) = v; }
+
 // mkdheat's grid-point stages (dynamics/wgsl/mkdheat.wgsl).
 __global__ void __launch_bounds__(kBlock) k_mkdheat(Model m, int stage) {
   const Dims& d = m.d;
-  const int slot = blockIdx.x * kBlock / d.NHOR;  // kBlock divides NHOR
-  const int c = blockIdx.x * kBlock + threadIdx.x;
+  const int slot = blockIdx.x * kCols4 / d.NHOR;
+  const int c = blockIdx.x * kCols4 + 4 * threadIdx.x;
   const int l = blockIdx.y;
   const size_t i = (size_t)l * d.S * d.NHOR + c;
   const int h = c - slot * d.NHOR;
@@ -337,22 +347,36 @@ __global__ void __launch_bounds__(kBlock) k_mkdheat(Model m, int stage) {
   const PlanetConst& K = m.pc[slot];
   const float ds = m.tabs[(size_t)slot * m.to.stride + m.to.dsigma + l];
   const FieldPtrs& F = m.f;
-  const float heat = 1.f + K.ADV * F.dq[i];
+  const float4 dq = ld4(F.dq, i);
+  const float4 heat = make_float4(1.f + K.ADV * dq.x, 1.f + K.ADV * dq.y, 1.f + K.ADV * dq.z, 1.f + K.ADV * dq.w);
   if (stage == 3) {
-    const float dp = F.dp[c];
-    const float dtdt = -F.zdekin[i] * 0.5f / K.ACPD / heat / dp * K.GA / ds;
-    F.zdtdt[i] = dtdt / K.CT / K.WW;
+    const float4 dp = ld4(F.dp, c), ek = ld4(F.zdekin, i);
+    auto one = [&](float e, float ht, float p) {
+      const float dtdt = -e * 0.5f / K.ACPD / ht / p * K.GA / ds;
+      return dtdt / K.CT / K.WW;
+    };
+    st4(F.zdtdt, i, make_float4(one(ek.x, heat.x, dp.x), one(ek.y, heat.y, dp.y), one(ek.z, heat.z, dp.z),
+                                one(ek.w, heat.w, dp.w)));
     return;
   }
-  const float scale = K.CV * sqrtf(m.sh.rcsq[h]);
-  const float u = F.zu[i] * scale, v = F.zv[i] * scale, du = F.zdu[i] * scale, dv = F.zdv[i] * scale;
-  const float change = du * (2.f * u + du) + dv * (2.f * v + dv);
-  if (stage == 1) {
-    const float dtdt = -change / P.deltsec2 * 0.5f / K.ACPD / heat;
-    F.zdtdt[i] = dtdt / K.CT / K.WW;
-  } else {
-    F.zdekin[i] = change / P.deltsec2 * F.dp[c] / K.GA * ds;
-  }
+  const float4 zu = ld4(F.zu, i), zv = ld4(F.zv, i), zdu = ld4(F.zdu, i), zdv = ld4(F.zdv, i);
+  const float4 rc = ld4(m.sh.rcsq, h);
+  const float4 dp = stage == 1 ? make_float4(0.f, 0.f, 0.f, 0.f) : ld4(F.dp, c);
+  auto one = [&](float r, float zu1, float zv1, float zdu1, float zdv1, float ht, float p) {
+    const float scale = K.CV * sqrtf(r);
+    const float u = zu1 * scale, v = zv1 * scale, du = zdu1 * scale, dv = zdv1 * scale;
+    const float change = du * (2.f * u + du) + dv * (2.f * v + dv);
+    if (stage == 1) {
+      const float dtdt = -change / P.deltsec2 * 0.5f / K.ACPD / ht;
+      return dtdt / K.CT / K.WW;
+    }
+    return change / P.deltsec2 * p / K.GA * ds;
+  };
+  const float4 r = make_float4(one(rc.x, zu.x, zv.x, zdu.x, zdv.x, heat.x, dp.x),
+                               one(rc.y, zu.y, zv.y, zdu.y, zdv.y, heat.y, dp.y),
+                               one(rc.z, zu.z, zv.z, zdu.z, zdv.z, heat.z, dp.z),
+                               one(rc.w, zu.w, zv.w, zdu.w, zdv.w, heat.w, dp.w));
+  st4(stage == 1 ? F.zdtdt : F.zdekin, i, r);
 }
 
 // mkdheat's zsdef(2:NESP,:) = 0 (dynamics/wgsl/mean-mode.wgsl).
@@ -467,25 +491,31 @@ __global__ void __launch_bounds__(kBlock) k_physics_in(Model m) {
 }
 
 // gridpointd after the parameterizations (dynamics/wgsl/physics-out.wgsl),
-// one thread per (level, column), inputs read before the stores.
+// four columns of one level per thread, inputs read before the stores.
 __global__ void __launch_bounds__(kBlock) k_physics_out(Model m) {
   const Dims& d = m.d;
-  const int slot = blockIdx.x * kBlock / d.NHOR;
+  const int slot = blockIdx.x * kCols4 / d.NHOR;
   if (!m.params[slot].active) return;
-  const int c = blockIdx.x * kBlock + threadIdx.x;
+  const int c = blockIdx.x * kCols4 + 4 * threadIdx.x;
   const int h = c - slot * d.NHOR;
   const size_t i = (size_t)blockIdx.y * d.S * d.NHOR + c;
   const PlanetConst& K = m.pc[slot];
   const float CV = K.CV, WW = K.WW, CT = K.CT, PSURF = K.PSURF;
   const FieldPtrs& F = m.f;
-  const float dudt = F.dudt[i], dvdt = F.dvdt[i], dtdt = F.dtdt[i], dqdt = F.dqdt[i];
-  const float gudt = F.gudt[i], gvdt = F.gvdt[i], gtdt = F.gtdt[i], gqdt = F.gqdt[i];
-  const float dp = F.dp[c];
-  const float scale = sqrtf(m.sh.rcsq[h]);
-  F.gudt[i] = dudt / scale / CV / WW + gudt;
-  F.gvdt[i] = dvdt / scale / CV / WW + gvdt;
-  F.gtdt[i] = dtdt / CT / WW + gtdt;
-  F.gqdt[i] = dqdt * dp / WW / PSURF + gqdt;
+  const float4 dudt = ld4(F.dudt, i), dvdt = ld4(F.dvdt, i), dtdt = ld4(F.dtdt, i), dqdt = ld4(F.dqdt, i);
+  const float4 gudt = ld4(F.gudt, i), gvdt = ld4(F.gvdt, i), gtdt = ld4(F.gtdt, i), gqdt = ld4(F.gqdt, i);
+  const float4 dp = ld4(F.dp, c), rc = ld4(m.sh.rcsq, h);
+  const float4 scale = make_float4(sqrtf(rc.x), sqrtf(rc.y), sqrtf(rc.z), sqrtf(rc.w));
+  auto wind = [&](float4 t, float4 g) {
+    return make_float4(t.x / scale.x / CV / WW + g.x, t.y / scale.y / CV / WW + g.y, t.z / scale.z / CV / WW + g.z,
+                       t.w / scale.w / CV / WW + g.w);
+  };
+  st4(F.gudt, i, wind(dudt, gudt));
+  st4(F.gvdt, i, wind(dvdt, gvdt));
+  st4(F.gtdt, i, make_float4(dtdt.x / CT / WW + gtdt.x, dtdt.y / CT / WW + gtdt.y, dtdt.z / CT / WW + gtdt.z,
+                             dtdt.w / CT / WW + gtdt.w));
+  st4(F.gqdt, i, make_float4(dqdt.x * dp.x / WW / PSURF + gqdt.x, dqdt.y * dp.y / WW / PSURF + gqdt.y,
+                             dqdt.z * dp.z / WW / PSURF + gqdt.z, dqdt.w * dp.w / WW / PSURF + gqdt.w));
 }
 
 inline unsigned blocks(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -512,7 +542,7 @@ void dyn_spectrald_diffusion(const Model& m, cudaStream_t st) {
   k_spectrald_diffusion<<<grid, kBlock, 0, st>>>(m);
 }
 void dyn_mkdheat(const Model& m, int stage, cudaStream_t st) {
-  const dim3 grid(blocks((size_t)m.d.S * m.d.NHOR, kBlock), m.d.NLEV);
+  const dim3 grid((unsigned)((size_t)m.d.S * m.d.NHOR / kCols4), m.d.NLEV);
   k_mkdheat<<<grid, kBlock, 0, st>>>(m, stage);
 }
 void dyn_mean_mode(const Model& m, float* target, cudaStream_t st) {
@@ -531,7 +561,7 @@ void dyn_physics_in(const Model& m, cudaStream_t st) {
     k_physics_in<5><<<n, kBlock, 0, st>>>(m);
 }
 void dyn_physics_out(const Model& m, cudaStream_t st) {
-  const dim3 grid(blocks((size_t)m.d.S * m.d.NHOR, kBlock), m.d.NLEV);
+  const dim3 grid((unsigned)((size_t)m.d.S * m.d.NHOR / kCols4), m.d.NLEV);
   k_physics_out<<<grid, kBlock, 0, st>>>(m);
 }
 
