@@ -270,58 +270,63 @@ __global__ void __launch_bounds__(kBlock, 5) k_spectrala(Model m) {
   }
 }
 
-// spectrald up to mkdheat (dynamics/wgsl/spectrald-diffusion.wgsl), one
-// thread per (level, spectral coefficient). A thread reads all its inputs
-// before its first store: the fields are distinct arrays, but the compiler
-// cannot prove it, and would otherwise order each load after the stores
-// before it.
+__device__ __forceinline__ float2 ld2(const float* p, size_t i) { return *reinterpret_cast<const float2*>(p + i); }
+__device__ __forceinline__ void st2(float* p, size_t i, float2 v) { *reinterpret_cast<float2*>(p + i) = v; }
+
+// spectrald up to mkdheat (dynamics/wgsl/spectrald-diffusion.wgsl). A thread
+// owns two adjacent real coefficients (NRSP is even, so both are of one
+// slot) of one level. Every input is read before the slot's parameters are
+// tested and before the first store: the fields are distinct arrays, but
+// the compiler cannot prove it, and would otherwise order each load after
+// the stores before it.
 __global__ void __launch_bounds__(kBlock) k_spectrald_diffusion(Model m) {
   const Dims& d = m.d;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   if (c >= d.S * d.NRSP) return;
   const int l = blockIdx.y;
   const int slot = c / d.NRSP, s = c - slot * d.NRSP;
-  const StepParams& P = m.params[slot];
-  if (!P.active) return;
   const float* tb = slot_tabs(m, slot);
   const size_t at = (size_t)l * d.S * d.NRSP + c;
   const FieldPtrs& F = m.f;
-  const float D2 = P.delt2, PLAVOR = m.pc[slot].PLAVOR;
-  const float szp0 = F.szp[at], szt0 = F.szt[at], stp0 = F.stp[at], stt0 = F.stt[at];
-  const float sdp0 = F.sdp[at], sdt0 = F.sdt[at], sqp0 = F.sqp[at], sqt0 = F.sqt[at];
-  const float sakpp = tb[m.to.sakpp + l * d.NRSP + s];
+  const float2 szp0 = ld2(F.szp, at), szt0 = ld2(F.szt, at), stp0 = ld2(F.stp, at), stt0 = ld2(F.stt, at);
+  const float2 sdp0 = ld2(F.sdp, at), sdt0 = ld2(F.sdt, at), sqp0 = ld2(F.sqp, at), sqt0 = ld2(F.sqt, at);
+  const float* sak = tb + m.to.sakpp + l * d.NRSP + s;
+  const float* srpl = tb + m.to.srp + l * d.NRSP + s;
+  const float sakpp[2] = {sak[0], sak[1]}, srp[2] = {srpl[0], srpl[1]};
   const float damp = tb[m.to.damp + l], tdisst = tb[m.to.tdisst + l], tdissq = tb[m.to.tdissq + l];
   const float tdissd = tb[m.to.tdissd + l], tdissz = tb[m.to.tdissz + l], tfrc = tb[m.to.tfrc + l];
-  const float srp = tb[m.to.srp + l * d.NRSP + s];
-  const float szp = szp0 + D2 * szt0;
-  const float stp = stp0 + D2 * stt0;
-  const float sdp = sdp0 + D2 * sdt0;
-  const float sqp = sqp0 + D2 * sqt0;
-  const float stt = ((-damp - tdisst * sakpp) * stp + damp * srp) / (1.f + D2 * (damp + tdisst * sakpp));
-  const float sqt = -tdissq * sakpp * sqp / (1.f + D2 * tdissq * sakpp);
-  const float zsdt1 = -tfrc * sdp / (1.f + D2 * tfrc);
-  const float zsdt2 = -tdissd * sakpp * sdp / (1.f + D2 * tdissd * sakpp);
-  float zszt1 = -tfrc * szp / (1.f + D2 * tfrc);
-  float zszt2 = -tdissz * sakpp * szp / (1.f + D2 * tdissz * sakpp);
-  float szt = zszt1 + zszt2;
-  if (s == 2) {
-    zszt1 = zszt1 + PLAVOR * tfrc / (1.f + D2 * tfrc);
-    zszt2 = zszt2 + PLAVOR * tdissz * sakpp / (1.f + D2 * tdissz * sakpp);
-    szt = szt + PLAVOR * (tfrc / (1.f + D2 * tfrc) + tdissz * sakpp / (1.f + D2 * tdissz * sakpp));
+  const StepParams& P = m.params[slot];
+  if (!P.active) return;
+  const float D2 = P.delt2, PLAVOR = m.pc[slot].PLAVOR;
+  float o[12][2];  // szp, stp, sdp, sqp, stt, sqt, sdt, szt, zdsdp1, zdszp1, zdsdp2, zdszp2
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const float szp = (k ? szp0.y : szp0.x) + D2 * (k ? szt0.y : szt0.x);
+    const float stp = (k ? stp0.y : stp0.x) + D2 * (k ? stt0.y : stt0.x);
+    const float sdp = (k ? sdp0.y : sdp0.x) + D2 * (k ? sdt0.y : sdt0.x);
+    const float sqp = (k ? sqp0.y : sqp0.x) + D2 * (k ? sqt0.y : sqt0.x);
+    const float sk = sakpp[k];
+    const float stt = ((-damp - tdisst * sk) * stp + damp * srp[k]) / (1.f + D2 * (damp + tdisst * sk));
+    const float sqt = -tdissq * sk * sqp / (1.f + D2 * tdissq * sk);
+    const float zsdt1 = -tfrc * sdp / (1.f + D2 * tfrc);
+    const float zsdt2 = -tdissd * sk * sdp / (1.f + D2 * tdissd * sk);
+    float zszt1 = -tfrc * szp / (1.f + D2 * tfrc);
+    float zszt2 = -tdissz * sk * szp / (1.f + D2 * tdissz * sk);
+    float szt = zszt1 + zszt2;
+    if (s + k == 2) {
+      zszt1 = zszt1 + PLAVOR * tfrc / (1.f + D2 * tfrc);
+      zszt2 = zszt2 + PLAVOR * tdissz * sk / (1.f + D2 * tdissz * sk);
+      szt = szt + PLAVOR * (tfrc / (1.f + D2 * tfrc) + tdissz * sk / (1.f + D2 * tdissz * sk));
+    }
+    const float v[12] = {szp, stp, sdp, sqp, stt, sqt, zsdt1 + zsdt2, szt, zsdt1 * D2, zszt1 * D2, zsdt2 * D2,
+                         zszt2 * D2};
+#pragma unroll
+    for (int j = 0; j < 12; ++j) o[j][k] = v[j];
   }
-  if (l == 0 && s < 2) F.spp[c] = 0.f;
-  F.szp[at] = szp;
-  F.stp[at] = stp;
-  F.sdp[at] = sdp;
-  F.sqp[at] = sqp;
-  F.stt[at] = stt;
-  F.sqt[at] = sqt;
-  F.sdt[at] = zsdt1 + zsdt2;
-  F.szt[at] = szt;
-  F.zdsdp1[at] = zsdt1 * D2;
-  F.zdszp1[at] = zszt1 * D2;
-  F.zdsdp2[at] = zsdt2 * D2;
-  F.zdszp2[at] = zszt2 * D2;
+  if (l == 0 && s < 2) st2(F.spp, c, make_float2(0.f, 0.f));
+  float* const dst[12] = {F.szp, F.stp, F.sdp, F.sqp, F.stt, F.sqt, F.sdt, F.szt, F.zdsdp1, F.zdszp1, F.zdsdp2, F.zdszp2};
+#pragma unroll
+  for (int j = 0; j < 12; ++j) st2(dst[j], at, make_float2(o[j][0], o[j][1]));
 }
 
 // Elementwise grid-point kernels give each thread four adjacent columns of
@@ -342,15 +347,25 @@ __global__ void __launch_bounds__(kBlock) k_mkdheat(Model m, int stage) {
   const int l = blockIdx.y;
   const size_t i = (size_t)l * d.S * d.NHOR + c;
   const int h = c - slot * d.NHOR;
+  const FieldPtrs& F = m.f;
+  // inputs first, then the slot's parameters
+  const float4 dq = ld4(F.dq, i);
+  const float4 dp = stage == 1 ? make_float4(0.f, 0.f, 0.f, 0.f) : ld4(F.dp, c);
+  const float4 ek = stage == 3 ? ld4(F.zdekin, i) : make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 zu = ek, zv = ek, zdu = ek, zdv = ek, rc = ek;
+  if (stage != 3) {
+    zu = ld4(F.zu, i);
+    zv = ld4(F.zv, i);
+    zdu = ld4(F.zdu, i);
+    zdv = ld4(F.zdv, i);
+    rc = ld4(m.sh.rcsq, h);
+  }
+  const float ds = m.tabs[(size_t)slot * m.to.stride + m.to.dsigma + l];
   const StepParams& P = m.params[slot];
   if (!P.active) return;
   const PlanetConst& K = m.pc[slot];
-  const float ds = m.tabs[(size_t)slot * m.to.stride + m.to.dsigma + l];
-  const FieldPtrs& F = m.f;
-  const float4 dq = ld4(F.dq, i);
   const float4 heat = make_float4(1.f + K.ADV * dq.x, 1.f + K.ADV * dq.y, 1.f + K.ADV * dq.z, 1.f + K.ADV * dq.w);
   if (stage == 3) {
-    const float4 dp = ld4(F.dp, c), ek = ld4(F.zdekin, i);
     auto one = [&](float e, float ht, float p) {
       const float dtdt = -e * 0.5f / K.ACPD / ht / p * K.GA / ds;
       return dtdt / K.CT / K.WW;
@@ -359,9 +374,6 @@ __global__ void __launch_bounds__(kBlock) k_mkdheat(Model m, int stage) {
                                 one(ek.w, heat.w, dp.w)));
     return;
   }
-  const float4 zu = ld4(F.zu, i), zv = ld4(F.zv, i), zdu = ld4(F.zdu, i), zdv = ld4(F.zdv, i);
-  const float4 rc = ld4(m.sh.rcsq, h);
-  const float4 dp = stage == 1 ? make_float4(0.f, 0.f, 0.f, 0.f) : ld4(F.dp, c);
   auto one = [&](float r, float zu1, float zv1, float zdu1, float zdv1, float ht, float p) {
     const float scale = K.CV * sqrtf(r);
     const float u = zu1 * scale, v = zv1 * scale, du = zdu1 * scale, dv = zdv1 * scale;
@@ -387,58 +399,58 @@ __global__ void k_mean_mode(float* t, int nrsp) {
   t[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * nrsp + r] = 0.f;
 }
 
-// spectrald after mkdheat (dynamics/wgsl/spectrald-update.wgsl), one thread
-// per (level, spectral coefficient), all inputs read before the first store.
+// spectrald after mkdheat (dynamics/wgsl/spectrald-update.wgsl), two
+// adjacent real coefficients of one level per thread, inputs read first.
 __global__ void __launch_bounds__(kBlock) k_spectrald_update(Model m) {
   const Dims& d = m.d;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   if (c >= d.S * d.NRSP) return;
   const int l = blockIdx.y;
   const int slot = c / d.NRSP;
+  const size_t at = (size_t)l * d.S * d.NRSP + c;
+  const FieldPtrs& F = m.f;
+  const float2 stt0 = ld2(F.stt, at), zstt1 = ld2(F.zstt1, at), zstt2 = ld2(F.zstt2, at);
+  const float2 szp0 = ld2(F.szp, at), szt = ld2(F.szt, at), stp0 = ld2(F.stp, at), sdp0 = ld2(F.sdp, at);
+  const float2 sdt = ld2(F.sdt, at), sqp0 = ld2(F.sqp, at), sqt = ld2(F.sqt, at);
+  const bool surface = l == 0;  // the level-0 threads also update sp
+  const float2 spp = surface ? ld2(F.spp, c) : make_float2(0.f, 0.f);
   const StepParams& P = m.params[slot];
   if (!P.active) return;
   const float PNU = m.pc[slot].PNU;
-  const size_t at = (size_t)l * d.S * d.NRSP + c;
-  const FieldPtrs& F = m.f;
   const bool filter = P.filter != 0.f;
   const float D2 = P.delt2;
-  const float stt0 = F.stt[at], zstt1 = F.zstt1[at], zstt2 = F.zstt2[at];
-  const float szp0 = F.szp[at], szt = F.szt[at], stp0 = F.stp[at], sdp0 = F.sdp[at], sdt = F.sdt[at];
-  const float sqp0 = F.sqp[at], sqt = F.sqt[at];
-  float szm = 0.f, stm = 0.f, sdm = 0.f, sqm = 0.f;
+  float2 szm = make_float2(0.f, 0.f), stm = szm, sdm = szm, sqm = szm, spm = szm;
   if (filter) {
-    szm = F.szm[at];
-    stm = F.stm[at];
-    sdm = F.sdm[at];
-    sqm = F.sqm[at];
+    szm = ld2(F.szm, at);
+    stm = ld2(F.stm, at);
+    sdm = ld2(F.sdm, at);
+    sqm = ld2(F.sqm, at);
+    if (surface) spm = ld2(F.spm, c);
   }
-  const bool surface = l == 0;  // the level-0 thread also updates sp
-  const float spp = surface ? F.spp[c] : 0.f;
-  const float spm = surface && filter ? F.spm[c] : 0.f;
-  const float stt = stt0 + zstt1 + zstt2;
-  const float szp = szp0 + D2 * szt;
-  const float stp = stp0 + D2 * stt;
-  const float sdp = sdp0 + D2 * sdt;
-  const float sqp = sqp0 + D2 * sqt;
+  const float2 stt = make_float2(stt0.x + zstt1.x + zstt2.x, stt0.y + zstt1.y + zstt2.y);
+  const float2 szp = make_float2(szp0.x + D2 * szt.x, szp0.y + D2 * szt.y);
+  const float2 stp = make_float2(stp0.x + D2 * stt.x, stp0.y + D2 * stt.y);
+  const float2 sdp = make_float2(sdp0.x + D2 * sdt.x, sdp0.y + D2 * sdt.y);
+  const float2 sqp = make_float2(sqp0.x + D2 * sqt.x, sqp0.y + D2 * sqt.y);
   if (surface) {
-    if (filter) F.spm[c] = spm + PNU * spp;
-    F.sp[c] = spp;
+    if (filter) st2(F.spm, c, make_float2(spm.x + PNU * spp.x, spm.y + PNU * spp.y));
+    st2(F.sp, c, spp);
   }
-  F.stt[at] = stt;
-  F.szp[at] = szp;
-  F.stp[at] = stp;
-  F.sdp[at] = sdp;
-  F.sqp[at] = sqp;
+  st2(F.stt, at, stt);
+  st2(F.szp, at, szp);
+  st2(F.stp, at, stp);
+  st2(F.sdp, at, sdp);
+  st2(F.sqp, at, sqp);
   if (filter) {
-    F.szm[at] = szm + PNU * szp;
-    F.stm[at] = stm + PNU * stp;
-    F.sdm[at] = sdm + PNU * sdp;
-    F.sqm[at] = sqm + PNU * sqp;
+    st2(F.szm, at, make_float2(szm.x + PNU * szp.x, szm.y + PNU * szp.y));
+    st2(F.stm, at, make_float2(stm.x + PNU * stp.x, stm.y + PNU * stp.y));
+    st2(F.sdm, at, make_float2(sdm.x + PNU * sdp.x, sdm.y + PNU * sdp.y));
+    st2(F.sqm, at, make_float2(sqm.x + PNU * sqp.x, sqm.y + PNU * sqp.y));
   }
-  F.sz[at] = szp;
-  F.st[at] = stp;
-  F.sd[at] = sdp;
-  F.sq[at] = sqp;
+  st2(F.sz, at, szp);
+  st2(F.st, at, stp);
+  st2(F.sd, at, sdp);
+  st2(F.sq, at, sqp);
 }
 
 // gridpointd before the parameterizations (dynamics/wgsl/physics-in.wgsl),
@@ -495,16 +507,16 @@ __global__ void __launch_bounds__(kBlock) k_physics_in(Model m) {
 __global__ void __launch_bounds__(kBlock) k_physics_out(Model m) {
   const Dims& d = m.d;
   const int slot = blockIdx.x * kCols4 / d.NHOR;
-  if (!m.params[slot].active) return;
   const int c = blockIdx.x * kCols4 + 4 * threadIdx.x;
   const int h = c - slot * d.NHOR;
   const size_t i = (size_t)blockIdx.y * d.S * d.NHOR + c;
-  const PlanetConst& K = m.pc[slot];
-  const float CV = K.CV, WW = K.WW, CT = K.CT, PSURF = K.PSURF;
   const FieldPtrs& F = m.f;
   const float4 dudt = ld4(F.dudt, i), dvdt = ld4(F.dvdt, i), dtdt = ld4(F.dtdt, i), dqdt = ld4(F.dqdt, i);
   const float4 gudt = ld4(F.gudt, i), gvdt = ld4(F.gvdt, i), gtdt = ld4(F.gtdt, i), gqdt = ld4(F.gqdt, i);
   const float4 dp = ld4(F.dp, c), rc = ld4(m.sh.rcsq, h);
+  if (!m.params[slot].active) return;
+  const PlanetConst& K = m.pc[slot];
+  const float CV = K.CV, WW = K.WW, CT = K.CT, PSURF = K.PSURF;
   const float4 scale = make_float4(sqrtf(rc.x), sqrtf(rc.y), sqrtf(rc.z), sqrtf(rc.w));
   auto wind = [&](float4 t, float4 g) {
     return make_float4(t.x / scale.x / CV / WW + g.x, t.y / scale.y / CV / WW + g.y, t.z / scale.z / CV / WW + g.z,
@@ -538,7 +550,7 @@ void dyn_spectrala(const Model& m, cudaStream_t st) {
     k_spectrala<5><<<n, kBlock, 0, st>>>(m);
 }
 void dyn_spectrald_diffusion(const Model& m, cudaStream_t st) {
-  const dim3 grid(blocks((size_t)m.d.S * m.d.NRSP, kBlock), m.d.NLEV);
+  const dim3 grid(blocks((size_t)m.d.S * m.d.NRSP / 2, kBlock), m.d.NLEV);
   k_spectrald_diffusion<<<grid, kBlock, 0, st>>>(m);
 }
 void dyn_mkdheat(const Model& m, int stage, cudaStream_t st) {
@@ -550,7 +562,7 @@ void dyn_mean_mode(const Model& m, float* target, cudaStream_t st) {
   k_mean_mode<<<grid, 256, 0, st>>>(target, m.d.NRSP);
 }
 void dyn_spectrald_update(const Model& m, cudaStream_t st) {
-  const dim3 grid(blocks((size_t)m.d.S * m.d.NRSP, kBlock), m.d.NLEV);
+  const dim3 grid(blocks((size_t)m.d.S * m.d.NRSP / 2, kBlock), m.d.NLEV);
   k_spectrald_update<<<grid, kBlock, 0, st>>>(m);
 }
 void dyn_physics_in(const Model& m, cudaStream_t st) {
