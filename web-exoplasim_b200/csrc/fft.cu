@@ -165,11 +165,10 @@ struct Shape {
   static constexpr int XP = 9 * Q;  // exchange float2s per row
 };
 
-// Twiddles, the exchange rows and the coefficient stage, whose M + 1 rows
-// hold zeros from NTP1 on (the inverse reads c_k and c_{M-k} for every k).
+// Twiddles, the exchange rows and the coefficient stage of NTP1 rows.
 inline size_t chunk_smem(int Q, int T, int rows) {
-  return ((size_t)2 * 8 * Q + 9 * Q + (size_t)rows * 9 * Q + (size_t)(8 * Q + 1) * fc_pitch(rows, T)) *
-         sizeof(float2);
+  const int ntp1 = Q == 4 ? 22 : Q == 8 ? 43 : 64;
+  return ((size_t)2 * 8 * Q + 9 * Q + (size_t)rows * 9 * Q + (size_t)ntp1 * fc_pitch(rows, T)) * sizeof(float2);
 }
 
 // Twiddle tables into shared memory: tw[j] = e^{2 pi i j / N};
@@ -284,13 +283,13 @@ __global__ void __launch_bounds__(kMaxThreads) k_fft_inverse(const float* __rest
   const size_t plane = blockIdx.x / chunks;
   const int lat0 = (blockIdx.x % chunks) * rows;
   {
-    // rows * T threads: thread (m0, lat) stages m = m0, m0 + T, ... <= M,
-    // zeros from NTP1 on; Im c_0 is ignored.
+    // rows * T threads: thread (m0, lat) stages m = m0, m0 + T, ... < NTP1;
+    // Im c_0 is ignored.
     const int lat = threadIdx.x % rows, m0 = threadIdx.x / rows;
     const float2* src = reinterpret_cast<const float2*>(c) + plane * nlat * NTP1 + lat0 + lat;
 #pragma unroll 4
-    for (int m = m0; m <= M; m += T) {
-      float2 v = m < NTP1 ? src[(size_t)m * nlat] : make_float2(0.f, 0.f);
+    for (int m = m0; m < NTP1; m += T) {
+      float2 v = src[(size_t)m * nlat];
       if (m == 0) v.y = 0.f;
       fc[m * pitch + lat] = v;
     }
@@ -303,9 +302,11 @@ __global__ void __launch_bounds__(kMaxThreads) k_fft_inverse(const float* __rest
   for (int i = 0; i < Sh::QT; ++i)
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
-      const int k = Q * p + t + T * i;
-      const float2 gk = fc[k * pitch + r];
-      const float2 gmk = conj2(fc[(M - k) * pitch + r]);
+      // c_k is zero from NTP1 on (k = 0 reads c_M = 0); for most p the
+      // bounds are settled at compile time, t being below T
+      const int k = Q * p + t + T * i, km = M - k;
+      const float2 gk = k < NTP1 ? fc[k * pitch + r] : make_float2(0.f, 0.f);
+      const float2 gmk = conj2(km < NTP1 ? fc[km * pitch + r] : make_float2(0.f, 0.f));
       const float2 e = cadd(gk, gmk);
       const float2 o = cmul(csub(gk, gmk), tw[k]);
       a[i][p] = make_float2(e.x - o.y, e.y + o.x);  // e + i o

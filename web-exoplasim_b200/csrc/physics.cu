@@ -904,15 +904,29 @@ __global__ void __launch_bounds__(kBlock, 6) k_kuo(Model m) {
   const float D2 = P.deltsec2;
   const float dp = F.dp[c];
   float zdqt[NL], zqe[NL], zte[NL], zdqtot[NL], zalcpe[NL], zacpe[NL], zdqdt[NL], zdtdt[NL];
+  // Every field this column reads is loaded before its first store (the
+  // compiler cannot prove the fields distinct, and would otherwise wait for
+  // each later load in turn); dtdt and dqdt stay in registers.
+  float dqt_in[NL], dq_in[NL], dqdt_in[NL], dt_in[NL], dtdt_in[NL];
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SN + c;
-    zdqt[l] = F.dqt[at] * K.PSURF * K.WW / dp;
+    dqt_in[l] = F.dqt[at];
+    dq_in[l] = F.dq[at];
+    dqdt_in[l] = F.dqdt[at];
+    dt_in[l] = F.dt[at];
+    dtdt_in[l] = F.dtdt[at];
+  }
+  const float dt_surface = F.dt[NL * SN + c], dq_surface = F.dq[NL * SN + c];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    zdqt[l] = dqt_in[l] * K.PSURF * K.WW / dp;
     F.dqt[at] = zdqt[l];
-    const float dq = F.dq[at], dqdt = F.dqdt[at];
+    const float dq = dq_in[l], dqdt = dqdt_in[l];
     zdqtot[l] = (zdqt[l] + dqdt) * D2;
     zqe[l] = dq + dqdt * D2;
-    zte[l] = F.dt[at] + F.dtdt[at] * D2;
+    zte[l] = dt_in[l] + dtdt_in[l] * D2;
     zacpe[l] = K.ACPD * (1.f + K.ADV * dq);
     zalcpe[l] = K.ALV / zacpe[l];
     zdqdt[l] = 0.f;
@@ -923,11 +937,11 @@ __global__ void __launch_bounds__(kBlock, 6) k_kuo(Model m) {
   {
     const int n = NL - 1;
     const float dsn = ds[n];
-    const float ztsurf = F.dt[NL * SN + c] * tb[m.to.vdiff_skap + n];
+    const float ztsurf = dt_surface * tb[m.to.vdiff_skap + n];
     if (zdqtot[n] > 0.f && ztsurf > zte[n]) {
       const float p = dp * sg[n];
       const float zqsnl = sat_divided(K, zte[n], p);
-      const float zqnew = F.dq[NL * SN + c] * fminf(1.f, zqe[n] / zqsnl);
+      const float zqnew = dq_surface * fminf(1.f, zqe[n] / zqsnl);
       const Parcel parcel = condense(K, ztsurf, zqnew, p);
       if (parcel.saturated) {
         ilift = NL + 1;
@@ -1026,7 +1040,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_kuo(Model m) {
     float dprcl = 0.f, icclev = 0.f;
     if (ilift >= level && itop <= level && zi > 0.f && !shallow) {
       F.dqdt[at] = zaq * zdqdt[l] / D2 - zdqt[l];
-      F.dtdt[at] = zat * zdtdt[l] / D2 + F.dtdt[at];
+      F.dtdt[at] = zat * zdtdt[l] / D2 + dtdt_in[l];
       dprcl = zat * zdtdt[l] * ds[l] / zalcpe[l] / D2;
     }
     if (dprcl > 0.f) {
@@ -1082,9 +1096,10 @@ __global__ void __launch_bounds__(kBlock, 6) k_kuo(Model m) {
   diffuse_potential<NL>(ds, ztn, zkdiff, skap);
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
+    // a shallow column's deep-convection writes above did not run
     const size_t at = l * SN + c;
-    F.dtdt[at] = F.dtdt[at] + (ztn[l] - zte[l]) / D2;
-    F.dqdt[at] = F.dqdt[at] + (zqn[l] - zqe[l]) / D2;
+    F.dtdt[at] = dtdt_in[l] + (ztn[l] - zte[l]) / D2;
+    F.dqdt[at] = dqdt_in[l] + (zqn[l] - zqe[l]) / D2;
   }
 }
 
