@@ -143,6 +143,7 @@ struct Model {
   int mode;                  // 0 plain path, 1 optimized path (FFTs, latitude-pair Legendre, m-major Fourier),
                              // 2 optimized path with sp2fc / sp2fcdmu on the tensor cores
   Tuning tune;               // optimized path launch shapes
+  int keep_fourier;          // optimized path: fused transforms also write the Fourier fields they pass through
 };
 
 }  // namespace exogcm

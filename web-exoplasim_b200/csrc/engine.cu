@@ -123,6 +123,7 @@ struct exogcm_engine {
     m.fault = fault;
     m.mode = mode;
     m.tune = tune;
+    m.keep_fourier = 0;
     return m;
   }
 };
@@ -344,22 +345,17 @@ void stage_gridpointa(const Model& m, cudaStream_t st) {
   const FieldPtrs& F = m.f;
   const int LP = d.L * d.S, SP = d.S;
   tr_dv2uv(m, F.sd, F.sz, F.fgu, F.fgv, LP, 1.63299310207f, st);
-  tr_legendre_inverse(m, F.sd, F.fgd, LP, m.sh.qi, st);
-  tr_legendre_inverse(m, F.st, F.fgt, LP, m.sh.qi, st);
-  tr_legendre_inverse(m, F.sz, F.fgz, LP, m.sh.qi, st);
-  tr_legendre_inverse(m, F.sq, F.fgq, LP, m.sh.qi, st);
   tr_legendre_inverse(m, F.sp, F.fgp, SP, m.sh.qi, st);
-  tr_legendre_inverse(m, F.sp, F.fgpj, SP, m.sh.qj, st);
   tr_dlambda(m, F.fgp, F.fgpmt, SP, st);
   tr_fourier_inverse(m, F.fgu, F.gu, LP, st);
   tr_fourier_inverse(m, F.fgv, F.gv, LP, st);
-  tr_fourier_inverse(m, F.fgt, F.gt, LP, st);
-  tr_fourier_inverse(m, F.fgd, F.gd, LP, st);
-  tr_fourier_inverse(m, F.fgz, F.gz, LP, st);
-  tr_fourier_inverse(m, F.fgpj, F.gpj, SP, st);
+  tr_sp2gp(m, F.st, F.fgt, F.gt, LP, m.sh.qi, st);
+  tr_sp2gp(m, F.sd, F.fgd, F.gd, LP, m.sh.qi, st);
+  tr_sp2gp(m, F.sz, F.fgz, F.gz, LP, m.sh.qi, st);
+  tr_sp2gp(m, F.sp, F.fgpj, F.gpj, SP, m.sh.qj, st);
   tr_fourier_inverse(m, F.fgpmt, F.gpmt, SP, st);
   tr_fourier_inverse(m, F.fgp, F.gp, SP, st);
-  tr_fourier_inverse(m, F.fgq, F.gq, LP, st);
+  tr_sp2gp(m, F.sq, F.fgq, F.gq, LP, m.sh.qi, st);
   dyn_calcgp(m, st);
   tr_fourier_forward(m, F.gtn, F.fgtn, LP, st);
   tr_fourier_forward(m, F.gqn, F.fgqn, LP, st);
@@ -382,21 +378,17 @@ void stage_physics_in(const Model& m, cudaStream_t st) {
   const FieldPtrs& F = m.f;
   const int LP = d.L * d.S, SP = d.S;
   tr_dv2uv(m, F.sd, F.sz, F.fgu, F.fgv, LP, 1.63299310207f, st);
-  tr_legendre_inverse(m, F.sq, F.fgq, LP, m.sh.qi, st);
-  tr_legendre_inverse(m, F.st, F.fgt, LP, m.sh.qi, st);
-  tr_legendre_inverse(m, F.sp, F.fgp, SP, m.sh.qi, st);
   tr_fourier_inverse(m, F.fgu, F.gu, LP, st);
   tr_fourier_inverse(m, F.fgv, F.gv, LP, st);
-  tr_fourier_inverse(m, F.fgt, F.gt, LP, st);
-  tr_fourier_inverse(m, F.fgp, F.gp, SP, st);
-  tr_fourier_inverse(m, F.fgq, F.gq, LP, st);
+  tr_sp2gp(m, F.st, F.fgt, F.gt, LP, m.sh.qi, st);
+  tr_sp2gp(m, F.sp, F.fgp, F.gp, SP, m.sh.qi, st);
+  tr_sp2gp(m, F.sq, F.fgq, F.gq, LP, m.sh.qi, st);
   dyn_physics_in(m, st);
 }
 
 void stage_precipitation(const Model& m, cudaStream_t st) {
   const int LP = m.d.L * m.d.S;
-  tr_legendre_inverse(m, m.f.sqt, m.f.fdqt, LP, m.sh.qi, st);
-  tr_fourier_inverse(m, m.f.fdqt, m.f.dqt, LP, st);
+  tr_sp2gp(m, m.f.sqt, m.f.fdqt, m.f.dqt, LP, m.sh.qi, st);
   phy_precipitation_columns(m, st);
 }
 
@@ -434,8 +426,7 @@ void stage_spectrald(const Model& m, cudaStream_t st) {
   tr_fourier_forward(m, F.zdekin, F.fzdekin, LP, st);
   tr_legendre_forward(m, F.fzdekin, F.zsdef, LP, m.sh.qc, st);
   dyn_mean_mode(m, F.zsdef, st);
-  tr_legendre_inverse(m, F.zsdef, F.fzdekin, LP, m.sh.qi, st);
-  tr_fourier_inverse(m, F.fzdekin, F.zdekin, LP, st);
+  tr_sp2gp(m, F.zsdef, F.fzdekin, F.zdekin, LP, m.sh.qi, st);
   dyn_mkdheat(m, 3, st);
   tr_fourier_forward(m, F.zdtdt, F.fzdtdt, LP, st);
   tr_legendre_forward(m, F.fzdtdt, F.zstt2, LP, m.sh.qc, st);
@@ -1109,7 +1100,11 @@ int exogcm_run_stage(exogcm_engine* e, const char* stage) {
     }
     check(cudaMemcpyAsync(e->params, e->hparams, S * sizeof(StepParams), cudaMemcpyHostToDevice, e->stream),
           "params");
-    run_stage(e->model(0), stage, e->stream);
+    // Stage replay compares every field, so the fused transforms also write
+    // the Fourier fields they pass through.
+    Model m = e->model(0);
+    m.keep_fourier = 1;
+    run_stage(m, stage, e->stream);
     check(cudaGetLastError(), "stage launch");
     check(cudaStreamSynchronize(e->stream), "stage");
   });
@@ -1152,6 +1147,10 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
     } else if (k == "legendre_forward") {
       launch = [&] { tr_legendre_forward(m, F.fgtdt, F.zstt1, LP, m.sh.qc, e->stream); };
       b = LP * (four + spec);
+    } else if (k == "sp2gp") {
+      // fused sp2fc + fc2gp: the spectral plane in, the grid plane out
+      launch = [&] { tr_sp2gp(m, F.st, F.fgt, F.gt, LP, m.sh.qi, e->stream); };
+      b = LP * (spec + grid);
     } else if (k == "legendre_inverse") {
       launch = [&] { tr_legendre_inverse(m, F.st, F.fgt, LP, m.sh.qi, e->stream); };
       b = LP * (spec + four);

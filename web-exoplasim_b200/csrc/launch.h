@@ -15,6 +15,9 @@ void tr_fourier_forward(const Model& m, const float* g, float* c, int planes, cu
 void tr_fourier_inverse(const Model& m, const float* c, float* g, int planes, cudaStream_t st);
 void tr_dlambda(const Model& m, const float* a, float* b, int planes, cudaStream_t st);
 void tr_legendre_inverse(const Model& m, const float* s, float* f, int planes, const float* q, cudaStream_t st);
+// sp2fc then fc2gp of one field: f is the Fourier field between them (on the
+// optimized path written only when m.keep_fourier), g the grid field.
+void tr_sp2gp(const Model& m, const float* s, float* f, float* g, int planes, const float* q, cudaStream_t st);
 void tr_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V, int planes, float plavor,
               cudaStream_t st);
 void tr_legendre_forward(const Model& m, const float* f, float* s, int planes, const float* q, cudaStream_t st);
@@ -47,6 +50,8 @@ void tc_inverse(const Model& m, const float* s, float* f, int planes, bool deriv
 
 // fft.cu (optimized path; Fourier planes m-major)
 void fft_init();
+void grid_init();
+void grid_sp2gp(const Model& m, const float* s, float* f, float* g, int planes, bool derivative, cudaStream_t st);
 size_t fft_chunk_smem(const Dims& d, int rows);
 bool fft_rows_supported(const Dims& d, int rows);
 void fft_forward(const Model& m, const float* g, float* c, int planes, cudaStream_t st);

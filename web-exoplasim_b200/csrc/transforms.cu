@@ -329,6 +329,7 @@ void tr_init() {
   leg_init();
   tc_init();
   fft_init();
+  grid_init();
   allow_smem(k_dft_forward);
   allow_smem(k_dft_inverse);
   allow_smem(k_leg_inverse);
@@ -362,6 +363,12 @@ void tr_dlambda(const Model& m, const float* a, float* b, int planes, cudaStream
     return;
   }
   k_dlambda<<<(n + 255) / 256, 256, 0, st>>>(a, b, n, m.d.NTP1, m.d.NFC);
+}
+
+void tr_sp2gp(const Model& m, const float* s, float* f, float* g, int planes, const float* q, cudaStream_t st) {
+  if (m.mode == 1 && (q == m.sh.qi || q == m.sh.qj)) return grid_sp2gp(m, s, f, g, planes, q == m.sh.qj, st);
+  tr_legendre_inverse(m, s, f, planes, q, st);
+  tr_fourier_inverse(m, f, g, planes, st);
 }
 
 void tr_legendre_inverse(const Model& m, const float* s, float* f, int planes, const float* q,
