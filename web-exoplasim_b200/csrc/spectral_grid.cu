@@ -5,8 +5,11 @@
 // round trip through HBM.
 //
 // A block owns JR = 8 latitude pairs (16 rows of every plane) and walks a
-// range of planes two at a time. Its slice of the transposed northern table
-// ([mode][pair], padded to JR + 1) is staged once. Per plane pair:
+// range of planes two at a time. Its slice of the northern table is staged
+// once, pair-major ([pair][mode]): a row pitch of 4 (mod 32) banks and each
+// wavenumber's modes starting at a position of residue u (mod 4), for the
+// wavenumber pair u that reads them, put the 32 lanes of a warp (8 pairs x 4
+// wavenumber pairs) on 32 distinct banks. Per plane pair:
 //  1. Legendre: thread (wavenumber pair u, latitude pair jj) sums the modes of
 //     wavenumbers u and NTP1 - 1 - u for both planes: even-(n-m) and
 //     odd-(n-m) partial sums E, O in the order of the unfused latitude-pair
@@ -48,7 +51,8 @@ struct GridShape {
   static constexpr int THREADS = FROWS * T;
   static constexpr int GROUPS = (NTP1 + 1) / 2;
   static constexpr int TASKS = GROUPS * JR;
-  static constexpr int TR = JR + 1;       // padded table row
+  static constexpr int TL = NCSP + 3 * NTP1;                       // table row: modes plus alignment gaps
+  static constexpr int TP = TL + (((4 - TL) % 32) + 32) % 32;      // row pitch, 4 (mod 32)
   static constexpr int PITCH = (ROWS + (((16 / T - ROWS) % 16) + 16) % 16);
   static constexpr int FC = NTP1 * PITCH;  // float2s of one plane's coefficient stage
   static constexpr int SPEC = NCSP;        // float4s of the spectral stage (two planes)
@@ -57,7 +61,8 @@ struct GridShape {
   static constexpr int R = (NCSP + THREADS - 1) / THREADS;        // spectral float4s per thread
   static_assert((N + 9 * Q + PP * FC) % 2 == 0, "the spectral stage must start 16-byte aligned");
   static size_t smem() {
-    return ((size_t)N + 9 * Q + (size_t)PP * FC + SHARED) * sizeof(float2) + (size_t)NCSP * TR * sizeof(float);
+    return ((size_t)N + 9 * Q + (size_t)PP * FC + SHARED) * sizeof(float2) + (size_t)JR * TP * sizeof(float) +
+           (size_t)NTP1 * sizeof(int);
   }
 };
 
@@ -72,9 +77,10 @@ __device__ __forceinline__ int stage_lat(int rr, int j0) {
 template <int Q>
 __global__ void __launch_bounds__(GridShape<Q>::THREADS)
     k_sp2gp(const float* __restrict__ s, float* __restrict__ f, float* __restrict__ g, int planes, int per_block,
-            const float* __restrict__ qT, const float2* __restrict__ twg, int odd, int keep) {
+            const float* __restrict__ qT, const int* __restrict__ mode_m, const float2* __restrict__ twg, int odd,
+            int keep) {
   using G = GridShape<Q>;
-  constexpr int T = G::T, M = G::M, N = G::N, NTP1 = G::NTP1, JR = G::JR, JH = G::JH, TR = G::TR;
+  constexpr int T = G::T, M = G::M, N = G::N, NTP1 = G::NTP1, JR = G::JR, JH = G::JH, TP = G::TP;
   constexpr int NLAT = G::NLAT, ROWS = G::ROWS, PITCH = G::PITCH, NCSP = G::NCSP, R = G::R;
   constexpr size_t SPLANE = 2 * (size_t)NCSP;              // floats of a spectral plane (NRSP)
   constexpr size_t FPLANE = (size_t)NLAT * 2 * NTP1;       // floats of a Fourier plane
@@ -86,7 +92,8 @@ __global__ void __launch_bounds__(GridShape<Q>::THREADS)
   float2* shared = fc + G::PP * G::FC;    // spectral stage [NCSP] float4, or the FFT exchange rows
   float4* spec = reinterpret_cast<float4*>(shared);
   float2* xb = shared;
-  float* tab = reinterpret_cast<float*>(shared + G::SHARED);  // [NCSP][TR]
+  float* tab = reinterpret_cast<float*>(shared + G::SHARED);  // [JR][TP]
+  int* tpos = reinterpret_cast<int*>(tab + JR * TP);           // [NTP1] first position of m's modes
   const int chunks = JH / JR;
   const int j0 = (blockIdx.x % chunks) * JR;
   const int pbeg = (blockIdx.x / chunks) * per_block;
@@ -120,9 +127,21 @@ __global__ void __launch_bounds__(GridShape<Q>::THREADS)
 
   if (pbeg < pend) fetch(pbeg);
   load_twiddles<Q>(twg, tw, twq);
+  if (threadIdx.x == 0) {
+    // m is read by wavenumber pair u = m (m < GROUPS) or u = NTP1 - 1 - m
+    int at = 0;
+    for (int m = 0; m < NTP1; ++m) {
+      const int u = m < G::GROUPS ? m : NTP1 - 1 - m;
+      at += ((u - at) % 4 + 4) % 4;
+      tpos[m] = at;
+      at += NTP1 - m;
+    }
+  }
+  __syncthreads();
   for (int i = threadIdx.x; i < NCSP * JR; i += G::THREADS) {
     const int w = i / JR, jj = i - w * JR;
-    tab[w * TR + jj] = qT[(size_t)w * JH + j0 + jj];
+    const int m = mode_m[w];
+    tab[jj * TP + tpos[m] + (w - mode_start(m, NTP1))] = qT[(size_t)w * JH + j0 + jj];
   }
   store();
   __syncthreads();
@@ -141,12 +160,13 @@ __global__ void __launch_bounds__(GridShape<Q>::THREADS)
         const int m = side == 0 ? u : NTP1 - 1 - u;
         if (side == 1 && m == u) break;
         const int w0 = mode_start(m, NTP1), K = NTP1 - m;
-        const float* qc = tab + w0 * TR + jj;
+        const float* qc = tab + jj * TP + tpos[m];
         const float4* sc = spec + w0;
         float4 e = make_float4(0.f, 0.f, 0.f, 0.f), o = e;  // (re a, im a, re b, im b)
         int k = 0;
+#pragma unroll 2
         for (; k + 1 < K; k += 2) {
-          const float qe = qc[k * TR], qo = qc[(k + 1) * TR];
+          const float qe = qc[k], qo = qc[k + 1];
           const float4 ve = sc[k], vo = sc[k + 1];
           e.x = fmaf(qe, ve.x, e.x);
           e.y = fmaf(qe, ve.y, e.y);
@@ -158,7 +178,7 @@ __global__ void __launch_bounds__(GridShape<Q>::THREADS)
           o.w = fmaf(qo, vo.w, o.w);
         }
         if (k < K) {
-          const float qe = qc[k * TR];
+          const float qe = qc[k];
           const float4 ve = sc[k];
           e.x = fmaf(qe, ve.x, e.x);
           e.y = fmaf(qe, ve.y, e.y);
@@ -228,7 +248,7 @@ void launch_sp2gp(const Model& m, const float* s, float* f, float* g, int planes
   const int splits = std::max(1, std::min(pairs, (target + chunks - 1) / chunks));
   const int per_pairs = (pairs + splits - 1) / splits;
   const int blocks = chunks * ((pairs + per_pairs - 1) / per_pairs);
-  k_sp2gp<Q><<<blocks, G::THREADS, smem, st>>>(s, f, g, planes, 2 * per_pairs, qT,
+  k_sp2gp<Q><<<blocks, G::THREADS, smem, st>>>(s, f, g, planes, 2 * per_pairs, qT, m.sh.mode_m,
                                                 reinterpret_cast<const float2*>(m.sh.tw), odd, m.keep_fourier);
 }
 
