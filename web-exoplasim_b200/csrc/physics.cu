@@ -484,19 +484,21 @@ __device__ __forceinline__ void swr_band(const Model& m, const PlanetConst& K, c
   const float* sg = tb + m.to.sigma;
   const float dp = F.dp[c];
   const float zm = 35.f / sqrtf(1.f + 1224.f * mu0 * mu0);
-  auto amount_at = [&](int l) {
-    const float dsigma = ds[l];
-    return BAND == 0 ? ZFO3 * dsigma * dp * F.dqo3[l * SN + c] / K.GA
-                     : 0.1f * dsigma * F.dq[l * SN + c] * dp / K.GA * sqrtf(273.f / F.dt[l * SN + c]) * sg[l] * dp /
-                           100000.f;
+  // The absorber amount of level l from its loaded inputs (BAND 0: ozone;
+  // BAND 1: water vapour q and temperature t).
+  auto amount_of = [&](float dsigma, float q, float t, float sgl) {
+    return BAND == 0 ? ZFO3 * dsigma * dp * q / K.GA
+                     : 0.1f * dsigma * q * dp / K.GA * sqrtf(273.f / t) * sgl * dp / 100000.f;
   };
+  auto absorber = [&](int l) { return BAND == 0 ? F.dqo3[l * SN + c] : F.dq[l * SN + c]; };
+  auto amount_at = [&](int l) { return amount_of(ds[l], absorber(l), BAND == 0 ? 0.f : F.dt[l * SN + c], sg[l]); };
   auto absorption = [&](float x) {
     return BAND == 0 ? ozone_absorption(x, K.ZSOLAR1) : vapour_absorption(x, K.ZSOLAR2);
   };
   // Column totals of the absorber path (slant above the first cloud,
   // diffuse below).
   float pt = 0.f, xpt = 0.f, cs = 1.f;
-#pragma unroll 1
+#pragma unroll
   for (int l = 0; l < NL; ++l) {
     const float amount = amount_at(l);
     pt = pt + amount;
@@ -517,12 +519,26 @@ __device__ __forceinline__ void swr_band(const Model& m, const PlanetConst& K, c
   float tt = 1.f, ttu = 1.f - absorption(xpt + diffusivity * pt);
   float pl = 0.f, xpl = 0.f;
   cs = 1.f;
+  // Level l + 1's global inputs are loaded while level l is computed (the
+  // loop stays rolled to keep the cloud optics small in the instruction
+  // cache).
+  float cc_n = F.dcc[c], ql_n = F.dql[c], q_n = absorber(0), t_n = BAND == 0 ? 0.f : F.dt[c], ds_n = ds[0],
+        sg_n = sg[0];
 #pragma unroll 1
   for (int l = 0; l < NL; ++l) {
-    const float cc = F.dcc[l * SN + c];
+    const float cc = cc_n, ql = ql_n, ql_q = q_n, ql_t = t_n, dsl = ds_n, sgl = sg_n;
+    if (l + 1 < NL) {
+      const size_t at = (l + 1) * SN + c;
+      cc_n = F.dcc[at];
+      ql_n = F.dql[at];
+      q_n = absorber(l + 1);
+      t_n = BAND == 0 ? 0.f : F.dt[at];
+      ds_n = ds[l + 1];
+      sg_n = sg[l + 1];
+    }
     float rcl = 0.f, rcls = 0.f, tcl = 1.f, tcls = 1.f;
     if (cc > 0.f) {
-      const float lwp = fminf(1000.f, 1000.f * F.dql[l * SN + c] * dp / K.GA * ds[l]);
+      const float lwp = fminf(1000.f, 1000.f * ql * dp / K.GA * dsl);
       const float tau = 2.f * fpow(logf(lwp + 1.5f) * INV_LN10, 3.9f);
       if (BAND == 0) {
         rcls = 1.f - 1.f / (1.f + K.ZB3 * tau);
@@ -553,7 +569,7 @@ __device__ __forceinline__ void swr_band(const Model& m, const PlanetConst& K, c
         rcl = cs * direct2 + (1.f - cs) * rcls;
       }
     }
-    const float amount = amount_at(l);
+    const float amount = amount_of(dsl, ql_q, ql_t, sgl);
     pl = pl + amount;
     xpl = cs * (xpl + zm * amount) + (1.f - cs) * (xpl + diffusivity * amount);
     cs = cs * (1.f - cc);
