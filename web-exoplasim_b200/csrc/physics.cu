@@ -22,6 +22,10 @@ namespace {
 
 constexpr int kBlock = 128;
 
+// Column kernels take the planet constants and per-planet tables as
+// __restrict__ parameters: both are read-only during a launch, so the
+// compiler may keep their values across the kernel's stores to fields
+// instead of reloading them after every store.
 #define COLUMN_PROLOGUE                                              \
   const Dims& d = m.d;                                               \
   const int c = blockIdx.x * blockDim.x + threadIdx.x;               \
@@ -30,8 +34,8 @@ constexpr int kBlock = 128;
   const int h = c % d.NHOR;                                          \
   const StepParams& P = m.params[slot];                              \
   if (!P.active) return;                                             \
-  const PlanetConst& K = m.pc[slot];                                 \
-  const float* tb = m.tabs + (size_t)slot * m.to.stride;             \
+  const PlanetConst& K = pcr[slot];                                  \
+  const float* tb = tabr + (size_t)slot * m.to.stride;               \
   const size_t SN = (size_t)d.S * d.NHOR;                            \
   const FieldPtrs& F = m.f;                                          \
   (void)h; (void)K; (void)tb; (void)SN; (void)F; (void)P;
@@ -46,12 +50,12 @@ constexpr int kBlock = 128;
   const StepParams& P = m.params[slot];                              \
   if (!P.active) return;                                             \
   __shared__ PlanetConst s_planet;                                   \
-  stage_planet(m.pc + slot, &s_planet);                              \
+  stage_planet(pcr + slot, &s_planet);                               \
   const PlanetConst& K = s_planet;                                   \
   const int c = blockIdx.x * kBlock + threadIdx.x;                   \
   if (c >= d.S * d.NHOR) return;                                     \
   const int h = c - slot * d.NHOR;                                   \
-  const float* tb = m.tabs + (size_t)slot * m.to.stride;             \
+  const float* tb = tabr + (size_t)slot * m.to.stride;               \
   const size_t SN = (size_t)d.S * d.NHOR;                            \
   const FieldPtrs& F = m.f;                                          \
   (void)h; (void)K; (void)tb; (void)SN; (void)F; (void)P;
@@ -94,7 +98,7 @@ __device__ __forceinline__ float powi(float x, int n) {
 // ---------------------------------------------------------------- fixer
 // physics/fixer/wgsl/column.wgsl: fix0d per column.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_fixer_column(Model m) {
+__global__ void __launch_bounds__(kBlock) k_fixer_column(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const float* ds = tb + m.to.dsigma;
   float negative = 0.f, positive = 0.f;
@@ -188,7 +192,7 @@ __global__ void __launch_bounds__(kSumThreads) k_slot_sums(Model m, const float*
 
 // physics/fixer/wgsl/apply.wgsl: the global step, gqdt and the new dq.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_fixer_apply(Model m) {
+__global__ void __launch_bounds__(kBlock) k_fixer_apply(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const double zzneg = m.sums[slot * 4], zzpos = m.sums[slot * 4 + 1];
   const float scale = zzneg > 0.0 ? (float)((zzpos - zzneg) / zzpos) : 1.f;
@@ -206,7 +210,7 @@ __global__ void __launch_bounds__(kBlock) k_fixer_apply(Model m) {
 // physics/surface-flux/wgsl/surflx.wgsl: transfer coefficients, implicit
 // stress, sensible heat and evaporation.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_surflx(Model m) {
+__global__ void __launch_bounds__(kBlock) k_surflx(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const int low = NL - 1;
   const size_t lo = low * SN + c, sf = NL * SN + c;
@@ -320,7 +324,7 @@ __device__ __forceinline__ void diffuse_potential(const float* ds, float* x, con
 
 // physics/surface-flux/wgsl/vdiff.wgsl: Richardson-number vertical diffusion.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_vdiff(Model m) {
+__global__ void __launch_bounds__(kBlock) k_vdiff(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const float* ds = tb + m.to.dsigma;
   const float* sh = tb + m.to.sigmah;
@@ -420,7 +424,7 @@ constexpr float kTWOPI = kPI + kPI;
 
 // solang (physics/radiation/wgsl/solang.wgsl) and mko3 (mko3.wgsl) for one column.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_solang_mko3(Model m) {
+__global__ void __launch_bounds__(kBlock) k_solang_mko3(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const int lat = h / d.NLON, lon = h % d.NLON;
   float hangle = P.rad[2] + (float)lon * K.ZRLON - kPI;
@@ -697,7 +701,7 @@ __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
 template <int NL>
 // Six blocks per SM (at most 85 registers, no spills): the kernel is latency-bound,
 // and residency hides the field loads at either end of the O(L^2) rows.
-__global__ void __launch_bounds__(kBlock, 6) k_lwr_radstep(Model m) {
+__global__ void __launch_bounds__(kBlock, 6) k_lwr_radstep(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE_STAGED
   const int NP = NL + 1;
   const float ZERO = 1.0e-6f, ZFH2O = 0.1f, ZFO3 = 100.f / 2.14f;
@@ -912,7 +916,7 @@ __device__ __forceinline__ Parcel condense(const PlanetConst& K, float t0, float
 // mkdqtgp scaling, kuo and mkshallow (physics/precipitation/wgsl/kuo.wgsl).
 // Six resident blocks per SM (latency-bound; measured faster than four).
 template <int NL>
-__global__ void __launch_bounds__(kBlock, 6) k_kuo(Model m) {
+__global__ void __launch_bounds__(kBlock, 6) k_kuo(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const int NM = NL - 1;
   const float* ds = tb + m.to.dsigma;
@@ -1121,7 +1125,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_kuo(Model m) {
 
 // mkdca (physics/precipitation/wgsl/mkdca.wgsl): dry convective adjustment.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_mkdca(Model m) {
+__global__ void __launch_bounds__(kBlock) k_mkdca(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const int NM = NL - 1;
   const float D2 = P.deltsec2;
@@ -1214,7 +1218,9 @@ __global__ void __launch_bounds__(kSumThreads) k_mkdca_limit(Model m) {
 
 // column.wgsl: mkdca's adjustment (unless skipped), mklsp, mkrain, mkclouds.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_rain_column(Model m) {
+// Its parameters carry no __restrict__: with it the compiler keeps more
+// values in registers (165), and the lower occupancy measured slower.
+__global__ void __launch_bounds__(kBlock) k_rain_column(Model m, const PlanetConst* pcr, const float* tabr) {
   COLUMN_PROLOGUE
   const float* ds = tb + m.to.dsigma;
   const float* sg = tb + m.to.sigma;
@@ -1430,7 +1436,7 @@ __device__ __forceinline__ float surface_temperature(const PlanetConst& K, float
 
 // landmod's soilstep (physics/land/wgsl/soil.wgsl): tands, mktsoil, wandr.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_soil(Model m) {
+__global__ void __launch_bounds__(kBlock) k_soil(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const float DS = P.deltsec;
   const float dls = F.dls[c];
@@ -1586,7 +1592,7 @@ __device__ __forceinline__ float clim14(const float* f, const float* w3, int c, 
 // Land surface after mkradv (physics/land/wgsl/surface.wgsl) with vegstep
 // (vegetation/wgsl/vegstep.wgsl) and glacierstep (glacier/wgsl/glacierstep.wgsl).
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_land_surface(Model m) {
+__global__ void __launch_bounds__(kBlock) k_land_surface(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const float DS = P.deltsec;
   const float dls = F.dls[c];
@@ -1724,7 +1730,7 @@ __global__ void __launch_bounds__(kBlock) k_land_surface(Model m) {
 
 // seastep coupling and icestep up to getiflx (physics/sea-ice/wgsl/ice.wgsl).
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_sea_ice(Model m) {
+__global__ void __launch_bounds__(kBlock) k_sea_ice(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   if (P.coupled == 0.f) return;
   const bool sea = F.dls[c] < 0.5f;
@@ -1863,7 +1869,7 @@ __global__ void __launch_bounds__(kBlock) k_sea_ice(Model m) {
 // seastep (physics/sea/wgsl/seastep.wgsl) with ice_finish (sea-ice/wgsl/finish.wgsl)
 // and oceanstep (ocean/wgsl/oceanstep.wgsl).
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_sea(Model m) {
+__global__ void __launch_bounds__(kBlock) k_sea(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const bool coupled = P.coupled != 0.f;
   if (coupled) {
@@ -1951,7 +1957,7 @@ __global__ void __launch_bounds__(kBlock) k_sea(Model m) {
 
 // carbonstep (physics/carbon/wgsl/carbonstep.wgsl).
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_carbon(Model m) {
+__global__ void __launch_bounds__(kBlock) k_carbon(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const float precip = (F.dprc[c] + F.dprl[c]) * 3.154e9f;
   F.localprecip[c] = precip;
@@ -1976,7 +1982,7 @@ __global__ void __launch_bounds__(kBlock) k_carbon(Model m) {
 
 // snapshot/wgsl/pack.wgsl: the published fields, window extrema, RH.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_pack(Model m) {
+__global__ void __launch_bounds__(kBlock) k_pack(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const int step = (int)P.snap[0], window = (int)P.snap[1];
   const float t = F.dt[NL * SN + c];
@@ -2107,7 +2113,7 @@ void by_levels(int L, A&&... a) {
   template <int NL>                                                                        \
   struct name {                                                                            \
     static void run(const Model& m, cudaStream_t st) {                                     \
-      kernel<NL><<<nblocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);         \
+      kernel<NL><<<nblocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m, m.pc, m.tabs); \
     }                                                                                      \
   };
 
