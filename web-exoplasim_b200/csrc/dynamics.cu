@@ -244,29 +244,54 @@ __global__ void __launch_bounds__(kBlock, 5) k_spectrala(Model m) {
   F.spp[c] = sppNew;
   F.sp[c] = sppNew;
   F.spt[c] = spt;
+  // The last pass runs in two halves of levels, each reading all its inputs
+  // before its stores: the fields are distinct arrays, but the compiler
+  // cannot prove it and would otherwise wait for each level's loads in turn.
+  constexpr int H = (NL + 1) / 2;
+  const float PNU21 = K.PNU21, PNU = K.PNU;
 #pragma unroll
-  for (int l = 0; l < NL; ++l) {
-    const size_t at = l * SR + c;
-    if (filter) {
-      F.sdm[at] = K.PNU21 * F.sdp[at] + K.PNU * adm[l];
-      F.szm[at] = K.PNU21 * F.szp[at] + K.PNU * azm[l];
-      F.stm[at] = K.PNU21 * F.stp[at] + K.PNU * atm[l];
-      F.sqm[at] = K.PNU21 * F.sqp[at] + K.PNU * aqm[l];
+  for (int h0 = 0; h0 < NL; h0 += H) {
+    float szt_[H], sqt_[H], sdp_[H], szp_[H], stp_[H], sqp_[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+      const int l = h0 + i;
+      if (l >= NL) break;
+      const size_t at = l * SR + c;
+      szt_[i] = F.szt[at];
+      sqt_[i] = F.sqt[at];
+      if (filter) {
+        sdp_[i] = F.sdp[at];
+        szp_[i] = F.szp[at];
+        stp_[i] = F.stp[at];
+        sqp_[i] = F.sqp[at];
+      }
     }
-    const float sdp = 2.f * sdt[l] - adm[l];
-    const float stp = DELT2 * stt[l] + atm[l];
-    const float szp = DELT2 * F.szt[at] + azm[l];
-    const float sqp = DELT2 * F.sqt[at] + aqm[l];
-    F.sdt[at] = sdt[l];
-    F.stt[at] = stt[l];
-    F.sdp[at] = sdp;
-    F.stp[at] = stp;
-    F.szp[at] = szp;
-    F.sqp[at] = sqp;
-    F.sd[at] = sdp;
-    F.st[at] = stp;
-    F.sz[at] = szp;
-    F.sq[at] = sqp;
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+      const int l = h0 + i;
+      if (l >= NL) break;
+      const size_t at = l * SR + c;
+      if (filter) {
+        F.sdm[at] = PNU21 * sdp_[i] + PNU * adm[l];
+        F.szm[at] = PNU21 * szp_[i] + PNU * azm[l];
+        F.stm[at] = PNU21 * stp_[i] + PNU * atm[l];
+        F.sqm[at] = PNU21 * sqp_[i] + PNU * aqm[l];
+      }
+      const float sdp = 2.f * sdt[l] - adm[l];
+      const float stp = DELT2 * stt[l] + atm[l];
+      const float szp = DELT2 * szt_[i] + azm[l];
+      const float sqp = DELT2 * sqt_[i] + aqm[l];
+      F.sdt[at] = sdt[l];
+      F.stt[at] = stt[l];
+      F.sdp[at] = sdp;
+      F.stp[at] = stp;
+      F.szp[at] = szp;
+      F.sqp[at] = sqp;
+      F.sd[at] = sdp;
+      F.st[at] = stp;
+      F.sz[at] = szp;
+      F.sq[at] = sqp;
+    }
   }
 }
 
