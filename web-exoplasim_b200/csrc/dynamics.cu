@@ -61,8 +61,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_calcgp(Model m) {
   const size_t SN = (size_t)d.S * d.NHOR;
   const FieldPtrs& F = m.f;
   const float rcsq = m.sh.rcsq[c % d.NHOR];
+  // gp = exp(gp) is stored with the first tendencies below, after every
+  // load: a store here would hold back the loads that follow it.
   const float ps = expf(F.gp[c]);
-  F.gp[c] = ps;
   const float gpm = F.gpmt[c], gpj = F.gpj[c];
   float gu[NL], gv[NL], gt[NL], gd[NL], gz[NL], gq[NL], zvgpg[NL], ztv1[NL], ztv2[NL];
 #pragma unroll
@@ -105,6 +106,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_calcgp(Model m) {
   // Level tendencies go out as soon as they are formed (fewer live arrays).
   zsumd = zvgpg[0] * ds[0];
   const float rdsig0 = rd[0];
+  F.gp[c] = ps;
   F.gtn[c] = gt[0] * gd[0] - K.AKAP * ztv2[0] * gd[0] - rdsig0 * (gtd[0] + t01[0] * (sh[0] * gvp - zsumd));
   F.gqn[c] = -rdsig0 * gqm[0];
   F.guz[c] = -gu[0] * gz[0] - gpj * ztv1[0] - rdsig0 * gvd[0];
