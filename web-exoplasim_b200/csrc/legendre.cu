@@ -115,8 +115,12 @@ __global__ void k_sym_inverse(const float* __restrict__ s0, const float* __restr
       for (int p = threadIdx.x; p < np; p += blockDim.x) ss[((size_t)nt + (1 - w0)) * tile + p].x -= plavor;
       __syncthreads();
     }
+    // A thread owns pair j and PPT consecutive planes of the tile (2 for
+    // sp2fc; 4 for dv2uv, whose 16 multiply-adds per term and plane pair
+    // otherwise leave the loads a third of the issued instructions).
+    constexpr int PPT = KIND == 0 ? 2 : 4;
     const int j = threadIdx.x % JH;
-    const int pa = 2 * (threadIdx.x / JH);  // planes pa, pa + 1 of the tile
+    const int pa = PPT * (threadIdx.x / JH);
     const int south = d.NLAT - 1 - j;
     const bool has_a = pa < np, has_b = pa + 1 < np;
     float2* outa0 = reinterpret_cast<float2*>(f0 + (size_t)(p0 + pa) * plane_floats);
@@ -166,13 +170,19 @@ __global__ void k_sym_inverse(const float* __restrict__ s0, const float* __restr
         // Term t's contribution to u and v: a(t) * (dim, -dre, zim, -zre)
         // + b(t) * (zre, zim, -dre, -dim); the even-t a part and odd-t b
         // part go to X, the rest to Y: north = X + Y, south = X - Y.
-        float X[2][4] = {}, Y[2][4] = {};
+        float X[PPT][4] = {}, Y[PPT][4] = {};
         auto add = [&](float (*acc_a)[4], float (*acc_b)[4], float a, float b, int t) {
-          const float4 D = sc[t * step4], Z = zc[t * step4];
-          const float2 Dp[2] = {make_float2(D.x, D.y), make_float2(D.z, D.w)};
-          const float2 Zp[2] = {make_float2(Z.x, Z.y), make_float2(Z.z, Z.w)};
+          float2 Dp[PPT], Zp[PPT];
 #pragma unroll
-          for (int pp = 0; pp < 2; ++pp) {
+          for (int h = 0; h < PPT / 2; ++h) {
+            const float4 D = sc[t * step4 + h], Z = zc[t * step4 + h];
+            Dp[2 * h] = make_float2(D.x, D.y);
+            Dp[2 * h + 1] = make_float2(D.z, D.w);
+            Zp[2 * h] = make_float2(Z.x, Z.y);
+            Zp[2 * h + 1] = make_float2(Z.z, Z.w);
+          }
+#pragma unroll
+          for (int pp = 0; pp < PPT; ++pp) {
             acc_a[pp][0] = fmaf(a, Dp[pp].y, acc_a[pp][0]);
             acc_a[pp][1] = fmaf(-a, Dp[pp].x, acc_a[pp][1]);
             acc_a[pp][2] = fmaf(a, Zp[pp].y, acc_a[pp][2]);
@@ -189,19 +199,15 @@ __global__ void k_sym_inverse(const float* __restrict__ s0, const float* __restr
           add(Y, X, qc[(t + 1) * JH], qd[(t + 1) * JH], t + 1);
         }
         if (t < K) add(X, Y, qc[t * JH], qd[t * JH], t);
-        float2* outa1 = reinterpret_cast<float2*>(f1 + (size_t)(p0 + pa) * plane_floats);
-        float2* outb1 = outa1 + plane_floats / 2;
-        if (has_a) {
-          outa0[rn] = make_float2(X[0][0] + Y[0][0], X[0][1] + Y[0][1]);
-          outa0[rs] = make_float2(X[0][0] - Y[0][0], X[0][1] - Y[0][1]);
-          outa1[rn] = make_float2(X[0][2] + Y[0][2], X[0][3] + Y[0][3]);
-          outa1[rs] = make_float2(X[0][2] - Y[0][2], X[0][3] - Y[0][3]);
-        }
-        if (has_b) {
-          outb0[rn] = make_float2(X[1][0] + Y[1][0], X[1][1] + Y[1][1]);
-          outb0[rs] = make_float2(X[1][0] - Y[1][0], X[1][1] - Y[1][1]);
-          outb1[rn] = make_float2(X[1][2] + Y[1][2], X[1][3] + Y[1][3]);
-          outb1[rs] = make_float2(X[1][2] - Y[1][2], X[1][3] - Y[1][3]);
+#pragma unroll
+        for (int pp = 0; pp < PPT; ++pp) {
+          if (pa + pp >= np) break;
+          float2* u = reinterpret_cast<float2*>(f0 + (size_t)(p0 + pa + pp) * plane_floats);
+          float2* v = reinterpret_cast<float2*>(f1 + (size_t)(p0 + pa + pp) * plane_floats);
+          u[rn] = make_float2(X[pp][0] + Y[pp][0], X[pp][1] + Y[pp][1]);
+          u[rs] = make_float2(X[pp][0] - Y[pp][0], X[pp][1] - Y[pp][1]);
+          v[rn] = make_float2(X[pp][2] + Y[pp][2], X[pp][3] + Y[pp][3]);
+          v[rs] = make_float2(X[pp][2] - Y[pp][2], X[pp][3] - Y[pp][3]);
         }
       }
     }
@@ -503,7 +509,7 @@ void launch_inverse(const Model& m, const float* s0, const float* s1, float* f0,
                     const float* qa, const float* qb, int odd, float plavor, cudaStream_t st) {
   const int nin = KIND == 0 ? 1 : 2;
   const int group = m.tune.inv_group[KIND], tile = m.tune.inv_tile[KIND];
-  const int threads = (m.d.NLAT / 2) * tile / 2;
+  const int threads = (m.d.NLAT / 2) * tile / (KIND == 0 ? 2 : 4);
   const size_t smem = inverse_smem(m.d, nin, group, tile);
   const int items = ((m.d.NTP1 + group - 1) / group) * ((planes + tile - 1) / tile);
   const int grid = std::min(items, persistent_grid((const void*)k_sym_inverse<KIND>, threads, smem));
