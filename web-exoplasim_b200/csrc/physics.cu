@@ -855,6 +855,17 @@ __global__ void __launch_bounds__(kBlock, 6) k_lwr_radstep(Model m, const Planet
   const float reflected = (1.f - eps) * dftd[NL];
 #pragma unroll
   for (int l = 0; l < NL; ++l) dftu[l] = dftu[l] - tausf[l] * reflected;
+  // radstep's inputs are read before the first store (the compiler cannot
+  // prove the fields distinct and would otherwise wait for each in turn).
+  float sw[NL + 1], tl[NL], ql[NL], dtdt[NL];
+#pragma unroll
+  for (int l = 0; l < NP; ++l) sw[l] = F.dswfl[l * SN + c];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    tl[l] = F.dt[l * SN + c];
+    ql[l] = F.dq[l * SN + c];
+    dtdt[l] = F.dtdt[l * SN + c];
+  }
   float lw[NL + 1], flux[NL + 1];
 #pragma unroll
   for (int l = 0; l < NP; ++l) {
@@ -864,10 +875,8 @@ __global__ void __launch_bounds__(kBlock, 6) k_lwr_radstep(Model m, const Planet
     F.dlwfl[l * SN + c] = lw[l];
   }
   // radstep
-  float sw[NL + 1];
 #pragma unroll
   for (int l = 0; l < NP; ++l) {
-    sw[l] = F.dswfl[l * SN + c];
     flux[l] = lw[l] + sw[l];
     F.dflux[l * SN + c] = flux[l];
   }
@@ -876,9 +885,9 @@ __global__ void __launch_bounds__(kBlock, 6) k_lwr_radstep(Model m, const Planet
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SN + c;
-    const float zdh = -F.dt[at] * K.GASCON / K.GA * lnsig[l];
-    const float den = ds[l] * dp * K.ACPD * (1.f + K.ADV * F.dq[at]);
-    F.dtdt[at] = F.dtdt[at] - K.GA * (flux[l + 1] - flux[l]) / den;
+    const float zdh = -tl[l] * K.GASCON / K.GA * lnsig[l];
+    const float den = ds[l] * dp * K.ACPD * (1.f + K.ADV * ql[l]);
+    F.dtdt[at] = dtdt[l] - K.GA * (flux[l + 1] - flux[l]) / den;
     F.dtdtswr[at] = -K.GA * (sw[l + 1] - sw[l]) / den;
     F.dtdtlwr[at] = -K.GA * (lw[l + 1] - lw[l]) / den;
     F.dconv[at] = (flux[l] - flux[l + 1]) / (zdh + 1.0e-9f);
