@@ -164,9 +164,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_calcgp(Model m) {
 
 // spectrala for one real spectral coefficient (dynamics/wgsl/spectrala.wgsl):
 // the Hoskins-Simmons semi-implicit scheme with this slot's bm1 for its phase.
-// Five resident blocks per SM (latency-bound; measured faster than four).
+// At least three resident blocks per SM: with its last pass read ahead, the
+// registers that a looser bound allows measured faster than five blocks.
 template <int NL>
-__global__ void __launch_bounds__(kBlock, 5) k_spectrala(Model m) {
+__global__ void __launch_bounds__(kBlock, 3) k_spectrala(Model m) {
   const Dims& d = m.d;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.S * d.NRSP) return;
