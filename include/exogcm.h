@@ -180,7 +180,8 @@ int exogcm_last_step_ms(exogcm_engine* engine, float* ms);
  * on the engine's stream), with the algorithmic bytes one launch moves in
  * *bytes. Kernels: "fourier_forward", "fourier_inverse" (FFTs on the
  * optimized path, DFTs on the plain one), "legendre_forward",
- * "legendre_inverse", "dv2uv", "uv2dv", "qtend", "calcgp", "spectrala",
+ * "legendre_inverse", "sp2gp" (the fused inverse Legendre transform and FFT
+ * of the optimized path), "dv2uv", "uv2dv", "qtend", "calcgp", "spectrala",
  * "mkdheat" (its first stage), "physics_in", "physics_out", and the single
  * column kernels "vdiff", "swr", "lwr_radstep", "kuo", "rain_column". The
  * launches change the state; use it for measurement only. */
