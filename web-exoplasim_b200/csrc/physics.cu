@@ -197,11 +197,22 @@ __global__ void __launch_bounds__(kBlock) k_fixer_apply(Model m, const PlanetCon
   const double zzneg = m.sums[slot * 4], zzpos = m.sums[slot * 4 + 1];
   const float scale = zzneg > 0.0 ? (float)((zzpos - zzneg) / zzpos) : 1.f;
   const float dp = F.dp[c];
+  // every level's inputs are read before the first store (the compiler
+  // cannot prove the fields distinct)
+  float fq[NL], gq[NL], dq[NL];
+#pragma unroll
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SN + c;
-    float q = F.fixq[at];
+    fq[l] = F.fixq[at];
+    gq[l] = F.gqdt[at];
+    dq[l] = F.dq[at];
+  }
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    float q = fq[l];
     if (zzneg > 0.0) q = fmaxf(q * scale, 0.f);
-    F.gqdt[at] = F.gqdt[at] + dp * (q - F.dq[at]) / P.delt2 / K.PSURF;
+    F.gqdt[at] = gq[l] + dp * (q - dq[l]) / P.delt2 / K.PSURF;
     F.dq[at] = q;
   }
 }
@@ -216,6 +227,10 @@ __global__ void __launch_bounds__(kBlock) k_surflx(Model m, const PlanetConst* _
   const size_t lo = low * SN + c, sf = NL * SN + c;
   const float u = F.du[lo], v = F.dv[lo], t = F.dt[lo], q = F.dq[lo], ts = F.dt[sf], qs = F.dq[sf];
   const float dp = F.dp[c], dls = F.dls[c];
+  // the tendencies and surface values used after the first store are read
+  // here (the compiler cannot prove the fields distinct)
+  const float dudt0 = F.dudt[lo], dvdt0 = F.dvdt[lo], dtdt0 = F.dtdt[lo], dqdt0 = F.dqdt[lo];
+  const float drhs = F.drhs[c], dwatc = F.dwatc[c], dz0 = F.dz0[c];
   const float dsigma = tb[m.to.dsigma + low];
   const float zfac = tb[m.to.flux_sigfac], zlnsig = tb[m.to.flux_lnsig];
   const float moisture = 1.f / K.RDBRV - 1.f;
@@ -224,7 +239,7 @@ __global__ void __launch_bounds__(kBlock) k_surflx(Model m, const PlanetConst* _
   float dtsa = t * zfac * (1.f + moisture * q);
   const float zabsu2 = fmaxf(K.ZUMIN, u * u + v * v);
   const float znl = -K.GASCON * 0.5f * (t + dtsa) * zlnsig / K.GA;
-  const float zbz0 = znl / F.dz0[c];
+  const float zbz0 = znl / dz0;
   const float zri = K.GA * znl / (zabsu2 * dtsa) * (dtsa - ts * (1.f + moisture * qs));
   const float zkblnz = VK / logf(zbz0 + 1.f);
   const float zkblnz2 = zkblnz * zkblnz;
@@ -251,9 +266,9 @@ __global__ void __launch_bounds__(kBlock) k_surflx(Model m, const PlanetConst* _
   const float zkonst2 = dsigma / D2 / K.GA;
   const float zkdiffm = zkonst1 * transm / ts;
   const float zun = u / (1.f + zkdiffm), zvn = v / (1.f + zkdiffm);
-  F.dudt[lo] = F.dudt[lo] + (zun - u) / D2;
-  F.dvdt[lo] = F.dvdt[lo] + (zvn - v) / D2;
-  float dtdt = F.dtdt[lo];
+  F.dudt[lo] = dudt0 + (zun - u) / D2;
+  F.dvdt[lo] = dvdt0 + (zvn - v) / D2;
+  float dtdt = dtdt0;
   if (K.NDHEAT != 0.f) dtdt = dtdt + -(zun * zun - u * u + zvn * zvn - v * v) / D2 * 0.5f / K.ACPD / (1.f + K.ADV * q);
   const float taux = dp * zkonst2 * zkdiffm * zun, tauy = dp * zkonst2 * zkdiffm * zvn;
   F.dtaux[c] = taux;
@@ -269,10 +284,10 @@ __global__ void __launch_bounds__(kBlock) k_surflx(Model m, const PlanetConst* _
   F.dshdt[c] = -1.f * zkonst2 * zkdiffh * dp * K.ACPD * moist;
   dtsa = ztn * zfac;
   F.dtsa[c] = dtsa;
-  const float zkdiffq = F.drhs[c] * zkonst1 * transh / ts;
+  const float zkdiffq = drhs * zkonst1 * transh / ts;
   float zqn = fmaxf(q, (q + zkdiffq * qs) / (1.f + zkdiffq));
-  if (dls > 0.f) zqn = fminf(zqn, F.dwatc[c] / P.deltsec * 1000.f / dp / zkonst2 + q);
-  F.dqdt[lo] = F.dqdt[lo] + (zqn - q) / D2;
+  if (dls > 0.f) zqn = fminf(zqn, dwatc / P.deltsec * 1000.f / dp / zkonst2 + q);
+  F.dqdt[lo] = dqdt0 + (zqn - q) / D2;
   const float devap = -dp * zkonst2 / 1000.f * (zqn - q);
   F.devap[c] = devap;
   const float latent = (ts > K.TMELT || dls < 0.5f) ? K.ALV : K.ALS;
@@ -441,8 +456,12 @@ __global__ void __launch_bounds__(kBlock) k_solang_mko3(Model m, const PlanetCon
   const float* ds = tb + m.to.dsigma;
   const float* lnsig = tb + m.to.rad_lnsig;
   float o3t = za, zh = 0.f;
+  float t[NL];  // read before the stores below (possible aliasing would order them)
+#pragma unroll
+  for (int l = 1; l < NL; ++l) t[l] = F.dt[l * SN + c];
+#pragma unroll
   for (int l = NL - 1; l >= 1; --l) {
-    zh = zh - F.dt[l * SN + c] * K.GASCON / K.GA * lnsig[l];
+    zh = zh - t[l] * K.GASCON / K.GA * lnsig[l];
     const float o3 = -(za + za * K.ZCONST) / (1.f + expf((zh - K.BO3) / K.CO3)) + o3t;
     F.dqo3[l * SN + c] = o3 * K.GA / (ZFO3 * ds[l] * dp);
     o3t = o3t - o3;
@@ -1970,25 +1989,32 @@ __global__ void __launch_bounds__(kBlock) k_sea(Model m, const PlanetConst* __re
 template <int NL>
 __global__ void __launch_bounds__(kBlock) k_carbon(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
+  // inputs first: the compiler cannot prove the fields distinct
   const float precip = (F.dprc[c] + F.dprl[c]) * 3.154e9f;
+  const float avgprecip = F.localavgprecip[c];
+  const bool carbon = P.carbon != 0.f;
+  const float tsurf = carbon ? F.dt[NL * SN + c] : 0.f;
+  const float dls = carbon ? F.dls[c] : 0.f, co2 = carbon ? F.co2[slot] : 0.f, dp = carbon ? F.dp[c] : 0.f;
+  const float avgtemps = carbon ? F.localavgtemps[c] : 0.f, avgweather = carbon ? F.localavgweather[c] : 0.f;
+  float local_weathering = carbon ? F.localweathering[c] : 0.f;
   F.localprecip[c] = precip;
-  F.localavgprecip[c] = F.localavgprecip[c] + precip * K.TIMEWEIGHT;
-  if (P.carbon == 0.f) return;
-  const float tsurf = F.dt[NL * SN + c];
+  F.localavgprecip[c] = avgprecip + precip * K.TIMEWEIGHT;
+  if (!carbon) return;
   if (K.NCARBON != 0.f) {
     float weathering = 0.f;
-    if (F.dls[c] > 0.5f && tsurf >= 273.15f) {
-      const float pco2 = F.co2[slot] * F.dp[c] * 1.0e-5f;
+    if (dls > 0.5f && tsurf >= 273.15f) {
+      const float pco2 = co2 * dp * 1.0e-5f;
       weathering = fpow(pco2 / K.CO2EARTH, K.BETA) * expf(K.KACT * (tsurf - 288.f)) * fpow(precip / K.PEARTH, 0.65f);
       if (K.NSUPPLY != 0.f) {
         const float wmaxp = fmaxf(K.WMAX / K.VEARTH, 2.0e-15f);
         weathering = wmaxp * (1.f - expf(-weathering / wmaxp));
       }
     }
-    F.localweathering[c] = weathering * (K.PLARAD * K.PLARAD) / (K.RAD_EARTHSQ * 0.29f);
+    local_weathering = weathering * (K.PLARAD * K.PLARAD) / (K.RAD_EARTHSQ * 0.29f);
+    F.localweathering[c] = local_weathering;
   }
-  F.localavgtemps[c] = F.localavgtemps[c] + tsurf * K.TIMEWEIGHT;
-  F.localavgweather[c] = F.localavgweather[c] + F.localweathering[c] * K.TIMEWEIGHT;
+  F.localavgtemps[c] = avgtemps + tsurf * K.TIMEWEIGHT;
+  F.localavgweather[c] = avgweather + local_weathering * K.TIMEWEIGHT;
 }
 
 // snapshot/wgsl/pack.wgsl: the published fields, window extrema, RH.
