@@ -1770,23 +1770,21 @@ __global__ void __launch_bounds__(kBlock) k_sea_ice(Model m, const PlanetConst* 
     xheat = (F.dshfl[c] + F.dswfl[NL * SN + c] + F.dlwfl[NL * SN + c] + F.dlhfl[c] + F.sea_cheata[c]) / naccua;
     xprs = (F.dprs[c] + F.sea_cprsa[c]) / naccua;
   }
-  F.sea_cheata[c] = 0.f;
-  F.sea_cprsa[c] = 0.f;
-  F.sea_naccua[c] = 0.f;
+  // Every input is read before the first store (the compiler cannot prove
+  // the fields distinct); the stores come at the end.
   const float zrhoilfdt = K.CRHOI * K.CLFI / K.XDT;
-  F.xclssto[c] = clim14(F.xclsst, P.surf, c, SN);
-  F.xclsst2[c] = clim14(F.xclsst, P.surf + 3, c, SN);
+  const float clssto = clim14(F.xclsst, P.surf, c, SN);
+  const float clsst2 = clim14(F.xclsst, P.surf + 3, c, SN);
   const float cliced = fmaxf(clim14(F.xcliced, P.surf + 3, c, SN), 0.f);
   float clicec = fmaxf(clim14(F.xclicec, P.surf + 3, c, SN), 0.f);
   if (cliced <= 0.f) clicec = 0.f;
-  F.xcliced2[c] = cliced;
-  F.xclicec2[c] = clicec;
   const float xls = F.xls[c], xsst = F.xsst[c];
   float xiced = F.xiced[c], xsnow = F.xsnow[c], xicecc = F.xicecc[c], xcflux = F.xcflux[c], xcfluxf = F.xcfluxf[c];
-  F.ice_snowold[c] = xsnow;
+  const float snow_old = xsnow, xicec_in = F.xicec[c], xoflux = F.xoflux[c], zflx_in = F.ice_zflx[c];
+  const float xgw = F.xgw[c];
   const float zicedold = xls < 0.5f ? xiced : 0.f;
   float ximelt = 0.f, xsmelt = 0.f, xsmflx = 0.f, xscflx = 0.f, xsndch = 0.f, xcfluxr = 0.f;
-  if (F.xicec[c] >= K.CICEMIN) {
+  if (xicec_in >= K.CICEMIN) {
     xsnow = xsnow + xprs * K.XDT;
     xprs = 0.f;
   }
@@ -1808,8 +1806,6 @@ __global__ void __launch_bounds__(kBlock) k_sea_ice(Model m, const PlanetConst* 
     xts = xsst;
     if (xiced > 0.f) xqmelt = xheat;
   }
-  F.xts[c] = xts;
-  F.xqmelt[c] = xqmelt;
   if (xiced < K.XMIND) {
     xcflux = xheat;
     xcfluxf = 0.f;
@@ -1820,7 +1816,7 @@ __global__ void __launch_bounds__(kBlock) k_sea_ice(Model m, const PlanetConst* 
     xcflux = zckap * (xts - xsst) / (zhsnowc + xiced);
     xcfluxf = zckap * (K.TFREEZE - xsst) / (zhsnowc + xiced);
   }
-  if (F.xicec[c] < K.CICEMIN && xprs > 0.f) {
+  if (xicec_in < K.CICEMIN && xprs > 0.f) {
     xcflux = xcflux - xprs * 1000.f * K.CLFSN;
     xsmelt = xprs + xsmelt;
     xsmflx = xsmflx + xprs * 1000.f * K.CLFSN;
@@ -1855,7 +1851,7 @@ __global__ void __launch_bounds__(kBlock) k_sea_ice(Model m, const PlanetConst* 
     xsmelt = xsmelt - zdsnow / K.XDT;
     xsmflx = xsmflx - zdsnow * 1.0e3f * K.CLFSN / K.XDT;
   }
-  if (xls < 0.5f) xcflux = xcflux + F.xoflux[c];
+  if (xls < 0.5f) xcflux = xcflux + xoflux;
   if (xsst <= K.TFREEZE || xiced > 0.f) {
     ximelt = xcflux + xscflx - xcfluxf;
     xiced = xiced - ximelt / zrhoilfdt;
@@ -1877,10 +1873,19 @@ __global__ void __launch_bounds__(kBlock) k_sea_ice(Model m, const PlanetConst* 
     ximelt = ximelt + zcflux;
     xsndch = xsndch + zcflux * 1000.f / K.CRHOI / zrhoilfdt;
   }
-  float zflx = F.ice_zflx[c];
+  float zflx = zflx_in;
   if (xls < 1.f) zflx = fmaxf(0.f, K.XMAXD - xiced) * zrhoilfdt;
+  F.sea_cheata[c] = 0.f;
+  F.sea_cprsa[c] = 0.f;
+  F.sea_naccua[c] = 0.f;
+  F.xclssto[c] = clssto;
+  F.xclsst2[c] = clsst2;
+  F.xcliced2[c] = cliced;
+  F.xclicec2[c] = clicec;
+  F.ice_snowold[c] = snow_old;
+  F.xts[c] = xts;
+  F.xqmelt[c] = xqmelt;
   F.ice_zflx[c] = zflx;
-  const float xgw = F.xgw[c];
   F.ice_part1[c] = xls < 1.f ? xcfluxr * xgw : 0.f;
   F.ice_part2[c] = xls < 1.f ? zflx * xgw : 0.f;
   F.xiced[c] = xiced;
