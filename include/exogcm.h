@@ -134,6 +134,19 @@ int exogcm_step(exogcm_engine* engine, int steps, int publish_every);
  * NULL to query only. */
 int exogcm_read_snapshot(exogcm_engine* engine, int slot, float* values, size_t count, long* step);
 
+/* Starts copying every slot's snapshot field, as the last exogcm_step left
+ * it, into `values` (count = snapshot planes x slots x NHOR floats, laid out
+ * [plane][slot][point] as on the device) and returns at once: the copy to
+ * the host runs on a stream of its own, from a device-side copy taken on the
+ * engine's stream, so the next exogcm_step computes while it drains. Use
+ * pinned host memory for `values` to get that overlap. Only slots that
+ * published in that step hold a new snapshot (see exogcm_read_snapshot). A
+ * second call waits for the first copy; exogcm_snapshots_wait waits for the
+ * last one. There is no counterpart in the reference, whose worker maps one
+ * staging buffer per snapshot (stepper/index.ts:254-265). */
+int exogcm_snapshots_begin(exogcm_engine* engine, float* values, size_t count);
+int exogcm_snapshots_wait(exogcm_engine* engine);
+
 /* Stops a slot at model step `step`: later steps of a batch leave the slot
  * untouched (its kernels skip it), so a run ends exactly on its last step
  * whatever the batch length. A negative step removes the limit. */

@@ -243,6 +243,32 @@ def test_snapshot_publishes_on_schedule():
 
 
 @pytest.mark.gpu
+def test_bulk_snapshot_copy_overlaps_the_next_step():
+    """exogcm_snapshots_begin copies every slot's snapshot field while the
+    caller steps on: the copy keeps the day it was started on, equal to the
+    per-slot reads of that day, although the next step overwrites the field."""
+    torch = pytest.importorskip("torch")
+    e = pkg.Engine(21, 10, 3, mode=1)
+    for s in range(3):
+        e.configure(s, planets.make_planet(70 + s, truncation=21, levels=10))
+    e.step(3, publish_every=4)
+    e.step(4, publish_every=4)
+    per_slot = e.field_size("snapshot")
+    bulk = torch.empty(3 * per_slot, dtype=torch.float32, pin_memory=True).numpy()
+    for day in range(2):
+        ref = [e.snapshot(s)[1] for s in range(3)]
+        e.snapshots_begin(bulk)
+        e.step(4, publish_every=4)  # packs new snapshots over the field being copied
+        e.snapshots_wait()
+        got = bulk.reshape(101, 3, 2048)
+        for s in range(3):
+            assert np.array_equal(got[:, s, :], ref[s]), (day, s)
+        assert not np.array_equal(e.snapshot(0)[1], ref[0])
+    with pytest.raises(pkg.ExogcmError):
+        e.snapshots_begin(bulk[:-1])
+
+
+@pytest.mark.gpu
 def test_autotuned_shapes_leave_results_unchanged():
     """Each engine times its own transform shapes at its first configure;
     engines of 1 and 3 slots may pick different ones, and the shared planet

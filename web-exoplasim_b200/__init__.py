@@ -72,6 +72,8 @@ SIGNATURES = {
                                             _DP, ctypes.POINTER(ctypes.c_size_t)]),
     "exogcm_release": (ctypes.c_int, [_VP, ctypes.c_int]),
     "exogcm_step": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
+    "exogcm_snapshots_begin": (ctypes.c_int, [_VP, _FP, ctypes.c_size_t]),
+    "exogcm_snapshots_wait": (ctypes.c_int, [_VP]),
     "exogcm_read_snapshot": (ctypes.c_int, [_VP, ctypes.c_int, _FP, ctypes.c_size_t,
                                             ctypes.POINTER(ctypes.c_long)]),
     "exogcm_set_stop": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_long]),
@@ -262,6 +264,15 @@ class Engine:
         step = ctypes.c_long()
         _check(_lib.exogcm_read_snapshot(self.h, slot, out.ctypes.data_as(_FP), out.size, ctypes.byref(step)))
         return step.value
+
+    def snapshots_begin(self, out: np.ndarray) -> None:
+        """Starts copying every slot's snapshot field ([plane][slot][point],
+        float32, pinned for overlap) while the caller goes on stepping; see
+        snapshots_wait. `out` must stay alive until then."""
+        _check(_lib.exogcm_snapshots_begin(self.h, out.ctypes.data_as(_FP), out.size))
+
+    def snapshots_wait(self) -> None:
+        _check(_lib.exogcm_snapshots_wait(self.h))
 
     def slot_info(self, slot: int):
         step, left, active = ctypes.c_long(), ctypes.c_int(), ctypes.c_int()

@@ -104,6 +104,11 @@ struct exogcm_engine {
   double* sums = nullptr;
   int* flags = nullptr;
   int* fault = nullptr;  // device word: a kernel gave up a bounded wait
+  // overlapped snapshot copies (exogcm_snapshots_begin/wait)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t snap_staged = nullptr, snap_copied = nullptr;
+  float* snap_stage = nullptr;  // device copy of the snapshot field
+  bool copy_pending = false;
   std::vector<Slot> slots;
   std::map<int, cudaGraphExec_t> graphs;
   Tuning tune{};
@@ -775,6 +780,13 @@ int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine
 void exogcm_destroy(exogcm_engine* e) {
   if (!e) return;
   if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->copy_stream) {
+    cudaStreamSynchronize(e->copy_stream);
+    cudaStreamDestroy(e->copy_stream);
+  }
+  if (e->snap_staged) cudaEventDestroy(e->snap_staged);
+  if (e->snap_copied) cudaEventDestroy(e->snap_copied);
+  cudaFree(e->snap_stage);
   for (auto& g : e->graphs) cudaGraphExecDestroy(g.second);
   cudaFree(e->arena);
   cudaFree(e->shared_buf);
@@ -938,6 +950,46 @@ int exogcm_read_snapshot(exogcm_engine* e, int slot, float* values, size_t count
     const FieldInfo& fi = field(e, "snapshot");
     if (count != fi.plane * fi.count) throw Error(EXOGCM_EINVAL, "snapshot buffer size mismatch");
     copy_field(e, fi, slot, values, false);
+  });
+}
+
+int exogcm_snapshots_begin(exogcm_engine* e, float* values, size_t count) {
+  return guard([&] {
+    if (!e || !values) throw Error(EXOGCM_EINVAL, "null argument");
+    const FieldInfo& fi = field(e, "snapshot");
+    const size_t n = fi.plane * fi.count * e->d.S;
+    if (count != n) throw Error(EXOGCM_EINVAL, "snapshot buffer size mismatch (planes x slots x points)");
+    if (e->copy_pending) {
+      check(cudaEventSynchronize(e->snap_copied), "previous snapshot copy");
+      e->copy_pending = false;
+    }
+    if (!e->copy_stream) {
+      check(cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking), "copy stream");
+      check(cudaEventCreateWithFlags(&e->snap_staged, cudaEventDisableTiming), "event");
+      check(cudaEventCreateWithFlags(&e->snap_copied, cudaEventDisableTiming), "event");
+      check(cudaMalloc(&e->snap_stage, n * sizeof(float)), "snapshot staging");
+    }
+    // The device copy runs on the engine's stream, so the next step's graph
+    // (queued after it) may overwrite the field while the host copy drains
+    // the staging buffer on the copy stream.
+    check(cudaMemcpyAsync(e->snap_stage, e->arena + fi.offset, n * sizeof(float), cudaMemcpyDeviceToDevice,
+                          e->stream),
+          "snapshot staging");
+    check(cudaEventRecord(e->snap_staged, e->stream), "event");
+    check(cudaStreamWaitEvent(e->copy_stream, e->snap_staged, 0), "copy stream wait");
+    check(cudaMemcpyAsync(values, e->snap_stage, n * sizeof(float), cudaMemcpyDeviceToHost, e->copy_stream),
+          "snapshot copy");
+    check(cudaEventRecord(e->snap_copied, e->copy_stream), "event");
+    e->copy_pending = true;
+  });
+}
+
+int exogcm_snapshots_wait(exogcm_engine* e) {
+  return guard([&] {
+    if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    if (!e->copy_pending) return;
+    check(cudaEventSynchronize(e->snap_copied), "snapshot copy");
+    e->copy_pending = false;
   });
 }
 
