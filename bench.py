@@ -361,7 +361,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(device_ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "T42 L10 batched ensemble, 45-minute steps (configs[1] planet recipe, "
+            "config": {"workload": "T42 L10 batched ensemble, 45-minute steps (seeded synthetic planet recipe, "
                                    "seeded per planet)", "planets_per_gpu": slots, "global_batch": slots * world,
                        "seq_len": None, "parallelism": f"planets sharded over {world} GPU(s), no collective",
                        "l2": "state of the batch (GBs) far above the 126 MB L2; no flush needed",
