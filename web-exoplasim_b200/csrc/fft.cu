@@ -44,7 +44,7 @@ template <int Q>
 __global__ void __launch_bounds__(kMaxThreads) k_fft_forward(const float* __restrict__ g, float* __restrict__ c,
                                                              const float2* __restrict__ twg, int nlat, int rows) {
   using Sh = Shape<Q>;
-  constexpr int T = Sh::T, M = Sh::M, N = Sh::N, NTP1 = Sh::NTP1;
+  constexpr int T = Sh::T, N = Sh::N, NTP1 = Sh::NTP1;
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* twq = tw + N;
@@ -67,19 +67,25 @@ __global__ void __launch_bounds__(kMaxThreads) k_fft_forward(const float* __rest
   float2* xr = xb + r * Sh::XP;
   float2 b[Sh::KT][Q];
   four_step<Q, -1>(a, b, twq, xr, t);
-  __syncwarp();
-#pragma unroll
-  for (int j = 0; j < Sh::KT; ++j)
-#pragma unroll
-    for (int k2 = 0; k2 < Q; ++k2) xr[zpos(t + T * j + 8 * k2)] = b[j][k2];
-  __syncwarp();
+  // The split needs Z[m] and Z[(M - m) mod M] for m = t + T i. This thread
+  // holds Z[t + T j + 8 k2] in b[j][k2], so Z[m] is its own b[i % KT][i / KT];
+  // for t > 0 the partner value is b[KT-1-j][Q-1-k2] of lane T - t of the
+  // row's group (a shuffle), and for t = 0 it is this thread's own.
   const float inv_n = 1.f / (float)N;
+  const int lane = threadIdx.x & 31, src = lane - t + (T - t) % T;
 #pragma unroll
   for (int i = 0; i < (NTP1 + T - 1) / T; ++i) {
+    constexpr int KT = Sh::KT;
+    const int j = i % KT, k2 = i / KT;
+    const float2 send = b[KT - 1 - j][Q - 1 - k2];
+    float2 partner;
+    partner.x = __shfl_sync(0xffffffffu, send.x, src);
+    partner.y = __shfl_sync(0xffffffffu, send.y, src);
+    if (t == 0) partner = j == 0 ? b[0][(Q - k2) % Q] : b[j][Q - 1 - k2];
     const int m = t + T * i;
     if (m < NTP1) {
-      const float2 zm = xr[zpos(m)];
-      const float2 zc = conj2(xr[zpos(m == 0 ? 0 : M - m)]);
+      const float2 zm = b[j][k2];
+      const float2 zc = conj2(partner);
       const float2 even = make_float2(0.5f * (zm.x + zc.x), 0.5f * (zm.y + zc.y));
       // (zm - zc) / 2i = ((zm - zc).y, -(zm - zc).x) / 2
       const float2 odd = make_float2(0.5f * (zm.y - zc.y), -0.5f * (zm.x - zc.x));
