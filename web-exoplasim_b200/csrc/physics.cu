@@ -339,19 +339,28 @@ __device__ __forceinline__ void diffuse_potential(const float* ds, float* x, con
 
 // physics/surface-flux/wgsl/vdiff.wgsl: Richardson-number vertical diffusion.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_vdiff(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+__global__ void __launch_bounds__(kBlock, 3) k_vdiff(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const float* ds = tb + m.to.dsigma;
   const float* sh = tb + m.to.sigmah;
   const float D2 = P.deltsec2;
+  // Every field value used is read here, before the first store (the
+  // compiler cannot prove the fields distinct, so a store would order each
+  // later load after it).
   float zt[NL], zq[NL], zu[NL], zv[NL], zabsu[NL], zskap[NL], zskaph[NL];
+  float dtdt[NL], dqdt[NL], dudt[NL], dvdt[NL], dq[NL];
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SN + c;
-    zt[l] = F.dt[at] + F.dtdt[at] * D2;
-    zq[l] = F.dq[at] + F.dqdt[at] * D2;
-    zu[l] = F.du[at] + F.dudt[at] * D2;
-    zv[l] = F.dv[at] + F.dvdt[at] * D2;
+    dtdt[l] = F.dtdt[at];
+    dqdt[l] = F.dqdt[at];
+    dudt[l] = F.dudt[at];
+    dvdt[l] = F.dvdt[at];
+    dq[l] = F.dq[at];
+    zt[l] = F.dt[at] + dtdt[l] * D2;
+    zq[l] = dq[l] + dqdt[l] * D2;
+    zu[l] = F.du[at] + dudt[l] * D2;
+    zv[l] = F.dv[at] + dvdt[l] * D2;
     zabsu[l] = sqrtf(zu[l] * zu[l] + zv[l] * zv[l]);
     zskap[l] = tb[m.to.vdiff_skap + l];
     zskaph[l] = tb[m.to.vdiff_skaph + l];
@@ -401,8 +410,8 @@ __global__ void __launch_bounds__(kBlock) k_vdiff(Model m, const PlanetConst* __
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SN + c;
-    F.dudt[at] = F.dudt[at] + (zun[l] - zu[l]) / D2;
-    F.dvdt[at] = F.dvdt[at] + (zvn[l] - zv[l]) / D2;
+    F.dudt[at] = dudt[l] + (zun[l] - zu[l]) / D2;
+    F.dvdt[at] = dvdt[l] + (zvn[l] - zv[l]) / D2;
   }
   if (K.NDHEAT != 0.f) {
     float zke[NL], zken[NL];
@@ -411,10 +420,9 @@ __global__ void __launch_bounds__(kBlock) k_vdiff(Model m, const PlanetConst* __
     diffuse<NL>(ds, zken, km);
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
-      const size_t at = l * SN + c;
       const float zdtdt = -((zun[l] * zun[l] - zu[l] * zu[l] + zvn[l] * zvn[l] - zv[l] * zv[l]) / D2 -
-                            (zken[l] - zke[l]) / D2) * 0.5f / K.ACPD / (1.f + K.ADV * F.dq[at]);
-      F.dtdt[at] = F.dtdt[at] + zdtdt;
+                            (zken[l] - zke[l]) / D2) * 0.5f / K.ACPD / (1.f + K.ADV * dq[l]);
+      dtdt[l] = dtdt[l] + zdtdt;
     }
   }
   float zqn[NL];
@@ -422,7 +430,7 @@ __global__ void __launch_bounds__(kBlock) k_vdiff(Model m, const PlanetConst* __
   for (int l = 0; l < NL; ++l) zqn[l] = zq[l];
   diffuse<NL>(ds, zqn, kh);
 #pragma unroll
-  for (int l = 0; l < NL; ++l) F.dqdt[l * SN + c] = F.dqdt[l * SN + c] + (zqn[l] - zq[l]) / D2;
+  for (int l = 0; l < NL; ++l) F.dqdt[l * SN + c] = dqdt[l] + (zqn[l] - zq[l]) / D2;
 #pragma unroll
   for (int l = 0; l < NL - 1; ++l) kh[l] = kh[l] * zskaph[l];
   float ztn[NL];
@@ -430,7 +438,7 @@ __global__ void __launch_bounds__(kBlock) k_vdiff(Model m, const PlanetConst* __
   for (int l = 0; l < NL; ++l) ztn[l] = zt[l];
   diffuse_potential<NL>(ds, ztn, kh, zskap);
 #pragma unroll
-  for (int l = 0; l < NL; ++l) F.dtdt[l * SN + c] = F.dtdt[l * SN + c] + (ztn[l] - zt[l]) / D2;
+  for (int l = 0; l < NL; ++l) F.dtdt[l * SN + c] = dtdt[l] + (ztn[l] - zt[l]) / D2;
 }
 
 // ---------------------------------------------------------------- radiation
