@@ -483,7 +483,8 @@ __global__ void __launch_bounds__(kBlock) k_spectrald_update(Model m) {
 
 // gridpointd before the parameterizations (dynamics/wgsl/physics-in.wgsl),
 // one thread per column, every input read before the first store. A block's
-// columns share one slot: kBlock divides NHOR.
+// columns share one slot: kBlock divides NHOR. The grid tendencies are
+// zeroed only under single-stage replay (Model::zero_gdt).
 template <int NL>
 __global__ void __launch_bounds__(kBlock) k_physics_in(Model m) {
   const Dims& d = m.d;
@@ -518,10 +519,12 @@ __global__ void __launch_bounds__(kBlock) k_physics_in(Model m) {
     F.dtdt[at] = 0.f;
     F.dqdt[at] = 0.f;
     if (l < NL) {
-      F.gudt[at] = 0.f;
-      F.gvdt[at] = 0.f;
-      F.gtdt[at] = 0.f;
-      F.gqdt[at] = 0.f;
+      if (m.zero_gdt) {
+        F.gudt[at] = 0.f;
+        F.gvdt[at] = 0.f;
+        F.gtdt[at] = 0.f;
+        F.gqdt[at] = 0.f;
+      }
       F.du[at] = CV * gu[l] * scale;
       F.dv[at] = CV * gv[l] * scale;
       F.dt[at] = CT * (gt[l] + t0l[l]);
@@ -532,6 +535,8 @@ __global__ void __launch_bounds__(kBlock) k_physics_in(Model m) {
 
 // gridpointd after the parameterizations (dynamics/wgsl/physics-out.wgsl),
 // four columns of one level per thread, inputs read before the stores.
+// Within a full step gudt, gvdt, gtdt hold no earlier increment and are not
+// read (Model::zero_gdt): the sum adds +0 as the zeroed fields would.
 __global__ void __launch_bounds__(kBlock) k_physics_out(Model m) {
   const Dims& d = m.d;
   const int slot = blockIdx.x * kCols4 / d.NHOR;
@@ -540,7 +545,10 @@ __global__ void __launch_bounds__(kBlock) k_physics_out(Model m) {
   const size_t i = (size_t)blockIdx.y * d.S * d.NHOR + c;
   const FieldPtrs& F = m.f;
   const float4 dudt = ld4(F.dudt, i), dvdt = ld4(F.dvdt, i), dtdt = ld4(F.dtdt, i), dqdt = ld4(F.dqdt, i);
-  const float4 gudt = ld4(F.gudt, i), gvdt = ld4(F.gvdt, i), gtdt = ld4(F.gtdt, i), gqdt = ld4(F.gqdt, i);
+  const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+  const bool earlier = m.zero_gdt != 0;
+  const float4 gudt = earlier ? ld4(F.gudt, i) : z, gvdt = earlier ? ld4(F.gvdt, i) : z;
+  const float4 gtdt = earlier ? ld4(F.gtdt, i) : z, gqdt = ld4(F.gqdt, i);
   const float4 dp = ld4(F.dp, c), rc = ld4(m.sh.rcsq, h);
   if (!m.params[slot].active) return;
   const PlanetConst& K = m.pc[slot];

@@ -129,6 +129,7 @@ struct exogcm_engine {
     m.mode = mode;
     m.tune = tune;
     m.keep_fourier = 0;
+    m.zero_gdt = 0;
     return m;
   }
 };
@@ -1153,9 +1154,11 @@ int exogcm_run_stage(exogcm_engine* e, const char* stage) {
     check(cudaMemcpyAsync(e->params, e->hparams, S * sizeof(StepParams), cudaMemcpyHostToDevice, e->stream),
           "params");
     // Stage replay compares every field, so the fused transforms also write
-    // the Fourier fields they pass through.
+    // the Fourier fields they pass through, and physics_in zeroes the grid
+    // tendencies.
     Model m = e->model(0);
     m.keep_fourier = 1;
+    m.zero_gdt = 1;
     run_stage(m, stage, e->stream);
     check(cudaGetLastError(), "stage launch");
     check(cudaStreamSynchronize(e->stream), "stage");
@@ -1226,13 +1229,14 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
       launch = [&] { dyn_mkdheat(m, 1, e->stream); };
       b = cols * 4 * (6.0 * d.L + 1);
     } else if (k == "physics_in") {
-      // gp, u, v, t, q in; dp, the dimensional u, v, t, q and the zeroed tendencies out
+      // gp, u, v, t, q in; dp, the dimensional u, v, t, q and the zeroed
+      // dimensional tendencies out
       launch = [&] { dyn_physics_in(m, e->stream); };
-      b = cols * 4 * (4.0 * d.L + 1 + 1 + 4.0 * d.L + 4.0 * (d.L + 1) + 4.0 * d.L);
+      b = cols * 4 * (4.0 * d.L + 1 + 1 + 4.0 * d.L + 4.0 * (d.L + 1));
     } else if (k == "physics_out") {
-      // four physics tendencies, four dynamics tendencies and dp in; four tendencies out
+      // four physics tendencies, the fixer's gqdt and dp in; four tendencies out
       launch = [&] { dyn_physics_out(m, e->stream); };
-      b = cols * 4 * (8.0 * d.L + 1 + 4.0 * d.L);
+      b = cols * 4 * (5.0 * d.L + 1 + 4.0 * d.L);
     } else {
       // Column kernels: compulsory reads + writes per column, in floats.
       const std::map<std::string, double> per_column = {

@@ -190,7 +190,9 @@ __global__ void __launch_bounds__(kSumThreads) k_slot_sums(Model m, const float*
   }
 }
 
-// physics/fixer/wgsl/apply.wgsl: the global step, gqdt and the new dq.
+// physics/fixer/wgsl/apply.wgsl: the global step, gqdt and the new dq. The
+// fixer is the first to raise gqdt after physics_in zeroed it, so within a
+// full step (Model::zero_gdt = 0) it adds its increment to 0 unread.
 template <int NL>
 __global__ void __launch_bounds__(kBlock) k_fixer_apply(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
@@ -204,7 +206,7 @@ __global__ void __launch_bounds__(kBlock) k_fixer_apply(Model m, const PlanetCon
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SN + c;
     fq[l] = F.fixq[at];
-    gq[l] = F.gqdt[at];
+    gq[l] = m.zero_gdt ? F.gqdt[at] : 0.f;
     dq[l] = F.dq[at];
   }
 #pragma unroll
