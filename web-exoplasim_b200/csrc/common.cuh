@@ -144,13 +144,18 @@ struct Model {
                              // 2 optimized path with sp2fc / sp2fcdmu on the tensor cores
   Tuning tune;               // optimized path launch shapes
   int keep_fourier;          // optimized path: fused transforms also write the Fourier fields they pass through
-  // The grid tendencies gudt, gvdt, gtdt, gqdt are zeroed by physics_in,
-  // raised by the fixer (gqdt) and completed by physics_out. Within a full
-  // step (zero_gdt = 0) physics_in leaves them alone, the fixer writes gqdt
-  // as 0 + its increment and physics_out writes gudt, gvdt, gtdt as its
-  // increment + 0: the values the zeroed fields give. Single-stage replay
-  // compares every field after each stage, so there (zero_gdt = 1) the three
-  // kernels zero and read them as the reference does.
+  // physics_in zeroes the grid tendencies gudt, gvdt, gtdt, gqdt and the
+  // dimensional ones dudt, dvdt, dtdt, dqdt. The fixer first raises gqdt and
+  // physics_out completes the four grid ones; surflx first raises the
+  // lowest level of the dimensional ones and vdiff then updates every
+  // level. Within a full step (zero_gdt = 0) physics_in leaves all but the
+  // dimensional ones' surface level alone, and those kernels take the
+  // zeros as values instead of reading them (the fixer writes gqdt as
+  // 0 + its increment, physics_out gudt, gvdt, gtdt as its increment + 0,
+  // surflx its level as 0 + its increment; vdiff reads only that level):
+  // the values the zeroed fields give. Single-stage replay compares every
+  // field after each stage, so there (zero_gdt = 1) the kernels zero and
+  // read them as the reference does.
   int zero_gdt;
 };
 

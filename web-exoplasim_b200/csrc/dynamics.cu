@@ -483,8 +483,9 @@ __global__ void __launch_bounds__(kBlock) k_spectrald_update(Model m) {
 
 // gridpointd before the parameterizations (dynamics/wgsl/physics-in.wgsl),
 // one thread per column, every input read before the first store. A block's
-// columns share one slot: kBlock divides NHOR. The grid tendencies are
-// zeroed only under single-stage replay (Model::zero_gdt).
+// columns share one slot: kBlock divides NHOR. The grid tendencies, and the
+// dimensional ones below the surface level, are zeroed only under
+// single-stage replay (Model::zero_gdt).
 template <int NL>
 __global__ void __launch_bounds__(kBlock) k_physics_in(Model m) {
   const Dims& d = m.d;
@@ -514,10 +515,12 @@ __global__ void __launch_bounds__(kBlock) k_physics_in(Model m) {
 #pragma unroll
   for (int l = 0; l < NL + 1; ++l) {
     const size_t at = l * SN + c;
-    F.dudt[at] = 0.f;
-    F.dvdt[at] = 0.f;
-    F.dtdt[at] = 0.f;
-    F.dqdt[at] = 0.f;
+    if (m.zero_gdt || l == NL) {
+      F.dudt[at] = 0.f;
+      F.dvdt[at] = 0.f;
+      F.dtdt[at] = 0.f;
+      F.dqdt[at] = 0.f;
+    }
     if (l < NL) {
       if (m.zero_gdt) {
         F.gudt[at] = 0.f;

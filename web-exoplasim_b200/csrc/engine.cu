@@ -1229,10 +1229,10 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
       launch = [&] { dyn_mkdheat(m, 1, e->stream); };
       b = cols * 4 * (6.0 * d.L + 1);
     } else if (k == "physics_in") {
-      // gp, u, v, t, q in; dp, the dimensional u, v, t, q and the zeroed
-      // dimensional tendencies out
+      // gp, u, v, t, q in; dp, the dimensional u, v, t, q and the surface
+      // level of the zeroed dimensional tendencies out
       launch = [&] { dyn_physics_in(m, e->stream); };
-      b = cols * 4 * (4.0 * d.L + 1 + 1 + 4.0 * d.L + 4.0 * (d.L + 1));
+      b = cols * 4 * (4.0 * d.L + 1 + 1 + 4.0 * d.L + 4);
     } else if (k == "physics_out") {
       // four physics tendencies, the fixer's gqdt and dp in; four tendencies out
       launch = [&] { dyn_physics_out(m, e->stream); };
@@ -1240,7 +1240,7 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
     } else {
       // Column kernels: compulsory reads + writes per column, in floats.
       const std::map<std::string, double> per_column = {
-          {"vdiff", 12 * L},                                 // t, q, u, v and tendencies in; 4 tendencies out
+          {"vdiff", 8 * L + 4},                              // t, q, u, v, surflx's tendencies in; 4 tendencies out
           {"swr", 5 * L + 7 + 3 * (L + 1) + 3},              // dcc, dql, dq, dt, dqo3 + surface in; 3 fluxes + albedos out
           {"lwr_radstep", 7 * L + 4 + 4 * (L + 1) + 4 * L},  // t, q, o3, co2, clouds, sw flux, dtdt in; 4 fluxes + 4 rates out
           {"kuo", 5 * L + 3 + 6 * L + 1},                    // dqt, q, t and tendencies in; tendencies, rain, cloud levels out

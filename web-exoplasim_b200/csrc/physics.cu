@@ -230,8 +230,11 @@ __global__ void __launch_bounds__(kBlock) k_surflx(Model m, const PlanetConst* _
   const float u = F.du[lo], v = F.dv[lo], t = F.dt[lo], q = F.dq[lo], ts = F.dt[sf], qs = F.dq[sf];
   const float dp = F.dp[c], dls = F.dls[c];
   // the tendencies and surface values used after the first store are read
-  // here (the compiler cannot prove the fields distinct)
-  const float dudt0 = F.dudt[lo], dvdt0 = F.dvdt[lo], dtdt0 = F.dtdt[lo], dqdt0 = F.dqdt[lo];
+  // here (the compiler cannot prove the fields distinct); within a full step
+  // the tendencies hold physics_in's zeros, taken unread (Model::zero_gdt)
+  const bool earlier = m.zero_gdt != 0;
+  const float dudt0 = earlier ? F.dudt[lo] : 0.f, dvdt0 = earlier ? F.dvdt[lo] : 0.f;
+  const float dtdt0 = earlier ? F.dtdt[lo] : 0.f, dqdt0 = earlier ? F.dqdt[lo] : 0.f;
   const float drhs = F.drhs[c], dwatc = F.dwatc[c], dz0 = F.dz0[c];
   const float dsigma = tb[m.to.dsigma + low];
   const float zfac = tb[m.to.flux_sigfac], zlnsig = tb[m.to.flux_lnsig];
@@ -348,16 +351,18 @@ __global__ void __launch_bounds__(kBlock, 3) k_vdiff(Model m, const PlanetConst*
   const float D2 = P.deltsec2;
   // Every field value used is read here, before the first store (the
   // compiler cannot prove the fields distinct, so a store would order each
-  // later load after it).
+  // later load after it). Within a full step only surflx's lowest level of
+  // the tendencies holds more than physics_in's zeros (Model::zero_gdt).
   float zt[NL], zq[NL], zu[NL], zv[NL], zabsu[NL], zskap[NL], zskaph[NL];
   float dtdt[NL], dqdt[NL], dudt[NL], dvdt[NL], dq[NL];
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SN + c;
-    dtdt[l] = F.dtdt[at];
-    dqdt[l] = F.dqdt[at];
-    dudt[l] = F.dudt[at];
-    dvdt[l] = F.dvdt[at];
+    const bool held = m.zero_gdt || l == NL - 1;
+    dtdt[l] = held ? F.dtdt[at] : 0.f;
+    dqdt[l] = held ? F.dqdt[at] : 0.f;
+    dudt[l] = held ? F.dudt[at] : 0.f;
+    dvdt[l] = held ? F.dvdt[at] : 0.f;
     dq[l] = F.dq[at];
     zt[l] = F.dt[at] + dtdt[l] * D2;
     zq[l] = dq[l] + dqdt[l] * D2;
