@@ -1640,15 +1640,53 @@ template <int NL>
 __global__ void __launch_bounds__(kBlock) k_land_surface(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const float DS = P.deltsec;
-  const float dls = F.dls[c];
-  if (dls > 0.f) F.driver[c] = F.driver[c] + F.drunoff[c] * DS;
+  // Every input is read before the first store (the compiler cannot prove
+  // the fields distinct, so a store would order each later load after it).
+  // Each output is formed in registers and stored once, with the value of
+  // the shaders' last store to it.
+  const float dls = F.dls[c], dglac = F.dglac[c];
+  const bool land = dls > 0.f;
+  const bool wetsoil = K.NWETSOIL != 0.f && dls > 0.5f;
+  const bool veg = K.NVEG > 0.f && land && dglac < 0.90f;
+  const bool glacier = dglac > 0.5f && land;
+  const bool glaciers = K.NGLACIER != 0.f;
   const float dts = F.land_dts[c];
   float albclim = clim14(F.dalbcl, P.surf + 3, c, SN);
   float albclim1 = clim14(F.dalbcl1, P.surf + 3, c, SN);
   float albclim2 = clim14(F.dalbcl2, P.surf + 3, c, SN);
-  if (K.NWETSOIL != 0.f && dls > 0.5f) {
+  const float dwater = wetsoil ? F.dwater[c] : 0.f;
+  float driver = 0.f, drunoff = 0.f, dp = 0.f, dsnowz = 0.f, dforest = 0.f, dwmax = 0.f, dwatc = 0.f;
+  float soil[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  if (land) {
+    driver = F.driver[c];
+    drunoff = F.drunoff[c];
+    dp = F.dp[c];
+    dsnowz = F.dsnowz[c];
+    dforest = F.dforest[c];
+    dwmax = F.dwmax[c];
+    dwatc = F.dwatc[c];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) soil[i] = F.dsoilt[i * SN + c];
+  }
+  float co2 = 0.f, dq_low = 0.f, dcveg = 0.f, dcsoil = 0.f, dagg = 0.f, dfd = 0.f, devap = 0.f, dgrow = 0.f;
+  float dmr = 0.f, dsc = 0.f, z0c = 0.f;
+  if (veg) {
+    co2 = F.co2[slot];
+    dq_low = F.dq[(NL - 1) * SN + c];
+    dcveg = F.dcveg[c];
+    dcsoil = F.dcsoil[c];
+    dagg = F.dagg[c];
+    dfd = F.dfd[NL * SN + c];
+    devap = F.devap[c];
+    dgrow = F.dgrow[c];
+    dmr = F.dmr[c];
+    dsc = F.dsc[c];
+    if (K.NVEG == 2.f) z0c = F.dz0climo[c];
+  }
+  const float dpersist_in = glaciers ? F.dpersist[c] : 0.f;
+  if (wetsoil) {
     if (dts > 273.15f) {
-      const float bf = F.dwater[c] / K.WSMAX;
+      const float bf = dwater / K.WSMAX;
       const float al = 1.f / 5.2f * fpow(fpow(fmaxf(bf, 1.0e-3f), (1.f - 4.f) / 4.f) - 1.f, 1.f / 4.f);
       const float dry = expf(-powi(bf * 25.f, 6));
       const float wet = expf(-powi((1.f - bf) * 30.f, 9));
@@ -1661,18 +1699,14 @@ __global__ void __launch_bounds__(kBlock) k_land_surface(Model m, const PlanetCo
       albclim2 = K.DGROUNDALB2;
     }
   }
-  F.dalbclim[c] = albclim;
-  F.dalbclim1[c] = albclim1;
-  F.dalbclim2[c] = albclim2;
-  if (dls > 0.f) {
-    F.land_dtsm[c] = dts;
-    float dqs = K.RDBRV * K.RA1 * expf(K.RA2 * (dts - K.TMELT) / (dts - K.RA4)) / F.dp[c];
+  float dalb = 0.f, dsalb1 = 0.f, dsalb2 = 0.f, drhs = 0.f, dqs = 0.f;
+  bool put_alb = false, put_rhs = false;
+  if (land) {
+    dqs = K.RDBRV * K.RA1 * expf(K.RA2 * (dts - K.TMELT) / (dts - K.RA4)) / dp;
     dqs = dqs / (1.f - (1.f / K.RDBRV - 1.f) * dqs);
-    F.land_dqs[c] = dqs;
-    const float dsnow = F.dsnowz[c];
-    F.dsnow[c] = dsnow;
+    const float dsnow = dsnowz;
     if (dsnow > 0.f) {
-      const float forest = F.dforest[c];
+      const float forest = dforest;
       auto snow_albedo = [&](float mxf, float mxb, float mnf, float mnb) {
         const float zmax = forest * mxf + (1.f - forest) * mxb;
         const float zmin = forest * mnf + (1.f - forest) * mnb;
@@ -1682,61 +1716,55 @@ __global__ void __launch_bounds__(kBlock) k_land_surface(Model m, const PlanetCo
       const float s0 = snow_albedo(K.ALBSMAXF, K.ALBSMAX, K.ALBSMINF, K.ALBSMIN);
       const float s1 = snow_albedo(K.ALBSMAXF1, K.ALBSMAX1, K.ALBSMINF1, K.ALBSMIN1);
       const float s2 = snow_albedo(K.ALBSMAXF2, K.ALBSMAX2, K.ALBSMINF2, K.ALBSMIN2);
-      F.dalb[c] = albclim + (s0 - albclim) * dsnow / (dsnow + 0.01f);
-      F.dsalb[c] = albclim1 + (s1 - albclim1) * dsnow / (dsnow + 0.01f);
-      F.dsalb[SN + c] = albclim2 + (s2 - albclim2) * dsnow / (dsnow + 0.01f);
-      F.drhs[c] = 1.f;
+      dalb = albclim + (s0 - albclim) * dsnow / (dsnow + 0.01f);
+      dsalb1 = albclim1 + (s1 - albclim1) * dsnow / (dsnow + 0.01f);
+      dsalb2 = albclim2 + (s2 - albclim2) * dsnow / (dsnow + 0.01f);
+      drhs = 1.f;
+      put_rhs = true;
     } else {
-      F.dalb[c] = albclim;
-      F.dsalb[c] = albclim1;
-      F.dsalb[SN + c] = albclim2;
-      const float dwmax = F.dwmax[c];
-      if (dwmax > 0.f) F.drhs[c] = fminf(1.f, F.dwatc[c] / (K.DRHSFULL * dwmax));
+      dalb = albclim;
+      dsalb1 = albclim1;
+      dsalb2 = albclim2;
+      if (dwmax > 0.f) {
+        drhs = fminf(1.f, dwatc / (K.DRHSFULL * dwmax));
+        put_rhs = true;
+      }
     }
-    F.dtsoil[c] = F.dsoilt[c];
-    F.dtd2[c] = F.dsoilt[SN + c];
-    F.dtd3[c] = F.dsoilt[2 * SN + c];
-    F.dtd4[c] = F.dsoilt[3 * SN + c];
-    F.dtd5[c] = F.dsoilt[4 * SN + c];
-    F.dt[NL * SN + c] = dts;
-    F.dq[NL * SN + c] = dqs;
+    put_alb = true;
   }
-  if (K.NVEG > 0.f && F.dls[c] > 0.f && F.dglac[c] < 0.90f) {
-    const float co2 = F.co2[slot];
+  float npp = 0.f, cveg = 0.f, csoil = 0.f, vsoil = 0.f, lai = 0.f, dz0 = 0.f, wmax = 0.f, forest = 0.f;
+  if (veg) {
     float zbeta = 0.f;
     if (!(co2 < 1.0e-8f)) zbeta = fmaxf(0.f, 1.f + K.CO2_SENS * logf((co2 - K.CO2_COMP) / (K.CO2_REF - K.CO2_COMP)));
-    const float ts = F.dt[NL * SN + c], dp = F.dp[c], dwatc = F.dwatc[c], dsnow = F.dsnow[c];
-    float zwmax = F.dwmax[c];
-    const float zglacfree = 1.f - F.dglac[c];
+    const float ts = dts, dsnow = dsnowz;
+    float zwmax = dwmax;
+    const float zglacfree = 1.f - dglac;
     const float zsvp = K.RA1 * expf(K.RA2 * (ts - K.TMELT) / (ts - K.RA4));
-    const float zvpd = fmaxf(0.01f, zsvp - dp * F.dq[(NL - 1) * SN + c] / 0.622f);
-    float dcveg = F.dcveg[c], dcsoil = F.dcsoil[c];
-    const float zlaim = K.ZLAIMIN + 0.63661977236758f * K.ZLAIMAX * atanf(K.CVEG_L * 2.f * F.dagg[c] * dcveg);
+    const float zvpd = fmaxf(0.01f, zsvp - dp * dq_low / 0.622f);
+    cveg = dcveg;
+    csoil = dcsoil;
+    const float zlaim = K.ZLAIMIN + 0.63661977236758f * K.ZLAIMAX * atanf(K.CVEG_L * 2.f * dagg * cveg);
     const float zvegm = 1.f - expf(-K.CVEG_K * zlaim);
     float zveg = 0.f;
     if (zwmax > 0.f) zveg = fminf(fminf(1.f, zvegm), fmaxf(0.f, dwatc / (zwmax * K.VWS_CRIT)));
     const float zft = fminf(1.f, fmaxf(0.f, (ts - K.TMELT) / K.CT_CRIT));
-    const float zgppl = K.RLUE * zbeta * zft * zveg * F.dfd[NL * SN + c];
+    const float zgppl = K.RLUE * zbeta * zft * zveg * dfd;
     float zgppw = 0.f;
-    if (!(co2 < 1.0e-8f)) zgppw = K.CO2CONV * dp * zveg * (-F.devap[c]) / zvpd * (0.3f * co2);
+    if (!(co2 < 1.0e-8f)) zgppw = K.CO2CONV * dp * zveg * (-devap) / zvpd * (0.3f * co2);
     zgppw = fminf(1.f, fmaxf(0.f, zgppw));
     const float zgpp = fminf(zgppl, zgppw);
-    const float znpp = F.dgrow[c] * 0.5f * zgpp * zglacfree;
-    F.dnpp[c] = znpp;
-    const float zlitter = dcveg / K.TAU_VEG;
-    const float zres = fpow(K.Q10, (ts - K.TMELT - 10.f) / 10.f) * dcsoil / K.TAU_SOIL;
-    dcveg = dcveg + (znpp - zlitter) * DS * K.NCVEG;
-    dcsoil = dcsoil + (zlitter - zres) * DS * K.NCVEG;
-    const float zforest = fminf(1.f, fmaxf(0.f, (atanf(dcveg - K.CVEG_A) - K.CVEG_E) / (K.CVEG_C - K.CVEG_E)));
-    const float dvsoil = fminf(1.f, fmaxf(0.f, (atanf(dcveg - K.CVEG_F) - K.CVEG_G) / (K.CVEG_C - K.CVEG_G)));
-    F.dcveg[c] = dcveg;
-    F.dcsoil[c] = dcsoil;
-    F.dvsoil[c] = dvsoil;
-    F.dlai[c] = -logf(1.f - zveg) / K.CVEG_K;
-    const float zvz0 = F.dmr[c] * zforest + K.VZ0_MIN * (1.f - zforest);
+    npp = dgrow * 0.5f * zgpp * zglacfree;
+    const float zlitter = cveg / K.TAU_VEG;
+    const float zres = fpow(K.Q10, (ts - K.TMELT - 10.f) / 10.f) * csoil / K.TAU_SOIL;
+    cveg = cveg + (npp - zlitter) * DS * K.NCVEG;
+    csoil = csoil + (zlitter - zres) * DS * K.NCVEG;
+    const float zforest = fminf(1.f, fmaxf(0.f, (atanf(cveg - K.CVEG_A) - K.CVEG_E) / (K.CVEG_C - K.CVEG_E)));
+    vsoil = fminf(1.f, fmaxf(0.f, (atanf(cveg - K.CVEG_F) - K.CVEG_G) / (K.CVEG_C - K.CVEG_G)));
+    lai = -logf(1.f - zveg) / K.CVEG_K;
+    const float zvz0 = dmr * zforest + K.VZ0_MIN * (1.f - zforest);
     float zvalb = K.VALB_MIN * zveg + K.VALB_MAX * (1.f - zveg);
-    zwmax = K.VWMAX_MAX * dvsoil + K.VWMAX_MIN * (1.f - dvsoil);
-    float zvrhs = F.dsc[c] * fminf(1.f, fmaxf(0.f, dwatc / (zwmax * K.VWS_CRIT)));
+    zwmax = K.VWMAX_MAX * vsoil + K.VWMAX_MIN * (1.f - vsoil);
+    float zvrhs = dsc * fminf(1.f, fmaxf(0.f, dwatc / (zwmax * K.VWS_CRIT)));
     if (dsnow > 0.f) {
       float zalbsn = (K.ALBSMAX - K.ALBSMIN) * (ts - 263.16f) / (K.TMELT - 263.16f);
       zalbsn = fmaxf(K.ALBSMIN, fminf(K.ALBSMAX, K.ALBSMAX - zalbsn));
@@ -1745,32 +1773,81 @@ __global__ void __launch_bounds__(kBlock) k_land_surface(Model m, const PlanetCo
       zvrhs = 1.f;
     }
     if (K.NVEG == 2.f) {
-      const float z0c = F.dz0climo[c];
-      F.dz0[c] = sqrtf(zvz0 * zvz0 + z0c * z0c);
-      F.dwmax[c] = zwmax;
-      F.drhs[c] = zvrhs;
-      F.dalb[c] = zvalb;
-      F.dforest[c] = zforest;
+      dz0 = sqrtf(zvz0 * zvz0 + z0c * z0c);
+      wmax = zwmax;
+      drhs = zvrhs;
+      put_rhs = true;
+      dalb = zvalb;
+      forest = zforest;
     }
   }
-  if (F.dglac[c] > 0.5f && dls > 0.f) {
+  if (glacier) {
     auto glacier_albedo = [&](float mx, float mn) {
       return fmaxf(mn, fminf(mx, mx - (mx - mn) * (dts - 263.16f) / (K.TMELT - 263.16f)));
     };
-    F.dalb[c] = glacier_albedo(K.ALBGMAX, K.ALBGMIN);
-    F.dsalb[c] = glacier_albedo(K.ALBGMAX1, K.ALBGMIN1);
-    F.dsalb[SN + c] = glacier_albedo(K.ALBGMAX2, K.ALBGMIN2);
-    F.drhs[c] = 1.f;
+    dalb = glacier_albedo(K.ALBGMAX, K.ALBGMIN);
+    dsalb1 = glacier_albedo(K.ALBGMAX1, K.ALBGMIN1);
+    dsalb2 = glacier_albedo(K.ALBGMAX2, K.ALBGMIN2);
+    drhs = 1.f;
+    put_rhs = true;
   }
-  if (K.NGLACIER != 0.f) {
-    const bool lnd = F.dls[c] > 0.5f;
-    if (lnd && F.dsnowz[c] < K.GLACELIM) F.dpersist[c] = 0.f;
-    if (lnd && F.dsnowz[c] < 0.1f) F.dglac[c] = 0.f;
+  float dpersist = dpersist_in, glac = dglac;
+  bool put_persist = false, put_glac = false;
+  if (glaciers) {
+    const bool lnd = dls > 0.5f;
+    if (lnd && dsnowz < K.GLACELIM) {
+      dpersist = 0.f;
+      put_persist = true;
+    }
+    if (lnd && dsnowz < 0.1f) {
+      glac = 0.f;
+      put_glac = true;
+    }
     if (P.surf[6] > 0.5f) {
-      if (F.dpersist[c] > 0.5f) F.dglac[c] = 1.f;
-      F.dpersist[c] = F.dls[c] >= 0.5f ? 1.f : 0.f;
+      if (dpersist > 0.5f) {
+        glac = 1.f;
+        put_glac = true;
+      }
+      dpersist = dls >= 0.5f ? 1.f : 0.f;
+      put_persist = true;
     }
   }
+  F.dalbclim[c] = albclim;
+  F.dalbclim1[c] = albclim1;
+  F.dalbclim2[c] = albclim2;
+  if (land) {
+    F.driver[c] = driver + drunoff * DS;
+    F.land_dtsm[c] = dts;
+    F.land_dqs[c] = dqs;
+    F.dsnow[c] = dsnowz;
+    F.dtsoil[c] = soil[0];
+    F.dtd2[c] = soil[1];
+    F.dtd3[c] = soil[2];
+    F.dtd4[c] = soil[3];
+    F.dtd5[c] = soil[4];
+    F.dt[NL * SN + c] = dts;
+    F.dq[NL * SN + c] = dqs;
+  }
+  if (put_alb) {  // land: the land pass wrote all three albedos, and glaciers lie on land
+    F.dalb[c] = dalb;
+    F.dsalb[c] = dsalb1;
+    F.dsalb[SN + c] = dsalb2;
+  }
+  if (put_rhs) F.drhs[c] = drhs;
+  if (veg) {
+    F.dnpp[c] = npp;
+    F.dcveg[c] = cveg;
+    F.dcsoil[c] = csoil;
+    F.dvsoil[c] = vsoil;
+    F.dlai[c] = lai;
+    if (K.NVEG == 2.f) {
+      F.dz0[c] = dz0;
+      F.dwmax[c] = wmax;
+      F.dforest[c] = forest;
+    }
+  }
+  if (put_persist) F.dpersist[c] = dpersist;
+  if (put_glac) F.dglac[c] = glac;
 }
 
 // seastep coupling and icestep up to getiflx (physics/sea-ice/wgsl/ice.wgsl).
@@ -1922,39 +1999,71 @@ template <int NL>
 __global__ void __launch_bounds__(kBlock) k_sea(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const bool coupled = P.coupled != 0.f;
+  // Every input is read before the first store (the compiler cannot prove
+  // the fields distinct, so a store would order each later load after it);
+  // the values this column stores and reads again stay in registers.
+  const float dls = F.dls[c];
+  const bool open = dls < 0.5f;  // the atmosphere's sea column
+  float xls = 0.f, xcflux = 0.f, xcfluxr = 0.f, zflx_in = 0.f, xiced = 0.f, xicec_in = 0.f, xsnow = 0.f;
+  float xsmelt = 0.f, xsmflx = 0.f, yclsst2 = 0.f, yls = 0.f, ymld = 0.f, yfldo = 0.f, ysst = 0.f, xsndch = 0.f;
+  float snow_old = 0.f, naccua = 0.f;
   if (coupled) {
-    const float xls = F.xls[c];
-    float xcflux = F.xcflux[c], xcfluxr = F.xcfluxr[c];
+    xls = F.xls[c];
+    xcflux = F.xcflux[c];
+    xcfluxr = F.xcfluxr[c];
+    zflx_in = F.ice_zflx[c];
+    xiced = F.xiced[c];
+    xicec_in = F.xicec[c];
+    xsnow = F.xsnow[c];
+    xsmelt = F.xsmelt[c];
+    xsmflx = F.xsmflx[c];
+    yclsst2 = clim14(F.yclsst, P.surf + 3, c, SN);
+    yls = F.yls[c];
+    ymld = F.ymld[c];
+    yfldo = F.yfldo[c];
+    ysst = F.ysst[c];
+    xsndch = F.xsndch[c];
+    snow_old = F.ice_snowold[c];
+  } else {
+    naccua = F.sea_naccua[c];
+  }
+  float dts = 0.f, dicec = 0.f, dp = 0.f, taux = 0.f, tauy = 0.f, heat_sum = 0.f, cprsa = 0.f;
+  if (open) {
+    dts = F.xts[c];
+    dp = F.dp[c];
+    taux = F.dtaux[c];
+    tauy = F.dtauy[c];
+    if (!coupled) {
+      dicec = F.xicec[c];
+      heat_sum = F.dshfl[c] + F.dswfl[NL * SN + c] + F.dlwfl[NL * SN + c] + F.dlhfl[c] + F.sea_cheata[c];
+      cprsa = F.dprs[c] + F.sea_cprsa[c];
+    }
+  }
+  float zsst = 0.f;
+  if (coupled) {
     const double s1 = m.sums[slot * 4 + 2], s2 = m.sums[slot * 4 + 3];
     if (s1 > 0.0 && s2 > 0.0 && xls < 1.f) {
-      float zflx = F.ice_zflx[c];
+      float zflx = zflx_in;
       const float zfac = (float)(s1 / s2);
       if (zfac <= 1.f) zflx = zflx * zfac;
       xcfluxr = xcfluxr - zflx;
       xcflux = xcflux - zflx;
     }
-    F.xcfluxr[c] = xcfluxr;
-    const float xiced = F.xiced[c];
-    const float xicec = F.xicec[c] >= K.THICEC ? 1.f : 0.f;
-    float xsnow = F.xsnow[c], xsmelt = F.xsmelt[c];
-    if (xiced <= 0.f && xsnow > 0.f) {
+    const float xicec = xicec_in >= K.THICEC ? 1.f : 0.f;
+    const bool melt = xiced <= 0.f && xsnow > 0.f;
+    if (melt) {
       const float zcflux = xsnow * 1000.f * K.CLFSN / K.XDT;
       xsmelt = xsmelt + xsnow / K.XDT;
-      F.xsmflx[c] = F.xsmflx[c] + zcflux;
+      xsmflx = xsmflx + zcflux;
       xcflux = xcflux - zcflux;
       xsnow = 0.f;
     }
-    F.xicec[c] = xicec;
-    F.xsnow[c] = xsnow;
-    F.xsmelt[c] = xsmelt;
-    F.xcflux[c] = xcflux;
     const bool sea = xls < 0.5f;
     const float heat = sea ? xcflux : 0.f;
-    F.yclsst2[c] = clim14(F.yclsst, P.surf + 3, c, SN);
-    const float yls = F.yls[c], yiced = F.xiced[c], ymld = F.ymld[c], yfldo = F.yfldo[c];
+    const float yiced = xiced;
     const float zcpsdt = K.DTMIX / (K.CRHOS * K.CPS);
-    const float ysst = F.ysst[c];
-    float zsst = ysst, yiflux = 0.f;
+    float yiflux = 0.f;
+    zsst = ysst;
     if (yls < 1.f && yiced <= 0.f) zsst = zsst + (heat + yfldo) * zcpsdt / ymld;
     if (yls < 1.f && yiced > 0.f) yiflux = yiflux - yfldo - heat;
     if (ysst < K.TFREEZE && yls < 1.f) {
@@ -1966,38 +2075,46 @@ __global__ void __launch_bounds__(kBlock) k_sea(Model m, const PlanetConst* __re
       zsst = zsst + zf * zcpsdt / ymld;
       yiflux = yiflux + zf;
     }
+    if (sea) xsndch = xsndch + (xsnow - snow_old);
+    F.xcfluxr[c] = xcfluxr;
+    if (melt) F.xsmflx[c] = xsmflx;
+    F.xicec[c] = xicec;
+    F.xsnow[c] = xsnow;
+    F.xsmelt[c] = xsmelt;
+    F.xcflux[c] = xcflux;
+    F.yclsst2[c] = yclsst2;
     F.ysst[c] = zsst;
     F.xsst[c] = zsst;
     F.xmld[c] = ymld;
     F.xoheat[c] = -yiflux;
     F.xoflux[c] = -yiflux;
-    if (sea) F.xsndch[c] = F.xsndch[c] + (xsnow - F.ice_snowold[c]);
+    if (sea) F.xsndch[c] = xsndch;
+    dicec = xicec;
   } else {
-    F.sea_naccua[c] = F.sea_naccua[c] + 1.f;
+    F.sea_naccua[c] = naccua + 1.f;
   }
-  if (!(F.dls[c] < 0.5f)) return;
-  const float dts = F.xts[c], dicec = F.xicec[c];
+  if (!open) return;
   if (coupled) {
-    F.sea_dsst[c] = F.xsst[c];
+    F.sea_dsst[c] = zsst;
     F.sea_dts[c] = dts;
-    F.dmld[c] = F.xmld[c];
+    F.dmld[c] = ymld;
     F.dicec[c] = dicec;
-    F.diced[c] = F.xiced[c];
-    F.dsnow[c] = F.xsnow[c];
-    F.dsmelt[c] = F.xsmelt[c];
-    F.dsndch[c] = F.xsndch[c];
+    F.diced[c] = xiced;
+    F.dsnow[c] = xsnow;
+    F.dsmelt[c] = xsmelt;
+    F.dsndch[c] = xsndch;
   } else {
-    F.sea_cheata[c] = F.dshfl[c] + F.dswfl[NL * SN + c] + F.dlwfl[NL * SN + c] + F.dlhfl[c] + F.sea_cheata[c];
-    F.sea_cprsa[c] = F.dprs[c] + F.sea_cprsa[c];
+    F.sea_cheata[c] = heat_sum;
+    F.sea_cprsa[c] = cprsa;
   }
-  const float dp = F.dp[c];
   F.dt[NL * SN + c] = dts;
   float dqs = K.RDBRV * K.RA1 * expf(K.RA2 * (dts - K.TMELT) / (dts - K.RA4)) / dp;
   dqs = dqs / (1.f - (1.f / K.RDBRV - 1.f) * dqs);
   F.sea_dqs[c] = dqs;
   F.dq[NL * SN + c] = dqs;
-  const float taux = F.dtaux[c], tauy = F.dtauy[c];
-  const float zz0 = fmaxf(K.CHARNOCK * sqrtf(taux * taux + tauy * tauy) * K.GASCON * dts / (K.GA * dp), K.DZ0SEA);
+  // The stress magnitude's sum of squares is one explicit fused multiply-add,
+  // so that its rounding does not depend on where the loads above are placed.
+  const float zz0 = fmaxf(K.CHARNOCK * sqrtf(__fmaf_rn(taux, taux, tauy * tauy)) * K.GASCON * dts / (K.GA * dp), K.DZ0SEA);
   F.drhs[c] = K.DRHSSEA * (1.f - dicec) + K.DRHSICE * dicec;
   F.dalb[c] = K.ALBSEA * (1.f - dicec) + dicec * fminf(K.ALBICE, 0.5f + 0.025f * (273.f - dts));
   F.dsalb[c] = K.DOCEANALB1 * (1.f - dicec) + dicec * fminf(K.DICEALBMX1, K.DICEALBMN1 + 0.025f * (273.f - dts));
