@@ -101,12 +101,15 @@ template <int NL>
 __global__ void __launch_bounds__(kBlock) k_fixer_column(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const float* ds = tb + m.to.dsigma;
-  float negative = 0.f, positive = 0.f;
+  // dq stays in registers for the stores below (a reload after each store
+  // would wait for it: the compiler cannot prove the fields distinct)
+  float dq[NL], negative = 0.f, positive = 0.f;
+#pragma unroll
   for (int l = 0; l < NL; ++l) {
-    const float dq = F.dq[l * SN + c];
-    const float q = dq * ds[l];
-    if (dq < 0.f) negative = negative + q;
-    if (dq > 0.f) positive = positive + q;
+    dq[l] = F.dq[l * SN + c];
+    const float q = dq[l] * ds[l];
+    if (dq[l] < 0.f) negative = negative + q;
+    if (dq[l] > 0.f) positive = positive + q;
   }
   const float zgw = m.sh.zgw[h];
   float zneg = -negative * F.dp[c] * zgw;
@@ -118,39 +121,56 @@ __global__ void __launch_bounds__(kBlock) k_fixer_column(Model m, const PlanetCo
     zneg = 0.f;
     zpos = zpos * factor;
   }
-  for (int l = 0; l < NL; ++l) {
-    const float q = F.dq[l * SN + c];
-    F.fixq[l * SN + c] = fixed ? fmaxf(q * factor, 0.f) : q;
-  }
+#pragma unroll
+  for (int l = 0; l < NL; ++l) F.fixq[l * SN + c] = fixed ? fmaxf(dq[l] * factor, 0.f) : dq[l];
   F.fixneg[c] = zneg;
   F.fixpos[c] = zpos;
 }
 
-// physics/fixer/wgsl/row.wgsl: fix1d per latitude row, summed in longitude order.
+// physics/fixer/wgsl/row.wgsl: fix1d per latitude row, summed in longitude
+// order. One warp per row: its lanes stage the row in shared memory with
+// coalesced loads, lane 0 adds the values in longitude order (the shader's
+// sums, bit for bit), and the update of a fixed row runs over all lanes.
+constexpr int kRowWarps = 4;
+constexpr int kMaxNlon = 192;  // NLON at T63, the largest truncation an engine accepts
+
 template <int NL>
-__global__ void k_fixer_row(Model m) {
+__global__ void __launch_bounds__(32 * kRowWarps) k_fixer_row(Model m) {
+  __shared__ float stage[kRowWarps][kMaxNlon];
   const Dims& d = m.d;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= d.S * d.NLAT) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = blockIdx.x * kRowWarps + warp;
+  if (r >= d.S * d.NLAT) return;  // the whole warp
   const int slot = r / d.NLAT;
   if (!m.params[slot].active) return;
   const size_t SN = (size_t)d.S * d.NHOR;
   const FieldPtrs& F = m.f;
   const int first = r * d.NLON;  // slot * NHOR + lat * NLON
-  float zneg = 0.f;
-  for (int j = 0; j < d.NLON; ++j) zneg = zneg + F.fixneg[first + j];
+  float* row = stage[warp];
+  auto ordered_sum = [&](const float* src) {
+    for (int j = lane; j < d.NLON; j += 32) row[j] = src[first + j];
+    __syncwarp();
+    float sum = 0.f;
+    if (lane == 0)
+      for (int j = 0; j < d.NLON; ++j) sum = sum + row[j];
+    sum = __shfl_sync(0xffffffffu, sum, 0);
+    __syncwarp();  // the row buffer is staged again next
+    return sum;
+  };
+  const float zneg = ordered_sum(F.fixneg);
   if (zneg <= 0.f) return;
-  float zpos = 0.f;
-  for (int j = 0; j < d.NLON; ++j) zpos = zpos + F.fixpos[first + j];
+  const float zpos = ordered_sum(F.fixpos);
   if (zpos < zneg) return;
   const float factor = (zpos - zneg) / zpos;
-  for (int j = 0; j < d.NLON; ++j) {
-    for (int l = 0; l < NL; ++l) {
-      float& q = F.fixq[l * SN + first + j];
-      q = fmaxf(q * factor, 0.f);
-    }
+  for (int j = lane; j < d.NLON; j += 32) {
+    float q[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) q[l] = F.fixq[l * SN + first + j];
+    const float pos = F.fixpos[first + j];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) F.fixq[l * SN + first + j] = fmaxf(q[l] * factor, 0.f);
     F.fixneg[first + j] = 0.f;
-    F.fixpos[first + j] = F.fixpos[first + j] * factor;
+    F.fixpos[first + j] = pos * factor;
   }
 }
 
@@ -1487,8 +1507,14 @@ __global__ void __launch_bounds__(kBlock) k_soil(Model m, const PlanetConst* __r
   const float dls = F.dls[c];
   const bool land = dls > 0.f;
   const float snowStart = F.dsnowz[c];
+  // Every input is read before the first store (the compiler cannot prove
+  // the fields distinct, so a store would order each later load after it):
+  // the snow temperature is stored at the end, and the bucket's water and
+  // capacity are read here.
+  const float dwatc_in = land ? F.dwatc[c] : 0.f, dwmax = land ? F.dwmax[c] : 0.f;
   float dwater = 0.f, dsmelt = 0.f;
-  if (snowStart == 0.f) F.dsnowt[c] = K.TMELT;
+  bool put_snowt = snowStart == 0.f;
+  float snowt = K.TMELT;
   if (land) {
     const float glac = F.dglac[c];
     float soilz[NLSOIL], cap[NLSOIL], diff[NLSOIL];
@@ -1554,7 +1580,10 @@ __global__ void __launch_bounds__(kBlock) k_soil(Model m, const PlanetConst* __r
     const bool glacier = F.dglac[c] > 0.5f;
 #pragma unroll
     for (int l = 0; l < NLSOIL; ++l) F.dsoilt[l * SN + c] = glacier ? fminf(ztn[l], K.TMELT) : ztn[l];
-    if (dsnowz > 0.f) F.dsnowt[c] = dts;
+    if (dsnowz > 0.f) {
+      snowt = dts;
+      put_snowt = true;
+    }
     if (K.DSMAX > 0.f && dsnowz > K.DSMAX) {
       zdsnowz = (K.DSMAX - dsnowz) / DS;
       dsnowz = K.DSMAX;
@@ -1572,12 +1601,12 @@ __global__ void __launch_bounds__(kBlock) k_soil(Model m, const PlanetConst* __r
   F.dsmelt[c] = dsmelt;
   float drunoff = 0.f;
   if (land) {
-    const float dwatc = F.dwatc[c] + DS * dwater;
-    const float dwmax = F.dwmax[c];
+    const float dwatc = dwatc_in + DS * dwater;
     drunoff = fmaxf(0.f, dwatc - dwmax) / DS;
     F.dwatc[c] = fmaxf(fminf(dwmax, dwatc), 0.f);
   }
   F.drunoff[c] = drunoff;
+  if (put_snowt) F.dsnowt[c] = snowt;
 }
 
 // mkradv (physics/land/wgsl/mkradv.wgsl): river routing stencil within one
@@ -2316,7 +2345,7 @@ COLUMN_LAUNCHER(Pack, k_pack)
 template <int NL>
 struct FixerRow {
   static void run(const Model& m, cudaStream_t st) {
-    k_fixer_row<NL><<<nblocks((size_t)m.d.S * m.d.NLAT, 64), 64, 0, st>>>(m);
+    k_fixer_row<NL><<<nblocks((size_t)m.d.S * m.d.NLAT, kRowWarps), 32 * kRowWarps, 0, st>>>(m);
   }
 };
 
