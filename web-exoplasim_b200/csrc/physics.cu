@@ -978,8 +978,8 @@ __device__ __forceinline__ Parcel condense(const PlanetConst& K, float t0, float
 
 // mkdqtgp scaling, kuo and mkshallow (physics/precipitation/wgsl/kuo.wgsl).
 // Four resident blocks per SM: with the restrict parameters the compiler
-// keeps more values in registers, and four blocks without spills measured
-// faster than six with them.
+// keeps more values in registers, and four blocks measured faster than six
+// or three.
 template <int NL>
 __global__ void __launch_bounds__(kBlock, 4) k_kuo(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
@@ -1044,6 +1044,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_kuo(Model m, const PlanetConst* _
       }
     }
   }
+  // Both level loops are unrolled: a rolled loop would index the per-level
+  // arrays at run time and keep them in local memory.
+#pragma unroll
   for (int l = NM - 1; l >= 0; --l) {
     const int lp = l + 1;
     if (ilift == -1 && zdqtot[lp] > 0.f) {
@@ -1090,6 +1093,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_kuo(Model m, const PlanetConst* _
       }
     }
   }
+#pragma unroll
   for (int l = NM - 1; l >= 0; --l) {
     if (itop == l + 2) {
       const float p = dp * sg[l];
