@@ -22,6 +22,10 @@ namespace {
 
 constexpr int kBlock = 128;
 
+// Asks L2 for a line this thread reads after its first store, so that load
+// then hits L2 instead of DRAM (a hint: it moves no data into registers).
+__device__ __forceinline__ void prefetch_l2(const float* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // Column kernels take the planet constants and per-planet tables as
 // __restrict__ parameters: both are read-only during a launch, so the
 // compiler may keep their values across the kernel's stores to fields
@@ -1296,6 +1300,18 @@ __global__ void __launch_bounds__(kBlock) k_rain_column(Model m, const PlanetCon
   const float D2 = P.deltsec2;
   const bool skip = F.dca_skip[slot] != 0.f;
   const float dp = F.dp[c];
+  // mkrain's and mkclouds' inputs are read after mklsp's stores; registers
+  // cannot hold them from here, so they are fetched into L2 now.
+#pragma unroll
+  for (int l = 0; l < NL; ++l) {
+    const size_t at = l * SN + c;
+    prefetch_l2(F.dprscl + at);
+    prefetch_l2(F.dprcl + at);
+    prefetch_l2(F.icclev + at);
+    if (K.CLWFAC > 0.f) prefetch_l2(F.dw + at);
+  }
+  prefetch_l2(F.icctot + c);
+  prefetch_l2(F.dt + NL * SN + c);
   float dq_[NL], dt_[NL], dtdt_[NL], dqdt_[NL];
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
