@@ -557,6 +557,11 @@ __device__ __forceinline__ void swr_band(const Model& m, const PlanetConst& K, c
   auto absorption = [&](float x) {
     return BAND == 0 ? ozone_absorption(x, K.ZSOLAR1) : vapour_absorption(x, K.ZSOLAR2);
   };
+  // The downward pass reads each level's cloud water one level ahead; the
+  // column totals below read every other input, so only that one is
+  // fetched into L2 here.
+#pragma unroll
+  for (int l = 0; l < NL; ++l) prefetch_l2(F.dql + l * SN + c);
   // Column totals of the absorber path (slant above the first cloud,
   // diffuse below).
   float pt = 0.f, xpt = 0.f, cs = 1.f;
