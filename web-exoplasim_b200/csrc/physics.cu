@@ -762,9 +762,9 @@ __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
 
 // lwr (physics/radiation/wgsl/lwr.wgsl) then radstep (radstep.wgsl).
 template <int NL>
-// Six blocks per SM (at most 85 registers, no spills): the kernel is latency-bound,
-// and residency hides the field loads at either end of the O(L^2) rows.
-__global__ void __launch_bounds__(kBlock, 6) k_lwr_radstep(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+// Five blocks per SM (at most 102 registers): the kernel is latency-bound;
+// five measured faster than six (239 -> 224 us at 128 planets) or seven.
+__global__ void __launch_bounds__(kBlock, 5) k_lwr_radstep(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE_STAGED
   const int NP = NL + 1;
   const float ZERO = 1.0e-6f, ZFH2O = 0.1f, ZFO3 = 100.f / 2.14f;
