@@ -57,7 +57,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_calcgp(Model m) {
   }
   __syncthreads();
   const int c = blockIdx.x * kBlock + threadIdx.x;
-  const PlanetConst& K = m.pc[slot];
+  // The planet's constants are read once, before the first store (the
+  // compiler cannot prove the fields distinct from them and would reload
+  // each one after every store).
+  const PlanetConst& Kg = m.pc[slot];
+  struct {
+    float AKAP, PSURF, WW, CV, RDBRV, ADV;
+  } const K = {Kg.AKAP, Kg.PSURF, Kg.WW, Kg.CV, Kg.RDBRV, Kg.ADV};
   const size_t SN = (size_t)d.S * d.NHOR;
   const FieldPtrs& F = m.f;
   const float rcsq = m.sh.rcsq[c % d.NHOR];
