@@ -292,3 +292,28 @@ def test_autotuned_shapes_leave_results_unchanged():
     three.step(8)
     for name in ("st", "sz", "sd", "sq", "sp", "fgt", "gu"):
         assert np.array_equal(one.read(0, name), three.read(2, name)), name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [0, 1])
+def test_full_step_equals_its_stages_bitwise(mode):
+    """exogcm_step runs the stages as one graph and skips work whose result no
+    later kernel of the step reads: physics_in's zeroed tendencies (the fixer,
+    surflx, vdiff and physics_out take the zeros unread) and, on the optimized
+    path, the Fourier fields between fused transforms. After one step every
+    other field equals the same stages run one at a time through
+    exogcm_run_stage, which does that work, bit for bit."""
+    from tests.helpers import oracle_field_list
+    p = planets.make_planet(91, truncation=21, levels=10)
+    whole, staged = pkg.Engine(21, 10, 1, mode=mode), pkg.Engine(21, 10, 1, mode=mode)
+    for e in (whole, staged):
+        e.configure(0, p)
+        e.step(3)
+        e.step(4)
+    whole.step(1)
+    for stage in STAGES:
+        staged.run_stage(stage)
+    scratch = {"fgt", "fgd", "fgz", "fgq", "fgp", "fgpj", "fdqt", "fzdekin"} if mode else set()
+    names = [n for n in oracle_field_list() if n not in scratch]
+    differ = [n for n in names if not np.array_equal(whole.read(0, n), staged.read(0, n))]
+    assert not differ, differ
