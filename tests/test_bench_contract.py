@@ -38,9 +38,38 @@ def test_reference_arm_prints_the_contract_line(monkeypatch):
     assert line["config"]["workload"] and line["config"]["planets"] == 2
 
 
-def test_reference_arm_is_silent_on_other_ranks(monkeypatch):
+def test_reference_arm_is_silent_on_other_ranks():
     bench = load_bench()
     out = io.StringIO()
     with contextlib.redirect_stdout(out):
         bench.reference_arm(types.SimpleNamespace(gpus=2, steps=4, warmup=0, impl="reference"), 1)
     assert out.getvalue() == ""
+
+
+def test_roofline_takes_the_dominant_hbm_kernel_and_its_committed_traffic():
+    """roofline() times every kernel of PER_STEP, picks the HBM-bound one with
+    the most time per step, and reports its algorithmic bytes over its launch
+    time against the measured peak (or the fallback), with the DRAM traffic
+    of its committed ncu summary."""
+    bench = load_bench()
+    times = {k: 0.01 for k in bench.PER_STEP}
+    times["fourier_forward"] = 0.0175
+    nbytes = 70123520.0
+
+    class Engine:
+        def time_kernel(self, kernel, reps):
+            return times[kernel], nbytes
+
+    top = max(bench.HBM_BOUND, key=lambda k: times[k] * bench.PER_STEP[k])
+    r = bench.roofline(Engine(), {})
+    assert r["kernel"] == top and r["bound"] == "hbm" and r["unit"] == "GB/s"
+    assert r["peak"] == 6650.0 and r["peak_source"] == "fallback"
+    assert abs(r["achieved"] - nbytes / (times[top] * 1e-3) / 1e9) < 0.1
+    assert r["frac"] == round(r["achieved"] / r["peak"], 4)
+    assert set(r["per_kernel_ms_x_launches_per_step"]) == set(bench.PER_STEP)
+    measured = bench.roofline(Engine(), {"hbm_gbs": 7000.0})
+    assert measured["peak"] == 7000.0 and measured["peak_source"] == "measured"
+    traffic = bench.measured_traffic()
+    for kernel in ("fourier_forward", "fourier_inverse", "sp2gp"):
+        assert traffic.get(kernel, 0) > 0, kernel
+    assert r["traffic"] == traffic.get(top)
