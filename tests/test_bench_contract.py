@@ -73,3 +73,32 @@ def test_roofline_takes_the_dominant_hbm_kernel_and_its_committed_traffic():
     for kernel in ("fourier_forward", "fourier_inverse", "sp2gp"):
         assert traffic.get(kernel, 0) > 0, kernel
     assert r["traffic"] == traffic.get(top)
+
+
+def test_clock_summary_keeps_the_timed_region_and_its_reasons(tmp_path):
+    """The clocks line is the median SM clock of the nvidia-smi rows inside the
+    timed region, with every throttle reason seen Active there; a region
+    shorter than the sampling interval takes the rows on either side."""
+    import datetime
+    bench = load_bench()
+    base = datetime.datetime(2026, 1, 1, 12, 0, 0)
+
+    def at(seconds):
+        return base + datetime.timedelta(seconds=seconds)
+
+    def row(seconds, mhz, power_cap=False):
+        stamp = at(seconds).strftime("%Y/%m/%d %H:%M:%S.%f")[:-3]
+        cap = "Active" if power_cap else "Not Active"
+        return f"{stamp}, {mhz}, 1965, Not Active, Not Active, Not Active, {cap}"
+
+    clocks = bench.Clocks(0)
+    clocks.path = str(tmp_path / "clocks.csv")
+    rows = [row(0.0, 1000), row(1.0, 1965), row(1.05, 1965, power_cap=True), row(1.10, 1800), row(2.0, 1000)]
+    (tmp_path / "clocks.csv").write_text("\n".join(rows) + "\n")
+    clocks.t0, clocks.t1 = at(0.5).timestamp(), at(1.5).timestamp()
+    s = clocks.summary()
+    assert s["sm_mhz"] == 1965 and s["sm_max_mhz"] == 1965 and s["samples"] == 3
+    assert s["reasons"] == ["sw_power_cap"] and s["region_s"] == 1.0
+    clocks.t0, clocks.t1 = at(1.2).timestamp(), at(1.3).timestamp()
+    short = clocks.summary()
+    assert short["samples"] == 2 and short["sm_mhz"] == 1800 and short["reasons"] == []
