@@ -125,8 +125,27 @@ int exogcm_release(exogcm_engine* engine, int slot);
  * stepper/index.ts:203-276): per-step CPU values computed on the host,
  * uploaded once, then the whole batch as one CUDA graph. A slot whose step
  * number is a multiple of `publish_every` packs its snapshot on that step.
- * `steps` must not exceed `publish_every` so a slot publishes at most once. */
+ * `steps` must not exceed `publish_every` so a slot publishes at most once.
+ * Returns when the batch is done (exogcm_step_async + exogcm_wait). */
 int exogcm_step(exogcm_engine* engine, int steps, int publish_every);
+
+/* Submits the same batch and returns at once: the mapAsync-style pipelining
+ * of the reference's worker, which keeps IN_FLIGHT = 2 batches submitted
+ * (runner/webgpu/gcm.worker.ts:215-225, pump/submit :285-346). At most two
+ * batches are in flight; a third call waits for the oldest. While batches
+ * are in flight the engine accepts only exogcm_step_async, exogcm_poll,
+ * exogcm_wait, exogcm_slot_info and the query calls; every other call first
+ * waits for them (exogcm_configure computes the new planet's host set-up
+ * before it waits, so that work overlaps the device's). */
+int exogcm_step_async(exogcm_engine* engine, int steps, int publish_every);
+
+/* *done = 1 when no batch is in flight, else 0; never blocks. Retires
+ * every finished batch (exogcm_last_step_ms then reports the latest), and
+ * returns EXOGCM_EDEVICE if one of them reported a device fault. */
+int exogcm_poll(exogcm_engine* engine, int* done);
+
+/* Blocks until every submitted batch is done. */
+int exogcm_wait(exogcm_engine* engine);
 
 /* Snapshot of a slot published during the last exogcm_step (the 101/76
  * fields of snapshot/index.ts, each NHOR values): returns the step it was
@@ -222,13 +241,18 @@ int exogcm_graph_launches(exogcm_engine* engine, int steps, size_t* launches);
  * (device arrays [slots][points], the layout exogcm_device_field gives for a
  * one-level grid field), in double precision with a fixed order, written as
  * floats to the device array `sums` [2][slots] (first sums, then second).
+ * Every slot given is summed: unlike the step's reductions it does not skip
+ * inactive or uncoupled slots.
  * It calls no allocator: its scratch is a static device array sized for at
  * most 256 slots (1 MiB, held on every GPU that loads the library until the
  * process exits); larger `slots` are rejected with EXOGCM_EINVAL. The first
- * call on a device looks up that array's device address, so make the first
- * call before any stream capture. Every call shares the scratch and keeps
- * the last call's contents; calls that overlap on the GPU race. `stream` is
- * a cudaStream_t (NULL: the legacy default stream). */
+ * call on a device looks up that array's device address, which also commits
+ * the array to the device under CUDA's lazy module loading: a caller with a
+ * fixed footprint makes that first call during its own start-up, and before
+ * any stream capture. After a cudaDeviceReset, reload the library. Every
+ * call shares the scratch and keeps the last call's contents; calls that
+ * overlap on the GPU race. `stream` is a cudaStream_t (NULL: the legacy
+ * default stream). */
 int exogcm_slot_sums_noalloc(const float* first, const float* second, int slots, int points, float* sums,
                              void* stream);
 

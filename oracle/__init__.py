@@ -6,6 +6,11 @@ import this package.  It restates ryoung48/web-exoplasim's GCM set-up
 and drives the timestep in the reference's run order
 (runner/webgpu/gcm.worker.ts:53-176: start-up steps at the start step's date,
 then the main loop).
+
+Oracle(model, precision=32) steps the same loops in sequential f32
+(liboracle32.so): the comparator of the reference's "<= 2x sequential f32"
+and V3 gates (scripts/exoplasim-webgpu/verify-kernels.mjs:273,
+verify-dynamics.mjs:179-181).
 """
 from __future__ import annotations
 
@@ -19,20 +24,22 @@ from . import model_f64, setup_f64
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "build", "liboracle.so")
-_lib = None
+LIB32_PATH = os.path.join(HERE, "build", "liboracle32.so")
+_libs = {}
 
 
 def build():
-    """Compile liboracle.so from oracle.cpp (g++, C++17)."""
+    """Compile liboracle.so (f64) and liboracle32.so (sequential f32) from
+    oracle.cpp (g++, C++17)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
+def lib(precision=64):
+    if precision not in _libs:
+        path = {64: LIB_PATH, 32: LIB32_PATH}[precision]
+        if not os.path.exists(path):
             build()
-        L = ctypes.CDLL(LIB_PATH)
+        L = ctypes.CDLL(path)
         L.ora_create.restype = ctypes.c_void_p
         L.ora_create.argtypes = [ctypes.c_int, ctypes.c_int]
         L.ora_destroy.argtypes = [ctypes.c_void_p]
@@ -44,16 +51,17 @@ def lib():
         L.ora_get.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, dp, ctypes.c_long]
         L.ora_run.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         L.ora_last_error.restype = ctypes.c_char_p
-        _lib = L
-    return _lib
+        _libs[precision] = L
+    return _libs[precision]
 
 
 class Oracle:
-    """One planet stepped in FP64 on the CPU."""
+    """One planet stepped in FP64 (or sequential f32) on the CPU."""
 
-    def __init__(self, model: dict):
+    def __init__(self, model: dict, precision: int = 64):
         self.model = model
-        L = lib()
+        self.precision = precision
+        self.L = L = lib(precision)
         self.h = L.ora_create(model["truncation"], model["levels"])
         if not self.h:
             raise RuntimeError(L.ora_last_error().decode())
@@ -75,18 +83,18 @@ class Oracle:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().ora_destroy(self.h)
+            self.L.ora_destroy(self.h)
             self.h = None
 
     # -- raw access --------------------------------------------------------
     def size(self, name, kind=0):
-        return lib().ora_size(self.h, kind, name.encode())
+        return self.L.ora_size(self.h, kind, name.encode())
 
     def set(self, name, values, kind=0):
         arr = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(-1))
-        if lib().ora_set(self.h, kind, name.encode(), arr.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+        if self.L.ora_set(self.h, kind, name.encode(), arr.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                          arr.size) != 0:
-            raise RuntimeError(lib().ora_last_error().decode())
+            raise RuntimeError(self.L.ora_last_error().decode())
 
     def set_table(self, name, values):
         self.set(name, values, kind=1)
@@ -96,17 +104,17 @@ class Oracle:
         if n < 0:
             raise KeyError(name)
         out = np.zeros(n)
-        if lib().ora_get(self.h, kind, name.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n) != 0:
-            raise RuntimeError(lib().ora_last_error().decode())
+        if self.L.ora_get(self.h, kind, name.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n) != 0:
+            raise RuntimeError(self.L.ora_last_error().decode())
         return out
 
     def set_const(self, name, value):
-        if lib().ora_set_const(self.h, name.encode(), float(value)) != 0:
-            raise RuntimeError(lib().ora_last_error().decode())
+        if self.L.ora_set_const(self.h, name.encode(), float(value)) != 0:
+            raise RuntimeError(self.L.ora_last_error().decode())
 
     def run(self, stage):
-        if lib().ora_run(self.h, stage.encode()) != 0:
-            raise RuntimeError(lib().ora_last_error().decode())
+        if self.L.ora_run(self.h, stage.encode()) != 0:
+            raise RuntimeError(self.L.ora_last_error().decode())
 
     # -- schedule ----------------------------------------------------------
     def set_phase(self, kits):

@@ -7,10 +7,23 @@
 // ryoung48/web-exoplasim (paths relative to src/model/climate/gcm/) as a plain
 // loop over that kernel's threads, evaluated in double precision, in the
 // dispatch order of stepper/index.ts:148-161 and dynamics/index.ts:171-344.
-// State and tables live in named double arrays with the reference's layouts
+// State and tables live in named arrays of `real` with the reference's layouts
 // (spectral [plane][NRSP], Fourier [plane][lat][NFC], grid [plane][NHOR]).
 // The reference's WGSL helpers precise_log/exp/pow/divide/atan are f32
 // accuracy fixes; in f64 they are the plain libm functions.
+//
+// Sequential-f32 mode. Built with -DORACLE_REAL=float and
+// -fsingle-precision-constant (liboracle32.so), the same loops run with every
+// value, constant, table and intermediate in f32 and the f32 libm routines.
+// That is the comparator of the reference's gates
+// (scripts/exoplasim-webgpu/verify-kernels.mjs:273, "<= 2x sequential f32",
+// and verify-dynamics.mjs:179-181, V3: the GPU's error against f64 within
+// twice that of an f32 build replaying the same routine from the same state).
+// The C interface below exchanges doubles in both builds; the f32 build rounds
+// what it is given once, as the GPU's f32 state and tables are rounded.
+#ifndef ORACLE_REAL
+#define ORACLE_REAL double
+#endif
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -22,6 +35,8 @@
 #include "oracle_fields.h"
 
 namespace {
+
+using real = ORACLE_REAL;
 
 // Every kernel constant, under the reference's WGSL override names.
 #define ORACLE_CONSTS(X)                                                                          \
@@ -48,13 +63,13 @@ namespace {
   X(PEARTH) X(WMAX) X(VEARTH) X(PLARAD) X(RAD_EARTHSQ) X(JET) X(SIGMA_LOW)
 
 struct Consts {
-#define DECL(n) double n = 0;
+#define DECL(n) real n = 0;
   ORACLE_CONSTS(DECL)
 #undef DECL
 };
 
 constexpr int MAXL = 32;
-using Vec = std::vector<double>;
+using Vec = std::vector<real>;
 
 struct Model {
   int T, L, NLAT, NLON, NHOR, NTP1, NCSP, NRSP, NFC, NLEV, NLEM, NLEP;
@@ -85,12 +100,12 @@ struct Model {
     }
 #undef MAKE
   }
-  double* F(const char* n) {
+  real* F(const char* n) {
     auto it = state.find(n);
     if (it == state.end()) throw std::runtime_error(std::string("no field ") + n);
     return it->second.data();
   }
-  const double* TB(const char* n) {
+  const real* TB(const char* n) {
     auto it = tables.find(n);
     if (it == tables.end()) throw std::runtime_error(std::string("no table ") + n);
     return it->second.data();
@@ -104,12 +119,12 @@ struct Model {
 // ----------------------------------------------------------------- transforms
 // fourier/wgsl/forward.wgsl:1-18 (gp2fc): c[k] = sum_j table[j][k] g[j].
 void fourier_forward(Model& m, const char* src, const char* dst, int planes) {
-  const double* tab = m.TB("fourier_forward");
-  const double* g = m.F(src);
-  double* c = m.F(dst);
+  const real* tab = m.TB("fourier_forward");
+  const real* g = m.F(src);
+  real* c = m.F(dst);
   for (int row = 0; row < planes * m.NLAT; ++row)
     for (int k = 0; k < m.NFC; ++k) {
-      double s = 0;
+      real s = 0;
       for (int j = 0; j < m.NLON; ++j) s += tab[j * m.NFC + k] * g[row * m.NLON + j];
       c[row * m.NFC + k] = s;
     }
@@ -117,12 +132,12 @@ void fourier_forward(Model& m, const char* src, const char* dst, int planes) {
 
 // fourier/wgsl/inverse.wgsl:1-18 (fc2gp): g[j] = sum_k table[k][j] c[k].
 void fourier_inverse(Model& m, const char* src, const char* dst, int planes) {
-  const double* tab = m.TB("fourier_inverse");
-  const double* c = m.F(src);
-  double* g = m.F(dst);
+  const real* tab = m.TB("fourier_inverse");
+  const real* c = m.F(src);
+  real* g = m.F(dst);
   for (int row = 0; row < planes * m.NLAT; ++row)
     for (int j = 0; j < m.NLON; ++j) {
-      double s = 0;
+      real s = 0;
       for (int k = 0; k < m.NFC; ++k) s += tab[k * m.NLON + j] * c[row * m.NFC + k];
       g[row * m.NLON + j] = s;
     }
@@ -130,12 +145,12 @@ void fourier_inverse(Model& m, const char* src, const char* dst, int planes) {
 
 // fourier/wgsl/dlambda.wgsl:1-17: (re, im) * i m.
 void fourier_dlambda(Model& m, const char* src, const char* dst, int planes) {
-  const double* a = m.F(src);
-  double* b = m.F(dst);
+  const real* a = m.F(src);
+  real* b = m.F(dst);
   for (int i = 0; i < planes * m.NLAT * m.NTP1; ++i) {
     int mm = i % m.NTP1;
     int at = (i / m.NTP1) * m.NFC + 2 * mm;
-    double re = a[at], im = a[at + 1];
+    real re = a[at], im = a[at + 1];
     b[at] = -im * mm;
     b[at + 1] = re * mm;
   }
@@ -153,20 +168,20 @@ static void mode_of(const Model& m, int w, int& mm, int& n) {
 
 // legendre/wgsl/forward.wgsl:1-38 (fc2sp, single-process branch).
 void legendre_forward(Model& m, const char* src, const char* dst, const char* table, int planes) {
-  const double* q = m.TB(table);
-  const double* f = m.F(src);
-  double* s = m.F(dst);
+  const real* q = m.TB(table);
+  const real* f = m.F(src);
+  real* s = m.F(dst);
   for (int p = 0; p < planes; ++p)
     for (int w = 0; w < m.NCSP; ++w) {
       int mm, n;
       mode_of(m, w, mm, n);
-      double sign = (mm + n) % 2 == 0 ? 1.0 : -1.0;
-      const double* four = f + (size_t)p * m.NLAT * m.NFC + 2 * mm;
-      double re = 0, im = 0;
+      real sign = (mm + n) % 2 == 0 ? 1.0 : -1.0;
+      const real* four = f + (size_t)p * m.NLAT * m.NFC + 2 * mm;
+      real re = 0, im = 0;
       for (int l = 0; l < m.NLAT / 2; ++l) {
-        double qq = q[l * m.NCSP + w];
-        const double* north = four + l * m.NFC;
-        const double* south = four + (m.NLAT - 1 - l) * m.NFC;
+        real qq = q[l * m.NCSP + w];
+        const real* north = four + l * m.NFC;
+        const real* south = four + (m.NLAT - 1 - l) * m.NFC;
         re += qq * (north[0] + sign * south[0]);
         im += qq * (north[1] + sign * south[1]);
       }
@@ -177,18 +192,18 @@ void legendre_forward(Model& m, const char* src, const char* dst, const char* ta
 
 // legendre/wgsl/inverse.wgsl:1-27 (sp2fc, sp2fcdmu).
 void legendre_inverse(Model& m, const char* src, const char* dst, const char* table, int planes) {
-  const double* q = m.TB(table);
-  const double* s = m.F(src);
-  double* f = m.F(dst);
+  const real* q = m.TB(table);
+  const real* s = m.F(src);
+  real* f = m.F(dst);
   for (int i = 0; i < planes * m.NLAT * m.NTP1; ++i) {
     int mm = i % m.NTP1;
     int row = i / m.NTP1;
     int plane = row / m.NLAT, lat = row % m.NLAT;
     int first = mm * (2 * m.NTP1 - mm + 1) / 2;
-    const double* sp = s + (size_t)plane * m.NRSP;
-    double re = 0, im = 0;
+    const real* sp = s + (size_t)plane * m.NRSP;
+    real re = 0, im = 0;
     for (int w = first; w < first + m.NTP1 - mm; ++w) {
-      double qq = q[lat * m.NCSP + w];
+      real qq = q[lat * m.NCSP + w];
       re += qq * sp[2 * w];
       im += qq * sp[2 * w + 1];
     }
@@ -199,25 +214,25 @@ void legendre_inverse(Model& m, const char* src, const char* dst, const char* ta
 
 // legendre/wgsl/dv2uv.wgsl:1-43.
 void legendre_dv2uv(Model& m, const char* dname, const char* zname, const char* uname,
-                    const char* vname, int planes, double plavor) {
-  const double* qu = m.TB("legendre_qu");
-  const double* qv = m.TB("legendre_qv");
-  const double* D = m.F(dname);
-  const double* Z = m.F(zname);
-  double* U = m.F(uname);
-  double* V = m.F(vname);
+                    const char* vname, int planes, real plavor) {
+  const real* qu = m.TB("legendre_qu");
+  const real* qv = m.TB("legendre_qv");
+  const real* D = m.F(dname);
+  const real* Z = m.F(zname);
+  real* U = m.F(uname);
+  real* V = m.F(vname);
   for (int i = 0; i < planes * m.NLAT * m.NTP1; ++i) {
     int mm = i % m.NTP1;
     int row = i / m.NTP1;
     int plane = row / m.NLAT, lat = row % m.NLAT;
     int first = mm * (2 * m.NTP1 - mm + 1) / 2;
-    const double* d = D + (size_t)plane * m.NRSP;
-    const double* z = Z + (size_t)plane * m.NRSP;
-    double ure = 0, uim = 0, vre = 0, vim = 0;
+    const real* d = D + (size_t)plane * m.NRSP;
+    const real* z = Z + (size_t)plane * m.NRSP;
+    real ure = 0, uim = 0, vre = 0, vim = 0;
     for (int w = first; w < first + m.NTP1 - mm; ++w) {
-      double a = qu[lat * m.NCSP + w], b = qv[lat * m.NCSP + w];
-      double zre = w == 1 ? z[2 * w] - plavor : z[2 * w];
-      double zim = z[2 * w + 1], dre = d[2 * w], dim = d[2 * w + 1];
+      real a = qu[lat * m.NCSP + w], b = qv[lat * m.NCSP + w];
+      real zre = w == 1 ? z[2 * w] - plavor : z[2 * w];
+      real zim = z[2 * w + 1], dre = d[2 * w], dim = d[2 * w + 1];
       ure = ure + b * zre + a * dim;
       uim = uim + b * zim - a * dre;
       vre = vre + a * zim - b * dre;
@@ -234,30 +249,30 @@ void legendre_dv2uv(Model& m, const char* dname, const char* zname, const char* 
 // legendre/wgsl/uv2dv.wgsl:1-63 (uv2dv; mktend's with the kinetic term).
 void legendre_uv2dv(Model& m, const char* uname, const char* vname, const char* kname,
                     const char* dname, const char* zname, int planes) {
-  const double* qe = m.TB("legendre_qe");
-  const double* qm = m.TB("legendre_qm");
-  const double* qqt = m.TB("legendre_qq");
-  const double* U = m.F(uname);
-  const double* V = m.F(vname);
-  const double* K = kname ? m.F(kname) : nullptr;
-  double* D = m.F(dname);
-  double* Z = m.F(zname);
+  const real* qe = m.TB("legendre_qe");
+  const real* qm = m.TB("legendre_qm");
+  const real* qqt = m.TB("legendre_qq");
+  const real* U = m.F(uname);
+  const real* V = m.F(vname);
+  const real* K = kname ? m.F(kname) : nullptr;
+  real* D = m.F(dname);
+  real* Z = m.F(zname);
   for (int p = 0; p < planes; ++p)
     for (int w = 0; w < m.NCSP; ++w) {
       int mm, n;
       mode_of(m, w, mm, n);
-      double s = (mm + n) % 2 == 0 ? 1.0 : -1.0;
+      real s = (mm + n) % 2 == 0 ? 1.0 : -1.0;
       size_t column = (size_t)p * m.NLAT * m.NFC + 2 * mm;
-      double dre = 0, dim = 0, zre = 0, zim = 0;
+      real dre = 0, dim = 0, zre = 0, zim = 0;
       for (int l = 0; l < m.NLAT / 2; ++l) {
         size_t north = column + l * m.NFC, south = column + (m.NLAT - 1 - l) * m.NFC;
-        double e = qe[l * m.NCSP + w], mq = qm[l * m.NCSP + w];
-        double dure = U[north] - s * U[south], duim = U[north + 1] - s * U[south + 1];
-        double dvre = V[north] - s * V[south], dvim = V[north + 1] - s * V[south + 1];
-        double sure = U[north] + s * U[south], suim = U[north + 1] + s * U[south + 1];
-        double svre = V[north] + s * V[south], svim = V[north + 1] + s * V[south + 1];
+        real e = qe[l * m.NCSP + w], mq = qm[l * m.NCSP + w];
+        real dure = U[north] - s * U[south], duim = U[north + 1] - s * U[south + 1];
+        real dvre = V[north] - s * V[south], dvim = V[north + 1] - s * V[south + 1];
+        real sure = U[north] + s * U[south], suim = U[north + 1] + s * U[south + 1];
+        real svre = V[north] + s * V[south], svim = V[north + 1] + s * V[south + 1];
         if (K) {
-          double q2 = qqt[l * m.NCSP + w];
+          real q2 = qqt[l * m.NCSP + w];
           dre = dre + q2 * (K[north] + s * K[south]);
           dim = dim + q2 * (K[north + 1] + s * K[south + 1]);
         }
@@ -277,23 +292,23 @@ void legendre_uv2dv(Model& m, const char* uname, const char* vname, const char* 
 // legendre/wgsl/qtend.wgsl:1-46.
 void legendre_qtend(Model& m, const char* uname, const char* vname, const char* srcname,
                     const char* dst, int planes) {
-  const double* qe = m.TB("legendre_qe");
-  const double* qc = m.TB("legendre_qc");
-  const double* qm = m.TB("legendre_qm");
-  const double* U = m.F(uname);
-  const double* V = m.F(vname);
-  const double* Sx = m.F(srcname);
-  double* out = m.F(dst);
+  const real* qe = m.TB("legendre_qe");
+  const real* qc = m.TB("legendre_qc");
+  const real* qm = m.TB("legendre_qm");
+  const real* U = m.F(uname);
+  const real* V = m.F(vname);
+  const real* Sx = m.F(srcname);
+  real* out = m.F(dst);
   for (int p = 0; p < planes; ++p)
     for (int w = 0; w < m.NCSP; ++w) {
       int mm, n;
       mode_of(m, w, mm, n);
-      double s = (mm + n) % 2 == 0 ? 1.0 : -1.0;
+      real s = (mm + n) % 2 == 0 ? 1.0 : -1.0;
       size_t column = (size_t)p * m.NLAT * m.NFC + 2 * mm;
-      double re = 0, im = 0;
+      real re = 0, im = 0;
       for (int l = 0; l < m.NLAT / 2; ++l) {
         size_t north = column + l * m.NFC, south = column + (m.NLAT - 1 - l) * m.NFC;
-        double e = qe[l * m.NCSP + w], c = qc[l * m.NCSP + w], mq = qm[l * m.NCSP + w];
+        real e = qe[l * m.NCSP + w], c = qc[l * m.NCSP + w], mq = qm[l * m.NCSP + w];
         re = re + e * (V[north] - s * V[south]) + c * (Sx[north] + s * Sx[south]) +
              mq * (U[north + 1] + s * U[south + 1]);
         im = im + e * (V[north + 1] - s * V[south + 1]) + c * (Sx[north + 1] + s * Sx[south + 1]) -
@@ -309,20 +324,20 @@ void legendre_qtend(Model& m, const char* uname, const char* vname, const char* 
 void calcgp(Model& m) {
   const Consts& K = m.k;
   const int NL = m.NLEV, NH = m.NHOR;
-  const double *rcsqT = m.TB("rcsq"), *t0T = m.TB("t0"), *ds = m.TB("dsigma"), *sh = m.TB("sigmah");
-  const double *rd = m.TB("rdsig"), *t01 = m.TB("t01s2"), *tkpT = m.TB("tkp"), *C = m.TB("c"),
+  const real *rcsqT = m.TB("rcsq"), *t0T = m.TB("t0"), *ds = m.TB("dsigma"), *sh = m.TB("sigmah");
+  const real *rd = m.TB("rdsig"), *t01 = m.TB("t01s2"), *tkpT = m.TB("tkp"), *C = m.TB("c"),
                *G = m.TB("g");
-  double *GP = m.F("gp"), *GPMT = m.F("gpmt"), *GPJ = m.F("gpj"), *GU = m.F("gu"), *GV = m.F("gv"),
+  real *GP = m.F("gp"), *GPMT = m.F("gpmt"), *GPJ = m.F("gpj"), *GU = m.F("gu"), *GV = m.F("gv"),
          *GT = m.F("gt"), *GD = m.F("gd"), *GZ = m.F("gz"), *GQ = m.F("gq");
-  double *GTN = m.F("gtn"), *GQN = m.F("gqn"), *GUZ = m.F("guz"), *GVZ = m.F("gvz"), *DW = m.F("dw"),
+  real *GTN = m.F("gtn"), *GQN = m.F("gqn"), *GUZ = m.F("guz"), *GVZ = m.F("gvz"), *DW = m.F("dw"),
          *GUT = m.F("gut"), *GVT = m.F("gvt"), *GKE = m.F("gke"), *GUQ = m.F("guq"), *GVQ = m.F("gvq"),
          *DU0 = m.F("du0"), *DV0 = m.F("dv0"), *GVPP = m.F("gvpp"), *DP0 = m.F("dp0");
   for (int h = 0; h < NH; ++h) {
-    double rcsq = rcsqT[h];
-    double ps = std::exp(GP[h]);
+    real rcsq = rcsqT[h];
+    real ps = std::exp(GP[h]);
     GP[h] = ps;
-    double gpm = GPMT[h], gpj = GPJ[h];
-    double gu[MAXL], gv[MAXL], gt[MAXL], gd[MAXL], gz[MAXL], gq[MAXL], zvgpg[MAXL], ztv1[MAXL],
+    real gpm = GPMT[h], gpj = GPJ[h];
+    real gu[MAXL], gv[MAXL], gt[MAXL], gd[MAXL], gz[MAXL], gq[MAXL], zvgpg[MAXL], ztv1[MAXL],
         ztv2[MAXL];
     for (int l = 0; l < NL; ++l) {
       int at = l * NH + h;
@@ -333,15 +348,15 @@ void calcgp(Model& m) {
       gz[l] = GZ[at];
       gq[l] = GQ[at];
       zvgpg[l] = rcsq * (gu[l] * gpm + gv[l] * gpj);
-      double zq = std::max(gq[l] / ps, 0.0);
-      double t0 = t0T[l];
-      double tvirt = (gt[l] + t0) * (1.0 + (1.0 / K.RDBRV - 1.0) * zq);
+      real zq = std::max(gq[l] / ps, 0.0);
+      real t0 = t0T[l];
+      real tvirt = (gt[l] + t0) * (1.0 + (1.0 / K.RDBRV - 1.0) * zq);
       ztv1[l] = tvirt - t0;
       ztv2[l] = tvirt / (1.0 + K.ADV * zq) - t0;
     }
-    double zsdotp[MAXL];
-    double zsumd = ds[0] * gd[0];
-    double gvp = ds[0] * zvgpg[0];
+    real zsdotp[MAXL];
+    real zsumd = ds[0] * gd[0];
+    real gvp = ds[0] * zvgpg[0];
     zsdotp[0] = zsumd + gvp;
     for (int l = 1; l < NL - 1; ++l) {
       zsumd = zsumd + ds[l] * gd[l];
@@ -350,7 +365,7 @@ void calcgp(Model& m) {
     }
     zsumd = zsumd + ds[NL - 1] * gd[NL - 1];
     gvp = gvp + ds[NL - 1] * zvgpg[NL - 1];
-    double gtd[MAXL], gqm[MAXL], gud[MAXL], gvd[MAXL];
+    real gtd[MAXL], gqm[MAXL], gud[MAXL], gvd[MAXL];
     for (int l = 0; l < NL - 1; ++l) {
       zsdotp[l] = sh[l] * (zsumd + gvp) - zsdotp[l];
       gtd[l] = zsdotp[l] * (gt[l + 1] - gt[l]);
@@ -358,9 +373,9 @@ void calcgp(Model& m) {
       gud[l] = zsdotp[l] * (gu[l + 1] - gu[l]);
       gvd[l] = zsdotp[l] * (gv[l + 1] - gv[l]);
     }
-    double gtn[MAXL], gqn[MAXL], guz[MAXL], gvz[MAXL], dw[MAXL];
+    real gtn[MAXL], gqn[MAXL], guz[MAXL], gvz[MAXL], dw[MAXL];
     zsumd = zvgpg[0] * ds[0];
-    double rdsig0 = rd[0];
+    real rdsig0 = rd[0];
     gtn[0] = gt[0] * gd[0] - K.AKAP * ztv2[0] * gd[0] -
              rdsig0 * (gtd[0] + t01[0] * (sh[0] * gvp - zsumd));
     gqn[0] = -rdsig0 * gqm[0];
@@ -369,14 +384,14 @@ void calcgp(Model& m) {
     dw[0] = gd[0] * ps * K.PSURF * K.WW;
     for (int l = 1; l < NL; ++l) {
       int column = l * NL;
-      double ztpta = C[column] * zvgpg[0];
-      double ztptb = C[column] * (zvgpg[0] + gd[0]);
+      real ztpta = C[column] * zvgpg[0];
+      real ztptb = C[column] * (zvgpg[0] + gd[0]);
       for (int j = 1; j <= l; ++j) {
         ztpta = ztpta + C[column + j] * zvgpg[j];
         ztptb = ztptb + C[column + j] * (zvgpg[j] + gd[j]);
       }
-      double rdsig = rd[l], t01s2 = t01[l], t01s2m = t01[l - 1], sigmah = sh[l], sigmahm = sh[l - 1];
-      double tkp = tkpT[l];
+      real rdsig = rd[l], t01s2 = t01[l], t01s2m = t01[l - 1], sigmah = sh[l], sigmahm = sh[l - 1];
+      real tkp = tkpT[l];
       if (l < NL - 1) {
         zsumd = zsumd + zvgpg[l] * ds[l];
         gtn[l] = gt[l] * gd[l] + K.AKAP * ztv2[l] * (zvgpg[l] - ztptb) + tkp * (zvgpg[l] - ztpta) -
@@ -394,11 +409,11 @@ void calcgp(Model& m) {
       }
       dw[l] = (zvgpg[l] - ztptb) * ps * K.PSURF * K.WW;
     }
-    double scale = std::sqrt(rcsq);
+    real scale = std::sqrt(rcsq);
     for (int l = 0; l < NL; ++l) {
-      double gsum = 0;
+      real gsum = 0;
       for (int kk = 0; kk < NL; ++kk) gsum = gsum + G[l * NL + kk] * (ztv1[kk] - gt[kk]);
-      double gphi = gsum * 2.0 / rcsq;
+      real gphi = gsum * 2.0 / rcsq;
       int at = l * NH + h;
       GTN[at] = gtn[l];
       GQN[at] = gqn[l];
@@ -422,17 +437,17 @@ void calcgp(Model& m) {
 void spectrala(Model& m) {
   const Consts& K = m.k;
   const int NL = m.NLEV, NR = m.NRSP;
-  const double *G = m.TB("g"), *t0T = m.TB("t0"), *sop = m.TB("sop"), *nidx = m.TB("nindex"),
+  const real *G = m.TB("g"), *t0T = m.TB("t0"), *sop = m.TB("sop"), *nidx = m.TB("nindex"),
                *bm1 = m.TB("bm1"), *ds = m.TB("dsigma"), *tau = m.TB("tau");
-  double *SPM = m.F("spm"), *SPT = m.F("spt"), *SPP = m.F("spp"), *SP = m.F("sp");
-  double *SDM = m.F("sdm"), *SZM = m.F("szm"), *STM = m.F("stm"), *SQM = m.F("sqm"), *SDT = m.F("sdt"),
+  real *SPM = m.F("spm"), *SPT = m.F("spt"), *SPP = m.F("spp"), *SP = m.F("sp");
+  real *SDM = m.F("sdm"), *SZM = m.F("szm"), *STM = m.F("stm"), *SQM = m.F("sqm"), *SDT = m.F("sdt"),
          *STT = m.F("stt"), *SZT = m.F("szt"), *SQT = m.F("sqt"), *SDP = m.F("sdp"), *STP = m.F("stp"),
          *SZP = m.F("szp"), *SQP = m.F("sqp"), *SD = m.F("sd"), *ST = m.F("st"), *SZ = m.F("sz"),
          *SQ = m.F("sq");
   bool filter = K.FILTER != 0;
   for (int s = 0; s < NR; ++s) {
-    double apm = SPM[s];
-    double adm[MAXL], azm[MAXL], atm[MAXL], aqm[MAXL], adt[MAXL], stt[MAXL];
+    real apm = SPM[s];
+    real adm[MAXL], azm[MAXL], atm[MAXL], aqm[MAXL], adt[MAXL], stt[MAXL];
     for (int l = 0; l < NL; ++l) {
       int at = l * NR + s;
       adm[l] = SDM[at];
@@ -442,9 +457,9 @@ void spectrala(Model& m) {
       adt[l] = SDT[at];
       stt[l] = STT[at];
     }
-    double zgt[MAXL], zgm[MAXL];
+    real zgt[MAXL], zgm[MAXL];
     for (int l = 0; l < NL; ++l) {
-      double gt = 0, gm = 0;
+      real gt = 0, gm = 0;
       for (int kk = 0; kk < NL; ++kk) {
         gt = gt + G[l * NL + kk] * stt[kk];
         gm = gm + G[l * NL + kk] * atm[kk];
@@ -452,22 +467,22 @@ void spectrala(Model& m) {
       zgt[l] = gt;
       zgm[l] = gm;
     }
-    double spt = SPT[s];
-    double spm = apm;
-    double so = sop[s];
+    real spt = SPT[s];
+    real spm = apm;
+    real so = sop[s];
     int jn = (int)nidx[s];
-    double sdt[MAXL];
+    real sdt[MAXL];
     for (int l = 0; l < NL; ++l) {
-      double zsum = 0;
+      real zsum = 0;
       if (jn > 0) {
-        double zq = 1.0 / (double)(jn * (jn + 1));
+        real zq = 1.0 / (real)(jn * (jn + 1));
         for (int l2 = 0; l2 < NL; ++l2) {
-          double z0 = t0T[l2];
-          double zt = zgt[l2] - z0 * spt;
-          double zm = zgm[l2] + z0 * spm;
-          double za = adt[l2] * zq + so;
-          double zb = adm[l2] * zq;
-          double zz = zb + K.DELT * (zm + za + K.DELT * zt);
+          real z0 = t0T[l2];
+          real zt = zgt[l2] - z0 * spt;
+          real zm = zgm[l2] + z0 * spm;
+          real za = adt[l2] * zq + so;
+          real zb = adm[l2] * zq;
+          real zz = zb + K.DELT * (zm + za + K.DELT * zt);
           zsum = zsum + zz * bm1[((jn - 1) * NL + l) * NL + l2];
         }
       }
@@ -475,13 +490,13 @@ void spectrala(Model& m) {
     }
     for (int l = 0; l < NL; ++l) spt = spt + ds[l] * sdt[l];
     for (int l = 0; l < NL; ++l) {
-      double t = 0;
+      real t = 0;
       for (int kk = 0; kk < NL; ++kk) t = t + tau[l * NL + kk] * sdt[kk];
       stt[l] = stt[l] - t;
     }
-    double spp = SPP[s];
+    real spp = SPP[s];
     if (filter) SPM[s] = K.PNU21 * spp + K.PNU * apm;
-    double sppNew = s < 2 ? 0.0 : apm - K.DELT2 * spt;
+    real sppNew = s < 2 ? 0.0 : apm - K.DELT2 * spt;
     SPP[s] = sppNew;
     SP[s] = sppNew;
     SPT[s] = spt;
@@ -493,10 +508,10 @@ void spectrala(Model& m) {
         STM[at] = K.PNU21 * STP[at] + K.PNU * atm[l];
         SQM[at] = K.PNU21 * SQP[at] + K.PNU * aqm[l];
       }
-      double sdp = 2.0 * sdt[l] - adm[l];
-      double stp = K.DELT2 * stt[l] + atm[l];
-      double szp = K.DELT2 * SZT[at] + azm[l];
-      double sqp = K.DELT2 * SQT[at] + aqm[l];
+      real sdp = 2.0 * sdt[l] - adm[l];
+      real stp = K.DELT2 * stt[l] + atm[l];
+      real szp = K.DELT2 * SZT[at] + azm[l];
+      real sqp = K.DELT2 * SQT[at] + aqm[l];
       SDT[at] = sdt[l];
       STT[at] = stt[l];
       SDP[at] = sdp;
@@ -515,30 +530,30 @@ void spectrala(Model& m) {
 void spectrald_diffusion(Model& m) {
   const Consts& K = m.k;
   const int NL = m.NLEV, NR = m.NRSP;
-  const double *sak = m.TB("sakpp"), *dampT = m.TB("damp"), *tdt = m.TB("tdisst"), *tdq = m.TB("tdissq"),
+  const real *sak = m.TB("sakpp"), *dampT = m.TB("damp"), *tdt = m.TB("tdisst"), *tdq = m.TB("tdissq"),
                *tdd = m.TB("tdissd"), *tdz = m.TB("tdissz"), *tfr = m.TB("tfrc"), *srp = m.TB("srp");
-  double *SPP = m.F("spp"), *SZP = m.F("szp"), *STP = m.F("stp"), *SDP = m.F("sdp"), *SQP = m.F("sqp"),
+  real *SPP = m.F("spp"), *SZP = m.F("szp"), *STP = m.F("stp"), *SDP = m.F("sdp"), *SQP = m.F("sqp"),
          *SZT = m.F("szt"), *STT = m.F("stt"), *SDT = m.F("sdt"), *SQT = m.F("sqt"),
          *Z1 = m.F("zdsdp1"), *Z2 = m.F("zdszp1"), *Z3 = m.F("zdsdp2"), *Z4 = m.F("zdszp2");
-  const double D2 = K.DELT2;
+  const real D2 = K.DELT2;
   for (int s = 0; s < NR; ++s) {
     if (s < 2) SPP[s] = 0.0;
     for (int l = 0; l < NL; ++l) {
       int at = l * NR + s;
-      double szp = SZP[at] + D2 * SZT[at];
-      double stp = STP[at] + D2 * STT[at];
-      double sdp = SDP[at] + D2 * SDT[at];
-      double sqp = SQP[at] + D2 * SQT[at];
-      double sakpp = sak[at];
-      double damp = dampT[l], tdisst = tdt[l], tdissq = tdq[l], tdissd = tdd[l], tdissz = tdz[l],
+      real szp = SZP[at] + D2 * SZT[at];
+      real stp = STP[at] + D2 * STT[at];
+      real sdp = SDP[at] + D2 * SDT[at];
+      real sqp = SQP[at] + D2 * SQT[at];
+      real sakpp = sak[at];
+      real damp = dampT[l], tdisst = tdt[l], tdissq = tdq[l], tdissd = tdd[l], tdissz = tdz[l],
              tfrc = tfr[l];
-      double stt = ((-damp - tdisst * sakpp) * stp + damp * srp[at]) / (1.0 + D2 * (damp + tdisst * sakpp));
-      double sqt = -tdissq * sakpp * sqp / (1.0 + D2 * tdissq * sakpp);
-      double zsdt1 = -tfrc * sdp / (1.0 + D2 * tfrc);
-      double zsdt2 = -tdissd * sakpp * sdp / (1.0 + D2 * tdissd * sakpp);
-      double zszt1 = -tfrc * szp / (1.0 + D2 * tfrc);
-      double zszt2 = -tdissz * sakpp * szp / (1.0 + D2 * tdissz * sakpp);
-      double szt = zszt1 + zszt2;
+      real stt = ((-damp - tdisst * sakpp) * stp + damp * srp[at]) / (1.0 + D2 * (damp + tdisst * sakpp));
+      real sqt = -tdissq * sakpp * sqp / (1.0 + D2 * tdissq * sakpp);
+      real zsdt1 = -tfrc * sdp / (1.0 + D2 * tfrc);
+      real zsdt2 = -tdissd * sakpp * sdp / (1.0 + D2 * tdissd * sakpp);
+      real zszt1 = -tfrc * szp / (1.0 + D2 * tfrc);
+      real zszt2 = -tdissz * sakpp * szp / (1.0 + D2 * tdissz * sakpp);
+      real szt = zszt1 + zszt2;
       if (s == 2) {
         zszt1 = zszt1 + K.PLAVOR * tfrc / (1.0 + D2 * tfrc);
         zszt2 = zszt2 + K.PLAVOR * tdissz * sakpp / (1.0 + D2 * tdissz * sakpp);
@@ -564,23 +579,23 @@ void spectrald_diffusion(Model& m) {
 void mkdheat(Model& m, int stage) {
   const Consts& K = m.k;
   const int NH = m.NHOR;
-  const double *ds = m.TB("dsigma"), *rcsq = m.TB("rcsq");
-  double *DQ = m.F("dq"), *DP = m.F("dp"), *ZDEKIN = m.F("zdekin"), *ZDTDT = m.F("zdtdt"),
+  const real *ds = m.TB("dsigma"), *rcsq = m.TB("rcsq");
+  real *DQ = m.F("dq"), *DP = m.F("dp"), *ZDEKIN = m.F("zdekin"), *ZDTDT = m.F("zdtdt"),
          *ZU = m.F("zu"), *ZV = m.F("zv"), *ZDU = m.F("zdu"), *ZDV = m.F("zdv");
   for (int i = 0; i < m.NLEV * NH; ++i) {
     int l = i / NH, h = i % NH;
-    double heat = 1.0 + K.ADV * DQ[i];
+    real heat = 1.0 + K.ADV * DQ[i];
     if (stage == 3) {
-      double dp = DP[h];
-      double dtdt = -ZDEKIN[i] * 0.5 / K.ACPD / heat / dp * K.GA / ds[l];
+      real dp = DP[h];
+      real dtdt = -ZDEKIN[i] * 0.5 / K.ACPD / heat / dp * K.GA / ds[l];
       ZDTDT[i] = dtdt / K.CT / K.WW;
       continue;
     }
-    double scale = K.CV * std::sqrt(rcsq[h]);
-    double u = ZU[i] * scale, v = ZV[i] * scale, du = ZDU[i] * scale, dv = ZDV[i] * scale;
-    double change = du * (2.0 * u + du) + dv * (2.0 * v + dv);
+    real scale = K.CV * std::sqrt(rcsq[h]);
+    real u = ZU[i] * scale, v = ZV[i] * scale, du = ZDU[i] * scale, dv = ZDV[i] * scale;
+    real change = du * (2.0 * u + du) + dv * (2.0 * v + dv);
     if (stage == 1) {
-      double dtdt = -change / K.DELTSEC2 * 0.5 / K.ACPD / heat;
+      real dtdt = -change / K.DELTSEC2 * 0.5 / K.ACPD / heat;
       ZDTDT[i] = dtdt / K.CT / K.WW;
     } else {
       ZDEKIN[i] = change / K.DELTSEC2 * DP[h] / K.GA * ds[l];
@@ -590,7 +605,7 @@ void mkdheat(Model& m, int stage) {
 
 // dynamics/wgsl/mean-mode.wgsl:1-13.
 void mean_mode(Model& m, const char* name) {
-  double* t = m.F(name);
+  real* t = m.F(name);
   for (int i = 0; i < m.NLEV * m.NRSP; ++i)
     if (i % m.NRSP != 0) t[i] = 0.0;
 }
@@ -600,23 +615,23 @@ void spectrald_update(Model& m) {
   const Consts& K = m.k;
   const int NL = m.NLEV, NR = m.NRSP;
   bool filter = K.FILTER != 0;
-  double *SPP = m.F("spp"), *SPM = m.F("spm"), *SP = m.F("sp"), *STT = m.F("stt"), *Z1 = m.F("zstt1"),
+  real *SPP = m.F("spp"), *SPM = m.F("spm"), *SP = m.F("sp"), *STT = m.F("stt"), *Z1 = m.F("zstt1"),
          *Z2 = m.F("zstt2"), *SZP = m.F("szp"), *STP = m.F("stp"), *SDP = m.F("sdp"), *SQP = m.F("sqp"),
          *SZT = m.F("szt"), *SDT = m.F("sdt"), *SQT = m.F("sqt"), *SZM = m.F("szm"), *STM = m.F("stm"),
          *SDM = m.F("sdm"), *SQM = m.F("sqm"), *SZ = m.F("sz"), *ST = m.F("st"), *SD = m.F("sd"),
          *SQ = m.F("sq");
   for (int s = 0; s < NR; ++s) {
-    double spp = SPP[s];
+    real spp = SPP[s];
     if (filter) SPM[s] = SPM[s] + K.PNU * spp;
     SP[s] = spp;
     for (int l = 0; l < NL; ++l) {
       int at = l * NR + s;
-      double stt = STT[at] + Z1[at] + Z2[at];
+      real stt = STT[at] + Z1[at] + Z2[at];
       STT[at] = stt;
-      double szp = SZP[at] + K.DELT2 * SZT[at];
-      double stp = STP[at] + K.DELT2 * stt;
-      double sdp = SDP[at] + K.DELT2 * SDT[at];
-      double sqp = SQP[at] + K.DELT2 * SQT[at];
+      real szp = SZP[at] + K.DELT2 * SZT[at];
+      real stp = STP[at] + K.DELT2 * stt;
+      real sdp = SDP[at] + K.DELT2 * SDT[at];
+      real sqp = SQP[at] + K.DELT2 * SQT[at];
       SZP[at] = szp;
       STP[at] = stp;
       SDP[at] = sdp;
@@ -639,15 +654,15 @@ void spectrald_update(Model& m) {
 void physics_in(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR;
-  const double *rcsq = m.TB("rcsq"), *t0 = m.TB("t0");
-  double *GP = m.F("gp"), *DP = m.F("dp"), *DUDT = m.F("dudt"), *DVDT = m.F("dvdt"), *DTDT = m.F("dtdt"),
+  const real *rcsq = m.TB("rcsq"), *t0 = m.TB("t0");
+  real *GP = m.F("gp"), *DP = m.F("dp"), *DUDT = m.F("dudt"), *DVDT = m.F("dvdt"), *DTDT = m.F("dtdt"),
          *DQDT = m.F("dqdt"), *GUDT = m.F("gudt"), *GVDT = m.F("gvdt"), *GTDT = m.F("gtdt"),
          *GQDT = m.F("gqdt"), *DU = m.F("du"), *DV = m.F("dv"), *DT = m.F("dt"), *DQ = m.F("dq"),
          *GU = m.F("gu"), *GV = m.F("gv"), *GT = m.F("gt"), *GQ = m.F("gq");
   for (int h = 0; h < NH; ++h) {
-    double dp = K.PSURF * std::exp(GP[h]);
+    real dp = K.PSURF * std::exp(GP[h]);
     DP[h] = dp;
-    double scale = std::sqrt(rcsq[h]);
+    real scale = std::sqrt(rcsq[h]);
     for (int l = 0; l < m.NLEP; ++l) {
       int at = l * NH + h;
       DUDT[at] = 0;
@@ -672,12 +687,12 @@ void physics_in(Model& m) {
 void physics_out(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR;
-  const double* rcsq = m.TB("rcsq");
-  double *GUDT = m.F("gudt"), *GVDT = m.F("gvdt"), *GTDT = m.F("gtdt"), *GQDT = m.F("gqdt"),
+  const real* rcsq = m.TB("rcsq");
+  real *GUDT = m.F("gudt"), *GVDT = m.F("gvdt"), *GTDT = m.F("gtdt"), *GQDT = m.F("gqdt"),
          *DUDT = m.F("dudt"), *DVDT = m.F("dvdt"), *DTDT = m.F("dtdt"), *DQDT = m.F("dqdt"), *DP = m.F("dp");
   for (int i = 0; i < m.NLEV * NH; ++i) {
     int h = i % NH;
-    double scale = std::sqrt(rcsq[h]);
+    real scale = std::sqrt(rcsq[h]);
     GUDT[i] = DUDT[i] / scale / K.CV / K.WW + GUDT[i];
     GVDT[i] = DVDT[i] / scale / K.CV / K.WW + GVDT[i];
     GTDT[i] = DTDT[i] / K.CT / K.WW + GTDT[i];
@@ -690,19 +705,19 @@ void physics_out(Model& m) {
 void fixer(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NL = m.NLEV;
-  const double *ds = m.TB("dsigma"), *zgw = m.TB("zgw");
-  double *DQ = m.F("dq"), *DP = m.F("dp"), *FIXQ = m.F("fixq"), *FNEG = m.F("fixneg"), *FPOS = m.F("fixpos"),
+  const real *ds = m.TB("dsigma"), *zgw = m.TB("zgw");
+  real *DQ = m.F("dq"), *DP = m.F("dp"), *FIXQ = m.F("fixq"), *FNEG = m.F("fixneg"), *FPOS = m.F("fixpos"),
          *FSUM = m.F("fixsum"), *GQDT = m.F("gqdt");
   for (int h = 0; h < NH; ++h) {
-    double negative = 0, positive = 0;
+    real negative = 0, positive = 0;
     for (int l = 0; l < NL; ++l) {
-      double q = DQ[l * NH + h] * ds[l];
+      real q = DQ[l * NH + h] * ds[l];
       if (DQ[l * NH + h] < 0) negative = negative + q;
       if (DQ[l * NH + h] > 0) positive = positive + q;
     }
-    double zneg = -negative * DP[h] * zgw[h];
-    double zpos = positive * DP[h] * zgw[h];
-    double factor = 1.0;
+    real zneg = -negative * DP[h] * zgw[h];
+    real zpos = positive * DP[h] * zgw[h];
+    real factor = 1.0;
     bool fixed = zneg > 0.0 && zpos >= zneg;
     if (fixed) {
       factor = (zpos - zneg) / zpos;
@@ -710,7 +725,7 @@ void fixer(Model& m) {
       zpos = zpos * factor;
     }
     for (int l = 0; l < NL; ++l) {
-      double q = DQ[l * NH + h];
+      real q = DQ[l * NH + h];
       FIXQ[l * NH + h] = fixed ? std::max(q * factor, 0.0) : q;
     }
     FNEG[h] = zneg;
@@ -718,35 +733,35 @@ void fixer(Model& m) {
   }
   for (int row = 0; row < m.NLAT; ++row) {
     int first = row * m.NLON;
-    double zneg = 0;
+    real zneg = 0;
     for (int j = 0; j < m.NLON; ++j) zneg = zneg + FNEG[first + j];
     if (zneg <= 0) continue;
-    double zpos = 0;
+    real zpos = 0;
     for (int j = 0; j < m.NLON; ++j) zpos = zpos + FPOS[first + j];
     if (zpos < zneg) continue;
-    double factor = (zpos - zneg) / zpos;
+    real factor = (zpos - zneg) / zpos;
     for (int j = 0; j < m.NLON; ++j) {
       for (int l = 0; l < NL; ++l) {
-        double& q = FIXQ[l * NH + first + j];
+        real& q = FIXQ[l * NH + first + j];
         q = std::max(q * factor, 0.0);
       }
       FNEG[first + j] = 0;
       FPOS[first + j] = FPOS[first + j] * factor;
     }
   }
-  double a = 0, b = 0;
+  real a = 0, b = 0;
   for (int h = 0; h < NH; ++h) {
     a += FNEG[h];
     b += FPOS[h];
   }
   FSUM[0] = a;
   FSUM[1] = b;
-  double zzneg = FSUM[0], zzpos = FSUM[1];
+  real zzneg = FSUM[0], zzpos = FSUM[1];
   for (int h = 0; h < NH; ++h) {
-    double dp = DP[h];
+    real dp = DP[h];
     for (int l = 0; l < NL; ++l) {
       int at = l * NH + h;
-      double q = FIXQ[at];
+      real q = FIXQ[at];
       if (zzneg > 0) q = std::max(q * ((zzpos - zzneg) / zzpos), 0.0);
       GQDT[at] = GQDT[at] + dp * (q - DQ[at]) / K.DELT2 / K.PSURF;
       DQ[at] = q;
@@ -759,111 +774,111 @@ void fixer(Model& m) {
 void surflx(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, low = m.NLEV - 1;
-  const double dsigma = m.TB("dsigma")[low], zfac = m.TB("flux_sigfac")[0], zlnsig = m.TB("flux_lnsig")[0];
-  double *DU = m.F("du"), *DV = m.F("dv"), *DT = m.F("dt"), *DQ = m.F("dq"), *DP = m.F("dp"),
+  const real dsigma = m.TB("dsigma")[low], zfac = m.TB("flux_sigfac")[0], zlnsig = m.TB("flux_lnsig")[0];
+  real *DU = m.F("du"), *DV = m.F("dv"), *DT = m.F("dt"), *DQ = m.F("dq"), *DP = m.F("dp"),
          *DLS = m.F("dls"), *DZ0 = m.F("dz0"), *DTRANSH = m.F("dtransh"), *DTRANSM = m.F("dtransm"),
          *DUDT = m.F("dudt"), *DVDT = m.F("dvdt"), *DTDT = m.F("dtdt"), *DQDT = m.F("dqdt"),
          *DTAUX = m.F("dtaux"), *DTAUY = m.F("dtauy"), *DUST3 = m.F("dust3"), *DSHFL = m.F("dshfl"),
          *DSHDT = m.F("dshdt"), *DTSA = m.F("dtsa"), *DRHS = m.F("drhs"), *DWATC = m.F("dwatc"),
          *DEVAP = m.F("devap"), *DLHFL = m.F("dlhfl"), *DLHDT = m.F("dlhdt");
-  const double VK = 0.4, moisture = 1.0 / K.RDBRV - 1.0;
+  const real VK = 0.4, moisture = 1.0 / K.RDBRV - 1.0;
   for (int h = 0; h < NH; ++h) {
     int lo = low * NH + h, sf = m.NLEV * NH + h;
-    double u = DU[lo], v = DV[lo], t = DT[lo], q = DQ[lo], ts = DT[sf], qs = DQ[sf], dp = DP[h],
+    real u = DU[lo], v = DV[lo], t = DT[lo], q = DQ[lo], ts = DT[sf], qs = DQ[sf], dp = DP[h],
            dls = DLS[h];
-    double dtsa = t * zfac * (1.0 + moisture * q);
-    double zabsu2 = std::max(K.ZUMIN, u * u + v * v);
-    double znl = -K.GASCON * 0.5 * (t + dtsa) * zlnsig / K.GA;
-    double zbz0 = znl / DZ0[h];
-    double zri = K.GA * znl / (zabsu2 * dtsa) * (dtsa - ts * (1.0 + moisture * qs));
-    double zkblnz = VK / std::log(zbz0 + 1.0);
-    double zkblnz2 = zkblnz * zkblnz;
-    double zrifm, zrifh;
+    real dtsa = t * zfac * (1.0 + moisture * q);
+    real zabsu2 = std::max(K.ZUMIN, u * u + v * v);
+    real znl = -K.GASCON * 0.5 * (t + dtsa) * zlnsig / K.GA;
+    real zbz0 = znl / DZ0[h];
+    real zri = K.GA * znl / (zabsu2 * dtsa) * (dtsa - ts * (1.0 + moisture * qs));
+    real zkblnz = VK / std::log(zbz0 + 1.0);
+    real zkblnz2 = zkblnz * zkblnz;
+    real zrifm, zrifh;
     if (zri <= 0.0) {
-      double zdenom = 1.0 + 3.0 * K.VDIFF_C * K.VDIFF_B * std::sqrt(-1.0 * zri * (zbz0 + 1.0)) * zkblnz2;
+      real zdenom = 1.0 + 3.0 * K.VDIFF_C * K.VDIFF_B * std::sqrt(-1.0 * zri * (zbz0 + 1.0)) * zkblnz2;
       zrifm = 1.0 - 2.0 * K.VDIFF_B * zri / zdenom;
       if (dls < 1.0) {
-        double zdth = -(dtsa - ts * (1.0 + moisture * qs));
+        real zdth = -(dtsa - ts * (1.0 + moisture * qs));
         zrifh = std::pow(1.0 + std::pow(0.0016 * std::cbrt(zdth) / std::sqrt(zabsu2) / zkblnz2, 1.25), 0.8);
       } else {
         zrifh = 1.0 - 3.0 * K.VDIFF_B * zri / zdenom;
       }
     } else {
-      double zdenom = std::sqrt(1.0 + K.VDIFF_D * zri);
+      real zdenom = std::sqrt(1.0 + K.VDIFF_D * zri);
       zrifh = 1.0 / (1.0 + 3.0 * K.VDIFF_B * zri * zdenom);
       zrifm = 1.0 / (1.0 + 2.0 * K.VDIFF_B * zri / zdenom);
     }
-    double ztrans = std::sqrt(zabsu2) * zkblnz2;
-    double transh = ztrans * zrifh, transm = ztrans * zrifm;
+    real ztrans = std::sqrt(zabsu2) * zkblnz2;
+    real transh = ztrans * zrifh, transm = ztrans * zrifm;
     DTRANSH[h] = transh;
     DTRANSM[h] = transm;
-    double zkonst1 = K.GA * K.DELTSEC2 / (K.GASCON * dsigma);
-    double zkonst2 = dsigma / K.DELTSEC2 / K.GA;
-    double zkdiffm = zkonst1 * transm / ts;
-    double zun = u / (1.0 + zkdiffm), zvn = v / (1.0 + zkdiffm);
+    real zkonst1 = K.GA * K.DELTSEC2 / (K.GASCON * dsigma);
+    real zkonst2 = dsigma / K.DELTSEC2 / K.GA;
+    real zkdiffm = zkonst1 * transm / ts;
+    real zun = u / (1.0 + zkdiffm), zvn = v / (1.0 + zkdiffm);
     DUDT[lo] = DUDT[lo] + (zun - u) / K.DELTSEC2;
     DVDT[lo] = DVDT[lo] + (zvn - v) / K.DELTSEC2;
-    double dtdt = DTDT[lo];
+    real dtdt = DTDT[lo];
     if (K.NDHEAT != 0)
       dtdt = dtdt + -(zun * zun - u * u + zvn * zvn - v * v) / K.DELTSEC2 * 0.5 / K.ACPD / (1.0 + K.ADV * q);
-    double taux = dp * zkonst2 * zkdiffm * zun, tauy = dp * zkonst2 * zkdiffm * zvn;
+    real taux = dp * zkonst2 * zkdiffm * zun, tauy = dp * zkonst2 * zkdiffm * zvn;
     DTAUX[h] = taux;
     DTAUY[h] = tauy;
-    double ustar = std::sqrt(std::sqrt(taux * taux + tauy * tauy) * K.GASCON * ts / dp);
+    real ustar = std::sqrt(std::sqrt(taux * taux + tauy * tauy) * K.GASCON * ts / dp);
     DUST3[h] = ustar * ustar * ustar;
-    double zkdiffh = zkonst1 * transh / ts;
-    double ztn = (t + zkdiffh * ts) / (1.0 + zkdiffh * zfac);
+    real zkdiffh = zkonst1 * transh / ts;
+    real ztn = (t + zkdiffh * ts) / (1.0 + zkdiffh * zfac);
     dtdt = dtdt + (ztn - t) / K.DELTSEC2;
     DTDT[lo] = dtdt;
-    double moist = std::max(1.0, 1.0 + K.ADV * q);
+    real moist = std::max(1.0, 1.0 + K.ADV * q);
     DSHFL[h] = zkonst2 * zkdiffh * dp * K.ACPD * moist * (ztn * zfac - ts);
     DSHDT[h] = -1.0 * zkonst2 * zkdiffh * dp * K.ACPD * moist;
     dtsa = ztn * zfac;
     DTSA[h] = dtsa;
-    double zkdiffq = DRHS[h] * zkonst1 * transh / ts;
-    double zqn = std::max(q, (q + zkdiffq * qs) / (1.0 + zkdiffq));
+    real zkdiffq = DRHS[h] * zkonst1 * transh / ts;
+    real zqn = std::max(q, (q + zkdiffq * qs) / (1.0 + zkdiffq));
     if (dls > 0.0) zqn = std::min(zqn, DWATC[h] / K.DELTSEC * 1000.0 / dp / zkonst2 + q);
     DQDT[lo] = DQDT[lo] + (zqn - q) / K.DELTSEC2;
-    double devap = -dp * zkonst2 / 1000.0 * (zqn - q);
+    real devap = -dp * zkonst2 / 1000.0 * (zqn - q);
     DEVAP[h] = devap;
-    double latent = (ts > K.TMELT || dls < 0.5) ? K.ALV : K.ALS;
-    double dlhfl = devap * latent * 1000.0;
+    real latent = (ts > K.TMELT || dls < 0.5) ? K.ALV : K.ALS;
+    real dlhfl = devap * latent * 1000.0;
     DLHFL[h] = dlhfl;
-    double curvature = (ts - K.RA4) * (ts - K.RA4);
-    double dlhdt = -1.0 * latent * zkdiffq * zkonst2 * dp * K.RA2 * (K.TMELT - K.RA4) * qs / curvature;
+    real curvature = (ts - K.RA4) * (ts - K.RA4);
+    real dlhdt = -1.0 * latent * zkdiffq * zkonst2 * dp * K.RA2 * (K.TMELT - K.RA4) * qs / curvature;
     DLHDT[h] = dlhfl == 0.0 ? 0.0 : dlhdt;
   }
 }
 
 // physics/diffusion/wgsl/implicit.wgsl:1-24 (diffuse).
-static void diffuse(int NL, const double* ds, double* x, const double* k) {
-  double ebs[MAXL];
-  double ds0 = ds[0];
+static void diffuse(int NL, const real* ds, real* x, const real* k) {
+  real ebs[MAXL];
+  real ds0 = ds[0];
   ebs[0] = k[0] / (ds0 + k[0]);
   x[0] = ds0 * x[0] / (ds0 + k[0]);
   for (int l = 1; l < NL - 1; ++l) {
-    double den = ds[l] + k[l] + k[l - 1] * (1.0 - ebs[l - 1]);
+    real den = ds[l] + k[l] + k[l - 1] * (1.0 - ebs[l - 1]);
     ebs[l] = k[l] / den;
     x[l] = (x[l] * ds[l] + k[l - 1] * x[l - 1]) / den;
   }
-  double dsn = ds[NL - 1];
+  real dsn = ds[NL - 1];
   x[NL - 1] = (x[NL - 1] * dsn + k[NL - 2] * x[NL - 2]) / (dsn + k[NL - 2] * (1.0 - ebs[NL - 2]));
   for (int l = NL - 2; l >= 0; --l) x[l] = x[l] + ebs[l] * x[l + 1];
 }
 
 // physics/diffusion/wgsl/implicit.wgsl:26-47 (diffuse_potential).
-static void diffuse_potential(int NL, const double* ds, double* x, const double* k, const double* skap) {
-  double ebs[MAXL];
-  double ds0 = ds[0];
+static void diffuse_potential(int NL, const real* ds, real* x, const real* k, const real* skap) {
+  real ebs[MAXL];
+  real ds0 = ds[0];
   ebs[0] = k[0] / (ds0 + k[0] / skap[0]);
   x[0] = ds0 * x[0] / (ds0 + k[0] / skap[0]);
   for (int l = 1; l < NL - 1; ++l) {
-    double den = ds[l] + (k[l] + k[l - 1] * (1.0 - ebs[l - 1] / skap[l - 1])) / skap[l];
+    real den = ds[l] + (k[l] + k[l - 1] * (1.0 - ebs[l - 1] / skap[l - 1])) / skap[l];
     ebs[l] = k[l] / den;
     x[l] = (x[l] * ds[l] + k[l - 1] / skap[l - 1] * x[l - 1]) / den;
   }
   int last = NL - 1;
-  double dsn = ds[last];
+  real dsn = ds[last];
   x[last] = (x[last] * dsn + k[NL - 2] * x[NL - 2] / skap[NL - 2]) /
             (dsn + k[NL - 2] / skap[last] * (1.0 - ebs[NL - 2] / skap[NL - 2]));
   for (int l = NL - 2; l >= 0; --l) x[l] = x[l] + ebs[l] * x[l + 1] / skap[l + 1];
@@ -873,17 +888,17 @@ static void diffuse_potential(int NL, const double* ds, double* x, const double*
 void vdiff(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NL = m.NLEV;
-  const double *ds = m.TB("dsigma"), *sh = m.TB("sigmah"), *skapT = m.TB("vdiff_skap"),
+  const real *ds = m.TB("dsigma"), *sh = m.TB("sigmah"), *skapT = m.TB("vdiff_skap"),
                *skaphT = m.TB("vdiff_skaph"), *mixh2 = m.TB("vdiff_mixh2"), *mixm2 = m.TB("vdiff_mixm2"),
                *rdsg = m.TB("vdiff_rdsig"), *sh3 = m.TB("vdiff_sigmah3"), *kfac = m.TB("vdiff_kfac");
-  double *DT = m.F("dt"), *DTDT = m.F("dtdt"), *DQ = m.F("dq"), *DQDT = m.F("dqdt"), *DU = m.F("du"),
+  real *DT = m.F("dt"), *DTDT = m.F("dtdt"), *DQ = m.F("dq"), *DQDT = m.F("dqdt"), *DU = m.F("du"),
          *DUDT = m.F("dudt"), *DV = m.F("dv"), *DVDT = m.F("dvdt");
-  const double zkonst1 = K.GA * K.DELTSEC2 / K.GASCON;
-  const double zkonst2 = zkonst1 * K.GA / K.GASCON;
-  const double zkonst3 = zkonst2 * K.GA / K.GASCON;
-  const double moisture = 1.0 / K.RDBRV - 1.0;
+  const real zkonst1 = K.GA * K.DELTSEC2 / K.GASCON;
+  const real zkonst2 = zkonst1 * K.GA / K.GASCON;
+  const real zkonst3 = zkonst2 * K.GA / K.GASCON;
+  const real moisture = 1.0 / K.RDBRV - 1.0;
   for (int h = 0; h < NH; ++h) {
-    double zt[MAXL], zq[MAXL], zu[MAXL], zv[MAXL], zabsu[MAXL], zskap[MAXL], zskaph[MAXL];
+    real zt[MAXL], zq[MAXL], zu[MAXL], zv[MAXL], zabsu[MAXL], zskap[MAXL], zskaph[MAXL];
     for (int l = 0; l < NL; ++l) {
       int at = l * NH + h;
       zt[l] = DT[at] + DTDT[at] * K.DELTSEC2;
@@ -894,30 +909,30 @@ void vdiff(Model& m) {
       zskap[l] = skapT[l];
       zskaph[l] = skaphT[l];
     }
-    double kh[MAXL] = {0}, km[MAXL] = {0};
+    real kh[MAXL] = {0}, km[MAXL] = {0};
     for (int l = 0; l < NL - 1; ++l) {
       int lp = l + 1;
-      double sigmah = sh[l], dsigma = ds[l], dsigmap = ds[lp];
-      double zmixh2 = mixh2[l], zmixm2 = mixm2[l], zrdsig = rdsg[l], zfac = zkonst3 * sh3[l], zzkfac = kfac[l];
-      double zrthl = (dsigmap + dsigma) / (zt[l] * dsigmap + zt[lp] * dsigma);
-      double zdvds = std::max(K.ZUMIN, std::fabs(zabsu[l] - zabsu[lp])) * zrdsig;
-      double zdthds = (zt[l] * (1.0 + moisture * zq[l]) / zskap[l] - zt[lp] * (1.0 + moisture * zq[lp]) / zskap[lp]) * zrdsig;
-      double zri = zskaph[l] * K.GASCON * zdthds / (sigmah * zdvds * zdvds);
-      double zrifh, zrifm;
+      real sigmah = sh[l], dsigma = ds[l], dsigmap = ds[lp];
+      real zmixh2 = mixh2[l], zmixm2 = mixm2[l], zrdsig = rdsg[l], zfac = zkonst3 * sh3[l], zzkfac = kfac[l];
+      real zrthl = (dsigmap + dsigma) / (zt[l] * dsigmap + zt[lp] * dsigma);
+      real zdvds = std::max(K.ZUMIN, std::fabs(zabsu[l] - zabsu[lp])) * zrdsig;
+      real zdthds = (zt[l] * (1.0 + moisture * zq[l]) / zskap[l] - zt[lp] * (1.0 + moisture * zq[lp]) / zskap[lp]) * zrdsig;
+      real zri = zskaph[l] * K.GASCON * zdthds / (sigmah * zdvds * zdvds);
+      real zrifh, zrifm;
       if (zri <= 0.0) {
-        double dh = 1.0 + 3.0 * K.VDIFF_C * K.VDIFF_B * std::sqrt(-1.0 * zri) * zzkfac * zmixh2;
-        double dm = 1.0 + 3.0 * K.VDIFF_C * K.VDIFF_B * std::sqrt(-1.0 * zri) * zzkfac * zmixm2;
+        real dh = 1.0 + 3.0 * K.VDIFF_C * K.VDIFF_B * std::sqrt(-1.0 * zri) * zzkfac * zmixh2;
+        real dm = 1.0 + 3.0 * K.VDIFF_C * K.VDIFF_B * std::sqrt(-1.0 * zri) * zzkfac * zmixm2;
         zrifh = 1.0 - 3.0 * K.VDIFF_B * zri / dh;
         zrifm = 1.0 - 2.0 * K.VDIFF_B * zri / dm;
       } else {
-        double zdenom = std::sqrt(1.0 + K.VDIFF_D * zri);
+        real zdenom = std::sqrt(1.0 + K.VDIFF_D * zri);
         zrifh = 1.0 / (1.0 + 3.0 * K.VDIFF_B * zri * zdenom);
         zrifm = 1.0 / (1.0 + 2.0 * K.VDIFF_B * zri / zdenom);
       }
       kh[l] = zfac * zmixh2 * zrifh * zdvds * zrthl * zrthl * zrthl;
       km[l] = zfac * zmixm2 * zrifm * zdvds * zrthl * zrthl * zrthl;
     }
-    double zun[MAXL], zvn[MAXL];
+    real zun[MAXL], zvn[MAXL];
     for (int l = 0; l < NL; ++l) {
       zun[l] = zu[l];
       zvn[l] = zv[l];
@@ -930,22 +945,22 @@ void vdiff(Model& m) {
       DVDT[at] = DVDT[at] + (zvn[l] - zv[l]) / K.DELTSEC2;
     }
     if (K.NDHEAT != 0) {
-      double zke[MAXL], zken[MAXL];
+      real zke[MAXL], zken[MAXL];
       for (int l = 0; l < NL; ++l) zke[l] = zken[l] = 0.5 * zabsu[l] * zabsu[l];
       diffuse(NL, ds, zken, km);
       for (int l = 0; l < NL; ++l) {
         int at = l * NH + h;
-        double zdtdt = -((zun[l] * zun[l] - zu[l] * zu[l] + zvn[l] * zvn[l] - zv[l] * zv[l]) / K.DELTSEC2 -
+        real zdtdt = -((zun[l] * zun[l] - zu[l] * zu[l] + zvn[l] * zvn[l] - zv[l] * zv[l]) / K.DELTSEC2 -
                          (zken[l] - zke[l]) / K.DELTSEC2) * 0.5 / K.ACPD / (1.0 + K.ADV * DQ[at]);
         DTDT[at] = DTDT[at] + zdtdt;
       }
     }
-    double zqn[MAXL];
+    real zqn[MAXL];
     for (int l = 0; l < NL; ++l) zqn[l] = zq[l];
     diffuse(NL, ds, zqn, kh);
     for (int l = 0; l < NL; ++l) DQDT[l * NH + h] = DQDT[l * NH + h] + (zqn[l] - zq[l]) / K.DELTSEC2;
     for (int l = 0; l < NL - 1; ++l) kh[l] = kh[l] * zskaph[l];
-    double ztn[MAXL];
+    real ztn[MAXL];
     for (int l = 0; l < NL; ++l) ztn[l] = zt[l];
     diffuse_potential(NL, ds, ztn, kh, zskap);
     for (int l = 0; l < NL; ++l) DTDT[l * NH + h] = DTDT[l * NH + h] + (ztn[l] - zt[l]) / K.DELTSEC2;
@@ -953,21 +968,21 @@ void vdiff(Model& m) {
 }
 
 // ----------------------------------------------------------------- radiation
-constexpr double PI_ = 3.14159265359;
-constexpr double TWOPI_ = PI_ + PI_;
+constexpr real PI_ = 3.14159265359;
+constexpr real TWOPI_ = PI_ + PI_;
 
 // physics/radiation/wgsl/solang.wgsl:1-32.
 void solang(Model& m) {
   const Consts& K = m.k;
-  const double *sid = m.TB("sid"), *cola = m.TB("cola"), *RS = m.F("radiation_step");
-  double* GMU0 = m.F("gmu0");
+  const real *sid = m.TB("sid"), *cola = m.TB("cola"), *RS = m.F("radiation_step");
+  real* GMU0 = m.F("gmu0");
   for (int h = 0; h < m.NHOR; ++h) {
     int lat = h / m.NLON, lon = h % m.NLON;
-    double hangle = RS[2] + lon * K.ZRLON - PI_;
+    real hangle = RS[2] + lon * K.ZRLON - PI_;
     if (hangle < -PI_) hangle = hangle + TWOPI_;
     if (hangle > PI_) hangle = hangle - TWOPI_;
     if (K.NFIXED == 1) hangle = hangle + PI_;
-    double muz = RS[0] * sid[lat] + cola[lat] * RS[1] * std::cos(hangle);
+    real muz = RS[0] * sid[lat] + cola[lat] * RS[1] * std::cos(hangle);
     GMU0[h] = muz > K.ZDAWN ? muz : 0.0;
   }
 }
@@ -976,17 +991,17 @@ void solang(Model& m) {
 void mko3(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR;
-  const double *sidT = m.TB("sid"), *lnsig = m.TB("rad_lnsig"), *ds = m.TB("dsigma"), *RS = m.F("radiation_step");
-  double *DP = m.F("dp"), *DT = m.F("dt"), *DQO3 = m.F("dqo3");
-  const double ZFO3 = 100.0 / 2.14;
+  const real *sidT = m.TB("sid"), *lnsig = m.TB("rad_lnsig"), *ds = m.TB("dsigma"), *RS = m.F("radiation_step");
+  real *DP = m.F("dp"), *DT = m.F("dt"), *DQO3 = m.F("dqo3");
+  const real ZFO3 = 100.0 / 2.14;
   for (int h = 0; h < NH; ++h) {
-    double sid = sidT[h / m.NLON];
-    double za = K.A0O3 + K.A1O3 * std::fabs(sid) + K.ACO3 * sid * RS[4];
-    double dp = DP[h];
-    double o3t = za, zh = 0.0;
+    real sid = sidT[h / m.NLON];
+    real za = K.A0O3 + K.A1O3 * std::fabs(sid) + K.ACO3 * sid * RS[4];
+    real dp = DP[h];
+    real o3t = za, zh = 0.0;
     for (int l = m.NLEV - 1; l >= 1; --l) {
       zh = zh - DT[l * NH + h] * K.GASCON / K.GA * lnsig[l];
-      double o3 = -(za + za * K.ZCONST) / (1.0 + std::exp((zh - K.BO3) / K.CO3)) + o3t;
+      real o3 = -(za + za * K.ZCONST) / (1.0 + std::exp((zh - K.BO3) / K.CO3)) + o3t;
       DQO3[l * NH + h] = o3 * K.GA / (ZFO3 * ds[l] * dp);
       o3t = o3t - o3;
     }
@@ -994,27 +1009,27 @@ void mko3(Model& m) {
   }
 }
 
-static double fpow(double x, double y) { return x == 0.0 ? 0.0 : std::exp(y * std::log(x)); }
+static real fpow(real x, real y) { return x == 0.0 ? 0.0 : std::exp(y * std::log(x)); }
 
 // physics/radiation/wgsl/swr.wgsl:1-276.
 void swr(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NL = m.NLEV;
-  const double *ds = m.TB("dsigma"), *sg = m.TB("sigma"), *RS = m.F("radiation_step");
-  double *GMU0 = m.F("gmu0"), *DFU = m.F("dfu"), *DFD = m.F("dfd"), *DSWFL = m.F("dswfl"), *DP = m.F("dp"),
+  const real *ds = m.TB("dsigma"), *sg = m.TB("sigma"), *RS = m.F("radiation_step");
+  real *GMU0 = m.F("gmu0"), *DFU = m.F("dfu"), *DFD = m.F("dfd"), *DSWFL = m.F("dswfl"), *DP = m.F("dp"),
          *DCC = m.F("dcc"), *DQL = m.F("dql"), *DQO3 = m.F("dqo3"), *DQ = m.F("dq"), *DT = m.F("dt"),
          *DALB = m.F("dalb"), *DSALB = m.F("dsalb"), *DLS = m.F("dls"), *DICEC = m.F("dicec");
-  const double ZERO = 1.0e-6, ZBETTA = 1.66, ZMBAR = 1.9, ZFO3 = 100.0 / 2.14, ZMU00 = 0.5,
+  const real ZERO = 1.0e-6, ZBETTA = 1.66, ZMBAR = 1.9, ZFO3 = 100.0 / 2.14, ZMU00 = 0.5,
                INV_LN10 = 0.43429448190325176;
-  auto ozone = [&](double o3) {
+  auto ozone = [&](real o3) {
     return (0.02118 * o3 / (1.0 + 0.042 * o3 + 0.000323 * (o3 * o3)) + 1.082 * o3 / fpow(1.0 + 138.6 * o3, 0.805) +
             0.0658 * o3 / (1.0 + (103.6 * o3) * (103.6 * o3) * (103.6 * o3))) / K.ZSOLAR1;
   };
-  auto vapour = [&](double wv) { return 2.9 * wv / (fpow(1.0 + 141.5 * wv, 0.635) + 5.925 * wv) / K.ZSOLAR2; };
+  auto vapour = [&](real wv) { return 2.9 * wv / (fpow(1.0 + 141.5 * wv, 0.635) + 5.925 * wv) / K.ZSOLAR2; };
   for (int h = 0; h < NH; ++h) {
-    double mu0 = GMU0[h], gdist2 = RS[3];
-    double ftop1 = K.ZSOLAR1 * K.GSOL0 * gdist2 * mu0;
-    double ftop2 = K.ZSOLAR2 * K.GSOL0 * gdist2 * mu0;
+    real mu0 = GMU0[h], gdist2 = RS[3];
+    real ftop1 = K.ZSOLAR1 * K.GSOL0 * gdist2 * mu0;
+    real ftop2 = K.ZSOLAR2 * K.GSOL0 * gdist2 * mu0;
     if (!(ftop1 + ftop2 > ZERO)) {
       for (int l = 0; l < m.NLEP; ++l) {
         DFU[l * NH + h] = 0;
@@ -1023,26 +1038,26 @@ void swr(Model& m) {
       }
       continue;
     }
-    double dp = DP[h];
-    double rcl1[MAXL], rcl1s[MAXL], rcl2[MAXL], rcl2s[MAXL], tcl2[MAXL], tcl2s[MAXL];
-    double cs = 1.0;
+    real dp = DP[h];
+    real rcl1[MAXL], rcl1s[MAXL], rcl2[MAXL], rcl2s[MAXL], tcl2[MAXL], tcl2s[MAXL];
+    real cs = 1.0;
     for (int l = 0; l < NL; ++l) {
-      double cc = DCC[l * NH + h];
+      real cc = DCC[l * NH + h];
       rcl1[l] = rcl1s[l] = rcl2[l] = rcl2s[l] = 0;
       tcl2[l] = tcl2s[l] = 1;
       if (cc > 0) {
-        double lwp = std::min(1000.0, 1000.0 * DQL[l * NH + h] * dp / K.GA * ds[l]);
-        double tau = 2.0 * fpow(std::log(lwp + 1.5) * INV_LN10, 3.9);
-        double zlog = std::log(1000.0 / tau);
-        double b2 = K.ZB4 / std::log(3.0 + 0.1 * tau);
-        double om0 = std::min(0.9999, 1.0 - K.ZB5 * zlog);
-        double un = 1.0 - om0, uz = un + 2.0 * b2 * om0, u = std::sqrt(uz / un);
-        double ex = std::exp(std::min(25.0, tau * std::sqrt(uz * un) / ZMU00));
-        double r = (u + 1.0) * (u + 1.0) * ex - (u - 1.0) * (u - 1.0) / ex;
+        real lwp = std::min(1000.0, 1000.0 * DQL[l * NH + h] * dp / K.GA * ds[l]);
+        real tau = 2.0 * fpow(std::log(lwp + 1.5) * INV_LN10, 3.9);
+        real zlog = std::log(1000.0 / tau);
+        real b2 = K.ZB4 / std::log(3.0 + 0.1 * tau);
+        real om0 = std::min(0.9999, 1.0 - K.ZB5 * zlog);
+        real un = 1.0 - om0, uz = un + 2.0 * b2 * om0, u = std::sqrt(uz / un);
+        real ex = std::exp(std::min(25.0, tau * std::sqrt(uz * un) / ZMU00));
+        real r = (u + 1.0) * (u + 1.0) * ex - (u - 1.0) * (u - 1.0) / ex;
         rcl1s[l] = 1.0 - 1.0 / (1.0 + K.ZB3 * tau);
         tcl2s[l] = 4.0 * u / r;
         rcl2s[l] = (u * u - 1.0) / r * (ex - 1.0 / ex);
-        double b1 = K.TSWR1 * std::sqrt(mu0);
+        real b1 = K.TSWR1 * std::sqrt(mu0);
         b2 = K.TSWR2 * std::sqrt(mu0) / std::log(3.0 + 0.1 * tau);
         om0 = std::min(0.9999, 1.0 - K.TSWR3 * mu0 * mu0 * zlog);
         un = 1.0 - om0;
@@ -1050,46 +1065,46 @@ void swr(Model& m) {
         u = std::sqrt(uz / un);
         ex = std::exp(std::min(25.0, tau * std::sqrt(uz * un) / mu0));
         r = (u + 1.0) * (u + 1.0) * ex - (u - 1.0) * (u - 1.0) / ex;
-        double direct1 = 1.0 - 1.0 / (1.0 + b1 * tau / mu0);
-        double directT = 4.0 * u / r;
-        double direct2 = (u * u - 1.0) / r * (ex - 1.0 / ex);
+        real direct1 = 1.0 - 1.0 / (1.0 + b1 * tau / mu0);
+        real directT = 4.0 * u / r;
+        real direct2 = (u * u - 1.0) / r * (ex - 1.0 / ex);
         rcl1[l] = cs * direct1 + (1.0 - cs) * rcl1s[l];
         tcl2[l] = cs * directT + (1.0 - cs) * tcl2s[l];
         rcl2[l] = cs * direct2 + (1.0 - cs) * rcl2s[l];
       }
       cs = cs * (1.0 - cc);
     }
-    double zm = 35.0 / std::sqrt(1.0 + 1224.0 * mu0 * mu0);
-    double o3l[MAXL], xo3l[MAXL], wvl[MAXL], ywvl[MAXL];
-    double o3t = 0, xo3t = 0, wvt = 0, ywvt = 0;
+    real zm = 35.0 / std::sqrt(1.0 + 1224.0 * mu0 * mu0);
+    real o3l[MAXL], xo3l[MAXL], wvl[MAXL], ywvl[MAXL];
+    real o3t = 0, xo3t = 0, wvt = 0, ywvt = 0;
     cs = 1.0;
     for (int l = 0; l < NL; ++l) {
-      double dsigma = ds[l];
-      double o3 = ZFO3 * dsigma * dp * DQO3[l * NH + h] / K.GA;
+      real dsigma = ds[l];
+      real o3 = ZFO3 * dsigma * dp * DQO3[l * NH + h] / K.GA;
       o3t = o3t + o3;
       xo3t = cs * (xo3t + zm * o3) + (1.0 - cs) * (xo3t + ZMBAR * o3);
       o3l[l] = o3t;
       xo3l[l] = xo3t;
-      double wv = 0.1 * dsigma * DQ[l * NH + h] * dp / K.GA * std::sqrt(273.0 / DT[l * NH + h]) * sg[l] * dp / 100000.0;
+      real wv = 0.1 * dsigma * DQ[l * NH + h] * dp / K.GA * std::sqrt(273.0 / DT[l * NH + h]) * sg[l] * dp / 100000.0;
       wvt = wvt + wv;
       ywvt = cs * (ywvt + zm * wv) + (1.0 - cs) * (ywvt + ZBETTA * wv);
       wvl[l] = wvt;
       ywvl[l] = ywvt;
       cs = cs * (1.0 - DCC[l * NH + h]);
     }
-    double ta1 = 1, ta1s = 1, ra1 = 0, ra1s = 0, ta2 = 1, ta2s = 1, ra2 = 0, ra2s = 0;
-    double to3t = 1.0, to3tu = 1.0 - ozone(xo3t + ZMBAR * o3t);
-    double twvt = 1.0, twvtu = 1.0 - vapour(ywvt + ZBETTA * wvt);
-    double ccn = DCC[(NL - 1) * NH + h];
-    double scf = K.RCOEFF * dp / 101100.0 * 9.80665 / K.GA;
-    double diffuseRayleigh = 1.0 - std::exp(scf * K.LN_DIFFUSE_RAYLEIGH);
-    double rcsuSurface = diffuseRayleigh * (1.0 - ccn);
-    double rcsSurface = (1.0 - std::exp(scf * std::log(1.0 - 0.219 / (1.0 + 0.816 * mu0)))) * cs +
+    real ta1 = 1, ta1s = 1, ra1 = 0, ra1s = 0, ta2 = 1, ta2s = 1, ra2 = 0, ra2s = 0;
+    real to3t = 1.0, to3tu = 1.0 - ozone(xo3t + ZMBAR * o3t);
+    real twvt = 1.0, twvtu = 1.0 - vapour(ywvt + ZBETTA * wvt);
+    real ccn = DCC[(NL - 1) * NH + h];
+    real scf = K.RCOEFF * dp / 101100.0 * 9.80665 / K.GA;
+    real diffuseRayleigh = 1.0 - std::exp(scf * K.LN_DIFFUSE_RAYLEIGH);
+    real rcsuSurface = diffuseRayleigh * (1.0 - ccn);
+    real rcsSurface = (1.0 - std::exp(scf * std::log(1.0 - 0.219 / (1.0 + 0.816 * mu0)))) * cs +
                         diffuseRayleigh * (1.0 - cs - ccn);
-    double t1[MAXL + 1], t2[MAXL + 1], r1s[MAXL + 1], r2s[MAXL + 1];
-    double tb1[MAXL], tb1u[MAXL], rb1[MAXL], rb1s[MAXL], tb2[MAXL], tb2u[MAXL], rb2[MAXL], rb2s[MAXL];
+    real t1[MAXL + 1], t2[MAXL + 1], r1s[MAXL + 1], r2s[MAXL + 1];
+    real tb1[MAXL], tb1u[MAXL], rb1[MAXL], rb1s[MAXL], tb2[MAXL], tb2u[MAXL], rb2[MAXL], rb2s[MAXL];
     for (int l = 0; l < NL; ++l) {
-      double cc = DCC[l * NH + h];
+      real cc = DCC[l * NH + h];
       t1[l] = ta1;
       t2[l] = ta2;
       r1s[l] = ra1s;
@@ -1097,30 +1112,30 @@ void swr(Model& m) {
       bool surface = l == NL - 1;
       rb1[l] = (surface ? rcsSurface : 0.0) + rcl1[l] * cc;
       rb1s[l] = (surface ? rcsuSurface : 0.0) + rcl1s[l] * cc;
-      double o3 = xo3l[l];
-      double to3 = (1.0 - ozone(o3)) / to3t;
+      real o3 = xo3l[l];
+      real to3 = (1.0 - ozone(o3)) / to3t;
       to3t = to3t * to3;
       o3 = xo3t + ZMBAR * (o3t - o3l[l]);
-      double to3u = to3tu / (1.0 - ozone(o3));
+      real to3u = to3tu / (1.0 - ozone(o3));
       to3tu = to3tu / to3u;
       tb1[l] = 1.0 - (1.0 - to3) * (1.0 - cc) - rb1[l];
       tb1u[l] = 1.0 - (1.0 - to3u) * (1.0 - cc) - rb1s[l];
-      double m1 = 1.0 / (1.0 - ra1s * rb1s[l]);
+      real m1 = 1.0 / (1.0 - ra1s * rb1s[l]);
       ra1 = ra1 + ta1 * rb1[l] * ta1s * m1;
       ta1 = ta1 * tb1[l] * m1;
       ra1s = rb1s[l] + tb1u[l] * ra1s * tb1[l] * m1;
       ta1s = tb1u[l] * ta1s * m1;
       rb2[l] = rcl2[l] * cc;
       rb2s[l] = rcl2s[l] * cc;
-      double wv = ywvl[l];
-      double twv = (1.0 - vapour(wv)) / twvt;
+      real wv = ywvl[l];
+      real twv = (1.0 - vapour(wv)) / twvt;
       twvt = twvt * twv;
       wv = ywvt + ZBETTA * (wvt - wvl[l]);
-      double twvu = twvtu / (1.0 - vapour(wv));
+      real twvu = twvtu / (1.0 - vapour(wv));
       twvtu = twvtu / twvu;
       tb2[l] = 1.0 - (1.0 - twv) * (1.0 - cc) - (1.0 - tcl2[l]) * cc;
       tb2u[l] = 1.0 - (1.0 - twvu) * (1.0 - cc) - (1.0 - tcl2s[l]) * cc;
-      double m2 = 1.0 / (1.0 - ra2s * rb2s[l]);
+      real m2 = 1.0 / (1.0 - ra2s * rb2s[l]);
       ra2 = ra2 + ta2 * rb2[l] * ta2s * m2;
       ta2 = ta2 * tb2[l] * m2;
       ra2s = rb2s[l] + tb2u[l] * ra2s * tb2[l] * m2;
@@ -1131,29 +1146,29 @@ void swr(Model& m) {
     r1s[NL] = ra1s;
     r2s[NL] = ra2s;
     bool star = K.NSTARTEMP != 0;
-    double dalb = DALB[h], salb1 = DSALB[h], salb2 = DSALB[NH + h];
+    real dalb = DALB[h], salb1 = DSALB[h], salb2 = DSALB[NH + h];
     ra1s = star ? salb1 : dalb;
     ra2s = star ? salb2 : dalb;
-    double dls = DLS[h], dicec = DICEC[h];
-    double water = (1.0 - dls) * (1.0 - dicec) * std::min(0.05 / (mu0 + 0.15), 0.15);
-    double nalb1 = dls * salb1 + (1.0 - dls) * dicec * salb1 + water;
-    double nalb2 = dls * salb2 + (1.0 - dls) * dicec * salb2 + water;
+    real dls = DLS[h], dicec = DICEC[h];
+    real water = (1.0 - dls) * (1.0 - dicec) * std::min(0.05 / (mu0 + 0.15), 0.15);
+    real nalb1 = dls * salb1 + (1.0 - dls) * dicec * salb1 + water;
+    real nalb2 = dls * salb2 + (1.0 - dls) * dicec * salb2 + water;
     DSALB[h] = nalb1;
     DSALB[NH + h] = nalb2;
-    double albedo = star ? K.ZSOLARS1 * nalb1 + K.ZSOLARS2 * nalb2 : dls * dalb + (1.0 - dls) * dicec * dalb + water;
+    real albedo = star ? K.ZSOLARS1 * nalb1 + K.ZSOLARS2 * nalb2 : dls * dalb + (1.0 - dls) * dicec * dalb + water;
     DALB[h] = albedo;
     ra1 = star ? nalb1 : albedo;
     ra2 = star ? nalb2 : albedo;
-    double rl1[MAXL + 1], rl2[MAXL + 1], rl1s[MAXL + 1], rl2s[MAXL + 1];
+    real rl1[MAXL + 1], rl2[MAXL + 1], rl1s[MAXL + 1], rl2s[MAXL + 1];
     for (int l = NL - 1; l >= 0; --l) {
       rl1[l + 1] = ra1;
       rl2[l + 1] = ra2;
       rl1s[l + 1] = ra1s;
       rl2s[l + 1] = ra2s;
-      double d1 = 1.0 - ra1s * rb1s[l];
+      real d1 = 1.0 - ra1s * rb1s[l];
       ra1 = rb1[l] + tb1[l] * ra1 * tb1u[l] / d1;
       ra1s = rb1s[l] + tb1u[l] * ra1s * tb1u[l] / d1;
-      double d2 = 1.0 - ra2s * rb2s[l];
+      real d2 = 1.0 - ra2s * rb2s[l];
       ra2 = rb2[l] + tb2[l] * ra2 * tb2u[l] / d2;
       ra2s = rb2s[l] + tb2u[l] * ra2s * tb2u[l] / d2;
     }
@@ -1162,10 +1177,10 @@ void swr(Model& m) {
     rl1s[0] = ra1s;
     rl2s[0] = ra2s;
     for (int l = 0; l < m.NLEP; ++l) {
-      double m1 = 1.0 / (1.0 - r1s[l] * rl1s[l]);
-      double m2 = 1.0 / (1.0 - r2s[l] * rl2s[l]);
-      double fu = -t1[l] * rl1[l] * m1 * ftop1 + -t2[l] * rl2[l] * m2 * ftop2;
-      double fd = t1[l] * m1 * ftop1 + t2[l] * m2 * ftop2;
+      real m1 = 1.0 / (1.0 - r1s[l] * rl1s[l]);
+      real m2 = 1.0 / (1.0 - r2s[l] * rl2s[l]);
+      real fu = -t1[l] * rl1[l] * m1 * ftop1 + -t2[l] * rl2[l] * m2 * ftop2;
+      real fd = t1[l] * m1 * ftop1 + t2[l] * m2 * ftop2;
       DFU[l * NH + h] = fu;
       DFD[l * NH + h] = fd;
       DSWFL[l * NH + h] = fu + fd;
@@ -1177,67 +1192,67 @@ void swr(Model& m) {
 void lwr(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NL = m.NLEV, NP = m.NLEP;
-  const double *sg = m.TB("sigma"), *sh = m.TB("sigmah"), *zzf1 = m.TB("lwr_zzf1"), *zzf3 = m.TB("lwr_zzf3");
-  double *DP = m.F("dp"), *DT = m.F("dt"), *DLS = m.F("dls"), *DQ = m.F("dq"), *DQO3 = m.F("dqo3"),
+  const real *sg = m.TB("sigma"), *sh = m.TB("sigmah"), *zzf1 = m.TB("lwr_zzf1"), *zzf3 = m.TB("lwr_zzf3");
+  real *DP = m.F("dp"), *DT = m.F("dt"), *DLS = m.F("dls"), *DQ = m.F("dq"), *DQO3 = m.F("dqo3"),
          *DQCO2 = m.F("dqco2"), *DCC = m.F("dcc"), *DQL = m.F("dql"), *DFTU = m.F("dftu"), *DFTD = m.F("dftd"),
          *DLWFL = m.F("dlwfl");
-  const double ZERO = 1.0e-6, ZFH2O = 0.1, ZFO3 = 100.0 / 2.14;
+  const real ZERO = 1.0e-6, ZFH2O = 0.1, ZFO3 = 100.0 / 2.14;
   for (int h = 0; h < NH; ++h) {
-    double dp = DP[h], ps2 = dp * dp;
-    double st4[MAXL + 1], st4h[MAXL + 1];
+    real dp = DP[h], ps2 = dp * dp;
+    real st4[MAXL + 1], st4h[MAXL + 1];
     for (int l = 0; l < NP; ++l) {
-      double t = DT[l * NH + h], t2 = t * t;
+      real t = DT[l * NH + h], t2 = t * t;
       st4[l] = K.SBK * (t2 * t2);
     }
     st4h[0] = st4[0] - (st4[0] - st4[1]) * sg[0] / (sg[0] - sg[1]);
     for (int l = 1; l < NL; ++l) {
-      double above = sg[l - 1], half = sh[l - 1], level = sg[l];
+      real above = sg[l - 1], half = sh[l - 1], level = sg[l];
       st4h[l] = (st4[l] * (above - half) + st4[l - 1] * (half - level)) / (above - level);
     }
     int n = NL - 1;
     if ((st4[n] - st4h[n]) * (st4[n] - st4[NL]) > 0.0) {
       st4h[NL] = st4[NL];
     } else {
-      double sn = sg[n], sm = sg[n - 1];
+      real sn = sg[n], sm = sg[n - 1];
       st4h[NL] = st4[n] + (st4[n] - st4[n - 1]) * (1.0 - sn) / (sn - sm);
     }
-    double bu[MAXL + 2], bd[MAXL + 2];
+    real bu[MAXL + 2], bd[MAXL + 2];
     bd[0] = 0.0;
-    double dls = DLS[h];
-    double eps = dls + 0.98 * (1.0 - dls);
+    real dls = DLS[h];
+    real eps = dls + 0.98 * (1.0 - dls);
     bu[NP] = eps * st4[NL];
-    double q[MAXL], qo3[MAXL], qco2[MAXL], taucc0[MAXL];
+    real q[MAXL], qo3[MAXL], qco2[MAXL], taucc0[MAXL];
     for (int l = 0; l < NL; ++l) {
-      double sfac = zzf1[l] * ps2;
+      real sfac = zzf1[l] * ps2;
       q[l] = ZFH2O * sfac * DQ[l * NH + h];
       qo3[l] = ZFO3 * sfac * DQO3[l * NH + h];
       qco2[l] = K.ZFCO2_ZZF2 * sfac * DQCO2[l * NH + h];
       taucc0[l] = 1.0 - DCC[l * NH + h] * (1.0 - std::exp(zzf3[l] * DQL[l * NH + h] * dp));
     }
-    double dftu[MAXL + 1] = {0}, dftd[MAXL + 1] = {0};
-    double taucs[MAXL], tau[MAXL], tausf[MAXL];
+    real dftu[MAXL + 1] = {0}, dftd[MAXL + 1] = {0};
+    real taucs[MAXL], tau[MAXL], tausf[MAXL];
     for (int j = 0; j < NL; ++j) {
-      double taucc = 1.0, sumwv = 0, sumo3 = 0, sumco2 = 0;
+      real taucc = 1.0, sumwv = 0, sumo3 = 0, sumco2 = 0;
       for (int kk = j; kk < NL; ++kk) {
         sumwv = sumwv + q[kk];
         sumo3 = sumo3 + qo3[kk];
         sumco2 = sumco2 + qco2[kk];
-        double ah2o = sumwv <= 0.01 ? 0.846 * fpow(sumwv + 3.59e-5, 0.243) - K.ZH2O0A
+        real ah2o = sumwv <= 0.01 ? 0.846 * fpow(sumwv + 3.59e-5, 0.243) - K.ZH2O0A
                                     : 0.24 * std::log10(sumwv + 0.01) + K.ZAH2OC;
         if (K.TH2OC > 0.0) ah2o = std::min(ah2o + (1.0 - std::exp(-K.TH2OC * sumwv)), 1.0);
-        double aco2 = sumco2 <= 1.0 ? 0.0676 * fpow(sumco2 + 0.01022, 0.421) - K.ZCO20
+        real aco2 = sumco2 <= 1.0 ? 0.0676 * fpow(sumco2 + 0.01022, 0.421) - K.ZCO20
                                     : 0.0546 * std::log10(sumco2) + K.ZACO2C;
-        double th2o = sumwv <= 2.0 ? 1.0 - (0.832 * fpow(sumwv + 0.0286, 0.26) - K.ZH2O0)
+        real th2o = sumwv <= 2.0 ? 1.0 - (0.832 * fpow(sumwv + 0.0286, 0.26) - K.ZH2O0)
                                    : std::max(0.0, K.ZTH2OC - 0.1196 * std::log(sumwv - 0.6931));
-        double ao3 = sumo3 <= 0.01 ? 0.209 * fpow(sumo3 + 7.0e-5, 0.436) - K.ZAO30
+        real ao3 = sumo3 <= 0.01 ? 0.209 * fpow(sumo3 + 7.0e-5, 0.436) - K.ZAO30
                                    : 0.0212 * std::log10(sumo3) + K.ZAO3C;
-        double cs = std::min(1.0 - ZERO, std::max(ZERO, 1.0 - ah2o - ao3 - aco2 * th2o));
+        real cs = std::min(1.0 - ZERO, std::max(ZERO, 1.0 - ah2o - ao3 - aco2 * th2o));
         taucs[kk] = cs;
         taucc = taucc * taucc0[kk];
         tau[kk] = cs * taucc;
       }
       if (j == 0) {
-        double tau0 = 1.0 - ZERO;
+        real tau0 = 1.0 - ZERO;
         for (int kk = 0; kk < NL; ++kk) {
           tau0 = taucs[kk] / tau0 * taucc0[kk] * K.TPOFMT;
           tau0 = std::min(1.0 - ZERO, std::max(ZERO, tau0));
@@ -1253,7 +1268,7 @@ void lwr(Model& m) {
       }
       dftu[j] = dftu[j] - bu[j + 1];
       dftd[j] = dftd[j] + bd[j];
-      double bdl = bd[j] - bd[j + 1];
+      real bdl = bd[j] - bd[j + 1];
       for (int kk = j; kk < NL; ++kk) {
         dftu[j] = dftu[j] - (bu[kk + 2] - bu[kk + 1]) * tau[kk];
         dftd[kk + 1] = dftd[kk + 1] + bdl * tau[kk];
@@ -1262,7 +1277,7 @@ void lwr(Model& m) {
     }
     dftu[NL] = dftu[NL] - bu[NP];
     dftd[NL] = dftd[NL] + bd[NL];
-    double reflected = (1.0 - eps) * dftd[NL];
+    real reflected = (1.0 - eps) * dftd[NL];
     for (int l = 0; l < NL; ++l) dftu[l] = dftu[l] - tausf[l] * reflected;
     for (int l = 0; l < NP; ++l) {
       DFTU[l * NH + h] = dftu[l];
@@ -1276,18 +1291,18 @@ void lwr(Model& m) {
 void radstep(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR;
-  const double *lnsig = m.TB("rad_lnsig"), *ds = m.TB("dsigma");
-  double *DFLUX = m.F("dflux"), *DLWFL = m.F("dlwfl"), *DSWFL = m.F("dswfl"), *DP = m.F("dp"), *DT = m.F("dt"),
+  const real *lnsig = m.TB("rad_lnsig"), *ds = m.TB("dsigma");
+  real *DFLUX = m.F("dflux"), *DLWFL = m.F("dlwfl"), *DSWFL = m.F("dswfl"), *DP = m.F("dp"), *DT = m.F("dt"),
          *DQ = m.F("dq"), *DTDT = m.F("dtdt"), *DTDTSWR = m.F("dtdtswr"), *DTDTLWR = m.F("dtdtlwr"),
          *DCONV = m.F("dconv");
   for (int h = 0; h < NH; ++h) {
     for (int l = 0; l < m.NLEP; ++l) DFLUX[l * NH + h] = DLWFL[l * NH + h] + DSWFL[l * NH + h];
-    double dp = DP[h];
+    real dp = DP[h];
     for (int l = 0; l < m.NLEV; ++l) {
       int at = l * NH + h, bl = (l + 1) * NH + h;
-      double zdh = -DT[at] * K.GASCON / K.GA * lnsig[l];
-      double den = ds[l] * dp * K.ACPD * (1.0 + K.ADV * DQ[at]);
-      double flux = DFLUX[at], below = DFLUX[bl];
+      real zdh = -DT[at] * K.GASCON / K.GA * lnsig[l];
+      real den = ds[l] * dp * K.ACPD * (1.0 + K.ADV * DQ[at]);
+      real flux = DFLUX[at], below = DFLUX[bl];
       DTDT[at] = DTDT[at] - K.GA * (below - flux) / den;
       DTDTSWR[at] = -K.GA * (DSWFL[bl] - DSWFL[at]) / den;
       DTDTLWR[at] = -K.GA * (DLWFL[bl] - DLWFL[at]) / den;
@@ -1298,44 +1313,44 @@ void radstep(Model& m) {
 
 // ----------------------------------------------------------------- precipitation
 struct Parcel {
-  double t, q, cor;
+  real t, q, cor;
   bool saturated;
 };
 
-static double sat_capped(const Consts& K, double t, double p) {
+static real sat_capped(const Consts& K, real t, real p) {
   return std::min(K.RDBRV * K.RA1 * std::exp(K.RA2 * (t - K.TMELT) / (t - K.RA4)) / p, K.RDBRV);
 }
-static double sat_divided(const Consts& K, double t, double p) {
-  double q = sat_capped(K, t, p);
+static real sat_divided(const Consts& K, real t, real p) {
+  real q = sat_capped(K, t, p);
   return q / (1.0 - K.MOIST * q);
 }
 
 // physics/precipitation/wgsl/kuo.wgsl:20-43 (condense).
-static Parcel condense(const Consts& K, double t0, double q0, double p) {
-  double s = sat_capped(K, t0, p);
-  double cor = 1.0 / (1.0 - K.MOIST * s);
+static Parcel condense(const Consts& K, real t0, real q0, real p) {
+  real s = sat_capped(K, t0, p);
+  real cor = 1.0 / (1.0 - K.MOIST * s);
   s = s * cor;
   if (!(s < q0)) return {t0, q0, cor, false};
-  double t = t0, q = q0;
-  double lcp = (t0 < K.TMELT ? K.ALS : K.ALV) / (K.ACPD * (1.0 + K.ADV * q0));
+  real t = t0, q = q0;
+  real lcp = (t0 < K.TMELT ? K.ALS : K.ALV) / (K.ACPD * (1.0 + K.ADV * q0));
   for (int i = 0; i < 2; ++i) {
     if (i == 1) {
       s = sat_capped(K, t, p);
       cor = 1.0 / (1.0 - K.MOIST * s);
       s = s * cor;
     }
-    double dqsdt = K.RA2 * (K.TMELT - K.RA4) * s * cor / ((t - K.RA4) * (t - K.RA4));
-    double rain = (q - s) / (1.0 + lcp * dqsdt);
+    real dqsdt = K.RA2 * (K.TMELT - K.RA4) * s * cor / ((t - K.RA4) * (t - K.RA4));
+    real rain = (q - s) / (1.0 + lcp * dqsdt);
     t = t + lcp * rain;
     q = q - rain;
   }
   return {t, q, cor, true};
 }
 
-static double powi(double x, int n) {
-  double base = x;
+static real powi(real x, int n) {
+  real base = x;
   unsigned mm = (unsigned)std::abs(n);
-  double result = (mm & 1u) ? x : 1.0;
+  real result = (mm & 1u) ? x : 1.0;
   mm >>= 1;
   while (mm) {
     base = base * base;
@@ -1349,19 +1364,19 @@ static double powi(double x, int n) {
 void kuo(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NL = m.NLEV, NM = m.NLEM;
-  const double *ds = m.TB("dsigma"), *sg = m.TB("sigma"), *sh = m.TB("sigmah"), *skapT = m.TB("vdiff_skap"),
+  const real *ds = m.TB("dsigma"), *sg = m.TB("sigma"), *sh = m.TB("sigmah"), *skapT = m.TB("vdiff_skap"),
                *skaph = m.TB("vdiff_skaph"), *vrd = m.TB("vdiff_rdsig"), *zfacT = m.TB("kuo_zfac");
-  double *DP = m.F("dp"), *DQT = m.F("dqt"), *DQ = m.F("dq"), *DQDT = m.F("dqdt"), *DT = m.F("dt"),
+  real *DP = m.F("dp"), *DQT = m.F("dqt"), *DQ = m.F("dq"), *DQDT = m.F("dqdt"), *DT = m.F("dt"),
          *DTDT = m.F("dtdt"), *DPRCL = m.F("dprcl"), *DPRSCL = m.F("dprscl"), *ICCLEV = m.F("icclev"),
          *ICCTOT = m.F("icctot");
   for (int h = 0; h < NH; ++h) {
-    double dp = DP[h];
-    double zdqt[MAXL], zqe[MAXL], zte[MAXL], zdqtot[MAXL], zalcpe[MAXL], zacpe[MAXL], zdqdt[MAXL], zdtdt[MAXL];
+    real dp = DP[h];
+    real zdqt[MAXL], zqe[MAXL], zte[MAXL], zdqtot[MAXL], zalcpe[MAXL], zacpe[MAXL], zdqdt[MAXL], zdtdt[MAXL];
     for (int l = 0; l < NL; ++l) {
       int at = l * NH + h;
       zdqt[l] = DQT[at] * K.PSURF * K.WW / dp;
       DQT[at] = zdqt[l];
-      double dq = DQ[at], dqdt = DQDT[at];
+      real dq = DQ[at], dqdt = DQDT[at];
       zdqtot[l] = (zdqt[l] + dqdt) * K.DELTSEC2;
       zqe[l] = dq + dqdt * K.DELTSEC2;
       zte[l] = DT[at] + DTDT[at] * K.DELTSEC2;
@@ -1371,21 +1386,21 @@ void kuo(Model& m) {
       zdtdt[l] = 0;
     }
     int ilift = -1, itop = -1;
-    double zi = 0, zpt = 0, zpq = 0, zbeta = 0, zpbeta = 0, ztp = 0, zqp = 0;
+    real zi = 0, zpt = 0, zpq = 0, zbeta = 0, zpbeta = 0, ztp = 0, zqp = 0;
     int n = NL - 1;
-    double dsn = ds[n];
-    double ztsurf = DT[NL * NH + h] * skapT[n];
+    real dsn = ds[n];
+    real ztsurf = DT[NL * NH + h] * skapT[n];
     if (zdqtot[n] > 0.0 && ztsurf > zte[n]) {
-      double p = dp * sg[n];
-      double zqsnl = sat_divided(K, zte[n], p);
-      double zqnew = DQ[NL * NH + h] * std::min(1.0, zqe[n] / zqsnl);
+      real p = dp * sg[n];
+      real zqsnl = sat_divided(K, zte[n], p);
+      real zqnew = DQ[NL * NH + h] * std::min(1.0, zqe[n] / zqsnl);
       Parcel parcel = condense(K, ztsurf, zqnew, p);
       if (parcel.saturated) {
         ilift = m.NLEP;
         itop = NL;
         ztp = parcel.t;
         zqp = parcel.q;
-        double zqsa = sat_divided(K, zte[n], p);
+        real zqsa = sat_divided(K, zte[n], p);
         zdqdt[n] = std::max(zqsa - zqe[n], 0.0);
         zdtdt[n] = ztp - zte[n];
         zpt = zdtdt[n] * dsn * zacpe[n];
@@ -1398,35 +1413,35 @@ void kuo(Model& m) {
     for (int l = NM - 1; l >= 0; --l) {
       int lu = l, lp = l + 1;
       if (ilift == -1 && zdqtot[lp] > 0.0) {
-        double p = dp * sg[lu];
+        real p = dp * sg[lu];
         Parcel parcel = condense(K, zte[lp] * zfacT[lu], zqe[lp], p);
         if (parcel.saturated && parcel.t > zte[lu]) {
-          double dsl = ds[lu], dsp = ds[lp];
+          real dsl = ds[lu], dsp = ds[lp];
           ilift = l + 2;
           itop = l + 1;
           ztp = parcel.t;
           zqp = parcel.q;
-          double zqsa = sat_divided(K, zte[lu], p);
+          real zqsa = sat_divided(K, zte[lu], p);
           zdqdt[lu] = std::max(zqsa - zqe[lu], 0.0);
           zdtdt[lu] = ztp - zte[lu];
           zpt = zdtdt[lu] * dsl * zacpe[lu];
           zpq = zdqdt[lu] * dsl * K.ALV;
           zbeta = std::min(1.0, zqe[lu] / zqsa) * dsl;
           zpbeta = dsl;
-          double pp = dp * sg[lp];
-          double zqsnl = sat_divided(K, zte[lp], pp);
+          real pp = dp * sg[lp];
+          real zqsnl = sat_divided(K, zte[lp], pp);
           if (zqe[lp] > zqsnl) {
-            double t = zte[lp], q = zqe[lp];
-            double lcp = (t < K.TMELT ? K.ALS : K.ALV) / (K.ACPD * (1.0 + K.ADV * q));
-            double cor = parcel.cor;
+            real t = zte[lp], q = zqe[lp];
+            real lcp = (t < K.TMELT ? K.ALS : K.ALV) / (K.ACPD * (1.0 + K.ADV * q));
+            real cor = parcel.cor;
             for (int i = 0; i < 2; ++i) {
               if (i == 1) {
                 zqsnl = sat_capped(K, t, pp);
                 cor = 1.0 / (1.0 - K.MOIST * zqsnl);
                 zqsnl = zqsnl * cor;
               }
-              double dqsdt = K.RA2 * (K.TMELT - K.RA4) * zqsnl * cor / ((t - K.RA4) * (t - K.RA4));
-              double rain = (q - zqsnl) / (1.0 + lcp * dqsdt);
+              real dqsdt = K.RA2 * (K.TMELT - K.RA4) * zqsnl * cor / ((t - K.RA4) * (t - K.RA4));
+              real rain = (q - zqsnl) / (1.0 + lcp * dqsdt);
               t = t + lcp * rain;
               q = q - rain;
             }
@@ -1444,14 +1459,14 @@ void kuo(Model& m) {
     for (int l = NM - 1; l >= 0; --l) {
       int lu = l;
       if (itop == l + 2) {
-        double p = dp * sg[lu];
+        real p = dp * sg[lu];
         Parcel parcel = condense(K, ztp * zfacT[lu], zqp, p);
         if (parcel.saturated && parcel.t > zte[lu]) {
-          double dsl = ds[lu];
+          real dsl = ds[lu];
           itop = l + 1;
           ztp = parcel.t;
           zqp = parcel.q;
-          double zqsa = sat_divided(K, zte[lu], p);
+          real zqsa = sat_divided(K, zte[lu], p);
           zdqdt[lu] = std::max(zqsa - zqe[lu], 0.0);
           zdtdt[lu] = ztp - zte[lu];
           zpt = zdtdt[lu] * dsl * zacpe[lu] + zpt;
@@ -1463,16 +1478,16 @@ void kuo(Model& m) {
       }
     }
     zi = std::max(0.0, zi);
-    double zrhm = zpbeta > 0.0 ? zbeta / zpbeta : 0.0;
-    double beta = 1.0;
+    real zrhm = zpbeta > 0.0 ? zbeta / zpbeta : 0.0;
+    real beta = 1.0;
     if (zrhm >= K.RHBETA) beta = powi((1.0 - zrhm) / (1.0 - K.RHBETA), (int)K.NBETA);
-    double zat = zpt > 0.0 ? zi * (1.0 - beta) / zpt : 0.0;
-    double zaq = zpq > 0.0 ? zi * beta / zpq : 0.0;
+    real zat = zpt > 0.0 ? zi * (1.0 - beta) / zpt : 0.0;
+    real zaq = zpq > 0.0 ? zi * beta / zpq : 0.0;
     bool shallow = itop > 0 && (dp * sg[itop - 1] > K.PDEEP || zi <= 0.0);
-    double icctot = 0;
+    real icctot = 0;
     for (int l = 0; l < NL; ++l) {
       int level = l + 1, at = l * NH + h;
-      double dprcl = 0, icclev = 0;
+      real dprcl = 0, icclev = 0;
       if (ilift >= level && itop <= level && zi > 0.0 && !shallow) {
         DQDT[at] = zaq * zdqdt[l] / K.DELTSEC2 - zdqt[l];
         DTDT[at] = zat * zdtdt[l] / K.DELTSEC2 + DTDT[at];
@@ -1489,32 +1504,32 @@ void kuo(Model& m) {
     }
     ICCTOT[h] = icctot;
     if (!shallow) continue;
-    double zkonst1 = K.GA * K.DELTSEC2 / K.GASCON;
-    double zkonst2 = K.RKSHALLOW * zkonst1 * K.GA / K.GASCON;
+    real zkonst1 = K.GA * K.DELTSEC2 / K.GASCON;
+    real zkonst2 = K.RKSHALLOW * zkonst1 * K.GA / K.GASCON;
     int kktop = 1;
     for (int level = 2; level <= NM; ++level)
       if (dp * sg[level - 1] < K.PDEEPTH) kktop = level;
     int ktop = std::max(itop, kktop);
-    double zkdiff[MAXL] = {0}, skap[MAXL];
+    real zkdiff[MAXL] = {0}, skap[MAXL];
     for (int l = 0; l < NL; ++l) skap[l] = skapT[l];
     for (int l = 0; l < NM; ++l) {
       int lp = l + 1, level = l + 1;
-      double sigmah = sh[l];
-      double zfac = zkonst2 * sigmah * sigmah * vrd[l];
-      double dsl = ds[l], dsp = ds[lp];
-      double zrthl = (dsp + dsl) / (zte[l] * dsp + zte[lp] * dsl);
+      real sigmah = sh[l];
+      real zfac = zkonst2 * sigmah * sigmah * vrd[l];
+      real dsl = ds[l], dsp = ds[lp];
+      real zrthl = (dsp + dsl) / (zte[l] * dsp + zte[lp] * dsl);
       if (level >= ktop && level < ilift) zkdiff[l] = zfac * zrthl * zrthl;
       if (level + 1 == ktop) {
-        double zzqs = sat_capped(K, zte[l], dp * sg[l]);
+        real zzqs = sat_capped(K, zte[l], dp * sg[l]);
         zzqs = zzqs * (1.0 / (1.0 - K.MOIST * zzqs));
-        double zzqsp = sat_capped(K, zte[lp], dp * sg[lp]);
+        real zzqsp = sat_capped(K, zte[lp], dp * sg[lp]);
         zzqsp = zzqsp * (1.0 / (1.0 - K.MOIST * zzqsp));
-        double zrh = zqe[l] / zzqs, zrhp = zqe[lp] / zzqsp;
-        double zzf = std::fabs((zrh - 0.8) / 0.2 * (zrhp - zrh));
+        real zrh = zqe[l] / zzqs, zrhp = zqe[lp] / zzqsp;
+        real zzf = std::fabs((zrh - 0.8) / 0.2 * (zrhp - zrh));
         zkdiff[l] = zfac * zrthl * zrthl * zzf;
       }
     }
-    double zqn[MAXL], ztn[MAXL];
+    real zqn[MAXL], ztn[MAXL];
     for (int l = 0; l < NL; ++l) {
       zqn[l] = zqe[l];
       ztn[l] = zte[l];
@@ -1534,12 +1549,12 @@ void kuo(Model& m) {
 void mkdca(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NL = m.NLEV, NM = m.NLEM;
-  const double *skapT = m.TB("vdiff_skap"), *dsT = m.TB("dsigma");
-  double *DT = m.F("dt"), *DTDT = m.F("dtdt"), *DQ = m.F("dq"), *DQDT = m.F("dqdt"),
+  const real *skapT = m.TB("vdiff_skap"), *dsT = m.TB("dsigma");
+  real *DT = m.F("dt"), *DTDT = m.F("dtdt"), *DQ = m.F("dq"), *DQDT = m.F("dqdt"),
          *DCA_DTDT = m.F("dca_dtdt"), *DCA_DQDT = m.F("dca_dqdt"), *LIM = m.F("dca_limited");
-  double skip = 0;
+  real skip = 0;
   for (int h = 0; h < NH; ++h) {
-    double zt[MAXL], zth[MAXL], zq[MAXL], zqn[MAXL], skap[MAXL], ds[MAXL];
+    real zt[MAXL], zth[MAXL], zq[MAXL], zqn[MAXL], skap[MAXL], ds[MAXL];
     bool mixed[MAXL] = {false};
     for (int l = 0; l < NL; ++l) {
       int at = l * NH + h;
@@ -1550,12 +1565,12 @@ void mkdca(Model& m) {
       zq[l] = DQ[at] + DQDT[at] * K.DELTSEC2;
       zqn[l] = zq[l];
     }
-    double limited = 0;
+    real limited = 0;
     int passes = 0;
     for (;;) {
       bool unstable = false;
       int ibase = 0, itop = NL;
-      double ztht = 0, zqt = 0, zsum1 = 0, zsum2 = 0, zsumq1 = 0, zsumq2 = 0;
+      real ztht = 0, zqt = 0, zsum1 = 0, zsum2 = 0, zsumq1 = 0, zsumq2 = 0;
       for (int l = 0; l < NM; ++l) {
         int lp = l + 1;
         if (zth[l] < zth[lp]) {
@@ -1612,13 +1627,13 @@ void mkdca(Model& m) {
 void rain_column(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NL = m.NLEV;
-  const double *ds = m.TB("dsigma"), *sg = m.TB("sigma"), *rcrit = m.TB("rcrit"), *lnsig = m.TB("rad_lnsig");
-  double *DTDT = m.F("dtdt"), *DQDT = m.F("dqdt"), *CA_T = m.F("dca_dtdt"), *CA_Q = m.F("dca_dqdt"),
+  const real *ds = m.TB("dsigma"), *sg = m.TB("sigma"), *rcrit = m.TB("rcrit"), *lnsig = m.TB("rad_lnsig");
+  real *DTDT = m.F("dtdt"), *DQDT = m.F("dqdt"), *CA_T = m.F("dca_dtdt"), *CA_Q = m.F("dca_dqdt"),
          *DP = m.F("dp"), *DPRSLL = m.F("dprsll"), *DPRLL = m.F("dprll"), *DQ = m.F("dq"), *DT = m.F("dt"),
          *DPRCL = m.F("dprcl"), *DPRSCL = m.F("dprscl"), *DPRC = m.F("dprc"), *DPRL = m.F("dprl"),
          *DPRS = m.F("dprs"), *ICCTOT = m.F("icctot"), *ICCLEV = m.F("icclev"), *DW = m.F("dw"),
          *DQVI = m.F("dqvi"), *DQL = m.F("dql"), *DCC = m.F("dcc");
-  const double skip = m.F("dca_skip")[0];
+  const real skip = m.F("dca_skip")[0];
   for (int h = 0; h < NH; ++h) {
     if (skip == 0.0)
       for (int l = 0; l < NL; ++l) {
@@ -1627,30 +1642,30 @@ void rain_column(Model& m) {
         DQDT[at] = DQDT[at] + CA_Q[at];
       }
     // mklsp
-    double dp = DP[h];
+    real dp = DP[h];
     for (int l = 0; l < NL; ++l) {
       int at = l * NH + h;
       DPRSLL[at] = 0;
-      double dprll = 0, dq = DQ[at];
-      double zq = dq + DQDT[at] * K.DELTSEC2;
-      double zt = DT[at] + DTDT[at] * K.DELTSEC2;
-      double zlcpe = K.ALV / (K.ACPD * (1.0 + K.ADV * dq));
-      double p = dp * sg[l];
-      double zqsat = sat_capped(K, zt, p);
-      double zcor = 1.0 / (1.0 - K.MOIST * zqsat);
+      real dprll = 0, dq = DQ[at];
+      real zq = dq + DQDT[at] * K.DELTSEC2;
+      real zt = DT[at] + DTDT[at] * K.DELTSEC2;
+      real zlcpe = K.ALV / (K.ACPD * (1.0 + K.ADV * dq));
+      real p = dp * sg[l];
+      real zqsat = sat_capped(K, zt, p);
+      real zcor = 1.0 / (1.0 - K.MOIST * zqsat);
       zqsat = zqsat * zcor;
       if (zqsat < 0.0) zqsat = 0.0;
       if (zq > zqsat) {
-        double zdqdt = (zqsat - zq) / (1.0 + zlcpe * K.RA2 * (K.TMELT - K.RA4) * zqsat * zcor / ((zt - K.RA4) * (zt - K.RA4)));
-        double ztn = zt - zdqdt * zlcpe;
-        double zqn = zq + zdqdt;
+        real zdqdt = (zqsat - zq) / (1.0 + zlcpe * K.RA2 * (K.TMELT - K.RA4) * zqsat * zcor / ((zt - K.RA4) * (zt - K.RA4)));
+        real ztn = zt - zdqdt * zlcpe;
+        real zqn = zq + zdqdt;
         zqsat = sat_capped(K, ztn, p);
         zcor = 1.0 / (1.0 - K.MOIST * zqsat);
         zqsat = zqsat * zcor;
         zdqdt = (zqsat - zqn) / (1.0 + zlcpe * K.RA2 * (K.TMELT - K.RA4) * zqsat * zcor / ((ztn - K.RA4) * (ztn - K.RA4)));
         ztn = ztn - zdqdt * zlcpe;
         zqn = zqn + zdqdt;
-        double dqdt = (zqn - zq) / K.DELTSEC2, dtdt = (ztn - zt) / K.DELTSEC2;
+        real dqdt = (zqn - zq) / K.DELTSEC2, dtdt = (ztn - zt) / K.DELTSEC2;
         DQDT[at] = DQDT[at] + dqdt;
         DTDT[at] = DTDT[at] + dtdt;
         dprll = -std::min(dqdt, 0.0) * ds[l];
@@ -1658,19 +1673,19 @@ void rain_column(Model& m) {
       DPRLL[at] = dprll;
     }
     // mkrain
-    double zprc = 0, zprl = 0, zprsc = 0, zprsl = 0;
+    real zprc = 0, zprl = 0, zprsc = 0, zprsl = 0;
     for (int l = 0; l < NL; ++l) {
       int at = l * NH + h;
-      double dsl = ds[l], dq = DQ[at];
-      double zdtdt = 0, zdqdtl = 0, zdqdts = 0;
+      real dsl = ds[l], dq = DQ[at];
+      real zdtdt = 0, zdqdtl = 0, zdqdts = 0;
       zprc = zprc + DPRCL[at] - DPRSCL[at];
       zprl = zprl + DPRLL[at] - DPRSLL[at];
       zprsc = zprsc + DPRSCL[at];
       zprsl = zprsl + DPRSLL[at];
       int surface = l == NL - 1 ? 2 : 1;
       for (int below = 0; below < surface; ++below) {
-        double temperature = DT[(l + below) * NH + h];
-        double zlcp = (K.ALS - K.ALV) / (K.ACPD * (1.0 + K.ADV * dq));
+        real temperature = DT[(l + below) * NH + h];
+        real zlcp = (K.ALS - K.ALV) / (K.ACPD * (1.0 + K.ADV * dq));
         if (zprsc + zprsl > 0.0 && temperature > K.TMELT) {
           zdtdt = -(zprsc + zprsl) / dsl * zlcp + zdtdt;
           zprc = zprsc + zprc;
@@ -1685,40 +1700,40 @@ void rain_column(Model& m) {
           zprl = 0;
         }
       }
-      double zq = dq + DQDT[at] * K.DELTSEC2;
-      double zt = DT[at] + DTDT[at] * K.DELTSEC2;
-      double zqsat = sat_capped(K, zt, dp * sg[l]);
-      double zcor = 1.0 / (1.0 - K.MOIST * zqsat);
+      real zq = dq + DQDT[at] * K.DELTSEC2;
+      real zt = DT[at] + DTDT[at] * K.DELTSEC2;
+      real zqsat = sat_capped(K, zt, dp * sg[l]);
+      real zcor = 1.0 / (1.0 - K.MOIST * zqsat);
       zqsat = zqsat * zcor;
       if (zqsat < 0.0) zqsat = 0.0;
       if (zq < zqsat) {
-        double deficit = zqsat - zq;
-        double water = K.ALV / (K.ACPD * (1.0 + K.ADV * dq));
-        double ice = K.ALS / (K.ACPD * (1.0 + K.ADV * dq));
-        auto evap = [&](double& flux, double zlcpe) {
-          double zd = std::min(K.GAMMA * deficit * dsl / K.DELTSEC2 /
+        real deficit = zqsat - zq;
+        real water = K.ALV / (K.ACPD * (1.0 + K.ADV * dq));
+        real ice = K.ALS / (K.ACPD * (1.0 + K.ADV * dq));
+        auto evap = [&](real& flux, real zlcpe) {
+          real zd = std::min(K.GAMMA * deficit * dsl / K.DELTSEC2 /
                                    (1.0 + zlcpe * K.RA2 * (K.TMELT - K.RA4) * zqsat * zcor / ((zt - K.RA4) * (zt - K.RA4))),
                                flux);
           flux = flux - zd;
           return zd / dsl;
         };
         if (zprl > 0.0) {
-          double e = evap(zprl, water);
+          real e = evap(zprl, water);
           zdtdt = zdtdt - e * water;
           zdqdtl = zdqdtl + e;
         }
         if (zprc > 0.0) {
-          double e = evap(zprc, water);
+          real e = evap(zprc, water);
           zdtdt = zdtdt - e * water;
           zdqdtl = zdqdtl + e;
         }
         if (zprsl > 0.0) {
-          double e = evap(zprsl, ice);
+          real e = evap(zprsl, ice);
           zdtdt = zdtdt - e * ice;
           zdqdts = zdqdts + e;
         }
         if (zprsc > 0.0) {
-          double e = evap(zprsc, ice);
+          real e = evap(zprsc, ice);
           zdtdt = zdtdt - e * ice;
           zdqdts = zdqdts + e;
         }
@@ -1730,41 +1745,41 @@ void rain_column(Model& m) {
     DPRL[h] = (zprl + zprsl) * dp / K.GA / 1000.0;
     DPRS[h] = (zprsc + zprsl) * dp / K.GA / 1000.0;
     // mkclouds
-    const double ZCLMAX = 1.0, ZCCA = 0.245, ZCCB = 0.125, ZCCMAX = 0.8, ZCCMIN = 0.05;
-    double zcctot = ZCCMIN, zccconv = ZCCMIN;
-    double dprc = DPRC[h];
+    const real ZCLMAX = 1.0, ZCCA = 0.245, ZCCB = 0.125, ZCCMAX = 0.8, ZCCMIN = 0.05;
+    real zcctot = ZCCMIN, zccconv = ZCCMIN;
+    real dprc = DPRC[h];
     if (dprc > 0.0) {
       zcctot = ZCCA + ZCCB * std::log(dprc * K.ZRFAC);
       zcctot = std::min(ZCCMAX, std::max(ZCCMIN, zcctot));
-      double levels = ICCTOT[h];
+      real levels = ICCTOT[h];
       zccconv = levels == 0.0 ? 1.0 : 1.0 - fpow(1.0 - zcctot, 1.0 / levels);
     }
-    double cover[MAXL];
+    real cover[MAXL];
     for (int l = 0; l < NL; ++l) {
       int at = l * NH + h;
-      double zt = DT[at] + DTDT[at] * K.DELTSEC2;
-      double zq = DQ[at] + DQDT[at] * K.DELTSEC2;
-      double zqsat = sat_divided(K, zt, dp * sg[l]);
-      double zrh = zq / zqsat;
-      double icclev = ICCLEV[at];
-      double dcc = icclev > 0.0 ? zccconv : 0.0;
+      real zt = DT[at] + DTDT[at] * K.DELTSEC2;
+      real zq = DQ[at] + DQDT[at] * K.DELTSEC2;
+      real zqsat = sat_divided(K, zt, dp * sg[l]);
+      real zrh = zq / zqsat;
+      real icclev = ICCLEV[at];
+      real dcc = icclev > 0.0 ? zccconv : 0.0;
       if (icclev == 2.0 && zcctot >= 0.3) dcc = std::min(dcc + 2.0 * (zcctot - 0.3), ZCLMAX);
       zrh = zrh * (1.0 - dcc);
-      double zrcrit = rcrit[l];
-      double zwfac = 1.0;
+      real zrcrit = rcrit[l];
+      real zwfac = 1.0;
       if (sg[l] > 0.8 && K.CLWFAC > 0.0) {
-        double dw = DW[at];
+        real dw = DW[at];
         zwfac = K.CLWFAC * std::max(0.0, K.CLWCRIT1 - dw);
         if (K.CLWCRIT2 > dw) zwfac = 1.0;
       }
-      double excess = std::max(0.0, (zrh - zrcrit) / (1.0 - zrcrit));
+      real excess = std::max(0.0, (zrh - zrcrit) / (1.0 - zrcrit));
       cover[l] = std::min(dcc + zwfac * (excess * excess), ZCLMAX);
     }
-    double zzf[MAXL];
-    double dqvi = 0, zzh = 0;
+    real zzf[MAXL];
+    real dqvi = 0, zzh = 0;
     for (int l = NL - 1; l >= 1; --l) {
       dqvi = DQ[l * NH + h] * ds[l] + dqvi;
-      double zdh = -DT[l * NH + h] * K.GASCON / K.GA * lnsig[l];
+      real zdh = -DT[l * NH + h] * K.GASCON / K.GA * lnsig[l];
       zzf[l] = zzh + zdh * 0.5;
       zzh = zzh + zdh;
     }
@@ -1773,10 +1788,10 @@ void rain_column(Model& m) {
     dqvi = dqvi * dp / K.GA;
     DQVI[h] = dqvi;
     zzh = 700.0 * std::log(1.0 + dqvi);
-    double clear = 1.0;
+    real clear = 1.0;
     for (int l = 0; l < NL; ++l) {
       int at = l * NH + h;
-      double dql = 0;
+      real dql = 0;
       if (zzh > 0.0 && cover[l] > 0.0) {
         dql = 0.00021 * std::exp(-zzf[l] / zzh) * K.GASCON * DT[at] / (sg[l] * dp);
         dql = std::max(dql, 1.0e-9);
@@ -1795,57 +1810,57 @@ void rain_column(Model& m) {
 void soil(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NLS = 5;
-  const double* dsoilz = m.TB("dsoilz");
-  double *DLS = m.F("dls"), *DSNOWZ = m.F("dsnowz"), *DSNOWT = m.F("dsnowt"), *DGLAC = m.F("dglac"),
+  const real* dsoilz = m.TB("dsoilz");
+  real *DLS = m.F("dls"), *DSNOWZ = m.F("dsnowz"), *DSNOWT = m.F("dsnowt"), *DGLAC = m.F("dglac"),
          *DSHFL = m.F("dshfl"), *DLHFL = m.F("dlhfl"), *DFLUX = m.F("dflux"), *DEVAP = m.F("devap"),
          *DPRS = m.F("dprs"), *DPRL = m.F("dprl"), *DPRC = m.F("dprc"), *LAND_DTSM = m.F("land_dtsm"),
          *DSOILT = m.F("dsoilt"), *LAND_DTS = m.F("land_dts"), *DSNDCH = m.F("dsndch"), *DWATER = m.F("dwater"),
          *DSMELT = m.F("dsmelt"), *DWATC = m.F("dwatc"), *DWMAX = m.F("dwmax"), *DRUNOFF = m.F("drunoff");
   struct Layer {
-    double ctop, soilz1, diff1, cap1;
+    real ctop, soilz1, diff1, cap1;
   };
-  auto snow_layer = [&](double snowz, double cap0, double diff0, double soilz0) {
-    double zsntop = std::min(snowz * 1000.0 / K.RHOSNOW, K.DZTOP);
-    double ctop = cap0 * K.SNOWCAP * K.DZTOP / (cap0 * zsntop + K.SNOWCAP * (K.DZTOP - zsntop));
-    double zsnowz = std::min(snowz * 1000.0 / K.RHOSNOW, 1.0) - zsntop;
-    double soilz1 = soilz0 + zsnowz;
-    double diff1 = diff0 * K.SNOWDIFF * soilz1 / (K.SNOWDIFF * soilz0 + diff0 * zsnowz);
-    double cap1 = cap0 * K.SNOWCAP * soilz1 / (cap0 * zsnowz + K.SNOWCAP * soilz0);
+  auto snow_layer = [&](real snowz, real cap0, real diff0, real soilz0) {
+    real zsntop = std::min(snowz * 1000.0 / K.RHOSNOW, K.DZTOP);
+    real ctop = cap0 * K.SNOWCAP * K.DZTOP / (cap0 * zsntop + K.SNOWCAP * (K.DZTOP - zsntop));
+    real zsnowz = std::min(snowz * 1000.0 / K.RHOSNOW, 1.0) - zsntop;
+    real soilz1 = soilz0 + zsnowz;
+    real diff1 = diff0 * K.SNOWDIFF * soilz1 / (K.SNOWDIFF * soilz0 + diff0 * zsnowz);
+    real cap1 = cap0 * K.SNOWCAP * soilz1 / (cap0 * zsnowz + K.SNOWCAP * soilz0);
     return Layer{ctop, soilz1, diff1, cap1};
   };
-  auto surface_temperature = [&](const Layer& ly, double dtsm, double flux, double soil1) {
-    double conduction = 2.0 * ly.diff1;
+  auto surface_temperature = [&](const Layer& ly, real dtsm, real flux, real soil1) {
+    real conduction = 2.0 * ly.diff1;
     return (ly.ctop * K.DZTOP * dtsm / K.DELTSEC + flux + conduction * soil1 / ly.soilz1) /
            (ly.ctop * K.DZTOP / K.DELTSEC + conduction / ly.soilz1);
   };
   for (int h = 0; h < NH; ++h) {
-    double dls = DLS[h];
+    real dls = DLS[h];
     bool land = dls > 0.0;
-    double snowStart = DSNOWZ[h];
-    double dwater = 0, dsmelt = 0;
+    real snowStart = DSNOWZ[h];
+    real dwater = 0, dsmelt = 0;
     if (snowStart == 0.0) DSNOWT[h] = K.TMELT;
     if (land) {
-      double glac = DGLAC[h];
-      double soilz[NLS], cap[NLS], diff[NLS];
+      real glac = DGLAC[h];
+      real soilz[NLS], cap[NLS], diff[NLS];
       for (int l = 0; l < NLS; ++l) {
         cap[l] = K.SICECAP * glac + K.SOILCAP * (1.0 - glac);
         diff[l] = K.SICEDIFF * glac + K.SOILDIFF * (1.0 - glac);
         soilz[l] = dsoilz[l];
       }
-      double zhfla = DSHFL[h] + DLHFL[h] + DFLUX[m.NLEV * NH + h];
-      double devap = DEVAP[h];
-      double zdsnowz = 0;
+      real zhfla = DSHFL[h] + DLHFL[h] + DFLUX[m.NLEV * NH + h];
+      real devap = DEVAP[h];
+      real zdsnowz = 0;
       if (DPRS[h] > 0.0) zdsnowz = DPRS[h];
       if (snowStart > 0.0) zdsnowz = zdsnowz + devap;
-      double zsnowz = std::max(0.0, snowStart + zdsnowz * K.DELTSEC);
+      real zsnowz = std::max(0.0, snowStart + zdsnowz * K.DELTSEC);
       zdsnowz = (zsnowz - snowStart) / K.DELTSEC;
       dwater = devap + DPRL[h] + DPRC[h] - zdsnowz;
-      double dsnowz = zsnowz;
-      double dtsm = LAND_DTSM[h], soil1 = DSOILT[h];
+      real dsnowz = zsnowz;
+      real dtsm = LAND_DTSM[h], soil1 = DSOILT[h];
       Layer layer = snow_layer(dsnowz, cap[0], diff[0], soilz[0]);
-      double dts = surface_temperature(layer, dtsm, zhfla, soil1);
-      double zhfls = 2.0 * layer.diff1 / layer.soilz1 * (dts - soil1);
-      double zhflm = 0;
+      real dts = surface_temperature(layer, dtsm, zhfla, soil1);
+      real zhfls = 2.0 * layer.diff1 / layer.soilz1 * (dts - soil1);
+      real zhflm = 0;
       if (dsnowz > 0.0 && dts > K.TMELT) {
         dts = K.TMELT;
         zhflm = std::max(0.0, zhfla - layer.ctop * K.DZTOP * (dts - dtsm) / K.DELTSEC +
@@ -1867,7 +1882,7 @@ void soil(Model& m) {
       cap[0] = layer.cap1;
       diff[0] = layer.diff1;
       // mktsoil
-      double zdiff[NLS], zcap[NLS], zebs[NLS], ztn[NLS];
+      real zdiff[NLS], zcap[NLS], zebs[NLS], ztn[NLS];
       int n = NLS - 1;
       zdiff[n - 1] = 2.0 * diff[n] * diff[n - 1] / (diff[n] * soilz[n - 1] + diff[n - 1] * soilz[n]);
       zcap[n] = cap[n] * soilz[n] / K.DELTSEC;
@@ -1901,10 +1916,10 @@ void soil(Model& m) {
     }
     DWATER[h] = dwater;
     DSMELT[h] = dsmelt;
-    double drunoff = 0;
+    real drunoff = 0;
     if (land) {
-      double dwatc = DWATC[h] + K.DELTSEC * dwater;
-      double dwmax = DWMAX[h];
+      real dwatc = DWATC[h] + K.DELTSEC * dwater;
+      real dwmax = DWMAX[h];
       drunoff = std::max(0.0, dwatc - dwmax) / K.DELTSEC;
       DWATC[h] = std::max(std::min(dwmax, dwatc), 0.0);
     }
@@ -1915,20 +1930,20 @@ void soil(Model& m) {
 // physics/land/wgsl/mkradv.wgsl:1-59 (river routing; reads only driver).
 void mkradv(Model& m) {
   const int NH = m.NHOR, NLON = m.NLON, NLAT = m.NLAT;
-  double *DRIVER = m.F("driver"), *DAREA = m.F("darea"), *DLS = m.F("dls"), *DUROFF = m.F("duroff"),
+  real *DRIVER = m.F("driver"), *DAREA = m.F("darea"), *DLS = m.F("dls"), *DUROFF = m.F("duroff"),
          *DVROFF = m.F("dvroff"), *DRUNOFF = m.F("drunoff");
-  std::vector<double> out(NH);
+  std::vector<real> out(NH);
   auto river = [&](int h) { return DRIVER[h] * DAREA[h] * DLS[h]; };
-  auto eastward = [&](int row, int lon, double& o, double& in) {
+  auto eastward = [&](int row, int lon, real& o, real& in) {
     int h = row + lon, nx = row + (lon + 1) % NLON;
-    double u = DUROFF[h];
-    double water = u > 0.0 ? river(h) : river(nx);
+    real u = DUROFF[h];
+    real water = u > 0.0 ? river(h) : river(nx);
     o = u * water / DAREA[h];
     in = u * water / DAREA[nx];
   };
   for (int h = 0; h < NH; ++h) {
     int lat = h / NLON, lon = h % NLON, row = lat * NLON;
-    double runoff = DRUNOFF[h], o, in;
+    real runoff = DRUNOFF[h], o, in;
     if (lon == 0) {
       eastward(row, 0, o, in);
       runoff = runoff - o;
@@ -1940,16 +1955,16 @@ void mkradv(Model& m) {
       eastward(row, lon, o, in);
       runoff = runoff - o;
     }
-    double area = DAREA[h], v = DVROFF[h];
-    double below = lat + 1 < NLAT ? river(h + NLON) : 0.0;
+    real area = DAREA[h], v = DVROFF[h];
+    real below = lat + 1 < NLAT ? river(h + NLON) : 0.0;
     if (v < 0.0)
       runoff = runoff + v * river(h) / area;
     else
       runoff = runoff + v * below / area;
-    double fromAbove = 0;
+    real fromAbove = 0;
     if (lat > 0) {
       int above = h - NLON;
-      double va = DVROFF[above];
+      real va = DVROFF[above];
       fromAbove = va < 0.0 ? -va * river(above) : -va * river(h);
     }
     out[h] = runoff + fromAbove / area;
@@ -1962,7 +1977,7 @@ void mkradv(Model& m) {
 void land_surface(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NL = m.NLEV;
-  double *DLS = m.F("dls"), *DRIVER = m.F("driver"), *DRUNOFF = m.F("drunoff"), *LAND_DTS = m.F("land_dts"),
+  real *DLS = m.F("dls"), *DRIVER = m.F("driver"), *DRUNOFF = m.F("drunoff"), *LAND_DTS = m.F("land_dts"),
          *SS = m.F("surface_step"), *DALBCL = m.F("dalbcl"), *DALBCL1 = m.F("dalbcl1"), *DALBCL2 = m.F("dalbcl2"),
          *DWATER = m.F("dwater"), *DALBCLIM = m.F("dalbclim"), *DALBCLIM1 = m.F("dalbclim1"),
          *DALBCLIM2 = m.F("dalbclim2"), *LAND_DTSM = m.F("land_dtsm"), *DP = m.F("dp"), *LAND_DQS = m.F("land_dqs"),
@@ -1970,33 +1985,33 @@ void land_surface(Model& m) {
          *DSALB = m.F("dsalb"), *DRHS = m.F("drhs"), *DWMAX = m.F("dwmax"), *DWATC = m.F("dwatc"),
          *DTSOIL = m.F("dtsoil"), *DTD2 = m.F("dtd2"), *DTD3 = m.F("dtd3"), *DTD4 = m.F("dtd4"), *DTD5 = m.F("dtd5"),
          *DSOILT = m.F("dsoilt"), *DT = m.F("dt"), *DQ = m.F("dq"), *DGLAC = m.F("dglac"), *DPERSIST = m.F("dpersist");
-  double *CO2 = m.F("co2"), *DCVEG = m.F("dcveg"), *DCSOIL = m.F("dcsoil"), *DAGG = m.F("dagg"), *DFD = m.F("dfd"),
+  real *CO2 = m.F("co2"), *DCVEG = m.F("dcveg"), *DCSOIL = m.F("dcsoil"), *DAGG = m.F("dagg"), *DFD = m.F("dfd"),
          *DEVAP = m.F("devap"), *DGROW = m.F("dgrow"), *DNPP = m.F("dnpp"), *DVSOIL = m.F("dvsoil"),
          *DLAI = m.F("dlai"), *DMR = m.F("dmr"), *DSC = m.F("dsc"), *DZ0CLIMO = m.F("dz0climo"), *DZ0 = m.F("dz0");
-  auto clim = [&](const double* f, int h) {
-    double w = SS[5];
+  auto clim = [&](const real* f, int h) {
+    real w = SS[5];
     return (1.0 - w) * f[(int)SS[3] * NH + h] + w * f[(int)SS[4] * NH + h];
   };
-  auto snow_albedo = [&](double forest, double mxf, double mxb, double mnf, double mnb, double ts) {
-    double zmax = forest * mxf + (1.0 - forest) * mxb;
-    double zmin = forest * mnf + (1.0 - forest) * mnb;
-    double zd = (zmax - zmin) * (ts - 263.16) / (K.TMELT - 263.16);
+  auto snow_albedo = [&](real forest, real mxf, real mxb, real mnf, real mnb, real ts) {
+    real zmax = forest * mxf + (1.0 - forest) * mxb;
+    real zmin = forest * mnf + (1.0 - forest) * mnb;
+    real zd = (zmax - zmin) * (ts - 263.16) / (K.TMELT - 263.16);
     return std::max(zmin, std::min(zmax, zmax - zd));
   };
-  auto glacier_albedo = [&](double mx, double mn, double ts) {
+  auto glacier_albedo = [&](real mx, real mn, real ts) {
     return std::max(mn, std::min(mx, mx - (mx - mn) * (ts - 263.16) / (K.TMELT - 263.16)));
   };
   for (int h = 0; h < NH; ++h) {
-    double dls = DLS[h];
+    real dls = DLS[h];
     if (dls > 0.0) DRIVER[h] = DRIVER[h] + DRUNOFF[h] * K.DELTSEC;
-    double dts = LAND_DTS[h];
-    double albclim = clim(DALBCL, h), albclim1 = clim(DALBCL1, h), albclim2 = clim(DALBCL2, h);
+    real dts = LAND_DTS[h];
+    real albclim = clim(DALBCL, h), albclim1 = clim(DALBCL1, h), albclim2 = clim(DALBCL2, h);
     if (K.NWETSOIL != 0 && dls > 0.5) {
       if (dts > 273.15) {
-        double bf = DWATER[h] / K.WSMAX;
-        double al = 1.0 / 5.2 * fpow(fpow(std::max(bf, 1.0e-3), (1.0 - 4.0) / 4.0) - 1.0, 1.0 / 4.0);
-        double dry = std::exp(-powi(bf * 25.0, 6));
-        double wet = std::exp(-powi((1.0 - bf) * 30.0, 9));
+        real bf = DWATER[h] / K.WSMAX;
+        real al = 1.0 / 5.2 * fpow(fpow(std::max(bf, 1.0e-3), (1.0 - 4.0) / 4.0) - 1.0, 1.0 / 4.0);
+        real dry = std::exp(-powi(bf * 25.0, 6));
+        real wet = std::exp(-powi((1.0 - bf) * 30.0, 9));
         albclim = K.ALBLANDMAX * dry + al * (1.0 - dry - wet) + K.DOCEANALB1 * wet;
         albclim1 = albclim;
         albclim2 = K.ALBLANDMAX * dry + al * (1.0 - dry - wet) + K.DOCEANALB2 * wet;
@@ -2011,16 +2026,16 @@ void land_surface(Model& m) {
     DALBCLIM2[h] = albclim2;
     if (dls > 0.0) {
       LAND_DTSM[h] = dts;
-      double dqs = K.RDBRV * K.RA1 * std::exp(K.RA2 * (dts - K.TMELT) / (dts - K.RA4)) / DP[h];
+      real dqs = K.RDBRV * K.RA1 * std::exp(K.RA2 * (dts - K.TMELT) / (dts - K.RA4)) / DP[h];
       dqs = dqs / (1.0 - (1.0 / K.RDBRV - 1.0) * dqs);
       LAND_DQS[h] = dqs;
-      double dsnow = DSNOWZ[h];
+      real dsnow = DSNOWZ[h];
       DSNOW[h] = dsnow;
       if (dsnow > 0.0) {
-        double forest = DFOREST[h];
-        double s0 = snow_albedo(forest, K.ALBSMAXF, K.ALBSMAX, K.ALBSMINF, K.ALBSMIN, dts);
-        double s1 = snow_albedo(forest, K.ALBSMAXF1, K.ALBSMAX1, K.ALBSMINF1, K.ALBSMIN1, dts);
-        double s2 = snow_albedo(forest, K.ALBSMAXF2, K.ALBSMAX2, K.ALBSMINF2, K.ALBSMIN2, dts);
+        real forest = DFOREST[h];
+        real s0 = snow_albedo(forest, K.ALBSMAXF, K.ALBSMAX, K.ALBSMINF, K.ALBSMIN, dts);
+        real s1 = snow_albedo(forest, K.ALBSMAXF1, K.ALBSMAX1, K.ALBSMINF1, K.ALBSMIN1, dts);
+        real s2 = snow_albedo(forest, K.ALBSMAXF2, K.ALBSMAX2, K.ALBSMINF2, K.ALBSMIN2, dts);
         DALB[h] = albclim + (s0 - albclim) * dsnow / (dsnow + 0.01);
         DSALB[h] = albclim1 + (s1 - albclim1) * dsnow / (dsnow + 0.01);
         DSALB[NH + h] = albclim2 + (s2 - albclim2) * dsnow / (dsnow + 0.01);
@@ -2029,7 +2044,7 @@ void land_surface(Model& m) {
         DALB[h] = albclim;
         DSALB[h] = albclim1;
         DSALB[NH + h] = albclim2;
-        double dwmax = DWMAX[h];
+        real dwmax = DWMAX[h];
         if (dwmax > 0.0) DRHS[h] = std::min(1.0, DWATC[h] / (K.DRHSFULL * dwmax));
       }
       DTSOIL[h] = DSOILT[h];
@@ -2042,51 +2057,51 @@ void land_surface(Model& m) {
     }
     if (K.NVEG > 0 && DLS[h] > 0.0 && DGLAC[h] < 0.90) {
       // vegstep
-      double co2 = CO2[0];
-      double zbeta = 0;
+      real co2 = CO2[0];
+      real zbeta = 0;
       if (!(co2 < 1.0e-8))
         zbeta = std::max(0.0, 1.0 + K.CO2_SENS * std::log((co2 - K.CO2_COMP) / (K.CO2_REF - K.CO2_COMP)));
-      double ts = DT[NL * NH + h], dp = DP[h], dwatc = DWATC[h], dsnow = DSNOW[h];
-      double zwmax = DWMAX[h];
-      double zglacfree = 1.0 - DGLAC[h];
-      double zsvp = K.RA1 * std::exp(K.RA2 * (ts - K.TMELT) / (ts - K.RA4));
-      double zvpd = std::max(0.01, zsvp - dp * DQ[(NL - 1) * NH + h] / 0.622);
-      double dcveg = DCVEG[h], dcsoil = DCSOIL[h];
-      double zlaim = K.ZLAIMIN + 0.63661977236758 * K.ZLAIMAX * std::atan(K.CVEG_L * 2.0 * DAGG[h] * dcveg);
-      double zvegm = 1.0 - std::exp(-K.CVEG_K * zlaim);
-      double zveg = 0;
+      real ts = DT[NL * NH + h], dp = DP[h], dwatc = DWATC[h], dsnow = DSNOW[h];
+      real zwmax = DWMAX[h];
+      real zglacfree = 1.0 - DGLAC[h];
+      real zsvp = K.RA1 * std::exp(K.RA2 * (ts - K.TMELT) / (ts - K.RA4));
+      real zvpd = std::max(0.01, zsvp - dp * DQ[(NL - 1) * NH + h] / 0.622);
+      real dcveg = DCVEG[h], dcsoil = DCSOIL[h];
+      real zlaim = K.ZLAIMIN + 0.63661977236758 * K.ZLAIMAX * std::atan(K.CVEG_L * 2.0 * DAGG[h] * dcveg);
+      real zvegm = 1.0 - std::exp(-K.CVEG_K * zlaim);
+      real zveg = 0;
       if (zwmax > 0.0) zveg = std::min(std::min(1.0, zvegm), std::max(0.0, dwatc / (zwmax * K.VWS_CRIT)));
-      double zft = std::min(1.0, std::max(0.0, (ts - K.TMELT) / K.CT_CRIT));
-      double zgppl = K.RLUE * zbeta * zft * zveg * DFD[NL * NH + h];
-      double zgppw = 0;
+      real zft = std::min(1.0, std::max(0.0, (ts - K.TMELT) / K.CT_CRIT));
+      real zgppl = K.RLUE * zbeta * zft * zveg * DFD[NL * NH + h];
+      real zgppw = 0;
       if (!(co2 < 1.0e-8)) zgppw = K.CO2CONV * dp * zveg * (-DEVAP[h]) / zvpd * (0.3 * co2);
       zgppw = std::min(1.0, std::max(0.0, zgppw));
-      double zgpp = std::min(zgppl, zgppw);
-      double znpp = DGROW[h] * 0.5 * zgpp * zglacfree;
+      real zgpp = std::min(zgppl, zgppw);
+      real znpp = DGROW[h] * 0.5 * zgpp * zglacfree;
       DNPP[h] = znpp;
-      double zlitter = dcveg / K.TAU_VEG;
-      double zres = fpow(K.Q10, (ts - K.TMELT - 10.0) / 10.0) * dcsoil / K.TAU_SOIL;
+      real zlitter = dcveg / K.TAU_VEG;
+      real zres = fpow(K.Q10, (ts - K.TMELT - 10.0) / 10.0) * dcsoil / K.TAU_SOIL;
       dcveg = dcveg + (znpp - zlitter) * K.DELTSEC * K.NCVEG;
       dcsoil = dcsoil + (zlitter - zres) * K.DELTSEC * K.NCVEG;
-      double zforest = std::min(1.0, std::max(0.0, (std::atan(dcveg - K.CVEG_A) - K.CVEG_E) / (K.CVEG_C - K.CVEG_E)));
-      double dvsoil = std::min(1.0, std::max(0.0, (std::atan(dcveg - K.CVEG_F) - K.CVEG_G) / (K.CVEG_C - K.CVEG_G)));
+      real zforest = std::min(1.0, std::max(0.0, (std::atan(dcveg - K.CVEG_A) - K.CVEG_E) / (K.CVEG_C - K.CVEG_E)));
+      real dvsoil = std::min(1.0, std::max(0.0, (std::atan(dcveg - K.CVEG_F) - K.CVEG_G) / (K.CVEG_C - K.CVEG_G)));
       DCVEG[h] = dcveg;
       DCSOIL[h] = dcsoil;
       DVSOIL[h] = dvsoil;
       DLAI[h] = -std::log(1.0 - zveg) / K.CVEG_K;
-      double zvz0 = DMR[h] * zforest + K.VZ0_MIN * (1.0 - zforest);
-      double zvalb = K.VALB_MIN * zveg + K.VALB_MAX * (1.0 - zveg);
+      real zvz0 = DMR[h] * zforest + K.VZ0_MIN * (1.0 - zforest);
+      real zvalb = K.VALB_MIN * zveg + K.VALB_MAX * (1.0 - zveg);
       zwmax = K.VWMAX_MAX * dvsoil + K.VWMAX_MIN * (1.0 - dvsoil);
-      double zvrhs = DSC[h] * std::min(1.0, std::max(0.0, dwatc / (zwmax * K.VWS_CRIT)));
+      real zvrhs = DSC[h] * std::min(1.0, std::max(0.0, dwatc / (zwmax * K.VWS_CRIT)));
       if (dsnow > 0.0) {
-        double zalbsn = (K.ALBSMAX - K.ALBSMIN) * (ts - 263.16) / (K.TMELT - 263.16);
+        real zalbsn = (K.ALBSMAX - K.ALBSMIN) * (ts - 263.16) / (K.TMELT - 263.16);
         zalbsn = std::max(K.ALBSMIN, std::min(K.ALBSMAX, K.ALBSMAX - zalbsn));
         zvalb = zvalb + (zalbsn - zvalb) * dsnow / (dsnow + 0.01);
         zvalb = K.VSALB_MIN * zforest + zvalb * (1.0 - zforest);
         zvrhs = 1.0;
       }
       if (K.NVEG == 2) {
-        double z0c = DZ0CLIMO[h];
+        real z0c = DZ0CLIMO[h];
         DZ0[h] = std::sqrt(zvz0 * zvz0 + z0c * z0c);
         DWMAX[h] = zwmax;
         DRHS[h] = zvrhs;
@@ -2116,7 +2131,7 @@ void land_surface(Model& m) {
 void sea_ice(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NL = m.NLEV;
-  double *DLS = m.F("dls"), *NACC = m.F("sea_naccua"), *DSHFL = m.F("dshfl"), *DSWFL = m.F("dswfl"),
+  real *DLS = m.F("dls"), *NACC = m.F("sea_naccua"), *DSHFL = m.F("dshfl"), *DSWFL = m.F("dswfl"),
          *DLWFL = m.F("dlwfl"), *DLHFL = m.F("dlhfl"), *CHEATA = m.F("sea_cheata"), *DPRS = m.F("dprs"),
          *CPRSA = m.F("sea_cprsa"), *SS = m.F("surface_step"), *XCLSSTO = m.F("xclssto"), *XCLSST = m.F("xclsst"),
          *XCLSST2 = m.F("xclsst2"), *XCLICED = m.F("xcliced"), *XCLICEC = m.F("xclicec"), *XCLICED2 = m.F("xcliced2"),
@@ -2126,47 +2141,47 @@ void sea_ice(Model& m) {
          *XOFLUX = m.F("xoflux"), *ZFLX = m.F("ice_zflx"), *XGW = m.F("xgw"), *P1 = m.F("ice_part1"),
          *P2 = m.F("ice_part2"), *XCFLUXR = m.F("xcfluxr"), *XIMELT = m.F("ximelt"), *XSMELT = m.F("xsmelt"),
          *XSMFLX = m.F("xsmflx"), *XSNDCH = m.F("xsndch"), *SUMS = m.F("ice_sums");
-  auto clim = [&](const double* f, int h, int off) {
-    double w = SS[off + 2];
+  auto clim = [&](const real* f, int h, int off) {
+    real w = SS[off + 2];
     return (1.0 - w) * f[(int)SS[off] * NH + h] + w * f[(int)SS[off + 1] * NH + h];
   };
   for (int h = 0; h < NH; ++h) {
     bool sea = DLS[h] < 0.5;
-    double xheat = 0, xprs = 0;
+    real xheat = 0, xprs = 0;
     if (sea) {
-      double naccua = NACC[h] + 1.0;
+      real naccua = NACC[h] + 1.0;
       xheat = (DSHFL[h] + DSWFL[NL * NH + h] + DLWFL[NL * NH + h] + DLHFL[h] + CHEATA[h]) / naccua;
       xprs = (DPRS[h] + CPRSA[h]) / naccua;
     }
     CHEATA[h] = 0;
     CPRSA[h] = 0;
     NACC[h] = 0;
-    double zrhoilfdt = K.CRHOI * K.CLFI / K.XDT;
+    real zrhoilfdt = K.CRHOI * K.CLFI / K.XDT;
     XCLSSTO[h] = clim(XCLSST, h, 0);
     XCLSST2[h] = clim(XCLSST, h, 3);
-    double cliced = std::max(clim(XCLICED, h, 3), 0.0);
-    double clicec = std::max(clim(XCLICEC, h, 3), 0.0);
+    real cliced = std::max(clim(XCLICED, h, 3), 0.0);
+    real clicec = std::max(clim(XCLICEC, h, 3), 0.0);
     if (cliced <= 0.0) clicec = 0.0;
     XCLICED2[h] = cliced;
     XCLICEC2[h] = clicec;
-    double xls = XLS[h], xsst = XSST[h], xiced = XICED[h], xsnow = XSNOW[h], xicecc = XICECC[h],
+    real xls = XLS[h], xsst = XSST[h], xiced = XICED[h], xsnow = XSNOW[h], xicecc = XICECC[h],
            xcflux = XCFLUX[h], xcfluxf = XCFLUXF[h];
     SNOWOLD[h] = xsnow;
-    double zicedold = xls < 0.5 ? xiced : 0.0;
-    double ximelt = 0, xsmelt = 0, xsmflx = 0, xscflx = 0, xsndch = 0, xcfluxr = 0;
+    real zicedold = xls < 0.5 ? xiced : 0.0;
+    real ximelt = 0, xsmelt = 0, xsmflx = 0, xscflx = 0, xsndch = 0, xcfluxr = 0;
     if (XICEC[h] >= K.CICEMIN) {
       xsnow = xsnow + xprs * K.XDT;
       xprs = 0;
     }
-    double xts = XTS[h], xqmelt = 0;
-    double ztso = std::min(K.TMELT, xts);
-    double zhsnow = 1.0e3 / K.CRHOSN * xsnow;
+    real xts = XTS[h], xqmelt = 0;
+    real ztso = std::min(K.TMELT, xts);
+    real zhsnow = 1.0e3 / K.CRHOSN * xsnow;
     if (xiced >= K.XMIND) {
-      double zcpdt = K.XMIND * K.CRHOI * K.CPI / K.XDT;
-      double zckap = (K.CKAPSN * zhsnow + K.CKAPI * xiced) / (zhsnow + xiced);
-      double zkapz = zckap / (xiced + zhsnow);
+      real zcpdt = K.XMIND * K.CRHOI * K.CPI / K.XDT;
+      real zckap = (K.CKAPSN * zhsnow + K.CKAPI * xiced) / (zhsnow + xiced);
+      real zkapz = zckap / (xiced + zhsnow);
       if (xiced >= K.XMAXD && K.XMAXD >= 0.0) zkapz = 0.0;
-      double zflx = xheat + zkapz * xsst;
+      real zflx = xheat + zkapz * xsst;
       xts = (zcpdt * ztso + zflx) / (zcpdt + zkapz);
       if (xts > K.TMELT) {
         xqmelt = xheat + zkapz * (xsst - K.TMELT) - zcpdt * (K.TMELT - ztso);
@@ -2182,8 +2197,8 @@ void sea_ice(Model& m) {
       xcflux = xheat;
       xcfluxf = 0.0;
     } else {
-      double zhsnowc = 1.0e3 / K.CRHOSN * xsnow;
-      double zckap = (K.CKAPSN * zhsnowc + K.CKAPI * xiced) / (zhsnowc + xiced);
+      real zhsnowc = 1.0e3 / K.CRHOSN * xsnow;
+      real zckap = (K.CKAPSN * zhsnowc + K.CKAPI * xiced) / (zhsnowc + xiced);
       if (K.XMAXD >= 0.0 && xiced >= K.XMAXD) zckap = 0.0;
       xcflux = zckap * (xts - xsst) / (zhsnowc + xiced);
       xcfluxf = zckap * (K.TFREEZE - xsst) / (zhsnowc + xiced);
@@ -2194,7 +2209,7 @@ void sea_ice(Model& m) {
       xsmflx = xsmflx + xprs * 1000.0 * K.CLFSN;
       xprs = 0;
     }
-    double zqmelt = xqmelt;
+    real zqmelt = xqmelt;
     if (xiced > 0.0) {
       if (xqmelt > xsnow * 1000.0 * K.CLFSN / K.XDT) {
         xsmelt = xsmelt + xsnow / K.XDT;
@@ -2215,9 +2230,9 @@ void sea_ice(Model& m) {
       xsnow = 0;
     }
     if (xls < 0.5 && 1.0e3 * xsnow > (K.CRHOS - K.CRHOI) * xiced) {
-      double zhice = (1.0e3 * xsnow + K.CRHOI * xiced) / K.CRHOS;
-      double zdice = zhice - xiced;
-      double zdsnow = -zdice * K.CRHOI / 1.0e3;
+      real zhice = (1.0e3 * xsnow + K.CRHOI * xiced) / K.CRHOS;
+      real zdice = zhice - xiced;
+      real zdsnow = -zdice * K.CRHOI / 1.0e3;
       xsnow = xsnow + zdsnow;
       xscflx = zdsnow * 1.0e3 * K.CLFSN / K.XDT;
       xsmelt = xsmelt - zdsnow / K.XDT;
@@ -2239,16 +2254,16 @@ void sea_ice(Model& m) {
     if (xiced < zicedold) xicecc = std::max(xicecc + xicecc * (xiced - zicedold) / (2.0 * zicedold), 0.0);
     if (xiced <= 0.0) xicecc = 0;
     if (K.XMAXD >= 0.0 && xiced > K.XMAXD) {
-      double zcflux = (xiced - K.XMAXD) * zrhoilfdt;
+      real zcflux = (xiced - K.XMAXD) * zrhoilfdt;
       xiced = K.XMAXD;
       xcfluxr = xcfluxr + zcflux;
       ximelt = ximelt + zcflux;
       xsndch = xsndch + zcflux * 1000.0 / K.CRHOI / zrhoilfdt;
     }
-    double zflx = ZFLX[h];
+    real zflx = ZFLX[h];
     if (xls < 1.0) zflx = std::max(0.0, K.XMAXD - xiced) * zrhoilfdt;
     ZFLX[h] = zflx;
-    double xgw = XGW[h];
+    real xgw = XGW[h];
     P1[h] = xls < 1.0 ? xcfluxr * xgw : 0.0;
     P2[h] = xls < 1.0 ? zflx * xgw : 0.0;
     XICED[h] = xiced;
@@ -2263,7 +2278,7 @@ void sea_ice(Model& m) {
     XSMFLX[h] = xsmflx;
     XSNDCH[h] = xsndch;
   }
-  double a = 0, b = 0;
+  real a = 0, b = 0;
   for (int h = 0; h < NH; ++h) {
     a += P1[h];
     b += P2[h];
@@ -2278,7 +2293,7 @@ void sea(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NL = m.NLEV;
   const bool coupled = K.ICE_COUPLED != 0;
-  double *XLS = m.F("xls"), *XCFLUX = m.F("xcflux"), *XCFLUXR = m.F("xcfluxr"), *SUMS = m.F("ice_sums"),
+  real *XLS = m.F("xls"), *XCFLUX = m.F("xcflux"), *XCFLUXR = m.F("xcfluxr"), *SUMS = m.F("ice_sums"),
          *ZFLX = m.F("ice_zflx"), *XICED = m.F("xiced"), *XICEC = m.F("xicec"), *XSNOW = m.F("xsnow"),
          *XSMELT = m.F("xsmelt"), *XSMFLX = m.F("xsmflx"), *XOFLUX = m.F("xoflux"), *XOHEAT = m.F("xoheat"),
          *XSNDCH = m.F("xsndch"), *SNOWOLD = m.F("ice_snowold"), *SS = m.F("surface_step"), *YCLSST = m.F("yclsst"),
@@ -2293,20 +2308,20 @@ void sea(Model& m) {
   for (int h = 0; h < NH; ++h) {
     if (coupled) {
       // ice_finish
-      double xls = XLS[h], xcflux = XCFLUX[h], xcfluxr = XCFLUXR[h], s1 = SUMS[0], s2 = SUMS[1];
+      real xls = XLS[h], xcflux = XCFLUX[h], xcfluxr = XCFLUXR[h], s1 = SUMS[0], s2 = SUMS[1];
       if (s1 > 0.0 && s2 > 0.0 && xls < 1.0) {
-        double zflx = ZFLX[h];
-        double zfac = s1 / s2;
+        real zflx = ZFLX[h];
+        real zfac = s1 / s2;
         if (zfac <= 1.0) zflx = zflx * zfac;
         xcfluxr = xcfluxr - zflx;
         xcflux = xcflux - zflx;
       }
       XCFLUXR[h] = xcfluxr;
-      double xiced = XICED[h];
-      double xicec = XICEC[h] >= K.THICEC ? 1.0 : 0.0;
-      double xsnow = XSNOW[h], xsmelt = XSMELT[h];
+      real xiced = XICED[h];
+      real xicec = XICEC[h] >= K.THICEC ? 1.0 : 0.0;
+      real xsnow = XSNOW[h], xsmelt = XSMELT[h];
       if (xiced <= 0.0 && xsnow > 0.0) {
-        double zcflux = xsnow * 1000.0 * K.CLFSN / K.XDT;
+        real zcflux = xsnow * 1000.0 * K.CLFSN / K.XDT;
         xsmelt = xsmelt + xsnow / K.XDT;
         XSMFLX[h] = XSMFLX[h] + zcflux;
         xcflux = xcflux - zcflux;
@@ -2317,13 +2332,13 @@ void sea(Model& m) {
       XSMELT[h] = xsmelt;
       XCFLUX[h] = xcflux;
       bool sea = xls < 0.5;
-      double heat = sea ? xcflux : 0.0;
+      real heat = sea ? xcflux : 0.0;
       // oceanstep
-      double w = SS[5];
+      real w = SS[5];
       YCLSST2[h] = (1.0 - w) * YCLSST[(int)SS[3] * NH + h] + w * YCLSST[(int)SS[4] * NH + h];
-      double yls = YLS[h], yiced = XICED[h], ymld = YMLD[h], yfldo = YFLDO[h];
-      double zcpsdt = K.DTMIX / (K.CRHOS * K.CPS);
-      double ysst = YSST[h], zsst = ysst, yiflux = 0;
+      real yls = YLS[h], yiced = XICED[h], ymld = YMLD[h], yfldo = YFLDO[h];
+      real zcpsdt = K.DTMIX / (K.CRHOS * K.CPS);
+      real ysst = YSST[h], zsst = ysst, yiflux = 0;
       if (yls < 1.0 && yiced <= 0.0) zsst = zsst + (heat + yfldo) * zcpsdt / ymld;
       if (yls < 1.0 && yiced > 0.0) yiflux = yiflux - yfldo - heat;
       if (ysst < K.TFREEZE && yls < 1.0) {
@@ -2331,7 +2346,7 @@ void sea(Model& m) {
         zsst = K.TFREEZE;
       }
       if (yiced > 0.0 && yls < 1.0) {
-        double zf = (K.TFREEZE - zsst) * ymld / zcpsdt;
+        real zf = (K.TFREEZE - zsst) * ymld / zcpsdt;
         zsst = zsst + zf * zcpsdt / ymld;
         yiflux = yiflux + zf;
       }
@@ -2345,7 +2360,7 @@ void sea(Model& m) {
       NACC[h] = NACC[h] + 1.0;
     }
     if (!(DLS[h] < 0.5)) continue;
-    double dts = XTS[h], dicec = XICEC[h];
+    real dts = XTS[h], dicec = XICEC[h];
     if (coupled) {
       SEA_DSST[h] = XSST[h];
       SEA_DTS[h] = dts;
@@ -2359,14 +2374,14 @@ void sea(Model& m) {
       CHEATA[h] = DSHFL[h] + DSWFL[NL * NH + h] + DLWFL[NL * NH + h] + DLHFL[h] + CHEATA[h];
       CPRSA[h] = DPRS[h] + CPRSA[h];
     }
-    double dp = DP[h];
+    real dp = DP[h];
     DT[NL * NH + h] = dts;
-    double dqs = K.RDBRV * K.RA1 * std::exp(K.RA2 * (dts - K.TMELT) / (dts - K.RA4)) / dp;
+    real dqs = K.RDBRV * K.RA1 * std::exp(K.RA2 * (dts - K.TMELT) / (dts - K.RA4)) / dp;
     dqs = dqs / (1.0 - (1.0 / K.RDBRV - 1.0) * dqs);
     SEA_DQS[h] = dqs;
     DQ[NL * NH + h] = dqs;
-    double taux = DTAUX[h], tauy = DTAUY[h];
-    double zz0 = std::max(K.CHARNOCK * std::sqrt(taux * taux + tauy * tauy) * K.GASCON * dts / (K.GA * dp), K.DZ0SEA);
+    real taux = DTAUX[h], tauy = DTAUY[h];
+    real zz0 = std::max(K.CHARNOCK * std::sqrt(taux * taux + tauy * tauy) * K.GASCON * dts / (K.GA * dp), K.DZ0SEA);
     DRHS[h] = K.DRHSSEA * (1.0 - dicec) + K.DRHSICE * dicec;
     DALB[h] = K.ALBSEA * (1.0 - dicec) + dicec * std::min(K.ALBICE, 0.5 + 0.025 * (273.0 - dts));
     DSALB[h] = K.DOCEANALB1 * (1.0 - dicec) + dicec * std::min(K.DICEALBMX1, K.DICEALBMN1 + 0.025 * (273.0 - dts));
@@ -2379,22 +2394,22 @@ void sea(Model& m) {
 void carbon(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NL = m.NLEV;
-  double *DPRC = m.F("dprc"), *DPRL = m.F("dprl"), *LP = m.F("localprecip"), *LAP = m.F("localavgprecip"),
+  real *DPRC = m.F("dprc"), *DPRL = m.F("dprl"), *LP = m.F("localprecip"), *LAP = m.F("localavgprecip"),
          *CS = m.F("carbon_step"), *DT = m.F("dt"), *DLS = m.F("dls"), *CO2 = m.F("co2"), *DP = m.F("dp"),
          *LW = m.F("localweathering"), *LAT = m.F("localavgtemps"), *LAW = m.F("localavgweather");
   for (int h = 0; h < NH; ++h) {
-    double precip = (DPRC[h] + DPRL[h]) * 3.154e9;
+    real precip = (DPRC[h] + DPRL[h]) * 3.154e9;
     LP[h] = precip;
     LAP[h] = LAP[h] + precip * K.TIMEWEIGHT;
     if (CS[0] == 0.0) continue;
-    double tsurf = DT[NL * NH + h];
+    real tsurf = DT[NL * NH + h];
     if (K.NCARBON != 0) {
-      double weathering = 0;
+      real weathering = 0;
       if (DLS[h] > 0.5 && tsurf >= 273.15) {
-        double pco2 = CO2[0] * DP[h] * 1.0e-5;
+        real pco2 = CO2[0] * DP[h] * 1.0e-5;
         weathering = fpow(pco2 / K.CO2EARTH, K.BETA) * std::exp(K.KACT * (tsurf - 288.0)) * fpow(precip / K.PEARTH, 0.65);
         if (K.NSUPPLY != 0) {
-          double wmaxp = std::max(K.WMAX / K.VEARTH, 2.0e-15);
+          real wmaxp = std::max(K.WMAX / K.VEARTH, 2.0e-15);
           weathering = wmaxp * (1.0 - std::exp(-weathering / wmaxp));
         }
       }
@@ -2409,11 +2424,11 @@ void carbon(Model& m) {
 void pack(Model& m) {
   const Consts& K = m.k;
   const int NH = m.NHOR, NL = m.NLEV;
-  double *SNAP = m.F("snapshot"), *TR = m.F("snapshot_tracking"), *SS = m.F("snapshot_step"), *DT = m.F("dt");
+  real *SNAP = m.F("snapshot"), *TR = m.F("snapshot_tracking"), *SS = m.F("snapshot_step"), *DT = m.F("dt");
   int step = (int)SS[0], window = (int)SS[1];
   int jet = (int)K.JET;
-  auto put = [&](int index, int h, double v) { SNAP[index * NH + h] = v; };
-  double *DTSA = m.F("dtsa"), *DU = m.F("du"), *DV = m.F("dv"), *DCC = m.F("dcc"), *DPRC = m.F("dprc"),
+  auto put = [&](int index, int h, real v) { SNAP[index * NH + h] = v; };
+  real *DTSA = m.F("dtsa"), *DU = m.F("du"), *DV = m.F("dv"), *DCC = m.F("dcc"), *DPRC = m.F("dprc"),
          *DPRL = m.F("dprl"), *DP = m.F("dp"), *DQVI = m.F("dqvi"), *DICEC = m.F("dicec"), *DSNOW = m.F("dsnow"),
          *DWATC = m.F("dwatc"), *DALB = m.F("dalb"), *DLWFL = m.F("dlwfl"), *DLS = m.F("dls"), *DSWFL = m.F("dswfl"),
          *DSMELT = m.F("dsmelt"), *DSHFL = m.F("dshfl"), *DLHFL = m.F("dlhfl"), *DEVAP = m.F("devap"),
@@ -2421,8 +2436,8 @@ void pack(Model& m) {
          *DICED = m.F("diced"), *DGLAC = m.F("dglac"), *DNPP = m.F("dnpp"), *GMU0 = m.F("gmu0"), *DQ = m.F("dq");
   const char* storm[9] = {"capen", "lnb", "mpoti", "chim", "laav", "venti", "vrmpi", "gpi", "shear"};
   for (int h = 0; h < NH; ++h) {
-    double t = DT[NL * NH + h];
-    double* tr = TR + h;
+    real t = DT[NL * NH + h];
+    real* tr = TR + h;
     if (tr[7 * NH] == 0.0) {
       tr[0] = t;
       tr[NH] = t;
@@ -2431,7 +2446,7 @@ void pack(Model& m) {
     tr[0] = std::min(tr[0], t);
     tr[NH] = std::max(tr[NH], t);
     if (step > 0 && step % window == 0) {
-      double range = tr[NH] - tr[0];
+      real range = tr[NH] - tr[0];
       tr[2 * NH] = tr[0];
       tr[3 * NH] = tr[NH];
       tr[4 * NH] = range;
@@ -2494,7 +2509,7 @@ void pack(Model& m) {
     }
     for (int i = 0; i < 9; ++i) put(42 + i, h, m.F(storm[i])[h]);
     int lowest = NL - 1;
-    double qsat = sat_divided(K, DT[lowest * NH + h], DP[h] * K.SIGMA_LOW);
+    real qsat = sat_divided(K, DT[lowest * NH + h], DP[h] * K.SIGMA_LOW);
     put(51 + 5 * lowest + 3, h, std::max(0.0, DQ[lowest * NH + h]) / std::max(1.17549435e-38, qsat));
   }
 }
@@ -2639,7 +2654,7 @@ int ora_set_const(void* p, const char* name, double value) {
   Model& m = *static_cast<Model*>(p);
 #define SETC(n)                     \
   if (std::strcmp(name, #n) == 0) { \
-    m.k.n = value;                  \
+    m.k.n = (real)value;            \
     return 0;                       \
   }
   ORACLE_CONSTS(SETC)
@@ -2665,9 +2680,11 @@ int ora_set(void* p, int kind, const char* name, const double* values, long n) {
       g_error = std::string("bad state field ") + name;
       return -1;
     }
-    std::memcpy(it->second.data(), values, sizeof(double) * n);
+    for (long i = 0; i < n; ++i) it->second[i] = (real)values[i];
   } else {
-    m.tables[name] = Vec(values, values + n);
+    Vec v((size_t)n);
+    for (long i = 0; i < n; ++i) v[i] = (real)values[i];
+    m.tables[name] = std::move(v);
   }
   return 0;
 }
@@ -2680,7 +2697,7 @@ int ora_get(void* p, int kind, const char* name, double* values, long n) {
     g_error = std::string("bad field ") + name;
     return -1;
   }
-  std::memcpy(values, it->second.data(), sizeof(double) * n);
+  for (long i = 0; i < n; ++i) values[i] = (double)it->second[i];
   return 0;
 }
 

@@ -49,3 +49,57 @@ def rel_rms_without_worst_columns(got, ref, nhor, drop):
     keep = np.ones(nhor, dtype=bool)
     keep[np.argsort(col)[::-1][:drop]] = False
     return rel_rms(got[:, keep], ref[:, keep])
+
+
+# The reference's V3 gate (scripts/exoplasim-webgpu/verify-dynamics.mjs:56-59,
+# 179-204). A point is off when it differs from f64 by more than
+# POINT_TOLERANCE of the field's RMS; a field passes when the GPU's relative
+# RMS error is within twice the sequential-f32 build's and its off-point count
+# within twice the f32 count plus one. A grid field that fails because one
+# column holds more than OUTLIER_SHARE of the GPU's squared error is judged
+# again without that one column.
+POINT_TOLERANCE = 1e-5
+OUTLIER_SHARE = 0.5
+
+
+def _rms(values, reference=None):
+    values = np.asarray(values, dtype=np.float64)
+    d = values if reference is None else values - np.asarray(reference, dtype=np.float64)
+    return float(np.sqrt(np.mean(d * d))) if d.size else 0.0
+
+
+def count_off(values, reference, scale):
+    d = np.abs(np.asarray(values, dtype=np.float64) - np.asarray(reference, dtype=np.float64))
+    return int(np.count_nonzero(d > POINT_TOLERANCE * scale))
+
+
+def within_gate(gpu_error, f32_error, gpu_off, f32_off):
+    return gpu_error <= 2 * f32_error and gpu_off <= 2 * f32_off + 1
+
+
+def v3_gate(gpu, exact, f32, points=None):
+    """Judges one field as verify-dynamics.mjs does. `points` is the grid's
+    column count for grid fields (the outlier rule applies to them only).
+    Returns a dict with the errors, counts, the verdict and any outlier."""
+    gpu = np.asarray(gpu, dtype=np.float64).reshape(-1)
+    exact = np.asarray(exact, dtype=np.float64).reshape(-1)
+    f32 = np.asarray(f32, dtype=np.float64).reshape(-1)
+    scale = _rms(exact)
+    if scale == 0:
+        ok = _rms(gpu) == 0
+        return dict(gpu=0.0 if ok else np.inf, f32=0.0, gpu_off=0, f32_off=0, ok=ok, outlier=None)
+    r = dict(gpu=_rms(gpu, exact) / scale, f32=_rms(f32, exact) / scale,
+             gpu_off=count_off(gpu, exact, scale), f32_off=count_off(f32, exact, scale), outlier=None)
+    r["ok"] = within_gate(r["gpu"], r["f32"], r["gpu_off"], r["f32_off"])
+    if not r["ok"] and points and gpu.size % points == 0:
+        sq = ((gpu - exact) ** 2).reshape(-1, points).sum(axis=0)
+        total = sq.sum()
+        column = int(np.argmax(sq))
+        if total > 0 and sq[column] / total > OUTLIER_SHARE:
+            keep = np.arange(gpu.size) % points != column
+            g, e, s = gpu[keep], exact[keep], f32[keep]
+            out = dict(column=column, share=float(sq[column] / total), gpu=_rms(g, e) / scale,
+                       f32=_rms(s, e) / scale, gpu_off=count_off(g, e, scale), f32_off=count_off(s, e, scale))
+            r["outlier"] = out
+            r["ok"] = within_gate(out["gpu"], out["f32"], out["gpu_off"], out["f32_off"])
+    return r

@@ -72,6 +72,9 @@ SIGNATURES = {
                                             _DP, ctypes.POINTER(ctypes.c_size_t)]),
     "exogcm_release": (ctypes.c_int, [_VP, ctypes.c_int]),
     "exogcm_step": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
+    "exogcm_step_async": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
+    "exogcm_poll": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int)]),
+    "exogcm_wait": (ctypes.c_int, [_VP]),
     "exogcm_snapshots_begin": (ctypes.c_int, [_VP, _FP, ctypes.c_size_t]),
     "exogcm_snapshots_wait": (ctypes.c_int, [_VP]),
     "exogcm_read_snapshot": (ctypes.c_int, [_VP, ctypes.c_int, _FP, ctypes.c_size_t,
@@ -219,6 +222,19 @@ class Engine:
 
     def step(self, steps: int = 1, publish_every: int | None = None) -> None:
         _check(_lib.exogcm_step(self.h, steps, publish_every or max(steps, 1 << 20)))
+
+    def step_async(self, steps: int = 1, publish_every: int | None = None) -> None:
+        """Submits a batch and returns at once (at most two in flight)."""
+        _check(_lib.exogcm_step_async(self.h, steps, publish_every or max(steps, 1 << 20)))
+
+    def poll(self) -> bool:
+        """True when no batch is in flight; never blocks."""
+        done = ctypes.c_int()
+        _check(_lib.exogcm_poll(self.h, ctypes.byref(done)))
+        return bool(done.value)
+
+    def wait(self) -> None:
+        _check(_lib.exogcm_wait(self.h))
 
     def run_stage(self, stage: str) -> None:
         _check(_lib.exogcm_run_stage(self.h, stage.encode()))

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <functional>
 #include <map>
 #include <memory>
@@ -73,6 +74,7 @@ struct Slot {
 };
 
 constexpr int kMaxBatch = 64;
+constexpr int kInFlight = 2;  // batches exogcm_step_async keeps submitted
 
 }  // namespace
 
@@ -100,7 +102,19 @@ struct exogcm_engine {
   float* tabs = nullptr;
   PlanetConst* pc = nullptr;
   StepParams* params = nullptr;   // device [kMaxBatch][S]
-  StepParams* hparams = nullptr;  // pinned host
+  StepParams* hparams = nullptr;  // pinned host [1 + kInFlight][kMaxBatch][S]: row 0 for synchronous calls
+  // Batches submitted by exogcm_step_async and not yet retired, oldest first
+  // (the reference's worker keeps IN_FLIGHT = 2 batches submitted,
+  // runner/webgpu/gcm.worker.ts:215-225). Batch b uploads its step values
+  // from its own pinned row 1 + b, so the host never overwrites values a
+  // queued copy has yet to read, and copies the device fault word into its
+  // own pinned int before recording its end event.
+  struct Batch {
+    cudaEvent_t start = nullptr, end = nullptr, done = nullptr;
+    int* fault_host = nullptr;
+  };
+  Batch batch[kInFlight];
+  std::deque<int> pending;
   double* sums = nullptr;
   int* flags = nullptr;
   int* fault = nullptr;  // device word: a kernel gave up a bounded wait
@@ -722,6 +736,35 @@ void autotune(exogcm_engine* e) {
   }
 }
 
+// Retires the oldest batch in flight once its stream has passed it:
+// blocking waits for it, otherwise a batch not yet done is left alone and
+// false returned. Reports a fault word a tensor-core transform set.
+bool retire_oldest(exogcm_engine* e, bool blocking) {
+  if (e->pending.empty()) return false;
+  exogcm_engine::Batch& B = e->batch[e->pending.front()];
+  if (blocking) {
+    check(cudaEventSynchronize(B.done), "step");
+  } else {
+    const cudaError_t q = cudaEventQuery(B.done);
+    if (q == cudaErrorNotReady) return false;
+    check(q, "step");
+  }
+  e->pending.pop_front();
+  check(cudaEventElapsedTime(&e->last_ms, B.start, B.end), "event time");
+  if (*B.fault_host) {
+    *B.fault_host = 0;
+    throw Error(EXOGCM_EDEVICE, "a tensor-core transform gave up waiting for its MMAs; this step's results are invalid");
+  }
+  return true;
+}
+
+// Every call other than exogcm_step_async/poll/wait first retires the batches
+// in flight: they read and write host slot state and device memory the
+// batches use, through copies that do not order with the engine's stream.
+void retire_all(exogcm_engine* e) {
+  while (!e->pending.empty()) retire_oldest(e, true);
+}
+
 }  // namespace
 
 extern "C" {
@@ -762,7 +805,15 @@ int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine
     check(cudaMemset(e->pc, 0, slots * sizeof(PlanetConst)), "constants");
     check(cudaMalloc(&e->params, (size_t)kMaxBatch * slots * sizeof(StepParams)), "params");
     check(cudaMemset(e->params, 0, (size_t)kMaxBatch * slots * sizeof(StepParams)), "params");
-    check(cudaMallocHost(&e->hparams, (size_t)kMaxBatch * slots * sizeof(StepParams)), "pinned params");
+    check(cudaMallocHost(&e->hparams, (size_t)(1 + kInFlight) * kMaxBatch * slots * sizeof(StepParams)),
+          "pinned params");
+    for (auto& b : e->batch) {
+      check(cudaEventCreate(&b.start), "event");
+      check(cudaEventCreate(&b.end), "event");
+      check(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming), "event");
+      check(cudaMallocHost(&b.fault_host, sizeof(int)), "pinned fault word");
+      *b.fault_host = 0;
+    }
     check(cudaMalloc(&e->sums, (size_t)slots * 4 * sizeof(double)), "sums");
     check(cudaMemset(e->sums, 0, (size_t)slots * 4 * sizeof(double)), "sums");
     check(cudaMalloc(&e->flags, slots * sizeof(int)), "flags");
@@ -801,6 +852,12 @@ void exogcm_destroy(exogcm_engine* e) {
   cudaFree(e->fault);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
+  for (auto& b : e->batch) {
+    if (b.start) cudaEventDestroy(b.start);
+    if (b.end) cudaEventDestroy(b.end);
+    if (b.done) cudaEventDestroy(b.done);
+    cudaFreeHost(b.fault_host);
+  }
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -812,6 +869,7 @@ int exogcm_configure(exogcm_engine* e, int slot, const exogcm_planet* planet, co
     if (planet->truncation != e->d.T || planet->levels != e->d.L)
       throw Error(EXOGCM_EINVAL, "planet resolution differs from the engine's");
     if (!e->shared_ready) {
+      retire_all(e);
       e->shared_setup = build_shared(e->d.T, planet->filter_kind, planet->filter_gp, planet->filter_sp);
       upload_shared(e, e->shared_setup);
       if (e->mode >= 1) autotune(e);
@@ -822,7 +880,10 @@ int exogcm_configure(exogcm_engine* e, int slot, const exogcm_planet* planet, co
                planet->filter_sp != e->filter_sp) {
       throw Error(EXOGCM_EINVAL, "planets of one engine share the physics filter setting");
     }
+    // The host set-up runs while batches already submitted step on the
+    // device; the slot's upload waits for them.
     PlanetSetup ps = build_planet(*planet, *boundary, e->shared_setup);
+    retire_all(e);
     zero_slot(e, slot);
     for (auto& kv : ps.state) {
       const FieldInfo& fi = field(e, kv.first.c_str());
@@ -905,45 +966,73 @@ int exogcm_setup_preview(const exogcm_planet* planet, const exogcm_boundary* bou
 int exogcm_release(exogcm_engine* e, int slot) {
   return guard([&] {
     if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    retire_all(e);
     check_slot(e, slot);
     e->slots[slot].active = false;
     e->slots[slot].published = -1;
   });
 }
 
-int exogcm_step(exogcm_engine* e, int steps, int publish_every) {
+int exogcm_step_async(exogcm_engine* e, int steps, int publish_every) {
   return guard([&] {
     if (!e) throw Error(EXOGCM_EINVAL, "null engine");
     if (steps < 1 || steps > kMaxBatch) throw Error(EXOGCM_EINVAL, "steps must be 1..64");
     if (publish_every < 1 || steps > publish_every)
       throw Error(EXOGCM_EINVAL, "publish_every must be >= steps so each slot publishes at most once");
     if (!e->shared_ready) throw Error(EXOGCM_ESTATE, "no slot configured");
+    // A third batch waits for the oldest to finish (IN_FLIGHT = 2).
+    while ((int)e->pending.size() >= kInFlight) retire_oldest(e, true);
+    int b = 0;
+    while (std::find(e->pending.begin(), e->pending.end(), b) != e->pending.end()) ++b;
+    exogcm_engine::Batch& B = e->batch[b];
     const int S = e->d.S;
+    StepParams* rows = e->hparams + (size_t)(1 + b) * kMaxBatch * S;
     for (int s = 0; s < S; ++s) e->slots[s].published = -1;
     for (int k = 0; k < steps; ++k)
-      for (int s = 0; s < S; ++s) e->hparams[(size_t)k * S + s] = next_params(e->slots[s], publish_every, true);
-    check(cudaMemcpyAsync(e->params, e->hparams, (size_t)steps * S * sizeof(StepParams), cudaMemcpyHostToDevice,
+      for (int s = 0; s < S; ++s) rows[(size_t)k * S + s] = next_params(e->slots[s], publish_every, true);
+    check(cudaMemcpyAsync(e->params, rows, (size_t)steps * S * sizeof(StepParams), cudaMemcpyHostToDevice,
                           e->stream),
           "params upload");
     cudaGraphExec_t g = batch_graph(e, steps);
-    check(cudaEventRecord(e->ev0, e->stream), "event");
+    check(cudaEventRecord(B.start, e->stream), "event");
     check(cudaGraphLaunch(g, e->stream), "graph launch");
-    check(cudaEventRecord(e->ev1, e->stream), "event");
+    check(cudaEventRecord(B.end, e->stream), "event");
     phy_finite_check(e->model(steps - 1), e->stream);
-    check(cudaStreamSynchronize(e->stream), "step");
-    int fault = 0;
-    check(cudaMemcpy(&fault, e->fault, sizeof(int), cudaMemcpyDeviceToHost), "fault word");
-    if (fault) {
-      check(cudaMemset(e->fault, 0, sizeof(int)), "fault word");
-      throw Error(EXOGCM_EDEVICE, "a tensor-core transform gave up waiting for its MMAs; this step's results are invalid");
-    }
-    check(cudaEventElapsedTime(&e->last_ms, e->ev0, e->ev1), "event time");
+    check(cudaMemcpyAsync(B.fault_host, e->fault, sizeof(int), cudaMemcpyDeviceToHost, e->stream), "fault word");
+    check(cudaMemsetAsync(e->fault, 0, sizeof(int), e->stream), "fault word");
+    // start/end bracket the graph alone (the step time); done marks the
+    // fault word's arrival in host memory, after which the batch retires.
+    check(cudaEventRecord(B.done, e->stream), "event");
+    e->pending.push_back(b);
   });
+}
+
+int exogcm_poll(exogcm_engine* e, int* done) {
+  return guard([&] {
+    if (!e || !done) throw Error(EXOGCM_EINVAL, "null argument");
+    while (!e->pending.empty() && retire_oldest(e, false)) {
+    }
+    *done = e->pending.empty() ? 1 : 0;
+  });
+}
+
+int exogcm_wait(exogcm_engine* e) {
+  return guard([&] {
+    if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    retire_all(e);
+  });
+}
+
+int exogcm_step(exogcm_engine* e, int steps, int publish_every) {
+  const int rc = exogcm_step_async(e, steps, publish_every);
+  if (rc != EXOGCM_OK) return rc;
+  return exogcm_wait(e);
 }
 
 int exogcm_read_snapshot(exogcm_engine* e, int slot, float* values, size_t count, long* step) {
   return guard([&] {
     if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    retire_all(e);
     check_slot(e, slot);
     const long pub = e->slots[slot].published;
     if (step) *step = pub;
@@ -957,6 +1046,7 @@ int exogcm_read_snapshot(exogcm_engine* e, int slot, float* values, size_t count
 int exogcm_snapshots_begin(exogcm_engine* e, float* values, size_t count) {
   return guard([&] {
     if (!e || !values) throw Error(EXOGCM_EINVAL, "null argument");
+    retire_all(e);
     const FieldInfo& fi = field(e, "snapshot");
     const size_t n = fi.plane * fi.count * e->d.S;
     if (count != n) throw Error(EXOGCM_EINVAL, "snapshot buffer size mismatch (planes x slots x points)");
@@ -964,12 +1054,14 @@ int exogcm_snapshots_begin(exogcm_engine* e, float* values, size_t count) {
       check(cudaEventSynchronize(e->snap_copied), "previous snapshot copy");
       e->copy_pending = false;
     }
-    if (!e->copy_stream) {
+    // Each resource is created on its own test, so a call after a failed
+    // set-up (say, the staging allocation) retries what is missing instead of
+    // copying through a null staging buffer.
+    if (!e->copy_stream)
       check(cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking), "copy stream");
-      check(cudaEventCreateWithFlags(&e->snap_staged, cudaEventDisableTiming), "event");
-      check(cudaEventCreateWithFlags(&e->snap_copied, cudaEventDisableTiming), "event");
-      check(cudaMalloc(&e->snap_stage, n * sizeof(float)), "snapshot staging");
-    }
+    if (!e->snap_staged) check(cudaEventCreateWithFlags(&e->snap_staged, cudaEventDisableTiming), "event");
+    if (!e->snap_copied) check(cudaEventCreateWithFlags(&e->snap_copied, cudaEventDisableTiming), "event");
+    if (!e->snap_stage) check(cudaMalloc(&e->snap_stage, n * sizeof(float)), "snapshot staging");
     // The device copy runs on the engine's stream, so the next step's graph
     // (queued after it) may overwrite the field while the host copy drains
     // the staging buffer on the copy stream.
@@ -988,6 +1080,7 @@ int exogcm_snapshots_begin(exogcm_engine* e, float* values, size_t count) {
 int exogcm_snapshots_wait(exogcm_engine* e) {
   return guard([&] {
     if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    retire_all(e);
     if (!e->copy_pending) return;
     check(cudaEventSynchronize(e->snap_copied), "snapshot copy");
     e->copy_pending = false;
@@ -997,6 +1090,7 @@ int exogcm_snapshots_wait(exogcm_engine* e) {
 int exogcm_set_stop(exogcm_engine* e, int slot, long step) {
   return guard([&] {
     if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    retire_all(e);
     check_slot(e, slot);
     e->slots[slot].stop = step;
   });
@@ -1023,6 +1117,7 @@ int exogcm_field_size(exogcm_engine* e, const char* name, size_t* count) {
 int exogcm_read_field(exogcm_engine* e, int slot, const char* name, float* values, size_t count) {
   return guard([&] {
     if (!e || !values) throw Error(EXOGCM_EINVAL, "null argument");
+    retire_all(e);
     check_slot(e, slot);
     const FieldInfo& fi = field(e, name);
     if (count != fi.plane * fi.count) throw Error(EXOGCM_EINVAL, std::string(name) + ": wrong value count");
@@ -1033,6 +1128,7 @@ int exogcm_read_field(exogcm_engine* e, int slot, const char* name, float* value
 int exogcm_write_field(exogcm_engine* e, int slot, const char* name, const float* values, size_t count) {
   return guard([&] {
     if (!e || !values) throw Error(EXOGCM_EINVAL, "null argument");
+    retire_all(e);
     check_slot(e, slot);
     const FieldInfo& fi = field(e, name);
     if (count != fi.plane * fi.count) throw Error(EXOGCM_EINVAL, std::string(name) + ": wrong value count");
@@ -1043,6 +1139,7 @@ int exogcm_write_field(exogcm_engine* e, int slot, const char* name, const float
 int exogcm_read_table(exogcm_engine* e, int slot, const char* name, float* values, size_t count) {
   return guard([&] {
     if (!e || !values || !name) throw Error(EXOGCM_EINVAL, "null argument");
+    retire_all(e);
     check_slot(e, slot);
     int off = 0;
     for (auto& t : e->tab_list) {
@@ -1062,6 +1159,7 @@ int exogcm_read_table(exogcm_engine* e, int slot, const char* name, float* value
 int exogcm_checkpoint_save(exogcm_engine* e, int slot, void** buffer, size_t* size) {
   return guard([&] {
     if (!e || !buffer || !size) throw Error(EXOGCM_EINVAL, "null argument");
+    retire_all(e);
     check_slot(e, slot);
     const Slot& s = e->slots[slot];
     if (!s.active) throw Error(EXOGCM_ESTATE, "slot is not running");
@@ -1096,6 +1194,7 @@ int exogcm_checkpoint_save(exogcm_engine* e, int slot, void** buffer, size_t* si
 int exogcm_checkpoint_load(exogcm_engine* e, int slot, const void* buffer, size_t size) {
   return guard([&] {
     if (!e || !buffer) throw Error(EXOGCM_EINVAL, "null argument");
+    retire_all(e);
     check_slot(e, slot);
     Slot& s = e->slots[slot];
     if (!s.active) throw Error(EXOGCM_ESTATE, "configure the slot before loading a checkpoint");
@@ -1138,6 +1237,7 @@ void exogcm_free(void* buffer) { std::free(buffer); }
 int exogcm_unstable(exogcm_engine* e, int* flags, int n) {
   return guard([&] {
     if (!e || !flags || n != e->d.S) throw Error(EXOGCM_EINVAL, "flags must hold one int per slot");
+    retire_all(e);
     check(cudaMemcpy(flags, e->flags, n * sizeof(int), cudaMemcpyDeviceToHost), "flags");
   });
 }
@@ -1145,6 +1245,7 @@ int exogcm_unstable(exogcm_engine* e, int* flags, int n) {
 int exogcm_run_stage(exogcm_engine* e, const char* stage) {
   return guard([&] {
     if (!e || !stage) throw Error(EXOGCM_EINVAL, "null argument");
+    retire_all(e);
     if (!e->shared_ready) throw Error(EXOGCM_ESTATE, "no slot configured");
     const int S = e->d.S;
     for (int s = 0; s < S; ++s) {
@@ -1175,6 +1276,7 @@ int exogcm_last_step_ms(exogcm_engine* e, float* ms) {
 int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms, double* bytes) {
   return guard([&] {
     if (!e || !kernel || !ms || reps < 1) throw Error(EXOGCM_EINVAL, "bad argument");
+    retire_all(e);
     if (!e->shared_ready) throw Error(EXOGCM_ESTATE, "no slot configured");
     const Dims& d = e->d;
     const int S = d.S;

@@ -8,7 +8,14 @@
 // fixer and getiflx reductions compute (the kernel behind exogcm_step's
 // fixsum and ice_sums fields) with no allocation: the caller passes the
 // inputs and the output, and the kernels' scratch lives in one file-scope
-// device array.
+// device array. Unlike the step's reductions, which skip inactive slots (and,
+// for getiflx, slots without sea-ice coupling) and leave their outputs as
+// they were, this entry point sums every one of `slots` slots it is given.
+//
+// With CUDA's lazy module loading the array is committed to the device when
+// the first call on that device looks up its address, not when the library
+// loads: a caller whose footprint must be fixed after start-up makes one
+// call during its own start-up.
 //
 // The scratch is kNoAllocMaxSlots x 256 x 2 doubles (1 MiB). Every GPU that
 // loads this library holds it until the process exits. Every call shares it
@@ -18,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 #include "../../include/exogcm.h"
@@ -71,11 +79,15 @@ __global__ void __launch_bounds__(kSumThreads) k_combine(const double* __restric
   }
 }
 
-// Device address of the scratch array, looked up once per device. In host
-// code g_sum_partials is only a host-side stand-in for the symbol; a kernel
-// must be given the address cudaGetSymbolAddress returns for the current
-// device.
+// Device address of the scratch array, looked up once per device under a
+// per-device once-flag (host threads may call concurrently). In host code
+// g_sum_partials is only a host-side stand-in for the symbol; a kernel must
+// be given the address cudaGetSymbolAddress returns for the current device.
+// The address belongs to the device's primary context: after a
+// cudaDeviceReset the process must reload the library before calling again.
+std::once_flag g_scratch_once[kMaxDevices];
 double* g_scratch_address[kMaxDevices] = {nullptr};
+cudaError_t g_scratch_error[kMaxDevices] = {};
 
 }  // namespace
 
@@ -97,18 +109,20 @@ extern "C" int exogcm_slot_sums_noalloc(const float* first, const float* second,
     exogcm::set_error(std::string("exogcm_slot_sums_noalloc: no usable device: ") + cudaGetErrorString(err));
     return EXOGCM_EDEVICE;
   }
-  if (!g_scratch_address[device]) {
+  std::call_once(g_scratch_once[device], [device] {
     void* ptr = nullptr;
-    err = cudaGetSymbolAddress(&ptr, g_sum_partials);
-    if (err != cudaSuccess || !ptr) {
-      exogcm::set_error(std::string("exogcm_slot_sums_noalloc: scratch address: ") + cudaGetErrorString(err));
-      return EXOGCM_EDEVICE;
-    }
-    g_scratch_address[device] = static_cast<double*>(ptr);
+    g_scratch_error[device] = cudaGetSymbolAddress(&ptr, g_sum_partials);
+    if (g_scratch_error[device] == cudaSuccess) g_scratch_address[device] = static_cast<double*>(ptr);
+  });
+  double* scratch = g_scratch_address[device];
+  if (!scratch) {
+    exogcm::set_error(std::string("exogcm_slot_sums_noalloc: scratch address: ") +
+                      cudaGetErrorString(g_scratch_error[device]));
+    return EXOGCM_EDEVICE;
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  k_partials<<<slots, kSumThreads, 0, st>>>(first, second, points, g_scratch_address[device]);
-  k_combine<<<slots, kSumThreads, 0, st>>>(g_scratch_address[device], slots, sums);
+  k_partials<<<slots, kSumThreads, 0, st>>>(first, second, points, scratch);
+  k_combine<<<slots, kSumThreads, 0, st>>>(scratch, slots, sums);
   err = cudaGetLastError();
   if (err != cudaSuccess) {
     exogcm::set_error(std::string("exogcm_slot_sums_noalloc: launch: ") + cudaGetErrorString(err));
