@@ -2719,6 +2719,15 @@ int ora_run(void* p, const char* stage) {
     else if (s == "physics_out") physics_out_stage(m);
     else if (s == "spectrald") spectrald_stage(m);
     else if (s == "pack") pack(m);
+    // Single transforms on fixed fields, as the engine's kernel timer
+    // launches them (the reference's verify-kernels.mjs recipe).
+    else if (s == "tr_legendre_inverse") legendre_inverse(m, "st", "fgt", "legendre_qi", m.L);
+    else if (s == "tr_fourier_inverse") fourier_inverse(m, "fgu", "gu", m.L);
+    else if (s == "tr_fourier_forward") fourier_forward(m, "gtn", "fgtn", m.L);
+    else if (s == "tr_legendre_forward") legendre_forward(m, "fgtdt", "zstt1", "legendre_qc", m.L);
+    else if (s == "tr_dv2uv") legendre_dv2uv(m, "sd", "sz", "fgu", "fgv", m.L, (real)1.63299310207);
+    else if (s == "tr_uv2dv") legendre_uv2dv(m, "fgvz", "fguz", "fgke", "zdsdp1", "zdszp1", m.L);
+    else if (s == "tr_qtend") legendre_qtend(m, "fgut", "fgvt", "fgtn", "zstt2", m.L);
     else {
       g_error = "unknown stage " + s;
       return -1;

@@ -103,3 +103,17 @@ def v3_gate(gpu, exact, f32, points=None):
             r["outlier"] = out
             r["ok"] = within_gate(out["gpu"], out["f32"], out["gpu_off"], out["f32_off"])
     return r
+
+
+def carbon_counter(model, main_steps):
+    """The host's carbon-cycle counter (carbonmod's cstep) after the start-up
+    steps and `main_steps` main-loop steps of a run, as the engine and
+    Oracle.advance carry it (physics/carbon/index.ts:23-28)."""
+    from oracle import setup_f64
+    c = 0
+    start = model["start_step"]
+    for _ in range(model["nkits"]):
+        _, c = setup_f64.step_values(start, c, model["calendar"])
+    for k in range(main_steps):
+        _, c = setup_f64.step_values(start + k, c, model["calendar"])
+    return c

@@ -9,8 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from tests.helpers import pkg, planets, rel_rms
-from tests.test_gpu_parity import STAGES, TRANSFORM_TOL, PHYSICS_TOL, PHYSICS_FIELDS, FLIPPED_COLUMNS
+from tests.helpers import pkg, planets
 
 FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "earth_t21_climatology.npz")
 
@@ -56,25 +55,33 @@ def test_earth_climatology_setup_matches_oracle():
 @pytest.mark.gpu
 @pytest.mark.parametrize("mode", [0, 1])
 def test_earth_climatology_stage_replay(mode):
-    from tests.test_gpu_parity import _replay_errors
-    worst = _replay_errors(earth_planet(), 21, 10, 6, mode)
-    for name, (err, stage) in worst.items():
-        tol = PHYSICS_TOL if name in PHYSICS_FIELDS else TRANSFORM_TOL
-        assert err <= tol, f"{name} after {stage}: relative RMS {err:.3e} > {tol:g}"
+    """Every stage on the Earth SST and sea-ice climatology passes the
+    reference's V3 gate (see tests/test_gpu_parity.py)."""
+    from tests.test_gpu_parity import replay_v3
+    verdicts = replay_v3(earth_planet(), 21, 10, 6, mode)
+    failed = [(k, v) for k, v in verdicts.items() if not v["ok"]]
+    assert not failed, failed[:5]
 
 
 @pytest.mark.gpu
 def test_earth_climatology_one_day():
+    """One day on the Earth climatology (start-up included) by the reference's
+    V4 gate against the FP64 and sequential-f32 oracles."""
+    from tests.test_gpu_parity import v4_judge
     p = earth_planet(seed=6)
+    m = oracle.model_for(p)
+    m["state"] = {k: np.asarray(v, dtype=np.float64).astype(np.float32).astype(np.float64)
+                  for k, v in m["state"].items()}
     e = pkg.Engine(21, 10, 1, mode=1)
     e.configure(0, p)
-    o = oracle.Oracle(oracle.model_for(p))
+    for name, v in m["state"].items():
+        e.write(0, name, v.astype(np.float32))
+    o64, o32 = oracle.Oracle(m), oracle.Oracle(m, precision=32)
     e.step(3)
-    o.startup()
-    for _ in range(4):
-        e.step(8)
-        o.advance(8)
-    errs = {n: rel_rms(e.read(0, n), o.get(n)) for n in ("st", "sz", "sd", "sq", "sp", "dt", "xicec", "xsst")}
-    print("Earth climatology, 1 day vs FP64:", errs)
-    assert errs["st"] < 5e-3 and errs["sz"] < 1e-3 and errs["sq"] < 5e-2 and errs["sp"] < 5e-2
-    assert errs["dt"] < 1e-3 and errs["xsst"] < 1e-3
+    e.step(32)
+    for o in (o64, o32):
+        o.advance(32)
+    verdict = v4_judge(e, o64, o32, fields=("st", "sz", "sd", "sq", "sp", "dt", "xicec", "xsst", "xiced"))
+    print("Earth climatology, 1 day (GPU, f32) vs FP64:", verdict)
+    bad = {k: v for k, v in verdict.items() if not v[2]}
+    assert not bad, bad

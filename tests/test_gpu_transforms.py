@@ -1,0 +1,99 @@
+"""Each transform on random inputs against the FP64 oracle: the reference's
+kernel recipe (scripts/exoplasim-webgpu/verify-kernels.mjs:105-135 and
+:265-275). Ten random planes (one engine slot, ten levels) drawn from the
+recipe's linear congruential generator seeded with the truncation, the
+page-default exponential filter; each kernel runs once on its own f32 input
+through the C ABI's kernel timer. A kernel passes when its relative RMS error
+against FP64 is within 1e-5, within twice the sequential-f32 oracle's, and
+within twice the error the reference documents for its own FP32 kernels
+(docs/climate/exoplasim-webgpu.md:174-179, 199-204; T21 and T42 only)."""
+import numpy as np
+import pytest
+
+import oracle
+from tests.helpers import pkg, planets, rel_rms
+
+# kernel-timer name -> (oracle stage, inputs, outputs, documented relative RMS per output at T21, T42)
+KERNELS = {
+    "legendre_inverse": ("tr_legendre_inverse", ("st",), ("fgt",), {21: (9.9e-8,), 42: (1.33e-7,)}),  # sp2fc
+    "fourier_inverse": ("tr_fourier_inverse", ("fgu",), ("gu",), {21: (1.38e-7,), 42: (1.81e-7,)}),  # fc2gp
+    "fourier_forward": ("tr_fourier_forward", ("gtn",), ("fgtn",), {21: (1.42e-7,), 42: (2.03e-7,)}),  # gp2fc
+    "legendre_forward": ("tr_legendre_forward", ("fgtdt",), ("zstt1",), {21: (6.9e-8,), 42: (9.2e-8,)}),  # fc2sp
+    "dv2uv": ("tr_dv2uv", ("sd", "sz"), ("fgu", "fgv"), {21: (1.45e-7, 1.49e-7), 42: (2.03e-7, 2.12e-7)}),
+    # mktend's divergence and vorticity (uv2dv with the kinetic-energy term)
+    "uv2dv": ("tr_uv2dv", ("fgvz", "fguz", "fgke"), ("zdsdp1", "zdszp1"), {21: (1.70e-7, 1.09e-7),
+                                                                          42: (2.07e-7, 1.52e-7)}),
+    "qtend": ("tr_qtend", ("fgut", "fgvt", "fgtn"), ("zstt2",), {21: (1.26e-7,), 42: (1.76e-7,)}),
+}
+SPECTRAL = {"st", "sd", "sz"}
+FOURIER = {"fgu", "fgvz", "fguz", "fgke", "fgut", "fgvt", "fgtn", "fgtdt"}
+
+
+class Lcg:
+    """verify-kernels.mjs:105-109: seed = (seed * 1103515245 + 12345) mod 2^31."""
+
+    def __init__(self, seed):
+        self.seed = seed
+
+    def __call__(self):
+        self.seed = (self.seed * 1103515245 + 12345) % 2147483648
+        return self.seed / 2147483648 - 0.5
+
+
+def random_inputs(truncation, names, planes=10):
+    """Spectral planes with Im of the m = 0 modes zero, Fourier rows with
+    Im c_0 zero (verify-kernels.mjs:110-122), grid planes uniform."""
+    rnd = Lcg(truncation)
+    nlat = {21: 32, 42: 64, 63: 96}[truncation]
+    ncsp = (truncation + 1) * (truncation + 2) // 2
+    nfc = 2 * (truncation + 1)
+    out = {}
+    for name in names:
+        if name in SPECTRAL:
+            v = np.zeros((planes, ncsp, 2))
+            for p in range(planes):
+                for w in range(ncsp):
+                    v[p, w, 0] = rnd()
+                    v[p, w, 1] = 0.0 if w <= truncation else rnd()
+        elif name in FOURIER:
+            v = np.zeros((planes * nlat, nfc))
+            for r in range(planes * nlat):
+                for k in range(nfc):
+                    v[r, k] = 0.0 if k == 1 else rnd()
+        else:
+            v = np.array([rnd() for _ in range(planes * nlat * 2 * nlat)])
+        out[name] = v.reshape(-1).astype(np.float32)
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("truncation", [21, 42, 63])
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_transforms_on_random_planes(truncation, mode):
+    p = planets.make_planet(3, truncation=truncation, levels=10)
+    e = pkg.Engine(truncation, 10, 1, mode=mode)
+    e.configure(0, p)
+    m = oracle.model_for(p)
+    o64, o32 = oracle.Oracle(m), oracle.Oracle(m, precision=32)
+    report = {}
+    for kernel, (stage, inputs, outputs, documented) in KERNELS.items():
+        values = random_inputs(truncation, inputs)
+        for name, v in values.items():
+            e.write(0, name, v)
+            o64.set(name, v.astype(np.float64))
+            o32.set(name, v.astype(np.float64))
+        e.time_kernel(kernel, 1)
+        o64.run(stage)
+        o32.run(stage)
+        for i, out in enumerate(outputs):
+            ref = o64.get(out)
+            gpu = rel_rms(e.read(0, out), ref)
+            f32 = rel_rms(o32.get(out), ref)
+            doc = documented.get(truncation, (None,) * len(outputs))[i]
+            report[f"{kernel} {out}"] = (gpu, f32, doc)
+            assert gpu <= 1e-5, (kernel, out, gpu)
+            assert gpu <= 2 * f32, (kernel, out, gpu, f32)
+            if doc is not None:
+                assert gpu <= 2 * doc, (kernel, out, gpu, doc)
+    print(f"T{truncation} mode {mode} relative RMS (GPU, sequential f32, reference's FP32 kernel):",
+          {k: tuple(None if x is None else float(f"{x:.3g}") for x in v) for k, v in report.items()})

@@ -140,3 +140,27 @@ def test_oracle_deterministic(planets):
     b.advance(4)
     for name in ("st", "sz", "sd", "sq", "sp", "dt", "dq"):
         assert np.array_equal(a.get(name), b.get(name))
+
+
+@pytest.mark.parametrize("truncation", [21, 42])
+def test_f32_oracle_reproduces_the_reference_fp32_kernel_errors(truncation):
+    """Pins both oracle builds to numbers the reference publishes: on the
+    reference's random-plane recipe (verify-kernels.mjs:105-135), the
+    sequential-f32 oracle's relative RMS error against the FP64 oracle
+    matches the error the reference documents for its FP32 kernels against
+    the Fortran in f64 (docs/climate/exoplasim-webgpu.md:174-179, 199-204),
+    whose ratio to sequential f32 is 0.92-1.05, to within 30 %."""
+    from tests.helpers import planets, rel_rms
+    from tests.test_gpu_transforms import KERNELS, random_inputs
+    p = planets.make_planet(3, truncation=truncation, levels=10)
+    m = oracle.model_for(p)
+    o64, o32 = oracle.Oracle(m), oracle.Oracle(m, precision=32)
+    for kernel, (stage, inputs, outputs, documented) in KERNELS.items():
+        for name, v in random_inputs(truncation, inputs).items():
+            o64.set(name, v.astype(np.float64))
+            o32.set(name, v.astype(np.float64))
+        o64.run(stage)
+        o32.run(stage)
+        for out, doc in zip(outputs, documented[truncation]):
+            err = rel_rms(o32.get(out), o64.get(out))
+            assert 0.7 * doc <= err <= 1.3 * doc, (kernel, out, err, doc)

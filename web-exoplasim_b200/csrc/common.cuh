@@ -110,10 +110,11 @@ struct SharedTabs {
   const float* qjT;
   const float* quT;
   const float* qvT;
-  // Tensor-core inverse operands: per m, the hi and lo images of the full
-  // qi / qj tables in the MMA's shared-memory layout, at float offset tc_at[m].
-  const float* tc_qi;
-  const float* tc_qj;
+  // Tensor-core (mode 2) table operands: per image set (qi, qj, dv2uv,
+  // fc2sp, uv2dv, mktend, qtend) and m, the hi and lo TF32 images of the
+  // tables in the MMA's shared-memory layout, at float offset
+  // tc_at[set * (NTP1 + 1) + m] of tc_img.
+  const float* tc_img;
   const int* tc_at;
 };
 
@@ -141,7 +142,8 @@ struct Model {
   int* flags;                // per-slot status flags [S]
   int* fault;                // nonzero after a kernel gave up a bounded wait
   int mode;                  // 0 plain path, 1 optimized path (FFTs, latitude-pair Legendre, m-major Fourier),
-                             // 2 optimized path with sp2fc / sp2fcdmu on the tensor cores
+                             // 2 optimized path with every Legendre transform on the tensor cores
+                             // (split precision)
   Tuning tune;               // optimized path launch shapes
   int keep_fourier;          // optimized path: fused transforms also write the Fourier fields they pass through
   // physics_in zeroes the grid tendencies gudt, gvdt, gtdt, gqdt and the

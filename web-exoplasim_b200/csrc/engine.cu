@@ -312,17 +312,17 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
       for (int w = 0; w < d.NCSP; ++w) t[(size_t)w * JH + j] = q[(size_t)j * d.NCSP + w];
     qt[i] = put(t);
   }
-  // Tensor-core inverse: hi/lo images of the full qi and qj tables per m.
+  // Tensor-core transforms (mode 2): hi/lo images of every table operand per m.
   std::vector<int> tc_at;
-  const std::vector<float> img_qi = tc_table_images(d, s.q.at("qi"), tc_at);
-  const std::vector<float> img_qj = tc_table_images(d, s.q.at("qj"), tc_at);
+  const std::vector<float> img = e->mode == 2 ? tc_table_images(d, s.q, tc_at) : std::vector<float>();
+  if (tc_at.empty()) tc_at.assign(1, 0);
   auto put_floats = [&](const std::vector<float>& v) {
     while (buf.size() % 32) buf.push_back(0.f);
     const size_t at = buf.size();
     buf.insert(buf.end(), v.begin(), v.end());
     return at;
   };
-  const size_t itc_qi = put_floats(img_qi), itc_qj = put_floats(img_qj);
+  const size_t itc = put_floats(img);
   check(cudaMalloc(&e->shared_buf, buf.size() * sizeof(float)), "shared tables");
   check(cudaMemcpy(e->shared_buf, buf.data(), buf.size() * sizeof(float), cudaMemcpyHostToDevice), "shared tables");
   check(cudaMalloc(&e->mode_buf, (2 * d.NCSP + tc_at.size()) * sizeof(int)), "mode tables");
@@ -351,8 +351,7 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
   e->sh.qjT = b + qt[1];
   e->sh.quT = b + qt[2];
   e->sh.qvT = b + qt[3];
-  e->sh.tc_qi = b + itc_qi;
-  e->sh.tc_qj = b + itc_qj;
+  e->sh.tc_img = b + itc;
   e->sh.tc_at = e->mode_buf + 2 * d.NCSP;
   e->sh.mode_m = e->mode_buf;
   e->sh.mode_n = e->mode_buf + d.NCSP;
@@ -1248,9 +1247,11 @@ int exogcm_run_stage(exogcm_engine* e, const char* stage) {
     retire_all(e);
     if (!e->shared_ready) throw Error(EXOGCM_ESTATE, "no slot configured");
     const int S = e->d.S;
+    // A replayed step publishes (main loop), so the pack stage writes the
+    // snapshot the replay compares.
     for (int s = 0; s < S; ++s) {
       Slot copy = e->slots[s];
-      e->hparams[s] = next_params(copy, 1 << 30, false);
+      e->hparams[s] = next_params(copy, 1, false);
     }
     check(cudaMemcpyAsync(e->params, e->hparams, S * sizeof(StepParams), cudaMemcpyHostToDevice, e->stream),
           "params");

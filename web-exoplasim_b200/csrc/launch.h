@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -43,10 +44,18 @@ void leg_uv2dv(const Model& m, const float* u, const float* v, const float* ke, 
 void leg_qtend(const Model& m, const float* u, const float* v, const float* src, float* out, int planes,
                cudaStream_t st);
 
-// legendre_tc.cu (optimized path, tensor cores)
+// legendre_tc.cu (mode 2: the Legendre transforms on the tensor cores, split precision)
 void tc_init();
-std::vector<float> tc_table_images(const Dims& d, const std::vector<double>& q, std::vector<int>& at);
+std::vector<float> tc_table_images(const Dims& d, const std::map<std::string, std::vector<double>>& q,
+                                   std::vector<int>& at);
 void tc_inverse(const Model& m, const float* s, float* f, int planes, bool derivative, cudaStream_t st);
+void tc_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V, int planes, float plavor,
+              cudaStream_t st);
+void tc_forward(const Model& m, const float* f, float* s, int planes, cudaStream_t st);
+void tc_uv2dv(const Model& m, const float* u, const float* v, const float* ke, float* D, float* Z, int planes,
+              cudaStream_t st);
+void tc_qtend(const Model& m, const float* u, const float* v, const float* src, float* out, int planes,
+              cudaStream_t st);
 
 // fft.cu (optimized path; Fourier planes m-major)
 void fft_init();

@@ -77,6 +77,11 @@ __device__ __forceinline__ void stage_planet(const PlanetConst* src, PlanetConst
 __device__ __forceinline__ float sat_capped(const PlanetConst& K, float t, float p) {
   return fminf(K.RDBRV * K.RA1 * expf(K.RA2 * (t - K.TMELT) / (t - K.RA4)) / p, K.RDBRV);
 }
+// The same with IEEE divisions, for the large-scale condensation, whose
+// precipitation is the small difference of two iterated states.
+__device__ __forceinline__ float sat_capped_rn(const PlanetConst& K, float t, float p) {
+  return fminf(__fdiv_rn(K.RDBRV * K.RA1 * expf(__fdiv_rn(K.RA2 * (t - K.TMELT), t - K.RA4)), p), K.RDBRV);
+}
 __device__ __forceinline__ float sat_divided(const PlanetConst& K, float t, float p) {
   const float q = sat_capped(K, t, p);
   return q / (1.f - K.MOIST * q);
@@ -1338,23 +1343,27 @@ __global__ void __launch_bounds__(kBlock) k_rain_column(Model m, const PlanetCon
     const float dq = dq_[l];
     const float zq = dq + dqdt_[l] * D2;
     const float zt = dt_[l] + dtdt_[l] * D2;
-    const float zlcpe = K.ALV / (K.ACPD * (1.f + K.ADV * dq));
+    // IEEE divisions here (the file otherwise divides to 2 ulp): the
+    // large-scale precipitation is the difference of two iterated states.
+    const float zlcpe = __fdiv_rn(K.ALV, K.ACPD * (1.f + K.ADV * dq));
     const float p = dp * sg[l];
-    float zqsat = sat_capped(K, zt, p);
-    float zcor = 1.f / (1.f - K.MOIST * zqsat);
+    float zqsat = sat_capped_rn(K, zt, p);
+    float zcor = __fdiv_rn(1.f, 1.f - K.MOIST * zqsat);
     zqsat = zqsat * zcor;
     if (zqsat < 0.f) zqsat = 0.f;
     if (zq > zqsat) {
-      float zdqdt = (zqsat - zq) / (1.f + zlcpe * K.RA2 * (K.TMELT - K.RA4) * zqsat * zcor / ((zt - K.RA4) * (zt - K.RA4)));
+      float zdqdt = __fdiv_rn(zqsat - zq, 1.f + __fdiv_rn(zlcpe * K.RA2 * (K.TMELT - K.RA4) * zqsat * zcor,
+                                                          (zt - K.RA4) * (zt - K.RA4)));
       float ztn = zt - zdqdt * zlcpe;
       float zqn = zq + zdqdt;
-      zqsat = sat_capped(K, ztn, p);
-      zcor = 1.f / (1.f - K.MOIST * zqsat);
+      zqsat = sat_capped_rn(K, ztn, p);
+      zcor = __fdiv_rn(1.f, 1.f - K.MOIST * zqsat);
       zqsat = zqsat * zcor;
-      zdqdt = (zqsat - zqn) / (1.f + zlcpe * K.RA2 * (K.TMELT - K.RA4) * zqsat * zcor / ((ztn - K.RA4) * (ztn - K.RA4)));
+      zdqdt = __fdiv_rn(zqsat - zqn, 1.f + __fdiv_rn(zlcpe * K.RA2 * (K.TMELT - K.RA4) * zqsat * zcor,
+                                                     (ztn - K.RA4) * (ztn - K.RA4)));
       ztn = ztn - zdqdt * zlcpe;
       zqn = zqn + zdqdt;
-      const float dqdt = (zqn - zq) / D2, dtdt = (ztn - zt) / D2;
+      const float dqdt = __fdiv_rn(zqn - zq, D2), dtdt = __fdiv_rn(ztn - zt, D2);
       dqdt_[l] = dqdt_[l] + dqdt;
       dtdt_[l] = dtdt_[l] + dtdt;
       dprll[l] = -fminf(dqdt, 0.f) * ds[l];

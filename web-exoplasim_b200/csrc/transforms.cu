@@ -384,6 +384,7 @@ void tr_legendre_inverse(const Model& m, const float* s, float* f, int planes, c
 
 void tr_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V, int planes, float plavor,
               cudaStream_t st) {
+  if (m.mode == 2) return tc_dv2uv(m, D, Z, U, V, planes, plavor, st);
   if (m.mode >= 1) return leg_dv2uv(m, D, Z, U, V, planes, plavor, st);
   const InvTile t = inverse_tile(m.d, 2, 2);
   dim3 grid((planes + kInvPlanes - 1) / kInvPlanes, m.d.NLAT / t.lats);
@@ -392,6 +393,7 @@ void tr_dv2uv(const Model& m, const float* D, const float* Z, float* U, float* V
 
 void tr_legendre_forward(const Model& m, const float* f, float* s, int planes, const float* q,
                          cudaStream_t st) {
+  if (m.mode == 2 && q == m.sh.qc) return tc_forward(m, f, s, planes, st);
   if (m.mode >= 1) return leg_forward(m, f, s, planes, q, st);
   FwdIn<1> in{{f}};
   launch_forward<0, 1>(m, in, s, nullptr, planes, q, st);
@@ -399,6 +401,7 @@ void tr_legendre_forward(const Model& m, const float* f, float* s, int planes, c
 
 void tr_uv2dv(const Model& m, const float* u, const float* v, const float* ke, float* D, float* Z, int planes,
               cudaStream_t st) {
+  if (m.mode == 2) return tc_uv2dv(m, u, v, ke, D, Z, planes, st);
   if (m.mode >= 1) return leg_uv2dv(m, u, v, ke, D, Z, planes, st);
   if (ke) {
     FwdIn<3> in{{u, v, ke}};
@@ -411,6 +414,7 @@ void tr_uv2dv(const Model& m, const float* u, const float* v, const float* ke, f
 
 void tr_qtend(const Model& m, const float* u, const float* v, const float* src, float* out, int planes,
               cudaStream_t st) {
+  if (m.mode == 2) return tc_qtend(m, u, v, src, out, planes, st);
   if (m.mode >= 1) return leg_qtend(m, u, v, src, out, planes, st);
   FwdIn<3> in{{u, v, src}};
   launch_forward<3, 3>(m, in, out, nullptr, planes, nullptr, st);

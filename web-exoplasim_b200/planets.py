@@ -89,7 +89,10 @@ def saturation(t, p, gascon):
 
 
 def make_planet(seed: int, truncation: int = 21, levels: int = 10, land_fraction: float = 0.3,
-                **overrides) -> Planet:
+                noise_seed: int | None = None, **overrides) -> Planet:
+    """The planet of `seed`. With `noise_seed` the initial temperature noise
+    comes from that seed instead, so one terrain carries an ensemble of
+    initial states (the climatology gate's control runs)."""
     cfg = dict(BASE_CONFIG)
     cfg.update(truncation=truncation, layers=levels)
     cfg.update(overrides)
@@ -109,6 +112,8 @@ def make_planet(seed: int, truncation: int = 21, levels: int = 10, land_fraction
     nhor = nlat * nlon
     boundary = {172: mask, 129: oro, 169: np.full(nhor, 288.0), 210: np.zeros(nhor)}
     sigma = sigma_levels(levels)
+    if noise_seed is not None:
+        rng = np.random.default_rng([seed, noise_seed])
     t = 250.0 + 0.1 * rng.standard_normal((levels, nhor))
     p = sigma[:, None] * cfg["pressureBar"] * 1e5
     q = 0.8 * saturation(t, p, cfg["gasConstant"])

@@ -1,14 +1,21 @@
 """Serving: continuous batching of many planet runs on one GPU.
 
 Requests (a seeded planet, a resolution and a duration in simulated days)
-arrive over time. Each resolution (T, L) has one batched engine whose slot
-count is sized from an HBM budget by the per-slot state footprint. A request
-waits until a slot of its resolution is free, is admitted at the next batch
-boundary (configured into the slot while the other slots keep their state on
-the device), steps with everyone else in the same launches, and leaves when
-its last step is done: the engine stops a slot exactly at its final step
-(exogcm_set_stop), so a result does not depend on what else was running.
-Engines of different resolutions step concurrently on their own streams.
+arrive over time. Runs of one resolution (T, L) share batched engines
+("blocks" of slots). A request is admitted into a free slot of its
+resolution, or, when none is free, into a new block if the HBM budget has
+room for it: every resolution draws on one byte budget by its per-slot state
+footprint, blocks are created as requests need them and destroyed when they
+empty while another resolution waits for room. An admitted run is configured
+into its slot while the other slots keep their state on the device, steps
+with everyone else in the same launches, and leaves when its last step is
+done: the engine stops a slot exactly at its final step (exogcm_set_stop), so
+a result does not depend on what else was running.
+
+Every block with running slots is submitted with exogcm_step_async, so the
+blocks' batches run concurrently on their own streams while the host admits
+new arrivals (their host set-up overlaps the device work); the loop then
+waits for the batches and collects finished runs.
 
 Reported: time-to-result p50/p99, admission queue depth, and aggregate
 simulated days per second over the window.
@@ -71,15 +78,16 @@ def _field_names():
 
 
 class Group:
-    """One (T, L) engine and its slots."""
+    """One batched engine (a block of slots of one resolution)."""
 
-    def __init__(self, truncation, levels, slots, chunk):
+    def __init__(self, truncation, levels, slots, chunk, mode=1):
         self.truncation, self.levels, self.slots, self.chunk = truncation, levels, slots, chunk
-        self.engine = pkg.Engine(truncation, levels, slots, mode=1)
+        self.engine = pkg.Engine(truncation, levels, slots, mode=mode)
         self.free = deque(range(slots))
         self.running: dict[int, Request] = {}
         self.stop_step: dict[int, int] = {}
         self.sim_days = 0.0
+        self.in_flight = False
 
     def admit(self, req: Request, now: float):
         slot = self.free.popleft()
@@ -97,9 +105,19 @@ class Group:
         req.status = "running"
         self.running[slot] = req
 
-    def step(self):
+    def submit(self):
         if self.running:
-            self.engine.step(self.chunk, publish_every=1 << 30)
+            self.engine.step_async(self.chunk, publish_every=1 << 30)
+            self.in_flight = True
+
+    def wait(self):
+        if self.in_flight:
+            self.engine.wait()
+            self.in_flight = False
+
+    def step(self):
+        self.submit()
+        self.wait()
 
     def collect(self, now: float, done: list):
         unstable = self.engine.unstable() if self.running else None
@@ -117,37 +135,92 @@ class Group:
                 self.free.append(slot)
                 done.append(req)
 
+    def close(self):
+        self.wait()
+        self.engine.close()
+
 
 class Server:
-    """Continuous-batching loop over per-resolution engines."""
+    """Continuous-batching loop over blocks of batched engines.
 
-    def __init__(self, capacity: dict, chunk: int = 16, keep_results: bool = True):
-        self.groups = {key: Group(key[0], key[1], n, chunk) for key, n in capacity.items() if n > 0}
+    Server(capacity): one fixed block per (T, L) with the given slot counts.
+    Server(budget_bytes=B, block=n): blocks of n slots (fewer at the larger
+    resolutions, see `block_slots`) created and destroyed on demand within an
+    HBM budget of B bytes shared by every resolution."""
+
+    def __init__(self, capacity: dict | None = None, chunk: int = 16, keep_results: bool = True,
+                 budget_bytes: float | None = None, block: int = 32, mode: int = 1):
+        self.chunk, self.mode, self.block = chunk, mode, block
+        self.blocks: list[Group] = [Group(key[0], key[1], n, chunk, mode) for key, n in (capacity or {}).items()
+                                    if n > 0]
+        self.elastic = budget_bytes is not None
+        self.budget = float(budget_bytes or 0.0)
         self.queue: deque[Request] = deque()
         self.done: list[Request] = []
         self.queue_depth: list[int] = []
         self.keep_results = keep_results
+        self.peak_bytes = 0
+        self.blocks_created = 0
+        self.blocks_destroyed = 0
+
+    # kept for callers that address one block per resolution
+    @property
+    def groups(self) -> dict:
+        return {(b.truncation, b.levels): b for b in self.blocks}
 
     @staticmethod
     def capacity_for(budget_bytes: float, mix: dict, max_slots: int = 256) -> dict:
         """Slots per (T, L) from an HBM budget split by the expected mix of
         work (fraction of requests per resolution times its per-slot bytes)."""
-        global FIELD_NAMES
-        if not FIELD_NAMES:
-            FIELD_NAMES = _field_names()
-        sizes = {key: slot_bytes(*key) for key in mix}
+        sizes = {key: slot_bytes_cached(*key) for key in mix}
         weight = sum(mix[k] * sizes[k] for k in mix)
         return {k: int(min(max_slots, max(1, budget_bytes * mix[k] / weight))) for k in mix}
 
+    def block_slots(self, truncation: int, levels: int) -> int:
+        """Slots of a new block: `block` at T21, scaled down by the footprint
+        so a block's bytes stay about the same at every resolution."""
+        ratio = slot_bytes_cached(21, 5) / slot_bytes_cached(truncation, levels)
+        return max(1, int(round(self.block * min(1.0, 4 * ratio))))
+
+    def used_bytes(self) -> int:
+        return sum(b.slots * slot_bytes_cached(b.truncation, b.levels) for b in self.blocks)
+
     def submit(self, req: Request):
         self.queue.append(req)
+
+    def _free_slot(self, key):
+        for b in self.blocks:
+            if (b.truncation, b.levels) == key and b.free:
+                return b
+        return None
+
+    def _grow(self, key):
+        """A new block for `key` if the budget holds it, destroying empty
+        blocks of other resolutions to make room."""
+        if not self.elastic:
+            return None
+        n = self.block_slots(*key)
+        need = n * slot_bytes_cached(*key)
+        while self.used_bytes() + need > self.budget:
+            empty = [b for b in self.blocks if not b.running and (b.truncation, b.levels) != key]
+            if not empty:
+                return None
+            b = empty[0]
+            b.close()
+            self.blocks.remove(b)
+            self.blocks_destroyed += 1
+        block = Group(key[0], key[1], n, self.chunk, self.mode)
+        self.blocks.append(block)
+        self.blocks_created += 1
+        self.peak_bytes = max(self.peak_bytes, self.used_bytes())
+        return block
 
     def _admit(self, now: float):
         waiting = deque()
         while self.queue:
             req = self.queue.popleft()
-            group = self.groups.get((req.truncation, req.levels))
-            if group is None:
+            key = (req.truncation, req.levels)
+            if not self.elastic and key not in self.groups:
                 req.status = "rejected"
                 req.finished = now
                 self.done.append(req)
@@ -155,8 +228,9 @@ class Server:
             if req.arrival > now:
                 waiting.append(req)
                 continue
-            if group.free:
-                group.admit(req, now)
+            block = self._free_slot(key) or self._grow(key)
+            if block is not None:
+                block.admit(req, now)
             else:
                 waiting.append(req)
         self.queue = waiting
@@ -170,24 +244,25 @@ class Server:
             now = clock() - t0
             while pending and pending[0].arrival <= now:
                 self.queue.append(pending.popleft())
+            active = [b for b in self.blocks if b.running]
+            for b in active:
+                b.submit()
+            # arrivals are admitted while the submitted batches run
             self._admit(now)
             self.queue_depth.append(len(self.queue))
-            active = [g for g in self.groups.values() if g.running]
             if not active:
-                if not pending and not self.queue:
+                if not pending and not self.queue and not any(b.running for b in self.blocks):
                     break
                 if now > window and not drain:
                     break
-                time.sleep(0.001)
+                if not any(b.running for b in self.blocks):
+                    time.sleep(0.001)
                 continue
-            threads = [threading.Thread(target=g.step) for g in active]
-            for t in threads:
-                t.start()
-            for t in threads:
-                t.join()
+            for b in active:
+                b.wait()
             now = clock() - t0
-            for g in active:
-                g.collect(now, self.done)
+            for b in active:
+                b.collect(now, self.done)
             if not self.keep_results:
                 for r in self.done:
                     r.result = None
@@ -201,11 +276,15 @@ class Server:
         latency = np.array([r.finished - r.arrival for r in finished]) if finished else np.array([np.nan])
         days = sum(r.days for r in finished)
         partial = 0.0
-        for g in self.groups.values():
+        for g in self.blocks:
             for slot, req in g.running.items():
                 info = g.engine.slot_info(slot)
                 done_steps = req.steps - max(0, g.stop_step[slot] - info["step"])
                 partial += done_steps * STEP_MINUTES[g.truncation] / 1440.0
+        slots: dict = {}
+        for b in self.blocks:
+            k = f"T{b.truncation}L{b.levels}"
+            slots[k] = slots.get(k, 0) + b.slots
         return {
             "completed": len(finished),
             "failed": sum(r.status == "failed" for r in self.done),
@@ -215,8 +294,29 @@ class Server:
             "queue_depth_max": int(max(self.queue_depth)) if self.queue_depth else 0,
             "sim_days_per_s": (days + partial) / elapsed,
             "window_s": elapsed,
-            "slots": {f"T{k[0]}L{k[1]}": g.slots for k, g in self.groups.items()},
+            "slots": slots,
+            "blocks_created": self.blocks_created,
+            "blocks_destroyed": self.blocks_destroyed,
+            "peak_bytes": self.peak_bytes,
         }
+
+    def close(self):
+        for b in self.blocks:
+            b.close()
+        self.blocks = []
+
+
+_SLOT_BYTES: dict = {}
+
+
+def slot_bytes_cached(truncation: int, levels: int) -> int:
+    global FIELD_NAMES
+    key = (truncation, levels)
+    if key not in _SLOT_BYTES:
+        if not FIELD_NAMES:
+            FIELD_NAMES = _field_names()
+        _SLOT_BYTES[key] = slot_bytes(truncation, levels)
+    return _SLOT_BYTES[key]
 
 
 def poisson_requests(rate: float, window: float, seed: int, max_days: float = 365.0, min_days: float = 1.0,
@@ -255,5 +355,5 @@ if __name__ == "__main__":
         mix[(r.truncation, r.levels)] = mix.get((r.truncation, r.levels), 0) + r.days
     total = sum(mix.values())
     mix = {k: v / total for k, v in mix.items()}
-    server = Server(Server.capacity_for(args.budget_gb * 1e9, mix), keep_results=False)
+    server = Server(budget_bytes=args.budget_gb * 1e9, keep_results=False)
     print(json.dumps(server.run(reqs, args.window, drain=args.drain)))
