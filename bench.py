@@ -1,6 +1,8 @@
 """Benchmark: aggregate simulated days per second of the ExoPlaSim timestep at
 T42 L10 (45-minute steps), batched over many planets on each GPU, with the
-plain single-run figure beside it.
+plain single-run figure, the split-precision (tensor-core Legendre) arm, the
+T63 and mixed-resolution ensemble configurations and the served latency
+sample beside it.
 
 Default (our arm): python bench.py [--gpus N --steps K --warmup W]
   one process per GPU (torchrun for N > 1); every rank steps its own batch of
@@ -15,11 +17,9 @@ from __future__ import annotations
 
 import argparse
 import datetime
-import glob
 import importlib
 import json
 import os
-import re
 import subprocess
 import sys
 import threading
@@ -36,13 +36,16 @@ DAYS_PER_STEP = STEP_MINUTES / 1440.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=32)
+    ap.add_argument("--steps", type=int, default=320, help="timed model steps (about 1 s at 128 planets)")
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--slots", type=int, default=128)
     ap.add_argument("--chunk", type=int, default=32, help="model steps per engine call (one CUDA graph)")
     ap.add_argument("--no-baseline", action="store_true", help="skip the timed CPU baseline sample")
     ap.add_argument("--no-served", action="store_true", help="skip the continuous-batching latency sample")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the split-precision, T63 and mixed-ensemble configurations")
+    ap.add_argument("--served-seconds", type=float, default=30.0, help="serving window (config 5 asks 600 s)")
     return ap.parse_args()
 
 
@@ -151,17 +154,25 @@ HBM_BOUND = ("fourier_inverse", "sp2gp", "fourier_forward", "legendre_inverse", 
 
 
 def measured_traffic():
-    """DRAM bytes per launch (read + write) from the committed ncu summaries:
-    lines 'Traffic per launch (<kernel>, 128 planets): <bytes> bytes'."""
-    out = {}
-    pat = re.compile(r"^Traffic per launch \((\w+), 128 planets\): (\d+) bytes")
-    for path in glob.glob(os.path.join(ROOT, "profiles", "*.md")):
-        with open(path) as f:
-            for line in f:
-                mt = pat.match(line.strip())
-                if mt:
-                    out[mt.group(1)] = int(mt.group(2))
-    return out
+    """DRAM bytes per launch (read + write) of the HBM-bound kernels at 128
+    planets, from the committed data file profiles/dram_traffic.json (ncu
+    captures; the file names them)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
+            return {k: int(v) for k, v in json.load(f)["bytes_per_launch"].items()}
+    except (OSError, ValueError, KeyError):
+        return {}
+
+
+def compulsory_bytes(truncation, levels):
+    """The step's compulsory HBM traffic per planet: the state read and
+    written once, 4 * 2 * [(8L + 2) NRSP + (7L + 36) NHOR] bytes (the 10
+    spectral prognostics and about 37 grid fields of the reference's
+    trajectory field list)."""
+    nlat = {21: 32, 42: 64, 63: 96}[truncation]
+    nrsp = (truncation + 1) * (truncation + 2)
+    nhor = 2 * nlat * nlat
+    return 4 * 2 * ((8 * levels + 2) * nrsp + (7 * levels + 36) * nhor)
 
 
 def roofline(engine, peaks):
@@ -205,23 +216,129 @@ def cpu_baseline_sample(planet_list, threads, steps):
     return threads * steps * DAYS_PER_STEP / dt, dt
 
 
-def served_sample(seconds, slots, rate, seed=7):
-    """Continuous batching of T42 L10 runs of 0.5-2 simulated days arriving
-    as a Poisson stream: time from arrival to result (p50, p99) and the
-    simulated days served per second. Planets are built before the window
-    (they are the clients' input); admission, set-up and stepping are in
-    it."""
+def timed_steps(engine, steps, chunk=32):
+    """Device time (ms, CUDA events of exogcm_last_step_ms summed over the
+    calls) of `steps` model steps in calls of at most `chunk` steps, after
+    capturing each call's graph."""
+    calls = []
+    while steps > 0:
+        calls.append(min(chunk, steps))
+        steps -= calls[-1]
+    for k in set(calls):
+        engine.step(k, publish_every=1 << 20)
+    total = 0.0
+    for k in calls:
+        engine.step(k, publish_every=1 << 20)
+        total += engine.last_step_ms()
+    return total
+
+
+def engine_for(pkg, planet_list, mode):
+    cfg = planet_list[0].config
+    e = pkg.Engine(cfg["truncation"], cfg["layers"], len(planet_list), mode=mode)
+    for s, p in enumerate(planet_list):
+        e.configure(s, p)
+    e.step(3)  # start-up steps
+    e.step(4, publish_every=1 << 20)
+    return e
+
+
+def sim_days_per_s(planets_n, steps, minutes, ms):
+    return planets_n * steps * minutes / 1440.0 / (ms / 1000.0)
+
+
+def extra_configs(pkg, plist, steps):
+    """The metric's other configurations on one GPU:
+    split precision: the same 128 T42 L10 planets with every Legendre
+      transform on the tensor cores (engine mode 2);
+    single slot: one T42 L10 planet on the optimized path (mode 1);
+    T63 L10 (30-minute steps): one planet on the split-precision path, and 32
+      planets batched on both paths;
+    mixed ensemble: 128 T21 L5 + 96 T42 L10 + 32 T63 L10 planets with the
+      ensemble's seeded parameter draw, one simulated day (32, 32 and 48
+      steps) per launch of one CUDA graph holding the three engines' batch
+      graphs (exogcm_group_step), device-timed with CUDA events."""
+    import torch
+    planets = importlib.import_module("web-exoplasim_b200.planets")
+    out = {}
+    e = engine_for(pkg, plist, 2)
+    ms = timed_steps(e, steps)
+    out["split_precision"] = {"value": round(sim_days_per_s(len(plist), steps, 45.0, ms), 3), "unit": "sim-days/s",
+                              "ms_per_step": round(ms / steps, 4), "mode": 2, "launches_per_step": e.graph_launches(1)}
+    e.close()
+    e = engine_for(pkg, plist[:1], 1)
+    ms = timed_steps(e, 128)
+    out["single_slot_optimized"] = {"value": round(sim_days_per_s(1, 128, 45.0, ms), 3), "unit": "sim-days/s",
+                                    "ms_per_step": round(ms / 128, 4)}
+    e.close()
+    t63 = [planets.make_planet(3000 + i, truncation=63, levels=10, timestepMinutes=30.0) for i in range(32)]
+    e = engine_for(pkg, t63[:1], 2)
+    ms = timed_steps(e, 96)
+    out["t63_single_split"] = {"value": round(sim_days_per_s(1, 96, 30.0, ms), 3), "unit": "sim-days/s",
+                               "ms_per_step": round(ms / 96, 4)}
+    e.close()
+    for mode in (1, 2):
+        e = engine_for(pkg, t63, mode)
+        ms = timed_steps(e, 64)
+        out[f"t63_32planets_mode{mode}"] = {"value": round(sim_days_per_s(32, 64, 30.0, ms), 3),
+                                            "unit": "sim-days/s", "ms_per_step": round(ms / 64, 4)}
+        e.close()
+    groups = []
+    for (tr, lv, n, minutes, seed) in ((21, 5, 128, 45.0, 41), (42, 10, 96, 45.0, 42), (63, 10, 32, 30.0, 43)):
+        draws = planets.ensemble_parameters(seed, n)
+        ps = []
+        for i, d in enumerate(draws):
+            d = dict(d)
+            lf = d.pop("land_fraction")
+            ps.append(planets.make_planet(seed * 1000 + i, truncation=tr, levels=lv, land_fraction=lf,
+                                          timestepMinutes=minutes, **d))
+        groups.append((engine_for(pkg, ps, 1), n, minutes, int(round(1440 / minutes))))
+    engines = [e for e, *_ in groups]
+    per_day = [d for *_, d in groups]
+    pkg.group_step(engines, per_day)  # instantiates the group graph
+    rounds = 3
+    device_ms = 0.0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(rounds):
+        device_ms += pkg.group_step(engines, per_day)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    days = rounds * sum(n for _, n, _, _ in groups)
+    unstable = sum(int(e.unstable().sum()) for e in engines)
+    out["mixed_ensemble"] = {"value": round(days / (device_ms / 1000.0), 3), "unit": "sim-days/s",
+                             "planets": "128 T21L5 + 96 T42L10 + 32 T63L10", "simulated_days": days,
+                             "ms_per_simulated_day": round(device_ms / rounds, 3),
+                             "wall_value": round(days / wall, 3), "unstable_planets": unstable,
+                             "launch": "one CUDA graph per simulated day (exogcm_group_step): the three "
+                                       "engines' 32, 32 and 48-step batch graphs as child nodes"}
+    for e, *_ in groups:
+        e.close()
+    return out
+
+
+def served_config5(seconds, budget_gb=40.0, seed=7):
+    """Config 5's serving loop: Poisson arrivals at 20 runs/s of seeded
+    planets, resolution uniform over T21/T42/T63 x L5/L10, duration uniform
+    over 1-365 simulated days, admitted by HBM footprint into engine blocks
+    within one byte budget, stepped with exogcm_step_async. The window is
+    `seconds` (config 5 names 10 minutes); runs unfinished at its end count
+    toward throughput by the steps they completed."""
     serving = importlib.import_module("web-exoplasim_b200.serving")
     planets = importlib.import_module("web-exoplasim_b200.planets")
-    reqs = serving.poisson_requests(rate, seconds, seed=seed, max_days=2.0, min_days=0.5, resolutions=((42, 10),))
+    reqs = serving.poisson_requests(20.0, seconds, seed=seed, max_days=365.0, min_days=1.0)
     for r in reqs:
-        r.planet = planets.make_planet(r.seed, truncation=42, levels=10)
-    server = serving.Server({(42, 10): slots}, chunk=16, keep_results=False)
-    rep = server.run(reqs, window=seconds * 10, drain=True)
+        r.planet = planets.make_planet(r.seed, truncation=r.truncation, levels=r.levels,
+                                       timestepMinutes=serving.STEP_MINUTES[r.truncation])
+    server = serving.Server(budget_bytes=budget_gb * 1e9, chunk=32, keep_results=False)
+    rep = server.run(reqs, window=seconds, drain=False)
+    server.close()
     return {"p50_s": round(rep["p50_s"], 3), "p99_s": round(rep["p99_s"], 3), "completed": rep["completed"],
-            "failed": rep["failed"], "sim_days_per_s": round(rep["sim_days_per_s"], 2),
-            "requests": len(reqs), "arrival_rate_per_s": rate, "run_days": "0.5-2 (uniform)", "slots": slots,
-            "window_s": round(rep["window_s"], 2)}
+            "failed": rep["failed"], "sim_days_per_s": round(rep["sim_days_per_s"], 2), "requests": len(reqs),
+            "arrival_rate_per_s": 20.0, "run_days": "1-365 (uniform)", "resolutions": "T21/T42/T63 x L5/L10",
+            "window_s": round(rep["window_s"], 2), "queue_depth_mean": round(rep["queue_depth_mean"], 1),
+            "queue_depth_max": rep["queue_depth_max"], "budget_gb": budget_gb, "slots": rep["slots"],
+            "blocks_created": rep["blocks_created"], "blocks_destroyed": rep["blocks_destroyed"]}
 
 
 def reference_arm(args, rank):
@@ -344,12 +461,31 @@ def main():
 
     launches = engine.graph_launches(1) * args.steps
     roof = roofline(engine, peaks) if rank == 0 else None
+    if roof is not None:
+        # the path's roofline: the step's compulsory bytes over the step time
+        b_min = compulsory_bytes(42, 10) * slots
+        peak = peaks.get("hbm_gbs", 6650.0)
+        roof["path"] = {"compulsory_bytes_per_step": b_min, "ms_per_step": round(device_ms / args.steps, 4),
+                        "achieved": round(b_min / (device_ms / args.steps * 1e-3) / 1e9, 1), "peak": peak,
+                        "frac": round(b_min / (device_ms / args.steps * 1e-3) / 1e9 / peak, 4)}
     tuning = engine.tuning()
+    extra = None
     served = None
-    if rank == 0 and world == 1 and not args.no_served:
+    if rank == 0 and world == 1:
         engine.close()
         engine = None
-        served = served_sample(seconds=4.0, slots=64, rate=16.0)
+        # the extra configurations report an error in the line rather than
+        # losing the headline when one of them fails
+        if not args.no_extra:
+            try:
+                extra = extra_configs(pkg, plist, max(64, args.steps // 2))
+            except Exception as exc:  # noqa: BLE001
+                extra = {"extra_configs_error": f"{type(exc).__name__}: {exc}"}
+        if not args.no_served:
+            try:
+                served = served_config5(args.served_seconds)
+            except Exception as exc:  # noqa: BLE001
+                served = {"error": f"{type(exc).__name__}: {exc}"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_baseline:
         v, dt = cpu_baseline_sample(plist, 1, 4)
@@ -365,7 +501,9 @@ def main():
                                    "seeded per planet)", "planets_per_gpu": slots, "global_batch": slots * world,
                        "seq_len": None, "parallelism": f"planets sharded over {world} GPU(s), no collective",
                        "l2": "state of the batch (GBs) far above the 126 MB L2; no flush needed",
-                       "path": "optimized: FFT longitude transforms (mode 1); plain single run: mode 0"},
+                       "path": "optimized FP32: FFT longitude transforms, latitude-pair SIMT Legendre (mode 1); "
+                               "split_precision: Legendre transforms on tcgen05 in 3xTF32 (mode 2); "
+                               "plain single run: mode 0"},
             "plain_single_run": {"value": round(plain_value, 3), "unit": "sim-days/s",
                                  "ms_per_step": round(pms / 32, 4)},
             "e2e": {"value": round(e2e_value, 3), "unit": "sim-days/s", "h2d_bytes_per_step": h2d_per_step,
@@ -374,6 +512,8 @@ def main():
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks.summary(),
             "served": served, "tuning": tuning,
         }
+        if extra:
+            line.update(extra)
         print(json.dumps(line), flush=True)
     if engine is not None:
         unstable = engine.unstable()

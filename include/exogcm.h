@@ -93,9 +93,11 @@ int exogcm_last_error(char* buffer, size_t size);
  * `mode` 0: the plain path (truncated-DFT longitude transforms and one thread
  * per Legendre output, as the reference's shaders); 1: the optimized path
  * (warp-shuffle FFTs, latitude-pair Legendre transforms on m-major Fourier
- * planes); 2: the optimized path with sp2fc and sp2fcdmu as tcgen05 tensor-
- * core contractions in 3xTF32 (FP32-equivalent to about 2^-21). All compute
- * in FP32 and share the physics. */
+ * planes); 2: the optimized path with every Legendre transform (sp2fc,
+ * sp2fcdmu, dv2uv, fc2sp, uv2dv/mktend, qtend) as tcgen05 tensor-core
+ * contractions in split precision (3xTF32, FP32 accumulation; within 1e-5 of
+ * FP64, about 3x a sequential-f32 sum's error). All compute in FP32 and share
+ * the physics. */
 int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine** engine);
 void exogcm_destroy(exogcm_engine* engine);
 
@@ -146,6 +148,18 @@ int exogcm_poll(exogcm_engine* engine, int* done);
 
 /* Blocks until every submitted batch is done. */
 int exogcm_wait(exogcm_engine* engine);
+
+/* Steps several engines, of any resolutions, together: engine i runs
+ * steps[i] model steps (each as exogcm_step would), all as ONE launch of a
+ * CUDA graph whose nodes are the engines' captured batch graphs, so the
+ * batches of a mixed-resolution ensemble (128 T21 L5 + 96 T42 L10 + 32 T63
+ * L10 planets, say) run concurrently from one submission. Engines must be
+ * distinct and on one device; the group graph is instantiated once per
+ * (engines, steps) list and reused. Returns when every batch is done; *ms
+ * (may be NULL) receives the device time of the launch. No counterpart in
+ * the reference, whose worker steps one planet per device
+ * (runner/webgpu/gcm.worker.ts:215-346). */
+int exogcm_group_step(exogcm_engine** engines, int count, const int* steps, int publish_every, float* ms);
 
 /* Snapshot of a slot published during the last exogcm_step (the 101/76
  * fields of snapshot/index.ts, each NHOR values): returns the step it was

@@ -73,13 +73,14 @@ def count_off(values, reference, scale):
     return int(np.count_nonzero(d > POINT_TOLERANCE * scale))
 
 
-def within_gate(gpu_error, f32_error, gpu_off, f32_off):
-    return gpu_error <= 2 * f32_error and gpu_off <= 2 * f32_off + 1
+def within_gate(gpu_error, f32_error, gpu_off, f32_off, factor=2):
+    return gpu_error <= factor * f32_error and gpu_off <= factor * f32_off + 1
 
 
-def v3_gate(gpu, exact, f32, points=None):
-    """Judges one field as verify-dynamics.mjs does. `points` is the grid's
-    column count for grid fields (the outlier rule applies to them only).
+def v3_gate(gpu, exact, f32, points=None, factor=2):
+    """Judges one field as verify-dynamics.mjs does (`factor` 2). `points` is
+    the grid's column count for grid fields (the outlier rule applies to them
+    only).
     Returns a dict with the errors, counts, the verdict and any outlier."""
     gpu = np.asarray(gpu, dtype=np.float64).reshape(-1)
     exact = np.asarray(exact, dtype=np.float64).reshape(-1)
@@ -90,7 +91,7 @@ def v3_gate(gpu, exact, f32, points=None):
         return dict(gpu=0.0 if ok else np.inf, f32=0.0, gpu_off=0, f32_off=0, ok=ok, outlier=None)
     r = dict(gpu=_rms(gpu, exact) / scale, f32=_rms(f32, exact) / scale,
              gpu_off=count_off(gpu, exact, scale), f32_off=count_off(f32, exact, scale), outlier=None)
-    r["ok"] = within_gate(r["gpu"], r["f32"], r["gpu_off"], r["f32_off"])
+    r["ok"] = within_gate(r["gpu"], r["f32"], r["gpu_off"], r["f32_off"], factor)
     if not r["ok"] and points and gpu.size % points == 0:
         sq = ((gpu - exact) ** 2).reshape(-1, points).sum(axis=0)
         total = sq.sum()
@@ -101,7 +102,7 @@ def v3_gate(gpu, exact, f32, points=None):
             out = dict(column=column, share=float(sq[column] / total), gpu=_rms(g, e) / scale,
                        f32=_rms(s, e) / scale, gpu_off=count_off(g, e, scale), f32_off=count_off(s, e, scale))
             r["outlier"] = out
-            r["ok"] = within_gate(out["gpu"], out["f32"], out["gpu_off"], out["f32_off"])
+            r["ok"] = within_gate(out["gpu"], out["f32"], out["gpu_off"], out["f32_off"], factor)
     return r
 
 

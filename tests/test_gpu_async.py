@@ -65,3 +65,34 @@ def test_configure_during_async_batch_waits_and_keeps_results():
     ref.step(16)
     assert np.array_equal(e.read(0, "st"), ref.read(0, "st"))
     assert e.slot_info(1)["step"] > 0 or e.slot_info(1)["startup_left"] < 3
+
+
+@pytest.mark.gpu
+def test_group_step_runs_mixed_resolutions_as_one_graph():
+    """exogcm_group_step: engines of three resolutions stepped by one graph
+    launch give each engine's own exogcm_step results bit for bit, with
+    per-engine step counts (T63 at 30-minute steps takes more steps per day)."""
+    specs = [(21, 5, 2, 45.0, 16), (42, 10, 1, 45.0, 16), (63, 10, 1, 30.0, 24)]
+
+    def make():
+        out = []
+        for t, l, n, minutes, _ in specs:
+            e = pkg.Engine(t, l, n, mode=1)
+            for s in range(n):
+                e.configure(s, planets.make_planet(120 + s + t, truncation=t, levels=l, timestepMinutes=minutes))
+            e.step(3)
+            out.append(e)
+        return out
+
+    grouped, alone = make(), make()
+    steps = [k for *_, k in specs]
+    for _ in range(2):
+        ms = pkg.group_step(grouped, steps)
+        assert ms > 0
+        for e, k in zip(alone, steps):
+            e.step(k)
+    for (t, l, n, *_), g, a in zip(specs, grouped, alone):
+        for s in range(n):
+            for name in ("st", "sz", "sd", "sq", "sp", "dt"):
+                assert np.array_equal(g.read(s, name), a.read(s, name)), (t, l, s, name)
+        assert g.slot_info(0)["step"] == a.slot_info(0)["step"]

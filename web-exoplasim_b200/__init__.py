@@ -75,6 +75,8 @@ SIGNATURES = {
     "exogcm_step_async": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
     "exogcm_poll": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int)]),
     "exogcm_wait": (ctypes.c_int, [_VP]),
+    "exogcm_group_step": (ctypes.c_int, [ctypes.POINTER(_VP), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                         _FP]),
     "exogcm_snapshots_begin": (ctypes.c_int, [_VP, _FP, ctypes.c_size_t]),
     "exogcm_snapshots_wait": (ctypes.c_int, [_VP]),
     "exogcm_read_snapshot": (ctypes.c_int, [_VP, ctypes.c_int, _FP, ctypes.c_size_t,
@@ -171,6 +173,19 @@ def boundary_struct(planet, nhor: int, keep: dict) -> Boundary:
                     sst=ptr("sst", sst), sst_months=0 if sst is None else int(np.size(sst) // nhor),
                     ice_cover=ptr("ice", ice), ice_cover_months=0 if ice is None else int(np.size(ice) // nhor),
                     t_init=ptr("t", planet.t_grid), q_init=ptr("q", planet.q_grid))
+
+
+def group_step(engines, steps, publish_every: int | None = None) -> float:
+    """Steps several engines (any resolutions) as one CUDA graph launch
+    (exogcm_group_step): engine i runs steps[i] model steps. Returns the
+    launch's device time in ms."""
+    lib = load_library()
+    n = len(engines)
+    handles = (_VP * n)(*[e.h for e in engines])
+    counts = (ctypes.c_int * n)(*steps)
+    ms = ctypes.c_float()
+    _check(lib.exogcm_group_step(handles, n, counts, publish_every or max(max(steps), 1 << 20), ctypes.byref(ms)))
+    return ms.value
 
 
 def setup_preview(planet, name: str) -> np.ndarray:

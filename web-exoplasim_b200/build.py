@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libexogcm.so")
 SOURCES = ["engine.cu", "transforms.cu", "legendre.cu", "legendre_tc.cu", "fft.cu", "spectral_grid.cu", "dynamics.cu",
-           "physics.cu", "noalloc.cu", "setup.cpp"]
+           "physics.cu", "physics_flux.cu", "noalloc.cu", "setup.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
@@ -19,11 +19,16 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std
 # longwave fits and fluxes missed the reference's V3 gate (GPU error against
 # FP64 within twice a sequential-f32 build's) by 2-3x, while these flags pass
 # it; IEEE division and square root everywhere cost 45 % more step time at
-# T42. The large-scale condensation uses IEEE division explicitly.
+# T42. The large-scale condensation uses IEEE division explicitly, and the
+# fixer apply, surface-flux, vertical-diffusion and solar-angle kernels
+# (physics_flux.cu) are compiled with IEEE division and square root: with 2-ulp
+# division more points of vdiff's humidity tendency left V3's tolerance than
+# a sequential-f32 build's.
 # The grid-point dynamics kernels divide to 2 ulp as well (-prec-div=false):
 # elementwise kernels such as physics_out spent most of their issue slots in
 # the IEEE division sequence.
-FILE_FLAGS = {"physics.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"], "dynamics.cu": ["-prec-div=false"]}
+FILE_FLAGS = {"physics.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"], "physics_flux.cu": ["-ftz=true"],
+              "dynamics.cu": ["-prec-div=false"]}
 
 
 def stale() -> bool:

@@ -339,18 +339,21 @@ __global__ void __launch_bounds__(kBlock) k_spectrald_diffusion(Model m) {
     const float stp = (k ? stp0.y : stp0.x) + D2 * (k ? stt0.y : stt0.x);
     const float sdp = (k ? sdp0.y : sdp0.x) + D2 * (k ? sdt0.y : sdt0.x);
     const float sqp = (k ? sqp0.y : sqp0.x) + D2 * (k ? sqt0.y : sqt0.x);
+    // IEEE divisions (the file otherwise divides to 2 ulp): the diffusion
+    // and friction increments feed mkdheat's heating through two more
+    // transforms, where 2-ulp quotients left V3's bound.
     const float sk = sakpp[k];
-    const float stt = ((-damp - tdisst * sk) * stp + damp * srp[k]) / (1.f + D2 * (damp + tdisst * sk));
-    const float sqt = -tdissq * sk * sqp / (1.f + D2 * tdissq * sk);
-    const float zsdt1 = -tfrc * sdp / (1.f + D2 * tfrc);
-    const float zsdt2 = -tdissd * sk * sdp / (1.f + D2 * tdissd * sk);
-    float zszt1 = -tfrc * szp / (1.f + D2 * tfrc);
-    float zszt2 = -tdissz * sk * szp / (1.f + D2 * tdissz * sk);
+    const float stt = __fdiv_rn((-damp - tdisst * sk) * stp + damp * srp[k], 1.f + D2 * (damp + tdisst * sk));
+    const float sqt = __fdiv_rn(-tdissq * sk * sqp, 1.f + D2 * tdissq * sk);
+    const float zsdt1 = __fdiv_rn(-tfrc * sdp, 1.f + D2 * tfrc);
+    const float zsdt2 = __fdiv_rn(-tdissd * sk * sdp, 1.f + D2 * tdissd * sk);
+    float zszt1 = __fdiv_rn(-tfrc * szp, 1.f + D2 * tfrc);
+    float zszt2 = __fdiv_rn(-tdissz * sk * szp, 1.f + D2 * tdissz * sk);
     float szt = zszt1 + zszt2;
     if (s + k == 2) {
-      zszt1 = zszt1 + PLAVOR * tfrc / (1.f + D2 * tfrc);
-      zszt2 = zszt2 + PLAVOR * tdissz * sk / (1.f + D2 * tdissz * sk);
-      szt = szt + PLAVOR * (tfrc / (1.f + D2 * tfrc) + tdissz * sk / (1.f + D2 * tdissz * sk));
+      zszt1 = zszt1 + __fdiv_rn(PLAVOR * tfrc, 1.f + D2 * tfrc);
+      zszt2 = zszt2 + __fdiv_rn(PLAVOR * tdissz * sk, 1.f + D2 * tdissz * sk);
+      szt = szt + PLAVOR * (__fdiv_rn(tfrc, 1.f + D2 * tfrc) + __fdiv_rn(tdissz * sk, 1.f + D2 * tdissz * sk));
     }
     const float v[12] = {szp, stp, sdp, sqp, stt, sqt, zsdt1 + zsdt2, szt, zsdt1 * D2, zszt1 * D2, zsdt2 * D2,
                          zszt2 * D2};
@@ -400,9 +403,10 @@ __global__ void __launch_bounds__(kBlock) k_mkdheat(Model m, int stage) {
   const PlanetConst& K = m.pc[slot];
   const float4 heat = make_float4(1.f + K.ADV * dq.x, 1.f + K.ADV * dq.y, 1.f + K.ADV * dq.z, 1.f + K.ADV * dq.w);
   if (stage == 3) {
+    // IEEE divisions throughout mkdheat, as in spectrald's diffusion.
     auto one = [&](float e, float ht, float p) {
-      const float dtdt = -e * 0.5f / K.ACPD / ht / p * K.GA / ds;
-      return dtdt / K.CT / K.WW;
+      const float dtdt = __fdiv_rn(__fdiv_rn(__fdiv_rn(__fdiv_rn(-e * 0.5f, K.ACPD), ht), p) * K.GA, ds);
+      return __fdiv_rn(__fdiv_rn(dtdt, K.CT), K.WW);
     };
     st4(F.zdtdt, i, make_float4(one(ek.x, heat.x, dp.x), one(ek.y, heat.y, dp.y), one(ek.z, heat.z, dp.z),
                                 one(ek.w, heat.w, dp.w)));
@@ -413,10 +417,10 @@ __global__ void __launch_bounds__(kBlock) k_mkdheat(Model m, int stage) {
     const float u = zu1 * scale, v = zv1 * scale, du = zdu1 * scale, dv = zdv1 * scale;
     const float change = du * (2.f * u + du) + dv * (2.f * v + dv);
     if (stage == 1) {
-      const float dtdt = -change / P.deltsec2 * 0.5f / K.ACPD / ht;
-      return dtdt / K.CT / K.WW;
+      const float dtdt = __fdiv_rn(__fdiv_rn(__fdiv_rn(-change, P.deltsec2) * 0.5f, K.ACPD), ht);
+      return __fdiv_rn(__fdiv_rn(dtdt, K.CT), K.WW);
     }
-    return change / P.deltsec2 * p / K.GA * ds;
+    return __fdiv_rn(__fdiv_rn(change, P.deltsec2) * p, K.GA) * ds;
   };
   const float4 r = make_float4(one(rc.x, zu.x, zv.x, zdu.x, zdv.x, heat.x, dp.x),
                                one(rc.y, zu.y, zv.y, zdu.y, zdv.y, heat.y, dp.y),

@@ -22,6 +22,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -125,6 +126,7 @@ struct exogcm_engine {
   bool copy_pending = false;
   std::vector<Slot> slots;
   std::map<int, cudaGraphExec_t> graphs;
+  std::map<int, cudaGraph_t> graph_templates;  // the captured K-step graphs (child nodes of group graphs)
   Tuning tune{};
   SharedSetup shared_setup;  // host copy of the shared tables (set-up of later planets)
 
@@ -469,16 +471,16 @@ void run_stage(const Model& m, const std::string& s, cudaStream_t st) {
 }
 
 // master's step order (stepper/index.ts:148-161).
+// The physics runs as fused column kernels between the per-planet
+// reductions (physics.cu); exogcm_run_stage runs the same routines stage by
+// stage.
 void full_step(const Model& m, cudaStream_t st) {
   stage_gridpointa(m, st);
   dyn_spectrala(m, st);
   stage_physics_in(m, st);
-  phy_fixer(m, st);
-  phy_surface_flux(m, st);
-  phy_radiation(m, st);
-  stage_precipitation(m, st);
-  phy_surface(m, st);
-  phy_carbon(m, st);
+  phy_fused_through_radiation(m, st);
+  tr_sp2gp(m, m.f.sqt, m.f.fdqt, m.f.dqt, m.d.L * m.d.S, m.sh.qi, st);  // precipitation's dqt
+  phy_fused_precipitation_to_carbon(m, st);
   stage_physics_out(m, st);
   stage_spectrald(m, st);
   phy_pack(m, st);
@@ -529,7 +531,7 @@ cudaGraphExec_t batch_graph(exogcm_engine* e, int K) {
   check(cudaStreamEndCapture(e->stream, &graph), "capture end");
   cudaGraphExec_t exec;
   check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
-  cudaGraphDestroy(graph);
+  e->graph_templates[K] = graph;
   e->graphs[K] = exec;
   return exec;
 }
@@ -735,6 +737,26 @@ void autotune(exogcm_engine* e) {
   }
 }
 
+// Group graphs (exogcm_group_step): one instantiated graph per list of
+// (engine, steps), whose nodes are the engines' K-step batch graphs as
+// child graphs. Engines being destroyed drop the group graphs they are in.
+std::mutex g_group_mutex;
+std::map<std::vector<std::pair<const exogcm_engine*, int>>, cudaGraphExec_t> g_group_graphs;
+
+void drop_group_graphs(const exogcm_engine* e) {
+  std::lock_guard<std::mutex> lock(g_group_mutex);
+  for (auto it = g_group_graphs.begin(); it != g_group_graphs.end();) {
+    bool has = false;
+    for (const auto& m : it->first) has = has || m.first == e;
+    if (has) {
+      cudaGraphExecDestroy(it->second);
+      it = g_group_graphs.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
 // Retires the oldest batch in flight once its stream has passed it:
 // blocking waits for it, otherwise a batch not yet done is left alone and
 // false returned. Reports a fault word a tensor-core transform set.
@@ -838,7 +860,9 @@ void exogcm_destroy(exogcm_engine* e) {
   if (e->snap_staged) cudaEventDestroy(e->snap_staged);
   if (e->snap_copied) cudaEventDestroy(e->snap_copied);
   cudaFree(e->snap_stage);
+  drop_group_graphs(e);
   for (auto& g : e->graphs) cudaGraphExecDestroy(g.second);
+  for (auto& g : e->graph_templates) cudaGraphDestroy(g.second);
   cudaFree(e->arena);
   cudaFree(e->shared_buf);
   cudaFree(e->mode_buf);
@@ -1026,6 +1050,77 @@ int exogcm_step(exogcm_engine* e, int steps, int publish_every) {
   const int rc = exogcm_step_async(e, steps, publish_every);
   if (rc != EXOGCM_OK) return rc;
   return exogcm_wait(e);
+}
+
+int exogcm_group_step(exogcm_engine** engines, int count, const int* steps, int publish_every, float* ms) {
+  return guard([&] {
+    if (!engines || !steps || count < 1) throw Error(EXOGCM_EINVAL, "null argument or empty group");
+    std::vector<std::pair<const exogcm_engine*, int>> key;
+    for (int i = 0; i < count; ++i) {
+      exogcm_engine* e = engines[i];
+      if (!e) throw Error(EXOGCM_EINVAL, "null engine in group");
+      if (steps[i] < 1 || steps[i] > kMaxBatch) throw Error(EXOGCM_EINVAL, "steps must be 1..64");
+      if (publish_every < 1 || steps[i] > publish_every)
+        throw Error(EXOGCM_EINVAL, "publish_every must be >= steps so each slot publishes at most once");
+      if (!e->shared_ready) throw Error(EXOGCM_ESTATE, "an engine of the group has no slot configured");
+      if (e->device != engines[0]->device) throw Error(EXOGCM_EINVAL, "engines of a group share one device");
+      for (const auto& k : key)
+        if (k.first == e) throw Error(EXOGCM_EINVAL, "an engine appears twice in the group");
+      key.push_back({e, steps[i]});
+      retire_all(e);
+    }
+    exogcm_engine* lead = engines[0];
+    cudaStream_t st = lead->stream;
+    // Each engine's step values, uploaded to its own parameter block; its
+    // K-step graph (captured once) becomes a child node of the group graph.
+    for (int i = 0; i < count; ++i) {
+      exogcm_engine* e = engines[i];
+      const int S = e->d.S;
+      for (int s = 0; s < S; ++s) e->slots[s].published = -1;
+      for (int k = 0; k < steps[i]; ++k)
+        for (int s = 0; s < S; ++s) e->hparams[(size_t)k * S + s] = next_params(e->slots[s], publish_every, true);
+      check(cudaMemcpyAsync(e->params, e->hparams, (size_t)steps[i] * S * sizeof(StepParams),
+                            cudaMemcpyHostToDevice, st),
+            "params upload");
+      batch_graph(e, steps[i]);
+    }
+    cudaGraphExec_t exec = nullptr;
+    {
+      std::lock_guard<std::mutex> lock(g_group_mutex);
+      auto it = g_group_graphs.find(key);
+      if (it != g_group_graphs.end()) exec = it->second;
+    }
+    if (!exec) {
+      cudaGraph_t parent;
+      check(cudaGraphCreate(&parent, 0), "group graph");
+      for (int i = 0; i < count; ++i) {
+        cudaGraphNode_t node;
+        check(cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, engines[i]->graph_templates.at(steps[i])),
+              "group graph child");
+      }
+      check(cudaGraphInstantiate(&exec, parent, 0), "group graph instantiate");
+      cudaGraphDestroy(parent);
+      std::lock_guard<std::mutex> lock(g_group_mutex);
+      g_group_graphs[key] = exec;
+    }
+    check(cudaEventRecord(lead->ev0, st), "event");
+    check(cudaGraphLaunch(exec, st), "group graph launch");
+    check(cudaEventRecord(lead->ev1, st), "event");
+    for (int i = 0; i < count; ++i) phy_finite_check(engines[i]->model(steps[i] - 1), st);
+    check(cudaStreamSynchronize(st), "group step");
+    float t = 0.f;
+    check(cudaEventElapsedTime(&t, lead->ev0, lead->ev1), "event time");
+    if (ms) *ms = t;
+    for (int i = 0; i < count; ++i) {
+      int fault = 0;
+      check(cudaMemcpy(&fault, engines[i]->fault, sizeof(int), cudaMemcpyDeviceToHost), "fault word");
+      if (fault) {
+        check(cudaMemset(engines[i]->fault, 0, sizeof(int)), "fault word");
+        throw Error(EXOGCM_EDEVICE, "a tensor-core transform gave up waiting for its MMAs; this step's results are invalid");
+      }
+      engines[i]->last_ms = t;
+    }
+  });
 }
 
 int exogcm_read_snapshot(exogcm_engine* e, int slot, float* values, size_t count, long* step) {

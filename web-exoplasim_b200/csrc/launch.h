@@ -76,6 +76,12 @@ void dyn_spectrald_update(const Model& m, cudaStream_t st);
 void dyn_physics_in(const Model& m, cudaStream_t st);
 void dyn_physics_out(const Model& m, cudaStream_t st);
 
+// physics_flux.cu (IEEE division): fixer apply, surface fluxes, vdiff, solang/mko3
+void phy_fixer_apply(const Model& m, cudaStream_t st);
+void phy_solang_mko3(const Model& m, cudaStream_t st);
+void phy_fused_fixer_flux_solang(const Model& m, cudaStream_t st);
+bool phy_flux_launch_one(const Model& m, const std::string& kernel, cudaStream_t st);
+
 // physics.cu
 void phy_fixer(const Model& m, cudaStream_t st);
 void phy_surface_flux(const Model& m, cudaStream_t st);
@@ -83,6 +89,10 @@ void phy_radiation(const Model& m, cudaStream_t st);
 void phy_precipitation_columns(const Model& m, cudaStream_t st);
 void phy_surface(const Model& m, cudaStream_t st);
 void phy_carbon(const Model& m, cudaStream_t st);
+// The full step's fused physics (see physics.cu): fixer through radiation,
+// and (after the precipitation transform) precipitation through carbon.
+void phy_fused_through_radiation(const Model& m, cudaStream_t st);
+void phy_fused_precipitation_to_carbon(const Model& m, cudaStream_t st);
 void phy_pack(const Model& m, cudaStream_t st);
 void phy_finite_check(const Model& m, cudaStream_t st);
 // One named column kernel of the physics (for timing); false if unknown.

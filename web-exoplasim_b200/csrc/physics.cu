@@ -8,101 +8,13 @@
 // keeps its levels in registers (kernels are instantiated per level count).
 // The reference's per-planet global sums (fixer, getiflx) and the mkdca pass
 // limit run as one block per slot with a fixed summation order, in FP64.
-#include <cuda_runtime.h>
-
-#include <cmath>
-#include <string>
-
-#include "common.cuh"
-#include "launch.h"
+// The fixer's apply step, the surface fluxes, vertical diffusion, solar
+// angle and ozone are in physics_flux.cu (IEEE division).
+#include "physics_common.cuh"
 
 namespace exogcm {
 
 namespace {
-
-constexpr int kBlock = 128;
-
-// Asks L2 for a line this thread reads after its first store, so that load
-// then hits L2 instead of DRAM (a hint: it moves no data into registers).
-__device__ __forceinline__ void prefetch_l2(const float* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
-
-// Column kernels take the planet constants and per-planet tables as
-// __restrict__ parameters: both are read-only during a launch, so the
-// compiler may keep their values across the kernel's stores to fields
-// instead of reloading them after every store.
-#define COLUMN_PROLOGUE                                              \
-  const Dims& d = m.d;                                               \
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;               \
-  if (c >= d.S * d.NHOR) return;                                     \
-  const int slot = c / d.NHOR;                                       \
-  const int h = c % d.NHOR;                                          \
-  const StepParams& P = m.params[slot];                              \
-  if (!P.active) return;                                             \
-  const PlanetConst& K = pcr[slot];                                  \
-  const float* tb = tabr + (size_t)slot * m.to.stride;               \
-  const size_t SN = (size_t)d.S * d.NHOR;                            \
-  const FieldPtrs& F = m.f;                                          \
-  (void)h; (void)K; (void)tb; (void)SN; (void)F; (void)P;
-
-// The same for a kernel that reads its planet's constants inside long
-// loops: column kernels run kBlock threads per block over S * NHOR columns,
-// and kBlock divides NHOR (2048, 8192 or 18432), so a block's columns
-// belong to one slot, whose constants are staged once in shared memory.
-#define COLUMN_PROLOGUE_STAGED                                       \
-  const Dims& d = m.d;                                               \
-  const int slot = blockIdx.x * kBlock / d.NHOR;                     \
-  const StepParams& P = m.params[slot];                              \
-  if (!P.active) return;                                             \
-  __shared__ PlanetConst s_planet;                                   \
-  stage_planet(pcr + slot, &s_planet);                               \
-  const PlanetConst& K = s_planet;                                   \
-  const int c = blockIdx.x * kBlock + threadIdx.x;                   \
-  if (c >= d.S * d.NHOR) return;                                     \
-  const int h = c - slot * d.NHOR;                                   \
-  const float* tb = tabr + (size_t)slot * m.to.stride;               \
-  const size_t SN = (size_t)d.S * d.NHOR;                            \
-  const FieldPtrs& F = m.f;                                          \
-  (void)h; (void)K; (void)tb; (void)SN; (void)F; (void)P;
-
-// Copies one slot's constants into shared memory (all threads of the block
-// take part and meet at the barrier).
-__device__ __forceinline__ void stage_planet(const PlanetConst* src, PlanetConst* dst) {
-  constexpr int n = sizeof(PlanetConst) / sizeof(float);
-  const float* a = reinterpret_cast<const float*>(src);
-  float* b = reinterpret_cast<float*>(dst);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] = a[i];
-  __syncthreads();
-}
-
-__device__ __forceinline__ float sat_capped(const PlanetConst& K, float t, float p) {
-  return fminf(K.RDBRV * K.RA1 * expf(K.RA2 * (t - K.TMELT) / (t - K.RA4)) / p, K.RDBRV);
-}
-// The same with IEEE divisions, for the large-scale condensation, whose
-// precipitation is the small difference of two iterated states.
-__device__ __forceinline__ float sat_capped_rn(const PlanetConst& K, float t, float p) {
-  return fminf(__fdiv_rn(K.RDBRV * K.RA1 * expf(__fdiv_rn(K.RA2 * (t - K.TMELT), t - K.RA4)), p), K.RDBRV);
-}
-__device__ __forceinline__ float sat_divided(const PlanetConst& K, float t, float p) {
-  const float q = sat_capped(K, t, p);
-  return q / (1.f - K.MOIST * q);
-}
-// x^y for x >= 0 with 0^y = 0: precise_pow (src/model/shared/gpu/math/wgsl/
-// precise.wgsl:100-103) is exp(y * log(x)); here exp2(y * log2(x)) with
-// CUDA's own exp2f and log2f.
-__device__ __forceinline__ float fpow(float x, float y) { return x == 0.f ? 0.f : exp2f(y * log2f(x)); }
-// x^n by binary exponentiation, as libgcc's __powisf2 computes x**n.
-__device__ __forceinline__ float powi(float x, int n) {
-  float base = x;
-  unsigned mm = (unsigned)abs(n);
-  float result = (mm & 1u) ? x : 1.f;
-  mm >>= 1;
-  while (mm) {
-    base = base * base;
-    if (mm & 1u) result = result * base;
-    mm >>= 1;
-  }
-  return n < 0 ? 1.f / result : result;
-}
 
 // ---------------------------------------------------------------- fixer
 // physics/fixer/wgsl/column.wgsl: fix0d per column.
@@ -187,7 +99,6 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_fixer_row(Model m) {
 // reference's reduction/wgsl/sum.wgsl, kept in double as the build asks of
 // global budget reductions). Writes the sums as floats to target[0|1 * S + slot]
 // and as doubles to sums[slot * 4 + which * 2 + 0|1].
-constexpr int kSumThreads = 256;
 __global__ void __launch_bounds__(kSumThreads) k_slot_sums(Model m, const float* a, const float* b, float* target,
                                                            int which) {
   const Dims& d = m.d;
@@ -219,300 +130,7 @@ __global__ void __launch_bounds__(kSumThreads) k_slot_sums(Model m, const float*
   }
 }
 
-// physics/fixer/wgsl/apply.wgsl: the global step, gqdt and the new dq. The
-// fixer is the first to raise gqdt after physics_in zeroed it, so within a
-// full step (Model::zero_gdt = 0) it adds its increment to 0 unread.
-template <int NL>
-__global__ void __launch_bounds__(kBlock) k_fixer_apply(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
-  COLUMN_PROLOGUE
-  const double zzneg = m.sums[slot * 4], zzpos = m.sums[slot * 4 + 1];
-  const float scale = zzneg > 0.0 ? (float)((zzpos - zzneg) / zzpos) : 1.f;
-  const float dp = F.dp[c];
-  // every level's inputs are read before the first store (the compiler
-  // cannot prove the fields distinct)
-  float fq[NL], gq[NL], dq[NL];
-#pragma unroll
-  for (int l = 0; l < NL; ++l) {
-    const size_t at = l * SN + c;
-    fq[l] = F.fixq[at];
-    gq[l] = m.zero_gdt ? F.gqdt[at] : 0.f;
-    dq[l] = F.dq[at];
-  }
-#pragma unroll
-  for (int l = 0; l < NL; ++l) {
-    const size_t at = l * SN + c;
-    float q = fq[l];
-    if (zzneg > 0.0) q = fmaxf(q * scale, 0.f);
-    F.gqdt[at] = gq[l] + dp * (q - dq[l]) / P.delt2 / K.PSURF;
-    F.dq[at] = q;
-  }
-}
-
-// ---------------------------------------------------------------- surface flux
-// physics/surface-flux/wgsl/surflx.wgsl: transfer coefficients, implicit
-// stress, sensible heat and evaporation.
-template <int NL>
-__global__ void __launch_bounds__(kBlock) k_surflx(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
-  COLUMN_PROLOGUE
-  const int low = NL - 1;
-  const size_t lo = low * SN + c, sf = NL * SN + c;
-  const float u = F.du[lo], v = F.dv[lo], t = F.dt[lo], q = F.dq[lo], ts = F.dt[sf], qs = F.dq[sf];
-  const float dp = F.dp[c], dls = F.dls[c];
-  // the tendencies and surface values used after the first store are read
-  // here (the compiler cannot prove the fields distinct); within a full step
-  // the tendencies hold physics_in's zeros, taken unread (Model::zero_gdt)
-  const bool earlier = m.zero_gdt != 0;
-  const float dudt0 = earlier ? F.dudt[lo] : 0.f, dvdt0 = earlier ? F.dvdt[lo] : 0.f;
-  const float dtdt0 = earlier ? F.dtdt[lo] : 0.f, dqdt0 = earlier ? F.dqdt[lo] : 0.f;
-  const float drhs = F.drhs[c], dwatc = F.dwatc[c], dz0 = F.dz0[c];
-  const float dsigma = tb[m.to.dsigma + low];
-  const float zfac = tb[m.to.flux_sigfac], zlnsig = tb[m.to.flux_lnsig];
-  const float moisture = 1.f / K.RDBRV - 1.f;
-  const float VK = 0.4f;
-  const float D2 = P.deltsec2;
-  float dtsa = t * zfac * (1.f + moisture * q);
-  const float zabsu2 = fmaxf(K.ZUMIN, u * u + v * v);
-  const float znl = -K.GASCON * 0.5f * (t + dtsa) * zlnsig / K.GA;
-  const float zbz0 = znl / dz0;
-  const float zri = K.GA * znl / (zabsu2 * dtsa) * (dtsa - ts * (1.f + moisture * qs));
-  const float zkblnz = VK / logf(zbz0 + 1.f);
-  const float zkblnz2 = zkblnz * zkblnz;
-  float zrifm, zrifh;
-  if (zri <= 0.f) {
-    const float zdenom = 1.f + 3.f * K.VDIFF_C * K.VDIFF_B * sqrtf(-1.f * zri * (zbz0 + 1.f)) * zkblnz2;
-    zrifm = 1.f - 2.f * K.VDIFF_B * zri / zdenom;
-    if (dls < 1.f) {
-      const float zdth = -(dtsa - ts * (1.f + moisture * qs));
-      zrifh = powf(1.f + powf(0.0016f * powf(zdth, 1.f / 3.f) / sqrtf(zabsu2) / zkblnz2, 1.25f), 0.8f);
-    } else {
-      zrifh = 1.f - 3.f * K.VDIFF_B * zri / zdenom;
-    }
-  } else {
-    const float zdenom = sqrtf(1.f + K.VDIFF_D * zri);
-    zrifh = 1.f / (1.f + 3.f * K.VDIFF_B * zri * zdenom);
-    zrifm = 1.f / (1.f + 2.f * K.VDIFF_B * zri / zdenom);
-  }
-  const float ztrans = sqrtf(zabsu2) * zkblnz2;
-  const float transh = ztrans * zrifh, transm = ztrans * zrifm;
-  F.dtransh[c] = transh;
-  F.dtransm[c] = transm;
-  const float zkonst1 = K.GA * D2 / (K.GASCON * dsigma);
-  const float zkonst2 = dsigma / D2 / K.GA;
-  const float zkdiffm = zkonst1 * transm / ts;
-  const float zun = u / (1.f + zkdiffm), zvn = v / (1.f + zkdiffm);
-  F.dudt[lo] = dudt0 + (zun - u) / D2;
-  F.dvdt[lo] = dvdt0 + (zvn - v) / D2;
-  float dtdt = dtdt0;
-  if (K.NDHEAT != 0.f) dtdt = dtdt + -(zun * zun - u * u + zvn * zvn - v * v) / D2 * 0.5f / K.ACPD / (1.f + K.ADV * q);
-  const float taux = dp * zkonst2 * zkdiffm * zun, tauy = dp * zkonst2 * zkdiffm * zvn;
-  F.dtaux[c] = taux;
-  F.dtauy[c] = tauy;
-  const float ustar = sqrtf(sqrtf(taux * taux + tauy * tauy) * K.GASCON * ts / dp);
-  F.dust3[c] = ustar * ustar * ustar;
-  const float zkdiffh = zkonst1 * transh / ts;
-  const float ztn = (t + zkdiffh * ts) / (1.f + zkdiffh * zfac);
-  dtdt = dtdt + (ztn - t) / D2;
-  F.dtdt[lo] = dtdt;
-  const float moist = fmaxf(1.f, 1.f + K.ADV * q);
-  F.dshfl[c] = zkonst2 * zkdiffh * dp * K.ACPD * moist * (ztn * zfac - ts);
-  F.dshdt[c] = -1.f * zkonst2 * zkdiffh * dp * K.ACPD * moist;
-  dtsa = ztn * zfac;
-  F.dtsa[c] = dtsa;
-  const float zkdiffq = drhs * zkonst1 * transh / ts;
-  float zqn = fmaxf(q, (q + zkdiffq * qs) / (1.f + zkdiffq));
-  if (dls > 0.f) zqn = fminf(zqn, dwatc / P.deltsec * 1000.f / dp / zkonst2 + q);
-  F.dqdt[lo] = dqdt0 + (zqn - q) / D2;
-  const float devap = -dp * zkonst2 / 1000.f * (zqn - q);
-  F.devap[c] = devap;
-  const float latent = (ts > K.TMELT || dls < 0.5f) ? K.ALV : K.ALS;
-  const float dlhfl = devap * latent * 1000.f;
-  F.dlhfl[c] = dlhfl;
-  const float curvature = (ts - K.RA4) * (ts - K.RA4);
-  const float dlhdt = -1.f * latent * zkdiffq * zkonst2 * dp * K.RA2 * (K.TMELT - K.RA4) * qs / curvature;
-  F.dlhdt[c] = dlhfl == 0.f ? 0.f : dlhdt;
-}
-
-// physics/diffusion/wgsl/implicit.wgsl: ECHAM tridiagonal eliminations.
-template <int NL>
-__device__ __forceinline__ void diffuse(const float* ds, float* x, const float* k) {
-  float ebs[NL];
-  const float ds0 = ds[0];
-  ebs[0] = k[0] / (ds0 + k[0]);
-  x[0] = ds0 * x[0] / (ds0 + k[0]);
-#pragma unroll
-  for (int l = 1; l < NL - 1; ++l) {
-    const float den = ds[l] + k[l] + k[l - 1] * (1.f - ebs[l - 1]);
-    ebs[l] = k[l] / den;
-    x[l] = (x[l] * ds[l] + k[l - 1] * x[l - 1]) / den;
-  }
-  const float dsn = ds[NL - 1];
-  x[NL - 1] = (x[NL - 1] * dsn + k[NL - 2] * x[NL - 2]) / (dsn + k[NL - 2] * (1.f - ebs[NL - 2]));
-#pragma unroll
-  for (int l = NL - 2; l >= 0; --l) x[l] = x[l] + ebs[l] * x[l + 1];
-}
-
-template <int NL>
-__device__ __forceinline__ void diffuse_potential(const float* ds, float* x, const float* k, const float* skap) {
-  float ebs[NL];
-  const float ds0 = ds[0];
-  ebs[0] = k[0] / (ds0 + k[0] / skap[0]);
-  x[0] = ds0 * x[0] / (ds0 + k[0] / skap[0]);
-#pragma unroll
-  for (int l = 1; l < NL - 1; ++l) {
-    const float den = ds[l] + (k[l] + k[l - 1] * (1.f - ebs[l - 1] / skap[l - 1])) / skap[l];
-    ebs[l] = k[l] / den;
-    x[l] = (x[l] * ds[l] + k[l - 1] / skap[l - 1] * x[l - 1]) / den;
-  }
-  const int last = NL - 1;
-  const float dsn = ds[last];
-  x[last] = (x[last] * dsn + k[NL - 2] * x[NL - 2] / skap[NL - 2]) /
-            (dsn + k[NL - 2] / skap[last] * (1.f - ebs[NL - 2] / skap[NL - 2]));
-#pragma unroll
-  for (int l = NL - 2; l >= 0; --l) x[l] = x[l] + ebs[l] * x[l + 1] / skap[l + 1];
-}
-
-// physics/surface-flux/wgsl/vdiff.wgsl: Richardson-number vertical diffusion.
-template <int NL>
-__global__ void __launch_bounds__(kBlock, 3) k_vdiff(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
-  COLUMN_PROLOGUE
-  const float* ds = tb + m.to.dsigma;
-  const float* sh = tb + m.to.sigmah;
-  const float D2 = P.deltsec2;
-  // Every field value used is read here, before the first store (the
-  // compiler cannot prove the fields distinct, so a store would order each
-  // later load after it). Within a full step only surflx's lowest level of
-  // the tendencies holds more than physics_in's zeros (Model::zero_gdt).
-  float zt[NL], zq[NL], zu[NL], zv[NL], zabsu[NL], zskap[NL], zskaph[NL];
-  float dtdt[NL], dqdt[NL], dudt[NL], dvdt[NL], dq[NL];
-#pragma unroll
-  for (int l = 0; l < NL; ++l) {
-    const size_t at = l * SN + c;
-    const bool held = m.zero_gdt || l == NL - 1;
-    dtdt[l] = held ? F.dtdt[at] : 0.f;
-    dqdt[l] = held ? F.dqdt[at] : 0.f;
-    dudt[l] = held ? F.dudt[at] : 0.f;
-    dvdt[l] = held ? F.dvdt[at] : 0.f;
-    dq[l] = F.dq[at];
-    zt[l] = F.dt[at] + dtdt[l] * D2;
-    zq[l] = dq[l] + dqdt[l] * D2;
-    zu[l] = F.du[at] + dudt[l] * D2;
-    zv[l] = F.dv[at] + dvdt[l] * D2;
-    zabsu[l] = sqrtf(zu[l] * zu[l] + zv[l] * zv[l]);
-    zskap[l] = tb[m.to.vdiff_skap + l];
-    zskaph[l] = tb[m.to.vdiff_skaph + l];
-  }
-  const float zkonst1 = K.GA * D2 / K.GASCON;
-  const float zkonst2 = zkonst1 * K.GA / K.GASCON;
-  const float zkonst3 = zkonst2 * K.GA / K.GASCON;
-  const float moisture = 1.f / K.RDBRV - 1.f;
-  float kh[NL], km[NL];
-  kh[NL - 1] = 0.f;
-  km[NL - 1] = 0.f;
-#pragma unroll
-  for (int l = 0; l < NL - 1; ++l) {
-    const int lp = l + 1;
-    const float sigmah = sh[l], dsigma = ds[l], dsigmap = ds[lp];
-    const float zmixh2 = tb[m.to.vdiff_mixh2 + l], zmixm2 = tb[m.to.vdiff_mixm2 + l];
-    const float zrdsig = tb[m.to.vdiff_rdsig + l];
-    const float zfac = zkonst3 * tb[m.to.vdiff_sigmah3 + l];
-    const float zzkfac = tb[m.to.vdiff_kfac + l];
-    const float zrthl = (dsigmap + dsigma) / (zt[l] * dsigmap + zt[lp] * dsigma);
-    const float zdvds = fmaxf(K.ZUMIN, fabsf(zabsu[l] - zabsu[lp])) * zrdsig;
-    const float zdthds =
-        (zt[l] * (1.f + moisture * zq[l]) / zskap[l] - zt[lp] * (1.f + moisture * zq[lp]) / zskap[lp]) * zrdsig;
-    const float zri = zskaph[l] * K.GASCON * zdthds / (sigmah * zdvds * zdvds);
-    float zrifh, zrifm;
-    if (zri <= 0.f) {
-      const float dh = 1.f + 3.f * K.VDIFF_C * K.VDIFF_B * sqrtf(-1.f * zri) * zzkfac * zmixh2;
-      const float dm = 1.f + 3.f * K.VDIFF_C * K.VDIFF_B * sqrtf(-1.f * zri) * zzkfac * zmixm2;
-      zrifh = 1.f - 3.f * K.VDIFF_B * zri / dh;
-      zrifm = 1.f - 2.f * K.VDIFF_B * zri / dm;
-    } else {
-      const float zdenom = sqrtf(1.f + K.VDIFF_D * zri);
-      zrifh = 1.f / (1.f + 3.f * K.VDIFF_B * zri * zdenom);
-      zrifm = 1.f / (1.f + 2.f * K.VDIFF_B * zri / zdenom);
-    }
-    kh[l] = zfac * zmixh2 * zrifh * zdvds * zrthl * zrthl * zrthl;
-    km[l] = zfac * zmixm2 * zrifm * zdvds * zrthl * zrthl * zrthl;
-  }
-  float zun[NL], zvn[NL];
-#pragma unroll
-  for (int l = 0; l < NL; ++l) {
-    zun[l] = zu[l];
-    zvn[l] = zv[l];
-  }
-  diffuse<NL>(ds, zun, km);
-  diffuse<NL>(ds, zvn, km);
-#pragma unroll
-  for (int l = 0; l < NL; ++l) {
-    const size_t at = l * SN + c;
-    F.dudt[at] = dudt[l] + (zun[l] - zu[l]) / D2;
-    F.dvdt[at] = dvdt[l] + (zvn[l] - zv[l]) / D2;
-  }
-  if (K.NDHEAT != 0.f) {
-    float zke[NL], zken[NL];
-#pragma unroll
-    for (int l = 0; l < NL; ++l) zke[l] = zken[l] = 0.5f * zabsu[l] * zabsu[l];
-    diffuse<NL>(ds, zken, km);
-#pragma unroll
-    for (int l = 0; l < NL; ++l) {
-      const float zdtdt = -((zun[l] * zun[l] - zu[l] * zu[l] + zvn[l] * zvn[l] - zv[l] * zv[l]) / D2 -
-                            (zken[l] - zke[l]) / D2) * 0.5f / K.ACPD / (1.f + K.ADV * dq[l]);
-      dtdt[l] = dtdt[l] + zdtdt;
-    }
-  }
-  float zqn[NL];
-#pragma unroll
-  for (int l = 0; l < NL; ++l) zqn[l] = zq[l];
-  diffuse<NL>(ds, zqn, kh);
-#pragma unroll
-  for (int l = 0; l < NL; ++l) F.dqdt[l * SN + c] = dqdt[l] + (zqn[l] - zq[l]) / D2;
-#pragma unroll
-  for (int l = 0; l < NL - 1; ++l) kh[l] = kh[l] * zskaph[l];
-  float ztn[NL];
-#pragma unroll
-  for (int l = 0; l < NL; ++l) ztn[l] = zt[l];
-  diffuse_potential<NL>(ds, ztn, kh, zskap);
-#pragma unroll
-  for (int l = 0; l < NL; ++l) F.dtdt[l * SN + c] = dtdt[l] + (ztn[l] - zt[l]) / D2;
-}
-
 // ---------------------------------------------------------------- radiation
-constexpr float kPI = 3.14159265359f;
-constexpr float kTWOPI = kPI + kPI;
-
-// solang (physics/radiation/wgsl/solang.wgsl) and mko3 (mko3.wgsl) for one column.
-template <int NL>
-__global__ void __launch_bounds__(kBlock) k_solang_mko3(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
-  COLUMN_PROLOGUE
-  const int lat = h / d.NLON, lon = h % d.NLON;
-  float hangle = P.rad[2] + (float)lon * K.ZRLON - kPI;
-  if (hangle < -kPI) hangle = hangle + kTWOPI;
-  if (hangle > kPI) hangle = hangle - kTWOPI;
-  if (K.NFIXED == 1.f) hangle = hangle + kPI;
-  const float muz = P.rad[0] * m.sh.sid[lat] + m.sh.cola[lat] * P.rad[1] * cosf(hangle);
-  F.gmu0[c] = muz > K.ZDAWN ? muz : 0.f;
-  if (K.OZONE == 0.f) return;
-  const float ZFO3 = 100.f / 2.14f;
-  const float sid = m.sh.sid[lat];
-  const float za = K.A0O3 + K.A1O3 * fabsf(sid) + K.ACO3 * sid * P.rad[4];
-  const float dp = F.dp[c];
-  const float* ds = tb + m.to.dsigma;
-  const float* lnsig = tb + m.to.rad_lnsig;
-  float o3t = za, zh = 0.f;
-  float t[NL];  // read before the stores below (possible aliasing would order them)
-#pragma unroll
-  for (int l = 1; l < NL; ++l) t[l] = F.dt[l * SN + c];
-#pragma unroll
-  for (int l = NL - 1; l >= 1; --l) {
-    zh = zh - t[l] * K.GASCON / K.GA * lnsig[l];
-    const float o3 = -(za + za * K.ZCONST) / (1.f + expf((zh - K.BO3) / K.CO3)) + o3t;
-    F.dqo3[l * SN + c] = o3 * K.GA / (ZFO3 * ds[l] * dp);
-    o3t = o3t - o3;
-  }
-  F.dqo3[c] = o3t * K.GA / (ZFO3 * ds[0] * dp);
-}
-
 __device__ __forceinline__ float ozone_absorption(float o3, float zsolar1) {
   return (0.02118f * o3 / (1.f + 0.042f * o3 + 0.000323f * (o3 * o3)) + 1.082f * o3 / fpow(1.f + 138.6f * o3, 0.805f) +
           0.0658f * o3 / (1.f + (103.6f * o3) * (103.6f * o3) * (103.6f * o3))) /
@@ -995,7 +613,7 @@ __device__ __forceinline__ Parcel condense(const PlanetConst& K, float t0, float
 // keeps more values in registers, and four blocks measured faster than six
 // or three.
 template <int NL>
-__global__ void __launch_bounds__(kBlock, 4) k_kuo(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+__device__ __forceinline__ void b_kuo(const Model& m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const int NM = NL - 1;
   const float* ds = tb + m.to.dsigma;
@@ -1205,10 +823,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_kuo(Model m, const PlanetConst* _
     F.dqdt[at] = dqdt_in[l] + (zqn[l] - zqe[l]) / D2;
   }
 }
+template <int NL>
+__global__ void __launch_bounds__(kBlock, 4) k_kuo(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+  b_kuo<NL>(m, pcr, tabr);
+}
+
 
 // mkdca (physics/precipitation/wgsl/mkdca.wgsl): dry convective adjustment.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_mkdca(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+__device__ __forceinline__ void b_mkdca(const Model& m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const int NM = NL - 1;
   const float D2 = P.deltsec2;
@@ -1280,6 +903,11 @@ __global__ void __launch_bounds__(kBlock) k_mkdca(Model m, const PlanetConst* __
   }
   F.dca_limited[c] = limited;
 }
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_mkdca(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+  b_mkdca<NL>(m, pcr, tabr);
+}
+
 
 // mkdca-limit (physics/precipitation/wgsl/mkdca-limit.wgsl): per slot, skip
 // every adjustment when any column needed more than 2 NL passes.
@@ -1300,10 +928,10 @@ __global__ void __launch_bounds__(kSumThreads) k_mkdca_limit(Model m) {
 }
 
 // column.wgsl: mkdca's adjustment (unless skipped), mklsp, mkrain, mkclouds.
-template <int NL>
 // Its parameters carry no __restrict__: with it the compiler keeps more
 // values in registers (165), and the lower occupancy measured slower.
-__global__ void __launch_bounds__(kBlock) k_rain_column(Model m, const PlanetConst* pcr, const float* tabr) {
+template <int NL>
+__device__ __forceinline__ void b_rain_column(const Model& m, const PlanetConst* pcr, const float* tabr) {
   COLUMN_PROLOGUE
   const float* ds = tb + m.to.dsigma;
   const float* sg = tb + m.to.sigma;
@@ -1509,6 +1137,11 @@ __global__ void __launch_bounds__(kBlock) k_rain_column(Model m, const PlanetCon
   F.dql[NL * SN + c] = 0.f;
   F.dcc[NL * SN + c] = 1.f - clear;
 }
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_rain_column(Model m, const PlanetConst* pcr, const float* tabr) {
+  b_rain_column<NL>(m, pcr, tabr);
+}
+
 
 // ---------------------------------------------------------------- surface
 struct SnowLayer {
@@ -1535,7 +1168,7 @@ __device__ __forceinline__ float surface_temperature(const PlanetConst& K, float
 
 // landmod's soilstep (physics/land/wgsl/soil.wgsl): tands, mktsoil, wandr.
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_soil(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+__device__ __forceinline__ void b_soil(const Model& m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const float DS = P.deltsec;
   const float dls = F.dls[c];
@@ -1642,6 +1275,11 @@ __global__ void __launch_bounds__(kBlock) k_soil(Model m, const PlanetConst* __r
   F.drunoff[c] = drunoff;
   if (put_snowt) F.dsnowt[c] = snowt;
 }
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_soil(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+  b_soil<NL>(m, pcr, tabr);
+}
+
 
 // mkradv (physics/land/wgsl/mkradv.wgsl): river routing stencil within one
 // slot. Each thread reads only its own drunoff and its neighbours' driver,
@@ -1700,7 +1338,7 @@ __device__ __forceinline__ float clim14(const float* f, const float* w3, int c, 
 // Land surface after mkradv (physics/land/wgsl/surface.wgsl) with vegstep
 // (vegetation/wgsl/vegstep.wgsl) and glacierstep (glacier/wgsl/glacierstep.wgsl).
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_land_surface(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+__device__ __forceinline__ void b_land_surface(const Model& m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const float DS = P.deltsec;
   // Every input is read before the first store (the compiler cannot prove
@@ -1912,10 +1550,15 @@ __global__ void __launch_bounds__(kBlock) k_land_surface(Model m, const PlanetCo
   if (put_persist) F.dpersist[c] = dpersist;
   if (put_glac) F.dglac[c] = glac;
 }
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_land_surface(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+  b_land_surface<NL>(m, pcr, tabr);
+}
+
 
 // seastep coupling and icestep up to getiflx (physics/sea-ice/wgsl/ice.wgsl).
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_sea_ice(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+__device__ __forceinline__ void b_sea_ice(const Model& m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   if (P.coupled == 0.f) return;
   const bool sea = F.dls[c] < 0.5f;
@@ -2055,11 +1698,16 @@ __global__ void __launch_bounds__(kBlock) k_sea_ice(Model m, const PlanetConst* 
   F.xsmflx[c] = xsmflx;
   F.xsndch[c] = xsndch;
 }
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_sea_ice(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+  b_sea_ice<NL>(m, pcr, tabr);
+}
+
 
 // seastep (physics/sea/wgsl/seastep.wgsl) with ice_finish (sea-ice/wgsl/finish.wgsl)
 // and oceanstep (ocean/wgsl/oceanstep.wgsl).
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_sea(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+__device__ __forceinline__ void b_sea(const Model& m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const bool coupled = P.coupled != 0.f;
   // Every input is read before the first store (the compiler cannot prove
@@ -2184,10 +1832,15 @@ __global__ void __launch_bounds__(kBlock) k_sea(Model m, const PlanetConst* __re
   F.dsalb[SN + c] = K.DOCEANALB2 * (1.f - dicec) + dicec * fminf(K.DICEALBMX2, K.DICEALBMN2 + 0.025f * (273.f - dts));
   F.dz0[c] = zz0 * (1.f - dicec) + K.DZ0ICE * dicec;
 }
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_sea(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+  b_sea<NL>(m, pcr, tabr);
+}
+
 
 // carbonstep (physics/carbon/wgsl/carbonstep.wgsl).
 template <int NL>
-__global__ void __launch_bounds__(kBlock) k_carbon(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+__device__ __forceinline__ void b_carbon(const Model& m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   // inputs first: the compiler cannot prove the fields distinct
   const float precip = (F.dprc[c] + F.dprl[c]) * 3.154e9f;
@@ -2216,6 +1869,11 @@ __global__ void __launch_bounds__(kBlock) k_carbon(Model m, const PlanetConst* _
   F.localavgtemps[c] = avgtemps + tsurf * K.TIMEWEIGHT;
   F.localavgweather[c] = avgweather + local_weathering * K.TIMEWEIGHT;
 }
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_carbon(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+  b_carbon<NL>(m, pcr, tabr);
+}
+
 
 // snapshot/wgsl/pack.wgsl: the published fields, window extrema, RH.
 template <int NL>
@@ -2336,29 +1994,47 @@ __global__ void k_finite(Model m) {
   if (!isfinite(v)) m.flags[slot] = 1;
 }
 
-inline unsigned nblocks(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
-template <template <int> class Launch, typename... A>
-void by_levels(int L, A&&... a) {
-  if (L == 10)
-    Launch<10>::run(a...);
-  else if (L == 5)
-    Launch<5>::run(a...);
+
+// Fused column kernels of a full step (exogcm_step): the per-column routines
+// that follow one another between the per-planet reductions run in one
+// launch, each thread taking its column through them in the reference's
+// order (stepper/index.ts:148-161): fixer apply, surface fluxes, vertical
+// diffusion, solar angle and ozone | kuo and mkdca | rain and soil | land
+// surface and sea ice | sea and carbon. A routine re-reads the fields the one
+// before it just wrote or read for the same column from L1/L2 instead of
+// HBM, and five launches replace twelve. Stage replay (exogcm_run_stage)
+// keeps the separate kernels; a full step equals its stages bit for bit.
+template <int NL>
+__global__ void __launch_bounds__(kBlock, 4) k_fused_kuo_mkdca(Model m, const PlanetConst* __restrict__ pcr,
+                                                               const float* __restrict__ tabr) {
+  b_kuo<NL>(m, pcr, tabr);
+  b_mkdca<NL>(m, pcr, tabr);
+}
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_fused_rain_soil(Model m, const PlanetConst* pcr, const float* tabr) {
+  b_rain_column<NL>(m, pcr, tabr);
+  b_soil<NL>(m, pcr, tabr);
+}
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_fused_land_seaice(Model m, const PlanetConst* __restrict__ pcr,
+                                                              const float* __restrict__ tabr) {
+  b_land_surface<NL>(m, pcr, tabr);
+  b_sea_ice<NL>(m, pcr, tabr);
+}
+template <int NL>
+__global__ void __launch_bounds__(kBlock) k_fused_sea_carbon(Model m, const PlanetConst* __restrict__ pcr,
+                                                             const float* __restrict__ tabr) {
+  b_sea<NL>(m, pcr, tabr);
+  b_carbon<NL>(m, pcr, tabr);
 }
 
-#define COLUMN_LAUNCHER(name, kernel)                                                      \
-  template <int NL>                                                                        \
-  struct name {                                                                            \
-    static void run(const Model& m, cudaStream_t st) {                                     \
-      kernel<NL><<<nblocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m, m.pc, m.tabs); \
-    }                                                                                      \
-  };
 
 COLUMN_LAUNCHER(FixerColumn, k_fixer_column)
-COLUMN_LAUNCHER(FixerApply, k_fixer_apply)
-COLUMN_LAUNCHER(Surflx, k_surflx)
-COLUMN_LAUNCHER(Vdiff, k_vdiff)
-COLUMN_LAUNCHER(SolangMko3, k_solang_mko3)
+COLUMN_LAUNCHER(FusedKuoMkdca, k_fused_kuo_mkdca)
+COLUMN_LAUNCHER(FusedRainSoil, k_fused_rain_soil)
+COLUMN_LAUNCHER(FusedLandSeaice, k_fused_land_seaice)
+COLUMN_LAUNCHER(FusedSeaCarbon, k_fused_sea_carbon)
 template <int NL>
 struct Swr {
   static void run(const Model& m, cudaStream_t st) {
@@ -2389,16 +2065,11 @@ void phy_fixer(const Model& m, cudaStream_t st) {
   by_levels<FixerColumn>(m.d.L, m, st);
   by_levels<FixerRow>(m.d.L, m, st);
   k_slot_sums<<<m.d.S, kSumThreads, 0, st>>>(m, m.f.fixneg, m.f.fixpos, m.f.fixsum, 0);
-  by_levels<FixerApply>(m.d.L, m, st);
-}
-
-void phy_surface_flux(const Model& m, cudaStream_t st) {
-  by_levels<Surflx>(m.d.L, m, st);
-  by_levels<Vdiff>(m.d.L, m, st);
+  phy_fixer_apply(m, st);
 }
 
 void phy_radiation(const Model& m, cudaStream_t st) {
-  by_levels<SolangMko3>(m.d.L, m, st);
+  phy_solang_mko3(m, st);
   by_levels<Swr>(m.d.L, m, st);
   by_levels<LwrRadstep>(m.d.L, m, st);
 }
@@ -2421,6 +2092,32 @@ void phy_surface(const Model& m, cudaStream_t st) {
 
 void phy_carbon(const Model& m, cudaStream_t st) { by_levels<Carbon>(m.d.L, m, st); }
 
+// The full step's physics between physics_in and physics_out with the fused
+// column kernels: the fixer's column and row sums and its per-planet FP64
+// sum, then [fixer apply, surflx, vdiff, solang/mko3], swr, lwr/radstep; the
+// precipitation transform is the caller's; then [kuo, mkdca], the per-planet
+// mkdca limit, [rain column, soil], mkradv (a neighbour stencil), [land
+// surface, sea ice], the per-planet getiflx sum and [sea, carbon].
+void phy_fused_through_radiation(const Model& m, cudaStream_t st) {
+  by_levels<FixerColumn>(m.d.L, m, st);
+  by_levels<FixerRow>(m.d.L, m, st);
+  k_slot_sums<<<m.d.S, kSumThreads, 0, st>>>(m, m.f.fixneg, m.f.fixpos, m.f.fixsum, 0);
+  phy_fused_fixer_flux_solang(m, st);
+  by_levels<Swr>(m.d.L, m, st);
+  by_levels<LwrRadstep>(m.d.L, m, st);
+}
+
+void phy_fused_precipitation_to_carbon(const Model& m, cudaStream_t st) {
+  by_levels<FusedKuoMkdca>(m.d.L, m, st);
+  k_mkdca_limit<<<m.d.S, kSumThreads, 0, st>>>(m);
+  by_levels<FusedRainSoil>(m.d.L, m, st);
+  k_mkradv<<<nblocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);
+  by_levels<FusedLandSeaice>(m.d.L, m, st);
+  k_slot_sums<<<m.d.S, kSumThreads, 0, st>>>(m, m.f.ice_part1, m.f.ice_part2, m.f.ice_sums, 1);
+  by_levels<FusedSeaCarbon>(m.d.L, m, st);
+}
+
+
 void phy_pack(const Model& m, cudaStream_t st) { by_levels<Pack>(m.d.L, m, st); }
 
 void phy_finite_check(const Model& m, cudaStream_t st) {
@@ -2430,12 +2127,8 @@ void phy_finite_check(const Model& m, cudaStream_t st) {
 
 bool phy_launch_one(const Model& m, const std::string& kernel, cudaStream_t st) {
   const int L = m.d.L;
-  if (kernel == "surflx")
-    by_levels<Surflx>(L, m, st);
-  else if (kernel == "vdiff")
-    by_levels<Vdiff>(L, m, st);
-  else if (kernel == "solang_mko3")
-    by_levels<SolangMko3>(L, m, st);
+  if (phy_flux_launch_one(m, kernel, st))
+    return true;
   else if (kernel == "swr")
     by_levels<Swr>(L, m, st);
   else if (kernel == "lwr_radstep")
