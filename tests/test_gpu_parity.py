@@ -118,7 +118,7 @@ def test_stage_replay_passes_v3(truncation, levels, warm, mode):
 # Physics outputs that the transform stages pass through unchanged but that
 # carry the column physics' threshold sensitivity (precipitation's column
 # kernels, physics_in's dimensional frame is transforms only).
-PHYSICS_OUTPUTS = {"dqt", "dtdt", "dqdt", "dcc", "dql", "dprc", "dprl", "dprs", "dqvi", "icclev", "icctot", "dprcl",
+PHYSICS_OUTPUTS = {"dtdt", "dqdt", "dcc", "dql", "dprc", "dprl", "dprs", "dqvi", "icclev", "icctot", "dprcl",
                    "dprll", "dca_dtdt", "dca_dqdt", "dca_limited", "dconv", "localprecip"}
 
 

@@ -14,21 +14,22 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 # Column physics divides and takes square roots to 2 ulp (WGSL allows its
-# division 2.5 ulp) and flushes denormals to zero, but keeps CUDA's accurate
-# exp/log/pow: with the special-function-unit forms (-use_fast_math) the
-# longwave fits and fluxes missed the reference's V3 gate (GPU error against
-# FP64 within twice a sequential-f32 build's) by 2-3x, while these flags pass
-# it; IEEE division and square root everywhere cost 45 % more step time at
-# T42. The large-scale condensation uses IEEE division explicitly, and the
-# fixer apply, surface-flux, vertical-diffusion and solar-angle kernels
-# (physics_flux.cu) are compiled with IEEE division and square root: with 2-ulp
-# division more points of vdiff's humidity tendency left V3's tolerance than
-# a sequential-f32 build's.
+# division 2.5 ulp) and flushes denormals to zero; the longwave band fits take
+# their base-2 logarithm and power from the special-function unit
+# (EXOGCM_LWR_FAST_LOG2/EXP2); every other exp/log/pow is CUDA's accurate
+# one. With -use_fast_math everywhere the longwave fluxes missed the
+# reference's V3 gate (GPU error against FP64 within twice a sequential-f32
+# build's) by 2-3x; these flags pass it at T21 L5/L10, T42 L10 and T63 L10.
+# Where a tendency is a small difference of two states, the divisions are
+# IEEE explicitly (__fdiv_rn): the implicit vertical diffusion and vdiff's
+# tendencies, the large-scale condensation, spectrald's diffusion and mkdheat.
+# IEEE division everywhere in the physics cost 45 % more step time at T42.
 # The grid-point dynamics kernels divide to 2 ulp as well (-prec-div=false):
 # elementwise kernels such as physics_out spent most of their issue slots in
 # the IEEE division sequence.
-FILE_FLAGS = {"physics.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"], "physics_flux.cu": ["-ftz=true"],
-              "dynamics.cu": ["-prec-div=false"]}
+PHYSICS_FLAGS = ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]
+FILE_FLAGS = {"physics.cu": PHYSICS_FLAGS + ["-DEXOGCM_LWR_FAST_EXP2", "-DEXOGCM_LWR_FAST_LOG2"],
+              "physics_flux.cu": PHYSICS_FLAGS, "dynamics.cu": ["-prec-div=false"]}
 
 
 def stale() -> bool:

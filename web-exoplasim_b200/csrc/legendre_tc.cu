@@ -69,15 +69,17 @@ namespace exogcm {
 namespace {
 
 constexpr int kRows = 128;        // MMA M: (plane, column) rows of the data operand
-constexpr int kThreads = 192;     // warp 0 producer, warps 1-4 converters/epilogue, warp 5 MMA
-constexpr int kConv = 128;        // converter threads
+constexpr int kThreads = 320;     // warp 0 producer, warps 1-8 converters/epilogue, warp 9 MMA
+constexpr int kConv = 256;        // converter threads: two warps per scheduler hide the operand build's latency
+constexpr int kMmaWarp = 9;
 constexpr int kTmemCols = 256;    // two accumulators of up to 128 columns
 constexpr int kStepK = 8;         // K of one tf32 MMA
 constexpr int kChunkSteps = 4;    // K steps per pipeline chunk
 constexpr int kDataStepFloats = kRows * kStepK;  // one K step of hi (or lo) data operand
-constexpr int kNTab = 2;          // table stages
+constexpr int kMaxTab = 8;        // table stages at most (TcGeom::n_tab of them are used)
 constexpr int kNData = 2;         // data operand stages
 constexpr long kWaitLimit = 1L << 24;  // mbarrier polls before a role gives up
+constexpr size_t kTcSmemLimit = 227 * 1024;  // dynamic shared memory a CTA may ask
 
 // Kinds and their shapes: NR raw input fields, NA table blocks, NC output
 // columns per plane (TP = 128 / NC planes per item), FWD forward (K over
@@ -267,6 +269,8 @@ struct TcGeom {
   int box;          // inverse: TMA box width in floats (a multiple of 4)
   int out_plane;    // floats per output plane
   float plavor;     // dv2uv: planetary vorticity removed from mode (0, 1)
+  int n_tab;        // table stages in the ring (as many as shared memory holds, 2..kMaxTab)
+  int raw2d;        // inverse: the planes' rows arrive as one 2-D box (NRSP * 4 a multiple of 16)
 };
 
 struct TcMaps {
@@ -284,16 +288,16 @@ struct TcSmem {
   size_t tab, data, raw, stage, bars, total;
 };
 
-__host__ __device__ inline TcSmem tc_smem(int npad_max, int raw_floats) {
+__host__ __device__ inline TcSmem tc_smem(int npad_max, int raw_floats, int n_tab) {
   TcSmem s{};
   s.tab = 0;
   const size_t tab_stage = (size_t)kChunkSteps * npad_max * 2 * kStepK * 4;
-  s.data = s.tab + kNTab * tab_stage;
+  s.data = s.tab + n_tab * tab_stage;
   const size_t data_stage = (size_t)kChunkSteps * 2 * kDataStepFloats * 4;
   s.raw = s.data + kNData * data_stage;
   s.stage = s.raw + 2 * (size_t)raw_floats * 4;
-  s.bars = s.stage + 4 * 32 * 33 * 4;
-  s.total = s.bars + 32 * 8 + 16;
+  s.bars = s.stage + (kConv / 32) * 32 * 33 * 4;
+  s.total = s.bars + 32 * 8;
   return s;
 }
 
@@ -304,7 +308,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ unsigned char smem_raw_base[];
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw_base) + 127) & ~(uintptr_t)127);
-  const TcSmem L = tc_smem(g.npad_max, g.raw_floats);
+  const TcSmem L = tc_smem(g.npad_max, g.raw_floats, g.n_tab);
+  const int NT = g.n_tab;
   const size_t tab_stage_floats = (size_t)kChunkSteps * g.npad_max * 2 * kStepK;
   const size_t data_stage_floats = (size_t)kChunkSteps * 2 * kDataStepFloats;
   float* tab = reinterpret_cast<float*>(base + L.tab);
@@ -314,15 +319,15 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + L.bars);
   uint64_t* raw_full = bars;          // [2]
   uint64_t* raw_empty = bars + 2;     // [2]
-  uint64_t* tab_full = bars + 4;      // [kNTab]
-  uint64_t* tab_empty = bars + 6;     // [kNTab]
-  uint64_t* dat_full = bars + 8;      // [kNData]
-  uint64_t* dat_empty = bars + 10;    // [kNData]
-  uint64_t* acc_full = bars + 12;     // [2]
-  uint64_t* acc_empty = bars + 14;    // [2]
-  uint64_t* drain = bars + 16;        // MMA drain after an abort
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 17);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 18);
+  uint64_t* tab_full = bars + 4;      // [kMaxTab]
+  uint64_t* tab_empty = bars + 12;    // [kMaxTab]
+  uint64_t* dat_full = bars + 20;     // [kNData]
+  uint64_t* dat_empty = bars + 22;    // [kNData]
+  uint64_t* acc_full = bars + 24;     // [2]
+  uint64_t* acc_empty = bars + 26;    // [2]
+  uint64_t* drain = bars + 28;        // MMA drain after an abort
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 29);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 30);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp == 0) {
@@ -337,7 +342,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(acc_full + i, 1);
       mbar_init(acc_empty + i, kConv);
     }
-    for (int i = 0; i < kNTab; ++i) {
+    for (int i = 0; i < NT; ++i) {
       mbar_init(tab_full + i, 1);
       mbar_init(tab_empty + i, 1);
     }
@@ -415,20 +420,27 @@ __global__ void __launch_bounds__(kThreads, 1)
           } else {
             // per field and plane: the modes of m, from the 16-byte boundary
             // at or below the first coefficient
-            const uint32_t bytes = (uint32_t)(S::NR * np * g.box * 4);
-            mbar_expect_tx(raw_full + rb, bytes);
             const int w0 = first_mode(m, ntp1);
-            for (int f = 0; f < S::NR; ++f)
-              for (int p = 0; p < np; ++p) {
-                const int x = ((p0 + p) * d.NRSP + 2 * w0) & ~3;
-                tma_load_1d(r + ((size_t)f * S::TP + p) * g.raw_row, &maps.in[f], x, raw_full + rb);
-              }
+            if (g.raw2d) {
+              // one (box x TP planes) tile per field: every plane's row starts
+              // at the same 16-byte boundary below its first coefficient
+              mbar_expect_tx(raw_full + rb, (uint32_t)(S::NR * S::TP * g.box * 4));
+              for (int f = 0; f < S::NR; ++f)
+                tma_load_2d(r + (size_t)f * S::TP * g.raw_row, &maps.in[f], (2 * w0) & ~3, p0, raw_full + rb);
+            } else {
+              mbar_expect_tx(raw_full + rb, (uint32_t)(S::NR * np * g.box * 4));
+              for (int f = 0; f < S::NR; ++f)
+                for (int p = 0; p < np; ++p) {
+                  const int x = ((p0 + p) * d.NRSP + 2 * w0) & ~3;
+                  tma_load_1d(r + ((size_t)f * S::TP + p) * g.raw_row, &maps.in[f], x, raw_full + rb);
+                }
+            }
           }
           ++ri;
           const int per_unit = S::fwd ? S::NA : nchunks;
           for (int c = 0; c < per_unit && ok; ++c, ++chunk) {
-            const int ts = ti % kNTab;
-            if (!(ok = wait(tab_empty + ts, ((ti / kNTab) & 1) ^ 1))) break;
+            const int ts = ti % NT;
+            if (!(ok = wait(tab_empty + ts, ((ti / NT) & 1) ^ 1))) break;
             const int s0 = chunk * kChunkSteps, ns = min(kChunkSteps, total_steps - s0);
             const uint32_t bytes = (uint32_t)ns * npad * 2 * kStepK * 4;
             mbar_expect_tx(tab_full + ts, bytes);
@@ -443,13 +455,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (uint32_t k = (ri > 2 ? ri - 2 : 0); k < ri; ++k)
           for (long i = 0; i < kWaitLimit && !mbar_try_wait(raw_full + (k & 1), (k >> 1) & 1); ++i) {
           }
-        for (uint32_t k = (ti > kNTab ? ti - kNTab : 0); k < ti; ++k)
-          for (long i = 0; i < kWaitLimit && !mbar_try_wait(tab_full + k % kNTab, (k / kNTab) & 1); ++i) {
+        for (uint32_t k = (ti > (uint32_t)NT ? ti - NT : 0); k < ti; ++k)
+          for (long i = 0; i < kWaitLimit && !mbar_try_wait(tab_full + k % NT, (k / NT) & 1); ++i) {
           }
       }
     }
     __syncwarp();
-  } else if (warp == 5) {
+  } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------- MMA issuer
     if (lane == 0) {
       uint32_t ti = 0, di = 0, ii = 0;
@@ -464,8 +476,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t dtm = tmem + (uint32_t)(ab * 128);
         const uint32_t id = idesc(npad);
         for (int c = 0; c < nchunks && ok; ++c) {
-          const int ts = ti % kNTab, ds = di % kNData;
-          if (!(ok = wait(tab_full + ts, (ti / kNTab) & 1))) break;
+          const int ts = ti % NT, ds = di % kNData;
+          if (!(ok = wait(tab_full + ts, (ti / NT) & 1))) break;
           if (!(ok = wait(dat_full + ds, (di / kNData) & 1))) break;
           fence_after_sync();
           const int ns = min(kChunkSteps, total_steps - c * kChunkSteps);
@@ -500,16 +512,17 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncwarp();
   } else {
     // ------------------------------------------ converters and epilogue
-    const int t = threadIdx.x - 32;  // 0..127
+    const int t = threadIdx.x - 32;  // 0..255
     const int q = warp & 3;          // TMEM lane quarter of this warp
+    const int half = (warp - 1) >> 2;  // the two warps of a quarter drain alternate 32-column slices
     // Element idx of a K step (storage order) is (row, k) with row =
     // (idx >> 6) * 8 + ((idx >> 2) & 7) and k = ((idx >> 5) & 1) * 4 +
-    // (idx & 3) (the inverse of kmajor_offset); for idx = t + 128 i that is
-    // row = row_of_thread + 16 i and a fixed k and row % NC.
+    // (idx & 3) (the inverse of kmajor_offset); for idx = t + 256 i that is
+    // row = row_of_thread + 32 i and a fixed k and row % NC.
     const int row_of_thread = 8 * (t >> 6) + ((t >> 2) & 7);
     const int k_of_thread = ((t >> 5) & 1) * 4 + (t & 3);
     const int c_of_thread = row_of_thread % S::NC;
-    float* st = stage + (size_t)q * 32 * 33;
+    float* st = stage + (size_t)(warp - 1) * 32 * 33;
     uint32_t ri = 0, di = 0, ii = 0;
     bool ok = true;
     int prev_item = -1;
@@ -525,7 +538,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int ncols = S::fwd ? ntp1 - m : d.NLAT;
       const size_t out_base = S::fwd ? (size_t)2 * w0 : (size_t)2 * m * d.NLAT;
       constexpr int PPW = 32 / S::NC;  // planes per warp
-      for (int c0 = 0; c0 < ncols; c0 += 32) {
+      for (int c0 = 32 * half; c0 < ncols; c0 += 64) {
         float v[32];
         tmem_load32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * 128 + c0), v);
 #pragma unroll
@@ -586,7 +599,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
             for (int i = 0; i < kDataStepFloats / kConv; ++i) {
               const int idx = t + kConv * i;
-              const int p = (row_of_thread + 16 * i) / S::NC;
+              const int p = (row_of_thread + 32 * i) / S::NC;
               float x = 0.f;
               if (live && p < np) {
                 if (S::fwd) {
@@ -595,7 +608,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                   const float north = rn[2 * li + tm.comp], south = rs[2 * (15 - li) + tm.comp];
                   x = tm.sign * (half == 0 ? north + south : north - south);
                 } else {
-                  const int off = ((p0 + p) * d.NRSP + 2 * w0) & 3;
+                  const int off = ((g.raw2d ? 0 : (p0 + p) * d.NRSP) + 2 * w0) & 3;
                   float v = r[((size_t)tm.field * S::TP + p) * g.raw_row + off + 2 * tmode + tm.comp];
                   if (KIND == DV2UV && tm.field == 1 && tm.comp == 0 && m == 0 && tmode == 1) v -= g.plavor;
                   x = tm.sign * v;
@@ -661,13 +674,14 @@ CUtensorMap map_1d(const float* field, size_t floats, int box) {
   return map;
 }
 
-// 2-D map over a Fourier field [planes][NLAT * NFC], boxes of 32 floats x tp planes.
-CUtensorMap map_2d(const float* field, int plane_floats, int planes, int tp) {
+// 2-D map over a field of `planes` planes of `plane_floats` floats, boxes of
+// `box` floats x tp planes.
+CUtensorMap map_2d(const float* field, int plane_floats, int planes, int box, int tp) {
   CUtensorMap map;
   const cuuint64_t dim[2] = {(cuuint64_t)plane_floats, (cuuint64_t)planes};
   const cuuint64_t stride[1] = {(cuuint64_t)plane_floats * 4};
-  const cuuint32_t bdim[2] = {32, (cuuint32_t)tp}, estride[2] = {1, 1};
-  if ((reinterpret_cast<uintptr_t>(field) & 15) || stride[0] % 16)
+  const cuuint32_t bdim[2] = {(cuuint32_t)box, (cuuint32_t)tp}, estride[2] = {1, 1};
+  if ((reinterpret_cast<uintptr_t>(field) & 15) || stride[0] % 16 || (box * 4) % 16 || box > 256 || tp > 256)
     throw std::runtime_error("tensor-core transform: bad 2-D map");
   const CUresult r = encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(field), dim, stride, bdim,
                                estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -695,16 +709,23 @@ TcGeom geometry(const Dims& d, int planes, float plavor) {
   g.items = d.NTP1 * g.tiles;
   g.npad_max = S::fwd ? (d.NTP1 + 15) / 16 * 16 : d.NLAT;
   g.box = (2 * d.NTP1 + 4 + 3) / 4 * 4;
-  g.raw_row = (g.box + 31) / 32 * 32;
+  // a 2-D box lands as TP rows of `box` floats; per-plane 1-D boxes land on
+  // 128-byte row starts
+  g.raw2d = !S::fwd && (d.NRSP * 4) % 16 == 0 ? 1 : 0;
+  g.raw_row = g.raw2d ? g.box : (g.box + 31) / 32 * 32;
   g.raw_floats = S::fwd ? S::NR * 2 * S::TP * 32 : S::NR * S::TP * g.raw_row;
+  g.raw_floats = (g.raw_floats + 31) / 32 * 32;
   g.out_plane = S::fwd ? d.NRSP : d.NLAT * d.NFC;
   g.plavor = plavor;
+  // as many table stages as shared memory holds
+  g.n_tab = 2;
+  while (g.n_tab < kMaxTab && tc_smem(g.npad_max, g.raw_floats, g.n_tab + 1).total + 128 <= kTcSmemLimit) ++g.n_tab;
   return g;
 }
 
 template <int KIND>
 size_t smem_bytes(const TcGeom& g) {
-  return tc_smem(g.npad_max, g.raw_floats).total + 128;
+  return tc_smem(g.npad_max, g.raw_floats, g.n_tab).total + 128;
 }
 
 template <int KIND>
@@ -715,14 +736,16 @@ void launch(const Model& m, const float* const* in, float* out0, float* out1, in
   const TcGeom g = geometry<KIND>(d, planes, plavor);
   TcMaps maps{};
   for (int f = 0; f < S::NR; ++f)
-    maps.in[f] = S::fwd ? map_2d(in[f], d.NLAT * d.NFC, planes, S::TP) : map_1d(in[f], (size_t)planes * d.NRSP, g.box);
+    maps.in[f] = S::fwd    ? map_2d(in[f], d.NLAT * d.NFC, planes, 32, S::TP)
+                 : g.raw2d ? map_2d(in[f], d.NRSP, planes, g.box, S::TP)
+                           : map_1d(in[f], (size_t)planes * d.NRSP, g.box);
   TcOut io{};
   io.out[0] = out0;
   io.out[1] = out1;
   io.images = m.sh.tc_img;
   io.at = m.sh.tc_at + (size_t)set * (d.NTP1 + 1);
   const size_t smem = smem_bytes<KIND>(g);
-  if (smem > 227 * 1024) throw std::runtime_error("tensor-core transform: shared memory over budget");
+  if (smem > kTcSmemLimit) throw std::runtime_error("tensor-core transform: shared memory over budget");
   const int grid = std::min(g.items, sm_count());
   k_tc_legendre<KIND><<<grid, kThreads, smem, st>>>(maps, io, g, m.fault, d);
 }

@@ -458,16 +458,16 @@ __global__ void __launch_bounds__(kBlock, 5) k_lwr_radstep(Model m, const Planet
   auto clear_sky = [&](float sumwv, float sumo3, float sumco2) {
     const float LOG10_2 = 0.30102999566398120f, LN_2 = 0.69314718055994531f;
     const bool wv1 = sumwv <= 0.01f, wv2 = sumwv <= 2.f, co2 = sumco2 <= 1.f, o3 = sumo3 <= 0.01f;
-    const float lah = log2f(sumwv + (wv1 ? 3.59e-5f : 0.01f));
-    const float lth = log2f(wv2 ? sumwv + 0.0286f : sumwv - 0.6931f);
-    const float lco = log2f(co2 ? sumco2 + 0.01022f : sumco2);
-    const float lo3 = log2f(o3 ? sumo3 + 7.0e-5f : sumo3);
-    float ah2o = wv1 ? 0.846f * exp2f(0.243f * lah) - K.ZH2O0A : 0.24f * (LOG10_2 * lah) + K.ZAH2OC;
+    const float lah = fit_log2(sumwv + (wv1 ? 3.59e-5f : 0.01f));
+    const float lth = fit_log2(wv2 ? sumwv + 0.0286f : sumwv - 0.6931f);
+    const float lco = fit_log2(co2 ? sumco2 + 0.01022f : sumco2);
+    const float lo3 = fit_log2(o3 ? sumo3 + 7.0e-5f : sumo3);
+    float ah2o = wv1 ? 0.846f * fit_exp2(0.243f * lah) - K.ZH2O0A : 0.24f * (LOG10_2 * lah) + K.ZAH2OC;
     if (K.TH2OC > 0.f) ah2o = fminf(ah2o + (1.f - expf(-K.TH2OC * sumwv)), 1.f);
-    const float aco2 = co2 ? 0.0676f * exp2f(0.421f * lco) - K.ZCO20 : 0.0546f * (LOG10_2 * lco) + K.ZACO2C;
-    const float th2o = wv2 ? 1.f - (0.832f * exp2f(0.26f * lth) - K.ZH2O0)
+    const float aco2 = co2 ? 0.0676f * fit_exp2(0.421f * lco) - K.ZCO20 : 0.0546f * (LOG10_2 * lco) + K.ZACO2C;
+    const float th2o = wv2 ? 1.f - (0.832f * fit_exp2(0.26f * lth) - K.ZH2O0)
                            : fmaxf(0.f, K.ZTH2OC - 0.1196f * (LN_2 * lth));
-    const float ao3 = o3 ? 0.209f * exp2f(0.436f * lo3) - K.ZAO30 : 0.0212f * (LOG10_2 * lo3) + K.ZAO3C;
+    const float ao3 = o3 ? 0.209f * fit_exp2(0.436f * lo3) - K.ZAO30 : 0.0212f * (LOG10_2 * lo3) + K.ZAO3C;
     return fminf(1.f - ZERO, fmaxf(ZERO, 1.f - ah2o - ao3 - aco2 * th2o));
   };
   float dftu[NL + 1], tausf[NL];

@@ -80,10 +80,40 @@ __device__ __forceinline__ float sat_divided(const PlanetConst& K, float t, floa
   const float q = sat_capped(K, t, p);
   return q / (1.f - K.MOIST * q);
 }
+// The longwave band fits' base-2 logarithm and power: CUDA's accurate
+// log2f and exp2f, or, built with EXOGCM_LWR_FAST_LOG2 / EXOGCM_LWR_FAST_EXP2,
+// the special-function unit's lg2.approx / ex2.approx instructions.
+__device__ __forceinline__ float fit_log2(float x) {
+#ifdef EXOGCM_LWR_FAST_LOG2
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+#else
+  return log2f(x);
+#endif
+}
+__device__ __forceinline__ float fit_exp2(float x) {
+#ifdef EXOGCM_LWR_FAST_EXP2
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+#else
+  return exp2f(x);
+#endif
+}
 // x^y for x >= 0 with 0^y = 0: precise_pow (src/model/shared/gpu/math/wgsl/
 // precise.wgsl:100-103) is exp(y * log(x)); here exp2(y * log2(x)) with
 // CUDA's own exp2f and log2f.
-__device__ __forceinline__ float fpow(float x, float y) { return x == 0.f ? 0.f : exp2f(y * log2f(x)); }
+__device__ __forceinline__ float fpow(float x, float y) {
+#ifdef EXOGCM_FAST_POW
+  float l, r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"(x));
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y * l));
+  return x == 0.f ? 0.f : r;
+#else
+  return x == 0.f ? 0.f : exp2f(y * log2f(x));
+#endif
+}
 // x^n by binary exponentiation, as libgcc's __powisf2 computes x**n.
 __device__ __forceinline__ float powi(float x, int n) {
   float base = x;
@@ -107,21 +137,22 @@ inline unsigned nblocks(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 // Implicit vertical diffusion (physics/diffusion/wgsl/implicit.wgsl): the
 // tridiagonal solve of one column, for a quantity and for potential
-// temperature; each translation unit divides with its own precision flags.
+// temperature, with IEEE divisions (the tendencies are small differences of
+// the diffused and the old profiles).
 template <int NL>
 __device__ __forceinline__ void diffuse(const float* ds, float* x, const float* k) {
   float ebs[NL];
   const float ds0 = ds[0];
-  ebs[0] = k[0] / (ds0 + k[0]);
-  x[0] = ds0 * x[0] / (ds0 + k[0]);
+  ebs[0] = __fdiv_rn(k[0], ds0 + k[0]);
+  x[0] = __fdiv_rn(ds0 * x[0], ds0 + k[0]);
 #pragma unroll
   for (int l = 1; l < NL - 1; ++l) {
     const float den = ds[l] + k[l] + k[l - 1] * (1.f - ebs[l - 1]);
-    ebs[l] = k[l] / den;
-    x[l] = (x[l] * ds[l] + k[l - 1] * x[l - 1]) / den;
+    ebs[l] = __fdiv_rn(k[l], den);
+    x[l] = __fdiv_rn(x[l] * ds[l] + k[l - 1] * x[l - 1], den);
   }
   const float dsn = ds[NL - 1];
-  x[NL - 1] = (x[NL - 1] * dsn + k[NL - 2] * x[NL - 2]) / (dsn + k[NL - 2] * (1.f - ebs[NL - 2]));
+  x[NL - 1] = __fdiv_rn(x[NL - 1] * dsn + k[NL - 2] * x[NL - 2], dsn + k[NL - 2] * (1.f - ebs[NL - 2]));
 #pragma unroll
   for (int l = NL - 2; l >= 0; --l) x[l] = x[l] + ebs[l] * x[l + 1];
 }
@@ -130,20 +161,20 @@ template <int NL>
 __device__ __forceinline__ void diffuse_potential(const float* ds, float* x, const float* k, const float* skap) {
   float ebs[NL];
   const float ds0 = ds[0];
-  ebs[0] = k[0] / (ds0 + k[0] / skap[0]);
-  x[0] = ds0 * x[0] / (ds0 + k[0] / skap[0]);
+  ebs[0] = __fdiv_rn(k[0], ds0 + __fdiv_rn(k[0], skap[0]));
+  x[0] = __fdiv_rn(ds0 * x[0], ds0 + __fdiv_rn(k[0], skap[0]));
 #pragma unroll
   for (int l = 1; l < NL - 1; ++l) {
-    const float den = ds[l] + (k[l] + k[l - 1] * (1.f - ebs[l - 1] / skap[l - 1])) / skap[l];
-    ebs[l] = k[l] / den;
-    x[l] = (x[l] * ds[l] + k[l - 1] / skap[l - 1] * x[l - 1]) / den;
+    const float den = ds[l] + __fdiv_rn(k[l] + k[l - 1] * (1.f - __fdiv_rn(ebs[l - 1], skap[l - 1])), skap[l]);
+    ebs[l] = __fdiv_rn(k[l], den);
+    x[l] = __fdiv_rn(x[l] * ds[l] + __fdiv_rn(k[l - 1], skap[l - 1]) * x[l - 1], den);
   }
   const int last = NL - 1;
   const float dsn = ds[last];
-  x[last] = (x[last] * dsn + k[NL - 2] * x[NL - 2] / skap[NL - 2]) /
-            (dsn + k[NL - 2] / skap[last] * (1.f - ebs[NL - 2] / skap[NL - 2]));
+  x[last] = __fdiv_rn(x[last] * dsn + __fdiv_rn(k[NL - 2] * x[NL - 2], skap[NL - 2]),
+                      dsn + __fdiv_rn(k[NL - 2], skap[last]) * (1.f - __fdiv_rn(ebs[NL - 2], skap[NL - 2])));
 #pragma unroll
-  for (int l = NL - 2; l >= 0; --l) x[l] = x[l] + ebs[l] * x[l + 1] / skap[l + 1];
+  for (int l = NL - 2; l >= 0; --l) x[l] = x[l] + __fdiv_rn(ebs[l] * x[l + 1], skap[l + 1]);
 }
 
 

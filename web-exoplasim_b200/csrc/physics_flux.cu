@@ -1,12 +1,13 @@
 // The fixer's apply step, the surface fluxes and vertical diffusion, and the
-// solar angle and ozone columns, compiled with IEEE division and square root
-// (the rest of the column physics divides to 2 ulp): vdiff's humidity
-// tendency is a small difference of two implicitly diffused profiles, and
-// with approximate division more of its points left the reference's V3
-// tolerance than a sequential-f32 build's. Arithmetic follows
-// physics/fixer/wgsl/apply.wgsl, physics/surface-flux/wgsl/{surflx,vdiff}.wgsl,
-// physics/diffusion/wgsl/implicit.wgsl and physics/radiation/wgsl/
-// {solang,mko3}.wgsl; the full step runs the four as one fused column kernel.
+// solar angle and ozone columns. vdiff's tendencies are small differences of
+// two implicitly diffused profiles, so its tridiagonal solves
+// (physics_common.cuh) and the tendency quotients divide to IEEE precision
+// (__fdiv_rn); with 2-ulp quotients there, more points of its humidity
+// tendency left the reference's V3 tolerance than a sequential-f32 build's.
+// Arithmetic follows physics/fixer/wgsl/apply.wgsl, physics/surface-flux/
+// wgsl/{surflx,vdiff}.wgsl, physics/diffusion/wgsl/implicit.wgsl and
+// physics/radiation/wgsl/{solang,mko3}.wgsl; a full step runs the four as
+// one fused column kernel, stage replay as four launches.
 #include "physics_common.cuh"
 
 namespace exogcm {
@@ -212,8 +213,8 @@ __device__ __forceinline__ void b_vdiff(const Model& m, const PlanetConst* __res
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SN + c;
-    F.dudt[at] = dudt[l] + (zun[l] - zu[l]) / D2;
-    F.dvdt[at] = dvdt[l] + (zvn[l] - zv[l]) / D2;
+    F.dudt[at] = dudt[l] + __fdiv_rn(zun[l] - zu[l], D2);
+    F.dvdt[at] = dvdt[l] + __fdiv_rn(zvn[l] - zv[l], D2);
   }
   if (K.NDHEAT != 0.f) {
     float zke[NL], zken[NL];
@@ -232,7 +233,7 @@ __device__ __forceinline__ void b_vdiff(const Model& m, const PlanetConst* __res
   for (int l = 0; l < NL; ++l) zqn[l] = zq[l];
   diffuse<NL>(ds, zqn, kh);
 #pragma unroll
-  for (int l = 0; l < NL; ++l) F.dqdt[l * SN + c] = dqdt[l] + (zqn[l] - zq[l]) / D2;
+  for (int l = 0; l < NL; ++l) F.dqdt[l * SN + c] = dqdt[l] + __fdiv_rn(zqn[l] - zq[l], D2);
 #pragma unroll
   for (int l = 0; l < NL - 1; ++l) kh[l] = kh[l] * zskaph[l];
   float ztn[NL];
@@ -240,7 +241,7 @@ __device__ __forceinline__ void b_vdiff(const Model& m, const PlanetConst* __res
   for (int l = 0; l < NL; ++l) ztn[l] = zt[l];
   diffuse_potential<NL>(ds, ztn, kh, zskap);
 #pragma unroll
-  for (int l = 0; l < NL; ++l) F.dtdt[l * SN + c] = dtdt[l] + (ztn[l] - zt[l]) / D2;
+  for (int l = 0; l < NL; ++l) F.dtdt[l * SN + c] = dtdt[l] + __fdiv_rn(ztn[l] - zt[l], D2);
 }
 template <int NL>
 __global__ void __launch_bounds__(kBlock, 3) k_vdiff(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
