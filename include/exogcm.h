@@ -161,6 +161,30 @@ int exogcm_wait(exogcm_engine* engine);
  * (runner/webgpu/gcm.worker.ts:215-346). */
 int exogcm_group_step(exogcm_engine** engines, int count, const int* steps, int publish_every, float* ms);
 
+/* Per-planet global budgets in FP64, computed on the device on every step a
+ * slot publishes (the quantities of the reference's yearly energy balance,
+ * averages/index.ts:31-49 and balance/index.ts, plus the mass and water
+ * budgets): Gaussian-weighted global means of [0] surface pressure (Pa, the
+ * atmosphere's mass), [1] top-of-atmosphere net radiation (W/m^2), [2]
+ * surface net heat flux (W/m^2), [3] surface temperature (K), [4]
+ * precipitation (m/s), [5] evaporation (m/s), [6] column water vapour
+ * (kg/m^2), [7] the weights' mean (1). `last` (8 doubles, may be NULL) gets
+ * the last publishing step's values, `mean` (may be NULL) the mean over the
+ * `*samples` publishing steps since configure or the last reset; `reset`
+ * clears the means. */
+int exogcm_budgets(exogcm_engine* engine, int slot, double* last, double* mean, long* samples, int reset);
+
+/* Monthly means on the device (averages/index.ts:85-103 `add`/`close`):
+ * with averages enabled, every publishing step adds the slot's snapshot
+ * fields to FP64 running sums (snapshot planes x slots x NHOR doubles of
+ * device memory). exogcm_averages_read returns, per slot, their mean over
+ * the `*samples` publishing steps since the last reset as floats
+ * [plane][point] (count = snapshot planes x NHOR; `mean` may be NULL), and
+ * `reset` starts the next month. Enabling or disabling recaptures the
+ * engine's batch graphs. */
+int exogcm_averages_enable(exogcm_engine* engine, int enable);
+int exogcm_averages_read(exogcm_engine* engine, int slot, float* mean, size_t count, long* samples, int reset);
+
 /* Snapshot of a slot published during the last exogcm_step (the 101/76
  * fields of snapshot/index.ts, each NHOR values): returns the step it was
  * taken at in *step, or -1 when the slot did not publish. `values` may be

@@ -12,11 +12,15 @@ long_runs.npz -- the north star's configs 2 and 3 against the FP64 oracle:
   its RMS difference from f64 at most twice the f32 run's.
 
 climatology_t21.npz -- a one-year T21 L10 ensemble: planet seed 21 with
-  initial noise seeds 0..5, each run for 360 days by the FP64 oracle; the
-  daily global means of surface temperature, 2 m air temperature,
-  precipitation, total cloud cover, outgoing longwave, top-of-atmosphere net
-  flux and surface pressure (the fields scripts/exoplasim-wasm/
-  compare-climate.mjs:10-11 compares) are stored per seed.
+  initial noise seeds 0..5, each run for 360 days by the FP64 oracle
+  ("daily") and by the sequential-f32 oracle ("daily_f32"); the daily global
+  means of surface temperature, 2 m air temperature, precipitation, total
+  cloud cover, outgoing longwave, top-of-atmosphere net flux and surface
+  pressure (the fields scripts/exoplasim-wasm/compare-climate.mjs:10-11
+  compares) are stored per seed.
+
+  python make_long_runs.py            # everything
+  python make_long_runs.py f32-climate  # adds daily_f32 to an existing climatology_t21.npz
 """
 import importlib
 import multiprocessing as mp
@@ -76,11 +80,11 @@ def global_means(o, nlat):
     return np.array([np.sum(f * w) / np.sum(w) for f in fields])
 
 
-def climate_run(noise_seed):
+def climate_run(noise_seed, precision=64):
     import oracle
     planets = importlib.import_module("web-exoplasim_b200.planets")
     p = planets.make_planet(21, truncation=21, levels=10, noise_seed=noise_seed)
-    o = oracle.Oracle(rounded_model(p), precision=64)
+    o = oracle.Oracle(rounded_model(p), precision=precision)
     o.startup()
     daily = []
     for _ in range(CLIMATE_DAYS):
@@ -89,7 +93,23 @@ def climate_run(noise_seed):
     return noise_seed, np.array(daily)
 
 
+def climate_run_f32(noise_seed):
+    return climate_run(noise_seed, precision=32)
+
+
+def add_f32_climate():
+    path = os.path.join(HERE, "climatology_t21.npz")
+    with mp.get_context("spawn").Pool(min(8, os.cpu_count() or 1)) as pool:
+        clim32 = dict(pool.map(climate_run_f32, CLIMATE_SEEDS))
+    old = dict(np.load(path))
+    old["daily_f32"] = np.stack([clim32[s] for s in CLIMATE_SEEDS])
+    np.savez_compressed(path, **old)
+
+
 def main():
+    if sys.argv[1:] == ["f32-climate"]:
+        add_f32_climate()
+        return
     ctx = mp.get_context("spawn")
     with ctx.Pool(min(8, os.cpu_count() or 1)) as pool:
         long_jobs = pool.map_async(long_run, [(n, prec) for n in LONG_RUNS for prec in (64, 32)])
@@ -100,8 +120,10 @@ def main():
                 out[f"{name}_f{precision}_{k}"] = v
         np.savez_compressed(os.path.join(HERE, "long_runs.npz"), **out)
         clim = dict(climate_jobs.get())
+        clim32 = dict(pool.map(climate_run_f32, CLIMATE_SEEDS))
         np.savez_compressed(os.path.join(HERE, "climatology_t21.npz"),
                             daily=np.stack([clim[s] for s in CLIMATE_SEEDS]),
+                            daily_f32=np.stack([clim32[s] for s in CLIMATE_SEEDS]),
                             seeds=np.array(CLIMATE_SEEDS), fields=np.array(CLIMATE_FIELDS))
 
 

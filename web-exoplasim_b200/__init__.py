@@ -79,6 +79,10 @@ SIGNATURES = {
                                          _FP]),
     "exogcm_snapshots_begin": (ctypes.c_int, [_VP, _FP, ctypes.c_size_t]),
     "exogcm_snapshots_wait": (ctypes.c_int, [_VP]),
+    "exogcm_budgets": (ctypes.c_int, [_VP, ctypes.c_int, _DP, _DP, ctypes.POINTER(ctypes.c_long), ctypes.c_int]),
+    "exogcm_averages_enable": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "exogcm_averages_read": (ctypes.c_int, [_VP, ctypes.c_int, _FP, ctypes.c_size_t, ctypes.POINTER(ctypes.c_long),
+                                            ctypes.c_int]),
     "exogcm_read_snapshot": (ctypes.c_int, [_VP, ctypes.c_int, _FP, ctypes.c_size_t,
                                             ctypes.POINTER(ctypes.c_long)]),
     "exogcm_set_stop": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_long]),
@@ -250,6 +254,29 @@ class Engine:
 
     def wait(self) -> None:
         _check(_lib.exogcm_wait(self.h))
+
+    BUDGETS = ("surface_pressure", "toa_net", "surface_net", "surface_temperature", "precipitation", "evaporation",
+               "water_vapour", "weight")
+
+    def budgets(self, slot: int, reset: bool = False) -> dict:
+        """The slot's FP64 global budgets: {'last': {...}, 'mean': {...}, 'samples': n} (exogcm_budgets)."""
+        last = (ctypes.c_double * 8)()
+        mean = (ctypes.c_double * 8)()
+        n = ctypes.c_long()
+        _check(_lib.exogcm_budgets(self.h, slot, last, mean, ctypes.byref(n), 1 if reset else 0))
+        return {"last": dict(zip(self.BUDGETS, last[:])), "mean": dict(zip(self.BUDGETS, mean[:])),
+                "samples": n.value}
+
+    def averages_enable(self, enable: bool = True) -> None:
+        _check(_lib.exogcm_averages_enable(self.h, 1 if enable else 0))
+
+    def averages_read(self, slot: int, reset: bool = False):
+        """(mean snapshot [planes][NHOR] float32, samples) since the last reset."""
+        out = np.zeros(self.field_size("snapshot"), dtype=np.float32)
+        n = ctypes.c_long()
+        _check(_lib.exogcm_averages_read(self.h, slot, out.ctypes.data_as(_FP), out.size, ctypes.byref(n),
+                                         1 if reset else 0))
+        return out.reshape(-1, self.nhor), n.value
 
     def run_stage(self, stage: str) -> None:
         _check(_lib.exogcm_run_stage(self.h, stage.encode()))

@@ -24,6 +24,10 @@
 
 namespace exogcm {
 
+// Per-planet global budgets (budget.cu): quantities per published step.
+constexpr int kBudgetQuantities = 8;
+constexpr int kBudgetStride = 2 * kBudgetQuantities + 2;  // last[8], sums[8], samples, averaged samples
+
 constexpr int NLSOIL = 5;  // landmod's soil layers
 constexpr int MONTHS = 14; // climatology months with December before and January after
 
@@ -97,6 +101,7 @@ struct SharedTabs {
   const float* qu;
   const float* qv;
   const float* zgw;    // Gaussian weight per point [NHOR]
+  const double* wlat;  // Gaussian weight per latitude in FP64 [NLAT] (the budgets' global means)
   const float* rcsq;   // 1 / cos^2(latitude) per point [NHOR]
   const float* sid;    // sin(latitude) [NLAT]
   const float* cola;   // cos(latitude) [NLAT]
@@ -139,6 +144,8 @@ struct Model {
   const PlanetConst* pc;     // [S]
   const StepParams* params;  // [S] for the step being run
   double* sums;              // FP64 per-slot reductions scratch [S][4]
+  double* budget;            // FP64 per-slot budgets [S][kBudgetStride]: last values, running sums, samples
+  double* avg;               // FP64 running sums of the published snapshot fields, or null (averages off)
   int* flags;                // per-slot status flags [S]
   int* fault;                // nonzero after a kernel gave up a bounded wait
   int mode;                  // 0 plain path, 1 optimized path (FFTs, latitude-pair Legendre, m-major Fourier),

@@ -117,6 +117,9 @@ struct exogcm_engine {
   Batch batch[kInFlight];
   std::deque<int> pending;
   double* sums = nullptr;
+  double* budget = nullptr;  // [S][kBudgetStride] FP64 budgets (budget.cu)
+  double* avg = nullptr;     // FP64 running sums of the snapshot field, when averages are enabled
+  double* wlat64 = nullptr;  // FP64 Gaussian weights [NLAT]
   int* flags = nullptr;
   int* fault = nullptr;  // device word: a kernel gave up a bounded wait
   // overlapped snapshot copies (exogcm_snapshots_begin/wait)
@@ -140,6 +143,8 @@ struct exogcm_engine {
     m.pc = pc;
     m.params = params + (size_t)k * d.S;
     m.sums = sums;
+    m.budget = budget;
+    m.avg = avg;
     m.flags = flags;
     m.fault = fault;
     m.mode = mode;
@@ -344,6 +349,9 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
   e->sh.qu = b + q[6];
   e->sh.qv = b + q[7];
   e->sh.zgw = b + izgw;
+  check(cudaMalloc(&e->wlat64, d.NLAT * sizeof(double)), "FP64 weights");
+  check(cudaMemcpy(e->wlat64, s.weights.data(), d.NLAT * sizeof(double), cudaMemcpyHostToDevice), "FP64 weights");
+  e->sh.wlat = e->wlat64;
   e->sh.rcsq = b + ircsq;
   e->sh.sid = b + isid;
   e->sh.cola = b + icola;
@@ -471,9 +479,9 @@ void run_stage(const Model& m, const std::string& s, cudaStream_t st) {
 }
 
 // master's step order (stepper/index.ts:148-161).
-// The physics runs as fused column kernels between the per-planet
-// reductions (physics.cu); exogcm_run_stage runs the same routines stage by
-// stage.
+// The physics between the per-planet reductions runs as column kernels,
+// fused where that measured faster (physics.cu); exogcm_run_stage runs the
+// same routines stage by stage, unfused.
 void full_step(const Model& m, cudaStream_t st) {
   stage_gridpointa(m, st);
   dyn_spectrala(m, st);
@@ -484,6 +492,7 @@ void full_step(const Model& m, cudaStream_t st) {
   stage_physics_out(m, st);
   stage_spectrald(m, st);
   phy_pack(m, st);
+  phy_budget(m, m.d.P, st);
 }
 
 // The host values of one slot's next step; advances the slot's counters when
@@ -835,6 +844,8 @@ int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine
       check(cudaMallocHost(&b.fault_host, sizeof(int)), "pinned fault word");
       *b.fault_host = 0;
     }
+    check(cudaMalloc(&e->budget, (size_t)slots * kBudgetStride * sizeof(double)), "budgets");
+    check(cudaMemset(e->budget, 0, (size_t)slots * kBudgetStride * sizeof(double)), "budgets");
     check(cudaMalloc(&e->sums, (size_t)slots * 4 * sizeof(double)), "sums");
     check(cudaMemset(e->sums, 0, (size_t)slots * 4 * sizeof(double)), "sums");
     check(cudaMalloc(&e->flags, slots * sizeof(int)), "flags");
@@ -871,6 +882,9 @@ void exogcm_destroy(exogcm_engine* e) {
   cudaFree(e->params);
   cudaFreeHost(e->hparams);
   cudaFree(e->sums);
+  cudaFree(e->budget);
+  cudaFree(e->avg);
+  cudaFree(e->wlat64);
   cudaFree(e->flags);
   cudaFree(e->fault);
   if (e->ev0) cudaEventDestroy(e->ev0);
@@ -918,6 +932,11 @@ int exogcm_configure(exogcm_engine* e, int slot, const exogcm_planet* planet, co
     upload_slot_tables(e, slot, ps);
     int zero = 0;
     check(cudaMemcpy(e->flags + slot, &zero, sizeof(int), cudaMemcpyHostToDevice), "flags");
+    check(cudaMemset(e->budget + (size_t)slot * kBudgetStride, 0, kBudgetStride * sizeof(double)), "budgets");
+    if (e->avg)
+      for (int pl = 0; pl < e->d.P; ++pl)
+        check(cudaMemset(e->avg + ((size_t)pl * e->d.S + slot) * e->d.NHOR, 0, e->d.NHOR * sizeof(double)),
+              "averages");
     Slot& s = e->slots[slot];
     s = Slot{};
     s.active = true;
@@ -1120,6 +1139,86 @@ int exogcm_group_step(exogcm_engine** engines, int count, const int* steps, int 
       }
       engines[i]->last_ms = t;
     }
+  });
+}
+
+int exogcm_budgets(exogcm_engine* e, int slot, double* last, double* mean, long* samples, int reset) {
+  return guard([&] {
+    if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    retire_all(e);
+    check_slot(e, slot);
+    double b[kBudgetStride];
+    check(cudaMemcpy(b, e->budget + (size_t)slot * kBudgetStride, sizeof(b), cudaMemcpyDeviceToHost), "budgets");
+    const double n = b[2 * kBudgetQuantities];
+    for (int k = 0; k < kBudgetQuantities; ++k) {
+      if (last) last[k] = b[k];
+      if (mean) mean[k] = n > 0 ? b[kBudgetQuantities + k] / n : 0.0;
+    }
+    if (samples) *samples = (long)n;
+    if (reset) {
+      check(cudaMemset(e->budget + (size_t)slot * kBudgetStride + kBudgetQuantities, 0,
+                       (kBudgetQuantities + 1) * sizeof(double)),
+            "budgets");
+    }
+  });
+}
+
+int exogcm_averages_enable(exogcm_engine* e, int enable) {
+  return guard([&] {
+    if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    retire_all(e);
+    const size_t n = (size_t)e->d.P * e->d.S * e->d.NHOR;
+    if (enable && !e->avg) {
+      if (cudaMalloc(&e->avg, n * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        e->avg = nullptr;
+        throw Error(EXOGCM_ENOMEM, "device memory for the averages (" + std::to_string(n * 8 >> 20) + " MiB)");
+      }
+      check(cudaMemset(e->avg, 0, n * sizeof(double)), "averages");
+      for (int s = 0; s < e->d.S; ++s)
+        check(cudaMemset(e->budget + (size_t)s * kBudgetStride + 2 * kBudgetQuantities + 1, 0, sizeof(double)),
+              "averages");
+    } else if (!enable && e->avg) {
+      check(cudaStreamSynchronize(e->stream), "averages");
+      cudaFree(e->avg);
+      e->avg = nullptr;
+    } else {
+      return;
+    }
+    // The batch graphs hold the averages pointer: capture them again.
+    drop_group_graphs(e);
+    for (auto& g : e->graphs) cudaGraphExecDestroy(g.second);
+    for (auto& g : e->graph_templates) cudaGraphDestroy(g.second);
+    e->graphs.clear();
+    e->graph_templates.clear();
+  });
+}
+
+int exogcm_averages_read(exogcm_engine* e, int slot, float* mean, size_t count, long* samples, int reset) {
+  return guard([&] {
+    if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    retire_all(e);
+    check_slot(e, slot);
+    if (!e->avg) throw Error(EXOGCM_ESTATE, "averages are not enabled");
+    const size_t per = (size_t)e->d.P * e->d.NHOR;
+    if (mean && count != per) throw Error(EXOGCM_EINVAL, "averages buffer size mismatch (snapshot planes x points)");
+    double n = 0;
+    check(cudaMemcpy(&n, e->budget + (size_t)slot * kBudgetStride + 2 * kBudgetQuantities + 1, sizeof(double),
+                     cudaMemcpyDeviceToHost),
+          "averages");
+    if (samples) *samples = (long)n;
+    std::vector<double> row(e->d.NHOR);
+    for (int pl = 0; pl < e->d.P; ++pl) {
+      double* src = e->avg + ((size_t)pl * e->d.S + slot) * e->d.NHOR;
+      if (mean) {
+        check(cudaMemcpy(row.data(), src, e->d.NHOR * sizeof(double), cudaMemcpyDeviceToHost), "averages");
+        for (int h = 0; h < e->d.NHOR; ++h) mean[(size_t)pl * e->d.NHOR + h] = n > 0 ? (float)(row[h] / n) : 0.f;
+      }
+      if (reset) check(cudaMemset(src, 0, e->d.NHOR * sizeof(double)), "averages");
+    }
+    if (reset)
+      check(cudaMemset(e->budget + (size_t)slot * kBudgetStride + 2 * kBudgetQuantities + 1, 0, sizeof(double)),
+            "averages");
   });
 }
 
@@ -1443,6 +1542,11 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
           {"lwr_radstep", 7 * L + 4 + 4 * (L + 1) + 4 * L},  // t, q, o3, co2, clouds, sw flux, dtdt in; 4 fluxes + 4 rates out
           {"kuo", 5 * L + 3 + 6 * L + 1},                    // dqt, q, t and tendencies in; tendencies, rain, cloud levels out
           {"rain_column", 12 * L + 4 + 6 * L + 8},
+          // the full step's other column kernels and its fused ones (timed
+          // for the fusion choice; no byte count)
+          {"fixer_apply", 0}, {"surflx", 0}, {"solang_mko3", 0}, {"mkdca", 0}, {"soil", 0}, {"land_surface", 0},
+          {"sea_ice", 0}, {"sea", 0}, {"carbon", 0}, {"fused_fixer_flux_solang", 0}, {"fused_kuo_mkdca", 0},
+          {"fused_rain_soil", 0}, {"fused_land_seaice", 0}, {"fused_sea_carbon", 0},
       };
       auto it = per_column.find(k);
       if (it == per_column.end()) throw Error(EXOGCM_EINVAL, "unknown kernel " + k);

@@ -94,6 +94,9 @@ void phy_carbon(const Model& m, cudaStream_t st);
 void phy_fused_through_radiation(const Model& m, cudaStream_t st);
 void phy_fused_precipitation_to_carbon(const Model& m, cudaStream_t st);
 void phy_pack(const Model& m, cudaStream_t st);
+
+// budget.cu: per-slot FP64 global budgets and the snapshot's running sums
+void phy_budget(const Model& m, int snapshot_planes, cudaStream_t st);
 void phy_finite_check(const Model& m, cudaStream_t st);
 // One named column kernel of the physics (for timing); false if unknown.
 bool phy_launch_one(const Model& m, const std::string& kernel, cudaStream_t st);

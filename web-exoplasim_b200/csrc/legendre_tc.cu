@@ -294,7 +294,9 @@ __host__ __device__ inline TcSmem tc_smem(int npad_max, int raw_floats, int n_ta
   const size_t tab_stage = (size_t)kChunkSteps * npad_max * 2 * kStepK * 4;
   s.data = s.tab + n_tab * tab_stage;
   const size_t data_stage = (size_t)kChunkSteps * 2 * kDataStepFloats * 4;
-  s.raw = s.data + kNData * data_stage;
+  // raw stages 1024-byte aligned: the forward kinds' tiles arrive with the
+  // 128-byte swizzle, whose pattern repeats every 1024 bytes
+  s.raw = (s.data + kNData * data_stage + 1023) / 1024 * 1024;
   s.stage = s.raw + 2 * (size_t)raw_floats * 4;
   s.bars = s.stage + (kConv / 32) * 32 * 33 * 4;
   s.total = s.bars + 32 * 8;
@@ -307,7 +309,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   using S = Shape<KIND>;
   extern __shared__ unsigned char smem_raw_base[];
   unsigned char* base =
-      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw_base) + 127) & ~(uintptr_t)127);
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw_base) + 1023) & ~(uintptr_t)1023);
   const TcSmem L = tc_smem(g.npad_max, g.raw_floats, g.n_tab);
   const int NT = g.n_tab;
   const size_t tab_stage_floats = (size_t)kChunkSteps * g.npad_max * 2 * kStepK;
@@ -515,13 +517,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int t = threadIdx.x - 32;  // 0..255
     const int q = warp & 3;          // TMEM lane quarter of this warp
     const int half = (warp - 1) >> 2;  // the two warps of a quarter drain alternate 32-column slices
-    // Element idx of a K step (storage order) is (row, k) with row =
-    // (idx >> 6) * 8 + ((idx >> 2) & 7) and k = ((idx >> 5) & 1) * 4 +
-    // (idx & 3) (the inverse of kmajor_offset); for idx = t + 256 i that is
-    // row = row_of_thread + 32 i and a fixed k and row % NC.
-    const int row_of_thread = 8 * (t >> 6) + ((t >> 2) & 7);
-    const int k_of_thread = ((t >> 5) & 1) * 4 + (t & 3);
+    // Each converter thread builds one row's run of four K indices per K
+    // step: in the K-major layout (kmajor_offset) the floats 4 t .. 4 t + 3
+    // of a step are row (t >> 4) * 8 + (t & 7), K indices 4 ((t >> 3) & 1) +
+    // 0..3, so a thread writes one 16-byte hi and one 16-byte lo vector and a
+    // warp 512 contiguous bytes. Its row's output column row % NC, and so
+    // its term of every table block, is fixed.
+    const int row_of_thread = (t >> 4) * 8 + (t & 7);
+    const int kg_of_thread = (t >> 3) & 1;
     const int c_of_thread = row_of_thread % S::NC;
+    const int p_of_thread = row_of_thread / S::NC;
     float* st = stage + (size_t)(warp - 1) * 32 * 33;
     uint32_t ri = 0, di = 0, ii = 0;
     bool ok = true;
@@ -583,41 +588,58 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (!(ok = wait(dat_empty + ds, ((di / kNData) & 1) ^ 1))) break;
           float* db = dat + ds * data_stage_floats;
           const int s0 = chunk * kChunkSteps, ns = min(kChunkSteps, total_steps - s0);
-          for (int s = 0; s < ns; ++s) {
-            float* dh = db + (size_t)s * 2 * kDataStepFloats;
-            float* dl = dh + kDataStepFloats;
+#pragma unroll
+          for (int s = 0; s < kChunkSteps; ++s) {
+            if (s >= ns) break;
+            float4* dh = reinterpret_cast<float4*>(db + (size_t)s * 2 * kDataStepFloats) + t;
+            float4* dl = reinterpret_cast<float4*>(db + (size_t)s * 2 * kDataStepFloats + kDataStepFloats) + t;
             const int gstep = s0 + s;
-            // This thread's elements of the K step (storage order idx = t +
-            // 128 i) share one K index and one output column; their rows
-            // are 16 apart.
             const int a = S::fwd ? chunk % S::NA : gstep / ksb;
             const Term tm = term<KIND>(a, c_of_thread);
-            const int kk = 8 * s + k_of_thread;             // forward: index in the unit's 32
-            const int tmode = (gstep % ksb) * kStepK + k_of_thread;  // inverse: mode n - m
-            const bool live = S::fwd ? tm.field >= 0 : tmode < K;
-            const int half = kk >> 4, li = kk & 15;
+            const int p = p_of_thread;
+            float x[4] = {0.f, 0.f, 0.f, 0.f};
+            if (p < np) {
+              if (S::fwd) {
+                if (tm.field >= 0) {
+                  // K indices 8 s + 4 kg + j of the unit's 32: half kk >> 4, pair kk & 15
+                  const int kk0 = 8 * s + 4 * kg_of_thread, half = kk0 >> 4, li0 = kk0 & 15;
+                  // rows of 32 floats, 16-byte chunks XOR-swizzled by the row
+                  // index (the tile's 128-byte swizzle)
+                  const int rown = 2 * tm.field * S::TP + p, rows = rown + S::TP;
+                  const float* rn = r + (size_t)rown * 32;
+                  const float* rs = r + (size_t)rows * 32;
 #pragma unroll
-            for (int i = 0; i < kDataStepFloats / kConv; ++i) {
-              const int idx = t + kConv * i;
-              const int p = (row_of_thread + 32 * i) / S::NC;
-              float x = 0.f;
-              if (live && p < np) {
-                if (S::fwd) {
-                  const float* rn = r + ((size_t)(2 * tm.field) * S::TP + p) * 32;
-                  const float* rs = r + ((size_t)(2 * tm.field + 1) * S::TP + p) * 32;
-                  const float north = rn[2 * li + tm.comp], south = rs[2 * (15 - li) + tm.comp];
-                  x = tm.sign * (half == 0 ? north + south : north - south);
-                } else {
-                  const int off = ((g.raw2d ? 0 : (p0 + p) * d.NRSP) + 2 * w0) & 3;
-                  float v = r[((size_t)tm.field * S::TP + p) * g.raw_row + off + 2 * tmode + tm.comp];
+                  for (int j = 0; j < 4; ++j) {
+                    const int en = 2 * (li0 + j) + tm.comp, es = 2 * (15 - li0 - j) + tm.comp;
+                    const float north = rn[(((en >> 2) ^ (rown & 7)) << 2) | (en & 3)];
+                    const float south = rs[(((es >> 2) ^ (rows & 7)) << 2) | (es & 3)];
+                    x[j] = tm.sign * (half == 0 ? north + south : north - south);
+                  }
+                }
+              } else {
+                const int t0 = (gstep % ksb) * kStepK + 4 * kg_of_thread;  // mode n - m of j = 0
+                const int off = ((g.raw2d ? 0 : (p0 + p) * d.NRSP) + 2 * w0) & 3;
+                const float* rr = r + ((size_t)tm.field * S::TP + p) * g.raw_row + off + tm.comp;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                  const int tmode = t0 + j;
+                  float v = tmode < K ? rr[2 * tmode] : 0.f;
                   if (KIND == DV2UV && tm.field == 1 && tm.comp == 0 && m == 0 && tmode == 1) v -= g.plavor;
-                  x = tm.sign * v;
+                  x[j] = tm.sign * v;
                 }
               }
-              const float hi = tf32_round(x);
-              dh[idx] = hi;
-              dl[idx] = tf32_round(x - hi);
             }
+            float4 h, l;
+            h.x = tf32_round(x[0]);
+            h.y = tf32_round(x[1]);
+            h.z = tf32_round(x[2]);
+            h.w = tf32_round(x[3]);
+            l.x = tf32_round(x[0] - h.x);
+            l.y = tf32_round(x[1] - h.y);
+            l.z = tf32_round(x[2] - h.z);
+            l.w = tf32_round(x[3] - h.w);
+            *dh = h;
+            *dl = l;
           }
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the tensor cores
           mbar_arrive(dat_full + ds);
@@ -676,15 +698,17 @@ CUtensorMap map_1d(const float* field, size_t floats, int box) {
 
 // 2-D map over a field of `planes` planes of `plane_floats` floats, boxes of
 // `box` floats x tp planes.
-CUtensorMap map_2d(const float* field, int plane_floats, int planes, int box, int tp) {
+CUtensorMap map_2d(const float* field, int plane_floats, int planes, int box, int tp, bool swizzle = false) {
   CUtensorMap map;
   const cuuint64_t dim[2] = {(cuuint64_t)plane_floats, (cuuint64_t)planes};
   const cuuint64_t stride[1] = {(cuuint64_t)plane_floats * 4};
   const cuuint32_t bdim[2] = {(cuuint32_t)box, (cuuint32_t)tp}, estride[2] = {1, 1};
   if ((reinterpret_cast<uintptr_t>(field) & 15) || stride[0] % 16 || (box * 4) % 16 || box > 256 || tp > 256)
     throw std::runtime_error("tensor-core transform: bad 2-D map");
+  if (swizzle && box * 4 != 128) throw std::runtime_error("tensor-core transform: 128-byte swizzle needs 128-byte rows");
   const CUresult r = encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(field), dim, stride, bdim,
-                               estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                               swizzle ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled (2-D) failed: " + std::to_string((int)r));
   return map;
@@ -719,13 +743,13 @@ TcGeom geometry(const Dims& d, int planes, float plavor) {
   g.plavor = plavor;
   // as many table stages as shared memory holds
   g.n_tab = 2;
-  while (g.n_tab < kMaxTab && tc_smem(g.npad_max, g.raw_floats, g.n_tab + 1).total + 128 <= kTcSmemLimit) ++g.n_tab;
+  while (g.n_tab < kMaxTab && tc_smem(g.npad_max, g.raw_floats, g.n_tab + 1).total + 1024 <= kTcSmemLimit) ++g.n_tab;
   return g;
 }
 
 template <int KIND>
 size_t smem_bytes(const TcGeom& g) {
-  return tc_smem(g.npad_max, g.raw_floats, g.n_tab).total + 128;
+  return tc_smem(g.npad_max, g.raw_floats, g.n_tab).total + 1024;
 }
 
 template <int KIND>
@@ -736,7 +760,7 @@ void launch(const Model& m, const float* const* in, float* out0, float* out1, in
   const TcGeom g = geometry<KIND>(d, planes, plavor);
   TcMaps maps{};
   for (int f = 0; f < S::NR; ++f)
-    maps.in[f] = S::fwd    ? map_2d(in[f], d.NLAT * d.NFC, planes, 32, S::TP)
+    maps.in[f] = S::fwd    ? map_2d(in[f], d.NLAT * d.NFC, planes, 32, S::TP, true)
                  : g.raw2d ? map_2d(in[f], d.NRSP, planes, g.box, S::TP)
                            : map_1d(in[f], (size_t)planes * d.NRSP, g.box);
   TcOut io{};

@@ -1996,15 +1996,13 @@ __global__ void k_finite(Model m) {
 
 
 
-// Fused column kernels of a full step (exogcm_step): the per-column routines
-// that follow one another between the per-planet reductions run in one
-// launch, each thread taking its column through them in the reference's
-// order (stepper/index.ts:148-161): fixer apply, surface fluxes, vertical
-// diffusion, solar angle and ozone | kuo and mkdca | rain and soil | land
-// surface and sea ice | sea and carbon. A routine re-reads the fields the one
-// before it just wrote or read for the same column from L1/L2 instead of
-// HBM, and five launches replace twelve. Stage replay (exogcm_run_stage)
-// keeps the separate kernels; a full step equals its stages bit for bit.
+// Fused column kernels (each thread takes its column through consecutive
+// routines in the reference's order, stepper/index.ts:148-161): kuo + mkdca,
+// rain + soil, land surface + sea ice, sea + carbon. A routine re-reads what
+// the one before it wrote or read for the same column from L1/L2 instead of
+// HBM. The full step uses the two that measured faster than their parts
+// (see phy_fused_precipitation_to_carbon); stage replay (exogcm_run_stage)
+// runs the separate kernels, and a full step equals its stages bit for bit.
 template <int NL>
 __global__ void __launch_bounds__(kBlock, 4) k_fused_kuo_mkdca(Model m, const PlanetConst* __restrict__ pcr,
                                                                const float* __restrict__ tabr) {
@@ -2092,31 +2090,28 @@ void phy_surface(const Model& m, cudaStream_t st) {
 
 void phy_carbon(const Model& m, cudaStream_t st) { by_levels<Carbon>(m.d.L, m, st); }
 
-// The full step's physics between physics_in and physics_out with the fused
-// column kernels: the fixer's column and row sums and its per-planet FP64
-// sum, then [fixer apply, surflx, vdiff, solang/mko3], swr, lwr/radstep; the
-// precipitation transform is the caller's; then [kuo, mkdca], the per-planet
-// mkdca limit, [rain column, soil], mkradv (a neighbour stencil), [land
-// surface, sea ice], the per-planet getiflx sum and [sea, carbon].
+// The full step's physics between physics_in and physics_out. Fusing
+// consecutive per-column routines into one kernel was measured per pair at
+// 128 T42 L10 planets (CUDA events): land surface + sea ice (86.5 against
+// 88.7 us) and sea + carbon (57.7 against 60.2 us) pay and run fused; fixer
+// apply + surflx + vdiff + solang/mko3 (375.6 against 354.1 us), kuo + mkdca
+// (199.7 against 180.6 us) and rain + soil (274.0 against 259.5 us) lost more
+// to the fused kernels' register pressure and lower occupancy than they saved
+// in re-reads, and run as separate kernels.
 void phy_fused_through_radiation(const Model& m, cudaStream_t st) {
-  by_levels<FixerColumn>(m.d.L, m, st);
-  by_levels<FixerRow>(m.d.L, m, st);
-  k_slot_sums<<<m.d.S, kSumThreads, 0, st>>>(m, m.f.fixneg, m.f.fixpos, m.f.fixsum, 0);
-  phy_fused_fixer_flux_solang(m, st);
-  by_levels<Swr>(m.d.L, m, st);
-  by_levels<LwrRadstep>(m.d.L, m, st);
+  phy_fixer(m, st);
+  phy_surface_flux(m, st);
+  phy_radiation(m, st);
 }
 
 void phy_fused_precipitation_to_carbon(const Model& m, cudaStream_t st) {
-  by_levels<FusedKuoMkdca>(m.d.L, m, st);
-  k_mkdca_limit<<<m.d.S, kSumThreads, 0, st>>>(m);
-  by_levels<FusedRainSoil>(m.d.L, m, st);
+  phy_precipitation_columns(m, st);
+  by_levels<Soil>(m.d.L, m, st);
   k_mkradv<<<nblocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m);
   by_levels<FusedLandSeaice>(m.d.L, m, st);
   k_slot_sums<<<m.d.S, kSumThreads, 0, st>>>(m, m.f.ice_part1, m.f.ice_part2, m.f.ice_sums, 1);
   by_levels<FusedSeaCarbon>(m.d.L, m, st);
 }
-
 
 void phy_pack(const Model& m, cudaStream_t st) { by_levels<Pack>(m.d.L, m, st); }
 
@@ -2139,6 +2134,24 @@ bool phy_launch_one(const Model& m, const std::string& kernel, cudaStream_t st) 
     by_levels<Mkdca>(L, m, st);
   else if (kernel == "rain_column")
     by_levels<RainColumn>(L, m, st);
+  else if (kernel == "soil")
+    by_levels<Soil>(L, m, st);
+  else if (kernel == "land_surface")
+    by_levels<LandSurface>(L, m, st);
+  else if (kernel == "sea_ice")
+    by_levels<SeaIce>(L, m, st);
+  else if (kernel == "sea")
+    by_levels<Sea>(L, m, st);
+  else if (kernel == "carbon")
+    by_levels<Carbon>(L, m, st);
+  else if (kernel == "fused_kuo_mkdca")
+    by_levels<FusedKuoMkdca>(L, m, st);
+  else if (kernel == "fused_rain_soil")
+    by_levels<FusedRainSoil>(L, m, st);
+  else if (kernel == "fused_land_seaice")
+    by_levels<FusedLandSeaice>(L, m, st);
+  else if (kernel == "fused_sea_carbon")
+    by_levels<FusedSeaCarbon>(L, m, st);
   else
     return false;
   return true;

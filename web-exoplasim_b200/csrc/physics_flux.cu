@@ -322,6 +322,10 @@ void phy_fused_fixer_flux_solang(const Model& m, cudaStream_t st) {
 
 bool phy_flux_launch_one(const Model& m, const std::string& kernel, cudaStream_t st) {
   if (kernel == "vdiff") by_levels<Vdiff>(m.d.L, m, st);
+  else if (kernel == "surflx") by_levels<Surflx>(m.d.L, m, st);
+  else if (kernel == "fixer_apply") by_levels<FixerApply>(m.d.L, m, st);
+  else if (kernel == "solang_mko3") by_levels<SolangMko3>(m.d.L, m, st);
+  else if (kernel == "fused_fixer_flux_solang") by_levels<FusedFixerFluxSolang>(m.d.L, m, st);
   else return false;
   return true;
 }
