@@ -338,7 +338,37 @@ def served_config5(seconds, budget_gb=40.0, seed=7):
             "arrival_rate_per_s": 20.0, "run_days": "1-365 (uniform)", "resolutions": "T21/T42/T63 x L5/L10",
             "window_s": round(rep["window_s"], 2), "queue_depth_mean": round(rep["queue_depth_mean"], 1),
             "queue_depth_max": rep["queue_depth_max"], "budget_gb": budget_gb, "slots": rep["slots"],
-            "blocks_created": rep["blocks_created"], "blocks_destroyed": rep["blocks_destroyed"]}
+            "blocks_created": rep["blocks_created"], "blocks_destroyed": rep["blocks_destroyed"],
+            "configure_ms_p50": rep["configure_ms_p50"] and round(rep["configure_ms_p50"], 2),
+            "configure_ms_p99": rep["configure_ms_p99"] and round(rep["configure_ms_p99"], 2),
+            "setup_on_device": rep["setup_on_device"]}
+
+
+def admission_latency(pkg, repeats=5):
+    """exogcm_configure wall time (FP64 set-up plus upload) of one planet at
+    each resolution, with the heavy set-up loops on the host and on the
+    device; the median of `repeats` configures of a fresh planet into slot 0
+    of a 4-slot mode-1 engine whose shared tables are already built."""
+    planets = importlib.import_module("web-exoplasim_b200.planets")
+    out = {}
+    for truncation in (21, 42, 63):
+        plist = [planets.make_planet(500 + k, truncation=truncation, levels=10) for k in range(repeats + 1)]
+        row = {}
+        for where in ("host", "device"):
+            e = pkg.Engine(truncation, 10, 4, mode=1)
+            try:
+                e.setup_on_device(where == "device")
+                e.configure(1, plist[0])  # shared tables, autotuning, staging buffers
+                times = []
+                for p in plist[1:]:
+                    t = time.perf_counter()
+                    e.configure(0, p)
+                    times.append(time.perf_counter() - t)
+                row[where] = round(float(np.median(times)) * 1e3, 2)
+            finally:
+                e.close()
+        out[f"T{truncation}L10"] = row
+    return {"unit": "ms per planet (median of %d)" % repeats, **out}
 
 
 def reference_arm(args, rank):
@@ -481,6 +511,11 @@ def main():
                 extra = extra_configs(pkg, plist, max(64, args.steps // 2))
             except Exception as exc:  # noqa: BLE001
                 extra = {"extra_configs_error": f"{type(exc).__name__}: {exc}"}
+        if not args.no_extra:
+            try:
+                extra = dict(extra or {}, admission=admission_latency(pkg))
+            except Exception as exc:  # noqa: BLE001
+                extra = dict(extra or {}, admission={"error": f"{type(exc).__name__}: {exc}"})
         if not args.no_served:
             try:
                 served = served_config5(args.served_seconds)

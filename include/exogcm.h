@@ -70,6 +70,9 @@ typedef struct exogcm_planet {
   int filter_kind;               /* NFILTER: 0 none, 1 Cesaro, 2 exp, 3 Landau-Hoskins, 4 */
   double soil_depth_scale;
   double star_temperature_k;     /* 0: no stellar-spectrum albedo split */
+  int storm_diagnostics;         /* NSTORMDIAG: storm-climatology fields each step (GcmConfig.stormclim) */
+  double storm_ckcd;             /* CKCD, Ck/Cd; 0: 0.9 */
+  double storm_vithresh;         /* VITHRESH, ventilation threshold; 0: 0.145 */
 } exogcm_planet;
 
 /* Boundary and initial fields on the Gaussian grid (NLAT x 2 NLAT points,
@@ -101,12 +104,23 @@ int exogcm_last_error(char* buffer, size_t size);
 int exogcm_create(int truncation, int levels, int slots, int mode, exogcm_engine** engine);
 void exogcm_destroy(exogcm_engine* engine);
 
-/* Set-up of one slot in FP64 on the host and upload of its tables and
- * initial state (SETUP.state / SETUP.schedule, setup/index.ts:434-477;
- * LAYOUT.write, layout/index.ts:66-71). The slot then runs the reference's
- * start-up steps before its main loop. */
+/* Set-up of one slot in FP64 and upload of its tables and initial state
+ * (SETUP.state / SETUP.schedule, setup/index.ts:434-477; LAYOUT.write,
+ * layout/index.ts:66-71). The slot then runs the reference's start-up steps
+ * before its main loop. The heavy FP64 loops (the Legendre tables of the
+ * engine's first planet, legendre/index.ts:29-136; the grid -> spectral
+ * analysis of the orography and the initial temperature and humidity,
+ * legendre/index.ts:334-361; makebm's LU inverses,
+ * dynamics/setup/index.ts:154-239) run on the engine's device on a stream
+ * of their own, beside batches already stepping, unless
+ * exogcm_setup_on_device(engine, 0) moved them to the host; both give the
+ * same numbers bit for bit. */
 int exogcm_configure(exogcm_engine* engine, int slot, const exogcm_planet* planet,
                      const exogcm_boundary* boundary);
+
+/* Chooses where exogcm_configure runs its heavy FP64 set-up loops: on the
+ * engine's device (enable != 0, the default) or on the host. */
+int exogcm_setup_on_device(exogcm_engine* engine, int enable);
 
 /* Runs the FP64 set-up of exogcm_configure on the host only and returns one
  * of its arrays, with no device involved (a dry run of configure). `name`
@@ -119,6 +133,11 @@ int exogcm_configure(exogcm_engine* engine, int slot, const exogcm_planet* plane
  * start-up steps). `*count` returns the array length; values may be NULL. */
 int exogcm_setup_preview(const exogcm_planet* planet, const exogcm_boundary* boundary, const char* name,
                          double* values, size_t* count);
+
+/* exogcm_setup_preview with the heavy FP64 loops on the current device, as
+ * exogcm_configure runs them (needs a GPU). */
+int exogcm_setup_preview_device(const exogcm_planet* planet, const exogcm_boundary* boundary, const char* name,
+                                double* values, size_t* count);
 
 /* Frees a slot for another planet (continuous batching). */
 int exogcm_release(exogcm_engine* engine, int slot);

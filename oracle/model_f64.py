@@ -425,7 +425,8 @@ def phase_constants(pm, mods, kits, nlon):
         NCARBON=1.0 if carbon["ncarbon"] else 0.0, NSUPPLY=1.0 if carbon["nsupply"] else 0.0,
         TIMEWEIGHT=carbon["timeweight"], CO2EARTH=S.CO2EARTH, BETA=carbon["beta"], KACT=carbon["kact"],
         PEARTH=carbon["pearth"], WMAX=carbon["wmax"], VEARTH=carbon["vearth"], PLARAD=pm["plarad"],
-        RAD_EARTHSQ=S.RAD_EARTHSQ,
+        RAD_EARTHSQ=S.RAD_EARTHSQ, NSTORMDIAG=float(mods["storm"]["nstormdiag"]), CKCD=mods["storm"]["ckcd"],
+        VITHRESH=mods["storm"]["vithresh"],
     )
     c.update(S.lwr_offsets())
     return c

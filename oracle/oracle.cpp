@@ -60,7 +60,8 @@ using real = ORACLE_REAL;
   X(CRHOSN) X(CPI) X(CKAPI) X(CKAPSN) X(CLFI) X(CLFSN) X(DTMIX) X(CPS) X(CHARNOCK) X(DZ0SEA)     \
   X(DZ0ICE) X(DRHSSEA) X(DRHSICE) X(ALBSEA) X(ALBICE) X(DICEALBMX1) X(DICEALBMX2) X(DICEALBMN1)  \
   X(DICEALBMN2) X(ICE_COUPLED) X(NCARBON) X(NSUPPLY) X(TIMEWEIGHT) X(CO2EARTH) X(BETA) X(KACT)   \
-  X(PEARTH) X(WMAX) X(VEARTH) X(PLARAD) X(RAD_EARTHSQ) X(JET) X(SIGMA_LOW)
+  X(PEARTH) X(WMAX) X(VEARTH) X(PLARAD) X(RAD_EARTHSQ) X(JET) X(SIGMA_LOW) X(NSTORMDIAG) X(CKCD)   \
+  X(VITHRESH)
 
 struct Consts {
 #define DECL(n) real n = 0;
@@ -2420,6 +2421,159 @@ void carbon(Model& m) {
   }
 }
 
+// physics/storm/wgsl/storm.wgsl:1-208 (hurricanestep, after hurricanemod.f90):
+// environmental CAPE and its neutral-buoyancy pressure, potential intensity,
+// entropy deficit, absolute vorticity, ventilation, genesis potential and
+// shear per column; nothing when NSTORMDIAG is 0 (storm/index.ts:27).
+namespace storm_diag {
+const real CPD = 1005.7, CL = 2500.0, RVP = 461.5, ALV0 = 2.501e6, CPVMCL = -630.0;
+struct Cape {
+  real energy, temperature, pressure;
+};
+real es(real tc) { return 6.112 * std::exp(17.67 * tc / (243.5 + tc)); }                       // storm.wgsl:28-30
+real vapor(real r, real p, real rd) { return r * p / (rd / RVP + r); }                         // :32-35
+real mixing(real e, real p, real rd) { return (rd / RVP) * e / (p - e); }                      // :37-40
+real density(real t, real rt, real r, real rd) { return t * (1 + r / (rd / RVP)) / (1 + rt); }  // :42-45
+real entropy(real t, real r, real p, real rd) {                                                // :47-55
+  const real e = vapor(r, p, rd);
+  const real rh = std::min(e / es(t - 273.15), (real)1);
+  const real lv = ALV0 + CPVMCL * (t - 273.15);
+  const real dry = (CPD + r * CL) * std::log(t) - rd * std::log(p - e);
+  if (r == 0) return dry;
+  return dry + lv * r / t - r * RVP * std::log(rh);
+}
+// storm.wgsl:57-126; levels 0 (top) .. n - 1 (bottom).
+Cape cape(const real* st, const real* sr, const real* sp, int n, real tp, real rp, real pp, real rd) {
+  if (rp < 1e-6 || tp < 200 || pp <= 0) return {0, -1, -1};
+  const real rh = std::min(vapor(rp, pp, rd) / es(tp - 273.15), (real)1);
+  const real parcel = entropy(tp, rp, pp, rd);
+  const real plcl = pp * std::pow(rh, tp / (1669 - 122 * rh - tp));
+  real b[MAXL];
+  for (int l = n - 1; l >= 0; --l) {
+    real tg, rg = rp;
+    if (sp[l] >= plcl) {
+      tg = tp * std::pow(sp[l] / pp, rd / CPD);
+    } else {
+      real next = st[l];
+      tg = 0;
+      int count = 0;
+      while (!(std::fabs(next - tg) <= 0.001)) {
+        tg = next;
+        const real tc = tg - 273.15, enew = es(tc);
+        rg = mixing(enew, sp[l], rd);
+        ++count;
+        const real lv = ALV0 + CPVMCL * tc;
+        const real sl = (CPD + rp * CL + lv * lv * rg / (RVP * tg * tg)) / tg;
+        const real em = vapor(rg, sp[l], rd);
+        if (sp[l] - em <= 0 || tg <= 0) return {0, st[l], -1};
+        const real sg = (CPD + rp * CL) * std::log(tg) - rd * std::log(sp[l] - em) + lv * rg / tg;
+        next = tg + (count < 3 ? (real)0.3 : (real)1) * (parcel - sg) / sl;
+        if (count > 500 || enew > sp[l] - 1 || !(next > 0)) return {0, st[n - 1], sp[n - 1]};
+      }
+    }
+    b[l] = density(tg, rp, rg, rd) - density(st[l], sr[l], sr[l], rd);
+  }
+  int inb = n - 1;
+  for (int l = 0; l < n; ++l)
+    if (b[l] > 0) inb = std::min(inb, l);
+  if (inb == n - 1) return {0, st[n - 1], 0};
+  real area = 0;
+  for (int l = n - 2; l >= inb; --l) area += rd * (b[l] + b[l + 1]) * (sp[l + 1] - sp[l]) / (sp[l] + sp[l + 1]);
+  area += rd * (pp - sp[n - 1]) / (pp + sp[n - 1]) * b[n - 1];
+  real tob = st[inb], lnb = sp[inb];
+  if (inb > 0) {
+    lnb = (sp[inb - 1] * b[inb] - sp[inb] * b[inb - 1]) / (b[inb] - b[inb - 1]);
+    area += rd * b[inb] * (sp[inb] - lnb) / (sp[inb] + lnb);
+    tob = (st[inb] * (lnb - sp[inb - 1]) + st[inb - 1] * (sp[inb] - lnb)) / (sp[inb] - sp[inb - 1]);
+  }
+  return {std::max(area, (real)0), tob, lnb};
+}
+real reduced(real vi, real vithresh) {  // storm.wgsl:128-133
+  if (vi == 0 || std::fabs(vi) >= vithresh) return 0;
+  return 2 / std::sqrt((real)3) * std::cos(std::acos(-vi / vithresh) / 3);
+}
+}  // namespace storm_diag
+
+void storm(Model& m) {  // storm.wgsl:135-208
+  using namespace storm_diag;
+  const Consts& K = m.k;
+  if (K.NSTORMDIAG <= 0) return;
+  const int NH = m.NHOR, NL = m.NLEV;
+  const real *DT = m.F("dt"), *DQ = m.F("dq"), *DU = m.F("du"), *DV = m.F("dv"), *GZ = m.F("gz"), *DP = m.F("dp");
+  const real* sg = m.TB("sigma");
+  real *CAPEN = m.F("capen"), *LNB = m.F("lnb"), *MPOTI = m.F("mpoti"), *CHIM = m.F("chim"), *LAAV = m.F("laav"),
+       *VENTI = m.F("venti"), *VRMPI = m.F("vrmpi"), *GPI = m.F("gpi"), *SHEAR = m.F("shear");
+  const real rd = K.GASCON;
+  for (int h = 0; h < NH; ++h) {
+    real st[MAXL], sr[MAXL], sp[MAXL];
+    const real msl = DP[h] * 0.01, sst = DT[NL * NH + h];
+    int i600 = 0, i850 = 0, i200 = 0;
+    bool cold = false;
+    for (int l = 0; l < NL; ++l) {
+      st[l] = DT[l * NH + h];
+      sr[l] = DQ[l * NH + h];
+      sp[l] = msl * sg[l];
+      cold = cold || st[l] <= 100;
+      if (std::fabs(sg[l] - 0.6) < std::fabs(sg[i600] - 0.6)) i600 = l;
+      if (std::fabs(sg[l] - 0.85) < std::fabs(sg[i850] - 0.85)) i850 = l;
+      if (std::fabs(sg[l] - 0.2) < std::fabs(sg[i200] - 0.2)) i200 = l;
+    }
+    const int bottom = NL - 1;
+    const real u8 = DU[i850 * NH + h], v8 = DV[i850 * NH + h], u2 = DU[i200 * NH + h], v2 = DV[i200 * NH + h];
+    const real shear = std::fabs(std::sqrt(u2 * u2 + v2 * v2) - std::sqrt(u8 * u8 + v8 * v8));
+    const real vort = GZ[i850 * NH + h] * K.WW;
+    real deficit = 1;
+    if (sr[i600] > 0 && sr[bottom] > 0) {
+      const real smr = mixing(es(st[i600] - 273.15), sp[i600], rd);
+      const real sms = entropy(st[i600], smr, sp[i600], rd);
+      const real sme = entropy(st[i600], std::min(sr[i600], smr), sp[i600], rd);
+      const real smb = entropy(sst, DQ[NL * NH + h], msl, rd);
+      const real smo = entropy(sst, mixing(es(sst - 273.15), msl, rd), msl, rd);
+      if (smo != smb) deficit = (sms - sme) / (smo - smb);
+    }
+    Cape env{-1, -1, -1};
+    real vmax = -1;
+    if (sst > 278.15 && !cold && msl > 0) {
+      env = cape(st, sr, sp, NL, st[bottom], sr[bottom], sp[bottom], rd);
+      real pm = 970, old = pm, next = 0, capem = 0, capems = 0, ratio = 1;
+      bool failed = false;
+      int count = 0;
+      while (!(std::fabs(next - old) <= 0.5)) {
+        const real pp = std::min(pm, (real)1000);
+        const real rp = (rd / RVP) * sr[bottom] * msl / (pp * (rd / RVP + sr[bottom]) - sr[bottom] * msl);
+        capem = cape(st, sr, sp, NL, st[bottom], rp, pp, rd).energy;
+        const real rs = mixing(es(sst - 273.15), pp, rd);
+        const Cape sat = cape(st, sr, sp, NL, sst, rs, pp, rd);
+        capems = sat.energy;
+        ratio = sst / sat.temperature;
+        const real tvav = 0.5 * (density(st[bottom], sr[bottom], sr[bottom], rd) + density(sst, rs, rs, rd));
+        const real cat = std::max((capem - env.energy) + 0.5 * K.CKCD * ratio * (capems - capem), (real)0);
+        next = msl * std::exp(-cat / (rd * tvav));
+        old = pm;
+        pm = next;
+        ++count;
+        if (count > 200 || pm < 400 || !(pm > 0)) {
+          failed = true;
+          break;
+        }
+      }
+      if (!failed) vmax = std::sqrt(std::max((real)0, K.CKCD * ratio * std::max((real)0, capems - capem)));
+    }
+    const real vi = vmax > 0 ? shear * deficit / vmax : 1;
+    const real rh = vapor(sr[i600], sp[i600], rd) / es(st[i600] - 273.15);
+    const real v70 = vmax / 70, damp = 1 + 0.1 * shear;
+    CAPEN[h] = env.energy;
+    LNB[h] = env.pressure;
+    MPOTI[h] = vmax;
+    CHIM[h] = deficit;
+    LAAV[h] = vort;
+    VENTI[h] = vi;
+    VRMPI[h] = reduced(vi, K.VITHRESH);
+    GPI[h] = std::pow(std::fabs(vort * 1e5), (real)1.5) * std::pow(rh * 2, (real)3) * v70 * v70 * v70 / (damp * damp);
+    SHEAR[h] = shear;
+  }
+}
+
 // snapshot/wgsl/pack.wgsl:1-107.
 void pack(Model& m) {
   const Consts& K = m.k;
@@ -2626,6 +2780,7 @@ void full_step(Model& m) {
   precipitation_stage(m);
   surface_stage(m);
   carbon(m);
+  storm(m);
   physics_out_stage(m);
   spectrald_stage(m);
   pack(m);
@@ -2716,6 +2871,7 @@ int ora_run(void* p, const char* stage) {
     else if (s == "precipitation") precipitation_stage(m);
     else if (s == "surface") surface_stage(m);
     else if (s == "carbon") carbon(m);
+    else if (s == "storm") storm(m);
     else if (s == "physics_out") physics_out_stage(m);
     else if (s == "spectrald") spectrald_stage(m);
     else if (s == "pack") pack(m);

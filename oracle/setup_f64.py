@@ -329,7 +329,11 @@ def namelist_edits(config):
         "oceanmod_namelist": dict(MLDEPTH=config["oceanDepthM"]),
         "vegmod_namelist": dict(NCVEG=1, FORGROW=1.0, RINIDSC=1.0, RINIDMR=2.0, RINISOIL=0.0,
                                 RINIVEG=0.0, RINIDAGG=config["initialGrowth"]),
-        "hurricane_namelist": dict(NSTORMDIAG=0),
+        # namelist/index.ts:175: NSTORMDIAG = flag(config.stormclim); CKCD and
+        # VITHRESH only through namelist text, here config overrides.
+        "hurricane_namelist": dict(NSTORMDIAG=1 if config.get("stormclim") else 0,
+                                   **({"CKCD": config["stormCkcd"]} if config.get("stormCkcd") else {}),
+                                   **({"VITHRESH": config["stormVithresh"]} if config.get("stormVithresh") else {})),
         "glacier_namelist": dict(NGLACIER=1 if config["glaciersEnabled"] else 0,
                                  GLACELIM=config["glaciersMinDepthM"],
                                  ICESHEETH=config["glaciersInitialHeightM"]),
@@ -660,8 +664,10 @@ def module_setup(truncation, levels, files, pm):
     ocean = nl_read(files.get("oceanmod_namelist", {}), dict(mldepth=50.0))
     surf = nl_read(files.get("surfmod_namelist", {}), dict(nspinit=0, noromax=truncation))
     glacier = nl_read(files.get("glacier_namelist", {}), dict(nglacier=1, glacelim=2.0, icesheeth=-1.0))
+    # setup/index.ts:107-113: hurricane_namelist with its defaults.
+    storm = nl_read(files.get("hurricane_namelist", {}), dict(nstormdiag=0, ckcd=0.9, vithresh=0.145))
     return dict(rad=rad, rain=rain, flux=flux, land=land, sea=sea, ice=ice, veg=veg, carbon=carbon,
-                ocean=ocean, surf=surf, glacier=glacier, albedos=albedos)
+                ocean=ocean, surf=surf, glacier=glacier, albedos=albedos, storm=storm)
 
 
 # ---------------------------------------------------------------- dynamics set-up

@@ -118,3 +118,62 @@ def carbon_counter(model, main_steps):
     for k in range(main_steps):
         _, c = setup_f64.step_values(start + k, c, model["calendar"])
     return c
+
+
+# The storm diagnostics' synthetic columns (the reference's
+# scripts/exoplasim-webgpu/verify-storm.mjs:48-66 recipe): eleven climates at
+# one gas constant over the model's sigma levels; `t` and `r` carry the
+# surface value after the L levels, `u`, `v`, `z` only the L levels.
+STORM_CLIMATES = ("tropical", "warm", "cold", "hot", "dry", "stable", "thin", "humid", "cold-profile",
+                  "reversed-vorticity", "zero-shear")
+STORM_FIELDS = ("capen", "lnb", "mpoti", "chim", "laav", "venti", "vrmpi", "gpi", "shear")
+# verify-storm.mjs:126-129: |got - expected| <= absolute + 0.5 % |expected|.
+STORM_ABSOLUTE = (5.0, 1.0, 0.2, 0.005, 1e-9, 0.005, 0.005, 0.005, 1e-4)
+
+
+def storm_columns(sigma, rd):
+    import math
+    rows = []
+    for climate in STORM_CLIMATES:
+        msl = 500.0 if climate == "thin" else 1000.0
+        sst = {"cold": 270.0, "hot": 330.0, "warm": 300.0}.get(climate, 305.0)
+        t = [290.0 if climate == "stable" else 95 + 150 * s if climate == "cold-profile" else 195 + 108 * math.sqrt(s)
+             for s in sigma]
+
+        def e_of(temp):
+            return 6.112 * math.exp(17.67 * (temp - 273.15) / (temp - 29.65))
+        r = [0.0 if climate == "dry" else rd / 461.5 * e_of(tl) / (msl * sl - e_of(tl)) *
+             (0.98 if climate == "humid" else 0.7) for tl, sl in zip(t, sigma)]
+        es = e_of(sst)
+        r.append(0.0 if climate == "dry" else 0.8 * (rd / 461.5) * es / (msl - es))
+        rows.append(dict(climate=climate, msl=msl, sst=sst, t=t + [sst], r=r,
+                         u=[5.0 if climate == "zero-shear" else 3 + 20 * (1 - s) for s in sigma],
+                         v=[4.0] * len(sigma), z=[-1.2 if climate == "reversed-vorticity" else 1.2] * len(sigma)))
+    return rows
+
+
+def storm_state(rows, levels, nhor):
+    """Fields dt, dq (L + 1 levels), du, dv (L + 1, the last zero), gz (L)
+    and dp (Pa) with column h holding rows[h % len(rows)]."""
+    pick = [rows[h % len(rows)] for h in range(nhor)]
+    out = {}
+    for key, name, count in (("t", "dt", levels + 1), ("r", "dq", levels + 1), ("u", "du", levels + 1),
+                             ("v", "dv", levels + 1), ("z", "gz", levels)):
+        arr = np.zeros((count, nhor))
+        for h, row in enumerate(pick):
+            vals = row[key]
+            arr[:len(vals), h] = vals[:count]
+        out[name] = arr
+    out["dp"] = np.array([row["msl"] * 100.0 for row in pick])
+    return out
+
+
+def storm_within(got, expected):
+    """Per field, the columns outside the reference's storm tolerance."""
+    bad = {}
+    for i, name in enumerate(STORM_FIELDS):
+        g, e = np.asarray(got[name], float), np.asarray(expected[name], float)
+        off = ~(np.isfinite(g) & (np.abs(g - e) <= STORM_ABSOLUTE[i] + 0.005 * np.abs(e)))
+        if off.any():
+            bad[name] = np.flatnonzero(off)
+    return bad

@@ -44,7 +44,8 @@ class Planet(ctypes.Structure):
         ("initial_growth", ctypes.c_double), ("glaciers", ctypes.c_int), ("glacier_min_depth_m", ctypes.c_double),
         ("glacier_initial_height_m", ctypes.c_double), ("filter_gp", ctypes.c_int), ("filter_sp", ctypes.c_int),
         ("filter_kind", ctypes.c_int), ("soil_depth_scale", ctypes.c_double),
-        ("star_temperature_k", ctypes.c_double),
+        ("star_temperature_k", ctypes.c_double), ("storm_diagnostics", ctypes.c_int),
+        ("storm_ckcd", ctypes.c_double), ("storm_vithresh", ctypes.c_double),
     ]
 
 
@@ -70,6 +71,9 @@ SIGNATURES = {
     "exogcm_configure": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(Planet), ctypes.POINTER(Boundary)]),
     "exogcm_setup_preview": (ctypes.c_int, [ctypes.POINTER(Planet), ctypes.POINTER(Boundary), ctypes.c_char_p,
                                             _DP, ctypes.POINTER(ctypes.c_size_t)]),
+    "exogcm_setup_preview_device": (ctypes.c_int, [ctypes.POINTER(Planet), ctypes.POINTER(Boundary),
+                                                   ctypes.c_char_p, _DP, ctypes.POINTER(ctypes.c_size_t)]),
+    "exogcm_setup_on_device": (ctypes.c_int, [_VP, ctypes.c_int]),
     "exogcm_release": (ctypes.c_int, [_VP, ctypes.c_int]),
     "exogcm_step": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
     "exogcm_step_async": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
@@ -160,7 +164,9 @@ def planet_struct(config: dict) -> Planet:
         glaciers=int(bool(config["glaciersEnabled"])), glacier_min_depth_m=float(config["glaciersMinDepthM"]),
         glacier_initial_height_m=float(config["glaciersInitialHeightM"]), filter_gp=gp, filter_sp=sp,
         filter_kind=kind, soil_depth_scale=float(config["soilDepthScale"]),
-        star_temperature_k=float(config["starTemperatureK"]))
+        star_temperature_k=float(config["starTemperatureK"]),
+        storm_diagnostics=int(bool(config.get("stormclim", False))),
+        storm_ckcd=float(config.get("stormCkcd", 0.0)), storm_vithresh=float(config.get("stormVithresh", 0.0)))
 
 
 def boundary_struct(planet, nhor: int, keep: dict) -> Boundary:
@@ -192,19 +198,20 @@ def group_step(engines, steps, publish_every: int | None = None) -> float:
     return ms.value
 
 
-def setup_preview(planet, name: str) -> np.ndarray:
+def setup_preview(planet, name: str, on_device: bool = False) -> np.ndarray:
     """The FP64 set-up array `name` (see exogcm_setup_preview) for a planet,
-    computed on the host without a device."""
+    computed on the host without a device, or with the heavy loops on the
+    current device as exogcm_configure runs them (`on_device`)."""
     lib = load_library()
+    call = lib.exogcm_setup_preview_device if on_device else lib.exogcm_setup_preview
     nhor = 2 * {21: 32, 42: 64, 63: 96}[planet.config["truncation"]] ** 2
     keep = {}
     p = planet_struct(planet.config)
     b = boundary_struct(planet, nhor, keep)
     n = ctypes.c_size_t(0)
-    _check(lib.exogcm_setup_preview(ctypes.byref(p), ctypes.byref(b), name.encode(), None, ctypes.byref(n)))
+    _check(call(ctypes.byref(p), ctypes.byref(b), name.encode(), None, ctypes.byref(n)))
     out = np.zeros(n.value)
-    _check(lib.exogcm_setup_preview(ctypes.byref(p), ctypes.byref(b), name.encode(), out.ctypes.data_as(_DP),
-                                    ctypes.byref(n)))
+    _check(call(ctypes.byref(p), ctypes.byref(b), name.encode(), out.ctypes.data_as(_DP), ctypes.byref(n)))
     return out
 
 
@@ -228,6 +235,10 @@ class Engine:
 
     def __del__(self):
         self.close()
+
+    def setup_on_device(self, enable: bool = True) -> None:
+        """Where configure runs its heavy FP64 set-up loops (device by default)."""
+        _check(_lib.exogcm_setup_on_device(self.h, int(bool(enable))))
 
     def configure(self, slot: int, planet) -> None:
         """SETUP + LAYOUT.write for a planets.Planet."""

@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libexogcm.so")
 SOURCES = ["engine.cu", "transforms.cu", "legendre.cu", "legendre_tc.cu", "fft.cu", "spectral_grid.cu", "dynamics.cu",
-           "physics.cu", "physics_flux.cu", "budget.cu", "noalloc.cu", "setup.cpp"]
+           "physics.cu", "physics_flux.cu", "physics_storm.cu", "budget.cu", "noalloc.cu", "setup_device.cu", "setup.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
@@ -29,7 +29,10 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std
 # the IEEE division sequence.
 PHYSICS_FLAGS = ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]
 FILE_FLAGS = {"physics.cu": PHYSICS_FLAGS + ["-DEXOGCM_LWR_FAST_EXP2", "-DEXOGCM_LWR_FAST_LOG2"],
-              "physics_flux.cu": PHYSICS_FLAGS, "dynamics.cu": ["-prec-div=false"]}
+              "physics_flux.cu": PHYSICS_FLAGS, "dynamics.cu": ["-prec-div=false"],
+              # The FP64 set-up kernels follow the host loops operation for
+              # operation and must not contract a*b+c into one rounding.
+              "setup_device.cu": ["-fmad=false"]}
 
 
 def stale() -> bool:
@@ -40,7 +43,7 @@ def stale() -> bool:
         if os.path.getmtime(os.path.join(CSRC, name)) > built:
             return True
     header = os.path.join(HERE, "..", "include", "exogcm.h")
-    return os.path.getmtime(header) > built
+    return os.path.getmtime(header) > built or os.path.getmtime(os.path.abspath(__file__)) > built
 
 
 def build(force: bool = False, verbose: bool = False) -> str:

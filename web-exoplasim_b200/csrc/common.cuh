@@ -166,6 +166,7 @@ struct Model {
   // field after each stage, so there (zero_gdt = 1) the kernels zero and
   // read them as the reference does.
   int zero_gdt;
+  int storm;  // some slot runs the storm-climatology diagnostics (NSTORMDIAG > 0)
 };
 
 }  // namespace exogcm

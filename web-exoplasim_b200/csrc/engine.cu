@@ -72,6 +72,7 @@ struct Slot {
   long stop = -1;  // model step at which the slot stops (-1: never)
   double deltsec[4] = {0}, delt[4] = {0};
   Calendar cal{};
+  bool storm = false;  // NSTORMDIAG > 0: hurricanestep runs for this slot
 };
 
 constexpr int kMaxBatch = 64;
@@ -132,6 +133,12 @@ struct exogcm_engine {
   std::map<int, cudaGraph_t> graph_templates;  // the captured K-step graphs (child nodes of group graphs)
   Tuning tune{};
   SharedSetup shared_setup;  // host copy of the shared tables (set-up of later planets)
+  // FP64 set-up loops on this device (setup_device.cu), created at the first
+  // configure; exogcm_setup_on_device(e, 0) moves them to the host.
+  std::unique_ptr<SetupDevice> setup_device;
+  bool setup_on_device = true;
+  float* upload_stage = nullptr;  // pinned floats: one planet's fields and tables on their way in
+  size_t upload_stage_floats = 0;
 
   Model model(int k) const {
     Model m{};
@@ -151,6 +158,8 @@ struct exogcm_engine {
     m.tune = tune;
     m.keep_fourier = 0;
     m.zero_gdt = 0;
+    m.storm = 0;
+    for (const Slot& s : slots) m.storm |= s.storm ? 1 : 0;
     return m;
   }
 };
@@ -472,6 +481,7 @@ void run_stage(const Model& m, const std::string& s, cudaStream_t st) {
   else if (s == "precipitation") stage_precipitation(m, st);
   else if (s == "surface") phy_surface(m, st);
   else if (s == "carbon") phy_carbon(m, st);
+  else if (s == "storm") phy_storm(m, st);
   else if (s == "physics_out") stage_physics_out(m, st);
   else if (s == "spectrald") stage_spectrald(m, st);
   else if (s == "pack") phy_pack(m, st);
@@ -489,6 +499,7 @@ void full_step(const Model& m, cudaStream_t st) {
   phy_fused_through_radiation(m, st);
   tr_sp2gp(m, m.f.sqt, m.f.fdqt, m.f.dqt, m.d.L * m.d.S, m.sh.qi, st);  // precipitation's dqt
   phy_fused_precipitation_to_carbon(m, st);
+  phy_storm(m, st);
   stage_physics_out(m, st);
   stage_spectrald(m, st);
   phy_pack(m, st);
@@ -545,8 +556,9 @@ cudaGraphExec_t batch_graph(exogcm_engine* e, int K) {
   return exec;
 }
 
-void upload_slot_tables(exogcm_engine* e, int slot, const PlanetSetup& ps) {
-  std::vector<float> block(e->to.stride, 0.f);
+// The slot's table block [to.stride] in float, into `block`.
+void fill_slot_tables(exogcm_engine* e, const PlanetSetup& ps, float* block) {
+  std::fill(block, block + e->to.stride, 0.f);
   int off = 0;
   for (auto& t : e->tab_list) {
     auto it = ps.tables.find(t.first);
@@ -555,8 +567,13 @@ void upload_slot_tables(exogcm_engine* e, int slot, const PlanetSetup& ps) {
     for (int i = 0; i < t.second && i < (int)v.size(); ++i) block[off + i] = (float)v[i];
     off += t.second;
   }
-  check(cudaMemcpy(e->tabs + (size_t)slot * e->to.stride, block.data(), block.size() * sizeof(float),
-                   cudaMemcpyHostToDevice),
+}
+
+// Queues the slot's table block (filled by fill_slot_tables into pinned
+// `block`) and its constants on the engine's stream; the caller synchronises.
+void upload_slot_tables(exogcm_engine* e, int slot, const PlanetSetup& ps, float* block) {
+  check(cudaMemcpyAsync(e->tabs + (size_t)slot * e->to.stride, block, e->to.stride * sizeof(float),
+                        cudaMemcpyHostToDevice, e->stream),
         "slot tables");
   PlanetConst pc{};
 #define EXOGCM_SET_CONST(n)                                                    \
@@ -567,7 +584,10 @@ void upload_slot_tables(exogcm_engine* e, int slot, const PlanetSetup& ps) {
   }
   EXOGCM_CONSTS(EXOGCM_SET_CONST)
 #undef EXOGCM_SET_CONST
-  check(cudaMemcpy(e->pc + slot, &pc, sizeof(pc), cudaMemcpyHostToDevice), "slot constants");
+  // The constants ride in the staging area after the table block.
+  PlanetConst* staged = reinterpret_cast<PlanetConst*>(block + e->to.stride);
+  *staged = pc;
+  check(cudaMemcpyAsync(e->pc + slot, staged, sizeof(pc), cudaMemcpyHostToDevice, e->stream), "slot constants");
 }
 
 void zero_slot(exogcm_engine* e, int slot) {
@@ -766,6 +786,16 @@ void drop_group_graphs(const exogcm_engine* e) {
   }
 }
 
+// Destroys the engine's captured batch graphs (and the group graphs holding
+// them) so the next batch captures them again with the current Model.
+void drop_graphs(exogcm_engine* e) {
+  drop_group_graphs(e);
+  for (auto& g : e->graphs) cudaGraphExecDestroy(g.second);
+  for (auto& g : e->graph_templates) cudaGraphDestroy(g.second);
+  e->graphs.clear();
+  e->graph_templates.clear();
+}
+
 // Retires the oldest batch in flight once its stream has passed it:
 // blocking waits for it, otherwise a batch not yet done is left alone and
 // false returned. Reports a fault word a tensor-core transform set.
@@ -896,6 +926,8 @@ void exogcm_destroy(exogcm_engine* e) {
     cudaFreeHost(b.fault_host);
   }
   if (e->stream) cudaStreamDestroy(e->stream);
+  e->setup_device.reset();
+  cudaFreeHost(e->upload_stage);
   delete e;
 }
 
@@ -905,9 +937,14 @@ int exogcm_configure(exogcm_engine* e, int slot, const exogcm_planet* planet, co
     check_slot(e, slot);
     if (planet->truncation != e->d.T || planet->levels != e->d.L)
       throw Error(EXOGCM_EINVAL, "planet resolution differs from the engine's");
+    SetupDevice* dev = nullptr;
+    if (e->setup_on_device) {
+      if (!e->setup_device) e->setup_device = make_setup_device();
+      dev = e->setup_device.get();
+    }
     if (!e->shared_ready) {
       retire_all(e);
-      e->shared_setup = build_shared(e->d.T, planet->filter_kind, planet->filter_gp, planet->filter_sp);
+      e->shared_setup = build_shared(e->d.T, planet->filter_kind, planet->filter_gp, planet->filter_sp, dev);
       upload_shared(e, e->shared_setup);
       if (e->mode >= 1) autotune(e);
       e->filter_kind = planet->filter_kind;
@@ -919,27 +956,65 @@ int exogcm_configure(exogcm_engine* e, int slot, const exogcm_planet* planet, co
     }
     // The host set-up runs while batches already submitted step on the
     // device; the slot's upload waits for them.
-    PlanetSetup ps = build_planet(*planet, *boundary, e->shared_setup);
-    retire_all(e);
-    zero_slot(e, slot);
+    PlanetSetup ps = build_planet(*planet, *boundary, e->shared_setup, dev);
+    // Every field and the slot's tables go through one pinned staging area,
+    // converted to float (Fourier fields to the m-major layout) before the
+    // in-flight batches are retired, then copied with one synchronisation.
+    size_t need = e->to.stride + (sizeof(PlanetConst) + sizeof(float) - 1) / sizeof(float);
+    for (auto& kv : ps.state) {
+      const FieldInfo& fi = field(e, kv.first.c_str());
+      if (kv.second.size() != fi.plane * fi.count)
+        throw Error(EXOGCM_EINVAL, "set-up field " + kv.first + " has the wrong size");
+      need += fi.plane * fi.count;
+    }
+    if (need > e->upload_stage_floats) {
+      retire_all(e);
+      check(cudaStreamSynchronize(e->stream), "staging");
+      cudaFreeHost(e->upload_stage);
+      e->upload_stage = nullptr;
+      e->upload_stage_floats = 0;
+      check(cudaMallocHost(&e->upload_stage, need * sizeof(float)), "pinned staging");
+      e->upload_stage_floats = need;
+    }
+    float* stage = e->upload_stage;
+    std::vector<std::pair<const FieldInfo*, float*>> staged;
+    std::vector<float> plain;
     for (auto& kv : ps.state) {
       const FieldInfo& fi = field(e, kv.first.c_str());
       const size_t n = fi.plane * fi.count;
-      if (kv.second.size() != n) throw Error(EXOGCM_EINVAL, "set-up field " + kv.first + " has the wrong size");
-      std::vector<float> f(kv.second.begin(), kv.second.end());
-      copy_field(e, fi, slot, f.data(), true);
+      if (e->mode >= 1 && fi.shape == 'F') {
+        plain.assign(kv.second.begin(), kv.second.end());
+        fourier_to_m_major(e->d, plain.data(), stage, fi.count);
+      } else {
+        for (size_t i = 0; i < n; ++i) stage[i] = (float)kv.second[i];
+      }
+      staged.push_back({&fi, stage});
+      stage += n;
     }
-    upload_slot_tables(e, slot, ps);
-    int zero = 0;
-    check(cudaMemcpy(e->flags + slot, &zero, sizeof(int), cudaMemcpyHostToDevice), "flags");
-    check(cudaMemset(e->budget + (size_t)slot * kBudgetStride, 0, kBudgetStride * sizeof(double)), "budgets");
+    fill_slot_tables(e, ps, stage);
+    retire_all(e);
+    zero_slot(e, slot);
+    for (auto& f : staged) {
+      const FieldInfo& fi = *f.first;
+      float* base = e->arena + fi.offset + (size_t)slot * fi.plane;
+      check(cudaMemcpy2DAsync(base, fi.plane * e->d.S * sizeof(float), f.second, fi.plane * sizeof(float),
+                              fi.plane * sizeof(float), fi.count, cudaMemcpyHostToDevice, e->stream),
+            "write field");
+    }
+    upload_slot_tables(e, slot, ps, stage);
+    check(cudaMemsetAsync(e->flags + slot, 0, sizeof(int), e->stream), "flags");
+    check(cudaMemsetAsync(e->budget + (size_t)slot * kBudgetStride, 0, kBudgetStride * sizeof(double), e->stream),
+          "budgets");
     if (e->avg)
-      for (int pl = 0; pl < e->d.P; ++pl)
-        check(cudaMemset(e->avg + ((size_t)pl * e->d.S + slot) * e->d.NHOR, 0, e->d.NHOR * sizeof(double)),
-              "averages");
+      check(cudaMemset2DAsync(e->avg + (size_t)slot * e->d.NHOR, e->d.S * e->d.NHOR * sizeof(double), 0,
+                              e->d.NHOR * sizeof(double), e->d.P, e->stream),
+            "averages");
+    bool storm_before = false;
+    for (const Slot& o : e->slots) storm_before = storm_before || o.storm;
     Slot& s = e->slots[slot];
     s = Slot{};
     s.active = true;
+    s.storm = ps.consts.at("NSTORMDIAG") > 0;
     s.step = ps.start_step;
     s.carbon_step = 0;
     s.startup_left = ps.nkits;
@@ -948,16 +1023,24 @@ int exogcm_configure(exogcm_engine* e, int slot, const exogcm_planet* planet, co
       s.delt[k] = ps.delt[k];
     }
     s.cal = ps.cal;
+    bool storm_after = false;
+    for (const Slot& o : e->slots) storm_after = storm_after || o.storm;
+    // The batch graphs hold whether the storm diagnostics launch.
+    if (storm_after != storm_before) drop_graphs(e);
     check(cudaStreamSynchronize(e->stream), "configure");
   });
 }
 
-int exogcm_setup_preview(const exogcm_planet* planet, const exogcm_boundary* boundary, const char* name,
-                         double* values, size_t* count) {
+namespace {
+int setup_preview(const exogcm_planet* planet, const exogcm_boundary* boundary, const char* name, double* values,
+                  size_t* count, bool on_device) {
   return guard([&] {
     if (!planet || !boundary || !name || !count) throw Error(EXOGCM_EINVAL, "null argument");
-    const SharedSetup sh = build_shared(planet->truncation, planet->filter_kind, planet->filter_gp, planet->filter_sp);
-    const PlanetSetup ps = build_planet(*planet, *boundary, sh);
+    std::unique_ptr<SetupDevice> dev;
+    if (on_device) dev = make_setup_device();
+    const SharedSetup sh =
+        build_shared(planet->truncation, planet->filter_kind, planet->filter_gp, planet->filter_sp, dev.get());
+    const PlanetSetup ps = build_planet(*planet, *boundary, sh, dev.get());
     const std::string n(name);
     const size_t colon = n.find(':');
     if (colon == std::string::npos) throw Error(EXOGCM_EINVAL, "name needs a kind: prefix");
@@ -1002,6 +1085,24 @@ int exogcm_setup_preview(const exogcm_planet* planet, const exogcm_boundary* bou
       std::copy(out.begin(), out.end(), values);
     }
     *count = out.size();
+  });
+}
+}  // namespace
+
+int exogcm_setup_preview(const exogcm_planet* planet, const exogcm_boundary* boundary, const char* name,
+                         double* values, size_t* count) {
+  return setup_preview(planet, boundary, name, values, count, false);
+}
+
+int exogcm_setup_preview_device(const exogcm_planet* planet, const exogcm_boundary* boundary, const char* name,
+                                double* values, size_t* count) {
+  return setup_preview(planet, boundary, name, values, count, true);
+}
+
+int exogcm_setup_on_device(exogcm_engine* e, int enable) {
+  return guard([&] {
+    if (!e) throw Error(EXOGCM_EINVAL, "null engine");
+    e->setup_on_device = enable != 0;
   });
 }
 
@@ -1186,11 +1287,7 @@ int exogcm_averages_enable(exogcm_engine* e, int enable) {
       return;
     }
     // The batch graphs hold the averages pointer: capture them again.
-    drop_group_graphs(e);
-    for (auto& g : e->graphs) cudaGraphExecDestroy(g.second);
-    for (auto& g : e->graph_templates) cudaGraphDestroy(g.second);
-    e->graphs.clear();
-    e->graph_templates.clear();
+    drop_graphs(e);
   });
 }
 
@@ -1545,7 +1642,8 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
           // the full step's other column kernels and its fused ones (timed
           // for the fusion choice; no byte count)
           {"fixer_apply", 0}, {"surflx", 0}, {"solang_mko3", 0}, {"mkdca", 0}, {"soil", 0}, {"land_surface", 0},
-          {"sea_ice", 0}, {"sea", 0}, {"carbon", 0}, {"fused_fixer_flux_solang", 0}, {"fused_kuo_mkdca", 0},
+          {"sea_ice", 0}, {"sea", 0}, {"carbon", 0}, {"storm", 0}, {"fused_fixer_flux_solang", 0},
+          {"fused_kuo_mkdca", 0},
           {"fused_rain_soil", 0}, {"fused_land_seaice", 0}, {"fused_sea_carbon", 0},
       };
       auto it = per_column.find(k);

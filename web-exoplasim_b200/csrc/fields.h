@@ -81,7 +81,8 @@
   X(CRHOS) X(CRHOSN) X(CPI) X(CKAPI) X(CKAPSN) X(CLFI) X(CLFSN) X(DTMIX) X(CPS) X(CHARNOCK)        \
   X(DZ0SEA) X(DZ0ICE) X(DRHSSEA) X(DRHSICE) X(ALBSEA) X(ALBICE) X(DICEALBMX1) X(DICEALBMX2)        \
   X(DICEALBMN1) X(DICEALBMN2) X(NCARBON) X(NSUPPLY) X(TIMEWEIGHT) X(CO2EARTH) X(BETA) X(KACT)      \
-  X(PEARTH) X(WMAX) X(VEARTH) X(PLARAD) X(RAD_EARTHSQ) X(JET) X(SIGMA_LOW)
+  X(PEARTH) X(WMAX) X(VEARTH) X(PLARAD) X(RAD_EARTHSQ) X(JET) X(SIGMA_LOW) X(NSTORMDIAG) X(CKCD)    \
+  X(VITHRESH)
 
 // Per-planet constant tables (dynamics set-up, physics level constants):
 // name, element count in terms of L (levels), NRSP, NTRU.

@@ -89,6 +89,8 @@ void phy_radiation(const Model& m, cudaStream_t st);
 void phy_precipitation_columns(const Model& m, cudaStream_t st);
 void phy_surface(const Model& m, cudaStream_t st);
 void phy_carbon(const Model& m, cudaStream_t st);
+// hurricanestep (physics/storm/wgsl/storm.wgsl), for slots with NSTORMDIAG > 0.
+void phy_storm(const Model& m, cudaStream_t st);
 // The full step's fused physics (see physics.cu): fixer through radiation,
 // and (after the precipitation transform) precipitation through carbon.
 void phy_fused_through_radiation(const Model& m, cudaStream_t st);

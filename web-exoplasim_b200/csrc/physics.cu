@@ -2124,7 +2124,11 @@ bool phy_launch_one(const Model& m, const std::string& kernel, cudaStream_t st) 
   const int L = m.d.L;
   if (phy_flux_launch_one(m, kernel, st))
     return true;
-  else if (kernel == "swr")
+  else if (kernel == "storm") {
+    Model on = m;
+    on.storm = 1;
+    phy_storm(on, st);
+  } else if (kernel == "swr")
     by_levels<Swr>(L, m, st);
   else if (kernel == "lwr_radstep")
     by_levels<LwrRadstep>(L, m, st);

@@ -85,6 +85,8 @@ std::map<std::string, Vec> legini(const Vec& sines, const Vec& weights, int T) {
   const int modes = (T + 1) * (T + 2) / 2;
   std::map<std::string, Vec> out;
   for (const char* k : {"qi", "qj", "qc", "qe", "qm", "qq", "qu", "qv"}) out[k] = Vec((size_t)nlat * modes, 0);
+  Vec &qi = out["qi"], &qj = out["qj"], &qc = out["qc"], &qe = out["qe"], &qm = out["qm"], &qq = out["qq"],
+      &qu = out["qu"], &qv = out["qv"];
   Vec pli(modes + 1, 0), pld(modes + 1, 0);
   for (int lat = 0; lat < nlat; ++lat) {
     const double sin = sines[lat], weight = weights[lat];
@@ -127,14 +129,14 @@ std::map<std::string, Vec> legini(const Vec& sines, const Vec& weights, int T) {
         const double invdeg = n > 0 ? 1.0 / ((double)n * (n + 1)) : 0.0;
         const size_t at = (size_t)lat * modes + w;
         const double p = pli[w + 1], d = pld[w + 1];
-        out["qi"][at] = p;
-        out["qj"][at] = d;
-        out["qc"][at] = p * weight;
-        out["qu"][at] = p * invdeg * m;
-        out["qv"][at] = d * invdeg;
-        out["qe"][at] = d * wocs;
-        out["qq"][at] = p * wocs * n * (n + 1) * 0.5;
-        out["qm"][at] = p * wocs * m;
+        qi[at] = p;
+        qj[at] = d;
+        qc[at] = p * weight;
+        qu[at] = p * invdeg * m;
+        qv[at] = d * invdeg;
+        qe[at] = d * wocs;
+        qq[at] = p * wocs * n * (n + 1) * 0.5;
+        qm[at] = p * wocs * m;
         w++;
       }
   }
@@ -194,6 +196,23 @@ Vec analyse(const SharedSetup& sh, const double* grid) {
       }
   }
   return sp;
+}
+
+// `planes` grids [plane][points] -> spectra [plane][2 * modes], on the set-up
+// device when there is one.
+Vec analyse_planes(const SharedSetup& sh, const double* grids, int planes, SetupDevice* device) {
+  const int modes = (sh.truncation + 1) * (sh.truncation + 2) / 2;
+  const size_t points = (size_t)sh.nlat * sh.nlon;
+  Vec out((size_t)planes * 2 * modes);
+  if (device) {
+    device->analyse(sh, grids, planes, out.data());
+    return out;
+  }
+  for (int p = 0; p < planes; ++p) {
+    const Vec sp = analyse(sh, grids + p * points);
+    std::copy(sp.begin(), sp.end(), out.begin() + (size_t)p * 2 * modes);
+  }
+  return out;
 }
 
 // ---------------------------------------------------------------- calendar
@@ -544,8 +563,9 @@ Vec invert(Vec a, int n) {
   return inverse;
 }
 
-// dynamics/setup/index.ts:213-239 (makebm).
-Vec makebm(const Dyn& s, int T, double delt) {
+// dynamics/setup/index.ts:213-239 (makebm): the matrix before the
+// diagonal term 1 / (n (n + 1)), then the inverse of each degree's.
+Vec makebm_base(const Dyn& s, double delt) {
   const int n = (int)s.t0.size();
   const double d2 = delt * delt;
   Vec base((size_t)n * n);
@@ -555,6 +575,10 @@ Vec makebm(const Dyn& s, int T, double delt) {
       for (int k = 0; k < n; ++k) dot += s.g[(size_t)l1 * n + k] * s.tau[(size_t)k * n + l2];
       base[(size_t)l1 * n + l2] = d2 * (s.t0[l1] * s.dsigma[l2] + dot);
     }
+  return base;
+}
+
+Vec makebm(const Vec& base, int n, int T) {
   Vec bm1((size_t)n * n * T);
   for (int degree = 1; degree <= T; ++degree) {
     Vec mat = base;
@@ -731,7 +755,7 @@ Vec ice_thickness(const Vec& cover, int nlat, int nlon) {
 
 }  // namespace
 
-SharedSetup build_shared(int truncation, int filter_kind, int filter_gp, int filter_sp) {
+SharedSetup build_shared(int truncation, int filter_kind, int filter_gp, int filter_sp, SetupDevice* device) {
   SharedSetup sh;
   sh.truncation = truncation;
   sh.nlat = latitudes_for(truncation);
@@ -752,6 +776,10 @@ SharedSetup build_shared(int truncation, int filter_kind, int filter_gp, int fil
     }
   }
   filters(truncation, filter_kind, filter_gp, filter_sp, 8, 8, 15, sh.g2s, sh.s2g);
+  if (device) {
+    device->legini(sh.sines, sh.weights, truncation, sh.g2s, sh.s2g, sh.q, sh.qc_unfiltered);
+    return sh;
+  }
   auto tabs = legini(sh.sines, sh.weights, truncation);
   sh.qc_unfiltered = tabs["qc"];
   const int modes = (truncation + 1) * (truncation + 2) / 2;
@@ -772,7 +800,8 @@ SharedSetup build_shared(int truncation, int filter_kind, int filter_gp, int fil
   return sh;
 }
 
-PlanetSetup build_planet(const exogcm_planet& p, const exogcm_boundary& b, const SharedSetup& sh) {
+PlanetSetup build_planet(const exogcm_planet& p, const exogcm_boundary& b, const SharedSetup& sh,
+                         SetupDevice* device) {
   if (p.star_temperature_k > 0)
     throw std::invalid_argument("stellar-spectrum albedo split (star temperature) is not supported");
   if (p.levels != 5 && p.levels != 10) throw std::invalid_argument("levels must be 5 or 10");
@@ -898,7 +927,7 @@ PlanetSetup build_planet(const exogcm_planet& p, const exogcm_boundary& b, const
   }
   Vec duroff, dvroff;
   runoff(doro, dls, nlat, nlon, sh.sines, pm, duroff, dvroff);
-  Vec so = analyse(sh, doro.data());
+  Vec so = analyse_planes(sh, doro.data(), 1, device);
   for (double& v : so) v /= (pm.cv * pm.cv);
   if (nglacier == 1)
     for (int h = 0; h < points; ++h)
@@ -971,12 +1000,20 @@ PlanetSetup build_planet(const exogcm_planet& p, const exogcm_boundary& b, const
   Vec sr = setzt(dyn, T, pm);
   out.nkits = std::max(pm.nkits, 1);
   if (out.nkits > 3) throw std::invalid_argument("more than 3 start-up steps");
-  Vec bm1((size_t)4 * T * L * L, 0);
+  Vec bm1((size_t)4 * T * L * L, 0), bases((size_t)4 * L * L);
   for (int k = 0; k <= 3; ++k) {
     out.deltsec[k] = pm.day_24hr / pm.mtspd / std::pow(2.0, k);
     out.delt[k] = TWOPI / pm.ntspd / std::pow(2.0, k);
-    Vec b1 = makebm(dyn, T, out.delt[k]);
-    std::copy(b1.begin(), b1.end(), bm1.begin() + (size_t)k * T * L * L);
+    const Vec base = makebm_base(dyn, out.delt[k]);
+    std::copy(base.begin(), base.end(), bases.begin() + (size_t)k * L * L);
+  }
+  if (device) {
+    device->makebm(bases.data(), L, T, bm1.data());
+  } else {
+    for (int k = 0; k <= 3; ++k) {
+      const Vec b1 = makebm(Vec(bases.begin() + (size_t)k * L * L, bases.begin() + (size_t)(k + 1) * L * L), L, T);
+      std::copy(b1.begin(), b1.end(), bm1.begin() + (size_t)k * T * L * L);
+    }
   }
   auto& tb = out.tables;
   tb["t0"] = dyn.t0;
@@ -1110,69 +1147,77 @@ PlanetSetup build_planet(const exogcm_planet& p, const exogcm_boundary& b, const
   };
   // rainini's clwfac with the default clwcrit1 = -0.1 < clwcrit2 = 0.
   k["CLWFAC"] = -1.0;
+  // hurricane_namelist (setup/index.ts:107-113; defaults CKCD 0.9, VITHRESH
+  // 0.145); RD and OMEGA are GASCON and WW.
+  k["NSTORMDIAG"] = p.storm_diagnostics ? 1 : 0;
+  k["CKCD"] = p.storm_ckcd > 0 ? p.storm_ckcd : 0.9;
+  k["VITHRESH"] = p.storm_vithresh > 0 ? p.storm_vithresh : 0.145;
 
   // ---- initial state: the synthetic atmosphere transformed in f64, plus surfini's fields
   auto& st = out.state;
   Vec stv((size_t)L * nrsp, 0), sqv((size_t)L * nrsp, 0), szv((size_t)L * nrsp, 0);
-  Vec tmp(points);
-  for (int l = 0; l < L; ++l) {
-    for (int h = 0; h < points; ++h) tmp[h] = b.t_init[(size_t)l * points + h] / pm.ct - dyn.t0[l];
-    Vec a = analyse(sh, tmp.data());
-    std::copy(a.begin(), a.end(), stv.begin() + (size_t)l * nrsp);
-    Vec q = analyse(sh, b.q_init + (size_t)l * points);
-    std::copy(q.begin(), q.end(), sqv.begin() + (size_t)l * nrsp);
-    szv[(size_t)l * nrsp + 2] = pm.plavor;
+  {
+    // The L temperature planes then the L humidity planes, analysed together.
+    Vec grids((size_t)2 * L * points);
+    for (int l = 0; l < L; ++l)
+      for (int h = 0; h < points; ++h)
+        grids[(size_t)l * points + h] = b.t_init[(size_t)l * points + h] / pm.ct - dyn.t0[l];
+    std::copy(b.q_init, b.q_init + (size_t)L * points, grids.begin() + (size_t)L * points);
+    const Vec spec = analyse_planes(sh, grids.data(), 2 * L, device);
+    std::copy(spec.begin(), spec.begin() + (size_t)L * nrsp, stv.begin());
+    std::copy(spec.begin() + (size_t)L * nrsp, spec.end(), sqv.begin());
+    for (int l = 0; l < L; ++l) szv[(size_t)l * nrsp + 2] = pm.plavor;
   }
   Vec spv(nrsp, 0);
   st["sp"] = spv;
-  st["spm"] = spv;
+  st["spm"] = std::move(spv);
   st["st"] = stv;
-  st["stm"] = stv;
+  st["stm"] = std::move(stv);
   st["sz"] = szv;
-  st["szm"] = szv;
+  st["szm"] = std::move(szv);
   st["sd"] = Vec((size_t)L * nrsp, 0);
   st["sdm"] = Vec((size_t)L * nrsp, 0);
   st["sq"] = sqv;
-  st["sqm"] = sqv;
+  st["sqm"] = std::move(sqv);
   st["dls"] = dls;
-  st["dz0"] = dz0;
-  st["drhs"] = drhs;
-  st["dwatc"] = dwatc;
+  st["dz0"] = std::move(dz0);
+  st["drhs"] = std::move(drhs);
+  st["dwatc"] = std::move(dwatc);
   st["dqco2"] = Vec((size_t)L * points, co2 > 0 ? co2 : 0);
   st["co2"] = {co2};
-  st["dalb"] = dalb;
-  st["dsalb"] = dsalb;
-  st["dicec"] = dicec;
-  st["diced"] = diced;
-  st["dmld"] = dmld;
-  st["dforest"] = dforest;
-  st["dglac"] = dglac;
-  st["dpersist"] = dpersist;
-  st["dwmax"] = dwmax;
-  st["dsnow"] = dsnow;
+  st["dalb"] = std::move(dalb);
+  st["dsalb"] = std::move(dsalb);
+  st["dicec"] = std::move(dicec);
+  st["diced"] = std::move(diced);
+  st["dmld"] = std::move(dmld);
+  st["dforest"] = std::move(dforest);
+  st["dglac"] = std::move(dglac);
+  st["dpersist"] = std::move(dpersist);
+  st["dwmax"] = std::move(dwmax);
+  st["dsnow"] = std::move(dsnow);
   st["dtsoil"] = soilf[0];
   st["dtd2"] = soilf[1];
   st["dtd3"] = soilf[2];
   st["dtd4"] = soilf[3];
   st["dtd5"] = soilf[4];
-  st["dt"] = dt;
-  st["dq"] = dq;
-  st["land_dts"] = land_dts;
-  st["land_dtsm"] = land_dtsm;
-  st["land_dqs"] = land_dqs;
-  st["duroff"] = duroff;
-  st["dvroff"] = dvroff;
+  st["dt"] = std::move(dt);
+  st["dq"] = std::move(dq);
+  st["land_dts"] = std::move(land_dts);
+  st["land_dtsm"] = std::move(land_dtsm);
+  st["land_dqs"] = std::move(land_dqs);
+  st["duroff"] = std::move(duroff);
+  st["dvroff"] = std::move(dvroff);
   st["darea"] = roww;
-  st["dsnowt"] = dsnowt;
-  st["dsnowz"] = dsnowz;
-  st["dz0climo"] = dz0climo;
-  st["dalbclim"] = dalbclim;
-  st["dalbclim1"] = dalbclim1;
-  st["dalbclim2"] = dalbclim2;
-  st["dsoilt"] = dsoilt;
-  st["dalbcl"] = dalbcl;
-  st["dalbcl1"] = dalbcl1;
-  st["dalbcl2"] = dalbcl2;
+  st["dsnowt"] = std::move(dsnowt);
+  st["dsnowz"] = std::move(dsnowz);
+  st["dz0climo"] = std::move(dz0climo);
+  st["dalbclim"] = std::move(dalbclim);
+  st["dalbclim1"] = std::move(dalbclim1);
+  st["dalbclim2"] = std::move(dalbclim2);
+  st["dsoilt"] = std::move(dsoilt);
+  st["dalbcl"] = std::move(dalbcl);
+  st["dalbcl1"] = std::move(dalbcl1);
+  st["dalbcl2"] = std::move(dalbcl2);
   st["dagg"] = Vec(points, p.initial_growth);
   st["dgrow"] = Vec(points, 1.0);
   st["dsc"] = Vec(points, 1.0);
@@ -1180,25 +1225,25 @@ PlanetSetup build_planet(const exogcm_planet& p, const exogcm_boundary& b, const
   st["xts"] = yclsst2;
   st["xsst"] = yclsst2;
   st["xmld"] = ymld;
-  st["xls"] = xls;
-  st["xiced"] = xiced;
-  st["xicec"] = xicec;
-  st["xgw"] = roww;
-  st["xclsst2"] = xclsst2;
-  st["xclicec2"] = xclicec2;
-  st["xcliced2"] = xcliced2;
-  st["xclssto"] = xclssto;
-  st["xclsst"] = xclsst;
-  st["xclicec"] = xclicec;
-  st["xcliced"] = xcliced;
+  st["xls"] = std::move(xls);
+  st["xiced"] = std::move(xiced);
+  st["xicec"] = std::move(xicec);
+  st["xgw"] = std::move(roww);
+  st["xclsst2"] = std::move(xclsst2);
+  st["xclicec2"] = std::move(xclicec2);
+  st["xcliced2"] = std::move(xcliced2);
+  st["xclssto"] = std::move(xclssto);
+  st["xclsst"] = std::move(xclsst);
+  st["xclicec"] = std::move(xclicec);
+  st["xcliced"] = std::move(xcliced);
   st["ysst"] = yclsst2;
-  st["ymld"] = ymld;
-  st["yls"] = dls;
-  st["yclsst2"] = yclsst2;
-  st["yclsst"] = yclsst;
-  st["sea_dts"] = sea_dts;
-  st["sea_dqs"] = sea_dqs;
-  st["sea_dsst"] = sea_dsst;
+  st["ymld"] = std::move(ymld);
+  st["yls"] = std::move(dls);
+  st["yclsst2"] = std::move(yclsst2);
+  st["yclsst"] = std::move(yclsst);
+  st["sea_dts"] = std::move(sea_dts);
+  st["sea_dqs"] = std::move(sea_dqs);
+  st["sea_dsst"] = std::move(sea_dsst);
   (void)psurf_nl;
 
   // ---- calendar (setup/index.ts:304-318, calendar/index.ts:37-126 for a fixed orbit)

@@ -2,6 +2,7 @@
 // physics modules' *ini, initpm/initsi/makebm/setzt, surfini) and CALENDAR.
 #pragma once
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -61,8 +62,34 @@ struct PlanetSetup {
   int filter_kind, filter_gp, filter_sp;
 };
 
-SharedSetup build_shared(int truncation, int filter_kind, int filter_gp, int filter_sp);
-PlanetSetup build_planet(const exogcm_planet& planet, const exogcm_boundary& boundary, const SharedSetup& shared);
+// The set-up's heavy FP64 loops on a device (setup_device.cu). Each call
+// keeps the host loop's order of operations and is compiled without
+// multiply-add contraction, so it returns the host's numbers bit for bit.
+class SetupDevice {
+ public:
+  virtual ~SetupDevice() = default;
+  // legini and the filters of one resolution (legendre/index.ts:29-136):
+  // the eight filtered tables [lat][mode] into `q` and the unfiltered qc.
+  virtual void legini(const Vec& sines, const Vec& weights, int truncation, const Vec& g2s, const Vec& s2g,
+                      std::map<std::string, Vec>& q, Vec& qc_unfiltered) = 0;
+  // Grid -> spectral for `planes` grids [plane][lat][lon] in FP64
+  // (fourier/index.ts:95-115 then legendre/index.ts:334-361) into
+  // `spectra` [plane][2 * modes].
+  virtual void analyse(const SharedSetup& shared, const double* grids, int planes, double* spectra) = 0;
+  // makebm's inverses (dynamics/setup/index.ts:154-239) of the four phases:
+  // `base` holds each phase's n x n matrix before the diagonal term, `bm1`
+  // receives [phase][degree - 1][n][n].
+  virtual void makebm(const double* base, int n, int truncation, double* bm1) = 0;
+};
+
+// A set-up device on the current CUDA device (nullptr-free; throws on a
+// CUDA error).
+std::unique_ptr<SetupDevice> make_setup_device();
+
+// With `device` null every loop runs on the host.
+SharedSetup build_shared(int truncation, int filter_kind, int filter_gp, int filter_sp, SetupDevice* device = nullptr);
+PlanetSetup build_planet(const exogcm_planet& planet, const exogcm_boundary& boundary, const SharedSetup& shared,
+                         SetupDevice* device = nullptr);
 StepValues step_values(const Calendar& cal, long step, int carbon_step);
 
 }  // namespace exogcm

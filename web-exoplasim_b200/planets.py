@@ -34,7 +34,7 @@ BASE_CONFIG = dict(
     fixedOrbit=True, keplerian=False, wetSoil=False, vegetation=2, initialGrowth=0.5,
     glaciersEnabled=True, glaciersMinDepthM=2.0, glaciersInitialHeightM=-1.0,
     physicsFilter=("gp", "exp", "sp"), timestepMinutes=45.0, pressureBar=1.011,
-    gasConstant=EARTH_GAS_CONSTANT, co2Ppm=360.0, ozone=True, soilDepthScale=1.0,
+    gasConstant=EARTH_GAS_CONSTANT, co2Ppm=360.0, ozone=True, soilDepthScale=1.0, stormclim=False,
 )
 
 LATITUDES = {21: 32, 42: 64, 63: 96}

@@ -80,9 +80,11 @@ def _field_names():
 class Group:
     """One batched engine (a block of slots of one resolution)."""
 
-    def __init__(self, truncation, levels, slots, chunk, mode=1):
+    def __init__(self, truncation, levels, slots, chunk, mode=1, setup_on_device=True):
         self.truncation, self.levels, self.slots, self.chunk = truncation, levels, slots, chunk
         self.engine = pkg.Engine(truncation, levels, slots, mode=mode)
+        self.engine.setup_on_device(setup_on_device)
+        self.configure_s: list[float] = []  # wall time of each exogcm_configure (set-up + upload)
         self.free = deque(range(slots))
         self.running: dict[int, Request] = {}
         self.stop_step: dict[int, int] = {}
@@ -95,7 +97,9 @@ class Group:
         if planet is None:
             planet = planets_mod.make_planet(req.seed, truncation=req.truncation, levels=req.levels,
                                              timestepMinutes=STEP_MINUTES[req.truncation], **req.overrides)
+        t = time.perf_counter()
         self.engine.configure(slot, planet)
+        self.configure_s.append(time.perf_counter() - t)
         steps_per_day = 1440.0 / STEP_MINUTES[req.truncation]
         req.steps = max(1, int(round(req.days * steps_per_day)))
         start = self.engine.slot_info(slot)["step"]
@@ -149,10 +153,12 @@ class Server:
     HBM budget of B bytes shared by every resolution."""
 
     def __init__(self, capacity: dict | None = None, chunk: int = 16, keep_results: bool = True,
-                 budget_bytes: float | None = None, block: int = 32, mode: int = 1):
+                 budget_bytes: float | None = None, block: int = 32, mode: int = 1, setup_on_device: bool = True):
         self.chunk, self.mode, self.block = chunk, mode, block
-        self.blocks: list[Group] = [Group(key[0], key[1], n, chunk, mode) for key, n in (capacity or {}).items()
-                                    if n > 0]
+        self.setup_on_device = setup_on_device
+        self.blocks: list[Group] = [Group(key[0], key[1], n, chunk, mode, setup_on_device)
+                                    for key, n in (capacity or {}).items() if n > 0]
+        self.configure_s: list[float] = []  # of blocks already destroyed
         self.elastic = budget_bytes is not None
         self.budget = float(budget_bytes or 0.0)
         self.queue: deque[Request] = deque()
@@ -206,10 +212,11 @@ class Server:
             if not empty:
                 return None
             b = empty[0]
+            self.configure_s.extend(b.configure_s)
             b.close()
             self.blocks.remove(b)
             self.blocks_destroyed += 1
-        block = Group(key[0], key[1], n, self.chunk, self.mode)
+        block = Group(key[0], key[1], n, self.chunk, self.mode, self.setup_on_device)
         self.blocks.append(block)
         self.blocks_created += 1
         self.peak_bytes = max(self.peak_bytes, self.used_bytes())
@@ -281,6 +288,7 @@ class Server:
                 info = g.engine.slot_info(slot)
                 done_steps = req.steps - max(0, g.stop_step[slot] - info["step"])
                 partial += done_steps * STEP_MINUTES[g.truncation] / 1440.0
+        configure = np.array(self.configure_s + [t for b in self.blocks for t in b.configure_s])
         slots: dict = {}
         for b in self.blocks:
             k = f"T{b.truncation}L{b.levels}"
@@ -298,6 +306,9 @@ class Server:
             "blocks_created": self.blocks_created,
             "blocks_destroyed": self.blocks_destroyed,
             "peak_bytes": self.peak_bytes,
+            "setup_on_device": self.setup_on_device,
+            "configure_ms_p50": float(np.percentile(configure, 50)) * 1e3 if configure.size else None,
+            "configure_ms_p99": float(np.percentile(configure, 99)) * 1e3 if configure.size else None,
         }
 
     def close(self):
