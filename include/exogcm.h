@@ -204,6 +204,12 @@ int exogcm_budgets(exogcm_engine* engine, int slot, double* last, double* mean, 
 int exogcm_averages_enable(exogcm_engine* engine, int enable);
 int exogcm_averages_read(exogcm_engine* engine, int slot, float* mean, size_t count, long* samples, int reset);
 
+/* Calendar date of model step `step` for a slot's planet (calendar/date/
+ * index.ts:43-80; step < 0: the slot's current step): date[5] = year, month,
+ * day, hour, minute. The date a snapshot or checkpoint carries
+ * (types.ts GcmDate). */
+int exogcm_slot_date(exogcm_engine* engine, int slot, long step, int* date);
+
 /* Snapshot of a slot published during the last exogcm_step (the 101/76
  * fields of snapshot/index.ts, each NHOR values): returns the step it was
  * taken at in *step, or -1 when the slot did not publish. `values` may be
@@ -277,7 +283,10 @@ int exogcm_last_step_ms(exogcm_engine* engine, float* ms);
 int exogcm_time_kernel(exogcm_engine* engine, const char* kernel, int reps, float* ms, double* bytes);
 
 /* Launch shapes the autotuner chose for the optimized path's transforms at
- * the engine's first configure (plain path: the defaults): values[0] FFT
+ * the engine's first configure (plain path: the defaults; an engine of a
+ * shape - device, truncation, levels, slots, mode - the process tuned
+ * before reuses that choice, as it reuses the shared FP64 tables of a
+ * resolution): values[0] FFT
  * latitudes per block; [1], [2] sp2fc wavenumbers and planes per block;
  * [3], [4] the same for dv2uv; [5..8] forward Legendre planes per tile
  * for fc2sp, uv2dv, mktend's uv2dv and qtend. `count` must be at least 9.

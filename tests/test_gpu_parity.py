@@ -337,7 +337,8 @@ def test_bulk_snapshot_copy_overlaps_the_next_step():
 
 @pytest.mark.gpu
 def test_autotuned_shapes_leave_results_unchanged():
-    """Each engine times its own transform shapes at its first configure;
+    """The first engine of each shape (device, resolution, slots, mode) times
+    its transform shapes at its first configure, later ones reuse them;
     engines of 1 and 3 slots may pick different ones, and the shared planet
     must still step identically."""
     p = planets.make_planet(81, truncation=21, levels=10)

@@ -7,6 +7,7 @@ import pytest
 
 serving = importlib.import_module("web-exoplasim_b200.serving")
 runner = importlib.import_module("web-exoplasim_b200.runner")
+checkpoint = importlib.import_module("web-exoplasim_b200.checkpoint")
 planets = importlib.import_module("web-exoplasim_b200.planets")
 
 
@@ -64,7 +65,10 @@ def test_runner_publishes_pauses_checkpoints_and_stops():
     assert statuses[-1] == "finished", statuses
     assert [s.step for s in snaps][:3] == [0, 8, 16]
     assert all(np.all(np.isfinite(s.values)) for s in snaps)
-    assert saved and saved[0].startswith(b"GCM-WEBGPU-STATE\n")
+    # the format-21 container around the engine's restart file
+    assert saved and saved[0].startswith(checkpoint.MAGIC)
+    ckpt = checkpoint.decode(saved[0])
+    assert ckpt["meta"]["format"] == 21 and ckpt["restart"].startswith(b"GCM-WEBGPU-STATE\n")
 
 
 @pytest.mark.gpu

@@ -74,6 +74,7 @@ SIGNATURES = {
     "exogcm_setup_preview_device": (ctypes.c_int, [ctypes.POINTER(Planet), ctypes.POINTER(Boundary),
                                                    ctypes.c_char_p, _DP, ctypes.POINTER(ctypes.c_size_t)]),
     "exogcm_setup_on_device": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "exogcm_slot_date": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_long, ctypes.POINTER(ctypes.c_int)]),
     "exogcm_release": (ctypes.c_int, [_VP, ctypes.c_int]),
     "exogcm_step": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
     "exogcm_step_async": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
@@ -381,6 +382,13 @@ class Engine:
         n = ctypes.c_size_t()
         _check(_lib.exogcm_graph_launches(self.h, steps, ctypes.byref(n)))
         return n.value
+
+    def date(self, slot: int, step: int = -1) -> dict:
+        """GcmDate (year, month, day, hour, minute) of a model step of the
+        slot's planet; the slot's current step by default."""
+        out = (ctypes.c_int * 5)()
+        _check(_lib.exogcm_slot_date(self.h, slot, step, out))
+        return dict(zip(("year", "month", "day", "hour", "minute"), list(out)))
 
     def checkpoint_save(self, slot: int) -> bytes:
         buf, size = _VP(), ctypes.c_size_t()

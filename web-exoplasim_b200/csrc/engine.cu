@@ -25,6 +25,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/exogcm.h"
@@ -931,6 +932,43 @@ void exogcm_destroy(exogcm_engine* e) {
   delete e;
 }
 
+namespace {
+// Process-wide caches for the set-up of a new engine: the shared FP64 tables
+// of a resolution and filter setting, and the autotuned launch shapes of an
+// engine shape on a device (the shapes change no result). An elastic server
+// creating blocks of a resolution it served before pays neither again.
+std::mutex g_setup_cache_mutex;
+std::map<std::tuple<int, int, int, int>, SharedSetup> g_shared_cache;
+std::map<std::tuple<int, int, int, int, int>, Tuning> g_tuning_cache;
+
+SharedSetup cached_shared(int T, int kind, int gp, int sp, SetupDevice* dev) {
+  const auto key = std::make_tuple(T, kind, gp, sp);
+  {
+    std::lock_guard<std::mutex> lock(g_setup_cache_mutex);
+    auto it = g_shared_cache.find(key);
+    if (it != g_shared_cache.end()) return it->second;
+  }
+  SharedSetup sh = build_shared(T, kind, gp, sp, dev);
+  std::lock_guard<std::mutex> lock(g_setup_cache_mutex);
+  return g_shared_cache.emplace(key, std::move(sh)).first->second;
+}
+
+void cached_autotune(exogcm_engine* e) {
+  const auto key = std::make_tuple(e->device, e->d.T, e->d.L, e->d.S, e->mode);
+  {
+    std::lock_guard<std::mutex> lock(g_setup_cache_mutex);
+    auto it = g_tuning_cache.find(key);
+    if (it != g_tuning_cache.end()) {
+      e->tune = it->second;
+      return;
+    }
+  }
+  autotune(e);
+  std::lock_guard<std::mutex> lock(g_setup_cache_mutex);
+  g_tuning_cache[key] = e->tune;
+}
+}  // namespace
+
 int exogcm_configure(exogcm_engine* e, int slot, const exogcm_planet* planet, const exogcm_boundary* boundary) {
   return guard([&] {
     if (!e || !planet || !boundary) throw Error(EXOGCM_EINVAL, "null argument");
@@ -944,9 +982,9 @@ int exogcm_configure(exogcm_engine* e, int slot, const exogcm_planet* planet, co
     }
     if (!e->shared_ready) {
       retire_all(e);
-      e->shared_setup = build_shared(e->d.T, planet->filter_kind, planet->filter_gp, planet->filter_sp, dev);
+      e->shared_setup = cached_shared(e->d.T, planet->filter_kind, planet->filter_gp, planet->filter_sp, dev);
       upload_shared(e, e->shared_setup);
-      if (e->mode >= 1) autotune(e);
+      if (e->mode >= 1) cached_autotune(e);
       e->filter_kind = planet->filter_kind;
       e->filter_gp = planet->filter_gp;
       e->filter_sp = planet->filter_sp;
@@ -1097,6 +1135,16 @@ int exogcm_setup_preview(const exogcm_planet* planet, const exogcm_boundary* bou
 int exogcm_setup_preview_device(const exogcm_planet* planet, const exogcm_boundary* boundary, const char* name,
                                 double* values, size_t* count) {
   return setup_preview(planet, boundary, name, values, count, true);
+}
+
+int exogcm_slot_date(exogcm_engine* e, int slot, long step, int* date) {
+  return guard([&] {
+    if (!e || !date) throw Error(EXOGCM_EINVAL, "null argument");
+    check_slot(e, slot);
+    const Slot& s = e->slots[slot];
+    if (!s.active && s.cal.steps_per_day == 0) throw Error(EXOGCM_ESTATE, "slot was never configured");
+    calendar_date(s.cal, step < 0 ? s.step : step, date);
+  });
 }
 
 int exogcm_setup_on_device(exogcm_engine* e, int enable) {

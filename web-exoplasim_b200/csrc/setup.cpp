@@ -1282,6 +1282,15 @@ PlanetSetup build_planet(const exogcm_planet& p, const exogcm_boundary& b, const
 
 // stepper/index.ts:281-334 (values) with calendar/solar/index.ts:26-89,
 // radiation/index.ts:96-113, surface/index.ts:49-59 and carbon/index.ts:23-28.
+void calendar_date(const Calendar& cal, long step, int out[5]) {
+  const Date d = cal_date(step, cal.steps_per_day, cal.days_per_year, cal.step_minutes);
+  out[0] = (int)d.year;
+  out[1] = d.month;
+  out[2] = d.day;
+  out[3] = d.hour;
+  out[4] = d.minute;
+}
+
 StepValues step_values(const Calendar& cal, long step, int carbon_step) {
   StepValues v{};
   const double calendar_day = (double)(step % cal.steps_per_year) / cal.steps_per_year;

@@ -91,5 +91,8 @@ SharedSetup build_shared(int truncation, int filter_kind, int filter_gp, int fil
 PlanetSetup build_planet(const exogcm_planet& planet, const exogcm_boundary& boundary, const SharedSetup& shared,
                          SetupDevice* device = nullptr);
 StepValues step_values(const Calendar& cal, long step, int carbon_step);
+// The calendar date of a model step (calendar/date/index.ts:43-80):
+// year, month, day, hour, minute.
+void calendar_date(const Calendar& cal, long step, int out[5]);
 
 }  // namespace exogcm

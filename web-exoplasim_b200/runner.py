@@ -5,7 +5,8 @@ runner/types.ts:34-74 (GcmRunRequest, GcmRun, the status enum) and the
 WebGPU worker's loop (runner/webgpu/gcm.worker.ts:53-367): a run owns one
 engine slot on a worker thread, pumps batches of whole publish intervals,
 posts each published snapshot, pauses and resumes between batches, takes a
-checkpoint once the device is idle, and fails with the reference's messages
+checkpoint (the format-21 container, checkpoint.py) once the device is
+idle, and fails with the reference's messages
 ("GPU device lost: ...", "The model became unstable at step N",
 "This checkpoint's model state does not match ...").
 """
@@ -94,6 +95,7 @@ class GcmRun:
 
     def _work(self):
         pkg = importlib.import_module("web-exoplasim_b200")
+        checkpoint = importlib.import_module("web-exoplasim_b200.checkpoint")
         req = self.request
         cfg = req.planet.config
         try:
@@ -101,7 +103,10 @@ class GcmRun:
             engine.configure(0, req.planet)
             if req.restart is not None:
                 engine.step(3)  # a restarted run resumes in the main loop
-                engine.checkpoint_load(0, req.restart)
+                if bytes(req.restart[:len(checkpoint.MAGIC)]) == checkpoint.MAGIC:
+                    checkpoint.load(engine, 0, req.restart)  # the format-21 container
+                else:
+                    engine.checkpoint_load(0, req.restart)  # a bare restart file
             else:
                 engine.step(3)  # master's start-up steps at the start step's date
             info = engine.slot_info(0)
@@ -109,7 +114,7 @@ class GcmRun:
             if req.max_steps is not None:
                 engine.set_stop(0, start + req.max_steps)
             req.on_device("NVIDIA B200 (CUDA, sm_100a)")
-        except pkg.ExogcmError as err:
+        except (pkg.ExogcmError, checkpoint.CheckpointError) as err:
             self._fail(str(err))
             return
         except Exception as err:  # device unavailable and the like
@@ -121,7 +126,7 @@ class GcmRun:
             while not self._stop.is_set():
                 if self._checkpoint.is_set():
                     self._status("checkpointing")
-                    req.on_checkpoint(engine.checkpoint_save(0))
+                    req.on_checkpoint(checkpoint.save(engine, 0, req.planet))
                     self._checkpoint.clear()
                     self._status("paused" if self._paused.is_set() else "running")
                 if self._paused.is_set():
