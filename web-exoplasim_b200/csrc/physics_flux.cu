@@ -139,72 +139,115 @@ __global__ void __launch_bounds__(kBlock) k_surflx(Model m, const PlanetConst* _
 
 // physics/diffusion/wgsl/implicit.wgsl: ECHAM tridiagonal eliminations.
 // physics/surface-flux/wgsl/vdiff.wgsl: Richardson-number vertical diffusion.
-template <int NL>
+// HOLD: which levels of the tendencies dtdt, dqdt, dudt, dvdt hold values on
+// entry: 1 every level (stage replay, Model::zero_gdt), 0 only the lowest
+// (within a full step, where physics_in's zeros are taken as values and
+// surflx raised the lowest level), -1 decided at run time from zero_gdt.
+// With HOLD = 0 the other levels' tendencies are the constant 0 and need no
+// registers.
+// |(u, v)| with both squares rounded before the sum (no contraction), the
+// same wherever the speed is formed.
+__device__ __forceinline__ float wind_speed(float u, float v) {
+  return sqrtf(__fadd_rn(__fmul_rn(u, u), __fmul_rn(v, v)));
+}
+
+template <int NL, int HOLD = -1>
 __device__ __forceinline__ void b_vdiff(const Model& m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
   COLUMN_PROLOGUE
   const float* ds = tb + m.to.dsigma;
   const float* sh = tb + m.to.sigmah;
+  const float* skap = tb + m.to.vdiff_skap;
+  const float* skaph = tb + m.to.vdiff_skaph;
   const float D2 = P.deltsec2;
-  // Every field value used is read here, before the first store (the
-  // compiler cannot prove the fields distinct, so a store would order each
-  // later load after it). Within a full step only surflx's lowest level of
-  // the tendencies holds more than physics_in's zeros (Model::zero_gdt).
-  float zt[NL], zq[NL], zu[NL], zv[NL], zabsu[NL], zskap[NL], zskaph[NL];
-  float dtdt[NL], dqdt[NL], dudt[NL], dvdt[NL], dq[NL];
+  const bool all_held = HOLD < 0 ? m.zero_gdt != 0 : HOLD == 1;
+  // An incoming tendency: every level in stage replay; within a full step
+  // only the lowest holds more than physics_in's zeros (Model::zero_gdt).
+  auto tend = [&](const float* f, int l) { return all_held || l == NL - 1 ? f[l * SN + c] : 0.f; };
+  // The routine runs in three phases so that few level columns are live at
+  // once: the exchange coefficients, then humidity and temperature (whose
+  // profiles are then dropped), then the winds and the dissipative heating,
+  // whose inputs are read again (no field read here is written here). Each
+  // value is computed by the same expression as in one pass.
+  float zt[NL], zq[NL], kh[NL], km[NL];
+  {
+    float zabsu[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+      const size_t at = l * SN + c;
+      zt[l] = F.dt[at] + tend(F.dtdt, l) * D2;
+      zq[l] = F.dq[at] + tend(F.dqdt, l) * D2;
+      const float zu = F.du[at] + tend(F.dudt, l) * D2;
+      const float zv = F.dv[at] + tend(F.dvdt, l) * D2;
+      zabsu[l] = wind_speed(zu, zv);
+    }
+    const float zkonst1 = K.GA * D2 / K.GASCON;
+    const float zkonst2 = zkonst1 * K.GA / K.GASCON;
+    const float zkonst3 = zkonst2 * K.GA / K.GASCON;
+    const float moisture = 1.f / K.RDBRV - 1.f;
+    kh[NL - 1] = 0.f;
+    km[NL - 1] = 0.f;
+#pragma unroll
+    for (int l = 0; l < NL - 1; ++l) {
+      const int lp = l + 1;
+      const float sigmah = sh[l], dsigma = ds[l], dsigmap = ds[lp];
+      const float zmixh2 = tb[m.to.vdiff_mixh2 + l], zmixm2 = tb[m.to.vdiff_mixm2 + l];
+      const float zrdsig = tb[m.to.vdiff_rdsig + l];
+      const float zfac = zkonst3 * tb[m.to.vdiff_sigmah3 + l];
+      const float zzkfac = tb[m.to.vdiff_kfac + l];
+      const float zrthl = (dsigmap + dsigma) / (zt[l] * dsigmap + zt[lp] * dsigma);
+      const float zdvds = fmaxf(K.ZUMIN, fabsf(zabsu[l] - zabsu[lp])) * zrdsig;
+      const float zdthds =
+          (zt[l] * (1.f + moisture * zq[l]) / skap[l] - zt[lp] * (1.f + moisture * zq[lp]) / skap[lp]) * zrdsig;
+      const float zri = skaph[l] * K.GASCON * zdthds / (sigmah * zdvds * zdvds);
+      float zrifh, zrifm;
+      if (zri <= 0.f) {
+        const float dh = 1.f + 3.f * K.VDIFF_C * K.VDIFF_B * sqrtf(-1.f * zri) * zzkfac * zmixh2;
+        const float dm = 1.f + 3.f * K.VDIFF_C * K.VDIFF_B * sqrtf(-1.f * zri) * zzkfac * zmixm2;
+        zrifh = 1.f - 3.f * K.VDIFF_B * zri / dh;
+        zrifm = 1.f - 2.f * K.VDIFF_B * zri / dm;
+      } else {
+        const float zdenom = sqrtf(1.f + K.VDIFF_D * zri);
+        zrifh = 1.f / (1.f + 3.f * K.VDIFF_B * zri * zdenom);
+        zrifm = 1.f / (1.f + 2.f * K.VDIFF_B * zri / zdenom);
+      }
+      kh[l] = zfac * zmixh2 * zrifh * zdvds * zrthl * zrthl * zrthl;
+      km[l] = zfac * zmixm2 * zrifm * zdvds * zrthl * zrthl * zrthl;
+    }
+  }
+  // humidity, stored at once
+  {
+    float zqn[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) zqn[l] = zq[l];
+    diffuse<NL>(ds, zqn, kh);
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+      const size_t at = l * SN + c;
+      F.dqdt[at] = tend(F.dqdt, l) + __fdiv_rn(zqn[l] - zq[l], D2);
+    }
+  }
+  // temperature: its diffusion increment, stored with the heating below
+  float zdt[NL];
+  {
+    float zskap[NL], ztn[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+      zskap[l] = skap[l];
+      ztn[l] = zt[l];
+    }
+#pragma unroll
+    for (int l = 0; l < NL - 1; ++l) kh[l] = kh[l] * skaph[l];
+    diffuse_potential<NL>(ds, ztn, kh, zskap);
+#pragma unroll
+    for (int l = 0; l < NL; ++l) zdt[l] = __fdiv_rn(ztn[l] - zt[l], D2);
+  }
+  // winds and the dissipative heating
+  float zu[NL], zv[NL], zun[NL], zvn[NL];
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SN + c;
-    const bool held = m.zero_gdt || l == NL - 1;
-    dtdt[l] = held ? F.dtdt[at] : 0.f;
-    dqdt[l] = held ? F.dqdt[at] : 0.f;
-    dudt[l] = held ? F.dudt[at] : 0.f;
-    dvdt[l] = held ? F.dvdt[at] : 0.f;
-    dq[l] = F.dq[at];
-    zt[l] = F.dt[at] + dtdt[l] * D2;
-    zq[l] = dq[l] + dqdt[l] * D2;
-    zu[l] = F.du[at] + dudt[l] * D2;
-    zv[l] = F.dv[at] + dvdt[l] * D2;
-    zabsu[l] = sqrtf(zu[l] * zu[l] + zv[l] * zv[l]);
-    zskap[l] = tb[m.to.vdiff_skap + l];
-    zskaph[l] = tb[m.to.vdiff_skaph + l];
-  }
-  const float zkonst1 = K.GA * D2 / K.GASCON;
-  const float zkonst2 = zkonst1 * K.GA / K.GASCON;
-  const float zkonst3 = zkonst2 * K.GA / K.GASCON;
-  const float moisture = 1.f / K.RDBRV - 1.f;
-  float kh[NL], km[NL];
-  kh[NL - 1] = 0.f;
-  km[NL - 1] = 0.f;
-#pragma unroll
-  for (int l = 0; l < NL - 1; ++l) {
-    const int lp = l + 1;
-    const float sigmah = sh[l], dsigma = ds[l], dsigmap = ds[lp];
-    const float zmixh2 = tb[m.to.vdiff_mixh2 + l], zmixm2 = tb[m.to.vdiff_mixm2 + l];
-    const float zrdsig = tb[m.to.vdiff_rdsig + l];
-    const float zfac = zkonst3 * tb[m.to.vdiff_sigmah3 + l];
-    const float zzkfac = tb[m.to.vdiff_kfac + l];
-    const float zrthl = (dsigmap + dsigma) / (zt[l] * dsigmap + zt[lp] * dsigma);
-    const float zdvds = fmaxf(K.ZUMIN, fabsf(zabsu[l] - zabsu[lp])) * zrdsig;
-    const float zdthds =
-        (zt[l] * (1.f + moisture * zq[l]) / zskap[l] - zt[lp] * (1.f + moisture * zq[lp]) / zskap[lp]) * zrdsig;
-    const float zri = zskaph[l] * K.GASCON * zdthds / (sigmah * zdvds * zdvds);
-    float zrifh, zrifm;
-    if (zri <= 0.f) {
-      const float dh = 1.f + 3.f * K.VDIFF_C * K.VDIFF_B * sqrtf(-1.f * zri) * zzkfac * zmixh2;
-      const float dm = 1.f + 3.f * K.VDIFF_C * K.VDIFF_B * sqrtf(-1.f * zri) * zzkfac * zmixm2;
-      zrifh = 1.f - 3.f * K.VDIFF_B * zri / dh;
-      zrifm = 1.f - 2.f * K.VDIFF_B * zri / dm;
-    } else {
-      const float zdenom = sqrtf(1.f + K.VDIFF_D * zri);
-      zrifh = 1.f / (1.f + 3.f * K.VDIFF_B * zri * zdenom);
-      zrifm = 1.f / (1.f + 2.f * K.VDIFF_B * zri / zdenom);
-    }
-    kh[l] = zfac * zmixh2 * zrifh * zdvds * zrthl * zrthl * zrthl;
-    km[l] = zfac * zmixm2 * zrifm * zdvds * zrthl * zrthl * zrthl;
-  }
-  float zun[NL], zvn[NL];
-#pragma unroll
-  for (int l = 0; l < NL; ++l) {
+    zu[l] = F.du[at] + tend(F.dudt, l) * D2;
+    zv[l] = F.dv[at] + tend(F.dvdt, l) * D2;
     zun[l] = zu[l];
     zvn[l] = zv[l];
   }
@@ -213,39 +256,38 @@ __device__ __forceinline__ void b_vdiff(const Model& m, const PlanetConst* __res
 #pragma unroll
   for (int l = 0; l < NL; ++l) {
     const size_t at = l * SN + c;
-    F.dudt[at] = dudt[l] + __fdiv_rn(zun[l] - zu[l], D2);
-    F.dvdt[at] = dvdt[l] + __fdiv_rn(zvn[l] - zv[l], D2);
+    F.dudt[at] = tend(F.dudt, l) + __fdiv_rn(zun[l] - zu[l], D2);
+    F.dvdt[at] = tend(F.dvdt, l) + __fdiv_rn(zvn[l] - zv[l], D2);
   }
+  float heat[NL];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) heat[l] = tend(F.dtdt, l);
   if (K.NDHEAT != 0.f) {
     float zke[NL], zken[NL];
 #pragma unroll
-    for (int l = 0; l < NL; ++l) zke[l] = zken[l] = 0.5f * zabsu[l] * zabsu[l];
+    for (int l = 0; l < NL; ++l) {
+      const float zabsu = wind_speed(zu[l], zv[l]);
+      zke[l] = zken[l] = 0.5f * zabsu * zabsu;
+    }
     diffuse<NL>(ds, zken, km);
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
-      const float zdtdt = -((zun[l] * zun[l] - zu[l] * zu[l] + zvn[l] * zvn[l] - zv[l] * zv[l]) / D2 -
-                            (zken[l] - zke[l]) / D2) * 0.5f / K.ACPD / (1.f + K.ADV * dq[l]);
-      dtdt[l] = dtdt[l] + zdtdt;
+      const float dq = F.dq[l * SN + c];
+      // zun^2 - zu^2 + zvn^2 - zv^2 left to right; the squares of the winds
+      // before diffusion are rounded on their own
+      const float uu = __fmul_rn(zu[l], zu[l]), vv = __fmul_rn(zv[l], zv[l]);
+      const float dke = __fsub_rn(__fmaf_rn(zvn[l], zvn[l], __fmaf_rn(zun[l], zun[l], -uu)), vv);
+      const float zdtdt = -(dke / D2 - (zken[l] - zke[l]) / D2) * 0.5f / K.ACPD / (1.f + K.ADV * dq);
+      heat[l] = heat[l] + zdtdt;
     }
   }
-  float zqn[NL];
 #pragma unroll
-  for (int l = 0; l < NL; ++l) zqn[l] = zq[l];
-  diffuse<NL>(ds, zqn, kh);
-#pragma unroll
-  for (int l = 0; l < NL; ++l) F.dqdt[l * SN + c] = dqdt[l] + __fdiv_rn(zqn[l] - zq[l], D2);
-#pragma unroll
-  for (int l = 0; l < NL - 1; ++l) kh[l] = kh[l] * zskaph[l];
-  float ztn[NL];
-#pragma unroll
-  for (int l = 0; l < NL; ++l) ztn[l] = zt[l];
-  diffuse_potential<NL>(ds, ztn, kh, zskap);
-#pragma unroll
-  for (int l = 0; l < NL; ++l) F.dtdt[l * SN + c] = dtdt[l] + __fdiv_rn(ztn[l] - zt[l], D2);
+  for (int l = 0; l < NL; ++l) F.dtdt[l * SN + c] = heat[l] + zdt[l];
 }
-template <int NL>
-__global__ void __launch_bounds__(kBlock, 3) k_vdiff(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
-  b_vdiff<NL>(m, pcr, tabr);
+template <int NL, int HOLD>
+__global__ void __launch_bounds__(kBlock, HOLD == 0 ? 4 : 3)
+    k_vdiff(Model m, const PlanetConst* __restrict__ pcr, const float* __restrict__ tabr) {
+  b_vdiff<NL, HOLD>(m, pcr, tabr);
 }
 
 
@@ -301,7 +343,16 @@ __global__ void __launch_bounds__(kBlock, 3) k_fused_fixer_flux_solang(Model m, 
 
 COLUMN_LAUNCHER(FixerApply, k_fixer_apply)
 COLUMN_LAUNCHER(Surflx, k_surflx)
-COLUMN_LAUNCHER(Vdiff, k_vdiff)
+template <int NL>
+struct Vdiff {
+  static void run(const Model& m, cudaStream_t st) {
+    const unsigned blocks = nblocks((size_t)m.d.S * m.d.NHOR, kBlock);
+    if (m.zero_gdt)
+      k_vdiff<NL, 1><<<blocks, kBlock, 0, st>>>(m, m.pc, m.tabs);
+    else
+      k_vdiff<NL, 0><<<blocks, kBlock, 0, st>>>(m, m.pc, m.tabs);
+  }
+};
 COLUMN_LAUNCHER(SolangMko3, k_solang_mko3)
 COLUMN_LAUNCHER(FusedFixerFluxSolang, k_fused_fixer_flux_solang)
 
