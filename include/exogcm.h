@@ -289,7 +289,9 @@ int exogcm_time_kernel(exogcm_engine* engine, const char* kernel, int reps, floa
  * resolution): values[0] FFT
  * latitudes per block; [1], [2] sp2fc wavenumbers and planes per block;
  * [3], [4] the same for dv2uv; [5..8] forward Legendre planes per tile
- * for fc2sp, uv2dv, mktend's uv2dv and qtend. `count` must be at least 9.
+ * for fc2sp, uv2dv, mktend's uv2dv and qtend; [9..12] (when count >= 13)
+ * the staging buffers of those forward blocks (1 or 2). `count` must be at
+ * least 9.
  * The shapes split work differently but leave every result unchanged. */
 int exogcm_tuning(exogcm_engine* engine, int* values, int count);
 

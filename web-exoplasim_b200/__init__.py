@@ -230,6 +230,8 @@ class Engine:
         self._keep = []
 
     def close(self):
+        if _lib is None:  # interpreter shutdown: the library is gone already
+            return
         if getattr(self, "h", None):
             _lib.exogcm_destroy(self.h)
             self.h = None
@@ -373,10 +375,11 @@ class Engine:
 
     def tuning(self) -> dict:
         """The transform launch shapes chosen at the first configure."""
-        v = (ctypes.c_int * 9)()
-        _check(_lib.exogcm_tuning(self.h, v, 9))
+        v = (ctypes.c_int * 13)()
+        _check(_lib.exogcm_tuning(self.h, v, 13))
+        kinds = ("fc2sp", "uv2dv", "mktend", "qtend")
         return {"fft_rows": v[0], "sp2fc": (v[1], v[2]), "dv2uv": (v[3], v[4]),
-                "forward_tiles": {"fc2sp": v[5], "uv2dv": v[6], "mktend": v[7], "qtend": v[8]}}
+                "forward_tiles": dict(zip(kinds, v[5:9])), "forward_buffers": dict(zip(kinds, v[9:13]))}
 
     def graph_launches(self, steps: int) -> int:
         n = ctypes.c_size_t()

@@ -132,6 +132,7 @@ struct Tuning {
   int inv_group[2];  // wavenumbers per inverse Legendre block: [0] sp2fc, [1] dv2uv
   int inv_tile[2];   // planes per inverse Legendre block (even)
   int fwd_tile[4];   // planes per forward Legendre tile (8 or 16), by kind
+  int fwd_buffers[4];  // staging buffers of a forward Legendre block (1 or 2), by kind
 };
 
 // Everything a step kernel can reach.

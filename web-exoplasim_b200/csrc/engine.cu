@@ -747,10 +747,12 @@ void autotune(exogcm_engine* e) {
   }
   for (int k = 0; k < 4; ++k) {
     float best = 1e30f;
-    int pick = t.fwd_tile[k];
-    for (int tile : {8, 16}) {
+    int pick = t.fwd_tile[k], pick_buffers = t.fwd_buffers[k];
+    for (int shape = 0; shape < 4; ++shape) {
+      const int tile = shape & 1 ? 16 : 8, buffers = shape & 2 ? 1 : 2;
       if (leg_forward_smem(d, k, tile) > kLegSmemLimit) continue;
       t.fwd_tile[k] = tile;
+      t.fwd_buffers[k] = buffers;
       const float ms = time([&](const Model& m) {
         if (k == 0)
           tr_legendre_forward(m, F.fgtdt, F.zstt1, LP, m.sh.qc, e->stream);
@@ -761,9 +763,10 @@ void autotune(exogcm_engine* e) {
         else
           tr_qtend(m, F.fgut, F.fgvt, F.fgtn, F.zstt2, LP, e->stream);
       });
-      if (ms < best) best = ms, pick = tile;
+      if (ms < best) best = ms, pick = tile, pick_buffers = buffers;
     }
     t.fwd_tile[k] = pick;
+    t.fwd_buffers[k] = pick_buffers;
   }
 }
 
@@ -1717,9 +1720,10 @@ int exogcm_tuning(exogcm_engine* e, int* values, int count) {
   return guard([&] {
     if (!e || !values || count < 9) throw Error(EXOGCM_EINVAL, "need room for 9 values");
     const Tuning& t = e->tune;
-    const int v[9] = {t.fft_rows,     t.inv_group[0], t.inv_tile[0], t.inv_group[1], t.inv_tile[1],
-                      t.fwd_tile[0], t.fwd_tile[1], t.fwd_tile[2], t.fwd_tile[3]};
-    std::copy(v, v + 9, values);
+    const int v[13] = {t.fft_rows,      t.inv_group[0],   t.inv_tile[0],    t.inv_group[1],   t.inv_tile[1],
+                       t.fwd_tile[0],   t.fwd_tile[1],    t.fwd_tile[2],    t.fwd_tile[3],    t.fwd_buffers[0],
+                       t.fwd_buffers[1], t.fwd_buffers[2], t.fwd_buffers[3]};
+    std::copy(v, v + std::min(count, 13), values);
   });
 }
 

@@ -256,7 +256,10 @@ struct FwdShape {
   static constexpr int ROW = JH + 1;                                // float4s per staged row, padded
 };
 
-template <int KIND, int NIN, int JH, int TP>
+// NB staging buffers: with two, the next tile is stored while the current
+// one is read; with one, a barrier separates them and the block needs about
+// half the shared memory, so more blocks share an SM (the autotuner picks).
+template <int KIND, int NIN, int JH, int TP, int NB>
 __global__ void __launch_bounds__(FwdShape<JH, TP>::THREADS)
     k_sym_forward(SymIn<NIN> in, float* __restrict__ out0, float* __restrict__ out1, int planes, int per_block,
                   SharedTabs sh, const float* __restrict__ q, int ncsp) {
@@ -267,7 +270,7 @@ __global__ void __launch_bounds__(FwdShape<JH, TP>::THREADS)
   constexpr int CONV = NIN * TP * 2 * ROW;            // float4s of one staged tile
   extern __shared__ float4 fsm[];
   float* tab = reinterpret_cast<float*>(fsm);           // [NTAB][JH][NT]
-  float4* conv = fsm + (NTAB * JH * NT + 3) / 4;        // [2][NIN][TP][2][ROW]
+  float4* conv = fsm + (NTAB * JH * NT + 3) / 4;        // [NB][NIN][TP][2][ROW]
   const int g = blockIdx.x % S::GROUPS;
   const int pbeg = (blockIdx.x / S::GROUPS) * per_block;
   const int pend = min(planes, pbeg + per_block);
@@ -337,7 +340,7 @@ __global__ void __launch_bounds__(FwdShape<JH, TP>::THREADS)
   const float* tq = tab + t;
   int it = 0;
   for (int tile = pbeg; tile < pend; tile += TP, ++it) {
-    const float4* cur = conv + (it & 1) * CONV;
+    const float4* cur = conv + (NB == 2 ? (it & 1) * CONV : 0);
     const int next = tile + TP;
     if (next < pend) fetch(next);
     if (active) {
@@ -394,7 +397,12 @@ __global__ void __launch_bounds__(FwdShape<JH, TP>::THREADS)
         }
       }
     }
-    if (next < pend) store(conv + ((it + 1) & 1) * CONV);
+    if (NB == 2) {
+      if (next < pend) store(conv + ((it + 1) & 1) * CONV);
+    } else if (next < pend) {
+      __syncthreads();
+      store(conv);
+    }
     __syncthreads();
   }
 }
@@ -411,11 +419,11 @@ size_t inverse_smem(const Dims& d, int nin, int group, int tile) {
   return 2 * inverse_buffer_floats(d, nin, group, tile) * sizeof(float);
 }
 
-// Forward: the table slices of a wavenumber pair and two staged tiles.
-template <int KIND, int NIN, int JH, int TP>
+// Forward: the table slices of a wavenumber pair and NB staged tiles.
+template <int KIND, int NIN, int JH, int TP, int NB = 2>
 size_t forward_smem() {
   using S = FwdShape<JH, TP>;
-  return ((size_t)(FwdTables<KIND>::N * JH * S::NT + 3) / 4 + 2 * (size_t)NIN * TP * 2 * S::ROW) * sizeof(float4);
+  return ((size_t)(FwdTables<KIND>::N * JH * S::NT + 3) / 4 + NB * (size_t)NIN * TP * 2 * S::ROW) * sizeof(float4);
 }
 
 template <typename K>
@@ -423,12 +431,12 @@ void allow_smem(K kernel) {
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget);
 }
 
-template <int KIND, int NIN, int JH, int TP>
+template <int KIND, int NIN, int JH, int TP, int NB>
 void launch_forward_shape(const Model& m, SymIn<NIN> in, float* out0, float* out1, int planes, const float* q,
                           cudaStream_t st) {
   using S = FwdShape<JH, TP>;
-  const auto kernel = k_sym_forward<KIND, NIN, JH, TP>;
-  const size_t smem = forward_smem<KIND, NIN, JH, TP>();
+  const auto kernel = k_sym_forward<KIND, NIN, JH, TP, NB>;
+  const size_t smem = forward_smem<KIND, NIN, JH, TP, NB>();
   // Blocks per wavenumber pair: enough for every SM's resident blocks, in
   // whole tiles of planes.
   const int tiles = (planes + TP - 1) / TP;
@@ -442,21 +450,18 @@ void launch_forward_shape(const Model& m, SymIn<NIN> in, float* out0, float* out
 template <int KIND, int NIN>
 void launch_sym_forward(const Model& m, SymIn<NIN> in, float* out0, float* out1, int planes, const float* q,
                         cudaStream_t st) {
-  const bool big = m.tune.fwd_tile[KIND] == 16;
+  const bool big = m.tune.fwd_tile[KIND] == 16, one = m.tune.fwd_buffers[KIND] == 1;
+#define EXOGCM_FWD(JH)                                                                         \
+  (big ? (one ? launch_forward_shape<KIND, NIN, JH, 16, 1>(m, in, out0, out1, planes, q, st)  \
+              : launch_forward_shape<KIND, NIN, JH, 16, 2>(m, in, out0, out1, planes, q, st)) \
+       : (one ? launch_forward_shape<KIND, NIN, JH, 8, 1>(m, in, out0, out1, planes, q, st)   \
+              : launch_forward_shape<KIND, NIN, JH, 8, 2>(m, in, out0, out1, planes, q, st)))
   switch (m.d.NLAT) {
-    case 32:
-      big ? launch_forward_shape<KIND, NIN, 16, 16>(m, in, out0, out1, planes, q, st)
-          : launch_forward_shape<KIND, NIN, 16, 8>(m, in, out0, out1, planes, q, st);
-      break;
-    case 64:
-      big ? launch_forward_shape<KIND, NIN, 32, 16>(m, in, out0, out1, planes, q, st)
-          : launch_forward_shape<KIND, NIN, 32, 8>(m, in, out0, out1, planes, q, st);
-      break;
-    default:
-      big ? launch_forward_shape<KIND, NIN, 48, 16>(m, in, out0, out1, planes, q, st)
-          : launch_forward_shape<KIND, NIN, 48, 8>(m, in, out0, out1, planes, q, st);
-      break;
+    case 32: EXOGCM_FWD(16); break;
+    case 64: EXOGCM_FWD(32); break;
+    default: EXOGCM_FWD(48); break;
   }
+#undef EXOGCM_FWD
 }
 
 template <int KIND, int NIN>
@@ -485,14 +490,20 @@ int persistent_grid(const void* kernel, int threads, size_t smem) {
   return sms * (per_sm > 0 ? per_sm : 1);
 }
 
+template <int KIND, int NIN, int NB>
+void allow_forward_smem_nb() {
+  allow_smem(k_sym_forward<KIND, NIN, 16, 8, NB>);
+  allow_smem(k_sym_forward<KIND, NIN, 16, 16, NB>);
+  allow_smem(k_sym_forward<KIND, NIN, 32, 8, NB>);
+  allow_smem(k_sym_forward<KIND, NIN, 32, 16, NB>);
+  allow_smem(k_sym_forward<KIND, NIN, 48, 8, NB>);
+  allow_smem(k_sym_forward<KIND, NIN, 48, 16, NB>);
+}
+
 template <int KIND, int NIN>
 void allow_forward_smem() {
-  allow_smem(k_sym_forward<KIND, NIN, 16, 8>);
-  allow_smem(k_sym_forward<KIND, NIN, 16, 16>);
-  allow_smem(k_sym_forward<KIND, NIN, 32, 8>);
-  allow_smem(k_sym_forward<KIND, NIN, 32, 16>);
-  allow_smem(k_sym_forward<KIND, NIN, 48, 8>);
-  allow_smem(k_sym_forward<KIND, NIN, 48, 16>);
+  allow_forward_smem_nb<KIND, NIN, 1>();
+  allow_forward_smem_nb<KIND, NIN, 2>();
 }
 
 void leg_init() {
@@ -557,7 +568,10 @@ Tuning default_tuning(const Dims& d) {
         break;
       }
   }
-  for (int k = 0; k < 4; ++k) t.fwd_tile[k] = 8;
+  for (int k = 0; k < 4; ++k) {
+    t.fwd_tile[k] = 8;
+    t.fwd_buffers[k] = 2;
+  }
   return t;
 }
 
