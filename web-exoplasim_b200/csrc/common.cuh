@@ -24,6 +24,32 @@
 
 namespace exogcm {
 
+
+// Programmatic dependent launch. A kernel started by pdl_launch may become
+// resident while the kernel before it on the stream drains: it calls
+// pdl_wait() before its first access to any state an earlier kernel writes
+// (that returns once those kernels have finished and their stores are
+// visible), and pdl_release() to let the kernel after it start the same way.
+// In a kernel launched the ordinary way both return at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline void pdl_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Per-planet global budgets (budget.cu): quantities per published step.
 constexpr int kBudgetQuantities = 8;
 constexpr int kBudgetStride = 2 * kBudgetQuantities + 2;  // last[8], sums[8], samples, averaged samples

@@ -25,6 +25,8 @@ __device__ __forceinline__ void prefetch_l2(const float* p) { asm volatile("pref
 // compiler may keep their values across the kernel's stores to fields
 // instead of reloading them after every store.
 #define COLUMN_PROLOGUE                                              \
+  pdl_wait();                                                        \
+  pdl_release();                                                     \
   const Dims& d = m.d;                                               \
   const int c = blockIdx.x * blockDim.x + threadIdx.x;               \
   if (c >= d.S * d.NHOR) return;                                     \
@@ -43,6 +45,8 @@ __device__ __forceinline__ void prefetch_l2(const float* p) { asm volatile("pref
 // and kBlock divides NHOR (2048, 8192 or 18432), so a block's columns
 // belong to one slot, whose constants are staged once in shared memory.
 #define COLUMN_PROLOGUE_STAGED                                       \
+  pdl_wait();                                                        \
+  pdl_release();                                                     \
   const Dims& d = m.d;                                               \
   const int slot = blockIdx.x * kBlock / d.NHOR;                     \
   const StepParams& P = m.params[slot];                              \
@@ -186,12 +190,14 @@ void by_levels(int L, A&&... a) {
     Launch<5>::run(a...);
 }
 
-#define COLUMN_LAUNCHER(name, kernel)                                                      \
-  template <int NL>                                                                        \
-  struct name {                                                                            \
-    static void run(const Model& m, cudaStream_t st) {                                     \
-      kernel<NL><<<nblocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st>>>(m, m.pc, m.tabs); \
-    }                                                                                      \
+// Column kernels begin with COLUMN_PROLOGUE(_STAGED), whose pdl_wait comes
+// before any state access, so they start by programmatic dependent launch.
+#define COLUMN_LAUNCHER(name, kernel)                                                               \
+  template <int NL>                                                                                 \
+  struct name {                                                                                     \
+    static void run(const Model& m, cudaStream_t st) {                                              \
+      pdl_launch(kernel<NL>, nblocks((size_t)m.d.S * m.d.NHOR, kBlock), kBlock, 0, st, m, m.pc, m.tabs); \
+    }                                                                                               \
   };
 
 }  // namespace

@@ -348,9 +348,9 @@ struct Vdiff {
   static void run(const Model& m, cudaStream_t st) {
     const unsigned blocks = nblocks((size_t)m.d.S * m.d.NHOR, kBlock);
     if (m.zero_gdt)
-      k_vdiff<NL, 1><<<blocks, kBlock, 0, st>>>(m, m.pc, m.tabs);
+      pdl_launch(k_vdiff<NL, 1>, blocks, kBlock, 0, st, m, m.pc, m.tabs);
     else
-      k_vdiff<NL, 0><<<blocks, kBlock, 0, st>>>(m, m.pc, m.tabs);
+      pdl_launch(k_vdiff<NL, 0>, blocks, kBlock, 0, st, m, m.pc, m.tabs);
   }
 };
 COLUMN_LAUNCHER(SolangMko3, k_solang_mko3)
