@@ -135,3 +135,30 @@ def test_planet_from_files_sets_up_as_the_planet(files):
         a = pkg.setup_preview(p, name)
         b = pkg.setup_preview(q, name)
         np.testing.assert_allclose(b, a, rtol=1e-12, atol=1e-12 * max(1.0, np.abs(a).max()), err_msg=name)
+
+
+@pytest.mark.gpu
+def test_planet_from_files_steps_as_the_planet(files):
+    """A run's namelists and .sra files, read by planet_from_files, configure
+    and step the engine exactly as the planet they were written from."""
+    p = planets.make_planet(6, truncation=21, levels=10, stormclim=True)
+    nlat = 32
+    bd = dict(p.boundary)
+    run = formats.apply_edits({k: v for k, v in files.items() if k.endswith("_namelist")}, p.config)
+    run.update(formats.boundary_files(nlat, bd[172], bd.get(129, np.zeros(POINTS))))
+    sst = np.asarray(bd[169]).reshape(-1, POINTS)
+    run[formats.sra_name(nlat, 169)] = "".join(formats.write_sra(169, m, 2 * nlat, nlat) for m in sst)
+    q, _ = formats.planet_from_files(run, 21, 10, p.t_grid, p.q_grid)
+    p.boundary = dict(q.boundary)  # the boundary as the files carry it
+    engines = [pkg.Engine(21, 10, 1, mode=1) for _ in range(2)]
+    try:
+        engines[0].configure(0, p)
+        engines[1].configure(0, q)
+        for e in engines:
+            e.step(3)
+            e.step(8)
+        for name in ("st", "sz", "sd", "sq", "sp", "dt", "dq", "dp", "capen", "gpi"):
+            np.testing.assert_array_equal(engines[1].read(0, name), engines[0].read(0, name), err_msg=name)
+    finally:
+        for e in engines:
+            e.close()
