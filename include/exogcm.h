@@ -330,6 +330,55 @@ int exogcm_slot_sums_noalloc(const float* first, const float* second, int slots,
 int exogcm_device_field(exogcm_engine* engine, const char* name, void** pointer, size_t* floats);
 void* exogcm_stream(exogcm_engine* engine);
 
+/* ---------------------------------------------------------------- server
+ * A batched server above the engine calls: continuous batching of many planet
+ * runs on the current device. It has no counterpart in the reference, whose
+ * page runs one planet per worker (runner/webgpu/gcm.worker.ts); it runs many
+ * the way that worker runs one. Runs of one resolution share engines
+ * ("blocks" of slots) created within one device-byte budget by their per-slot
+ * footprint and destroyed when empty and another resolution needs the room;
+ * each run stops exactly at its last step, so its result does not depend on
+ * what else ran. One server is used from one host thread at a time. */
+typedef struct exogcm_server exogcm_server;
+
+typedef struct exogcm_server_options {
+  double budget_bytes; /* device bytes the blocks' state may take */
+  int block_slots;     /* slots of a T21 L5 block; fewer at larger resolutions, by footprint */
+  int chunk_steps;     /* model steps per batch of a block (1..64) */
+  int mode;            /* engine mode of every block (exogcm_create) */
+} exogcm_server_options;
+
+#define EXOGCM_REQUEST_QUEUED 0
+#define EXOGCM_REQUEST_RUNNING 1
+#define EXOGCM_REQUEST_FINISHED 2
+#define EXOGCM_REQUEST_FAILED 3   /* unstable ("model became unstable"), or its set-up failed */
+#define EXOGCM_REQUEST_REJECTED 4 /* one block of its resolution exceeds the budget */
+
+int exogcm_server_create(const exogcm_server_options* options, exogcm_server** server);
+void exogcm_server_destroy(exogcm_server* server);
+
+/* Queues a run of `steps` main-loop model steps (after the start-up steps)
+ * of a planet; the planet and its boundary arrays are copied. */
+int exogcm_server_submit(exogcm_server* server, const exogcm_planet* planet, const exogcm_boundary* boundary,
+                         long steps, long* request);
+
+/* One scheduling round: submits a batch of chunk_steps for every block with
+ * running runs (exogcm_step_async), admits queued runs into free slots or
+ * new blocks while those batches run, waits for them and collects the runs
+ * that finished or became unstable. `*active` returns the runs queued or
+ * running (may be NULL). */
+int exogcm_server_pump(exogcm_server* server, int* active);
+
+/* A run's status (EXOGCM_REQUEST_*) and main-loop steps done. */
+int exogcm_server_poll(exogcm_server* server, long request, int* status, long* steps_done);
+
+/* A finished run's final spectral prognostic field ("st", "sz", "sd", "sq"
+ * or "sp"; reference layout, `count` its exogcm_field_size). */
+int exogcm_server_result(exogcm_server* server, long request, const char* field, float* values, size_t count);
+
+/* Forgets a finished, failed or rejected run and its result. */
+int exogcm_server_release(exogcm_server* server, long request);
+
 #ifdef __cplusplus
 }
 #endif

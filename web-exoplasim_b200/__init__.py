@@ -58,6 +58,12 @@ class Boundary(ctypes.Structure):
                 ("ice_cover", _DP), ("ice_cover_months", ctypes.c_int), ("t_init", _DP), ("q_init", _DP)]
 
 
+class ServerOptions(ctypes.Structure):
+    """exogcm_server_options (include/exogcm.h)."""
+    _fields_ = [("budget_bytes", ctypes.c_double), ("block_slots", ctypes.c_int), ("chunk_steps", ctypes.c_int),
+                ("mode", ctypes.c_int)]
+
+
 _lib = None
 
 # Every entry point include/exogcm.h declares: name -> (restype, argtypes).
@@ -76,6 +82,15 @@ SIGNATURES = {
     "exogcm_setup_on_device": (ctypes.c_int, [_VP, ctypes.c_int]),
     "exogcm_slot_date": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_long, ctypes.POINTER(ctypes.c_int)]),
     "exogcm_release": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "exogcm_server_create": (ctypes.c_int, [ctypes.POINTER(ServerOptions), ctypes.POINTER(_VP)]),
+    "exogcm_server_destroy": (None, [_VP]),
+    "exogcm_server_submit": (ctypes.c_int, [_VP, ctypes.POINTER(Planet), ctypes.POINTER(Boundary), ctypes.c_long,
+                                            ctypes.POINTER(ctypes.c_long)]),
+    "exogcm_server_pump": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int)]),
+    "exogcm_server_poll": (ctypes.c_int, [_VP, ctypes.c_long, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_long)]),
+    "exogcm_server_result": (ctypes.c_int, [_VP, ctypes.c_long, ctypes.c_char_p, _FP, ctypes.c_size_t]),
+    "exogcm_server_release": (ctypes.c_int, [_VP, ctypes.c_long]),
     "exogcm_step": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
     "exogcm_step_async": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
     "exogcm_poll": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int)]),
@@ -214,6 +229,60 @@ def setup_preview(planet, name: str, on_device: bool = False) -> np.ndarray:
     out = np.zeros(n.value)
     _check(call(ctypes.byref(p), ctypes.byref(b), name.encode(), out.ctypes.data_as(_DP), ctypes.byref(n)))
     return out
+
+
+class NativeServer:
+    """The C ABI's batched server (exogcm_server_*): continuous batching of
+    planet runs within a device-byte budget, driven by pump()."""
+
+    STATUS = ("queued", "running", "finished", "failed", "rejected")
+
+    def __init__(self, budget_bytes: float, block_slots: int = 32, chunk_steps: int = 32, mode: int = 1):
+        lib = load_library()
+        opt = ServerOptions(budget_bytes=float(budget_bytes), block_slots=block_slots, chunk_steps=chunk_steps,
+                            mode=mode)
+        self.h = _VP()
+        _check(lib.exogcm_server_create(ctypes.byref(opt), ctypes.byref(self.h)))
+
+    def submit(self, planet, steps: int) -> int:
+        """Queues `steps` main-loop steps of a planets.Planet; returns the request id."""
+        nhor = 2 * {21: 32, 42: 64, 63: 96}[planet.config["truncation"]] ** 2
+        keep = {}
+        p = planet_struct(planet.config)
+        b = boundary_struct(planet, nhor, keep)
+        rid = ctypes.c_long()
+        _check(_lib.exogcm_server_submit(self.h, ctypes.byref(p), ctypes.byref(b), int(steps), ctypes.byref(rid)))
+        return rid.value
+
+    def pump(self) -> int:
+        """One scheduling round; returns the runs still queued or running."""
+        active = ctypes.c_int()
+        _check(_lib.exogcm_server_pump(self.h, ctypes.byref(active)))
+        return active.value
+
+    def poll(self, request: int):
+        """(status name, main-loop steps done) of a request."""
+        status, done = ctypes.c_int(), ctypes.c_long()
+        _check(_lib.exogcm_server_poll(self.h, request, ctypes.byref(status), ctypes.byref(done)))
+        return self.STATUS[status.value], done.value
+
+    def result(self, request: int, field: str, size: int) -> np.ndarray:
+        out = np.zeros(size, dtype=np.float32)
+        _check(_lib.exogcm_server_result(self.h, request, field.encode(), out.ctypes.data_as(_FP), size))
+        return out
+
+    def release(self, request: int) -> None:
+        _check(_lib.exogcm_server_release(self.h, request))
+
+    def close(self):
+        if _lib is None:
+            return
+        if getattr(self, "h", None):
+            _lib.exogcm_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 class Engine:

@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libexogcm.so")
 SOURCES = ["engine.cu", "transforms.cu", "legendre.cu", "legendre_tc.cu", "fft.cu", "spectral_grid.cu", "dynamics.cu",
-           "physics.cu", "physics_flux.cu", "physics_storm.cu", "budget.cu", "noalloc.cu", "setup_device.cu", "setup.cpp"]
+           "physics.cu", "physics_flux.cu", "physics_storm.cu", "budget.cu", "noalloc.cu", "setup_device.cu", "setup.cpp", "server.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
