@@ -1693,7 +1693,7 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
           // the full step's other column kernels and its fused ones (timed
           // for the fusion choice; no byte count)
           {"fixer_apply", 0}, {"surflx", 0}, {"solang_mko3", 0}, {"mkdca", 0}, {"soil", 0}, {"land_surface", 0},
-          {"sea_ice", 0}, {"sea", 0}, {"carbon", 0}, {"storm", 0}, {"swr_pair", 0}, {"fused_fixer_flux_solang", 0},
+          {"sea_ice", 0}, {"sea", 0}, {"carbon", 0}, {"storm", 0}, {"fused_fixer_flux_solang", 0},
           {"fused_kuo_mkdca", 0},
           {"fused_rain_soil", 0}, {"fused_land_seaice", 0}, {"fused_sea_carbon", 0},
       };

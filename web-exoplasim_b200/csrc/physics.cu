@@ -329,10 +329,7 @@ __device__ __forceinline__ void swr_band(const Model& m, const PlanetConst& K, c
 // block's warps pair up on the same 32 columns, one band each (no branch
 // diverges inside a warp), and add their fluxes through shared memory in the
 // shader's order (band 1 + band 2).
-// PAIR: the two warps of one column group (its two bands) meet at a named
-// 64-thread barrier instead of the block-wide one, so the other group of the
-// block need not wait for them.
-template <int NL, bool PAIR>
+template <int NL>
 __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
   static_assert(NL <= SwrLevels::MAXLEV, "swr level state holds at most MAXLEV levels");
   constexpr int NP = NL + 1;
@@ -367,11 +364,7 @@ __global__ void __launch_bounds__(kBlock) k_swr(Model m) {
         swr_band<NL, 1>(m, K, tb, SN, c, mu0, ftop2, lv, &sfu[1][0][lc], &sfd[1][0][lc], kCols, alb);
     }
   }
-  // both bands' fluxes are in, and both have read dalb, dsalb
-  if (PAIR)
-    asm volatile("bar.sync %0, 64;" ::"r"(1 + (warp >> 1)) : "memory");
-  else
-    __syncthreads();
+  __syncthreads();  // both bands' fluxes are in, and both have read dalb, dsalb
   if (!run) return;
   if (lit && band == 0) {
     F.dsalb[c] = alb[0];
@@ -2040,16 +2033,12 @@ COLUMN_LAUNCHER(FusedKuoMkdca, k_fused_kuo_mkdca)
 COLUMN_LAUNCHER(FusedRainSoil, k_fused_rain_soil)
 COLUMN_LAUNCHER(FusedLandSeaice, k_fused_land_seaice)
 COLUMN_LAUNCHER(FusedSeaCarbon, k_fused_sea_carbon)
-template <int NL, bool PAIR>
-struct SwrB {
+template <int NL>
+struct Swr {
   static void run(const Model& m, cudaStream_t st) {
-    k_swr<NL, PAIR><<<nblocks((size_t)m.d.S * m.d.NHOR, kBlock / 2), kBlock, 0, st>>>(m);
+    k_swr<NL><<<nblocks((size_t)m.d.S * m.d.NHOR, kBlock / 2), kBlock, 0, st>>>(m);
   }
 };
-template <int NL>
-using Swr = SwrB<NL, false>;
-template <int NL>
-using SwrPair = SwrB<NL, true>;
 COLUMN_LAUNCHER(LwrRadstep, k_lwr_radstep)
 COLUMN_LAUNCHER(Kuo, k_kuo)
 COLUMN_LAUNCHER(Mkdca, k_mkdca)
@@ -2135,8 +2124,6 @@ bool phy_launch_one(const Model& m, const std::string& kernel, cudaStream_t st) 
   const int L = m.d.L;
   if (phy_flux_launch_one(m, kernel, st))
     return true;
-  else if (kernel == "swr_pair")
-    by_levels<SwrPair>(L, m, st);
   else if (kernel == "storm") {
     Model on = m;
     on.storm = 1;
