@@ -311,6 +311,22 @@ class Server:
             "configure_ms_p99": float(np.percentile(configure, 99)) * 1e3 if configure.size else None,
         }
 
+    def prewarm(self, resolutions=((21, 5), (21, 10), (42, 5), (42, 10), (63, 5), (63, 10)), seed: int = 1):
+        """Creates one block per resolution before serving and configures (then
+        releases) a planet in it, so the shared tables and the autotuned launch
+        shapes of each block shape exist before the first request: a warm pool.
+        The blocks stay and take the first requests; returns the seconds taken."""
+        t0 = time.perf_counter()
+        for key in resolutions:
+            block = self._free_slot(key) or self._grow(key)
+            if block is None:
+                continue
+            planet = planets_mod.make_planet(seed, truncation=key[0], levels=key[1],
+                                             timestepMinutes=STEP_MINUTES[key[0]])
+            block.engine.configure(0, planet)
+            block.engine.release(0)
+        return time.perf_counter() - t0
+
     def close(self):
         for b in self.blocks:
             b.close()
