@@ -114,3 +114,24 @@ def test_budget_rejects_and_evicts():
         assert seen_b_queued_while_a_runs
     finally:
         server.close()
+
+
+@pytest.mark.gpu
+def test_unstable_and_rejected_set_up_runs_fail_alone():
+    good = planets.make_planet(321, truncation=21, levels=5)
+    nan = planets.make_planet(322, truncation=21, levels=5)
+    nan.t_grid[:] = np.nan  # a state that cannot be stepped
+    bad = planets.make_planet(323, truncation=21, levels=5, starTemperatureK=5000.0)  # set-up refuses it
+    server = pkg.NativeServer(budget_bytes=4e9, block_slots=4, chunk_steps=8, mode=1)
+    try:
+        ids = [server.submit(p, 16) for p in (good, nan, bad)]
+        for _ in range(100):
+            if server.pump() == 0:
+                break
+        assert [server.poll(i)[0] for i in ids] == ["finished", "failed", "failed"]
+        ref, _ = alone(good, 16)
+        np.testing.assert_array_equal(server.result(ids[0], "st", ref["st"].size), ref["st"])
+        with pytest.raises(pkg.ExogcmError):
+            server.result(ids[1], "st", ref["st"].size)
+    finally:
+        server.close()
