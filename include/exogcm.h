@@ -276,7 +276,8 @@ int exogcm_last_step_ms(exogcm_engine* engine, float* ms);
  * *bytes. Kernels: "fourier_forward", "fourier_inverse" (FFTs on the
  * optimized path, DFTs on the plain one), "legendre_forward",
  * "legendre_inverse", "sp2gp" (the fused inverse Legendre transform and FFT
- * of the optimized path), "dv2uv", "uv2dv", "qtend", "calcgp", "spectrala",
+ * of the optimized path; "sp2gp_planes2" and "sp2gp_planes4" run it at 2
+ * or 4 planes per pass whatever the tuning chose), "dv2uv", "uv2dv", "qtend", "calcgp", "spectrala",
  * "mkdheat" (its first stage), "physics_in", "physics_out", and the single
  * column kernels "vdiff", "swr", "lwr_radstep", "kuo", "rain_column". The
  * launches change the state; use it for measurement only. */
@@ -290,8 +291,9 @@ int exogcm_time_kernel(exogcm_engine* engine, const char* kernel, int reps, floa
  * latitudes per block; [1], [2] sp2fc wavenumbers and planes per block;
  * [3], [4] the same for dv2uv; [5..8] forward Legendre planes per tile
  * for fc2sp, uv2dv, mktend's uv2dv and qtend; [9..12] (when count >= 13)
- * the staging buffers of those forward blocks (1 or 2). `count` must be at
- * least 9.
+ * the staging buffers of those forward blocks (1 or 2); [13] (when count >=
+ * 14) the planes per pass of the fused inverse transform (2 or 4). `count`
+ * must be at least 9.
  * The shapes split work differently but leave every result unchanged. */
 int exogcm_tuning(exogcm_engine* engine, int* values, int count);
 

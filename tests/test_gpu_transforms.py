@@ -104,3 +104,24 @@ def test_transforms_on_random_planes(truncation, mode):
                 assert gpu <= 2 * doc, (kernel, out, gpu, doc)
     print(f"T{truncation} mode {mode} relative RMS (GPU, sequential f32, reference's FP32 kernel):",
           {k: tuple(None if x is None else float(f"{x:.3g}") for x in v) for k, v in report.items()})
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("truncation", [21, 42, 63])
+def test_sp2gp_planes_per_pass_bitwise(truncation):
+    """The fused inverse transform runs two or four planes per pass (the
+    autotuner picks the faster); each grid point takes the same sums in the
+    same order, so both shapes give the same grid planes bit for bit."""
+    e = pkg.Engine(truncation, 10, 3, mode=1)
+    for s in range(3):
+        e.configure(s, planets.make_planet(5 + s, truncation=truncation, levels=10))
+    e.step(3)
+    e.step(2)
+    assert e.tuning()["sp2gp_planes"] in (2, 4)
+    got = {}
+    for shape in ("sp2gp_planes2", "sp2gp_planes4"):
+        e.time_kernel(shape, 1)
+        got[shape] = [e.read(s, "gt").copy() for s in range(3)]
+    for a, b in zip(got["sp2gp_planes2"], got["sp2gp_planes4"]):
+        assert np.array_equal(a, b)
+    assert np.isfinite(got["sp2gp_planes2"][0]).all()

@@ -444,11 +444,12 @@ class Engine:
 
     def tuning(self) -> dict:
         """The transform launch shapes chosen at the first configure."""
-        v = (ctypes.c_int * 13)()
-        _check(_lib.exogcm_tuning(self.h, v, 13))
+        v = (ctypes.c_int * 14)()
+        _check(_lib.exogcm_tuning(self.h, v, 14))
         kinds = ("fc2sp", "uv2dv", "mktend", "qtend")
         return {"fft_rows": v[0], "sp2fc": (v[1], v[2]), "dv2uv": (v[3], v[4]),
-                "forward_tiles": dict(zip(kinds, v[5:9])), "forward_buffers": dict(zip(kinds, v[9:13]))}
+                "forward_tiles": dict(zip(kinds, v[5:9])), "forward_buffers": dict(zip(kinds, v[9:13])),
+                "sp2gp_planes": v[13]}
 
     def graph_launches(self, steps: int) -> int:
         n = ctypes.c_size_t()

@@ -159,6 +159,7 @@ struct Tuning {
   int inv_tile[2];   // planes per inverse Legendre block (even)
   int fwd_tile[4];   // planes per forward Legendre tile (8 or 16), by kind
   int fwd_buffers[4];  // staging buffers of a forward Legendre block (1 or 2), by kind
+  int sp2gp_planes;    // planes per pass of the fused inverse transform (2 or 4)
 };
 
 // Everything a step kernel can reach.

@@ -768,6 +768,17 @@ void autotune(exogcm_engine* e) {
     t.fwd_tile[k] = pick;
     t.fwd_buffers[k] = pick_buffers;
   }
+  {
+    float best = 1e30f;
+    int pick = t.sp2gp_planes;
+    for (int pp : {2, 4}) {
+      if (grid_sp2gp_smem(d, pp) > kLegSmemLimit) continue;
+      t.sp2gp_planes = pp;
+      const float ms = time([&](const Model& m) { tr_sp2gp(m, F.st, F.fgt, F.gt, LP, m.sh.qi, e->stream); });
+      if (ms < best) best = ms, pick = pp;
+    }
+    t.sp2gp_planes = pick;
+  }
 }
 
 // Group graphs (exogcm_group_step): one instantiated graph per list of
@@ -1651,6 +1662,16 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
       // fused sp2fc + fc2gp: the spectral plane in, the grid plane out
       launch = [&] { tr_sp2gp(m, F.st, F.fgt, F.gt, LP, m.sh.qi, e->stream); };
       b = LP * (spec + grid);
+    } else if (k == "sp2gp_planes2" || k == "sp2gp_planes4") {
+      // the fused transform at a fixed number of planes per pass
+      const int pp = k == "sp2gp_planes4" ? 4 : 2;
+      if (grid_sp2gp_smem(d, pp) > kLegSmemLimit) throw Error(EXOGCM_EINVAL, "shape needs too much shared memory");
+      launch = [&, pp] {
+        Model mp = m;
+        mp.tune.sp2gp_planes = pp;
+        tr_sp2gp(mp, F.st, F.fgt, F.gt, LP, mp.sh.qi, e->stream);
+      };
+      b = LP * (spec + grid);
     } else if (k == "legendre_inverse") {
       launch = [&] { tr_legendre_inverse(m, F.st, F.fgt, LP, m.sh.qi, e->stream); };
       b = LP * (spec + four);
@@ -1720,10 +1741,10 @@ int exogcm_tuning(exogcm_engine* e, int* values, int count) {
   return guard([&] {
     if (!e || !values || count < 9) throw Error(EXOGCM_EINVAL, "need room for 9 values");
     const Tuning& t = e->tune;
-    const int v[13] = {t.fft_rows,      t.inv_group[0],   t.inv_tile[0],    t.inv_group[1],   t.inv_tile[1],
+    const int v[14] = {t.fft_rows,      t.inv_group[0],   t.inv_tile[0],    t.inv_group[1],   t.inv_tile[1],
                        t.fwd_tile[0],   t.fwd_tile[1],    t.fwd_tile[2],    t.fwd_tile[3],    t.fwd_buffers[0],
-                       t.fwd_buffers[1], t.fwd_buffers[2], t.fwd_buffers[3]};
-    std::copy(v, v + std::min(count, 13), values);
+                       t.fwd_buffers[1], t.fwd_buffers[2], t.fwd_buffers[3], t.sp2gp_planes};
+    std::copy(v, v + std::min(count, 14), values);
   });
 }
 

@@ -59,6 +59,8 @@ void tc_qtend(const Model& m, const float* u, const float* v, const float* src, 
 
 // fft.cu (optimized path; Fourier planes m-major)
 void fft_init();
+// Shared memory of the fused inverse transform at 2 or 4 planes per pass.
+size_t grid_sp2gp_smem(const Dims& d, int planes_per_pass);
 void grid_init();
 void grid_sp2gp(const Model& m, const float* s, float* f, float* g, int planes, bool derivative, cudaStream_t st);
 size_t fft_chunk_smem(const Dims& d, int rows);

@@ -572,6 +572,7 @@ Tuning default_tuning(const Dims& d) {
     t.fwd_tile[k] = 8;
     t.fwd_buffers[k] = 2;
   }
+  t.sp2gp_planes = 2;
   return t;
 }
 

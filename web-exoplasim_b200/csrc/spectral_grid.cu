@@ -38,7 +38,7 @@ using namespace fftcore;
 
 __device__ __forceinline__ int mode_start(int m, int ntp1) { return m * (2 * ntp1 - m + 1) / 2; }
 
-template <int Q>
+template <int Q, int PPASS = 2>
 struct GridShape {
   using F = Shape<Q>;
   static constexpr int M = F::M, N = F::N, NTP1 = F::NTP1, T = F::T;
@@ -46,19 +46,20 @@ struct GridShape {
   static constexpr int NCSP = NTP1 * (NTP1 + 1) / 2;
   static constexpr int JR = 8;            // latitude pairs per block
   static constexpr int ROWS = 2 * JR;     // rows of a plane
-  static constexpr int PP = 2;            // planes per pass
+  static constexpr int PP = PPASS;        // planes per pass (2 or 4)
+  static constexpr int NPAIR = PP / 2;    // plane pairs per pass
   static constexpr int FROWS = PP * ROWS; // FFT rows per pass
   static constexpr int THREADS = FROWS * T;
   static constexpr int GROUPS = (NTP1 + 1) / 2;
-  static constexpr int TASKS = GROUPS * JR;
+  static constexpr int TASKS = GROUPS * JR * NPAIR;
   static constexpr int TL = NCSP + 3 * NTP1;                       // table row: modes plus alignment gaps
   static constexpr int TP = TL + (((4 - TL) % 32) + 32) % 32;      // row pitch, 4 (mod 32)
   static constexpr int PITCH = (ROWS + (((16 / T - ROWS) % 16) + 16) % 16);
   static constexpr int FC = NTP1 * PITCH;  // float2s of one plane's coefficient stage
-  static constexpr int SPEC = NCSP;        // float4s of the spectral stage (two planes)
-  static constexpr int XB = FROWS * 9 * Q; // float2s of the FFT exchange rows
+  static constexpr int SPEC = NPAIR * NCSP;  // float4s of the spectral stage ([pair][mode], two planes each)
+  static constexpr int XB = FROWS * 9 * Q;   // float2s of the FFT exchange rows
   static constexpr int SHARED = (2 * SPEC > XB ? 2 * SPEC : XB);  // float2s of the union
-  static constexpr int R = (NCSP + THREADS - 1) / THREADS;        // spectral float4s per thread
+  static constexpr int R = (SPEC + THREADS - 1) / THREADS;        // spectral float4s per thread
   static_assert((N + 9 * Q + PP * FC) % 2 == 0, "the spectral stage must start 16-byte aligned");
   static size_t smem() {
     return ((size_t)N + 9 * Q + (size_t)PP * FC + SHARED) * sizeof(float2) + (size_t)JR * TP * sizeof(float) +
@@ -74,12 +75,14 @@ __device__ __forceinline__ int stage_lat(int rr, int j0) {
   return rr < G::JR ? j0 + rr : G::NLAT - 2 * G::JR - j0 + rr;
 }
 
-template <int Q>
-__global__ void __launch_bounds__(GridShape<Q>::THREADS)
+// PP planes per pass: 2, or 4 (twice the threads and stages per block, the
+// table slice and the barriers shared by twice the planes; the autotuner picks).
+template <int Q, int PP>
+__global__ void __launch_bounds__(GridShape<Q, PP>::THREADS)
     k_sp2gp(const float* __restrict__ s, float* __restrict__ f, float* __restrict__ g, int planes, int per_block,
             const float* __restrict__ qT, const int* __restrict__ mode_m, const float2* __restrict__ twg, int odd,
             int keep) {
-  using G = GridShape<Q>;
+  using G = GridShape<Q, PP>;
   constexpr int T = G::T, M = G::M, N = G::N, NTP1 = G::NTP1, JR = G::JR, JH = G::JH, TP = G::TP;
   constexpr int NLAT = G::NLAT, ROWS = G::ROWS, PITCH = G::PITCH, NCSP = G::NCSP, R = G::R;
   constexpr size_t SPLANE = 2 * (size_t)NCSP;              // floats of a spectral plane (NRSP)
@@ -89,7 +92,7 @@ __global__ void __launch_bounds__(GridShape<Q>::THREADS)
   float2* tw = reinterpret_cast<float2*>(smem4);
   float2* twq = tw + N;
   float2* fc = twq + 9 * Q;               // [PP][NTP1][PITCH]
-  float2* shared = fc + G::PP * G::FC;    // spectral stage [NCSP] float4, or the FFT exchange rows
+  float2* shared = fc + G::PP * G::FC;    // spectral stage [NPAIR][NCSP] float4, or the FFT exchange rows
   float4* spec = reinterpret_cast<float4*>(shared);
   float2* xb = shared;
   float* tab = reinterpret_cast<float*>(shared + G::SHARED);  // [JR][TP]
@@ -99,19 +102,20 @@ __global__ void __launch_bounds__(GridShape<Q>::THREADS)
   const int pbeg = (blockIdx.x / chunks) * per_block;
   const int pend = min(planes, pbeg + per_block);
 
-  // Spectral coefficients of planes p, p + 1 as (re a, im a, re b, im b).
+  // Spectral coefficients of the pass's plane pairs (p + 2k, p + 2k + 1)
+  // as (re a, im a, re b, im b), pair-major.
   float4 rs[R];
   auto fetch = [&](int p) {
-    const bool hb = p + 1 < pend;
-    const float2* a = reinterpret_cast<const float2*>(s + (size_t)p * SPLANE);
-    const float2* b = reinterpret_cast<const float2*>(s + (size_t)(p + 1) * SPLANE);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
-      const int w = threadIdx.x + i * G::THREADS;
+      const int e = threadIdx.x + i * G::THREADS;
+      const int pair = e / NCSP, w = e - pair * NCSP;
+      const int pa = p + 2 * pair;
       float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (w < NCSP) {
-        const float2 x = a[w];
-        const float2 y = hb ? b[w] : make_float2(0.f, 0.f);
+      if (e < G::SPEC && pa < pend) {
+        const float2 x = reinterpret_cast<const float2*>(s + (size_t)pa * SPLANE)[w];
+        const float2 y = pa + 1 < pend ? reinterpret_cast<const float2*>(s + (size_t)(pa + 1) * SPLANE)[w]
+                                       : make_float2(0.f, 0.f);
         v = make_float4(x.x, x.y, y.x, y.y);
       }
       rs[i] = v;
@@ -120,8 +124,8 @@ __global__ void __launch_bounds__(GridShape<Q>::THREADS)
   auto store = [&]() {
 #pragma unroll
     for (int i = 0; i < R; ++i) {
-      const int w = threadIdx.x + i * G::THREADS;
-      if (w < NCSP) spec[w] = rs[i];
+      const int e = threadIdx.x + i * G::THREADS;
+      if (e < G::SPEC) spec[e] = rs[i];
     }
   };
 
@@ -151,17 +155,17 @@ __global__ void __launch_bounds__(GridShape<Q>::THREADS)
   const int pr = r / ROWS, rr = r - pr * ROWS;         // plane of the pass, stage row
   const int lat = stage_lat<G>(rr, j0);
   for (int p = pbeg; p < pend; p += G::PP) {
-    const bool hb = p + 1 < pend;
     // 1. Legendre sums into the coefficient stage.
     for (int task = threadIdx.x; task < G::TASKS; task += G::THREADS) {
-      const int u = task / JR, jj = task - u * JR;
+      const int pair = task / (G::GROUPS * JR), rest = task - pair * (G::GROUPS * JR);
+      const int u = rest / JR, jj = rest - u * JR;
 #pragma unroll 1
       for (int side = 0; side < 2; ++side) {
         const int m = side == 0 ? u : NTP1 - 1 - u;
         if (side == 1 && m == u) break;
         const int w0 = mode_start(m, NTP1), K = NTP1 - m;
         const float* qc = tab + jj * TP + tpos[m];
-        const float4* sc = spec + w0;
+        const float4* sc = spec + pair * NCSP + w0;
         float4 e = make_float4(0.f, 0.f, 0.f, 0.f), o = e;  // (re a, im a, re b, im b)
         int k = 0;
 #pragma unroll 2
@@ -185,7 +189,7 @@ __global__ void __launch_bounds__(GridShape<Q>::THREADS)
           e.z = fmaf(qe, ve.z, e.z);
           e.w = fmaf(qe, ve.w, e.w);
         }
-        float2* fa = fc + m * PITCH;
+        float2* fa = fc + (2 * pair) * G::FC + m * PITCH;
         float2* fb = fa + G::FC;
         const int rn = jj, rsouth = ROWS - 1 - jj;
         fa[rn] = make_float2(e.x + o.x, e.y + o.y);
@@ -198,7 +202,7 @@ __global__ void __launch_bounds__(GridShape<Q>::THREADS)
     if (keep) {
       for (int i = threadIdx.x; i < G::PP * NTP1 * ROWS; i += G::THREADS) {
         const int q = i / (NTP1 * ROWS), rem = i - q * NTP1 * ROWS, m = rem / ROWS, row = rem - m * ROWS;
-        if (q == 0 || hb)
+        if (p + q < pend)
           reinterpret_cast<float2*>(f + (size_t)(p + q) * FPLANE)[(size_t)m * NLAT + stage_lat<G>(row, j0)] =
               fc[q * G::FC + m * PITCH + row];
       }
@@ -222,7 +226,7 @@ __global__ void __launch_bounds__(GridShape<Q>::THREADS)
       }
     float2 b[G::F::KT][Q];
     four_step<Q, 1>(a, b, twq, xb + r * G::F::XP, t);
-    if (pr == 0 || hb) {
+    if (p + pr < pend) {
       float2* out = reinterpret_cast<float2*>(g + (size_t)(p + pr) * GPLANE + (size_t)lat * N);
 #pragma unroll
       for (int j = 0; j < G::F::KT; ++j)
@@ -237,36 +241,61 @@ __global__ void __launch_bounds__(GridShape<Q>::THREADS)
   }
 }
 
-template <int Q>
+template <int Q, int PP>
 void launch_sp2gp(const Model& m, const float* s, float* f, float* g, int planes, const float* qT, int odd,
                   cudaStream_t st) {
-  using G = GridShape<Q>;
+  using G = GridShape<Q, PP>;
   const size_t smem = G::smem();
   const int chunks = G::JH / G::JR;
-  const int pairs = (planes + 1) / 2;
-  const int target = persistent_grid((const void*)k_sp2gp<Q>, G::THREADS, smem);
-  const int splits = std::max(1, std::min(pairs, (target + chunks - 1) / chunks));
-  const int per_pairs = (pairs + splits - 1) / splits;
-  const int blocks = chunks * ((pairs + per_pairs - 1) / per_pairs);
-  k_sp2gp<Q><<<blocks, G::THREADS, smem, st>>>(s, f, g, planes, 2 * per_pairs, qT, m.sh.mode_m,
-                                                reinterpret_cast<const float2*>(m.sh.tw), odd, m.keep_fourier);
+  const int passes = (planes + PP - 1) / PP;
+  const int target = persistent_grid((const void*)k_sp2gp<Q, PP>, G::THREADS, smem);
+  const int splits = std::max(1, std::min(passes, (target + chunks - 1) / chunks));
+  const int per_passes = (passes + splits - 1) / splits;
+  const int blocks = chunks * ((passes + per_passes - 1) / per_passes);
+  k_sp2gp<Q, PP><<<blocks, G::THREADS, smem, st>>>(s, f, g, planes, PP * per_passes, qT, m.sh.mode_m,
+                                                    reinterpret_cast<const float2*>(m.sh.tw), odd, m.keep_fourier);
+}
+
+template <int Q, int PP>
+void allow_sp2gp_smem() {
+  cudaFuncSetAttribute(k_sp2gp<Q, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GridShape<Q, PP>::smem());
 }
 
 }  // namespace
 
 void grid_init() {
-  cudaFuncSetAttribute(k_sp2gp<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GridShape<4>::smem());
-  cudaFuncSetAttribute(k_sp2gp<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GridShape<8>::smem());
-  cudaFuncSetAttribute(k_sp2gp<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GridShape<12>::smem());
+  allow_sp2gp_smem<4, 2>();
+  allow_sp2gp_smem<8, 2>();
+  allow_sp2gp_smem<12, 2>();
+  allow_sp2gp_smem<4, 4>();
+  allow_sp2gp_smem<8, 4>();
+  allow_sp2gp_smem<12, 4>();
+}
+
+size_t grid_sp2gp_smem(const Dims& d, int planes_per_pass) {
+  const bool four = planes_per_pass == 4;
+  switch (d.NLON) {
+    case 64: return four ? GridShape<4, 4>::smem() : GridShape<4, 2>::smem();
+    case 128: return four ? GridShape<8, 4>::smem() : GridShape<8, 2>::smem();
+    default: return four ? GridShape<12, 4>::smem() : GridShape<12, 2>::smem();
+  }
 }
 
 void grid_sp2gp(const Model& m, const float* s, float* f, float* g, int planes, bool derivative, cudaStream_t st) {
   const float* qT = derivative ? m.sh.qjT : m.sh.qiT;
   const int odd = derivative ? 1 : 0;
+  const bool four = m.tune.sp2gp_planes == 4;
   switch (m.d.NLON) {
-    case 64: launch_sp2gp<4>(m, s, f, g, planes, qT, odd, st); break;
-    case 128: launch_sp2gp<8>(m, s, f, g, planes, qT, odd, st); break;
-    default: launch_sp2gp<12>(m, s, f, g, planes, qT, odd, st); break;
+    case 64:
+      four ? launch_sp2gp<4, 4>(m, s, f, g, planes, qT, odd, st) : launch_sp2gp<4, 2>(m, s, f, g, planes, qT, odd, st);
+      break;
+    case 128:
+      four ? launch_sp2gp<8, 4>(m, s, f, g, planes, qT, odd, st) : launch_sp2gp<8, 2>(m, s, f, g, planes, qT, odd, st);
+      break;
+    default:
+      four ? launch_sp2gp<12, 4>(m, s, f, g, planes, qT, odd, st)
+           : launch_sp2gp<12, 2>(m, s, f, g, planes, qT, odd, st);
+      break;
   }
 }
 
