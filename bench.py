@@ -451,7 +451,10 @@ def main():
 
     # End to end through the C ABI: host values uploaded every call, a
     # snapshot published per slot every model day (32 steps) and read back to
-    # host buffers, host wall clock around the calls.
+    # host buffers, host wall clock around the calls. Days are submitted as
+    # the reference's worker does (two batches in flight): exogcm_step_async
+    # and a snapshot copy queued behind it, so the host computes the next
+    # day's per-step values while the device runs the current one.
     publish = 32
     e2e_calls = max(4, args.steps // publish)  # several days, so each day's copy can overlap the next
     snap_floats = engine.field_size("snapshot")
@@ -469,7 +472,7 @@ def main():
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_calls):
-        engine.step(publish, publish_every=publish)
+        engine.step_async(publish, publish_every=publish)
         engine.snapshots_begin(host)
     engine.snapshots_wait()
     torch.cuda.synchronize()

@@ -155,8 +155,8 @@ int exogcm_step(exogcm_engine* engine, int steps, int publish_every);
  * (runner/webgpu/gcm.worker.ts:215-225, pump/submit :285-346). At most two
  * batches are in flight; a third call waits for the oldest. While batches
  * are in flight the engine accepts only exogcm_step_async, exogcm_poll,
- * exogcm_wait, exogcm_slot_info and the query calls; every other call first
- * waits for them (exogcm_configure computes the new planet's host set-up
+ * exogcm_wait, exogcm_snapshots_begin, exogcm_slot_info and the query calls;
+ * every other call first waits for them (exogcm_configure computes the new planet's host set-up
  * before it waits, so that work overlaps the device's). */
 int exogcm_step_async(exogcm_engine* engine, int steps, int publish_every);
 
@@ -216,11 +216,13 @@ int exogcm_slot_date(exogcm_engine* engine, int slot, long step, int* date);
  * NULL to query only. */
 int exogcm_read_snapshot(exogcm_engine* engine, int slot, float* values, size_t count, long* step);
 
-/* Starts copying every slot's snapshot field, as the last exogcm_step left
- * it, into `values` (count = snapshot planes x slots x NHOR floats, laid out
- * [plane][slot][point] as on the device) and returns at once: the copy to
- * the host runs on a stream of its own, from a device-side copy taken on the
- * engine's stream, so the next exogcm_step computes while it drains. Use
+/* Starts copying every slot's snapshot field, as the last submitted batch
+ * (exogcm_step or exogcm_step_async) leaves it, into `values` (count =
+ * snapshot planes x slots x NHOR floats, laid out [plane][slot][point] as on
+ * the device) and returns at once without waiting for batches in flight:
+ * the copy to the host runs on a stream of its own, from a device-side copy
+ * queued on the engine's stream behind that batch, so the next batches
+ * compute while it drains. Use
  * pinned host memory for `values` to get that overlap. Only slots that
  * published in that step hold a new snapshot (see exogcm_read_snapshot). A
  * second call waits for the first copy; exogcm_snapshots_wait waits for the

@@ -96,3 +96,34 @@ def test_group_step_runs_mixed_resolutions_as_one_graph():
             for name in ("st", "sz", "sd", "sq", "sp", "dt"):
                 assert np.array_equal(g.read(s, name), a.read(s, name)), (t, l, s, name)
         assert g.slot_info(0)["step"] == a.slot_info(0)["step"]
+
+
+@pytest.mark.gpu
+def test_snapshots_of_pipelined_days_equal_synchronous_days():
+    """exogcm_snapshots_begin does not wait for batches in flight: it copies
+    the snapshot the last submitted batch leaves. Days submitted with
+    step_async (two in flight) and a bulk snapshot copy after each give the
+    snapshots and states of exogcm_step day by day, bit for bit."""
+    sync, pipe = _engine(slots=3), _engine(slots=3)
+    for e in (sync, pipe):
+        e.step(3)
+    planes = sync.field_size("snapshot")
+    ref = []
+    for _ in range(3):
+        sync.step(32, publish_every=32)
+        out = np.zeros(planes * 3, dtype=np.float32)
+        sync.snapshots_begin(out)
+        sync.snapshots_wait()
+        ref.append(out)
+    got = [np.zeros(planes * 3, dtype=np.float32) for _ in range(3)]
+    for day in range(3):
+        pipe.step_async(32, publish_every=32)
+        pipe.snapshots_begin(got[day])
+    pipe.snapshots_wait()
+    assert pipe.poll()
+    for day in range(3):
+        assert np.array_equal(ref[day], got[day]), day
+    assert not np.array_equal(ref[0], ref[2])
+    for name in ("st", "sq", "sp"):
+        for s in range(3):
+            assert np.array_equal(sync.read(s, name), pipe.read(s, name)), (name, s)

@@ -1398,7 +1398,9 @@ int exogcm_read_snapshot(exogcm_engine* e, int slot, float* values, size_t count
 int exogcm_snapshots_begin(exogcm_engine* e, float* values, size_t count) {
   return guard([&] {
     if (!e || !values) throw Error(EXOGCM_EINVAL, "null argument");
-    retire_all(e);
+    // Batches in flight are not waited for: the staging copy below is queued
+    // on the engine's stream behind the last submitted batch, so it takes the
+    // snapshot that batch leaves while the host goes on submitting.
     const FieldInfo& fi = field(e, "snapshot");
     const size_t n = fi.plane * fi.count * e->d.S;
     if (count != n) throw Error(EXOGCM_EINVAL, "snapshot buffer size mismatch (planes x slots x points)");
