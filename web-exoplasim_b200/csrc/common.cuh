@@ -141,6 +141,10 @@ struct SharedTabs {
   const float* qjT;
   const float* quT;
   const float* qvT;
+  // qiT and qjT again as the fused inverse transform's per-block slices
+  // ([chunk of 8 latitude pairs][pair][padded mode row], grid_table_layout).
+  const float* qiG;
+  const float* qjG;
   // Tensor-core (mode 2) table operands: per image set (qi, qj, dv2uv,
   // fc2sp, uv2dv, mktend, qtend) and m, the hi and lo TF32 images of the
   // tables in the MMA's shared-memory layout, at float offset

@@ -320,6 +320,7 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
   const size_t itw = put(tw);
   // Transposed northern halves of qi, qj, qu, qv ([mode][pair]).
   size_t qt[4];
+  std::vector<float> grid_tables[2];
   const char* tnames[4] = {"qi", "qj", "qu", "qv"};
   for (int i = 0; i < 4; ++i) {
     const Vec& q = s.q.at(tnames[i]);
@@ -328,6 +329,7 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
     for (int j = 0; j < JH; ++j)
       for (int w = 0; w < d.NCSP; ++w) t[(size_t)w * JH + j] = q[(size_t)j * d.NCSP + w];
     qt[i] = put(t);
+    if (i < 2 && e->mode == 1) grid_tables[i] = grid_table_layout(d, t);
   }
   // Tensor-core transforms (mode 2): hi/lo images of every table operand per m.
   std::vector<int> tc_at;
@@ -340,6 +342,7 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
     return at;
   };
   const size_t itc = put_floats(img);
+  const size_t igi = put_floats(grid_tables[0]), igj = put_floats(grid_tables[1]);
   check(cudaMalloc(&e->shared_buf, buf.size() * sizeof(float)), "shared tables");
   check(cudaMemcpy(e->shared_buf, buf.data(), buf.size() * sizeof(float), cudaMemcpyHostToDevice), "shared tables");
   check(cudaMalloc(&e->mode_buf, (2 * d.NCSP + tc_at.size()) * sizeof(int)), "mode tables");
@@ -371,6 +374,8 @@ void upload_shared(exogcm_engine* e, const SharedSetup& s) {
   e->sh.qjT = b + qt[1];
   e->sh.quT = b + qt[2];
   e->sh.qvT = b + qt[3];
+  e->sh.qiG = b + igi;
+  e->sh.qjG = b + igj;
   e->sh.tc_img = b + itc;
   e->sh.tc_at = e->mode_buf + 2 * d.NCSP;
   e->sh.mode_m = e->mode_buf;

@@ -59,6 +59,10 @@ void tc_qtend(const Model& m, const float* u, const float* v, const float* src, 
 
 // fft.cu (optimized path; Fourier planes m-major)
 void fft_init();
+// The northern table (transposed, [mode][pair]) as the fused inverse
+// transform's blocks hold it: per chunk of 8 latitude pairs, one padded row
+// of modes per pair.
+std::vector<float> grid_table_layout(const Dims& d, const std::vector<double>& qT);
 // Shared memory of the fused inverse transform at 2 or 4 planes per pass.
 size_t grid_sp2gp_smem(const Dims& d, int planes_per_pass);
 void grid_init();

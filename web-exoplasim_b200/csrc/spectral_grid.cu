@@ -5,8 +5,10 @@
 // round trip through HBM.
 //
 // A block owns JR = 8 latitude pairs (16 rows of every plane) and walks a
-// range of planes two at a time. Its slice of the northern table is staged
-// once, pair-major ([pair][mode]): a row pitch of 4 (mod 32) banks and each
+// range of planes two (or four) at a time. Its slice of the northern table is
+// copied in once (16-byte asynchronous copies of a slice laid out in HBM as
+// it sits in shared memory), pair-major ([pair][mode]): a row pitch of 4
+// (mod 32) banks and each
 // wavenumber's modes starting at a position of residue u (mod 4), for the
 // wavenumber pair u that reads them, put the 32 lanes of a warp (8 pairs x 4
 // wavenumber pairs) on 32 distinct banks. Per plane pair:
@@ -26,17 +28,58 @@
 
 #include <algorithm>
 
+#include "async_copy.cuh"
 #include "common.cuh"
 #include "fft_core.cuh"
 #include "launch.h"
 
 namespace exogcm {
 
+// A block's slice of the northern table: JR latitude pairs, each a row of
+// grid_table_pitch floats holding every mode, wavenumber m's modes from
+// position grid_table_positions()[m]. The slices are laid out so in HBM
+// once per resolution (grid_table_layout), and a block copies its slice
+// into shared memory as it stands.
+constexpr int kGridPairs = 8;
+
+__host__ __device__ __forceinline__ int mode_start(int m, int ntp1) { return m * (2 * ntp1 - m + 1) / 2; }
+
+// Row pitch: every mode plus up to 3 floats of alignment gap per wavenumber,
+// rounded to 4 (mod 32) banks.
+__host__ __device__ constexpr int grid_table_pitch(int ntp1) {
+  return ntp1 * (ntp1 + 1) / 2 + 3 * ntp1 + ((((4 - (ntp1 * (ntp1 + 1) / 2 + 3 * ntp1)) % 32) + 32) % 32);
+}
+
+// m is read by wavenumber pair u = m (m < (NTP1 + 1) / 2) or u = NTP1 - 1 - m,
+// and its modes start at a position of residue u (mod 4).
+__host__ __device__ __forceinline__ void grid_table_positions(int ntp1, int* pos) {
+  const int groups = (ntp1 + 1) / 2;
+  int at = 0;
+  for (int m = 0; m < ntp1; ++m) {
+    const int u = m < groups ? m : ntp1 - 1 - m;
+    at += ((u - at) % 4 + 4) % 4;
+    pos[m] = at;
+    at += ntp1 - m;
+  }
+}
+
+std::vector<float> grid_table_layout(const Dims& d, const std::vector<double>& qT) {
+  const int JH = d.NLAT / 2, chunks = JH / kGridPairs, TP = grid_table_pitch(d.NTP1);
+  std::vector<int> pos(d.NTP1);
+  grid_table_positions(d.NTP1, pos.data());
+  std::vector<float> out((size_t)chunks * kGridPairs * TP, 0.f);
+  for (int c = 0; c < chunks; ++c)
+    for (int jj = 0; jj < kGridPairs; ++jj) {
+      float* row = out.data() + ((size_t)c * kGridPairs + jj) * TP;
+      for (int m = 0, w = 0; m < d.NTP1; ++m)
+        for (int k = 0; k < d.NTP1 - m; ++k, ++w) row[pos[m] + k] = (float)qT[(size_t)w * JH + c * kGridPairs + jj];
+    }
+  return out;
+}
+
 namespace {
 
 using namespace fftcore;
-
-__device__ __forceinline__ int mode_start(int m, int ntp1) { return m * (2 * ntp1 - m + 1) / 2; }
 
 template <int Q, int PPASS = 2>
 struct GridShape {
@@ -44,7 +87,7 @@ struct GridShape {
   static constexpr int M = F::M, N = F::N, NTP1 = F::NTP1, T = F::T;
   static constexpr int NLAT = M, JH = M / 2;
   static constexpr int NCSP = NTP1 * (NTP1 + 1) / 2;
-  static constexpr int JR = 8;            // latitude pairs per block
+  static constexpr int JR = kGridPairs;   // latitude pairs per block
   static constexpr int ROWS = 2 * JR;     // rows of a plane
   static constexpr int PP = PPASS;        // planes per pass (2 or 4)
   static constexpr int NPAIR = PP / 2;    // plane pairs per pass
@@ -52,8 +95,8 @@ struct GridShape {
   static constexpr int THREADS = FROWS * T;
   static constexpr int GROUPS = (NTP1 + 1) / 2;
   static constexpr int TASKS = GROUPS * JR * NPAIR;
-  static constexpr int TL = NCSP + 3 * NTP1;                       // table row: modes plus alignment gaps
-  static constexpr int TP = TL + (((4 - TL) % 32) + 32) % 32;      // row pitch, 4 (mod 32)
+  static constexpr int TP = grid_table_pitch(NTP1);                // table row pitch, 4 (mod 32)
+  static_assert((JR * TP) % 4 == 0, "a table slice is whole 16-byte chunks");
   static constexpr int PITCH = (ROWS + (((16 / T - ROWS) % 16) + 16) % 16);
   static constexpr int FC = NTP1 * PITCH;  // float2s of one plane's coefficient stage
   static constexpr int SPEC = NPAIR * NCSP;  // float4s of the spectral stage ([pair][mode], two planes each)
@@ -61,6 +104,7 @@ struct GridShape {
   static constexpr int SHARED = (2 * SPEC > XB ? 2 * SPEC : XB);  // float2s of the union
   static constexpr int R = (SPEC + THREADS - 1) / THREADS;        // spectral float4s per thread
   static_assert((N + 9 * Q + PP * FC) % 2 == 0, "the spectral stage must start 16-byte aligned");
+  static_assert((N + 9 * Q + PP * FC + SHARED) % 2 == 0, "the table slice must start 16-byte aligned");
   static size_t smem() {
     return ((size_t)N + 9 * Q + (size_t)PP * FC + SHARED) * sizeof(float2) + (size_t)JR * TP * sizeof(float) +
            (size_t)NTP1 * sizeof(int);
@@ -80,7 +124,7 @@ __device__ __forceinline__ int stage_lat(int rr, int j0) {
 template <int Q, int PP>
 __global__ void __launch_bounds__(GridShape<Q, PP>::THREADS)
     k_sp2gp(const float* __restrict__ s, float* __restrict__ f, float* __restrict__ g, int planes, int per_block,
-            const float* __restrict__ qT, const int* __restrict__ mode_m, const float2* __restrict__ twg, int odd,
+            const float* __restrict__ qT, const float2* __restrict__ twg, int odd,
             int keep) {
   using G = GridShape<Q, PP>;
   constexpr int T = G::T, M = G::M, N = G::N, NTP1 = G::NTP1, JR = G::JR, JH = G::JH, TP = G::TP;
@@ -129,25 +173,18 @@ __global__ void __launch_bounds__(GridShape<Q, PP>::THREADS)
     }
   };
 
+  {
+    // the block's table slice, laid out in HBM as it sits here
+    const float4* src = reinterpret_cast<const float4*>(qT + (size_t)(j0 / JR) * JR * TP);
+    float4* dst = reinterpret_cast<float4*>(tab);
+    for (int i = threadIdx.x; i < JR * TP / 4; i += G::THREADS) cp_async16(dst + i, src + i);
+    cp_async_commit();
+  }
   if (pbeg < pend) fetch(pbeg);
   load_twiddles<Q>(twg, tw, twq);
-  if (threadIdx.x == 0) {
-    // m is read by wavenumber pair u = m (m < GROUPS) or u = NTP1 - 1 - m
-    int at = 0;
-    for (int m = 0; m < NTP1; ++m) {
-      const int u = m < G::GROUPS ? m : NTP1 - 1 - m;
-      at += ((u - at) % 4 + 4) % 4;
-      tpos[m] = at;
-      at += NTP1 - m;
-    }
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < NCSP * JR; i += G::THREADS) {
-    const int w = i / JR, jj = i - w * JR;
-    const int m = mode_m[w];
-    tab[jj * TP + tpos[m] + (w - mode_start(m, NTP1))] = qT[(size_t)w * JH + j0 + jj];
-  }
+  if (threadIdx.x == 0) grid_table_positions(NTP1, tpos);
   store();
+  cp_async_wait_all();
   __syncthreads();
 
   const float sg = odd ? -1.f : 1.f;
@@ -252,7 +289,7 @@ void launch_sp2gp(const Model& m, const float* s, float* f, float* g, int planes
   const int splits = std::max(1, std::min(passes, (target + chunks - 1) / chunks));
   const int per_passes = (passes + splits - 1) / splits;
   const int blocks = chunks * ((passes + per_passes - 1) / per_passes);
-  k_sp2gp<Q, PP><<<blocks, G::THREADS, smem, st>>>(s, f, g, planes, PP * per_passes, qT, m.sh.mode_m,
+  k_sp2gp<Q, PP><<<blocks, G::THREADS, smem, st>>>(s, f, g, planes, PP * per_passes, qT,
                                                     reinterpret_cast<const float2*>(m.sh.tw), odd, m.keep_fourier);
 }
 
@@ -282,7 +319,7 @@ size_t grid_sp2gp_smem(const Dims& d, int planes_per_pass) {
 }
 
 void grid_sp2gp(const Model& m, const float* s, float* f, float* g, int planes, bool derivative, cudaStream_t st) {
-  const float* qT = derivative ? m.sh.qjT : m.sh.qiT;
+  const float* qT = derivative ? m.sh.qjG : m.sh.qiG;
   const int odd = derivative ? 1 : 0;
   const bool four = m.tune.sp2gp_planes == 4;
   switch (m.d.NLON) {
