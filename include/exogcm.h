@@ -276,7 +276,9 @@ int exogcm_last_step_ms(exogcm_engine* engine, float* ms);
  * every slot and returns its mean device time per launch in *ms (CUDA events
  * on the engine's stream), with the algorithmic bytes one launch moves in
  * *bytes. Kernels: "fourier_forward", "fourier_inverse" (FFTs on the
- * optimized path, DFTs on the plain one), "legendre_forward",
+ * optimized path, DFTs on the plain one; "fourier_forward_per_chunk",
+ * "fourier_forward_persistent" and the same for "fourier_inverse" run the
+ * FFT in that form whatever the tuning chose), "legendre_forward",
  * "legendre_inverse", "sp2gp" (the fused inverse Legendre transform and FFT
  * of the optimized path; "sp2gp_planes2" and "sp2gp_planes4" run it at 2
  * or 4 planes per pass whatever the tuning chose), "dv2uv", "uv2dv", "qtend", "calcgp", "spectrala",
@@ -294,8 +296,10 @@ int exogcm_time_kernel(exogcm_engine* engine, const char* kernel, int reps, floa
  * [3], [4] the same for dv2uv; [5..8] forward Legendre planes per tile
  * for fc2sp, uv2dv, mktend's uv2dv and qtend; [9..12] (when count >= 13)
  * the staging buffers of those forward blocks (1 or 2); [13] (when count >=
- * 14) the planes per pass of the fused inverse transform (2 or 4). `count`
- * must be at least 9.
+ * 14) the planes per pass of the fused inverse transform (2 or 4); [14],
+ * [15] (when count >= 16) 1 where the forward / inverse FFT runs as
+ * persistent blocks looping over latitude chunks, 0 for one block per
+ * chunk. `count` must be at least 9.
  * The shapes split work differently but leave every result unchanged. */
 int exogcm_tuning(exogcm_engine* engine, int* values, int count);
 

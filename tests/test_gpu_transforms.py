@@ -125,3 +125,27 @@ def test_sp2gp_planes_per_pass_bitwise(truncation):
     for a, b in zip(got["sp2gp_planes2"], got["sp2gp_planes4"]):
         assert np.array_equal(a, b)
     assert np.isfinite(got["sp2gp_planes2"][0]).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("truncation", [21, 42, 63])
+def test_fft_forms_bitwise(truncation):
+    """The FFTs run as one block per latitude chunk or as persistent blocks
+    looping over chunks (the autotuner picks per direction); a row's
+    arithmetic is the same in both, so the Fourier and grid planes agree bit
+    for bit."""
+    e = pkg.Engine(truncation, 10, 3, mode=1)
+    for s in range(3):
+        e.configure(s, planets.make_planet(11 + s, truncation=truncation, levels=10))
+    e.step(3)
+    e.step(2)
+    t = e.tuning()["fft_persistent"]
+    assert t["forward"] in (0, 1) and t["inverse"] in (0, 1)
+    for direction, out in (("forward", "fgtn"), ("inverse", "gu")):
+        got = {}
+        for form in ("per_chunk", "persistent"):
+            e.time_kernel(f"fourier_{direction}_{form}", 1)
+            got[form] = [e.read(s, out).copy() for s in range(3)]
+        for a, b in zip(got["per_chunk"], got["persistent"]):
+            assert np.array_equal(a, b), direction
+        assert np.isfinite(got["persistent"][2]).all()

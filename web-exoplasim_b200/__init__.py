@@ -444,12 +444,12 @@ class Engine:
 
     def tuning(self) -> dict:
         """The transform launch shapes chosen at the first configure."""
-        v = (ctypes.c_int * 14)()
-        _check(_lib.exogcm_tuning(self.h, v, 14))
+        v = (ctypes.c_int * 16)()
+        _check(_lib.exogcm_tuning(self.h, v, 16))
         kinds = ("fc2sp", "uv2dv", "mktend", "qtend")
         return {"fft_rows": v[0], "sp2fc": (v[1], v[2]), "dv2uv": (v[3], v[4]),
                 "forward_tiles": dict(zip(kinds, v[5:9])), "forward_buffers": dict(zip(kinds, v[9:13])),
-                "sp2gp_planes": v[13]}
+                "sp2gp_planes": v[13], "fft_persistent": {"forward": v[14], "inverse": v[15]}}
 
     def graph_launches(self, steps: int) -> int:
         n = ctypes.c_size_t()

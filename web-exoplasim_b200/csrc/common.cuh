@@ -159,6 +159,7 @@ struct SharedTabs {
 // depend on them.
 struct Tuning {
   int fft_rows;      // latitudes per FFT block (a multiple of 8 dividing NLAT)
+  int fft_persistent[2];  // FFT blocks loop over chunks (1) or take one each (0): [0] forward, [1] inverse
   int inv_group[2];  // wavenumbers per inverse Legendre block: [0] sp2fc, [1] dv2uv
   int inv_tile[2];   // planes per inverse Legendre block (even)
   int fwd_tile[4];   // planes per forward Legendre tile (8 or 16), by kind

@@ -730,6 +730,20 @@ void autotune(exogcm_engine* e) {
       if (ms < best) best = ms, pick = rows;
     }
     t.fft_rows = pick;
+    // per direction: one block per chunk, or persistent blocks looping over chunks
+    for (int dir = 0; dir < 2; ++dir) {
+      float ms[2];
+      for (int form = 0; form < 2; ++form) {
+        t.fft_persistent[dir] = form;
+        ms[form] = time([&](const Model& m) {
+          if (dir == 0)
+            tr_fourier_forward(m, F.gtn, F.fgtn, LP, e->stream);
+          else
+            tr_fourier_inverse(m, F.fgu, F.gu, LP, e->stream);
+        });
+      }
+      t.fft_persistent[dir] = ms[1] < ms[0] ? 1 : 0;
+    }
   }
   for (int k = 0; k < 2; ++k) {
     float best = 1e30f;
@@ -1662,6 +1676,20 @@ int exogcm_time_kernel(exogcm_engine* e, const char* kernel, int reps, float* ms
     } else if (k == "fourier_inverse") {
       launch = [&] { tr_fourier_inverse(m, F.fgu, F.gu, LP, e->stream); };
       b = LP * (four + grid);
+    } else if (k == "fourier_forward_per_chunk" || k == "fourier_forward_persistent" ||
+               k == "fourier_inverse_per_chunk" || k == "fourier_inverse_persistent") {
+      // an FFT in a fixed form whatever the tuning chose
+      const bool forward = k.compare(0, 15, "fourier_forward") == 0;
+      const int form = k.size() > 10 && k.compare(k.size() - 10, 10, "persistent") == 0 ? 1 : 0;
+      launch = [&, forward, form] {
+        Model mp = m;
+        mp.tune.fft_persistent[forward ? 0 : 1] = form;
+        if (forward)
+          tr_fourier_forward(mp, F.gtn, F.fgtn, LP, e->stream);
+        else
+          tr_fourier_inverse(mp, F.fgu, F.gu, LP, e->stream);
+      };
+      b = LP * (grid + four);
     } else if (k == "legendre_forward") {
       launch = [&] { tr_legendre_forward(m, F.fgtdt, F.zstt1, LP, m.sh.qc, e->stream); };
       b = LP * (four + spec);
@@ -1748,10 +1776,11 @@ int exogcm_tuning(exogcm_engine* e, int* values, int count) {
   return guard([&] {
     if (!e || !values || count < 9) throw Error(EXOGCM_EINVAL, "need room for 9 values");
     const Tuning& t = e->tune;
-    const int v[14] = {t.fft_rows,      t.inv_group[0],   t.inv_tile[0],    t.inv_group[1],   t.inv_tile[1],
-                       t.fwd_tile[0],   t.fwd_tile[1],    t.fwd_tile[2],    t.fwd_tile[3],    t.fwd_buffers[0],
-                       t.fwd_buffers[1], t.fwd_buffers[2], t.fwd_buffers[3], t.sp2gp_planes};
-    std::copy(v, v + std::min(count, 14), values);
+    const int v[16] = {t.fft_rows,       t.inv_group[0],   t.inv_tile[0],      t.inv_group[1],
+                       t.inv_tile[1],    t.fwd_tile[0],    t.fwd_tile[1],      t.fwd_tile[2],
+                       t.fwd_tile[3],    t.fwd_buffers[0], t.fwd_buffers[1],   t.fwd_buffers[2],
+                       t.fwd_buffers[3], t.sp2gp_planes,   t.fft_persistent[0], t.fft_persistent[1]};
+    std::copy(v, v + std::min(count, 16), values);
   });
 }
 

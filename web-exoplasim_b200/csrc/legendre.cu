@@ -559,6 +559,7 @@ size_t leg_forward_smem(const Dims& d, int kind, int tile) {
 Tuning default_tuning(const Dims& d) {
   Tuning t{};
   t.fft_rows = 16;
+  t.fft_persistent[0] = t.fft_persistent[1] = 0;
   for (int k = 0; k < 2; ++k) {
     t.inv_tile[k] = d.NLAT == 32 ? 32 : 16;
     t.inv_group[k] = 1;
