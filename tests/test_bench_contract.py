@@ -102,3 +102,37 @@ def test_clock_summary_keeps_the_timed_region_and_its_reasons(tmp_path):
     clocks.t0, clocks.t1 = at(1.2).timestamp(), at(1.3).timestamp()
     short = clocks.summary()
     assert short["samples"] == 2 and short["sm_mhz"] == 1800 and short["reasons"] == []
+
+
+def test_profile_kernels_brackets_each_timed_launch():
+    """bench.py --profile-kernels: each kernel's untimed launch runs outside
+    the profiler range, its timed launch inside it, and one JSON line (not a
+    bench line) reports the event times and the tuning."""
+    bench = load_bench()
+    events = []
+
+    class Profiler:
+        def start(self):
+            events.append("start")
+
+        def stop(self):
+            events.append("stop")
+
+    fake_torch = types.SimpleNamespace(
+        cuda=types.SimpleNamespace(synchronize=lambda: None, profiler=Profiler()))
+
+    class Engine:
+        def time_kernel(self, kernel, reps):
+            events.append(kernel)
+            return 0.0123456, 1000.0
+
+        def tuning(self):
+            return {"fft_rows": 32}
+
+    out = io.StringIO()
+    with contextlib.redirect_stdout(out):
+        bench.profile_kernels(fake_torch, Engine(), ["sp2gp", "calcgp"])
+    assert events == ["sp2gp", "start", "sp2gp", "stop", "calcgp", "start", "calcgp", "stop"]
+    line = json.loads(out.getvalue())
+    assert "metric" not in line and line["tuning"] == {"fft_rows": 32}
+    assert line["profile_kernels"]["calcgp"] == {"ms": 0.0123, "algorithmic_bytes": 1000.0}
