@@ -376,6 +376,19 @@ def admission_latency(pkg, repeats=5):
     return {"unit": "ms per planet (median of %d)" % repeats, **out}
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or the platform's processor string."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for row in f:
+                if row.startswith("model name"):
+                    return row.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def reference_arm(args, rank):
     if rank != 0:
         return
@@ -393,7 +406,8 @@ def reference_arm(args, rank):
                    "planets": cores, "seq_len": None},
         "cpu_baseline": {"value": round(value, 4), "unit": "sim-days/s", "cores": cores, "kind": "port",
                          "sample": f"{cores} planets x {sample_steps} main-loop steps after the 3 "
-                                   f"start-up steps ({dt:.1f} s)"},
+                                   f"start-up steps ({dt:.1f} s)",
+                         "cpu_model": cpu_model(), "host_threads": os.cpu_count()},
         "e2e": {"value": round(value, 4), "unit": "sim-days/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's engines need WebGPU (graphics API, unavailable on this box) or its Wasm binary "
                 "(closed); its timestep is timed as the FP64 restatement on the host cores",
@@ -558,7 +572,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_baseline:
         v, dt = cpu_baseline_sample(plist, 1, 4)
         cpu = {"value": round(v, 5), "unit": "sim-days/s", "cores": 1, "kind": "port",
-               "sample": f"1 T42 L10 planet, 4 FP64 main-loop steps after start-up ({dt:.1f} s)"}
+               "sample": f"1 T42 L10 planet, 4 FP64 main-loop steps after start-up ({dt:.1f} s)",
+               "cpu_model": cpu_model(), "host_threads": os.cpu_count()}
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "sim-days/s", "n_gpus": world,

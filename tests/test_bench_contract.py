@@ -35,6 +35,7 @@ def test_reference_arm_prints_the_contract_line(monkeypatch):
                            "d2h_bytes_per_step": 0}
     cpu = line["cpu_baseline"]
     assert cpu["kind"] == "port" and cpu["cores"] == 2 and cpu["value"] == line["value"] and cpu["sample"]
+    assert cpu["cpu_model"] and cpu["host_threads"] >= 1
     assert line["config"]["workload"] and line["config"]["planets"] == 2
 
 
