@@ -408,8 +408,9 @@ class Engine:
 
     def snapshots_begin(self, out: np.ndarray) -> None:
         """Starts copying every slot's snapshot field ([plane][slot][point],
-        float32, pinned for overlap) while the caller goes on stepping; see
-        snapshots_wait. `out` must stay alive until then."""
+        float32, pinned for overlap) as the last submitted batch leaves it,
+        without waiting for batches in flight, while the caller goes on
+        stepping; see snapshots_wait. `out` must stay alive until then."""
         _check(_lib.exogcm_snapshots_begin(self.h, out.ctypes.data_as(_FP), out.size))
 
     def snapshots_wait(self) -> None:
